@@ -1,0 +1,167 @@
+#!/usr/bin/env python3
+"""Build the reference's own CPU solver code into oracle/_ref/ (test infrastructure).
+
+Recipe, run in the build container only (the reference tree is not present on
+the GPU machines; the built libraries travel there instead):
+
+1. Transcode the reference solver sources (GBK / UTF-16LE, CRLF) to UTF-8 in
+   oracle/_ref/src/.  Line numbers are unchanged, so file:line citations into
+   the reference still hold.
+2. Augment the *copy* of SphBase.h with the particle / threshold members that
+   the solver sources use but this revision of SphBase.h does not declare
+   (DFSPH.cpp, IISph_M.cpp and WcSph.cpp come from a later revision), a
+   `friend class RefHarness;` line, and an #ifdef around the real_t typedef.
+   Each edit is inserted at a fixed anchor (AUGMENT); nothing else changes.
+3. Compile SphBase.cpp + one solver .cpp + oracle/refshim/ref_harness.cpp into
+   one shared library per solver (DFSPH.h, IISph.h and IISph_M.h share the
+   include guard II_SPH_H_, so each solver needs its own library):
+       oracle/_ref/libref_dfsph.so, libref_wcsph.so, libref_pcisph.so,
+       libref_iisphm.so
+   Two precisions: real_t=float (the reference as shipped, SphBase.h:40) and
+   real_t=double (the typedef switch the reference itself describes,
+   SphBase.h:37-39) -> suffix _f64.  A third DFSPH variant,
+   libref_dfsph_capped.so, changes only the density loop's bookkeeping (double
+   sum, iteration cap) so that large scenes terminate; see DF_CAP.
+   Flags: -O3 -fopenmp, no -march (x86-64 SSE2, so no FMA contraction), which
+   is what the parity statements assume.
+
+Nothing is written outside oracle/_ref/.
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF = os.environ.get("SPH_REFERENCE_SOURCE", "/root/reference/Source")
+OUT = os.path.join(HERE, "_ref")
+SRC = os.path.join(OUT, "src")
+SHIM = os.path.join(HERE, "refshim")
+
+FILES = ["SphBase.h", "SphBase.cpp", "Vec23.h", "DFSPH.h", "DFSPH.cpp", "WcSph.h",
+         "WcSph.cpp", "PciSph.h", "PciSph.cpp", "IISph_M.h", "IISph_M.cpp"]
+
+# (anchor line in SphBase.h, text inserted after it).  The anchors are the last
+# member of FluidParticle (SphBase.h:117), of BoundaryParticle (SphBase.h:198)
+# and of ThresholdsBase (SphBase.h:582).
+AUGMENT = [
+    ("    real_t VF_divergenceDeviation;\n\n    std::vector<real_t> MT_restVolumeFraction;",
+     "    real_t density, density_adv, DFalpha, DFalpha2, DFkappa, DFkappaV, divergenceDeviation;\n"
+     "    vec_t DFalpha1, vel_adv, acce_adv, angular_velocity, omega, vorticity, vortical_angular_velocity,\n"
+     "        laplacian_angular_velocity, psi, n0Vorticity, n1Vorticity, deltaVorticity, dOmega;\n",
+     "before"),
+    ("    real_t DF_divergenceDeviation;\n};\n\n//see 9",
+     "    vec_t singleVelocity, angular_velocity;\n", "before_close"),
+    ("        real_t sum_energy;\n    } m_TH;",
+     "        int enable_vortex = 0; real_t nu = 0, nu_t = 0, zeta = 0, alpha = 0;\n", "after_first_line"),
+    # the oracle harness class reads private members (mg_NS, ker_* and
+    # ker_update_numbers, SphBase.h:680-800)
+    ("class SphBase{\n\npublic:\n", "    friend class RefHarness;\n", "after_anchor"),
+    # the precision switch the reference describes at SphBase.h:37-40
+    ("typedef float real_t;\n",
+     "#ifdef REF_REAL_DOUBLE\ntypedef double real_t;\n#else\n", "wrap_typedef"),
+]
+
+# DFSPH.cpp's density loop (DFSPH.cpp:225-231, 566, 627-631, 696) sums the
+# density in float and has no iteration cap.  The "capped" build changes that
+# bookkeeping only: the sum becomes double and the loop stops after
+# REF_DF_MAXITER iterations.  Used for CPU-baseline timing of large scenes.
+DF_CAP = [
+    ("\t\treal_t densitySum = 0;\n\t\tint maximumIteration = 50;",
+     "\t\tdouble densitySum = 0;\n\t\tint maximumIteration = 50;"),
+    ("\t\twhile (errorRate > errorRateGoal || currentIteration < minimumIteration)\n",
+     "\t\twhile ((errorRate > errorRateGoal || currentIteration < minimumIteration) && currentIteration < REF_DF_MAXITER)\n"),
+]
+
+SOLVERS = {
+    "dfsph": ("DFSPH.cpp", "DFSPH.h", "DFSPH", []),
+    "dfsph_capped": ("DFSPH_capped.cpp", "DFSPH.h", "DFSPH", ["-DREF_DF_MAXITER=100"]),
+    "wcsph": ("WcSph.cpp", "WcSph.h", "WcSph", []),
+    "pcisph": ("PciSph.cpp", "PciSph.h", "PciSph", ["-DPREDICTION_PCISPH"]),
+    "iisphm": ("IISph_M.cpp", "IISph_M.h", "IISph_M", ["-DIISPH"]),
+}
+
+
+def transcode(name):
+    raw = open(os.path.join(REF, name), "rb").read()
+    if raw[:2] in (b"\xff\xfe", b"\xfe\xff"):
+        text = raw.decode("utf-16")
+    else:
+        try:
+            text = raw.decode("utf-8")
+        except UnicodeDecodeError:
+            text = raw.decode("gbk", errors="replace")
+    return text.replace("\r\n", "\n")
+
+
+def augment(text):
+    for anchor, ins, mode in AUGMENT:
+        pos = text.find(anchor)
+        if pos < 0:
+            raise SystemExit("anchor not found in SphBase.h: %r" % anchor[:40])
+        if mode == "before":
+            cut = pos + anchor.index("\n\n") + 1
+        elif mode == "before_close":
+            cut = pos + anchor.index("};")
+        elif mode == "after_anchor":
+            cut = pos + len(anchor)
+        elif mode == "wrap_typedef":
+            text = text[:pos] + ins + anchor + "#endif\n" + text[pos + len(anchor):]
+            continue
+        else:
+            cut = pos + anchor.index("\n") + 1
+        text = text[:cut] + ins + text[cut:]
+    return text
+
+
+def write_if_changed(dst, t):
+    if not os.path.exists(dst) or open(dst).read() != t:
+        open(dst, "w").write(t)
+
+
+def main():
+    if not os.path.isdir(REF):
+        print("reference sources not present (%s); keeping prebuilt oracle/_ref" % REF)
+        return 0
+    os.makedirs(SRC, exist_ok=True)
+    for f in FILES:
+        t = transcode(f)
+        if f == "SphBase.h":
+            t = augment(t)
+        write_if_changed(os.path.join(SRC, f), t)
+        if f == "DFSPH.cpp":
+            for old, new in DF_CAP:
+                if old not in t:
+                    raise SystemExit("DFSPH.cpp anchor not found: %r" % old[:40])
+                t = t.replace(old, new, 1)
+            write_if_changed(os.path.join(SRC, "DFSPH_capped.cpp"), t)
+    jobs = []
+    for tag, (cpp, hdr, cls, defs) in SOLVERS.items():
+        for real, suffix in (("float", ""), ("double", "_f64")):
+            so = os.path.join(OUT, "libref_%s%s.so" % (tag, suffix))
+            deps = [os.path.join(SRC, cpp), os.path.join(SRC, "SphBase.cpp"),
+                    os.path.join(SHIM, "ref_harness.cpp"), os.path.join(SRC, "SphBase.h")]
+            if os.path.exists(so) and all(os.path.getmtime(so) >= os.path.getmtime(d) for d in deps):
+                continue
+            cmd = ["g++", "-std=c++17", "-O3", "-fopenmp", "-fPIC", "-shared", "-w",
+                   
+                   "-DREF_SOLVER_HEADER=\"%s\"" % hdr, "-DREF_SOLVER_CLASS=" + cls,
+                   "-DREF_TAG_" + tag, "-I" + SRC, "-I" + SHIM] + defs + [
+                   os.path.join(SRC, "SphBase.cpp"), os.path.join(SRC, cpp),
+                   os.path.join(SHIM, "ref_harness.cpp"), "-o", so]
+            if real == "double":
+                cmd.insert(1, "-DREF_REAL_DOUBLE")
+            jobs.append((so, cmd))
+    procs = [(so, subprocess.Popen(cmd, stderr=subprocess.PIPE)) for so, cmd in jobs]
+    rc = 0
+    for so, p in procs:
+        _, err = p.communicate()
+        if p.returncode:
+            sys.stderr.write(err.decode()[-4000:])
+            rc = 1
+        else:
+            print("built", os.path.relpath(so, HERE))
+    return rc
+
+
+if __name__ == "__main__":
+    sys.exit(main())
