@@ -1,0 +1,343 @@
+#!/usr/bin/env python3
+"""Benchmark: DFSPH particle-steps/s on the 1M-particle dam break.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one "step" = one DFSPH solver step, DFSPH::sphStep): 100x100x100
+fluid particles (r = 0.01 m, seeded +-0.1 r jitter) in a 4 x 2 x 2 m box with
+2-layer static walls; cubic spline support 4r; density loop to 0.01 % mean
+density error (FP64), divergence loop to 0.1 % (mean Drho/Dt * dt / rho0, FP64),
+both capped at 100 iterations; CFL dt = min(0.4 d / max|v|, 5e-3 s).
+
+ours      : the sm_100a kernels through libsphgpu.so (C ABI).  `value` is timed
+            with CUDA events on the scene's stream over K steps with all
+            inputs resident in HBM (each step one CUDA graph); `e2e` drives the
+            same steps through sphgpu_step_host with pinned host buffers
+            (positions and velocities copied in and out every step).
+reference : the reference's own DFSPH CPU code (oracle/_ref, OpenMP, all host
+            cores), same scene and goals, on a time-bounded sample of steps.
+
+Multi-GPU (torchrun, one rank per GPU): the single-scene workload does not
+shard, so every rank runs an independent replica ("replicas only"); value is
+the sum over ranks of particle-steps divided by the max-over-ranks time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "DFSPH particle-steps/s @1M, plain vs learned warm-start at 0.01% rho error"
+UNIT = "particle-steps/s"
+PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM = 6650.0
+
+# Algorithmic bytes per fluid particle of each kernel class (compulsory
+# traffic: own-particle state and the neighbour index list; neighbour state
+# gathers are cache traffic and not counted).  nb = mean stored neighbours.
+ALG_BYTES = {
+    "df_density_a": lambda nb: 16 + 16 + 4 + 4 + 4 + 4 * nb + 4 + 4 + 4,   # pos,vadv,rho,alpha,cnt,list | kr,kappa,rho_adv
+    "df_density_b": lambda nb: 16 + 16 + 4 + 4 + 4 * nb + 16,              # pos,vadv,kr,cnt,list | vadv
+    "df_div_a": lambda nb: 16 + 16 + 4 + 4 + 4 + 4 * nb + 4 + 4 + 4,
+    "df_div_b": lambda nb: 16 + 16 + 4 + 4 + 4 * nb + 16,
+    "df_forces": lambda nb: 16 + 16 + 4 + 4 + 4 * nb + 16 + 16,            # pos,vel,rho,cnt,list | acc,vadv
+    "build_first": lambda nb: 16 + 4 + 4 * nb + 4 + 4,                     # pos | list,cnt,rho,alpha
+    "hash": lambda nb: 16 + 16 + 4 + 16 + 16 + 4 + 4 + 4,                  # pos,vadv,gid | pos_s,vel_s,gid_s,key,slot
+    "reorder": lambda nb: 4 + 4 + 4 + 16 + 16 + 4 + 16 + 16 + 4 + 4 + 4,  # scatter + rank-reorder
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--profile-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--cpu-budget", type=float, default=60.0, help="seconds of reference CPU work per sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--scale", type=int, default=100, help="fluid block edge (100 -> 1M particles)")
+    return ap.parse_args()
+
+
+def workload(scale):
+    """The 1M-particle dam break (scale=100); smaller blocks in the same box
+    for quick checks."""
+    from graphics_b200.scene import dam_break
+    return dam_break((scale, scale, scale), 0.01, (4.0, 2.0, 2.0), seed=0)
+
+
+SOLVER_KW = dict(cfl=1, cfl_factor=0.4, dt_max=5e-3, dt_min=1e-6, dt=5e-3, nu=1e-3,
+                 df_density_goal=1e-4, df_density_min_iter=2, df_density_max_iter=100,
+                 df_div_goal_abs=0.0, df_div_goal_rel=1e-3, df_div_min_iter=1, df_div_max_iter=100)
+
+
+def config_dict(sc, extra=None):
+    d = {"workload": "dfsph_dam_break_%dk" % (sc.n_fluid // 1000), "n_fluid": sc.n_fluid,
+         "n_boundary": sc.n_boundary, "r": sc.r, "box": list(sc.meta["box"]), "cfl": 0.4, "dt_max": 5e-3,
+         "density_goal": 1e-4, "divergence_goal": 1e-3, "max_iter": 100, "neighbour_cap": 48,
+         "l2": "inputs larger than L2 (neighbour lists %.0f MB + state)" % (sc.n_fluid * 48 * 4 / 1e6)}
+    if extra:
+        d.update(extra)
+    return d
+
+
+def peaks():
+    try:
+        j = json.load(open(PEAKS))
+        return float(j["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM, "fallback"
+
+
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.p = None
+        self.path = os.path.join(ROOT, "gpurun_out", "clocks_%d.csv" % gpu_index)
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + self.QUERY,
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(5)
+            except Exception:
+                self.p.kill()
+            self.f.close()
+
+    def summary(self):
+        if not self.p:
+            return None
+        sm, mx, reasons = [], 0.0, set()
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference_sample(sc, budget, dt):
+    """Time the reference's own DFSPH (capped-bookkeeping build, OpenMP on all
+    host cores) on the same scene: steps from rest until `budget` seconds."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import make_scene_oracle
+    t0 = time.perf_counter()
+    o = make_scene_oracle(sc, kind="reference", solver="dfsph_capped", nu=SOLVER_KW["nu"], dt=dt)
+    setup = time.perf_counter() - t0
+    steps, t_run = 0, 0.0
+    while True:
+        t1 = time.perf_counter()
+        o.stage("runOneStep")
+        t_run += time.perf_counter() - t1
+        steps += 1
+        if t_run >= budget or steps >= 50:
+            break
+    cores = o.threads()
+    rho = o.get("density")
+    o.close()
+    return {"value": sc.n_fluid * steps / t_run, "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": "%d DFSPH step(s) of the %d-particle dam break from rest at fixed dt=%.1e s "
+                      "(reference DFSPH.cpp via oracle/_ref, float, density loop FP64-summed and capped at 100, "
+                      "divergence goal 0.1%% relative), setup %.1f s untimed" % (steps, sc.n_fluid, dt, setup),
+            "seconds": t_run, "mean_density": float(np.mean(rho))}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    sc = workload(args.scale)
+    try:
+        cb = cpu_reference_sample(sc, budget=max(30.0, args.cpu_budget * 2), dt=SOLVER_KW["dt_max"])
+    except Exception as e:  # the reference build is missing
+        print(json.dumps({"impl": "reference", "unavailable": "reference CPU build not loadable: %s" % e}))
+        return
+    v = cb["value"]
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sc.n_fluid / v,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded dam break)", "config": config_dict(sc, {"parallelism": "cpu-openmp"}),
+            "cpu_baseline": cb, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def run_ours(args):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    from graphics_b200.sph import scene_to_gpu
+
+    sc = workload(args.scale)
+    g = scene_to_gpu(sc, device=local, **SOLVER_KW)
+    stream = torch.cuda.ExternalStream(g.lib.sphgpu_stream(g.h), device=torch.device("cuda", local))
+
+    # warm-up (also builds the step graph)
+    g.step("dfsph", max(args.warmup, 1))
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        g.step_async("dfsph", args.steps)
+        e1.record(stream)
+        st = g.synchronize()
+        barrier()
+    ms = e0.elapsed_time(e1)
+    ms_max = ms
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    n_active = st["n_fluid"]
+    total_particle_steps = n_active * args.steps * world
+    value = total_particle_steps / (ms_max / 1e3)
+    it_rho = st["total_iter_density"] / args.steps
+    it_div = st["total_iter_divergence"] / args.steps
+    launches = args.steps * 13 + 2 * (st["total_iter_density"] + st["total_iter_divergence"])
+
+    # per-kernel durations: the same kernels as individual launches bracketed
+    # by CUDA events (host-driven loops), right after the timed region
+    g.profile(True)
+    g.step("dfsph", args.profile_steps)
+    prof = g.profile_read()
+    g.profile(False)
+    st_p = g.synchronize()
+    nb = st_p["mean_neighbours"]
+    hbm, peak_kind = peaks()
+    kern = {}
+    for k, (tot_ms, cnt) in prof.items():
+        ent = {"total_ms": round(tot_ms, 4), "launches": cnt, "avg_us": round(1e3 * tot_ms / max(cnt, 1), 2)}
+        if k in ALG_BYTES:
+            b = ALG_BYTES[k](nb) * st_p["n_fluid"]
+            ent["alg_bytes"] = int(b)
+            ent["gbs"] = round(b / (tot_ms / cnt / 1e3) / 1e9, 1)
+        kern[k] = ent
+    dom = max((k for k in kern if k in ALG_BYTES), key=lambda k: kern[k]["total_ms"])
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "dram_traffic_1m.json")
+    if os.path.exists(tf):
+        try:
+            traffic = json.load(open(tf)).get(dom)
+        except Exception:
+            traffic = None
+    roof = {"bound": "hbm", "kernel": dom, "achieved": kern[dom]["gbs"], "peak": hbm, "unit": "GB/s",
+            "frac": round(kern[dom]["gbs"] / hbm, 4), "traffic": traffic,
+            "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
+            "alg_bytes_per_particle": round(ALG_BYTES[dom](nb), 1), "mean_neighbours": round(nb, 2)}
+    # neighbour + density kernels (hash, scan, reorder, list build with rho/alpha)
+    ns_keys = [k for k in ("hash", "scan", "reorder", "build_first") if k in kern]
+    ns_ms = sum(kern[k]["total_ms"] / kern[k]["launches"] for k in ns_keys)
+    ns_bytes = sum(ALG_BYTES[k](nb) * st_p["n_fluid"] for k in ns_keys if k in ALG_BYTES)
+    roof["neighbour_density_group"] = {"kernels": ns_keys, "us_per_step": round(ns_ms * 1e3, 1),
+                                       "gbs": round(ns_bytes / (ns_ms / 1e3) / 1e9, 1),
+                                       "frac": round(ns_bytes / (ns_ms / 1e3) / 1e9 / hbm, 4)}
+
+    # end to end through the C ABI with pinned host buffers
+    e2e = None
+    if args.e2e_steps > 0:
+        n = g.n_fluid
+        pos = torch.empty((n, 3), dtype=torch.float32, pin_memory=True).numpy()
+        vel = torch.empty((n, 3), dtype=torch.float32, pin_memory=True).numpy()
+        pos[:] = g.get("position")
+        vel[:] = g.get("velocity")
+        po = torch.empty((n, 3), dtype=torch.float32, pin_memory=True).numpy()
+        vo = torch.empty((n, 3), dtype=torch.float32, pin_memory=True).numpy()
+        g.step_host("dfsph", pos, vel, po, vo)  # warm (graph for the restaged state)
+        pos[:], vel[:] = po, vo
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            g.step_host("dfsph", pos, vel, po, vo)
+            pos, po = po, pos
+            vel, vo = vo, vel
+        t1 = time.perf_counter()
+        sec = t1 - t0
+        if dist:
+            t = torch.tensor([sec], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            sec = float(t.item())
+        e2e = {"value": n * args.e2e_steps * world / sec, "unit": UNIT, "h2d_bytes_per_step": int(n * 24),
+               "d2h_bytes_per_step": int(n * 24), "steps": args.e2e_steps,
+               "note": "sphgpu_step_host: pinned positions+velocities in, step (with re-search), out"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_reference_sample(sc, budget=args.cpu_budget, dt=SOLVER_KW["dt_max"])
+        except Exception as e:
+            cpu = {"unavailable": str(e)}
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded dam break)",
+                "config": config_dict(sc, {"parallelism": "replicas x%d" % world if world > 1 else "single"}),
+                "iterations_per_step": {"density": it_rho, "divergence": it_div},
+                "last_step": {"err_density": st["err_density"], "err_divergence": st["err_divergence"],
+                              "dt": st["dt"], "status": st["status"], "neighbour_overflow": st["neighbour_overflow"]},
+                "roofline": roof, "kernels": kern, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+                "clocks": clk.summary()}
+        print(json.dumps(line))
+    g.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

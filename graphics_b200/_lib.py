@@ -1,0 +1,96 @@
+"""ctypes binding of libsphgpu.so (the C ABI declared in include/sphgpu.h).
+
+The library is built in-tree by graphics_b200/csrc/build.py.  There is no
+fallback: if the library cannot be loaded, or no CUDA device is present when
+a scene is created, the calls raise.
+"""
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsphgpu.so")
+
+OK, EINVAL, ENOMEM, ECUDA, EMAXITER, ENAN, ENEIGHBOUR_OVERFLOW, EOUT_OF_DOMAIN, ENOTIMPL = 0, -1, -2, -3, -4, -5, -6, -7, -8
+WCSPH, PCISPH, IISPH_M, DFSPH = 0, 1, 2, 3
+STATUS_MAXITER_DENSITY, STATUS_MAXITER_DIVERGENCE, STATUS_NAN = 1, 2, 4
+STATUS_NEIGHBOUR_OVERFLOW, STATUS_OUT_OF_DOMAIN, STATUS_ZERO_DISTANCE = 8, 16, 32
+
+_f3 = C.c_float * 3
+
+
+class SphParams(C.Structure):
+    _fields_ = [("spacing_r", C.c_float), ("smoothRadius_h", C.c_float), ("particle_d", C.c_float),
+                ("dt", C.c_float), ("gravity", _f3), ("spaceMin", _f3), ("spaceMax", _f3),
+                ("soundSpeed_cs", C.c_float), ("nu", C.c_float), ("densityErro_eta", C.c_float),
+                ("boundary_visc", C.c_float), ("max_neighbours", C.c_int),
+                ("df_density_goal", C.c_double), ("df_density_min_iter", C.c_int),
+                ("df_density_max_iter", C.c_int), ("df_div_goal_abs", C.c_double),
+                ("df_div_goal_rel", C.c_double), ("df_div_min_iter", C.c_int), ("df_div_max_iter", C.c_int),
+                ("cfl", C.c_int), ("cfl_factor", C.c_float), ("dt_max", C.c_float), ("dt_min", C.c_float),
+                ("wc_gamma", C.c_float), ("pci_min_iter", C.c_int), ("pci_max_iter", C.c_int),
+                ("ii_omega", C.c_float), ("ii_eta_rel", C.c_float), ("ii_min_iter", C.c_int),
+                ("ii_max_iter", C.c_int), ("warm_start", C.c_int), ("reserved", C.c_int * 7)]
+
+
+class SphStepStats(C.Structure):
+    _fields_ = [("n_fluid", C.c_int), ("iter_density", C.c_int), ("iter_divergence", C.c_int),
+                ("removed", C.c_int), ("err_density", C.c_double), ("err_divergence", C.c_double),
+                ("dt", C.c_double), ("status", C.c_uint32), ("neighbour_overflow", C.c_int),
+                ("zero_distance", C.c_int), ("max_neighbours_seen", C.c_int), ("mean_neighbours", C.c_double),
+                ("total_iter_density", C.c_int), ("total_iter_divergence", C.c_int), ("steps", C.c_int),
+                ("reserved", C.c_int * 5)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+# every symbol include/sphgpu.h declares, with (restype, argtypes)
+_vp, _i, _f, _d = C.c_void_p, C.c_int, C.c_float, C.c_double
+_fp, _ip, _cp = C.POINTER(C.c_float), C.POINTER(C.c_int), C.c_char_p
+SIGNATURES = {
+    "sphgpu_abi_version": (_i, []),
+    "sphgpu_params_default": (_i, [C.POINTER(SphParams)]),
+    "sphgpu_create": (_i, [C.POINTER(SphParams), _i, _i, C.POINTER(_vp)]),
+    "sphgpu_destroy": (_i, [_vp]),
+    "sphgpu_set_params": (_i, [_vp, C.POINTER(SphParams)]),
+    "sphgpu_set_boundary": (_i, [_vp, _i, _fp, _ip, _fp]),
+    "sphgpu_add_fluid": (_i, [_vp, _i, _fp, _fp, _f, _f]),
+    "sphgpu_num_fluid": (_i, [_vp]),
+    "sphgpu_step": (_i, [_vp, _i, _i, C.POINTER(SphStepStats)]),
+    "sphgpu_step_async": (_i, [_vp, _i, _i]),
+    "sphgpu_synchronize": (_i, [_vp, C.POINTER(SphStepStats)]),
+    "sphgpu_step_host": (_i, [_vp, _i, _fp, _fp, _fp, _fp, C.POINTER(SphStepStats)]),
+    "sphgpu_get_fluid": (_i, [_vp, _cp, _fp]),
+    "sphgpu_set_fluid": (_i, [_vp, _cp, _fp]),
+    "sphgpu_get_boundary": (_i, [_vp, _cp, _fp]),
+    "sphgpu_stage": (_i, [_vp, _cp, C.POINTER(SphStepStats)]),
+    "sphgpu_get_neighbours": (_i, [_vp, _ip, _ip, _ip]),
+    "sphgpu_get_cells": (_i, [_vp, C.POINTER(C.c_longlong)]),
+    "sphgpu_stream": (_vp, [_vp]),
+    "sphgpu_profile": (_i, [_vp, _i]),
+    "sphgpu_profile_read": (_i, [_vp, _cp, _i, C.POINTER(C.c_double), _ip, _i]),
+    "sphgpu_last_error": (_i, [_vp, _cp, _i]),
+}
+EXTRA = {"sphgpu_debug_set": (_i, [_vp, _cp, _i])}
+
+_lib = None
+
+
+def load():
+    """Load libsphgpu.so (raises OSError if it is missing or unloadable)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError("libsphgpu.so not built (run graphics_b200/csrc/build.py): " + LIB_PATH)
+        lib = C.CDLL(LIB_PATH)
+        for name, (res, args) in {**SIGNATURES, **EXTRA}.items():
+            f = getattr(lib, name)
+            f.restype, f.argtypes = res, args
+        _lib = lib
+    return _lib
+
+
+class SphGpuError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("sphgpu error %d: %s" % (code, msg))
+        self.code = code

@@ -1,0 +1,155 @@
+// sph_common.cuh -- device-side definitions shared by the SPH kernels.
+//
+// Data layout in HBM (all fluid arrays in cell-sorted order, rebuilt every
+// neighbour search):
+//   pos   float4 (x, y, z, phase as int bits)   16 B/particle
+//   vel   float4 (vx, vy, vz, 0)                16 B/particle
+//   gid   int   global fluid index (phase-major insertion order; the
+//               reference's m_Fluids[k].fluidParticles[i] order)
+//   rho, alpha, ... float per particle
+//   nbr   int   ELL neighbour list, column-major: entry k of particle p at
+//               nbr[k * stride + p]; fluid neighbour j -> j, boundary
+//               neighbour b -> b | BND_FLAG
+//   boundary: bpos float4 (x, y, z, volume), bvel float4
+//
+// Cell keys: the reference's uniform grid (cell = smoothRadius_h,
+// SphBase.cpp:963-988) with cells enumerated brick by brick (4x4x4 bricks,
+// Morton order inside a brick) so that particles sorted by key are
+// spatially local in memory.  The reference's linear cell index
+// (SpaceGridStruct::gridOfPos, SphBase.h:700-701) is derived from the same
+// integer cell coordinates when a caller asks for it.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define BND_FLAG 0x80000000u
+#define BND_MASK 0x7fffffffu
+
+struct GridGeom {
+    float min[3];      // SpaceGridStruct::min = spaceMin - 2h
+    float divisor;     // 1/h
+    int num[3];        // cells per axis
+    int nb[3];         // 4x4x4 bricks per axis
+    int nkeys;         // nb.x*nb.y*nb.z*64 + 1 (last key: removed particles)
+};
+
+// Kernel constants of the reference's single-h cubic spline
+// (SphBase::ker_update_numbers, SphBase.h:808-829).
+struct KerConst {
+    float h, inv_h, theta, thetah;
+};
+
+struct SolverConst {
+    KerConst k;
+    float hs;          // smoothRadius_h (viscosity epsilon uses it)
+    float h2cut;       // (d + d)^2 neighbour cut (SphBase.cpp:883-886)
+    float dpart;       // particle diameter
+    float fm0;         // rho0 * spacing_r^3 (phase 0)
+    float rho0;        // phase 0 rest density
+    float gravity[3];
+    float nu;
+    float cs;
+    float visc_alpha;  // phase 0 artificial viscosity (WCSPH)
+    float bvisc;       // boundary viscosity alpha
+    float wc_B, wc_gamma;
+    float rho0_ph[4];  // per phase rest density
+    float fm_ph[4];    // per phase mass
+    float alpha_ph[4]; // per phase viscosity alpha
+    int nphase;
+    int cap;           // neighbour cap
+    int stride;        // ELL column stride (>= fluid capacity)
+};
+
+// -------- cubic spline, SphBase.h:840-889 (single-h forms) --------
+__device__ __forceinline__ float ker_W(const KerConst& k, float r) {
+    float q = r / k.h, qm2 = 2.f - q;
+    return q <= 1.f ? k.theta * (1.f - 1.5f * q * q + 0.75f * q * q * q)
+                    : k.theta * (0.25f * qm2 * qm2 * qm2);
+}
+__device__ __forceinline__ float ker_Wg(const KerConst& k, float r) {
+    float q = r / k.h, qm2 = 2.f - q;
+    return q <= 1.f ? k.thetah * (3.f * q - 2.25f * q * q) : k.thetah * 0.75f * qm2 * qm2;
+}
+// per-pair-h spline with range check, SphBase.h:855-871
+__device__ __forceinline__ float ker_W_h(float r, float h) {
+    float q = r / h, qm2 = 2.f - q;
+    float th = 1.f / 3.14159265358979323846f / (h * h * h);
+    if (!(q >= 0.f && q <= 2.f)) return 0.f;
+    return q <= 1.f ? th * (1.f - 1.5f * q * q + 0.75f * q * q * q) : th * (0.25f * qm2 * qm2 * qm2);
+}
+
+// Squared distance exactly as vec3::dis_square (Vec23.h:170-171) evaluates
+// it in float without contraction: ((dx*dx + dy*dy) + dz*dz).
+__device__ __forceinline__ float dis_square_rn(float ax, float ay, float az, float bx, float by, float bz) {
+    float dx = __fsub_rn(ax, bx), dy = __fsub_rn(ay, by), dz = __fsub_rn(az, bz);
+    return __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+}
+
+// Integer cell coordinate per axis: int((pos - min) * divisor), SphBase.h:700-701.
+__device__ __forceinline__ int cell_coord(float p, float mn, float div) {
+    return (int)__fmul_rn(__fsub_rn(p, mn), div);
+}
+
+__device__ __forceinline__ int morton2x3(int x, int y, int z) {
+    return (x & 1) | ((y & 1) << 1) | ((z & 1) << 2) | ((x & 2) << 2) | ((y & 2) << 3) | ((z & 2) << 4);
+}
+
+__device__ __forceinline__ int cell_key(const GridGeom& g, int cx, int cy, int cz) {
+    int b = ((cz >> 2) * g.nb[1] + (cy >> 2)) * g.nb[0] + (cx >> 2);
+    return b * 64 + morton2x3(cx & 3, cy & 3, cz & 3);
+}
+
+__device__ __forceinline__ bool cell_inside(const GridGeom& g, int cx, int cy, int cz) {
+    return cx >= 0 && cy >= 0 && cz >= 0 && cx < g.num[0] && cy < g.num[1] && cz < g.num[2];
+}
+
+__device__ __forceinline__ int phase_of(float4 p) { return __float_as_int(p.w); }
+
+// ---- reductions ----
+template <int NT>
+__device__ __forceinline__ double block_sum_double(double v, double* sh) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    double r = 0;
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int i = 0; i < NT / 32; ++i) r += sh[i];
+    }
+    __syncthreads();
+    return r;  // valid in thread 0
+}
+
+template <int NT>
+__device__ __forceinline__ int block_sum_int(int v, int* sh) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    int r = 0;
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int i = 0; i < NT / 32; ++i) r += sh[i];
+    }
+    __syncthreads();
+    return r;
+}
+
+template <int NT>
+__device__ __forceinline__ int block_max_int(int v, int* sh) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_down_sync(0xffffffffu, v, o));
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    int r = 0;
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int i = 0; i < NT / 32; ++i) r = max(r, sh[i]);
+    }
+    __syncthreads();
+    return r;
+}

@@ -1,0 +1,1072 @@
+// sph_engine.cu -- host engine behind the C ABI in include/sphgpu.h.
+//
+// One sphgpu_scene owns the device buffers of one SPH scene, one CUDA stream
+// and the step graphs.  A DFSPH step is one CUDA graph: its two Jacobi loops
+// are conditional WHILE nodes whose bodies (two kernels each) decide on the
+// device whether another iteration runs, so a step needs no host round trip.
+// Profiling mode runs the same kernels as individual launches bracketed by
+// CUDA events (host-driven loops) to time each kernel class.
+#include <cub/device/device_scan.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/sphgpu.h"
+#include "sph_kernels.cuh"
+
+namespace {
+
+struct EvPair {
+    const char* name;
+    cudaEvent_t a, b;
+};
+
+struct Prof {
+    bool on = false;
+    std::vector<cudaEvent_t> pool;
+    size_t used = 0;
+    std::vector<EvPair> pending;
+    std::map<std::string, std::pair<double, int>> acc;
+};
+
+}  // namespace
+
+struct sphgpu_scene {
+    SphParams P;
+    int device = 0;
+    cudaStream_t stream = nullptr, stream2 = nullptr;
+    int cap = 0, stride = 0, ncap = 48;
+    GridGeom g{};
+    SolverConst c{};
+    DevScene d{};
+    std::vector<float> rho0_ph, alpha_ph;
+    std::vector<int> phase_n;
+    int n_total = 0;  // particles known to the host (before removals)
+    bool ns_valid = false, in_staging = true;
+    int frame = 0;
+    double time = 0;
+    void* cub_tmp = nullptr;
+    size_t cub_bytes = 0;
+    DevStats* h_stats = nullptr;
+    int* h_cont = nullptr;
+    // graphs: key -> exec
+    std::map<int, cudaGraphExec_t> graphs;
+    bool use_graphs = true;
+    Prof prof;
+    std::string err;
+    std::vector<int> bgid_h;
+    std::vector<int> bsolid_h;
+    int nb = 0;
+    bool have_kwarm = false;
+    int record_ksum = 0;
+    long long total_removed = 0;  // gid stays a permutation of [0, n) while 0
+};
+
+namespace {
+
+#define CK(x)                                                                                 \
+    do {                                                                                      \
+        cudaError_t e_ = (x);                                                                 \
+        if (e_ != cudaSuccess) {                                                              \
+            h->err = std::string(#x) + ": " + cudaGetErrorString(e_);                         \
+            return SPHGPU_ECUDA;                                                              \
+        }                                                                                     \
+    } while (0)
+
+#define CKV(x)                                                                                \
+    do {                                                                                      \
+        cudaError_t e_ = (x);                                                                 \
+        if (e_ != cudaSuccess && h->err.empty()) h->err = std::string(#x) + ": " + cudaGetErrorString(e_); \
+    } while (0)
+
+inline int roundup(int a, int b) { return (a + b - 1) / b * b; }
+
+inline float int_bits_as_float(int v) {
+    float f;
+    memcpy(&f, &v, sizeof f);
+    return f;
+}
+
+// ---- profiling launch wrapper ----
+template <class F>
+void launch(sphgpu_scene* h, const char* name, cudaStream_t st, F&& f) {
+    if (h->prof.on) {
+        if (h->prof.used + 2 > h->prof.pool.size()) {
+            for (int i = 0; i < 64; ++i) {
+                cudaEvent_t e;
+                cudaEventCreate(&e);
+                h->prof.pool.push_back(e);
+            }
+        }
+        cudaEvent_t a = h->prof.pool[h->prof.used++], b = h->prof.pool[h->prof.used++];
+        cudaEventRecord(a, st);
+        f();
+        cudaEventRecord(b, st);
+        h->prof.pending.push_back({name, a, b});
+    } else {
+        f();
+    }
+}
+
+void prof_collect(sphgpu_scene* h) {
+    if (!h->prof.on) return;
+    cudaStreamSynchronize(h->stream);
+    for (auto& p : h->prof.pending) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, p.a, p.b);
+        auto& e = h->prof.acc[p.name];
+        e.first += ms;
+        e.second += 1;
+    }
+    h->prof.pending.clear();
+    h->prof.used = 0;
+}
+
+// Grid geometry exactly as SpaceGridStruct::initialize computes it in float
+// (SphBase.cpp:963-988), plus the brick enumeration of the cell keys.
+GridGeom make_grid(const SphParams& P) {
+    GridGeom g{};
+    float hr = P.smoothRadius_h;
+    for (int i = 0; i < 3; ++i) g.min[i] = P.spaceMin[i] - hr * 2;
+    g.divisor = 1 / hr;
+    for (int i = 0; i < 3; ++i) {
+        float t = (P.spaceMax[i] - P.spaceMin[i]) + hr * 2;
+        g.num[i] = (int)(t * g.divisor) + 2;
+        g.nb[i] = (g.num[i] + 3) / 4;
+    }
+    g.nkeys = g.nb[0] * g.nb[1] * g.nb[2] * 64 + 1;
+    return g;
+}
+
+void fill_solver_const(sphgpu_scene* h) {
+    const SphParams& P = h->P;
+    SolverConst& c = h->c;
+    // ker_update_numbers, SphBase.h:808-829 (float arithmetic)
+    float kh = P.smoothRadius_h / 2;
+    c.k.h = kh;
+    c.k.inv_h = 1.f / kh;
+    c.k.theta = 1 / (float)M_PI / (kh * kh * kh);
+    c.k.thetah = 1 / (float)M_PI / (kh * kh * kh) / kh;
+    c.hs = P.smoothRadius_h;
+    float dd = P.particle_d + P.particle_d;
+    c.h2cut = (float)std::pow((double)dd, 2);
+    c.dpart = P.particle_d;
+    float v0 = (float)std::pow((double)P.spacing_r, 3);
+    c.nphase = (int)h->rho0_ph.size();
+    for (int i = 0; i < 4; ++i) {
+        float r0 = i < c.nphase ? h->rho0_ph[i] : 1000.f;
+        c.rho0_ph[i] = r0;
+        c.fm_ph[i] = r0 * v0;
+        c.alpha_ph[i] = i < c.nphase ? h->alpha_ph[i] : 0.f;
+    }
+    c.rho0 = c.rho0_ph[0];
+    c.fm0 = c.fm_ph[0];
+    for (int i = 0; i < 3; ++i) c.gravity[i] = P.gravity[i];
+    c.nu = P.nu;
+    c.cs = P.soundSpeed_cs;
+    c.visc_alpha = c.alpha_ph[0];
+    c.bvisc = P.boundary_visc;
+    c.wc_gamma = P.wc_gamma;
+    c.wc_B = c.rho0 * P.soundSpeed_cs * P.soundSpeed_cs / P.wc_gamma;
+    c.cap = h->ncap;
+    c.stride = h->stride;
+}
+
+template <class T>
+int dalloc(sphgpu_scene* h, T** p, size_t n) {
+    cudaError_t e = cudaMalloc((void**)p, std::max<size_t>(n, 1) * sizeof(T));
+    if (e != cudaSuccess) {
+        h->err = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+        return SPHGPU_ENOMEM;
+    }
+    return 0;
+}
+
+int alloc_scene(sphgpu_scene* h) {
+    const int n = h->cap;
+    DevScene& d = h->d;
+    int r = 0;
+    r |= dalloc(h, &d.pos, n); r |= dalloc(h, &d.vel, n); r |= dalloc(h, &d.gid, n);
+    r |= dalloc(h, &d.rho, n); r |= dalloc(h, &d.alpha, n); r |= dalloc(h, &d.vadv, n);
+    r |= dalloc(h, &d.acc, n); r |= dalloc(h, &d.kr, n); r |= dalloc(h, &d.kappa, n);
+    r |= dalloc(h, &d.ksum, n); r |= dalloc(h, &d.aux0, n); r |= dalloc(h, &d.aux1, n);
+    r |= dalloc(h, &d.aux4, n); r |= dalloc(h, &d.kwarm, n);
+    r |= dalloc(h, &d.pos_s, n); r |= dalloc(h, &d.vel_s, n); r |= dalloc(h, &d.gid_s, n);
+    r |= dalloc(h, &d.kwarm_s, n);
+    r |= dalloc(h, &d.key, n); r |= dalloc(h, &d.slot, n); r |= dalloc(h, &d.tmp, n);
+    r |= dalloc(h, &d.cell_count, (size_t)h->g.nkeys + 1);
+    r |= dalloc(h, &d.cell_start, (size_t)h->g.nkeys + 1);
+    r |= dalloc(h, &d.bcell_start, (size_t)h->g.nkeys + 1);
+    r |= dalloc(h, &d.nbr, (size_t)h->stride * h->ncap);
+    r |= dalloc(h, &d.ncount, n);
+    r |= dalloc(h, &d.partial, (size_t)n / 64 + 4096);
+    r |= dalloc(h, &d.st, 1);
+    if (r) return SPHGPU_ENOMEM;
+    d.cap_fluid = n;
+    d.dt = &d.st->dt;
+    d.nb = 0;
+    cudaMemsetAsync(d.st, 0, sizeof(DevStats), h->stream);
+    cudaMemsetAsync(d.bcell_start, 0, sizeof(int) * ((size_t)h->g.nkeys + 1), h->stream);
+    cudaMemsetAsync(d.ksum, 0, sizeof(float) * n, h->stream);
+    cudaMemsetAsync(d.kwarm, 0, sizeof(float) * n, h->stream);
+    cudaMemsetAsync(d.kwarm_s, 0, sizeof(float) * n, h->stream);
+    // CUB scan scratch
+    cub::DeviceScan::ExclusiveSum(nullptr, h->cub_bytes, d.cell_count, d.cell_start, h->g.nkeys + 1, h->stream);
+    if (cudaMalloc(&h->cub_tmp, h->cub_bytes + 16) != cudaSuccess) return SPHGPU_ENOMEM;
+    if (cudaMallocHost((void**)&h->h_stats, sizeof(DevStats)) != cudaSuccess) return SPHGPU_ENOMEM;
+    if (cudaMallocHost((void**)&h->h_cont, sizeof(int)) != cudaSuccess) return SPHGPU_ENOMEM;
+    memset(h->h_stats, 0, sizeof(DevStats));
+    float dt = h->P.dt;
+    cudaMemcpyAsync(d.dt, &dt, sizeof(float), cudaMemcpyHostToDevice, h->stream);
+    return cudaStreamSynchronize(h->stream) == cudaSuccess ? 0 : SPHGPU_ECUDA;
+}
+
+void free_scene(sphgpu_scene* h) {
+    DevScene& d = h->d;
+    void* ptrs[] = {d.pos, d.vel, d.gid, d.rho, d.alpha, d.vadv, d.acc, d.kr, d.kappa, d.ksum, d.aux0,
+                    d.aux1, d.aux4, d.kwarm, d.pos_s, d.vel_s, d.gid_s, d.kwarm_s, d.key, d.slot, d.tmp,
+                    d.cell_count, d.cell_start, d.bcell_start, d.nbr, d.ncount, d.partial, d.st,
+                    d.bpos, d.bvel, d.bgid, h->cub_tmp};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (h->h_stats) cudaFreeHost(h->h_stats);
+    if (h->h_cont) cudaFreeHost(h->h_cont);
+    for (auto& kv : h->graphs) cudaGraphExecDestroy(kv.second);
+    for (auto e : h->prof.pool) cudaEventDestroy(e);
+}
+
+// ---------------- step building blocks ----------------
+
+void enq_ns(sphgpu_scene* h, int integrate, int build_mode, cudaStream_t st) {
+    DevScene& d = h->d;
+    cudaMemsetAsync(d.cell_count, 0, sizeof(int) * ((size_t)h->g.nkeys + 1), st);
+    launch(h, "hash", st, [&] { launch_hash(d, h->g, h->P.spaceMin, h->P.spaceMax, integrate, h->cap, st); });
+    launch(h, "scan", st, [&] {
+        size_t b = h->cub_bytes;
+        cub::DeviceScan::ExclusiveSum(h->cub_tmp, b, d.cell_count, d.cell_start, h->g.nkeys + 1, st);
+    });
+    launch(h, "reorder", st, [&] { launch_scatter_reorder(d, h->g, h->cap, h->have_kwarm ? 1 : 0, st); });
+    launch_count_active(d, h->g, st);
+    launch(h, build_mode == 1 ? "build_first" : (build_mode == 2 ? "build_pressure" : "build"), st,
+           [&] { launch_build(d, h->g, h->c, build_mode, h->cap, st); });
+}
+
+// Jacobi loop: a conditional WHILE node while capturing, host-driven otherwise.
+template <class Body>
+int enq_loop(sphgpu_scene* h, bool capturing, Body&& body) {
+    if (capturing) {
+        cudaStreamCaptureStatus cs;
+        cudaGraph_t cg;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t ndeps = 0;
+        CK(cudaStreamGetCaptureInfo(h->stream, &cs, nullptr, &cg, &deps, &ndeps));
+        cudaGraphConditionalHandle handle;
+        CK(cudaGraphConditionalHandleCreate(&handle, cg, 1, cudaGraphCondAssignDefault));
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = handle;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        CK(cudaGraphAddNode(&node, cg, deps, ndeps, &cp));
+        CK(cudaStreamUpdateCaptureDependencies(h->stream, &node, 1, cudaStreamSetCaptureDependencies));
+        cudaGraph_t bodyg = cp.conditional.phGraph_out[0];
+        CK(cudaStreamBeginCaptureToGraph(h->stream2, bodyg, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+        body(h->stream2, (unsigned long long)handle, 1);
+        CK(cudaStreamEndCapture(h->stream2, &bodyg));
+        return 0;
+    }
+    for (int guard = 0; guard < 100000; ++guard) {
+        body(h->stream, 0ull, 0);
+        CK(cudaMemcpyAsync(h->h_cont, &h->d.st->cont, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        if (!*h->h_cont) break;
+    }
+    return 0;
+}
+
+int enq_df_density_loop(sphgpu_scene* h, bool capturing) {
+    DevScene& d = h->d;
+    const SphParams& P = h->P;
+    launch_df_loop_reset(d, 0, h->stream);
+    return enq_loop(h, capturing, [&](cudaStream_t st, unsigned long long hd, int use) {
+        launch(h, "df_density_a", st, [&] { launch_df_dens_a(d, h->c, h->cap, h->record_ksum, st); });
+        launch(h, "df_density_b", st, [&] {
+            launch_df_dens_b(d, h->c, h->cap, P.df_density_goal, P.df_density_min_iter, P.df_density_max_iter, hd,
+                             use, st);
+        });
+    });
+}
+
+int enq_df_div_loop(sphgpu_scene* h, bool capturing) {
+    DevScene& d = h->d;
+    const SphParams& P = h->P;
+    launch_df_loop_reset(d, 1, h->stream);
+    return enq_loop(h, capturing, [&](cudaStream_t st, unsigned long long hd, int use) {
+        launch(h, "df_div_a", st, [&] { launch_df_div_a(d, h->c, h->cap, st); });
+        launch(h, "df_div_b", st, [&] {
+            launch_df_div_b(d, h->c, h->cap, P.df_div_goal_abs, P.df_div_goal_rel, P.df_div_min_iter,
+                            P.df_div_max_iter, hd, use, st);
+        });
+    });
+}
+
+// The body of one DFSPH step after the first neighbour search
+// (DFSPH::sphStep, DFSPH.cpp:52-62).
+int enq_df_step(sphgpu_scene* h, bool capturing) {
+    DevScene& d = h->d;
+    cudaStream_t st = h->stream;
+    launch_step_begin(d, st);
+    if (h->P.cfl)
+        launch(h, "cfl", st, [&] { launch_cfl(d, h->cap, h->P.cfl_factor, h->P.particle_d, h->P.dt_max, h->P.dt_min, st); });
+    const int warm = h->P.warm_start && h->have_kwarm;
+    launch(h, "df_forces", st, [&] { launch_df_forces(d, h->c, h->cap, warm, st); });
+    if (warm) launch(h, "df_warm", st, [&] { launch_df_warm_correction(d, h->c, h->cap, st); });
+    int r = enq_df_density_loop(h, capturing);
+    if (r) return r;
+    enq_ns(h, 1, 1, st);
+    r = enq_df_div_loop(h, capturing);
+    if (r) return r;
+    CK(cudaMemcpyAsync(h->h_stats, d.st, sizeof(DevStats), cudaMemcpyDeviceToHost, st));
+    return 0;
+}
+
+int run_initial_ns(sphgpu_scene* h, int build_mode) {
+    if (!h->in_staging) {
+        // state is in the sorted arrays: stage it (copy) so the sort sees it
+        int n = h->h_stats->n_active;
+        cudaMemcpyAsync(h->d.pos_s, h->d.pos, sizeof(float4) * n, cudaMemcpyDeviceToDevice, h->stream);
+        cudaMemcpyAsync(h->d.vel_s, h->d.vel, sizeof(float4) * n, cudaMemcpyDeviceToDevice, h->stream);
+        cudaMemcpyAsync(h->d.gid_s, h->d.gid, sizeof(int) * n, cudaMemcpyDeviceToDevice, h->stream);
+        cudaMemcpyAsync(h->d.kwarm_s, h->d.kwarm, sizeof(float) * n, cudaMemcpyDeviceToDevice, h->stream);
+    }
+    enq_ns(h, 0, build_mode, h->stream);
+    h->in_staging = false;
+    h->ns_valid = build_mode == 1;
+    CK(cudaMemcpyAsync(h->h_stats, h->d.st, sizeof(DevStats), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int graph_for(sphgpu_scene* h, int key, cudaGraphExec_t* out, int (*build)(sphgpu_scene*, bool)) {
+    auto it = h->graphs.find(key);
+    if (it != h->graphs.end()) {
+        *out = it->second;
+        return 0;
+    }
+    cudaGraph_t gph;
+    CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeRelaxed));
+    int r = build(h, true);
+    cudaError_t e = cudaStreamEndCapture(h->stream, &gph);
+    if (r) return r;
+    if (e != cudaSuccess) {
+        h->err = std::string("graph capture: ") + cudaGetErrorString(e);
+        return SPHGPU_ECUDA;
+    }
+    cudaGraphExec_t ex;
+    e = cudaGraphInstantiate(&ex, gph, 0);
+    cudaGraphDestroy(gph);
+    if (e != cudaSuccess) {
+        h->err = std::string("graph instantiate: ") + cudaGetErrorString(e);
+        return SPHGPU_ECUDA;
+    }
+    h->graphs[key] = ex;
+    *out = ex;
+    return 0;
+}
+
+int df_graph_build(sphgpu_scene* h, bool cap) { return enq_df_step(h, cap); }
+
+void invalidate_graphs(sphgpu_scene* h) {
+    for (auto& kv : h->graphs) cudaGraphExecDestroy(kv.second);
+    h->graphs.clear();
+}
+
+int status_to_rc(unsigned s) {
+    if (s & SPHGPU_STATUS_NAN) return SPHGPU_ENAN;
+    if (s & (SPHGPU_STATUS_MAXITER_DENSITY | SPHGPU_STATUS_MAXITER_DIVERGENCE)) return SPHGPU_EMAXITER;
+    return 0;
+}
+
+void fill_stats(sphgpu_scene* h, SphStepStats* o, int steps) {
+    if (!o) return;
+    const DevStats& s = *h->h_stats;
+    memset(o, 0, sizeof(*o));
+    o->n_fluid = s.n_active;
+    o->iter_density = s.it_density;
+    o->iter_divergence = s.it_div;
+    o->removed = s.removed;
+    o->err_density = s.err_density;
+    o->err_divergence = s.err_div;
+    o->dt = s.dt;
+    o->status = s.status;
+    o->neighbour_overflow = s.overflow;
+    o->zero_distance = s.zero_dis;
+    o->max_neighbours_seen = s.max_nbrs;
+    o->mean_neighbours = s.n_active ? (double)s.nbr_total / s.n_active : 0.0;
+    o->total_iter_density = s.total_it_density;
+    o->total_iter_divergence = s.total_it_div;
+    o->steps = steps;
+}
+
+int enq_steps(sphgpu_scene* h, int solver, int nsteps) {
+    if (solver != SPHGPU_DFSPH && solver != SPHGPU_WCSPH) {
+        h->err = "solver not available in this build";
+        return SPHGPU_ENOTIMPL;
+    }
+    if (h->h_stats->n_active <= 0 && h->n_total <= 0) {
+        h->err = "no fluid particles";
+        return SPHGPU_EINVAL;
+    }
+    if (solver == SPHGPU_DFSPH && h->rho0_ph.size() != 1) {
+        h->err = "DFSPH path supports one fluid phase";
+        return SPHGPU_ENOTIMPL;
+    }
+    // reset the per-call iteration totals
+    cudaMemsetAsync(&h->d.st->total_it_density, 0, sizeof(int) * 2, h->stream);
+    if (solver == SPHGPU_DFSPH) {
+        if (!h->ns_valid) {
+            int r = run_initial_ns(h, 1);
+            if (r) return r;
+        }
+        for (int s = 0; s < nsteps; ++s) {
+            if (h->use_graphs && !h->prof.on) {
+                cudaGraphExec_t ex;
+                int key = (h->P.warm_start && h->have_kwarm ? 1 : 0) | (h->record_ksum ? 2 : 0) | (h->P.cfl ? 4 : 0);
+                int r = graph_for(h, key, &ex, df_graph_build);
+                if (r) return r;
+                CK(cudaGraphLaunch(ex, h->stream));
+            } else {
+                int r = enq_df_step(h, false);
+                if (r) return r;
+                prof_collect(h);
+            }
+            h->frame++;
+        }
+        return 0;
+    }
+    // WCSPH: NS + density/pressure (fused), forces + integrate into staging
+    for (int s = 0; s < nsteps; ++s) {
+        if (!h->in_staging) {
+            int n = h->cap;
+            cudaMemcpyAsync(h->d.pos_s, h->d.pos, sizeof(float4) * n, cudaMemcpyDeviceToDevice, h->stream);
+            cudaMemcpyAsync(h->d.vel_s, h->d.vel, sizeof(float4) * n, cudaMemcpyDeviceToDevice, h->stream);
+            cudaMemcpyAsync(h->d.gid_s, h->d.gid, sizeof(int) * n, cudaMemcpyDeviceToDevice, h->stream);
+        }
+        launch_step_begin(h->d, h->stream);
+        enq_ns(h, 0, 2, h->stream);
+        launch(h, "wc_force", h->stream, [&] { launch_wc_force(h->d, h->c, h->cap, h->stream); });
+        h->in_staging = true;
+        h->ns_valid = false;
+        CK(cudaMemcpyAsync(h->h_stats, h->d.st, sizeof(DevStats), cudaMemcpyDeviceToHost, h->stream));
+        prof_collect(h);
+        h->frame++;
+    }
+    return 0;
+}
+
+// host-order gather helpers
+int download_gid(sphgpu_scene* h, std::vector<int>& gid, int& n, bool staging) {
+    CK(cudaStreamSynchronize(h->stream));
+    n = h->h_stats->n_active;
+    gid.resize(n);
+    if (n) CK(cudaMemcpy(gid.data(), staging ? h->d.gid_s : h->d.gid, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+// order[k] = sorted slot holding the k-th particle in reference order
+void ref_order(const std::vector<int>& gid, std::vector<int>& order) {
+    order.resize(gid.size());
+    std::iota(order.begin(), order.end(), 0);
+    std::sort(order.begin(), order.end(), [&](int a, int b) { return gid[a] < gid[b]; });
+}
+
+}  // namespace
+
+// ======================= C ABI =======================
+extern "C" {
+
+int sphgpu_abi_version(void) { return SPHGPU_ABI_VERSION; }
+
+int sphgpu_params_default(SphParams* p) {
+    if (!p) return SPHGPU_EINVAL;
+    memset(p, 0, sizeof(*p));
+    // SphBase::SphBase (SphBase.cpp:214-225), DFSPH/WcSph constructors
+    p->spacing_r = 0.1f;
+    p->smoothRadius_h = 0.2f;
+    p->particle_d = 0.1f;
+    p->dt = 0.001f;
+    p->gravity[1] = -9.8f;
+    for (int i = 0; i < 3; ++i) { p->spaceMin[i] = 0.f; p->spaceMax[i] = 1.f; }
+    p->soundSpeed_cs = 100.f;
+    p->nu = 0.f;
+    p->densityErro_eta = 0.01f;
+    p->boundary_visc = 0.f;
+    p->max_neighbours = 48;
+    p->df_density_goal = 1e-4;
+    p->df_density_min_iter = 2;
+    p->df_density_max_iter = 100;
+    p->df_div_goal_abs = 2.5;
+    p->df_div_goal_rel = 1e-3;
+    p->df_div_min_iter = 1;
+    p->df_div_max_iter = 30;
+    p->cfl = 0;
+    p->cfl_factor = 0.4f;
+    p->dt_max = 5e-3f;
+    p->dt_min = 1e-6f;
+    p->wc_gamma = 7.f;
+    p->pci_min_iter = 3;
+    p->pci_max_iter = 10;
+    p->ii_omega = 0.5f;
+    p->ii_eta_rel = 1e-3f;
+    p->ii_min_iter = 2;
+    p->ii_max_iter = 100;
+    p->warm_start = 0;
+    return 0;
+}
+
+int sphgpu_create(const SphParams* p, int device, int max_fluid, sphgpu_t* out) {
+    if (!p || !out || max_fluid <= 0) return SPHGPU_EINVAL;
+    if (p->max_neighbours <= 0 || p->max_neighbours > 128) return SPHGPU_EINVAL;
+    if (!(p->smoothRadius_h > 0) || !(p->particle_d > 0) || !(p->spacing_r > 0)) return SPHGPU_EINVAL;
+    for (int i = 0; i < 3; ++i)
+        if (!(p->spaceMax[i] > p->spaceMin[i])) return SPHGPU_EINVAL;
+    *out = nullptr;
+    sphgpu_scene* h = new sphgpu_scene();
+    h->P = *p;
+    h->device = device;
+    if (cudaSetDevice(device) != cudaSuccess) {
+        delete h;
+        return SPHGPU_ECUDA;
+    }
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&h->stream2, cudaStreamNonBlocking) != cudaSuccess) {
+        delete h;
+        return SPHGPU_ECUDA;
+    }
+    h->cap = max_fluid;
+    h->stride = roundup(max_fluid, 32);
+    h->ncap = p->max_neighbours;
+    h->g = make_grid(*p);
+    fill_solver_const(h);
+    int r = alloc_scene(h);
+    if (r) {
+        free_scene(h);
+        delete h;
+        return r;
+    }
+    *out = h;
+    return 0;
+}
+
+int sphgpu_destroy(sphgpu_t h) {
+    if (!h) return SPHGPU_EINVAL;
+    cudaSetDevice(h->device);
+    cudaStreamSynchronize(h->stream);
+    free_scene(h);
+    cudaStreamDestroy(h->stream);
+    cudaStreamDestroy(h->stream2);
+    delete h;
+    return 0;
+}
+
+int sphgpu_set_params(sphgpu_t h, const SphParams* p) {
+    if (!h || !p) return SPHGPU_EINVAL;
+    for (int i = 0; i < 3; ++i)
+        if (p->spaceMin[i] != h->P.spaceMin[i] || p->spaceMax[i] != h->P.spaceMax[i]) {
+            h->err = "the simulation domain is fixed at creation";
+            return SPHGPU_EINVAL;
+        }
+    if (p->smoothRadius_h != h->P.smoothRadius_h || p->max_neighbours != h->P.max_neighbours) {
+        h->err = "smoothRadius_h and max_neighbours are fixed at creation";
+        return SPHGPU_EINVAL;
+    }
+    cudaSetDevice(h->device);
+    h->P = *p;
+    fill_solver_const(h);
+    invalidate_graphs(h);
+    float dt = p->dt;
+    CK(cudaMemcpyAsync(h->d.dt, &dt, sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int sphgpu_set_boundary(sphgpu_t h, int n, const float* xyz, const int* solid_id, const float* volume) {
+    if (!h || n < 0 || (n > 0 && !xyz)) return SPHGPU_EINVAL;
+    cudaSetDevice(h->device);
+    DevScene& d = h->d;
+    if (d.bpos) { cudaFree(d.bpos); cudaFree(d.bvel); cudaFree(d.bgid); d.bpos = nullptr; }
+    h->nb = n;
+    d.nb = n;
+    std::vector<float4> bp(n);
+    for (int i = 0; i < n; ++i) bp[i] = make_float4(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], volume ? volume[i] : 0.f);
+    if (dalloc(h, &d.bpos, n) || dalloc(h, &d.bvel, n) || dalloc(h, &d.bgid, n)) return SPHGPU_ENOMEM;
+    std::vector<int> keys(n);
+    int* dkeys = nullptr;
+    if (dalloc(h, &dkeys, n)) return SPHGPU_ENOMEM;
+    CK(cudaMemcpy(d.bpos, bp.data(), sizeof(float4) * n, cudaMemcpyHostToDevice));
+    launch_boundary_keys(d.bpos, n, h->g, dkeys, h->stream);
+    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaMemcpy(keys.data(), dkeys, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    cudaFree(dkeys);
+    // reference insertion rank: solids in order, each in index order (the
+    // caller's order, grouped by solid id)
+    std::vector<int> rank(n);
+    {
+        std::vector<int> ord(n);
+        std::iota(ord.begin(), ord.end(), 0);
+        if (solid_id)
+            std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return solid_id[a] < solid_id[b]; });
+        for (int i = 0; i < n; ++i) rank[ord[i]] = i;
+    }
+    for (int i = 0; i < n; ++i)
+        if (keys[i] < 0) {
+            h->err = "boundary particle outside the grid";
+            return SPHGPU_EINVAL;
+        }
+    std::vector<int> perm(n);
+    std::iota(perm.begin(), perm.end(), 0);
+    std::sort(perm.begin(), perm.end(), [&](int a, int b) {
+        return keys[a] != keys[b] ? keys[a] < keys[b] : rank[a] > rank[b];
+    });
+    std::vector<float4> sp(n), sv(n, make_float4(0, 0, 0, 0));
+    h->bgid_h.resize(n);
+    h->bsolid_h.resize(n);
+    std::vector<int> start(h->g.nkeys + 1, 0);
+    for (int i = 0; i < n; ++i) {
+        sp[i] = bp[perm[i]];
+        h->bgid_h[i] = perm[i];
+        h->bsolid_h[i] = solid_id ? solid_id[perm[i]] : 0;
+        start[keys[perm[i]] + 1]++;
+    }
+    for (int k = 0; k < h->g.nkeys; ++k) start[k + 1] += start[k];
+    CK(cudaMemcpy(d.bpos, sp.data(), sizeof(float4) * n, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d.bvel, sv.data(), sizeof(float4) * n, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d.bgid, h->bgid_h.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d.bcell_start, start.data(), sizeof(int) * (h->g.nkeys + 1), cudaMemcpyHostToDevice));
+    if (!volume) {
+        launch_boundary_volume(d, h->g, h->P.particle_d, h->c.h2cut, h->ncap, h->stream);
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    invalidate_graphs(h);
+    h->ns_valid = false;
+    return 0;
+}
+
+int sphgpu_add_fluid(sphgpu_t h, int n, const float* xyz, const float* vel, float rho0, float visc_alpha) {
+    if (!h || n <= 0 || !xyz || !(rho0 > 0)) return SPHGPU_EINVAL;
+    if (h->rho0_ph.size() >= 4) { h->err = "at most 4 fluid phases"; return SPHGPU_EINVAL; }
+    cudaSetDevice(h->device);
+    CK(cudaStreamSynchronize(h->stream));
+    int cur = h->h_stats->n_active;
+    if (cur + n > h->cap) { h->err = "fluid capacity exceeded"; return SPHGPU_EINVAL; }
+    int phase = (int)h->rho0_ph.size();
+    // bring the existing particles into staging in reference order
+    std::vector<float4> P(cur + n), V(cur + n);
+    if (cur > 0) {
+        std::vector<int> gid;
+        int m;
+        if (download_gid(h, gid, m, h->in_staging)) return SPHGPU_ECUDA;
+        std::vector<float4> tp(m), tv(m);
+        CK(cudaMemcpy(tp.data(), h->in_staging ? h->d.pos_s : h->d.pos, sizeof(float4) * m, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(tv.data(), h->in_staging ? h->d.vel_s : h->d.vel, sizeof(float4) * m, cudaMemcpyDeviceToHost));
+        std::vector<int> order;
+        ref_order(gid, order);
+        for (int k = 0; k < m; ++k) { P[k] = tp[order[k]]; V[k] = tv[order[k]]; }
+    }
+    for (int i = 0; i < n; ++i) {
+        P[cur + i] = make_float4(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], int_bits_as_float(phase));
+        V[cur + i] = vel ? make_float4(vel[3 * i], vel[3 * i + 1], vel[3 * i + 2], 0.f) : make_float4(0, 0, 0, 0);
+    }
+    std::vector<int> G(cur + n);
+    std::iota(G.begin(), G.end(), 0);
+    CK(cudaMemcpy(h->d.pos_s, P.data(), sizeof(float4) * (cur + n), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->d.vel_s, V.data(), sizeof(float4) * (cur + n), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->d.gid_s, G.data(), sizeof(int) * (cur + n), cudaMemcpyHostToDevice));
+    h->h_stats->n_active = cur + n;
+    CK(cudaMemcpy(&h->d.st->n_active, &h->h_stats->n_active, sizeof(int), cudaMemcpyHostToDevice));
+    h->rho0_ph.push_back(rho0);
+    h->alpha_ph.push_back(visc_alpha);
+    h->phase_n.push_back(n);
+    h->n_total = cur + n;
+    fill_solver_const(h);
+    invalidate_graphs(h);
+    h->in_staging = true;
+    h->ns_valid = false;
+    return phase;
+}
+
+int sphgpu_num_fluid(sphgpu_t h) {
+    if (!h) return SPHGPU_EINVAL;
+    cudaStreamSynchronize(h->stream);
+    return h->h_stats->n_active;
+}
+
+int sphgpu_step_async(sphgpu_t h, int solver, int nsteps) {
+    if (!h || nsteps < 0) return SPHGPU_EINVAL;
+    cudaSetDevice(h->device);
+    h->err.clear();
+    return enq_steps(h, solver, nsteps);
+}
+
+int sphgpu_synchronize(sphgpu_t h, SphStepStats* stats) {
+    if (!h) return SPHGPU_EINVAL;
+    cudaSetDevice(h->device);
+    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaGetLastError());
+    h->total_removed += h->h_stats->removed;
+    fill_stats(h, stats, 0);
+    int rc = status_to_rc(h->h_stats->status);
+    if (rc == SPHGPU_ENAN) h->err = "non-finite particle state";
+    else if (rc == SPHGPU_EMAXITER) h->err = "solver loop reached its iteration cap";
+    return rc;
+}
+
+int sphgpu_step(sphgpu_t h, int solver, int nsteps, SphStepStats* stats) {
+    int r = sphgpu_step_async(h, solver, nsteps);
+    if (r) return r;
+    r = sphgpu_synchronize(h, stats);
+    if (stats) stats->steps = nsteps;
+    return r;
+}
+
+int sphgpu_step_host(sphgpu_t h, int solver, const float* xyz, const float* vel, float* xyz_out, float* vel_out,
+                     SphStepStats* stats) {
+    if (!h) return SPHGPU_EINVAL;
+    int r = 0;
+    if (xyz) r = sphgpu_set_fluid(h, "position", xyz);
+    if (!r && vel) r = sphgpu_set_fluid(h, "velocity", vel);
+    if (r) return r;
+    r = sphgpu_step(h, solver, 1, stats);
+    if (r && r != SPHGPU_EMAXITER) return r;
+    int r2 = 0;
+    if (xyz_out) r2 = sphgpu_get_fluid(h, "position", xyz_out) < 0 ? SPHGPU_ECUDA : 0;
+    if (!r2 && vel_out) r2 = sphgpu_get_fluid(h, "velocity", vel_out) < 0 ? SPHGPU_ECUDA : 0;
+    return r2 ? r2 : r;
+}
+
+int sphgpu_get_fluid(sphgpu_t h, const char* field, float* out) {
+    if (!h || !field || !out) return SPHGPU_EINVAL;
+    cudaSetDevice(h->device);
+    std::string f(field);
+    bool state = (f == "position" || f == "velocity");
+    bool staging = state && h->in_staging;
+    if (state && h->total_removed == 0) {
+        // device-side reorder into reference order, one copy out
+        CK(cudaStreamSynchronize(h->stream));
+        int n = h->h_stats->n_active;
+        const float4* src = f == "position" ? (staging ? h->d.pos_s : h->d.pos) : (staging ? h->d.vel_s : h->d.vel);
+        float* tmp3 = (float*)h->d.aux4;
+        launch_to_ref_order(src, staging ? h->d.gid_s : h->d.gid, n, tmp3, h->stream);
+        CK(cudaMemcpyAsync(out, tmp3, sizeof(float) * 3 * (size_t)n, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        return n;
+    }
+    std::vector<int> gid;
+    int n;
+    if (download_gid(h, gid, n, staging)) return SPHGPU_ECUDA;
+    std::vector<int> order;
+    ref_order(gid, order);
+    int comps = 1;
+    const void* src = nullptr;
+    bool f4 = false;
+    DevScene& d = h->d;
+    if (f == "position") { src = staging ? d.pos_s : d.pos; f4 = true; comps = 3; }
+    else if (f == "velocity") { src = staging ? d.vel_s : d.vel; f4 = true; comps = 3; }
+    else if (f == "vel_adv") { src = d.vadv; f4 = true; comps = 3; }
+    else if (f == "acce_adv" || f == "acceleration") { src = d.acc; f4 = true; comps = 3; }
+    else if (f == "density") src = d.rho;
+    else if (f == "DFalpha") src = d.alpha;
+    else if (f == "DFkappa" || f == "DFkappaV") src = d.kappa;
+    else if (f == "kappa_sum") src = d.ksum;
+    else if (f == "kappa_warm") src = d.kwarm;
+    else if (f == "density_adv" || f == "divergenceDeviation") src = d.aux0;
+    else if (f == "presure") src = d.kr;
+    else if (f == "neighbour_count") {
+        std::vector<int> cnt(n);
+        CK(cudaMemcpy(cnt.data(), d.ncount, sizeof(int) * n, cudaMemcpyDeviceToHost));
+        for (int k = 0; k < n; ++k) out[k] = (float)cnt[order[k]];
+        return n;
+    } else {
+        h->err = "unknown field " + f;
+        return SPHGPU_EINVAL;
+    }
+    if (f4) {
+        std::vector<float4> t(n);
+        CK(cudaMemcpy(t.data(), src, sizeof(float4) * n, cudaMemcpyDeviceToHost));
+        for (int k = 0; k < n; ++k) {
+            const float4& v = t[order[k]];
+            out[3 * k] = v.x; out[3 * k + 1] = v.y; out[3 * k + 2] = v.z;
+        }
+    } else {
+        std::vector<float> t(n);
+        CK(cudaMemcpy(t.data(), src, sizeof(float) * n, cudaMemcpyDeviceToHost));
+        for (int k = 0; k < n; ++k) out[k] = t[order[k]];
+    }
+    (void)comps;
+    return n;
+}
+
+int sphgpu_set_fluid(sphgpu_t h, const char* field, const float* in) {
+    if (!h || !field || !in) return SPHGPU_EINVAL;
+    cudaSetDevice(h->device);
+    std::string f(field);
+    std::vector<int> gid;
+    int n;
+    bool staging = h->in_staging && (f == "position" || f == "velocity");
+    if (download_gid(h, gid, n, staging)) return SPHGPU_ECUDA;
+    DevScene& d = h->d;
+    if ((f == "position" || f == "velocity") && h->total_removed == 0) {
+        float4* dst = f == "position" ? (staging ? d.pos_s : d.pos) : (staging ? d.vel_s : d.vel);
+        float* tmp3 = (float*)d.aux4;
+        CK(cudaMemcpyAsync(tmp3, in, sizeof(float) * 3 * (size_t)n, cudaMemcpyHostToDevice, h->stream));
+        launch_from_ref_order(tmp3, staging ? d.gid_s : d.gid, n, dst, h->stream);
+        if (f == "position" && !staging) {
+            h->ns_valid = false;
+            CK(cudaMemcpyAsync(d.pos_s, d.pos, sizeof(float4) * n, cudaMemcpyDeviceToDevice, h->stream));
+            CK(cudaMemcpyAsync(d.vel_s, d.vel, sizeof(float4) * n, cudaMemcpyDeviceToDevice, h->stream));
+            CK(cudaMemcpyAsync(d.gid_s, d.gid, sizeof(int) * n, cudaMemcpyDeviceToDevice, h->stream));
+            CK(cudaMemcpyAsync(d.kwarm_s, d.kwarm, sizeof(float) * n, cudaMemcpyDeviceToDevice, h->stream));
+            h->in_staging = true;
+        }
+        CK(cudaStreamSynchronize(h->stream));
+        return n;
+    }
+    if (f == "position" || f == "velocity") {
+        float4* dst = f == "position" ? (staging ? d.pos_s : d.pos) : (staging ? d.vel_s : d.vel);
+        std::vector<float4> t(n);
+        CK(cudaMemcpy(t.data(), dst, sizeof(float4) * n, cudaMemcpyDeviceToHost));
+        std::vector<int> order;
+        ref_order(gid, order);
+        for (int k = 0; k < n; ++k) {
+            float4& v = t[order[k]];
+            v.x = in[3 * k]; v.y = in[3 * k + 1]; v.z = in[3 * k + 2];
+        }
+        CK(cudaMemcpy(dst, t.data(), sizeof(float4) * n, cudaMemcpyHostToDevice));
+        if (f == "position" && !staging) {
+            // positions changed: lists and rho/alpha must be rebuilt
+            h->ns_valid = false;
+            // the sorted arrays are the state; stage them for the next sort
+            CK(cudaMemcpy(d.pos_s, d.pos, sizeof(float4) * n, cudaMemcpyDeviceToDevice));
+            CK(cudaMemcpy(d.vel_s, d.vel, sizeof(float4) * n, cudaMemcpyDeviceToDevice));
+            CK(cudaMemcpy(d.gid_s, d.gid, sizeof(int) * n, cudaMemcpyDeviceToDevice));
+            CK(cudaMemcpy(d.kwarm_s, d.kwarm, sizeof(float) * n, cudaMemcpyDeviceToDevice));
+            h->in_staging = true;
+        }
+        return n;
+    }
+    float* dst = nullptr;
+    if (f == "density") dst = d.rho;
+    else if (f == "DFalpha") dst = d.alpha;
+    else if (f == "kappa_warm") { dst = d.kwarm; h->have_kwarm = true; invalidate_graphs(h); }
+    else if (f == "kappa_sum") dst = d.ksum;
+    else { h->err = "field not settable: " + f; return SPHGPU_EINVAL; }
+    std::vector<int> order;
+    ref_order(gid, order);
+    std::vector<float> t(n);
+    for (int k = 0; k < n; ++k) t[order[k]] = in[k];
+    CK(cudaMemcpy(dst, t.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
+    return n;
+}
+
+int sphgpu_get_boundary(sphgpu_t h, const char* field, float* out) {
+    if (!h || !field || !out) return SPHGPU_EINVAL;
+    cudaSetDevice(h->device);
+    int n = h->nb;
+    std::vector<float4> t(n);
+    CK(cudaMemcpy(t.data(), h->d.bpos, sizeof(float4) * n, cudaMemcpyDeviceToHost));
+    std::string f(field);
+    for (int i = 0; i < n; ++i) {
+        int k = h->bgid_h[i];
+        if (f == "position") { out[3 * k] = t[i].x; out[3 * k + 1] = t[i].y; out[3 * k + 2] = t[i].z; }
+        else if (f == "volume") out[k] = t[i].w;
+        else { h->err = "unknown boundary field"; return SPHGPU_EINVAL; }
+    }
+    return n;
+}
+
+int sphgpu_stage(sphgpu_t h, const char* name, SphStepStats* stats) {
+    if (!h || !name) return SPHGPU_EINVAL;
+    cudaSetDevice(h->device);
+    h->err.clear();
+    std::string s(name);
+    DevScene& d = h->d;
+    cudaStream_t st = h->stream;
+    int r = 0;
+    launch_step_begin(d, st);
+    if (s == "neighbourSearch" || s == "DF_constantDensitySolverFirst" || s == "wc_computePressure") {
+        int mode = s == "wc_computePressure" ? 2 : 1;
+        if (h->in_staging) {
+            enq_ns(h, 0, mode, st);
+            h->in_staging = false;
+        } else {
+            launch_build(d, h->g, h->c, mode, h->cap, st);
+        }
+        h->ns_valid = mode == 1;
+    } else if (s == "DF_forceExceptPressure") {
+        if (h->in_staging) { h->err = "run neighbourSearch first"; return SPHGPU_EINVAL; }
+        launch_df_forces(d, h->c, h->cap, 0, st);
+    } else if (s == "DF_constantDensitySolverSecond") {
+        if (h->in_staging) { h->err = "run neighbourSearch first"; return SPHGPU_EINVAL; }
+        if (h->P.cfl) launch_cfl(d, h->cap, h->P.cfl_factor, h->P.particle_d, h->P.dt_max, h->P.dt_min, st);
+        int warm = h->P.warm_start && h->have_kwarm;
+        launch_df_forces(d, h->c, h->cap, warm, st);
+        if (warm) launch_df_warm_correction(d, h->c, h->cap, st);
+        r = enq_df_density_loop(h, false);
+        if (r) return r;
+        // integrate into staging (the reference updates positions in place)
+        cudaMemsetAsync(d.cell_count, 0, sizeof(int) * ((size_t)h->g.nkeys + 1), st);
+        launch_hash(d, h->g, h->P.spaceMin, h->P.spaceMax, 1, h->cap, st);
+        h->in_staging = true;
+        h->ns_valid = false;
+    } else if (s == "DF_divergenceFreeSolver") {
+        if (h->in_staging) { h->err = "run neighbourSearch first"; return SPHGPU_EINVAL; }
+        r = enq_df_div_loop(h, false);
+        if (r) return r;
+    } else if (s == "wc_computeForce") {
+        if (h->in_staging) { h->err = "run neighbourSearch first"; return SPHGPU_EINVAL; }
+        launch_wc_force(d, h->c, h->cap, st);
+        h->in_staging = true;
+        h->ns_valid = false;
+    } else {
+        h->err = "unknown stage " + s;
+        return SPHGPU_EINVAL;
+    }
+    CK(cudaMemcpyAsync(h->h_stats, d.st, sizeof(DevStats), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    CK(cudaGetLastError());
+    h->total_removed += h->h_stats->removed;
+    fill_stats(h, stats, 0);
+    return status_to_rc(h->h_stats->status);
+}
+
+int sphgpu_get_neighbours(sphgpu_t h, int* counts, int* t, int* idx) {
+    if (!h || !counts || !t || !idx) return SPHGPU_EINVAL;
+    cudaSetDevice(h->device);
+    if (h->in_staging) { h->err = "no neighbour lists (run neighbourSearch)"; return SPHGPU_EINVAL; }
+    std::vector<int> gid;
+    int n;
+    if (download_gid(h, gid, n, false)) return SPHGPU_ECUDA;
+    std::vector<int> cnt(n), L((size_t)h->stride * h->ncap);
+    CK(cudaMemcpy(cnt.data(), h->d.ncount, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(L.data(), h->d.nbr, sizeof(int) * L.size(), cudaMemcpyDeviceToHost));
+    std::vector<float4> pos(n);
+    CK(cudaMemcpy(pos.data(), h->d.pos, sizeof(float4) * n, cudaMemcpyDeviceToHost));
+    // phase starts in global fluid index space
+    std::vector<int> pstart(h->phase_n.size() + 1, 0);
+    for (size_t k = 0; k < h->phase_n.size(); ++k) pstart[k + 1] = pstart[k] + h->phase_n[k];
+    auto fluid_pidx = [&](int g, int& tt, int& ii) {
+        int k = 0;
+        while (k + 1 < (int)pstart.size() - 1 && g >= pstart[k + 1]) ++k;
+        tt = -(k + 1);
+        ii = g - pstart[k];
+    };
+    // boundary: solid ids and within-solid index
+    int ns = 0;
+    for (int v : h->bsolid_h) ns = std::max(ns, v + 1);
+    std::vector<int> solid_of(h->nb), idx_in_solid(h->nb);
+    {
+        std::vector<int> sid(h->nb);
+        for (int i = 0; i < h->nb; ++i) sid[h->bgid_h[i]] = h->bsolid_h[i];
+        std::vector<int> cntS(std::max(ns, 1), 0);
+        for (int g = 0; g < h->nb; ++g) { idx_in_solid[g] = cntS[sid[g]]++; solid_of[g] = sid[g]; }
+    }
+    std::vector<int> order;
+    ref_order(gid, order);
+    const int cap = h->ncap;
+    for (int k = 0; k < n; ++k) {
+        int p = order[k];
+        counts[k] = cnt[p];
+        for (int j = 0; j < cnt[p]; ++j) {
+            unsigned e = (unsigned)L[(size_t)j * h->stride + p];
+            int tt, ii;
+            if (e & BND_FLAG) {
+                int g = h->bgid_h[e & BND_MASK];
+                tt = solid_of[g] + 1;
+                ii = idx_in_solid[g];
+            } else {
+                fluid_pidx(gid[e], tt, ii);
+            }
+            t[(size_t)k * cap + j] = tt;
+            idx[(size_t)k * cap + j] = ii;
+        }
+    }
+    return cap;
+}
+
+int sphgpu_get_cells(sphgpu_t h, long long* cell) {
+    if (!h || !cell) return SPHGPU_EINVAL;
+    cudaSetDevice(h->device);
+    std::vector<float> p(3 * (size_t)std::max(1, h->h_stats->n_active));
+    int n = sphgpu_get_fluid(h, "position", p.data());
+    if (n < 0) return n;
+    // gridOfPos (SphBase.h:700-701) on the host from the same float values;
+    // the device computes keys with the identical round-to-nearest ops.
+    const GridGeom& g = h->g;
+    for (int i = 0; i < n; ++i) {
+        int c[3];
+        for (int a = 0; a < 3; ++a) {
+            volatile float t = p[3 * i + a] - g.min[a];
+            volatile float u = t * g.divisor;
+            c[a] = (int)u;
+        }
+        cell[i] = (long long)c[0] + (long long)c[1] * g.num[0] + (long long)c[2] * g.num[0] * g.num[1];
+    }
+    return n;
+}
+
+void* sphgpu_stream(sphgpu_t h) { return h ? (void*)h->stream : nullptr; }
+
+int sphgpu_profile(sphgpu_t h, int enable) {
+    if (!h) return SPHGPU_EINVAL;
+    h->prof.on = enable != 0;
+    h->prof.acc.clear();
+    return 0;
+}
+
+int sphgpu_profile_read(sphgpu_t h, char* names, int name_len, double* ms, int* launches, int cap) {
+    if (!h) return SPHGPU_EINVAL;
+    int i = 0;
+    for (auto& kv : h->prof.acc) {
+        if (i >= cap) break;
+        if (names) {
+            strncpy(names + (size_t)i * name_len, kv.first.c_str(), name_len - 1);
+            names[(size_t)i * name_len + name_len - 1] = 0;
+        }
+        if (ms) ms[i] = kv.second.first;
+        if (launches) launches[i] = kv.second.second;
+        ++i;
+    }
+    return i;
+}
+
+int sphgpu_last_error(sphgpu_t h, char* buf, int len) {
+    if (!h || !buf || len <= 0) return SPHGPU_EINVAL;
+    strncpy(buf, h->err.c_str(), len - 1);
+    buf[len - 1] = 0;
+    return (int)h->err.size();
+}
+
+// Internal controls used by the Python host layer (not part of the
+// reference-facing surface): record the summed density-loop stiffness per
+// particle (training labels for the warm-start network), and switch CUDA
+// graphs off (host-driven loops).
+int sphgpu_debug_set(sphgpu_t h, const char* key, int value) {
+    if (!h || !key) return SPHGPU_EINVAL;
+    std::string k(key);
+    if (k == "record_kappa_sum") { h->record_ksum = value; invalidate_graphs(h); return 0; }
+    if (k == "use_graphs") { h->use_graphs = value != 0; return 0; }
+    if (k == "reset_kappa_sum") {
+        cudaMemsetAsync(h->d.ksum, 0, sizeof(float) * h->cap, h->stream);
+        return cudaStreamSynchronize(h->stream) == cudaSuccess ? 0 : SPHGPU_ECUDA;
+    }
+    return SPHGPU_EINVAL;
+}
+
+}  // extern "C"

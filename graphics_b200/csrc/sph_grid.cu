@@ -1,0 +1,317 @@
+// sph_grid.cu -- uniform-grid neighbour search on the GPU.
+//
+// Replaces SphBase::gridSetup + SphBase::neighbourSearch
+// (SphBase.cpp:849-1089).  The reference inserts every particle at the head
+// of a per-cell linked list (solids first, then fluids, each in index order)
+// and walks the 27 surrounding cells (x fastest, then y, then z;
+// SphBase.cpp:980-986) and each list in list order, keeping a neighbour j when
+// its float squared distance is < (d_i + d_j)^2 and stopping at 48 entries.
+// The list order is therefore: per cell, fluids in descending (phase, index),
+// then solids in descending (solid, index).
+//
+// Here: one counting sort per step by cell key (atomic histogram, exclusive
+// scan, scatter), then a within-cell rank step that orders each cell's
+// particles by descending global index -- exactly the reference's list order
+// -- while reordering the particle state into the new layout.  Boundary
+// particles are sorted once into their own cell table.  The neighbour-list
+// kernel then walks the 27 cells in the reference's offset order, the fluid
+// range of a cell before its boundary range, so the stored lists (and which
+// entries a 48-cap truncates) are the reference's.  The cut test uses
+// round-to-nearest float ops in the reference's evaluation order, so the
+// neighbour sets are bit-identical.
+#include "sph_kernels.cuh"
+
+namespace {
+constexpr int NT = 256;
+
+__global__ void __launch_bounds__(NT) k_hash(DevScene s, GridGeom g, float3 smin, float3 smax, int integrate) {
+    const int n = s.st->n_active;
+    if (blockIdx.x == 0 && threadIdx.x == 0) s.st->pad0 = n;  // staged count
+    int i = blockIdx.x * NT + threadIdx.x;
+    int removed = 0, nan = 0;
+    if (i < n) {
+        float4 p, v;
+        if (integrate) {
+            // Second loop 2.4: velocity = vel_adv; position += velocity*dt
+            // (DFSPH.cpp:705-715), in round-to-nearest float ops.
+            float dt = *s.dt;
+            p = s.pos[i];
+            v = s.vadv[i];
+            p.x = __fadd_rn(p.x, __fmul_rn(v.x, dt));
+            p.y = __fadd_rn(p.y, __fmul_rn(v.y, dt));
+            p.z = __fadd_rn(p.z, __fmul_rn(v.z, dt));
+            v.w = 0.f;
+            s.pos_s[i] = p;
+            s.vel_s[i] = v;
+            s.gid_s[i] = s.gid[i];
+            if (s.kwarm_s) s.kwarm_s[i] = s.kwarm[i];
+        } else {
+            p = s.pos_s[i];
+        }
+        // SphFluid::removeOutsideParts test (SphBase.cpp:34-44, Vec23.h:193-194)
+        bool in = smin.x <= p.x && smin.y <= p.y && smin.z <= p.z && p.x <= smax.x && p.y <= smax.y &&
+                  p.z <= smax.z;
+        int key = g.nkeys - 1;
+        if (in) {
+            int cx = cell_coord(p.x, g.min[0], g.divisor);
+            int cy = cell_coord(p.y, g.min[1], g.divisor);
+            int cz = cell_coord(p.z, g.min[2], g.divisor);
+            if (cell_inside(g, cx, cy, cz)) key = cell_key(g, cx, cy, cz);
+            else removed = 1;
+        } else {
+            removed = 1;
+            if (!(isfinite(p.x) && isfinite(p.y) && isfinite(p.z))) nan = 1;
+        }
+        s.key[i] = key;
+        s.slot[i] = atomicAdd(&s.cell_count[key], 1);
+    }
+    if (__syncthreads_or(removed)) {
+        if (removed) atomicOr(&s.st->status, 16u | (nan ? 4u : 0u));
+    }
+}
+
+__global__ void __launch_bounds__(NT) k_scatter(DevScene s) {
+    const int n = s.st->pad0;
+    int i = blockIdx.x * NT + threadIdx.x;
+    if (i < n) s.tmp[s.cell_start[s.key[i]] + s.slot[i]] = i;
+}
+
+// For sorted slot q: its particle i, its cell range [a, b); its final place is
+// a + #{particles of the cell with larger global index}.
+__global__ void __launch_bounds__(NT) k_rank_reorder(DevScene s, int dead_key, int carry_kwarm) {
+    const int n = s.st->pad0;
+    int q = blockIdx.x * NT + threadIdx.x;
+    if (q >= n) return;
+    int i = s.tmp[q];
+    int key = s.key[i];
+    if (key == dead_key) return;
+    int a = s.cell_start[key], b = s.cell_start[key + 1];
+    int my = s.gid_s[i], cnt = 0;
+    for (int r = a; r < b; ++r) cnt += s.gid_s[s.tmp[r]] > my;
+    int p = a + cnt;
+    s.pos[p] = s.pos_s[i];
+    s.vel[p] = s.vel_s[i];
+    s.gid[p] = my;
+    if (carry_kwarm) s.kwarm[p] = s.kwarm_s[i];
+}
+
+__global__ void k_count_active(DevScene s, int dead_key) {
+    int staged = s.st->pad0;
+    int act = s.cell_start[dead_key];
+    s.st->removed += staged - act;
+    s.st->n_active = act;
+}
+
+// mode 0: neighbour lists only; 1: + DFSPH rho and alpha
+// (DF_constantDensitySolverFirst, DFSPH.cpp:84-193); 2: + WCSPH rho and Tait
+// pressure (WcSph::wc_computePressure, WcSph.cpp:99-153).
+template <int MODE>
+__global__ void __launch_bounds__(128) k_build(DevScene s, GridGeom g, SolverConst c) {
+    const int n = s.st->n_active;
+    int p = blockIdx.x * 128 + threadIdx.x;
+    int cnt = 0, over = 0;
+    bool act = p < n;
+    if (act) {
+        const float4 pa = s.pos[p];
+        const int ph = phase_of(pa);
+        const float fm0 = c.fm_ph[ph], rho0 = c.rho0_ph[ph];
+        const int cx = cell_coord(pa.x, g.min[0], g.divisor);
+        const int cy = cell_coord(pa.y, g.min[1], g.divisor);
+        const int cz = cell_coord(pa.z, g.min[2], g.divisor);
+        float density = ker_W(c.k, 0.f) * fm0;
+        float a1x = 0.f, a1y = 0.f, a1z = 0.f, a2 = 0.f;
+        int* out = s.nbr + p;
+        const int stride = c.stride, cap = c.cap;
+        for (int dz = -1; dz <= 1; ++dz)
+            for (int dy = -1; dy <= 1; ++dy)
+                for (int dx = -1; dx <= 1; ++dx) {
+                    int x = cx + dx, y = cy + dy, z = cz + dz;
+                    if (!cell_inside(g, x, y, z)) continue;
+                    int key = cell_key(g, x, y, z);
+                    int a = s.cell_start[key], b = s.cell_start[key + 1];
+                    for (int q = a; q < b; ++q) {
+                        if (q == p) continue;
+                        float4 pb = s.pos[q];
+                        float len2 = dis_square_rn(pa.x, pa.y, pa.z, pb.x, pb.y, pb.z);
+                        if (len2 < c.h2cut) {
+                            if (cnt < cap) {
+                                out[(size_t)cnt * stride] = q;
+                                ++cnt;
+                                if (MODE != 0) {
+                                    float dis = sqrtf(len2);
+                                    density += fm0 * ker_W(c.k, dis);
+                                    if (MODE == 1) {
+                                        float gs = -ker_Wg(c.k, dis);
+                                        float f = gs / dis;
+                                        a1x += (pa.x - pb.x) * f * fm0;
+                                        a1y += (pa.y - pb.y) * f * fm0;
+                                        a1z += (pa.z - pb.z) * f * fm0;
+                                        float t = gs * fm0;
+                                        a2 = (float)((double)a2 + (double)t * (double)t);
+                                    }
+                                }
+                            } else {
+                                ++over;
+                            }
+                        }
+                    }
+                    int ba = s.bcell_start[key], bb = s.bcell_start[key + 1];
+                    for (int q = ba; q < bb; ++q) {
+                        float4 pb = s.bpos[q];
+                        float len2 = dis_square_rn(pa.x, pa.y, pa.z, pb.x, pb.y, pb.z);
+                        if (len2 < c.h2cut) {
+                            if (cnt < cap) {
+                                out[(size_t)cnt * stride] = q | (int)BND_FLAG;
+                                ++cnt;
+                                if (MODE != 0) {
+                                    float dis = sqrtf(len2);
+                                    float vol = pb.w;
+                                    density += rho0 * vol * ker_W(c.k, dis);
+                                    if (MODE == 1) {
+                                        float gs = -ker_Wg(c.k, dis);
+                                        float f = gs / dis;
+                                        a1x += (pa.x - pb.x) * f * rho0 * vol;
+                                        a1y += (pa.y - pb.y) * f * rho0 * vol;
+                                        a1z += (pa.z - pb.z) * f * rho0 * vol;
+                                    }
+                                }
+                            } else {
+                                ++over;
+                            }
+                        }
+                    }
+                }
+        s.ncount[p] = cnt;
+        if (MODE == 1) {
+            s.rho[p] = density;
+            float al = a1x * a1x + a1y * a1y + a1z * a1z + a2;
+            if (al < 1.0e-6f) al = 1.0e-6f;
+            s.alpha[p] = density / al;
+        } else if (MODE == 2) {
+            s.rho[p] = density;
+            // Tait, WcSph.cpp:142-146 (NEGLECT_NEGATIVE_PRESSURE)
+            float pr = c.wc_B * (powf(density / rho0, c.wc_gamma) - 1.f);
+            if (pr < 0.f) pr = 0.f;
+            s.kr[p] = pr;
+        }
+    }
+    __shared__ int sh[4];
+    int tot = block_sum_int<128>(act ? cnt : 0, sh);
+    int ov = block_sum_int<128>(over, sh);
+    int mx = block_max_int<128>(act ? cnt : 0, sh);
+    if (threadIdx.x == 0) {
+        if (tot) atomicAdd(&s.st->nbr_total, (unsigned long long)tot);
+        if (ov) { atomicAdd(&s.st->overflow, ov); atomicOr(&s.st->status, 8u); }
+        if (mx) atomicMax(&s.st->max_nbrs, mx);
+    }
+}
+
+__global__ void k_boundary_keys(const float4* bpos, int nb, GridGeom g, int* keys) {
+    int i = blockIdx.x * NT + threadIdx.x;
+    if (i >= nb) return;
+    float4 p = bpos[i];
+    int cx = cell_coord(p.x, g.min[0], g.divisor);
+    int cy = cell_coord(p.y, g.min[1], g.divisor);
+    int cz = cell_coord(p.z, g.min[2], g.divisor);
+    keys[i] = cell_inside(g, cx, cy, cz) ? cell_key(g, cx, cy, cz) : -1;
+}
+
+// Boundary volume of a static rigid wall, SphBase::prepareSolidPartWeight
+// (SphBase.cpp:766-813) with only boundary particles in the grid:
+// V_b = 1 / (W(0, d) + sum over the (capped) boundary neighbour list of
+// W(dis, (d_a + d_b)/2)).
+__global__ void __launch_bounds__(128) k_boundary_volume(DevScene s, GridGeom g, float dpart, float h2cut, int cap) {
+    int p = blockIdx.x * 128 + threadIdx.x;
+    if (p >= s.nb) return;
+    float4 pa = s.bpos[p];
+    int cx = cell_coord(pa.x, g.min[0], g.divisor);
+    int cy = cell_coord(pa.y, g.min[1], g.divisor);
+    int cz = cell_coord(pa.z, g.min[2], g.divisor);
+    float h = dpart;
+    float sum = ker_W_h(0.f, h);
+    int cnt = 0;
+    float hp = (dpart + dpart) / 2;
+    for (int dz = -1; dz <= 1; ++dz)
+        for (int dy = -1; dy <= 1; ++dy)
+            for (int dx = -1; dx <= 1; ++dx) {
+                int x = cx + dx, y = cy + dy, z = cz + dz;
+                if (!cell_inside(g, x, y, z)) continue;
+                int key = cell_key(g, x, y, z);
+                int a = s.bcell_start[key], b = s.bcell_start[key + 1];
+                for (int q = a; q < b; ++q) {
+                    if (q == p) continue;
+                    float4 pb = s.bpos[q];
+                    float len2 = dis_square_rn(pa.x, pa.y, pa.z, pb.x, pb.y, pb.z);
+                    if (len2 < h2cut && cnt < cap) {
+                        ++cnt;
+                        sum += ker_W_h(sqrtf(len2), hp);
+                    }
+                }
+            }
+    s.bpos[p].w = 1.f / sum;
+}
+
+// Reference-order transfers: gid is a permutation of [0, n) while no
+// particle has been removed.
+__global__ void k_to_ref_order(const float4* src, const int* gid, int n, float* dst3) {
+    int p = blockIdx.x * NT + threadIdx.x;
+    if (p >= n) return;
+    float4 v = src[p];
+    size_t g = (size_t)gid[p] * 3;
+    dst3[g] = v.x;
+    dst3[g + 1] = v.y;
+    dst3[g + 2] = v.z;
+}
+__global__ void k_from_ref_order(const float* src3, const int* gid, int n, float4* dst) {
+    int p = blockIdx.x * NT + threadIdx.x;
+    if (p >= n) return;
+    size_t g = (size_t)gid[p] * 3;
+    float4 v = dst[p];
+    v.x = src3[g];
+    v.y = src3[g + 1];
+    v.z = src3[g + 2];
+    dst[p] = v;
+}
+}  // namespace
+
+static inline int nblk(int n, int nt) { return (n + nt - 1) / nt; }
+
+void launch_to_ref_order(const float4* src, const int* gid, int n, float* dst3, cudaStream_t st) {
+    if (n > 0) k_to_ref_order<<<nblk(n, NT), NT, 0, st>>>(src, gid, n, dst3);
+}
+void launch_from_ref_order(const float* src3, const int* gid, int n, float4* dst, cudaStream_t st) {
+    if (n > 0) k_from_ref_order<<<nblk(n, NT), NT, 0, st>>>(src3, gid, n, dst);
+}
+
+
+void launch_hash(const DevScene& s, const GridGeom& g, const float* smin, const float* smax, int integrate,
+                 int n_old, cudaStream_t st) {
+    k_hash<<<nblk(n_old > 0 ? n_old : 1, NT), NT, 0, st>>>(s, g, make_float3(smin[0], smin[1], smin[2]),
+                                                          make_float3(smax[0], smax[1], smax[2]), integrate);
+}
+
+void launch_scatter_reorder(const DevScene& s, const GridGeom& g, int n_old, int carry_kwarm, cudaStream_t st) {
+    int nb = nblk(n_old > 0 ? n_old : 1, NT);
+    k_scatter<<<nb, NT, 0, st>>>(s);
+    k_rank_reorder<<<nb, NT, 0, st>>>(s, g.nkeys - 1, carry_kwarm);
+}
+
+void launch_count_active(const DevScene& s, const GridGeom& g, cudaStream_t st) {
+    k_count_active<<<1, 1, 0, st>>>(s, g.nkeys - 1);
+}
+
+void launch_build(const DevScene& s, const GridGeom& g, const SolverConst& c, int mode, int n_max, cudaStream_t st) {
+    int nb = nblk(n_max > 0 ? n_max : 1, 128);
+    if (mode == 0) k_build<0><<<nb, 128, 0, st>>>(s, g, c);
+    else if (mode == 1) k_build<1><<<nb, 128, 0, st>>>(s, g, c);
+    else k_build<2><<<nb, 128, 0, st>>>(s, g, c);
+}
+
+void launch_boundary_keys(const float4* bpos, int nb, const GridGeom& g, int* keys, cudaStream_t st) {
+    if (nb > 0) k_boundary_keys<<<nblk(nb, NT), NT, 0, st>>>(bpos, nb, g, keys);
+}
+
+void launch_boundary_volume(const DevScene& s, const GridGeom& g, float dpart, float h2cut, int cap,
+                            cudaStream_t st) {
+    if (s.nb > 0) k_boundary_volume<<<nblk(s.nb, 128), 128, 0, st>>>(s, g, dpart, h2cut, cap);
+}

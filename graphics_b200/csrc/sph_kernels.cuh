@@ -1,0 +1,98 @@
+// sph_kernels.cuh -- kernel declarations and the device-side state shared by
+// the neighbour-search, DFSPH, WCSPH, PCISPH and IISPH kernels.
+#pragma once
+#include "sph_common.cuh"
+
+// Device statistics of the current step (one instance per scene, in device
+// memory; copied to pinned host memory at the end of each step).
+struct DevStats {
+    int n_active;          // fluid particles after the last neighbour search
+    int it_density;        // iterations of the current/last density loop
+    int it_div;            // iterations of the current/last divergence loop
+    int removed;           // particles removed this step
+    int overflow;          // pairs dropped by the neighbour cap
+    int zero_dis;          // zero-distance pairs
+    int max_nbrs;          // largest neighbour count
+    int cont;              // loop-continue flag (host-driven loops)
+    unsigned long long nbr_total;
+    unsigned status;
+    int total_it_density, total_it_div, steps, pad0;
+    double err_density, err_div;
+    double vmax;           // FP64 max |v| (CFL)
+    float dt;              // current step length
+    float pad1;
+    unsigned ticket[4];    // last-block tickets of the reductions
+};
+
+// Per-scene device pointers passed to every kernel by value.
+struct DevScene {
+    // fluid, cell-sorted
+    float4* pos;
+    float4* vel;
+    int* gid;
+    float* rho;
+    float* alpha;
+    float4* vadv;       // DFSPH advected velocity / WCSPH acceleration / scratch
+    float4* acc;        // a_adv (DFSPH) / acceleration (WCSPH) / pressure accel (PCISPH, IISPH)
+    float* kr;          // kappa/rho (DFSPH), pressure (WCSPH/PCISPH/IISPH)
+    float* kappa;       // DFkappa / DFkappaV of the last iteration (per particle)
+    float* ksum;        // summed kappa over the density loop (warm-start label)
+    float* aux0;        // rho_adv (DFSPH density), divergence deviation, aii (IISPH)
+    float* aux1;        // IISPH rho_adv, PCISPH rho*
+    float4* aux4;       // IISPH d_ii / sum d_ij p_j, PCISPH predicted position
+    float* kwarm;       // predicted initial kappa (learned warm start)
+    // staging (unsorted) copies used by the reorder
+    float4* pos_s;
+    float4* vel_s;
+    int* gid_s;
+    float* kwarm_s;
+    int* key;
+    int* slot;
+    int* tmp;
+    int* cell_count;    // nkeys + 1
+    int* cell_start;    // nkeys + 1
+    // neighbour lists (ELL, column-major)
+    int* nbr;
+    int* ncount;
+    // boundary, sorted once
+    float4* bpos;       // (x, y, z, volume)
+    float4* bvel;
+    int* bcell_start;   // nkeys + 1
+    int* bgid;          // boundary reference index (solid-major)
+    int nb;
+    int cap_fluid;      // fluid array capacity
+    // reductions
+    double* partial;    // >= number of blocks of a particle launch
+    DevStats* st;
+    float* dt;          // == &st->dt
+};
+
+// ---- neighbour search (sph_grid.cu) ----
+void launch_hash(const DevScene& s, const GridGeom& g, const float* smin, const float* smax, int integrate,
+                 int n_old, cudaStream_t st);
+void launch_scatter_reorder(const DevScene& s, const GridGeom& g, int n_old, int carry_kwarm, cudaStream_t st);
+void launch_count_active(const DevScene& s, const GridGeom& g, cudaStream_t st);
+// mode 0: lists only; 1: lists + DFSPH rho/alpha; 2: lists + WCSPH rho/pressure
+void launch_build(const DevScene& s, const GridGeom& g, const SolverConst& c, int mode, int n_max, cudaStream_t st);
+void launch_to_ref_order(const float4* src, const int* gid, int n, float* dst3, cudaStream_t st);
+void launch_from_ref_order(const float* src3, const int* gid, int n, float4* dst, cudaStream_t st);
+void launch_boundary_keys(const float4* bpos, int nb, const GridGeom& g, int* keys, cudaStream_t st);
+void launch_boundary_volume(const DevScene& s, const GridGeom& g, float dpart, float h2cut, int cap,
+                            cudaStream_t st);
+
+// ---- DFSPH (sph_dfsph.cu) ----
+void launch_df_first(const DevScene& s, const SolverConst& c, int n_max, cudaStream_t st);
+void launch_df_forces(const DevScene& s, const SolverConst& c, int n_max, int warm, cudaStream_t st);
+void launch_df_dens_a(const DevScene& s, const SolverConst& c, int n_max, int record, cudaStream_t st);
+void launch_df_dens_b(const DevScene& s, const SolverConst& c, int n_max, double goal, int min_it, int max_it,
+                      unsigned long long cond_handle, int use_handle, cudaStream_t st);
+void launch_df_div_a(const DevScene& s, const SolverConst& c, int n_max, cudaStream_t st);
+void launch_df_div_b(const DevScene& s, const SolverConst& c, int n_max, double goal_abs, double goal_rel,
+                     int min_it, int max_it, unsigned long long cond_handle, int use_handle, cudaStream_t st);
+void launch_df_warm_correction(const DevScene& s, const SolverConst& c, int n_max, cudaStream_t st);
+void launch_df_loop_reset(const DevScene& s, int which, cudaStream_t st);
+void launch_cfl(const DevScene& s, int n_max, float cfl, float d, float dt_max, float dt_min, cudaStream_t st);
+void launch_step_begin(const DevScene& s, cudaStream_t st);
+
+// ---- WCSPH (sph_wcsph.cu) ----
+void launch_wc_force(const DevScene& s, const SolverConst& c, int n_max, cudaStream_t st);

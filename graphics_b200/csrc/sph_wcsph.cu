@@ -1,0 +1,114 @@
+// sph_wcsph.cu -- WCSPH kernels (reference: WcSph.cpp).
+//
+// WcSph::sphStep (WcSph.cpp:23-96) is neighbourSearch -> wc_computePressure ->
+// wc_computeForce -> updateFluids.  The density + Tait pressure pass is fused
+// into the neighbour-list kernel (sph_grid.cu, mode 2); this file holds the
+// force pass, fused with the Euler-Cromer update (SphBase.cpp:377-402), which
+// writes the new state into the staging arrays that the next neighbour search
+// sorts.  Surface tension and adhesion (WcSph.cpp:188-211, 300-311) are not on
+// this path: they vanish for m_TH.r = m_TH.bt = 0, the plain method.
+#include "sph_kernels.cuh"
+
+namespace {
+constexpr int NT = 128;
+
+__global__ void __launch_bounds__(NT) k_wc_force(DevScene s, SolverConst c) {
+    const int n = s.st->n_active;
+    const int p = blockIdx.x * NT + threadIdx.x;
+    int zero = 0;
+    if (p < n) {
+        const float dt = *s.dt;
+        const float4 pa = s.pos[p];
+        const float4 va = s.vel[p];
+        const int ph = phase_of(pa);
+        const float ra = s.rho[p], pra = s.kr[p];
+        const float fma = c.fm_ph[ph], rho0 = c.rho0_ph[ph], alpha = c.alpha_ph[ph];
+        const float den0 = 0.01f * c.hs * c.hs;
+        const float pa_term = pra / (ra * ra);
+        float ax = c.gravity[0], ay = c.gravity[1], az = c.gravity[2];
+        const int cnt = s.ncount[p];
+        const int* L = s.nbr + p;
+        for (int k = 0; k < cnt; ++k) {
+            const unsigned e = (unsigned)L[(size_t)k * c.stride];
+            float acce;
+            float4 pb;
+            float xx, xy, xz, dis;
+            if (e & BND_FLAG) {
+                // wc_fluidPartForce_bound, WcSph.cpp:262-299
+                const unsigned b = e & BND_MASK;
+                pb = s.bpos[b];
+                const float4 vb = s.bvel[b];
+                xx = pa.x - pb.x; xy = pa.y - pb.y; xz = pa.z - pb.z;
+                const float len2 = xx * xx + xy * xy + xz * xz;
+                if (len2 == 0.f) { ++zero; continue; }
+                dis = sqrtf(len2);
+                const float grad = -ker_Wg(c.k, dis) / dis;
+                const float vol = pb.w;
+                acce = 0.f;
+                if (pra > 0.f) acce += grad * (-rho0 * vol * (pa_term * 2.f));
+                const float pro = (va.x - vb.x) * xx + (va.y - vb.y) * xy + (va.z - vb.z) * xz;
+                if (pro < 0.f) {
+                    const float nu = 2.f * c.bvisc * c.hs * c.cs / (ra * 2.f);
+                    const float pi = -nu * pro / (len2 + den0);
+                    acce += grad * (-rho0 * vol * pi);
+                }
+            } else {
+                pb = s.pos[e];
+                const float4 vb = s.vel[e];
+                xx = pa.x - pb.x; xy = pa.y - pb.y; xz = pa.z - pb.z;
+                const float len2 = xx * xx + xy * xy + xz * xz;
+                if (len2 == 0.f) { ++zero; continue; }
+                dis = sqrtf(len2);
+                const float grad = -ker_Wg(c.k, dis) / dis;
+                const float rb = s.rho[e], prb = s.kr[e];
+                const int phb = phase_of(pb);
+                const float pro = (va.x - vb.x) * xx + (va.y - vb.y) * xy + (va.z - vb.z) * xz;
+                if (phb == ph) {
+                    // wc_fluidPartForce_fsame, WcSph.cpp:174-187
+                    acce = grad * (-fma * (pa_term + prb / (rb * rb)));
+                    if (pro < 0.f) {
+                        const float nu = 2.f * alpha * c.hs * c.cs / (ra + rb);
+                        const float pi = -nu * pro / (len2 + den0);
+                        acce += grad * (-fma * pi);
+                    }
+                } else {
+                    // wc_fluidPartForce_fdiff, WcSph.cpp:239-253
+                    const float fmb = c.fm_ph[phb];
+                    const float al = (alpha + c.alpha_ph[phb]) / 2.f;
+                    const float da = ra / fma, db = rb / fmb;
+                    acce = grad * (-1.f / fma * (pra / (da * da) + prb / (db * db)));
+                    if (pro < 0.f) {
+                        const float nu = 2.f * al * c.hs * c.cs / (ra + rb);
+                        const float pi = -nu * pro / (len2 + den0);
+                        acce += grad * (-(fma + fmb) / 2.f * pi);
+                    }
+                }
+            }
+            ax += xx * acce;
+            ay += xy * acce;
+            az += xz * acce;
+        }
+        s.acc[p] = make_float4(ax, ay, az, 0.f);
+        // Euler-Cromer: v += a dt; x += v dt (SphBase.cpp:390-392)
+        float4 v, x;
+        v.x = __fadd_rn(va.x, __fmul_rn(ax, dt));
+        v.y = __fadd_rn(va.y, __fmul_rn(ay, dt));
+        v.z = __fadd_rn(va.z, __fmul_rn(az, dt));
+        v.w = 0.f;
+        x.x = __fadd_rn(pa.x, __fmul_rn(v.x, dt));
+        x.y = __fadd_rn(pa.y, __fmul_rn(v.y, dt));
+        x.z = __fadd_rn(pa.z, __fmul_rn(v.z, dt));
+        x.w = pa.w;
+        s.pos_s[p] = x;
+        s.vel_s[p] = v;
+        s.gid_s[p] = s.gid[p];
+    }
+    if (__syncthreads_or(zero)) {
+        if (zero) atomicAdd(&s.st->zero_dis, zero);
+    }
+}
+}  // namespace
+
+void launch_wc_force(const DevScene& s, const SolverConst& c, int n_max, cudaStream_t st) {
+    k_wc_force<<<(n_max + NT - 1) / NT, NT, 0, st>>>(s, c);
+}

@@ -1,0 +1,199 @@
+/*
+ * sphgpu.h -- C ABI of the B200 (sm_100a) SPH particle hot path.
+ *
+ * One handle = one SPH scene resident in GPU memory (fluid phases + static
+ * boundary particles), driven through the reference's solver step
+ * semantics.  Plain pointers and sizes only; caller arrays are borrowed for
+ * the duration of a call and never retained.  All functions return 0 on
+ * success or a negative SPHGPU_E* code; sphgpu_last_error() gives the text.
+ *
+ * Reference interfaces this replaces (Artemisaturn/GRAPHICS, Source/):
+ *   SphBase::runOneStep / sphStep         SphBase.h:395,411; SphBase.cpp:348-354
+ *   DFSPH::sphStep                         DFSPH.h:35;  DFSPH.cpp:9-75
+ *   WcSph::sphStep                         WcSph.h:50;  WcSph.cpp:23-96
+ *   PciSph::sphStep                        PciSph.h:39; PciSph.cpp:31-94
+ *   IISph_M::sphStep                       IISph_M.h:35; IISph_M.cpp:10-75
+ *   SphBase::neighbourSearch               SphBase.h:673; SphBase.cpp:849-960
+ *   m_Fluids / m_Solids particle arrays    SphBase.h:650-651, getters :513-541
+ *   m_TH thresholds                        SphBase.h:546-583
+ *   m_EC error counters                    SphBase.h:586-592
+ */
+#ifndef SPHGPU_H_
+#define SPHGPU_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SPHGPU_ABI_VERSION 1
+
+/* error codes */
+#define SPHGPU_OK 0
+#define SPHGPU_EINVAL (-1)              /* bad argument / state */
+#define SPHGPU_ENOMEM (-2)              /* device allocation failed */
+#define SPHGPU_ECUDA (-3)               /* CUDA runtime error */
+#define SPHGPU_EMAXITER (-4)            /* a solver loop hit its iteration cap */
+#define SPHGPU_ENAN (-5)                /* non-finite particle state */
+#define SPHGPU_ENEIGHBOUR_OVERFLOW (-6) /* a particle had more neighbours than the cap */
+#define SPHGPU_EOUT_OF_DOMAIN (-7)      /* particles left [spaceMin, spaceMax] and were removed */
+#define SPHGPU_ENOTIMPL (-8)
+
+/* solvers (reference classes) */
+#define SPHGPU_WCSPH 0   /* WcSph   */
+#define SPHGPU_PCISPH 1  /* PciSph  */
+#define SPHGPU_IISPH_M 2 /* IISph_M */
+#define SPHGPU_DFSPH 3   /* DFSPH   */
+
+/* step status bits (SphStepStats.status) */
+#define SPHGPU_STATUS_MAXITER_DENSITY 1u
+#define SPHGPU_STATUS_MAXITER_DIVERGENCE 2u
+#define SPHGPU_STATUS_NAN 4u
+#define SPHGPU_STATUS_NEIGHBOUR_OVERFLOW 8u
+#define SPHGPU_STATUS_OUT_OF_DOMAIN 16u
+#define SPHGPU_STATUS_ZERO_DISTANCE 32u
+
+typedef struct sphgpu_scene* sphgpu_t;
+
+/* Scene parameters: the m_TH fields the hot path reads (SphBase.h:546-583),
+ * plus the solver controls the reference hard-codes. */
+typedef struct SphParams {
+    float spacing_r;       /* m_TH.spacing_r: particle mass = rho0 * spacing_r^3 */
+    float smoothRadius_h;  /* m_TH.smoothRadius_h: kernel support; ker h = /2 */
+    float particle_d;      /* FluidParticle::d / BoundaryParticle::d (all particles) */
+    float dt;              /* m_TH.dt (fixed step; initial step when cfl != 0) */
+    float gravity[3];      /* m_TH.gravity_g */
+    float spaceMin[3];     /* m_TH.spaceMin */
+    float spaceMax[3];     /* m_TH.spaceMax */
+    float soundSpeed_cs;   /* m_TH.soundSpeed_cs */
+    float nu;              /* m_TH.nu: DFSPH / IISPH_M viscosity */
+    float densityErro_eta; /* m_TH.densityErro_eta (PCISPH) */
+    float boundary_visc;   /* SphSolid::viscosity_alpha of the walls */
+    int max_neighbours;    /* NeigbStr::maxNeigbNum, reference 48 (<= 128) */
+    /* DFSPH controls (reference values in brackets) */
+    double df_density_goal;    /* mean (rho_adv/rho0 - 1) goal [1e-4, DFSPH.cpp:225] */
+    int df_density_min_iter;   /* [2, DFSPH.cpp:229] */
+    int df_density_max_iter;   /* [none in the reference] */
+    double df_div_goal_abs;    /* >0: absolute mean Drho/Dt goal [2.5, DFSPH.cpp:762] */
+    double df_div_goal_rel;    /* used if abs <= 0: mean(Drho/Dt)*dt/rho0 */
+    int df_div_min_iter;       /* [1, DFSPH.cpp:765] */
+    int df_div_max_iter;       /* loop breaks when it > this [30, DFSPH.cpp:764,772] */
+    /* adaptive time step (not in the reference): dt = cfl*d/max|v| in FP64 */
+    int cfl;
+    float cfl_factor, dt_max, dt_min;
+    /* WCSPH */
+    float wc_gamma;            /* Tait exponent [7, WcSph.h:34] */
+    /* PCISPH (PciSph.h:35, PciSph.cpp:114-123) */
+    int pci_min_iter, pci_max_iter;
+    /* IISPH_M (IISph_M.cpp:280-358) */
+    float ii_omega;            /* relaxation [0.5] */
+    float ii_eta_rel;          /* relative avg density error [0.001] */
+    int ii_min_iter, ii_max_iter;
+    /* learned warm start for the DFSPH density solve (0 = plain method) */
+    int warm_start;
+    int reserved[7];
+} SphParams;
+
+/* Per-step statistics (replaces m_EC and the CALL_TIME log rows). */
+typedef struct SphStepStats {
+    int n_fluid;                 /* active fluid particles after the step */
+    int iter_density;            /* constant-density / pressure loop iterations */
+    int iter_divergence;         /* divergence-free loop iterations */
+    int removed;                 /* particles removed (outside the domain) */
+    double err_density;          /* final FP64 error of the density loop */
+    double err_divergence;       /* final FP64 error of the divergence loop */
+    double dt;                   /* step length used */
+    uint32_t status;             /* SPHGPU_STATUS_* bits */
+    int neighbour_overflow;      /* pairs dropped by the cap (m_EC.tooManyNeigb) */
+    int zero_distance;           /* zero-distance pairs (m_EC.zeroDis) */
+    int max_neighbours_seen;
+    double mean_neighbours;
+    int total_iter_density;      /* summed over the steps of this call */
+    int total_iter_divergence;
+    int steps;
+    int reserved[5];
+} SphStepStats;
+
+int sphgpu_abi_version(void);
+
+/* Reference-valued defaults (DFSPH/WcSph constructors, SphBase.cpp:210-225). */
+int sphgpu_params_default(SphParams* p);
+
+/* Scene lifetime.  device = CUDA ordinal; max_fluid = capacity of the fluid
+ * arrays (particles can be added up to it). */
+int sphgpu_create(const SphParams* p, int device, int max_fluid, sphgpu_t* out);
+int sphgpu_destroy(sphgpu_t h);
+int sphgpu_set_params(sphgpu_t h, const SphParams* p);
+
+/* Static boundary particles (a static rigid SphSolid per solid_id, or one
+ * solid if solid_id is NULL).  volume == NULL: compute the Akinci volume as
+ * SphBase::prepareSolidPartWeight does (SphBase.cpp:766-813) before fluid is
+ * present.  Replaces any previous boundary. */
+int sphgpu_set_boundary(sphgpu_t h, int n, const float* xyz, const int* solid_id, const float* volume);
+
+/* Append a fluid phase (SphWithIO::addFluidCuboid(newFluid=true)).  vel may be
+ * NULL.  Returns the phase index (>= 0) or an error. */
+int sphgpu_add_fluid(sphgpu_t h, int n, const float* xyz, const float* vel, float rho0, float visc_alpha);
+
+/* Number of active fluid particles. */
+int sphgpu_num_fluid(sphgpu_t h);
+
+/* Advance nsteps steps of `solver`; blocks until done and fills *stats
+ * (may be NULL).  Returns SPHGPU_EMAXITER / ENAN / ... after completing the
+ * steps if the corresponding status bit was raised (the state is kept). */
+int sphgpu_step(sphgpu_t h, int solver, int nsteps, SphStepStats* stats);
+
+/* Same, but only enqueues the work on the scene's stream and returns; the
+ * statistics of the last step become available after sphgpu_synchronize(). */
+int sphgpu_step_async(sphgpu_t h, int solver, int nsteps);
+int sphgpu_synchronize(sphgpu_t h, SphStepStats* stats);
+
+/* Host-buffer round trip for one step (the drop-in path, where the host
+ * arrays stay authoritative): upload xyz/vel (n*3 floats, reference order),
+ * run one step, download positions and velocities into xyz_out/vel_out. */
+int sphgpu_step_host(sphgpu_t h, int solver, const float* xyz, const float* vel, float* xyz_out,
+                     float* vel_out, SphStepStats* stats);
+
+/* Fluid fields in reference order (phase by phase, each in insertion order).
+ * field: "position","velocity" (n*3); "density","DFalpha","DFkappa",
+ * "DFkappaV","density_adv","divergenceDeviation","presure" (n);
+ * "vel_adv","acce_adv","acceleration" (n*3).  Returns the count written. */
+int sphgpu_get_fluid(sphgpu_t h, const char* field, float* out);
+int sphgpu_set_fluid(sphgpu_t h, const char* field, const float* in);
+int sphgpu_get_boundary(sphgpu_t h, const char* field, float* out); /* "position","volume" */
+
+/* Stage-level entry points (parity tests run "given state S, call stage X"):
+ *   "neighbourSearch"                 grid + neighbour lists (+ rho/alpha)
+ *   "DF_constantDensitySolverFirst"   rho, alpha            (DFSPH.cpp:84-193)
+ *   "DF_forceExceptPressure"          a_adv                 (DFSPH.cpp:1419-1475)
+ *   "DF_constantDensitySolverSecond"  forces+density loop+integrate (:195-738)
+ *   "DF_divergenceFreeSolver"         divergence loop       (:740-1024)
+ *   "wc_computePressure", "wc_computeForce"                 (WcSph.cpp:99-462)
+ */
+int sphgpu_stage(sphgpu_t h, const char* name, SphStepStats* stats);
+
+/* Neighbour lists in the reference's encoding, per fluid particle in
+ * reference order: counts[n]; t/idx[n*cap] = PartIdx (t<0: fluid phase -t-1,
+ * t>0: solid t-1; i = index in that phase/solid), list order as
+ * SphBase::neighbourSearch produces it.  Returns cap. */
+int sphgpu_get_neighbours(sphgpu_t h, int* counts, int* t, int* idx);
+/* Reference cell index (SpaceGridStruct::gridOfPos) per fluid particle. */
+int sphgpu_get_cells(sphgpu_t h, long long* cell);
+
+/* CUDA stream (cudaStream_t) of the scene. */
+void* sphgpu_stream(sphgpu_t h);
+
+/* Timing of the last sphgpu_step/step_async call measured with CUDA events on
+ * the scene's stream: per-kernel-class accumulated milliseconds and launch
+ * counts.  names/ms/launches arrays of length cap; returns entries written. */
+int sphgpu_profile(sphgpu_t h, int enable);
+int sphgpu_profile_read(sphgpu_t h, char* names, int name_len, double* ms, int* launches, int cap);
+
+/* Copy of the last error message. */
+int sphgpu_last_error(sphgpu_t h, char* buf, int len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPHGPU_H_ */

@@ -20,8 +20,9 @@ the GPU machines; the built libraries travel there instead):
    Two precisions: real_t=float (the reference as shipped, SphBase.h:40) and
    real_t=double (the typedef switch the reference itself describes,
    SphBase.h:37-39) -> suffix _f64.  A third DFSPH variant,
-   libref_dfsph_capped.so, changes only the density loop's bookkeeping (double
-   sum, iteration cap) so that large scenes terminate; see DF_CAP.
+   libref_dfsph_capped.so, changes only the loops' bookkeeping (double density
+   sum, iteration caps of 100, the divergence goal in relative form) so that
+   large scenes terminate under the same goals as the GPU run; see DF_CAP.
    Flags: -O3 -fopenmp, no -march (x86-64 SSE2, so no FMA contraction), which
    is what the parity statements assume.
 
@@ -66,6 +67,12 @@ AUGMENT = [
 # bookkeeping only: the sum becomes double and the loop stops after
 # REF_DF_MAXITER iterations.  Used for CPU-baseline timing of large scenes.
 DF_CAP = [
+    # divergence goal (DFSPH.cpp:762): absolute 2.5 -> the relative definition
+    # mean(Drho/Dt) * dt / rho0 <= REF_DIV_REL, as the GPU configuration uses
+    ("\t\treal_t errorRateGoal = 2.5;\n",
+     "\t\treal_t errorRateGoal = real_t(REF_DIV_REL * rho0 / m_TH.dt);\n"),
+    ("\t\tint maximumIteration = 30;\n\t\tint minimumIteration = 1;",
+     "\t\tint maximumIteration = REF_DIV_MAXITER;\n\t\tint minimumIteration = 1;"),
     ("\t\treal_t densitySum = 0;\n\t\tint maximumIteration = 50;",
      "\t\tdouble densitySum = 0;\n\t\tint maximumIteration = 50;"),
     ("\t\twhile (errorRate > errorRateGoal || currentIteration < minimumIteration)\n",
@@ -74,7 +81,8 @@ DF_CAP = [
 
 SOLVERS = {
     "dfsph": ("DFSPH.cpp", "DFSPH.h", "DFSPH", []),
-    "dfsph_capped": ("DFSPH_capped.cpp", "DFSPH.h", "DFSPH", ["-DREF_DF_MAXITER=100"]),
+    "dfsph_capped": ("DFSPH_capped.cpp", "DFSPH.h", "DFSPH", ["-DREF_DF_MAXITER=100", "-DREF_DIV_REL=1e-3",
+                                                         "-DREF_DIV_MAXITER=100"]),
     "wcsph": ("WcSph.cpp", "WcSph.h", "WcSph", []),
     "pcisph": ("PciSph.cpp", "PciSph.h", "PciSph", ["-DPREDICTION_PCISPH"]),
     "iisphm": ("IISph_M.cpp", "IISph_M.h", "IISph_M", ["-DIISPH"]),

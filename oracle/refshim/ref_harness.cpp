@@ -153,6 +153,10 @@ public:
         FluidParticle p = FluidParticle();
         p.d = real_t(d);
         p.restDensity = real_t(rho0);
+        /* WcSph::wc_computePressure reads the neighbours' density before it is
+         * first computed (WcSph.cpp:131, for the surface normal); start from
+         * the rest density so that read is finite. */
+        p.density = real_t(rho0);
         for (int i = 0; i < n; ++i) {
             p.position = vec_t(real_t(xyz[3 * i]), real_t(xyz[3 * i + 1]), real_t(xyz[3 * i + 2]));
             p.velocity = vel ? vec_t(real_t(vel[3 * i]), real_t(vel[3 * i + 1]), real_t(vel[3 * i + 2]))

@@ -963,6 +963,7 @@ int orc_add_fluid(void* h, int n, const double* xyz, const double* vel, double d
     F->ndis = (real*)calloc((size_t)n * s->P.cap + 1, sizeof(real));
     F->next = (PIdx*)calloc((size_t)n + 1, sizeof(PIdx));
     for (long i = 0; i < 3L * n; ++i) { F->pos[i] = (real)xyz[i]; F->vel[i] = vel ? (real)vel[i] : 0; }
+    for (long i = 0; i < n; ++i) F->density[i] = (real)rho0; /* as the oracle harness of the reference */
     return s->nf - 1;
 }
 

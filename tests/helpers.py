@@ -1,0 +1,46 @@
+"""Shared set-up for the parity tests: one seeded scene loaded both into the
+GPU path (through the C ABI) and into the CPU oracle (restatement)."""
+import numpy as np
+
+from graphics_b200.scene import small_dam_break
+from graphics_b200.sph import GpuScene, params_for_scene
+from oracle import make_scene_oracle
+
+COMMON = dict(dt=1e-3, nu=1e-3, soundSpeed_cs=100.0, df_density_goal=1e-4, df_density_min_iter=2,
+              df_density_max_iter=100, df_div_goal_abs=2.5, df_div_goal_rel=1e-3, df_div_min_iter=1,
+              df_div_max_iter=30, cfl=0, cfl_factor=0.4, dt_max=5e-3, dt_min=1e-6, wc_gamma=7.0)
+GPU_ONLY = ("max_neighbours", "boundary_visc", "warm_start")
+
+
+def make_pair(scene=None, visc_alpha=0.0, boundary_visc=0.0, cap=48, **kw):
+    if scene is None:
+        scene = small_dam_break((12, 12, 12), r=0.025, seed=7)
+    p = dict(COMMON)
+    p.update(kw)
+    gp = params_for_scene(scene, max_neighbours=cap, boundary_visc=boundary_visc,
+                          **{k: v for k, v in p.items() if k not in ("float_err",)})
+    g = GpuScene(gp, scene.n_fluid)
+    g.set_boundary(scene.boundary_pos)
+    if scene.phase is None:
+        g.add_fluid(scene.fluid_pos, scene.fluid_vel, rho0=scene.rho0, visc_alpha=visc_alpha)
+    else:
+        for ph, rho in enumerate(scene.rho0_phases):
+            m = scene.phase == ph
+            g.add_fluid(scene.fluid_pos[m], scene.fluid_vel[m], rho0=rho, visc_alpha=visc_alpha)
+    o = make_scene_oracle(scene, visc_alpha=visc_alpha, solid_visc=boundary_visc, cap=cap,
+                          **{k: v for k, v in p.items() if k not in GPU_ONLY})
+    return scene, g, o
+
+
+def rel_err(a, b, scale=None):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    if scale is None:
+        scale = np.max(np.abs(b)) if b.size else 1.0
+    return float(np.max(np.abs(a - b)) / max(scale, 1e-30)) if a.size else 0.0
+
+
+def elem_rel(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-30))) if a.size else 0.0
