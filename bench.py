@@ -65,6 +65,7 @@ def parse():
     ap.add_argument("--cpu-budget", type=float, default=60.0, help="seconds of reference CPU work per sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--scale", type=int, default=100, help="fluid block edge (100 -> 1M particles)")
+    ap.add_argument("--max-iter", type=int, default=1000, help="density-loop iteration cap")
     return ap.parse_args()
 
 
@@ -76,14 +77,15 @@ def workload(scale):
 
 
 SOLVER_KW = dict(cfl=1, cfl_factor=0.4, dt_max=5e-3, dt_min=1e-6, dt=5e-3, nu=1e-3,
-                 df_density_goal=1e-4, df_density_min_iter=2, df_density_max_iter=100,
+                 df_density_goal=1e-4, df_density_min_iter=2, df_density_max_iter=1000,
                  df_div_goal_abs=0.0, df_div_goal_rel=1e-3, df_div_min_iter=1, df_div_max_iter=100)
 
 
 def config_dict(sc, extra=None):
     d = {"workload": "dfsph_dam_break_%dk" % (sc.n_fluid // 1000), "n_fluid": sc.n_fluid,
          "n_boundary": sc.n_boundary, "r": sc.r, "box": list(sc.meta["box"]), "cfl": 0.4, "dt_max": 5e-3,
-         "density_goal": 1e-4, "divergence_goal": 1e-3, "max_iter": 100, "neighbour_cap": 48,
+         "density_goal": 1e-4, "divergence_goal": 1e-3, "max_iter": SOLVER_KW["df_density_max_iter"],
+         "div_max_iter": SOLVER_KW["df_div_max_iter"], "neighbour_cap": 48,
          "l2": "inputs larger than L2 (neighbour lists %.0f MB + state)" % (sc.n_fluid * 48 * 4 / 1e6)}
     if extra:
         d.update(extra)
@@ -223,6 +225,15 @@ def run_ours(args):
             dist.barrier()
         torch.cuda.synchronize()
 
+    # snapshot of the state the timed region starts from; the end-to-end run
+    # replays the same steps from it through the host-buffer API
+    n0 = g.n_fluid
+    snap_pos = torch.empty((n0, 3), dtype=torch.float32, pin_memory=True).numpy()
+    snap_vel = torch.empty((n0, 3), dtype=torch.float32, pin_memory=True).numpy()
+    snap_pos[:] = g.get("position")
+    snap_vel[:] = g.get("velocity")
+    g.set("position", snap_pos)  # same restaging the host-buffer path performs
+    g.step("dfsph", 0)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier()
     with ClockSampler(local) as clk:
@@ -232,6 +243,7 @@ def run_ours(args):
         st = g.synchronize()
         barrier()
     ms = e0.elapsed_time(e1)
+    end_pos = g.get("position")
     ms_max = ms
     if dist:
         t = torch.tensor([ms], device="cuda")
@@ -246,13 +258,22 @@ def run_ours(args):
 
     # per-kernel durations: the same kernels as individual launches bracketed
     # by CUDA events (host-driven loops), right after the timed region
+    hbm, peak_kind = peaks()
+    kern, roof = {}, None
+    if args.profile_steps > 0:
+        roof, kern = profile_kernels(g, args, hbm, peak_kind)
+    e2e = None
+    return run_tail(args, g, sc, st, value, ms_max, it_rho, it_div, launches, roof, kern, clk, world, rank, dist,
+                    barrier, torch, snap_pos, snap_vel, end_pos)
+
+
+def profile_kernels(g, args, hbm, peak_kind):
     g.profile(True)
     g.step("dfsph", args.profile_steps)
     prof = g.profile_read()
     g.profile(False)
     st_p = g.synchronize()
     nb = st_p["mean_neighbours"]
-    hbm, peak_kind = peaks()
     kern = {}
     for k, (tot_ms, cnt) in prof.items():
         ent = {"total_ms": round(tot_ms, 4), "launches": cnt, "avg_us": round(1e3 * tot_ms / max(cnt, 1), 2)}
@@ -280,22 +301,22 @@ def run_ours(args):
     roof["neighbour_density_group"] = {"kernels": ns_keys, "us_per_step": round(ns_ms * 1e3, 1),
                                        "gbs": round(ns_bytes / (ns_ms / 1e3) / 1e9, 1),
                                        "frac": round(ns_bytes / (ns_ms / 1e3) / 1e9 / hbm, 4)}
+    return roof, kern
 
-    # end to end through the C ABI with pinned host buffers
+
+def run_tail(args, g, sc, st, value, ms_max, it_rho, it_div, launches, roof, kern, clk, world, rank, dist,
+             barrier, torch, snap_pos, snap_vel, end_pos):
+    # end to end through the C ABI with pinned host buffers: the same K steps,
+    # replayed from the snapshot taken before the timed region
     e2e = None
     if args.e2e_steps > 0:
-        n = g.n_fluid
-        pos = torch.empty((n, 3), dtype=torch.float32, pin_memory=True).numpy()
-        vel = torch.empty((n, 3), dtype=torch.float32, pin_memory=True).numpy()
-        pos[:] = g.get("position")
-        vel[:] = g.get("velocity")
+        n = snap_pos.shape[0]
+        pos, vel = snap_pos, snap_vel
         po = torch.empty((n, 3), dtype=torch.float32, pin_memory=True).numpy()
         vo = torch.empty((n, 3), dtype=torch.float32, pin_memory=True).numpy()
-        g.step_host("dfsph", pos, vel, po, vo)  # warm (graph for the restaged state)
-        pos[:], vel[:] = po, vo
         barrier()
         t0 = time.perf_counter()
-        for _ in range(args.e2e_steps):
+        for _ in range(args.steps):
             g.step_host("dfsph", pos, vel, po, vo)
             pos, po = po, pos
             vel, vo = vo, vel
@@ -305,9 +326,10 @@ def run_ours(args):
             t = torch.tensor([sec], device="cuda")
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             sec = float(t.item())
-        e2e = {"value": n * args.e2e_steps * world / sec, "unit": UNIT, "h2d_bytes_per_step": int(n * 24),
-               "d2h_bytes_per_step": int(n * 24), "steps": args.e2e_steps,
-               "note": "sphgpu_step_host: pinned positions+velocities in, step (with re-search), out"}
+        e2e = {"value": n * args.steps * world / sec, "unit": UNIT, "h2d_bytes_per_step": int(n * 24),
+               "d2h_bytes_per_step": int(n * 24), "steps": args.steps,
+               "same_trajectory_as_timed": bool(np.array_equal(pos, end_pos)),
+               "note": "sphgpu_step_host: pinned positions+velocities in, step, positions+velocities out"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -333,6 +355,7 @@ def run_ours(args):
 
 def main():
     args = parse()
+    SOLVER_KW["df_density_max_iter"] = args.max_iter
     if args.impl == "reference":
         run_reference(args)
     else:

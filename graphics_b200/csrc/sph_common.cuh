@@ -37,6 +37,8 @@ struct GridGeom {
 // (SphBase::ker_update_numbers, SphBase.h:808-829).
 struct KerConst {
     float h, inv_h, theta, thetah;
+    float g_in;   // -thetah / h      : -W'(r)/r = g_in * (3 - 2.25 q)     for q <= 1
+    float g_out;  // -0.75 * thetah   : -W'(r)/r = g_out * (2 - q)^2 / r   for q > 1
 };
 
 struct SolverConst {
@@ -70,6 +72,18 @@ __device__ __forceinline__ float ker_Wg(const KerConst& k, float r) {
     float q = r / k.h, qm2 = 2.f - q;
     return q <= 1.f ? k.thetah * (3.f * q - 2.25f * q * q) : k.thetah * 0.75f * qm2 * qm2;
 }
+// -W'(r)/r from r^2 with one reciprocal square root and no division: the
+// fast form of the reference's `-ker_W_grad(dis) / dis` (SphBase.h:876-889),
+// used by the Jacobi sweeps (relative error a few ulp).
+__device__ __forceinline__ float grad_over_r(const KerConst& k, float len2) {
+    const float inv_r = rsqrtf(len2);
+    const float q = len2 * inv_r * k.inv_h;
+    const float t = 2.f - q;
+    const float fin = k.g_in * fmaf(-2.25f, q, 3.f);
+    const float fout = k.g_out * t * t * inv_r;
+    return q <= 1.f ? fin : fout;
+}
+
 // per-pair-h spline with range check, SphBase.h:855-871
 __device__ __forceinline__ float ker_W_h(float r, float h) {
     float q = r / h, qm2 = 2.f - q;

@@ -55,18 +55,27 @@ __device__ __forceinline__ bool finish_sum(double* partial, unsigned* ticket, do
     return threadIdx.x == 0;
 }
 
+// per-step counters (the last step's values are reported)
 __global__ void k_step_begin(DevScene s) {
     DevStats* st = s.st;
-    st->removed = 0;
-    st->overflow = 0;
-    st->zero_dis = 0;
     st->max_nbrs = 0;
     st->nbr_total = 0ull;
-    st->status = 0u;
     st->it_density = 0;
     st->it_div = 0;
     st->err_density = 0;
     st->err_div = 0;
+}
+
+// per-call counters: status bits are OR-ed and removals / dropped pairs
+// summed over all steps of one API call
+__global__ void k_call_begin(DevScene s) {
+    DevStats* st = s.st;
+    st->removed = 0;
+    st->overflow = 0;
+    st->zero_dis = 0;
+    st->status = 0u;
+    st->total_it_density = 0;
+    st->total_it_div = 0;
 }
 
 __global__ void k_loop_reset(DevScene s, int which) {
@@ -110,7 +119,7 @@ __global__ void __launch_bounds__(NT) k_df_forces(DevScene s, SolverConst c, int
             if (len2 == 0.f) { ++zero; continue; }
             const float pro = (va.x - vb.x) * xx + (va.y - vb.y) * xy + (va.z - vb.z) * xz;
             if (pro < 0.f) {
-                const float f = grad_factor(c.k, len2);
+                const float f = grad_over_r(c.k, len2);
                 const float t = f * pro / (len2 + den0) * m * visc;
                 ax += xx * t;
                 ay += xy * t;
@@ -133,6 +142,33 @@ __global__ void __launch_bounds__(NT) k_df_forces(DevScene s, SolverConst c, int
     }
 }
 
+// Neighbour-sum of m_j gradW_ij . (v_i - v_j) over the stored list: the
+// common sweep of the density loop (DFSPH.cpp:589-617) and of the divergence
+// loop (DFSPH.cpp:795-825).  Fluid and boundary neighbours are read through
+// one select of the base pointers so the loads of consecutive entries can be
+// issued back to back (unrolled by 4).
+__device__ __forceinline__ float div_sweep(const DevScene& s, const SolverConst& c, const float4* V, int p,
+                                           float4 pa, float4 va) {
+    const int cnt = s.ncount[p];
+    const int* L = s.nbr + p;
+    const size_t stride = (size_t)c.stride;
+    float acc = 0.f;
+#pragma unroll 4
+    for (int k = 0; k < cnt; ++k) {
+        const unsigned e = (unsigned)__ldg(L + k * stride);
+        const bool bnd = (e & BND_FLAG) != 0u;
+        const unsigned j = e & BND_MASK;
+        const float4 pb = __ldg((bnd ? s.bpos : s.pos) + j);
+        const float4 vb = __ldg((bnd ? s.bvel : V) + j);
+        const float m = bnd ? c.rho0 * pb.w : c.fm0;
+        const float xx = pa.x - pb.x, xy = pa.y - pb.y, xz = pa.z - pb.z;
+        const float f = grad_over_r(c.k, xx * xx + xy * xy + xz * xz);
+        const float dot = xx * (va.x - vb.x) + xy * (va.y - vb.y) + xz * (va.z - vb.z);
+        acc = fmaf(dot * f, m, acc);
+    }
+    return acc;
+}
+
 // density loop, part A: rho_adv, kappa, FP64 sum of rho_adv
 __global__ void __launch_bounds__(NT) k_df_dens_a(DevScene s, SolverConst c, int record) {
     const int n = s.st->n_active;
@@ -142,31 +178,10 @@ __global__ void __launch_bounds__(NT) k_df_dens_a(DevScene s, SolverConst c, int
         const float dt = *s.dt;
         const float4 pa = s.pos[p];
         const float4 va = s.vadv[p];
-        const float rho0 = c.rho0, fm0 = c.fm0;
-        float acc = 0.f;
-        const int cnt = s.ncount[p];
-        const int* L = s.nbr + p;
-        for (int k = 0; k < cnt; ++k) {
-            const unsigned e = (unsigned)L[(size_t)k * c.stride];
-            float4 pb, vb;
-            float m;
-            if (e & BND_FLAG) {
-                const unsigned b = e & BND_MASK;
-                pb = s.bpos[b];
-                vb = s.bvel[b];
-                m = rho0 * pb.w;
-            } else {
-                pb = s.pos[e];
-                vb = s.vadv[e];
-                m = fm0;
-            }
-            const float xx = pa.x - pb.x, xy = pa.y - pb.y, xz = pa.z - pb.z;
-            const float f = grad_factor(c.k, xx * xx + xy * xy + xz * xz);
-            const float dot = (xx * (va.x - vb.x) + xy * (va.y - vb.y) + xz * (va.z - vb.z)) * f;
-            acc += dot * m;
-        }
-        float rho = s.rho[p];
-        float dadv = rho + acc * dt;
+        const float rho0 = c.rho0;
+        const float acc = div_sweep(s, c, s.vadv, p, pa, va);
+        const float rho = s.rho[p];
+        float dadv = fmaf(acc, dt, rho);
         if (dadv < rho0) dadv = rho0;
         // kappa = (rho_adv - rho0) / pow(dt,2) * alpha  (DFSPH.cpp:641)
         const float kap = (float)((double)(dadv - rho0) / ((double)dt * (double)dt) * (double)s.alpha[p]);
@@ -198,30 +213,28 @@ __global__ void __launch_bounds__(NT) k_df_vupdate(DevScene s, SolverConst c, do
         float4* V = DIV ? s.vel : s.vadv;
         float4 va = V[p];
         const float ka = s.kr[p];
-        const float rho0 = c.rho0, fm0 = c.fm0;
+        const float fa = c.fm0 * ka, ba = c.rho0 * ka;
         float dx = 0.f, dy = 0.f, dz = 0.f;
         const int cnt = s.ncount[p];
         const int* L = s.nbr + p;
+        const size_t stride = (size_t)c.stride;
+#pragma unroll 4
         for (int k = 0; k < cnt; ++k) {
-            const unsigned e = (unsigned)L[(size_t)k * c.stride];
-            float4 pb;
-            float w;
-            if (e & BND_FLAG) {
-                pb = s.bpos[e & BND_MASK];
-                w = rho0 * pb.w * ka;
-            } else {
-                pb = s.pos[e];
-                w = fm0 * (ka + s.kr[e]);
-            }
+            const unsigned e = (unsigned)__ldg(L + k * stride);
+            const bool bnd = (e & BND_FLAG) != 0u;
+            const unsigned j = e & BND_MASK;
+            const float4 pb = __ldg((bnd ? s.bpos : s.pos) + j);
+            const float kj = bnd ? 0.f : __ldg(s.kr + j);
+            const float w = bnd ? ba * pb.w : fmaf(c.fm0, kj, fa);
             const float xx = pa.x - pb.x, xy = pa.y - pb.y, xz = pa.z - pb.z;
-            const float f = grad_factor(c.k, xx * xx + xy * xy + xz * xz) * w;
-            dx += xx * f;
-            dy += xy * f;
-            dz += xz * f;
+            const float f = grad_over_r(c.k, xx * xx + xy * xy + xz * xz) * w;
+            dx = fmaf(xx, f, dx);
+            dy = fmaf(xy, f, dy);
+            dz = fmaf(xz, f, dz);
         }
-        va.x -= dx * dt;
-        va.y -= dy * dt;
-        va.z -= dz * dt;
+        va.x = fmaf(-dx, dt, va.x);
+        va.y = fmaf(-dy, dt, va.y);
+        va.z = fmaf(-dz, dt, va.z);
         V[p] = va;
     }
     if (DECIDE && blockIdx.x == 0 && threadIdx.x == 0) {
@@ -259,30 +272,9 @@ __global__ void __launch_bounds__(NT) k_df_div_a(DevScene s, SolverConst c) {
         const float dt = *s.dt;
         const float4 pa = s.pos[p];
         const float4 va = s.vel[p];
-        const float rho0 = c.rho0, fm0 = c.fm0;
-        float dd = 0.f;
-        const int cnt = s.ncount[p];
-        const int* L = s.nbr + p;
-        for (int k = 0; k < cnt; ++k) {
-            const unsigned e = (unsigned)L[(size_t)k * c.stride];
-            float4 pb, vb;
-            float m;
-            if (e & BND_FLAG) {
-                const unsigned b = e & BND_MASK;
-                pb = s.bpos[b];
-                vb = s.bvel[b];
-                m = rho0 * pb.w;
-            } else {
-                pb = s.pos[e];
-                vb = s.vel[e];
-                m = fm0;
-            }
-            const float xx = pa.x - pb.x, xy = pa.y - pb.y, xz = pa.z - pb.z;
-            const float f = grad_factor(c.k, xx * xx + xy * xy + xz * xz);
-            dd += (xx * (va.x - vb.x) + xy * (va.y - vb.y) + xz * (va.z - vb.z)) * f * m;
-        }
+        float dd = div_sweep(s, c, s.vel, p, pa, va);
         const float rho = s.rho[p];
-        if (dd < 0.f || (rho + dd * dt) < rho0) dd = 0.f;  // DFSPH.cpp:829-832
+        if (dd < 0.f || (rho + dd * dt) < c.rho0) dd = 0.f;  // DFSPH.cpp:829-832
         const float kv = dd * s.alpha[p] / dt;              // DFSPH.cpp:835
         s.kr[p] = kv / rho;
         s.kappa[p] = kv;
@@ -336,6 +328,7 @@ __global__ void __launch_bounds__(NT) k_cfl(DevScene s, float cfl, float d, floa
 static inline int nblk(int n) { return (n > 0 ? n + NT - 1 : NT) / NT; }
 
 void launch_step_begin(const DevScene& s, cudaStream_t st) { k_step_begin<<<1, 1, 0, st>>>(s); }
+void launch_call_begin(const DevScene& s, cudaStream_t st) { k_call_begin<<<1, 1, 0, st>>>(s); }
 void launch_df_loop_reset(const DevScene& s, int which, cudaStream_t st) { k_loop_reset<<<1, 1, 0, st>>>(s, which); }
 
 void launch_df_forces(const DevScene& s, const SolverConst& c, int n_max, int warm, cudaStream_t st) {

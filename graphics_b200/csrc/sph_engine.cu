@@ -153,6 +153,8 @@ void fill_solver_const(sphgpu_scene* h) {
     c.k.inv_h = 1.f / kh;
     c.k.theta = 1 / (float)M_PI / (kh * kh * kh);
     c.k.thetah = 1 / (float)M_PI / (kh * kh * kh) / kh;
+    c.k.g_in = -c.k.thetah / kh;
+    c.k.g_out = -0.75f * c.k.thetah;
     c.hs = P.smoothRadius_h;
     float dd = P.particle_d + P.particle_d;
     c.h2cut = (float)std::pow((double)dd, 2);
@@ -428,8 +430,7 @@ int enq_steps(sphgpu_scene* h, int solver, int nsteps) {
         h->err = "DFSPH path supports one fluid phase";
         return SPHGPU_ENOTIMPL;
     }
-    // reset the per-call iteration totals
-    cudaMemsetAsync(&h->d.st->total_it_density, 0, sizeof(int) * 2, h->stream);
+    launch_call_begin(h->d, h->stream);
     if (solver == SPHGPU_DFSPH) {
         if (!h->ns_valid) {
             int r = run_initial_ns(h, 1);
@@ -899,6 +900,7 @@ int sphgpu_stage(sphgpu_t h, const char* name, SphStepStats* stats) {
     DevScene& d = h->d;
     cudaStream_t st = h->stream;
     int r = 0;
+    launch_call_begin(d, st);
     launch_step_begin(d, st);
     if (s == "neighbourSearch" || s == "DF_constantDensitySolverFirst" || s == "wc_computePressure") {
         int mode = s == "wc_computePressure" ? 2 : 1;

@@ -93,6 +93,7 @@ void launch_df_warm_correction(const DevScene& s, const SolverConst& c, int n_ma
 void launch_df_loop_reset(const DevScene& s, int which, cudaStream_t st);
 void launch_cfl(const DevScene& s, int n_max, float cfl, float d, float dt_max, float dt_min, cudaStream_t st);
 void launch_step_begin(const DevScene& s, cudaStream_t st);
+void launch_call_begin(const DevScene& s, cudaStream_t st);
 
 // ---- WCSPH (sph_wcsph.cu) ----
 void launch_wc_force(const DevScene& s, const SolverConst& c, int n_max, cudaStream_t st);

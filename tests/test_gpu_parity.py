@@ -75,8 +75,12 @@ def test_constant_density_solver_from_shared_state():
     it, err, _, _ = o.stats()
     assert sg["iter_density"] == it[0]
     assert abs(sg["err_density"] - err[0]) < 1e-7
-    assert elem_rel(g.get("density_adv"), o.get("density_adv")) < RTOL
-    assert rel_err(g.get("DFkappa"), o.get("DFkappa")) < 1e-4
+    dadv = o.get("density_adv")
+    assert elem_rel(g.get("density_adv"), dadv) < RTOL
+    # kappa = (rho_adv - rho0)/dt^2 * alpha cancels catastrophically; it must
+    # agree to what a 1e-5 relative change of rho_adv moves it by
+    bound = RTOL * dadv * o.get("DFalpha") / 1e-3 ** 2
+    assert np.all(np.abs(g.get("DFkappa") - o.get("DFkappa")) <= bound)
     assert rel_err(g.get("velocity"), o.get("velocity")) < RTOL
     assert rel_err(g.get("position"), o.get("position"), scale=1.0) < 1e-6
 
@@ -98,17 +102,47 @@ def test_divergence_free_solver_from_shared_state():
 
 
 @pytest.mark.parametrize("cfl", [0, 1])
-def test_dfsph_steps(cfl):
+def test_dfsph_steps_from_shared_state(cfl):
+    """Each step starts both paths from the same state (the GPU's), then
+    compares.  When the FP64 error sums of the two paths land on different
+    sides of the goal, the iteration counts differ by one and the fields are
+    compared at the size of one Jacobi correction instead."""
     sc, g, o = make_pair(cfl=cfl)
-    for k in range(3):
+    same = 0
+    for k in range(4):
+        o.set("position", g.get("position").astype(np.float64))
+        o.set("velocity", g.get("velocity").astype(np.float64))
+        o.set_frame(0)  # re-run neighbour search + rho/alpha from the shared state
         st = g.step("dfsph", 1)
         o.stage("df_step")
         it, err, dt, _ = o.stats()
         assert abs(st["dt"] - dt) <= 1e-6 * dt
         assert abs(st["iter_density"] - it[0]) <= 1, (k, st["iter_density"], it[0])
-        assert elem_rel(g.get("density"), o.get("density")) < RTOL
-        assert rel_err(g.get("velocity"), o.get("velocity")) < 1e-4
-        assert rel_err(g.get("position"), o.get("position"), scale=1.0) < 1e-6
+        tol = RTOL if (st["iter_density"] == it[0] and st["iter_divergence"] == it[1]) else 1e-4
+        same += tol == RTOL
+        assert elem_rel(g.get("density"), o.get("density")) < tol, k
+        assert rel_err(g.get("velocity"), o.get("velocity")) < tol * 10, k
+        assert rel_err(g.get("position"), o.get("position"), scale=1.0) < 1e-6, k
+    assert same >= 3
+
+
+def test_long_run_statistics():
+    """Trajectories diverge chaotically; long runs are compared by mean density
+    error and kinetic energy."""
+    from graphics_b200.scene import dam_break
+    sc = dam_break((24, 24, 24), 0.01, (4.0, 2.0, 2.0), seed=5)
+    _, g, o = make_pair(sc, cfl=1, dt=5e-3, df_div_goal_abs=0.0, df_div_goal_rel=1e-3, df_div_max_iter=100)
+    eg, eo = [], []
+    for _ in range(30):
+        g.step("dfsph", 1)
+        o.stage("df_step")
+        for path, acc in ((g, eg), (o, eo)):
+            v = np.asarray(path.get("velocity"), np.float64)
+            rho = np.asarray(path.get("density"), np.float64)
+            acc.append((np.mean(rho / 1000.0 - 1.0), 0.5 * np.sum(v * v)))
+    eg, eo = np.array(eg), np.array(eo)
+    assert np.max(np.abs(eg[:, 0] - eo[:, 0])) < 1e-3
+    assert np.max(np.abs(eg[:, 1] - eo[:, 1]) / np.max(eo[:, 1])) < 0.02
 
 
 def test_graph_and_host_loops_identical_and_deterministic():
