@@ -741,9 +741,8 @@ int sphgpu_step_host(sphgpu_t h, int solver, const float* xyz, const float* vel,
                      SphStepStats* stats) {
     if (!h) return SPHGPU_EINVAL;
     int r = 0;
-    if (xyz) r = sphgpu_set_fluid(h, "position", xyz);
-    if (!r && vel) r = sphgpu_set_fluid(h, "velocity", vel);
-    if (r) return r;
+    if (xyz && (r = sphgpu_set_fluid(h, "position", xyz)) < 0) return r;
+    if (vel && (r = sphgpu_set_fluid(h, "velocity", vel)) < 0) return r;
     r = sphgpu_step(h, solver, 1, stats);
     if (r && r != SPHGPU_EMAXITER) return r;
     int r2 = 0;

@@ -188,11 +188,13 @@ def test_out_of_domain_particles_removed_with_status():
 
 
 def test_nan_particle_reported():
+    from graphics_b200._lib import ENAN, SphGpuError
     sc = small_dam_break((8, 8, 8), r=0.025, seed=2)
     sc.fluid_vel[5] = np.nan
     sc2, g, o = make_pair(sc)
-    st = g.step("dfsph", 2)
-    assert st["status"] & (4 | 16)
+    with pytest.raises(SphGpuError) as e:
+        g.step("dfsph", 2)
+    assert e.value.code == ENAN
 
 
 def test_no_boundary_scene():
