@@ -196,7 +196,7 @@ int alloc_scene(sphgpu_scene* h) {
     int r = 0;
     r |= dalloc(h, &d.pos, n); r |= dalloc(h, &d.vel, n); r |= dalloc(h, &d.gid, n);
     r |= dalloc(h, &d.rho, n); r |= dalloc(h, &d.alpha, n); r |= dalloc(h, &d.vadv, n);
-    r |= dalloc(h, &d.acc, n); r |= dalloc(h, &d.kr, n); r |= dalloc(h, &d.kappa, n); r |= dalloc(h, &d.kappav, n);
+    r |= dalloc(h, &d.acc, n); r |= dalloc(h, &d.kr, n); r |= dalloc(h, &d.kappa, n);
     r |= dalloc(h, &d.ksum, n); r |= dalloc(h, &d.aux0, n); r |= dalloc(h, &d.aux1, n);
     r |= dalloc(h, &d.aux4, n); r |= dalloc(h, &d.kwarm, n);
     r |= dalloc(h, &d.pos_s, n); r |= dalloc(h, &d.vel_s, n); r |= dalloc(h, &d.gid_s, n);
@@ -206,11 +206,8 @@ int alloc_scene(sphgpu_scene* h) {
     r |= dalloc(h, &d.cell_start, (size_t)h->g.nkeys + 1);
     r |= dalloc(h, &d.bcell_start, (size_t)h->g.nkeys + 1);
     r |= dalloc(h, &d.nbr, (size_t)h->stride * h->ncap);
-    r |= dalloc(h, &d.nbr16, (size_t)h->stride * h->ncap);
     r |= dalloc(h, &d.ncount, n);
-    const int nbricks = h->g.nb[0] * h->g.nb[1] * h->g.nb[2];
-    r |= dalloc(h, &d.brick_wide, (size_t)nbricks);
-    r |= dalloc(h, &d.partial, (size_t)std::max(n / 64, nbricks) + 4096);
+    r |= dalloc(h, &d.partial, (size_t)n / 64 + 4096);
     r |= dalloc(h, &d.st, 1);
     if (r) return SPHGPU_ENOMEM;
     d.cap_fluid = n;
@@ -234,7 +231,7 @@ int alloc_scene(sphgpu_scene* h) {
 
 void free_scene(sphgpu_scene* h) {
     DevScene& d = h->d;
-    void* ptrs[] = {d.pos, d.vel, d.gid, d.rho, d.alpha, d.vadv, d.acc, d.kr, d.kappa, d.kappav, d.nbr16, d.brick_wide, d.ksum, d.aux0,
+    void* ptrs[] = {d.pos, d.vel, d.gid, d.rho, d.alpha, d.vadv, d.acc, d.kr, d.kappa, d.ksum, d.aux0,
                     d.aux1, d.aux4, d.kwarm, d.pos_s, d.vel_s, d.gid_s, d.kwarm_s, d.key, d.slot, d.tmp,
                     d.cell_count, d.cell_start, d.bcell_start, d.nbr, d.ncount, d.partial, d.st,
                     d.bpos, d.bvel, d.bgid, h->cub_tmp};
@@ -301,9 +298,9 @@ int enq_df_density_loop(sphgpu_scene* h, bool capturing) {
     const SphParams& P = h->P;
     launch_df_loop_reset(d, 0, h->stream);
     return enq_loop(h, capturing, [&](cudaStream_t st, unsigned long long hd, int use) {
-        launch(h, "df_density_a", st, [&] { launch_df_dens_a(d, h->g, h->c, h->record_ksum, st); });
+        launch(h, "df_density_a", st, [&] { launch_df_dens_a(d, h->c, h->cap, h->record_ksum, st); });
         launch(h, "df_density_b", st, [&] {
-            launch_df_dens_b(d, h->g, h->c, P.df_density_goal, P.df_density_min_iter, P.df_density_max_iter, hd,
+            launch_df_dens_b(d, h->c, h->cap, P.df_density_goal, P.df_density_min_iter, P.df_density_max_iter, hd,
                              use, st);
         });
     });
@@ -314,9 +311,9 @@ int enq_df_div_loop(sphgpu_scene* h, bool capturing) {
     const SphParams& P = h->P;
     launch_df_loop_reset(d, 1, h->stream);
     return enq_loop(h, capturing, [&](cudaStream_t st, unsigned long long hd, int use) {
-        launch(h, "df_div_a", st, [&] { launch_df_div_a(d, h->g, h->c, st); });
+        launch(h, "df_div_a", st, [&] { launch_df_div_a(d, h->c, h->cap, st); });
         launch(h, "df_div_b", st, [&] {
-            launch_df_div_b(d, h->g, h->c, P.df_div_goal_abs, P.df_div_goal_rel, P.df_div_min_iter,
+            launch_df_div_b(d, h->c, h->cap, P.df_div_goal_abs, P.df_div_goal_rel, P.df_div_min_iter,
                             P.df_div_max_iter, hd, use, st);
         });
     });
@@ -331,8 +328,8 @@ int enq_df_step(sphgpu_scene* h, bool capturing) {
     if (h->P.cfl)
         launch(h, "cfl", st, [&] { launch_cfl(d, h->cap, h->P.cfl_factor, h->P.particle_d, h->P.dt_max, h->P.dt_min, st); });
     const int warm = h->P.warm_start && h->have_kwarm;
-    launch(h, "df_forces", st, [&] { launch_df_forces(d, h->g, h->c, warm, st); });
-    if (warm) launch(h, "df_warm", st, [&] { launch_df_warm_correction(d, h->g, h->c, st); });
+    launch(h, "df_forces", st, [&] { launch_df_forces(d, h->c, h->cap, warm, st); });
+    if (warm) launch(h, "df_warm", st, [&] { launch_df_warm_correction(d, h->c, h->cap, st); });
     int r = enq_df_density_loop(h, capturing);
     if (r) return r;
     enq_ns(h, 1, 1, st);
@@ -465,7 +462,7 @@ int enq_steps(sphgpu_scene* h, int solver, int nsteps) {
         }
         launch_step_begin(h->d, h->stream);
         enq_ns(h, 0, 2, h->stream);
-        launch(h, "wc_force", h->stream, [&] { launch_wc_force(h->d, h->g, h->c, h->stream); });
+        launch(h, "wc_force", h->stream, [&] { launch_wc_force(h->d, h->c, h->cap, h->stream); });
         h->in_staging = true;
         h->ns_valid = false;
         CK(cudaMemcpyAsync(h->h_stats, h->d.st, sizeof(DevStats), cudaMemcpyDeviceToHost, h->stream));
@@ -559,8 +556,6 @@ int sphgpu_create(const SphParams* p, int device, int max_fluid, sphgpu_t* out) 
     h->ncap = p->max_neighbours;
     h->g = make_grid(*p);
     fill_solver_const(h);
-    dfsph_init_attributes();
-    wcsph_init_attributes();
     int r = alloc_scene(h);
     if (r) {
         free_scene(h);
@@ -788,12 +783,10 @@ int sphgpu_get_fluid(sphgpu_t h, const char* field, float* out) {
     else if (f == "acce_adv" || f == "acceleration") { src = d.acc; f4 = true; comps = 3; }
     else if (f == "density") src = d.rho;
     else if (f == "DFalpha") src = d.alpha;
-    else if (f == "DFkappa") src = d.kappa;
-    else if (f == "DFkappaV") src = d.kappav;
+    else if (f == "DFkappa" || f == "DFkappaV") src = d.kappa;
     else if (f == "kappa_sum") src = d.ksum;
     else if (f == "kappa_warm") src = d.kwarm;
-    else if (f == "density_adv") src = d.aux0;
-    else if (f == "divergenceDeviation") src = d.aux1;
+    else if (f == "density_adv" || f == "divergenceDeviation") src = d.aux0;
     else if (f == "presure") src = d.kr;
     else if (f == "neighbour_count") {
         std::vector<int> cnt(n);
@@ -919,13 +912,13 @@ int sphgpu_stage(sphgpu_t h, const char* name, SphStepStats* stats) {
         h->ns_valid = mode == 1;
     } else if (s == "DF_forceExceptPressure") {
         if (h->in_staging) { h->err = "run neighbourSearch first"; return SPHGPU_EINVAL; }
-        launch_df_forces(d, h->g, h->c, 0, st);
+        launch_df_forces(d, h->c, h->cap, 0, st);
     } else if (s == "DF_constantDensitySolverSecond") {
         if (h->in_staging) { h->err = "run neighbourSearch first"; return SPHGPU_EINVAL; }
         if (h->P.cfl) launch_cfl(d, h->cap, h->P.cfl_factor, h->P.particle_d, h->P.dt_max, h->P.dt_min, st);
         int warm = h->P.warm_start && h->have_kwarm;
-        launch_df_forces(d, h->g, h->c, warm, st);
-        if (warm) launch_df_warm_correction(d, h->g, h->c, st);
+        launch_df_forces(d, h->c, h->cap, warm, st);
+        if (warm) launch_df_warm_correction(d, h->c, h->cap, st);
         r = enq_df_density_loop(h, false);
         if (r) return r;
         // integrate into staging (the reference updates positions in place)
@@ -939,7 +932,7 @@ int sphgpu_stage(sphgpu_t h, const char* name, SphStepStats* stats) {
         if (r) return r;
     } else if (s == "wc_computeForce") {
         if (h->in_staging) { h->err = "run neighbourSearch first"; return SPHGPU_EINVAL; }
-        launch_wc_force(d, h->g, h->c, st);
+        launch_wc_force(d, h->c, h->cap, st);
         h->in_staging = true;
         h->ns_valid = false;
     } else {
@@ -961,8 +954,6 @@ int sphgpu_get_neighbours(sphgpu_t h, int* counts, int* t, int* idx) {
     std::vector<int> gid;
     int n;
     if (download_gid(h, gid, n, false)) return SPHGPU_ECUDA;
-    launch_expand_lists(h->d, h->g, h->c, h->stream);
-    CK(cudaStreamSynchronize(h->stream));
     std::vector<int> cnt(n), L((size_t)h->stride * h->ncap);
     CK(cudaMemcpy(cnt.data(), h->d.ncount, sizeof(int) * n, cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(L.data(), h->d.nbr, sizeof(int) * L.size(), cudaMemcpyDeviceToHost));

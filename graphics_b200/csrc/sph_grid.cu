@@ -14,11 +14,11 @@
 // particles by descending global index -- exactly the reference's list order
 // -- while reordering the particle state into the new layout.  Boundary
 // particles are sorted once into their own cell table.  The neighbour-list
-// kernel (k_build_win, sph_dfsph.cu) then walks the 27 cells in the
-// reference's offset order, the fluid range of a cell before its boundary
-// range, so the stored lists (and which entries a 48-cap truncates) are the
-// reference's.  The cut test uses round-to-nearest float ops in the
-// reference's evaluation order, so the neighbour sets are bit-identical.
+// kernel then walks the 27 cells in the reference's offset order, the fluid
+// range of a cell before its boundary range, so the stored lists (and which
+// entries a 48-cap truncates) are the reference's.  The cut test uses
+// round-to-nearest float ops in the reference's evaluation order, so the
+// neighbour sets are bit-identical.
 #include "sph_kernels.cuh"
 
 namespace {
@@ -100,6 +100,110 @@ __global__ void k_count_active(DevScene s, int dead_key) {
     int act = s.cell_start[dead_key];
     s.st->removed += staged - act;
     s.st->n_active = act;
+}
+
+// mode 0: neighbour lists only; 1: + DFSPH rho and alpha
+// (DF_constantDensitySolverFirst, DFSPH.cpp:84-193); 2: + WCSPH rho and Tait
+// pressure (WcSph::wc_computePressure, WcSph.cpp:99-153).
+template <int MODE>
+__global__ void __launch_bounds__(128) k_build(DevScene s, GridGeom g, SolverConst c) {
+    const int n = s.st->n_active;
+    int p = blockIdx.x * 128 + threadIdx.x;
+    int cnt = 0, over = 0;
+    bool act = p < n;
+    if (act) {
+        const float4 pa = s.pos[p];
+        const int ph = phase_of(pa);
+        const float fm0 = c.fm_ph[ph], rho0 = c.rho0_ph[ph];
+        const int cx = cell_coord(pa.x, g.min[0], g.divisor);
+        const int cy = cell_coord(pa.y, g.min[1], g.divisor);
+        const int cz = cell_coord(pa.z, g.min[2], g.divisor);
+        float density = ker_W(c.k, 0.f) * fm0;
+        float a1x = 0.f, a1y = 0.f, a1z = 0.f, a2 = 0.f;
+        int* out = s.nbr + p;
+        const int stride = c.stride, cap = c.cap;
+        for (int dz = -1; dz <= 1; ++dz)
+            for (int dy = -1; dy <= 1; ++dy)
+                for (int dx = -1; dx <= 1; ++dx) {
+                    int x = cx + dx, y = cy + dy, z = cz + dz;
+                    if (!cell_inside(g, x, y, z)) continue;
+                    int key = cell_key(g, x, y, z);
+                    int a = s.cell_start[key], b = s.cell_start[key + 1];
+                    for (int q = a; q < b; ++q) {
+                        if (q == p) continue;
+                        float4 pb = s.pos[q];
+                        float len2 = dis_square_rn(pa.x, pa.y, pa.z, pb.x, pb.y, pb.z);
+                        if (len2 < c.h2cut) {
+                            if (cnt < cap) {
+                                out[(size_t)cnt * stride] = q;
+                                ++cnt;
+                                if (MODE != 0) {
+                                    float dis = sqrtf(len2);
+                                    density += fm0 * ker_W(c.k, dis);
+                                    if (MODE == 1) {
+                                        float gs = -ker_Wg(c.k, dis);
+                                        float f = gs / dis;
+                                        a1x += (pa.x - pb.x) * f * fm0;
+                                        a1y += (pa.y - pb.y) * f * fm0;
+                                        a1z += (pa.z - pb.z) * f * fm0;
+                                        float t = gs * fm0;
+                                        a2 = (float)((double)a2 + (double)t * (double)t);
+                                    }
+                                }
+                            } else {
+                                ++over;
+                            }
+                        }
+                    }
+                    int ba = s.bcell_start[key], bb = s.bcell_start[key + 1];
+                    for (int q = ba; q < bb; ++q) {
+                        float4 pb = s.bpos[q];
+                        float len2 = dis_square_rn(pa.x, pa.y, pa.z, pb.x, pb.y, pb.z);
+                        if (len2 < c.h2cut) {
+                            if (cnt < cap) {
+                                out[(size_t)cnt * stride] = q | (int)BND_FLAG;
+                                ++cnt;
+                                if (MODE != 0) {
+                                    float dis = sqrtf(len2);
+                                    float vol = pb.w;
+                                    density += rho0 * vol * ker_W(c.k, dis);
+                                    if (MODE == 1) {
+                                        float gs = -ker_Wg(c.k, dis);
+                                        float f = gs / dis;
+                                        a1x += (pa.x - pb.x) * f * rho0 * vol;
+                                        a1y += (pa.y - pb.y) * f * rho0 * vol;
+                                        a1z += (pa.z - pb.z) * f * rho0 * vol;
+                                    }
+                                }
+                            } else {
+                                ++over;
+                            }
+                        }
+                    }
+                }
+        s.ncount[p] = cnt;
+        if (MODE == 1) {
+            s.rho[p] = density;
+            float al = a1x * a1x + a1y * a1y + a1z * a1z + a2;
+            if (al < 1.0e-6f) al = 1.0e-6f;
+            s.alpha[p] = density / al;
+        } else if (MODE == 2) {
+            s.rho[p] = density;
+            // Tait, WcSph.cpp:142-146 (NEGLECT_NEGATIVE_PRESSURE)
+            float pr = c.wc_B * (powf(density / rho0, c.wc_gamma) - 1.f);
+            if (pr < 0.f) pr = 0.f;
+            s.kr[p] = pr;
+        }
+    }
+    __shared__ int sh[4];
+    int tot = block_sum_int<128>(act ? cnt : 0, sh);
+    int ov = block_sum_int<128>(over, sh);
+    int mx = block_max_int<128>(act ? cnt : 0, sh);
+    if (threadIdx.x == 0) {
+        if (tot) atomicAdd(&s.st->nbr_total, (unsigned long long)tot);
+        if (ov) { atomicAdd(&s.st->overflow, ov); atomicOr(&s.st->status, 8u); }
+        if (mx) atomicMax(&s.st->max_nbrs, mx);
+    }
 }
 
 __global__ void k_boundary_keys(const float4* bpos, int nb, GridGeom g, int* keys) {
@@ -194,6 +298,13 @@ void launch_scatter_reorder(const DevScene& s, const GridGeom& g, int n_old, int
 
 void launch_count_active(const DevScene& s, const GridGeom& g, cudaStream_t st) {
     k_count_active<<<1, 1, 0, st>>>(s, g.nkeys - 1);
+}
+
+void launch_build(const DevScene& s, const GridGeom& g, const SolverConst& c, int mode, int n_max, cudaStream_t st) {
+    int nb = nblk(n_max > 0 ? n_max : 1, 128);
+    if (mode == 0) k_build<0><<<nb, 128, 0, st>>>(s, g, c);
+    else if (mode == 1) k_build<1><<<nb, 128, 0, st>>>(s, g, c);
+    else k_build<2><<<nb, 128, 0, st>>>(s, g, c);
 }
 
 void launch_boundary_keys(const float4* bpos, int nb, const GridGeom& g, int* keys, cudaStream_t st) {

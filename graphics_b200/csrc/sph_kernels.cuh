@@ -22,8 +22,6 @@ struct DevStats {
     float dt;              // current step length
     float pad1;
     unsigned ticket[4];    // last-block tickets of the reductions
-    int wide_bricks;       // bricks whose window did not fit in shared memory
-    int pad2;
 };
 
 // Per-scene device pointers passed to every kernel by value.
@@ -37,11 +35,10 @@ struct DevScene {
     float4* vadv;       // DFSPH advected velocity / WCSPH acceleration / scratch
     float4* acc;        // a_adv (DFSPH) / acceleration (WCSPH) / pressure accel (PCISPH, IISPH)
     float* kr;          // kappa/rho (DFSPH), pressure (WCSPH/PCISPH/IISPH)
-    float* kappa;       // DFkappa of the last density iteration
-    float* kappav;      // DFkappaV of the last divergence iteration
+    float* kappa;       // DFkappa / DFkappaV of the last iteration (per particle)
     float* ksum;        // summed kappa over the density loop (warm-start label)
-    float* aux0;        // rho_adv (DFSPH density loop), aii (IISPH)
-    float* aux1;        // divergence deviation (DFSPH), IISPH rho_adv, PCISPH rho*
+    float* aux0;        // rho_adv (DFSPH density), divergence deviation, aii (IISPH)
+    float* aux1;        // IISPH rho_adv, PCISPH rho*
     float4* aux4;       // IISPH d_ii / sum d_ij p_j, PCISPH predicted position
     float* kwarm;       // predicted initial kappa (learned warm start)
     // staging (unsorted) copies used by the reorder
@@ -54,12 +51,9 @@ struct DevScene {
     int* tmp;
     int* cell_count;    // nkeys + 1
     int* cell_start;    // nkeys + 1
-    // neighbour lists (ELL, column-major): 16-bit brick-window slots, and
-    // 32-bit global indices for particles of wide bricks
-    unsigned short* nbr16;
+    // neighbour lists (ELL, column-major)
     int* nbr;
     int* ncount;
-    int* brick_wide;
     // boundary, sorted once
     float4* bpos;       // (x, y, z, volume)
     float4* bvel;
@@ -80,9 +74,6 @@ void launch_scatter_reorder(const DevScene& s, const GridGeom& g, int n_old, int
 void launch_count_active(const DevScene& s, const GridGeom& g, cudaStream_t st);
 // mode 0: lists only; 1: lists + DFSPH rho/alpha; 2: lists + WCSPH rho/pressure
 void launch_build(const DevScene& s, const GridGeom& g, const SolverConst& c, int mode, int n_max, cudaStream_t st);
-void launch_expand_lists(const DevScene& s, const GridGeom& g, const SolverConst& c, cudaStream_t st);
-void dfsph_init_attributes();
-void wcsph_init_attributes();
 void launch_to_ref_order(const float4* src, const int* gid, int n, float* dst3, cudaStream_t st);
 void launch_from_ref_order(const float* src3, const int* gid, int n, float4* dst, cudaStream_t st);
 void launch_boundary_keys(const float4* bpos, int nb, const GridGeom& g, int* keys, cudaStream_t st);
@@ -90,18 +81,19 @@ void launch_boundary_volume(const DevScene& s, const GridGeom& g, float dpart, f
                             cudaStream_t st);
 
 // ---- DFSPH (sph_dfsph.cu) ----
-void launch_df_forces(const DevScene& s, const GridGeom& g, const SolverConst& c, int warm, cudaStream_t st);
-void launch_df_dens_a(const DevScene& s, const GridGeom& g, const SolverConst& c, int record, cudaStream_t st);
-void launch_df_dens_b(const DevScene& s, const GridGeom& g, const SolverConst& c, double goal, int min_it,
-                      int max_it, unsigned long long cond_handle, int use_handle, cudaStream_t st);
-void launch_df_div_a(const DevScene& s, const GridGeom& g, const SolverConst& c, cudaStream_t st);
-void launch_df_div_b(const DevScene& s, const GridGeom& g, const SolverConst& c, double goal_abs, double goal_rel,
+void launch_df_first(const DevScene& s, const SolverConst& c, int n_max, cudaStream_t st);
+void launch_df_forces(const DevScene& s, const SolverConst& c, int n_max, int warm, cudaStream_t st);
+void launch_df_dens_a(const DevScene& s, const SolverConst& c, int n_max, int record, cudaStream_t st);
+void launch_df_dens_b(const DevScene& s, const SolverConst& c, int n_max, double goal, int min_it, int max_it,
+                      unsigned long long cond_handle, int use_handle, cudaStream_t st);
+void launch_df_div_a(const DevScene& s, const SolverConst& c, int n_max, cudaStream_t st);
+void launch_df_div_b(const DevScene& s, const SolverConst& c, int n_max, double goal_abs, double goal_rel,
                      int min_it, int max_it, unsigned long long cond_handle, int use_handle, cudaStream_t st);
-void launch_df_warm_correction(const DevScene& s, const GridGeom& g, const SolverConst& c, cudaStream_t st);
+void launch_df_warm_correction(const DevScene& s, const SolverConst& c, int n_max, cudaStream_t st);
 void launch_df_loop_reset(const DevScene& s, int which, cudaStream_t st);
 void launch_cfl(const DevScene& s, int n_max, float cfl, float d, float dt_max, float dt_min, cudaStream_t st);
 void launch_step_begin(const DevScene& s, cudaStream_t st);
 void launch_call_begin(const DevScene& s, cudaStream_t st);
 
 // ---- WCSPH (sph_wcsph.cu) ----
-void launch_wc_force(const DevScene& s, const GridGeom& g, const SolverConst& c, cudaStream_t st);
+void launch_wc_force(const DevScene& s, const SolverConst& c, int n_max, cudaStream_t st);
