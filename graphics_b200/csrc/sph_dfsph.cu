@@ -11,11 +11,13 @@
 //   divergence loop   k_df_div_a / k_df_div_b             (DFSPH.cpp:769-900)
 //
 // The loop kernels read neighbour indices from the ELL lists and recompute
-// the kernel gradient from positions (the reference stores the distance per
-// pair; recomputing costs a sqrt and a few flops and saves 4 bytes per pair
-// of HBM traffic in every sweep).  Per-particle arithmetic is FP32; the
-// convergence sums are FP64 block partials reduced in a fixed order by the
-// last block, so results are run-to-run deterministic.
+// the kernel gradient from positions (-W'(r)/r with one rsqrt; the reference
+// stores the distance per pair, recomputing saves 4 bytes per pair of HBM
+// traffic in every sweep).  Neighbour state is gathered as one packed record
+// per neighbour: {position, loop velocity} (32 B) in the A sweeps and
+// (x, y, z, kappa/rho) (16 B) in the B sweeps.  Per-particle arithmetic is
+// FP32; the convergence sums are FP64 block partials reduced in a fixed order
+// by the last block, so results are run-to-run deterministic.
 //
 // Loop control: k_*_b decides whether another iteration runs.  Inside a CUDA
 // graph the loop is a conditional WHILE node and the decision is written with
@@ -24,12 +26,6 @@
 
 namespace {
 constexpr int NT = 128;
-
-// gradient factor f = -W'(r)/r and r from a squared distance
-__device__ __forceinline__ float grad_factor(const KerConst& k, float len2) {
-    float dis = sqrtf(len2);
-    return -ker_Wg(k, dis) / dis;
-}
 
 // last-block FP64 reduction of per-block partials; returns true in the
 // thread that holds the total (thread 0 of the last block).
@@ -127,15 +123,14 @@ __global__ void __launch_bounds__(NT) k_df_forces(DevScene s, SolverConst c, int
             }
         }
         s.acc[p] = make_float4(ax, ay, az, 0.f);
-        float4 v = make_float4(va.x + ax * dt, va.y + ay * dt, va.z + az * dt, 0.f);
+        s.pv[2 * p + 1] = make_float4(va.x + ax * dt, va.y + ay * dt, va.z + az * dt, 0.f);
         if (warm) {
             // learned warm start: the predicted stiffness is applied once before
             // the Jacobi loop as a pressure-velocity correction of the form of
-            // DFSPH.cpp:674 (launch_df_warm_correction, kr = kwarm/rho); the
-            // unmodified loop then runs to the same tolerance.
-            s.kr[p] = s.kwarm[p] / rhoa;
+            // DFSPH.cpp:674 (launch_df_warm_correction with kappa/rho =
+            // kwarm/rho); the unmodified loop then runs to the same tolerance.
+            s.pk[p].w = s.kwarm[p] / rhoa;
         }
-        s.vadv[p] = v;
     }
     if (__syncthreads_or(zero)) {
         if (zero) atomicAdd(&s.st->zero_dis, zero);
@@ -144,11 +139,10 @@ __global__ void __launch_bounds__(NT) k_df_forces(DevScene s, SolverConst c, int
 
 // Neighbour-sum of m_j gradW_ij . (v_i - v_j) over the stored list: the
 // common sweep of the density loop (DFSPH.cpp:589-617) and of the divergence
-// loop (DFSPH.cpp:795-825).  Fluid and boundary neighbours are read through
-// one select of the base pointers so the loads of consecutive entries can be
-// issued back to back (unrolled by 4).
-__device__ __forceinline__ float div_sweep(const DevScene& s, const SolverConst& c, const float4* V, int p,
-                                           float4 pa, float4 va) {
+// loop (DFSPH.cpp:795-825).  Each neighbour costs one 32-byte record
+// {position, loop velocity} (pv / bpv), so a gather touches one sector; the
+// loop is unrolled so consecutive records are in flight together.
+__device__ __forceinline__ float div_sweep(const DevScene& s, const SolverConst& c, int p, float4 pa, float4 va) {
     const int cnt = s.ncount[p];
     const int* L = s.nbr + p;
     const size_t stride = (size_t)c.stride;
@@ -157,9 +151,9 @@ __device__ __forceinline__ float div_sweep(const DevScene& s, const SolverConst&
     for (int k = 0; k < cnt; ++k) {
         const unsigned e = (unsigned)__ldg(L + k * stride);
         const bool bnd = (e & BND_FLAG) != 0u;
-        const unsigned j = e & BND_MASK;
-        const float4 pb = __ldg((bnd ? s.bpos : s.pos) + j);
-        const float4 vb = __ldg((bnd ? s.bvel : V) + j);
+        const float4* rec = (bnd ? s.bpv : s.pv) + 2 * (e & BND_MASK);
+        const float4 pb = __ldg(rec);
+        const float4 vb = __ldg(rec + 1);
         const float m = bnd ? c.rho0 * pb.w : c.fm0;
         const float xx = pa.x - pb.x, xy = pa.y - pb.y, xz = pa.z - pb.z;
         const float f = grad_over_r(c.k, xx * xx + xy * xy + xz * xz);
@@ -176,16 +170,16 @@ __global__ void __launch_bounds__(NT) k_df_dens_a(DevScene s, SolverConst c, int
     double mine = 0.0;
     if (p < n) {
         const float dt = *s.dt;
-        const float4 pa = s.pos[p];
-        const float4 va = s.vadv[p];
+        const float4 pa = s.pv[2 * p];
+        const float4 va = s.pv[2 * p + 1];
         const float rho0 = c.rho0;
-        const float acc = div_sweep(s, c, s.vadv, p, pa, va);
+        const float acc = div_sweep(s, c, p, pa, va);
         const float rho = s.rho[p];
         float dadv = fmaf(acc, dt, rho);
         if (dadv < rho0) dadv = rho0;
         // kappa = (rho_adv - rho0) / pow(dt,2) * alpha  (DFSPH.cpp:641)
         const float kap = (float)((double)(dadv - rho0) / ((double)dt * (double)dt) * (double)s.alpha[p]);
-        s.kr[p] = kap / rho;
+        s.pk[p].w = kap / rho;
         s.kappa[p] = kap;
         if (record) s.ksum[p] += kap;
         s.aux0[p] = dadv;
@@ -199,8 +193,9 @@ __global__ void __launch_bounds__(NT) k_df_dens_a(DevScene s, SolverConst c, int
     }
 }
 
-// density/divergence loop, part B: v_adv update with kr = kappa/rho
-// (DFSPH.cpp:647-693 / 840-883); then the loop decision.
+// density/divergence loop, part B: v_adv update with k = kappa/rho
+// (DFSPH.cpp:647-693 / 840-883); then the loop decision.  Each neighbour
+// costs one 16-byte record (x, y, z, k) (pk; boundary: (x, y, z, volume)).
 template <int DIV, int DECIDE>
 __global__ void __launch_bounds__(NT) k_df_vupdate(DevScene s, SolverConst c, double goal_abs, double goal_rel,
                                                    int min_it, int max_it, cudaGraphConditionalHandle h,
@@ -209,10 +204,9 @@ __global__ void __launch_bounds__(NT) k_df_vupdate(DevScene s, SolverConst c, do
     const int p = blockIdx.x * NT + threadIdx.x;
     if (p < n) {
         const float dt = *s.dt;
-        const float4 pa = s.pos[p];
-        float4* V = DIV ? s.vel : s.vadv;
-        float4 va = V[p];
-        const float ka = s.kr[p];
+        const float4 pa = s.pk[p];
+        float4 va = s.pv[2 * p + 1];
+        const float ka = pa.w;
         const float fa = c.fm0 * ka, ba = c.rho0 * ka;
         float dx = 0.f, dy = 0.f, dz = 0.f;
         const int cnt = s.ncount[p];
@@ -223,9 +217,8 @@ __global__ void __launch_bounds__(NT) k_df_vupdate(DevScene s, SolverConst c, do
             const unsigned e = (unsigned)__ldg(L + k * stride);
             const bool bnd = (e & BND_FLAG) != 0u;
             const unsigned j = e & BND_MASK;
-            const float4 pb = __ldg((bnd ? s.bpos : s.pos) + j);
-            const float kj = bnd ? 0.f : __ldg(s.kr + j);
-            const float w = bnd ? ba * pb.w : fmaf(c.fm0, kj, fa);
+            const float4 pb = __ldg(bnd ? s.bpv + 2 * j : s.pk + j);
+            const float w = bnd ? ba * pb.w : fmaf(c.fm0, pb.w, fa);
             const float xx = pa.x - pb.x, xy = pa.y - pb.y, xz = pa.z - pb.z;
             const float f = grad_over_r(c.k, xx * xx + xy * xy + xz * xz) * w;
             dx = fmaf(xx, f, dx);
@@ -235,7 +228,8 @@ __global__ void __launch_bounds__(NT) k_df_vupdate(DevScene s, SolverConst c, do
         va.x = fmaf(-dx, dt, va.x);
         va.y = fmaf(-dy, dt, va.y);
         va.z = fmaf(-dz, dt, va.z);
-        V[p] = va;
+        s.pv[2 * p + 1] = va;
+        if (DIV) s.vel[p] = va;  // velocity = vel_adv (DFSPH.cpp:909)
     }
     if (DECIDE && blockIdx.x == 0 && threadIdx.x == 0) {
         // convergence decision of the iteration that just finished
@@ -270,15 +264,15 @@ __global__ void __launch_bounds__(NT) k_df_div_a(DevScene s, SolverConst c) {
     double mine = 0.0;
     if (p < n) {
         const float dt = *s.dt;
-        const float4 pa = s.pos[p];
-        const float4 va = s.vel[p];
-        float dd = div_sweep(s, c, s.vel, p, pa, va);
+        const float4 pa = s.pv[2 * p];
+        const float4 va = s.pv[2 * p + 1];
+        float dd = div_sweep(s, c, p, pa, va);
         const float rho = s.rho[p];
         if (dd < 0.f || (rho + dd * dt) < c.rho0) dd = 0.f;  // DFSPH.cpp:829-832
         const float kv = dd * s.alpha[p] / dt;              // DFSPH.cpp:835
-        s.kr[p] = kv / rho;
-        s.kappa[p] = kv;
-        s.aux0[p] = dd;
+        s.pk[p].w = kv / rho;
+        s.kappav[p] = kv;
+        s.aux1[p] = dd;
         mine = (double)dd;
     }
     __shared__ double sh[NT / 32];

@@ -196,7 +196,8 @@ int alloc_scene(sphgpu_scene* h) {
     int r = 0;
     r |= dalloc(h, &d.pos, n); r |= dalloc(h, &d.vel, n); r |= dalloc(h, &d.gid, n);
     r |= dalloc(h, &d.rho, n); r |= dalloc(h, &d.alpha, n); r |= dalloc(h, &d.vadv, n);
-    r |= dalloc(h, &d.acc, n); r |= dalloc(h, &d.kr, n); r |= dalloc(h, &d.kappa, n);
+    r |= dalloc(h, &d.acc, n); r |= dalloc(h, &d.kr, n); r |= dalloc(h, &d.kappa, n); r |= dalloc(h, &d.kappav, n);
+    r |= dalloc(h, &d.pv, 2 * (size_t)n); r |= dalloc(h, &d.pk, n);
     r |= dalloc(h, &d.ksum, n); r |= dalloc(h, &d.aux0, n); r |= dalloc(h, &d.aux1, n);
     r |= dalloc(h, &d.aux4, n); r |= dalloc(h, &d.kwarm, n);
     r |= dalloc(h, &d.pos_s, n); r |= dalloc(h, &d.vel_s, n); r |= dalloc(h, &d.gid_s, n);
@@ -231,7 +232,7 @@ int alloc_scene(sphgpu_scene* h) {
 
 void free_scene(sphgpu_scene* h) {
     DevScene& d = h->d;
-    void* ptrs[] = {d.pos, d.vel, d.gid, d.rho, d.alpha, d.vadv, d.acc, d.kr, d.kappa, d.ksum, d.aux0,
+    void* ptrs[] = {d.pos, d.vel, d.gid, d.rho, d.alpha, d.vadv, d.pv, d.pk, d.bpv, d.kappav, d.acc, d.kr, d.kappa, d.ksum, d.aux0,
                     d.aux1, d.aux4, d.kwarm, d.pos_s, d.vel_s, d.gid_s, d.kwarm_s, d.key, d.slot, d.tmp,
                     d.cell_count, d.cell_start, d.bcell_start, d.nbr, d.ncount, d.partial, d.st,
                     d.bpos, d.bvel, d.bgid, h->cub_tmp};
@@ -602,12 +603,13 @@ int sphgpu_set_boundary(sphgpu_t h, int n, const float* xyz, const int* solid_id
     if (!h || n < 0 || (n > 0 && !xyz)) return SPHGPU_EINVAL;
     cudaSetDevice(h->device);
     DevScene& d = h->d;
-    if (d.bpos) { cudaFree(d.bpos); cudaFree(d.bvel); cudaFree(d.bgid); d.bpos = nullptr; }
+    if (d.bpos) { cudaFree(d.bpos); cudaFree(d.bvel); cudaFree(d.bgid); cudaFree(d.bpv); d.bpos = nullptr; }
     h->nb = n;
     d.nb = n;
     std::vector<float4> bp(n);
     for (int i = 0; i < n; ++i) bp[i] = make_float4(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], volume ? volume[i] : 0.f);
-    if (dalloc(h, &d.bpos, n) || dalloc(h, &d.bvel, n) || dalloc(h, &d.bgid, n)) return SPHGPU_ENOMEM;
+    if (dalloc(h, &d.bpos, n) || dalloc(h, &d.bvel, n) || dalloc(h, &d.bgid, n) || dalloc(h, &d.bpv, 2 * (size_t)n))
+        return SPHGPU_ENOMEM;
     std::vector<int> keys(n);
     int* dkeys = nullptr;
     if (dalloc(h, &dkeys, n)) return SPHGPU_ENOMEM;
@@ -654,6 +656,12 @@ int sphgpu_set_boundary(sphgpu_t h, int n, const float* xyz, const int* solid_id
     if (!volume) {
         launch_boundary_volume(d, h->g, h->P.particle_d, h->c.h2cut, h->ncap, h->stream);
         CK(cudaStreamSynchronize(h->stream));
+    }
+    // packed {(x, y, z, volume), velocity} records for the sweeps
+    if (n) {
+        CK(cudaMemcpy2D(d.bpv, 2 * sizeof(float4), d.bpos, sizeof(float4), sizeof(float4), n, cudaMemcpyDeviceToDevice));
+        CK(cudaMemcpy2D(d.bpv + 1, 2 * sizeof(float4), d.bvel, sizeof(float4), sizeof(float4), n,
+                        cudaMemcpyDeviceToDevice));
     }
     invalidate_graphs(h);
     h->ns_valid = false;
@@ -779,14 +787,22 @@ int sphgpu_get_fluid(sphgpu_t h, const char* field, float* out) {
     DevScene& d = h->d;
     if (f == "position") { src = staging ? d.pos_s : d.pos; f4 = true; comps = 3; }
     else if (f == "velocity") { src = staging ? d.vel_s : d.vel; f4 = true; comps = 3; }
-    else if (f == "vel_adv") { src = d.vadv; f4 = true; comps = 3; }
+    else if (f == "vel_adv") {
+        CK(cudaMemcpy2D(d.vadv, sizeof(float4), d.pv + 1, 2 * sizeof(float4), sizeof(float4), n,
+                        cudaMemcpyDeviceToDevice));
+        src = d.vadv;
+        f4 = true;
+        comps = 3;
+    }
     else if (f == "acce_adv" || f == "acceleration") { src = d.acc; f4 = true; comps = 3; }
     else if (f == "density") src = d.rho;
     else if (f == "DFalpha") src = d.alpha;
-    else if (f == "DFkappa" || f == "DFkappaV") src = d.kappa;
+    else if (f == "DFkappa") src = d.kappa;
+    else if (f == "DFkappaV") src = d.kappav;
     else if (f == "kappa_sum") src = d.ksum;
     else if (f == "kappa_warm") src = d.kwarm;
-    else if (f == "density_adv" || f == "divergenceDeviation") src = d.aux0;
+    else if (f == "density_adv") src = d.aux0;
+    else if (f == "divergenceDeviation") src = d.aux1;
     else if (f == "presure") src = d.kr;
     else if (f == "neighbour_count") {
         std::vector<int> cnt(n);
@@ -827,7 +843,9 @@ int sphgpu_set_fluid(sphgpu_t h, const char* field, const float* in) {
         float* tmp3 = (float*)d.aux4;
         CK(cudaMemcpyAsync(tmp3, in, sizeof(float) * 3 * (size_t)n, cudaMemcpyHostToDevice, h->stream));
         launch_from_ref_order(tmp3, staging ? d.gid_s : d.gid, n, dst, h->stream);
-        if (f == "position" && !staging) {
+        if (!staging) {
+            // the sorted arrays are the state: stage them so the next search
+            // rebuilds lists, rho/alpha and the packed sweep records
             h->ns_valid = false;
             CK(cudaMemcpyAsync(d.pos_s, d.pos, sizeof(float4) * n, cudaMemcpyDeviceToDevice, h->stream));
             CK(cudaMemcpyAsync(d.vel_s, d.vel, sizeof(float4) * n, cudaMemcpyDeviceToDevice, h->stream));
@@ -849,7 +867,7 @@ int sphgpu_set_fluid(sphgpu_t h, const char* field, const float* in) {
             v.x = in[3 * k]; v.y = in[3 * k + 1]; v.z = in[3 * k + 2];
         }
         CK(cudaMemcpy(dst, t.data(), sizeof(float4) * n, cudaMemcpyHostToDevice));
-        if (f == "position" && !staging) {
+        if (!staging) {
             // positions changed: lists and rho/alpha must be rebuilt
             h->ns_valid = false;
             // the sorted arrays are the state; stage them for the next sort

@@ -36,7 +36,7 @@ __global__ void __launch_bounds__(NT) k_hash(DevScene s, GridGeom g, float3 smin
             // (DFSPH.cpp:705-715), in round-to-nearest float ops.
             float dt = *s.dt;
             p = s.pos[i];
-            v = s.vadv[i];
+            v = s.pv[2 * i + 1];  // v_adv of the density loop
             p.x = __fadd_rn(p.x, __fmul_rn(v.x, dt));
             p.y = __fadd_rn(p.y, __fmul_rn(v.y, dt));
             p.z = __fadd_rn(p.z, __fmul_rn(v.z, dt));
@@ -89,8 +89,12 @@ __global__ void __launch_bounds__(NT) k_rank_reorder(DevScene s, int dead_key, i
     int my = s.gid_s[i], cnt = 0;
     for (int r = a; r < b; ++r) cnt += s.gid_s[s.tmp[r]] > my;
     int p = a + cnt;
-    s.pos[p] = s.pos_s[i];
-    s.vel[p] = s.vel_s[i];
+    const float4 x = s.pos_s[i], v = s.vel_s[i];
+    s.pos[p] = x;
+    s.vel[p] = v;
+    s.pv[2 * p] = x;
+    s.pv[2 * p + 1] = v;
+    s.pk[p] = make_float4(x.x, x.y, x.z, 0.f);
     s.gid[p] = my;
     if (carry_kwarm) s.kwarm[p] = s.kwarm_s[i];
 }

@@ -32,13 +32,18 @@ struct DevScene {
     int* gid;
     float* rho;
     float* alpha;
-    float4* vadv;       // DFSPH advected velocity / WCSPH acceleration / scratch
+    float4* vadv;       // scratch (reference-order transfers)
+    float4* pv;         // 2 per particle: {position, loop velocity} -- the one
+                        // 32-byte record the A sweeps gather per neighbour
+    float4* pk;         // (x, y, z, kappa/rho) -- the record the B sweeps gather
+    float4* bpv;        // 2 per boundary particle: {(x,y,z,volume), velocity}
     float4* acc;        // a_adv (DFSPH) / acceleration (WCSPH) / pressure accel (PCISPH, IISPH)
     float* kr;          // kappa/rho (DFSPH), pressure (WCSPH/PCISPH/IISPH)
-    float* kappa;       // DFkappa / DFkappaV of the last iteration (per particle)
+    float* kappa;       // DFkappa of the last density iteration
+    float* kappav;      // DFkappaV of the last divergence iteration
     float* ksum;        // summed kappa over the density loop (warm-start label)
-    float* aux0;        // rho_adv (DFSPH density), divergence deviation, aii (IISPH)
-    float* aux1;        // IISPH rho_adv, PCISPH rho*
+    float* aux0;        // rho_adv (DFSPH density loop), aii (IISPH)
+    float* aux1;        // divergence deviation (DFSPH), IISPH rho_adv, PCISPH rho*
     float4* aux4;       // IISPH d_ii / sum d_ij p_j, PCISPH predicted position
     float* kwarm;       // predicted initial kappa (learned warm start)
     // staging (unsorted) copies used by the reorder
