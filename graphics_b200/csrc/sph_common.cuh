@@ -7,9 +7,10 @@
 //   gid   int   global fluid index (phase-major insertion order; the
 //               reference's m_Fluids[k].fluidParticles[i] order)
 //   rho, alpha, ... float per particle
-//   nbr   int   ELL neighbour list, column-major: entry k of particle p at
-//               nbr[k * stride + p]; fluid neighbour j -> j, boundary
-//               neighbour b -> b | BND_FLAG
+//   nbr   int   ELL neighbour list in groups of four, column-major: entry k
+//               of particle p at nbr[((k / 4) * stride + p) * 4 + k % 4], so
+//               one 16-byte load gives a thread four entries; fluid
+//               neighbour j -> j, boundary neighbour b -> b | BND_FLAG
 //   boundary: bpos float4 (x, y, z, volume), bvel float4
 //
 // Cell keys: the reference's uniform grid (cell = smoothRadius_h,
@@ -118,6 +119,15 @@ __device__ __forceinline__ bool cell_inside(const GridGeom& g, int cx, int cy, i
 }
 
 __device__ __forceinline__ int phase_of(float4 p) { return __float_as_int(p.w); }
+
+// ELL4 addressing (see the layout note at the top)
+__device__ __forceinline__ size_t ell_index(size_t stride, int p, int k) {
+    return ((size_t)(k >> 2) * stride + (size_t)p) * 4 + (k & 3);
+}
+__device__ __forceinline__ int ell_get(const int* L, size_t stride, int p, int k) { return L[ell_index(stride, p, k)]; }
+__device__ __forceinline__ int4 ell_group(const int* L, size_t stride, int p, int g) {
+    return __ldg(reinterpret_cast<const int4*>(L) + (size_t)g * stride + p);
+}
 
 // ---- reductions ----
 template <int NT>

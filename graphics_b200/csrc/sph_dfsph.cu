@@ -95,9 +95,9 @@ __global__ void __launch_bounds__(NT) k_df_forces(DevScene s, SolverConst c, int
         const float visc = 10.f * c.nu;
         float ax = c.gravity[0], ay = c.gravity[1], az = c.gravity[2];
         const int cnt = s.ncount[p];
-        const int* L = s.nbr + p;
+        const size_t stride = (size_t)c.stride;
         for (int k = 0; k < cnt; ++k) {
-            const unsigned e = (unsigned)L[(size_t)k * c.stride];
+            const unsigned e = (unsigned)ell_get(s.nbr, stride, p, k);
             float4 pb, vb;
             float m;
             if (e & BND_FLAG) {
@@ -139,26 +139,41 @@ __global__ void __launch_bounds__(NT) k_df_forces(DevScene s, SolverConst c, int
 
 // Neighbour-sum of m_j gradW_ij . (v_i - v_j) over the stored list: the
 // common sweep of the density loop (DFSPH.cpp:589-617) and of the divergence
-// loop (DFSPH.cpp:795-825).  Each neighbour costs one 32-byte record
-// {position, loop velocity} (pv / bpv), so a gather touches one sector; the
-// loop is unrolled so consecutive records are in flight together.
+// loop (DFSPH.cpp:795-825).  Indices come four at a time (one 16-byte load),
+// the next group's load is issued before the current group's four record
+// gathers, and each neighbour costs one 32-byte record {position, loop
+// velocity} (pv / bpv).  Entries past the count read the particle's own
+// record and are masked out.
 __device__ __forceinline__ float div_sweep(const DevScene& s, const SolverConst& c, int p, float4 pa, float4 va) {
     const int cnt = s.ncount[p];
-    const int* L = s.nbr + p;
+    const int ng = (cnt + 3) >> 2;
     const size_t stride = (size_t)c.stride;
     float acc = 0.f;
-#pragma unroll 4
-    for (int k = 0; k < cnt; ++k) {
-        const unsigned e = (unsigned)__ldg(L + k * stride);
-        const bool bnd = (e & BND_FLAG) != 0u;
-        const float4* rec = (bnd ? s.bpv : s.pv) + 2 * (e & BND_MASK);
-        const float4 pb = __ldg(rec);
-        const float4 vb = __ldg(rec + 1);
-        const float m = bnd ? c.rho0 * pb.w : c.fm0;
-        const float xx = pa.x - pb.x, xy = pa.y - pb.y, xz = pa.z - pb.z;
-        const float f = grad_over_r(c.k, xx * xx + xy * xy + xz * xz);
-        const float dot = xx * (va.x - vb.x) + xy * (va.y - vb.y) + xz * (va.z - vb.z);
-        acc = fmaf(dot * f, m, acc);
+    int4 nxt = ng ? ell_group(s.nbr, stride, p, 0) : make_int4(0, 0, 0, 0);
+    for (int gi = 0; gi < ng; ++gi) {
+        const int4 cur = nxt;
+        if (gi + 1 < ng) nxt = ell_group(s.nbr, stride, p, gi + 1);
+        const unsigned e[4] = {(unsigned)cur.x, (unsigned)cur.y, (unsigned)cur.z, (unsigned)cur.w};
+        float4 pb[4], vb[4];
+        bool ok[4], bnd[4];
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            ok[t] = gi * 4 + t < cnt;
+            const unsigned u = ok[t] ? e[t] : (unsigned)p;
+            bnd[t] = (u & BND_FLAG) != 0u;
+            const float4* rec = (bnd[t] ? s.bpv : s.pv) + 2 * (size_t)(u & BND_MASK);
+            pb[t] = __ldg(rec);
+            vb[t] = __ldg(rec + 1);
+        }
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            const float m = bnd[t] ? c.rho0 * pb[t].w : c.fm0;
+            const float xx = pa.x - pb[t].x, xy = pa.y - pb[t].y, xz = pa.z - pb[t].z;
+            const float f = grad_over_r(c.k, xx * xx + xy * xy + xz * xz);
+            const float dot = xx * (va.x - vb[t].x) + xy * (va.y - vb[t].y) + xz * (va.z - vb[t].z);
+            const float nacc = fmaf(dot * f, m, acc);
+            acc = ok[t] ? nacc : acc;
+        }
     }
     return acc;
 }
@@ -210,20 +225,32 @@ __global__ void __launch_bounds__(NT) k_df_vupdate(DevScene s, SolverConst c, do
         const float fa = c.fm0 * ka, ba = c.rho0 * ka;
         float dx = 0.f, dy = 0.f, dz = 0.f;
         const int cnt = s.ncount[p];
-        const int* L = s.nbr + p;
+        const int ng = (cnt + 3) >> 2;
         const size_t stride = (size_t)c.stride;
-#pragma unroll 4
-        for (int k = 0; k < cnt; ++k) {
-            const unsigned e = (unsigned)__ldg(L + k * stride);
-            const bool bnd = (e & BND_FLAG) != 0u;
-            const unsigned j = e & BND_MASK;
-            const float4 pb = __ldg(bnd ? s.bpv + 2 * j : s.pk + j);
-            const float w = bnd ? ba * pb.w : fmaf(c.fm0, pb.w, fa);
-            const float xx = pa.x - pb.x, xy = pa.y - pb.y, xz = pa.z - pb.z;
-            const float f = grad_over_r(c.k, xx * xx + xy * xy + xz * xz) * w;
-            dx = fmaf(xx, f, dx);
-            dy = fmaf(xy, f, dy);
-            dz = fmaf(xz, f, dz);
+        int4 nxt = ng ? ell_group(s.nbr, stride, p, 0) : make_int4(0, 0, 0, 0);
+        for (int gi = 0; gi < ng; ++gi) {
+            const int4 cur = nxt;
+            if (gi + 1 < ng) nxt = ell_group(s.nbr, stride, p, gi + 1);
+            const unsigned e[4] = {(unsigned)cur.x, (unsigned)cur.y, (unsigned)cur.z, (unsigned)cur.w};
+            float4 pb[4];
+            bool ok[4], bnd[4];
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                ok[t] = gi * 4 + t < cnt;
+                const unsigned u = ok[t] ? e[t] : (unsigned)p;
+                bnd[t] = (u & BND_FLAG) != 0u;
+                const unsigned j = u & BND_MASK;
+                pb[t] = __ldg(bnd[t] ? s.bpv + 2 * (size_t)j : s.pk + j);
+            }
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                const float w = bnd[t] ? ba * pb[t].w : fmaf(c.fm0, pb[t].w, fa);
+                const float xx = pa.x - pb[t].x, xy = pa.y - pb[t].y, xz = pa.z - pb[t].z;
+                const float f = ok[t] ? grad_over_r(c.k, xx * xx + xy * xy + xz * xz) * w : 0.f;
+                dx = fmaf(xx, f, dx);
+                dy = fmaf(xy, f, dy);
+                dz = fmaf(xz, f, dz);
+            }
         }
         va.x = fmaf(-dx, dt, va.x);
         va.y = fmaf(-dy, dt, va.y);

@@ -206,7 +206,7 @@ int alloc_scene(sphgpu_scene* h) {
     r |= dalloc(h, &d.cell_count, (size_t)h->g.nkeys + 1);
     r |= dalloc(h, &d.cell_start, (size_t)h->g.nkeys + 1);
     r |= dalloc(h, &d.bcell_start, (size_t)h->g.nkeys + 1);
-    r |= dalloc(h, &d.nbr, (size_t)h->stride * h->ncap);
+    r |= dalloc(h, &d.nbr, (size_t)h->stride * ((h->ncap + 3) / 4) * 4);
     r |= dalloc(h, &d.ncount, n);
     r |= dalloc(h, &d.partial, (size_t)n / 64 + 4096);
     r |= dalloc(h, &d.st, 1);
@@ -972,7 +972,7 @@ int sphgpu_get_neighbours(sphgpu_t h, int* counts, int* t, int* idx) {
     std::vector<int> gid;
     int n;
     if (download_gid(h, gid, n, false)) return SPHGPU_ECUDA;
-    std::vector<int> cnt(n), L((size_t)h->stride * h->ncap);
+    std::vector<int> cnt(n), L((size_t)h->stride * ((h->ncap + 3) / 4) * 4);
     CK(cudaMemcpy(cnt.data(), h->d.ncount, sizeof(int) * n, cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(L.data(), h->d.nbr, sizeof(int) * L.size(), cudaMemcpyDeviceToHost));
     std::vector<float4> pos(n);
@@ -1003,7 +1003,7 @@ int sphgpu_get_neighbours(sphgpu_t h, int* counts, int* t, int* idx) {
         int p = order[k];
         counts[k] = cnt[p];
         for (int j = 0; j < cnt[p]; ++j) {
-            unsigned e = (unsigned)L[(size_t)j * h->stride + p];
+            unsigned e = (unsigned)L[((size_t)(j >> 2) * h->stride + p) * 4 + (j & 3)];
             int tt, ii;
             if (e & BND_FLAG) {
                 int g = h->bgid_h[e & BND_MASK];

@@ -124,7 +124,7 @@ __global__ void __launch_bounds__(128) k_build(DevScene s, GridGeom g, SolverCon
         const int cz = cell_coord(pa.z, g.min[2], g.divisor);
         float density = ker_W(c.k, 0.f) * fm0;
         float a1x = 0.f, a1y = 0.f, a1z = 0.f, a2 = 0.f;
-        int* out = s.nbr + p;
+        int* out = s.nbr;
         const int stride = c.stride, cap = c.cap;
         for (int dz = -1; dz <= 1; ++dz)
             for (int dy = -1; dy <= 1; ++dy)
@@ -139,7 +139,7 @@ __global__ void __launch_bounds__(128) k_build(DevScene s, GridGeom g, SolverCon
                         float len2 = dis_square_rn(pa.x, pa.y, pa.z, pb.x, pb.y, pb.z);
                         if (len2 < c.h2cut) {
                             if (cnt < cap) {
-                                out[(size_t)cnt * stride] = q;
+                                out[ell_index(stride, p, cnt)] = q;
                                 ++cnt;
                                 if (MODE != 0) {
                                     float dis = sqrtf(len2);
@@ -165,7 +165,7 @@ __global__ void __launch_bounds__(128) k_build(DevScene s, GridGeom g, SolverCon
                         float len2 = dis_square_rn(pa.x, pa.y, pa.z, pb.x, pb.y, pb.z);
                         if (len2 < c.h2cut) {
                             if (cnt < cap) {
-                                out[(size_t)cnt * stride] = q | (int)BND_FLAG;
+                                out[ell_index(stride, p, cnt)] = q | (int)BND_FLAG;
                                 ++cnt;
                                 if (MODE != 0) {
                                     float dis = sqrtf(len2);

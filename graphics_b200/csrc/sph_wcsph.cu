@@ -27,9 +27,9 @@ __global__ void __launch_bounds__(NT) k_wc_force(DevScene s, SolverConst c) {
         const float pa_term = pra / (ra * ra);
         float ax = c.gravity[0], ay = c.gravity[1], az = c.gravity[2];
         const int cnt = s.ncount[p];
-        const int* L = s.nbr + p;
+        const size_t stride = (size_t)c.stride;
         for (int k = 0; k < cnt; ++k) {
-            const unsigned e = (unsigned)L[(size_t)k * c.stride];
+            const unsigned e = (unsigned)ell_get(s.nbr, stride, p, k);
             float acce;
             float4 pb;
             float xx, xy, xz, dis;
