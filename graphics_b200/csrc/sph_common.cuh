@@ -120,6 +120,14 @@ __device__ __forceinline__ bool cell_inside(const GridGeom& g, int cx, int cy, i
 
 __device__ __forceinline__ int phase_of(float4 p) { return __float_as_int(p.w); }
 
+// One 32-byte record in a single 256-bit load (sm_100 ld.global.v8; the
+// address must be 32-byte aligned, which the packed pv/bpv arrays are).
+__device__ __forceinline__ void ld_record32(const float4* p, float4& a, float4& b) {
+    asm volatile("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
+                 : "l"(p));
+}
+
 // ELL4 addressing (see the layout note at the top)
 __device__ __forceinline__ size_t ell_index(size_t stride, int p, int k) {
     return ((size_t)(k >> 2) * stride + (size_t)p) * 4 + (k & 3);

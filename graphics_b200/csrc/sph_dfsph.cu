@@ -142,7 +142,7 @@ __global__ void __launch_bounds__(NT) k_df_forces(DevScene s, SolverConst c, int
 // loop (DFSPH.cpp:795-825).  Indices come four at a time (one 16-byte load),
 // the next group's load is issued before the current group's four record
 // gathers, and each neighbour costs one 32-byte record {position, loop
-// velocity} (pv / bpv).  Entries past the count read the particle's own
+// velocity} (pv / bpv) fetched by one 256-bit load.  Entries past the count read the particle's own
 // record and are masked out.
 __device__ __forceinline__ float div_sweep(const DevScene& s, const SolverConst& c, int p, float4 pa, float4 va) {
     const int cnt = s.ncount[p];
@@ -162,8 +162,7 @@ __device__ __forceinline__ float div_sweep(const DevScene& s, const SolverConst&
             const unsigned u = ok[t] ? e[t] : (unsigned)p;
             bnd[t] = (u & BND_FLAG) != 0u;
             const float4* rec = (bnd[t] ? s.bpv : s.pv) + 2 * (size_t)(u & BND_MASK);
-            pb[t] = __ldg(rec);
-            vb[t] = __ldg(rec + 1);
+            ld_record32(rec, pb[t], vb[t]);
         }
 #pragma unroll
         for (int t = 0; t < 4; ++t) {
