@@ -70,7 +70,23 @@ SIGNATURES = {
     "sphgpu_profile": (_i, [_vp, _i]),
     "sphgpu_profile_read": (_i, [_vp, _cp, _i, C.POINTER(C.c_double), _ip, _i]),
     "sphgpu_last_error": (_i, [_vp, _cp, _i]),
+    "sphgpu_mlp_create": (_i, [_i, _i, C.c_uint64, C.POINTER(_vp)]),
+    "sphgpu_mlp_destroy": (_i, [_vp]),
+    "sphgpu_mlp_set_params": (_i, [_vp, _fp]),
+    "sphgpu_mlp_get_params": (_i, [_vp, _fp]),
+    "sphgpu_mlp_set_norm": (_i, [_vp, _fp]),
+    "sphgpu_mlp_get_norm": (_i, [_vp, _fp]),
+    "sphgpu_mlp_dataset_size": (_i, [_vp]),
+    "sphgpu_mlp_dataset_set": (_i, [_vp, _fp, _fp, _i]),
+    "sphgpu_mlp_dataset_get": (_i, [_vp, _fp, _fp, _i]),
+    "sphgpu_mlp_dataset_shuffle": (_i, [_vp, C.c_uint64]),
+    "sphgpu_mlp_train": (_i, [_vp, _i, _i, _f, _fp]),
+    "sphgpu_mlp_gradient": (_i, [_vp, _fp, _fp, _i, _fp, _fp]),
+    "sphgpu_mlp_predict": (_i, [_vp, _fp, _fp, _i]),
+    "sphgpu_attach_warm_start": (_i, [_vp, _vp, _i, _i]),
 }
+MLP_NPARAM = 5313
+MLP_IN = 16
 EXTRA = {"sphgpu_debug_set": (_i, [_vp, _cp, _i])}
 
 _lib = None

@@ -19,6 +19,16 @@
 
 #include "../../include/sphgpu.h"
 #include "sph_kernels.cuh"
+#include "sph_mlp.cuh"
+
+// warm-start kernels (sph_mlp.cu)
+void mlp_init_attributes();
+void ws_init_attributes();
+void launch_ws_features(const DevScene& s, const SolverConst& c, const MlpDev& m, int infer, float dt_max,
+                        float alpha_ref, float* Xout, int n_max, cudaStream_t st);
+void launch_ws_post(const DevScene& s, const SolverConst& c, float* yout, int n_max, cudaStream_t st);
+void launch_ws_append(const float* X, const float* y, int n_max, const int* n_act, int every, int offset, float* dsX,
+                      float* dsy, int* ds_count, int ds_cap, cudaStream_t st);
 
 namespace {
 
@@ -36,6 +46,19 @@ struct Prof {
 };
 
 }  // namespace
+
+// Warm-start network + its training set (one per sphgpu_mlp handle).
+struct sphgpu_mlp {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    MlpDev m{};
+    float* dsX = nullptr;
+    float* dsy = nullptr;
+    int* ds_count = nullptr;
+    int ds_cap = 0;
+    int adam_t = 0;
+    std::string err;
+};
 
 struct sphgpu_scene {
     SphParams P;
@@ -63,8 +86,15 @@ struct sphgpu_scene {
     std::vector<int> bgid_h;
     std::vector<int> bsolid_h;
     int nb = 0;
-    bool have_kwarm = false;
     int record_ksum = 0;
+    // learned warm start: 0 off, 1 apply the network, 2 record training data
+    sphgpu_mlp* mlp = nullptr;
+    int ws_mode = 0;
+    int ws_every = 10;
+    int ws_offset = 0;
+    float* recX = nullptr;  // [cap][16] features of the step being recorded
+    float* recY = nullptr;  // [cap] labels
+    float alpha_ref = 1.f;
     long long total_removed = 0;  // gid stays a permutation of [0, n) while 0
 };
 
@@ -178,6 +208,24 @@ void fill_solver_const(sphgpu_scene* h) {
     c.wc_B = c.rho0 * P.soundSpeed_cs * P.soundSpeed_cs / P.wc_gamma;
     c.cap = h->ncap;
     c.stride = h->stride;
+    // alpha of an interior particle of the ideal cubic lattice (spacing d),
+    // the normalisation of the warm-start feature log(alpha / alpha_ref)
+    {
+        double hk = kh, th = c.k.theta, thh = c.k.thetah, d = P.particle_d, rho = 0, s2 = 0;
+        auto W = [&](double r) { double q = r / hk, t = 2 - q; return q <= 1 ? th * (1 - 1.5 * q * q + 0.75 * q * q * q) : th * 0.25 * t * t * t; };
+        auto Wg = [&](double r) { double q = r / hk, t = 2 - q; return q <= 1 ? thh * (3 * q - 2.25 * q * q) : thh * 0.75 * t * t; };
+        rho = W(0);
+        for (int i = -2; i <= 2; ++i)
+            for (int j = -2; j <= 2; ++j)
+                for (int k = -2; k <= 2; ++k) {
+                    double r = d * std::sqrt((double)(i * i + j * j + k * k));
+                    if (r <= 0 || r >= 2 * d) continue;
+                    rho += W(r);
+                    s2 += (c.fm0 * Wg(r)) * (c.fm0 * Wg(r));
+                }
+        rho *= c.fm0;
+        h->alpha_ref = s2 > 0 ? (float)(rho / s2) : 1.f;
+    }
 }
 
 template <class T>
@@ -199,9 +247,9 @@ int alloc_scene(sphgpu_scene* h) {
     r |= dalloc(h, &d.acc, n); r |= dalloc(h, &d.kr, n); r |= dalloc(h, &d.kappa, n); r |= dalloc(h, &d.kappav, n);
     r |= dalloc(h, &d.pv, 2 * (size_t)n); r |= dalloc(h, &d.pk, n);
     r |= dalloc(h, &d.ksum, n); r |= dalloc(h, &d.aux0, n); r |= dalloc(h, &d.aux1, n);
-    r |= dalloc(h, &d.aux4, n); r |= dalloc(h, &d.kwarm, n);
+    r |= dalloc(h, &d.aux4, n); r |= dalloc(h, &d.kwarm, n); r |= dalloc(h, &d.hist, n); r |= dalloc(h, &d.wsbuf, n);
     r |= dalloc(h, &d.pos_s, n); r |= dalloc(h, &d.vel_s, n); r |= dalloc(h, &d.gid_s, n);
-    r |= dalloc(h, &d.kwarm_s, n);
+    r |= dalloc(h, &d.hist_s, n);
     r |= dalloc(h, &d.key, n); r |= dalloc(h, &d.slot, n); r |= dalloc(h, &d.tmp, n);
     r |= dalloc(h, &d.cell_count, (size_t)h->g.nkeys + 1);
     r |= dalloc(h, &d.cell_start, (size_t)h->g.nkeys + 1);
@@ -218,7 +266,8 @@ int alloc_scene(sphgpu_scene* h) {
     cudaMemsetAsync(d.bcell_start, 0, sizeof(int) * ((size_t)h->g.nkeys + 1), h->stream);
     cudaMemsetAsync(d.ksum, 0, sizeof(float) * n, h->stream);
     cudaMemsetAsync(d.kwarm, 0, sizeof(float) * n, h->stream);
-    cudaMemsetAsync(d.kwarm_s, 0, sizeof(float) * n, h->stream);
+    cudaMemsetAsync(d.hist, 0, sizeof(float4) * n, h->stream);
+    cudaMemsetAsync(d.hist_s, 0, sizeof(float4) * n, h->stream);
     // CUB scan scratch
     cub::DeviceScan::ExclusiveSum(nullptr, h->cub_bytes, d.cell_count, d.cell_start, h->g.nkeys + 1, h->stream);
     if (cudaMalloc(&h->cub_tmp, h->cub_bytes + 16) != cudaSuccess) return SPHGPU_ENOMEM;
@@ -233,7 +282,8 @@ int alloc_scene(sphgpu_scene* h) {
 void free_scene(sphgpu_scene* h) {
     DevScene& d = h->d;
     void* ptrs[] = {d.pos, d.vel, d.gid, d.rho, d.alpha, d.vadv, d.pv, d.pk, d.bpv, d.kappav, d.acc, d.kr, d.kappa, d.ksum, d.aux0,
-                    d.aux1, d.aux4, d.kwarm, d.pos_s, d.vel_s, d.gid_s, d.kwarm_s, d.key, d.slot, d.tmp,
+                    d.aux1, d.aux4, d.kwarm, d.hist, d.wsbuf, d.pos_s, d.vel_s, d.gid_s, d.hist_s, d.key, d.slot, d.tmp,
+                    h->recX, h->recY,
                     d.cell_count, d.cell_start, d.bcell_start, d.nbr, d.ncount, d.partial, d.st,
                     d.bpos, d.bvel, d.bgid, h->cub_tmp};
     for (void* p : ptrs)
@@ -254,7 +304,7 @@ void enq_ns(sphgpu_scene* h, int integrate, int build_mode, cudaStream_t st) {
         size_t b = h->cub_bytes;
         cub::DeviceScan::ExclusiveSum(h->cub_tmp, b, d.cell_count, d.cell_start, h->g.nkeys + 1, st);
     });
-    launch(h, "reorder", st, [&] { launch_scatter_reorder(d, h->g, h->cap, h->have_kwarm ? 1 : 0, st); });
+    launch(h, "reorder", st, [&] { launch_scatter_reorder(d, h->g, h->cap, 1, st); });
     launch_count_active(d, h->g, st);
     launch(h, build_mode == 1 ? "build_first" : (build_mode == 2 ? "build_pressure" : "build"), st,
            [&] { launch_build(d, h->g, h->c, build_mode, h->cap, st); });
@@ -321,18 +371,39 @@ int enq_df_div_loop(sphgpu_scene* h, bool capturing) {
 }
 
 // The body of one DFSPH step after the first neighbour search
-// (DFSPH::sphStep, DFSPH.cpp:52-62).
+// (DFSPH::sphStep, DFSPH.cpp:52-62), with the learned warm start when a
+// network is attached (ws_mode 1) or training-data recording (ws_mode 2).
 int enq_df_step(sphgpu_scene* h, bool capturing) {
     DevScene& d = h->d;
     cudaStream_t st = h->stream;
     launch_step_begin(d, st);
     if (h->P.cfl)
         launch(h, "cfl", st, [&] { launch_cfl(d, h->cap, h->P.cfl_factor, h->P.particle_d, h->P.dt_max, h->P.dt_min, st); });
-    const int warm = h->P.warm_start && h->have_kwarm;
-    launch(h, "df_forces", st, [&] { launch_df_forces(d, h->c, h->cap, warm, st); });
-    if (warm) launch(h, "df_warm", st, [&] { launch_df_warm_correction(d, h->c, h->cap, st); });
+    const int ws = h->mlp ? h->ws_mode : 0;
+    launch(h, "df_forces", st, [&] { launch_df_forces(d, h->c, h->cap, 0, st); });
+    if (ws == 1) {
+        launch(h, "ws_features_infer", st, [&] {
+            launch_ws_features(d, h->c, h->mlp->m, 1, h->P.dt_max, h->alpha_ref, nullptr, h->cap, st);
+        });
+        launch(h, "df_warm", st, [&] { launch_df_warm_correction(d, h->c, h->cap, st); });
+    } else if (ws == 2) {
+        launch(h, "ws_features", st, [&] {
+            launch_ws_features(d, h->c, h->mlp->m, 0, h->P.dt_max, h->alpha_ref, h->recX, h->cap, st);
+        });
+    }
+    const int rec = h->record_ksum;
+    h->record_ksum = rec || ws != 0;
     int r = enq_df_density_loop(h, capturing);
+    h->record_ksum = rec;
     if (r) return r;
+    if (ws) {
+        launch(h, "ws_post", st, [&] { launch_ws_post(d, h->c, ws == 2 ? h->recY : nullptr, h->cap, st); });
+        if (ws == 2) {
+            sphgpu_mlp* m = h->mlp;
+            launch_ws_append(h->recX, h->recY, h->cap, &d.st->n_active, h->ws_every, h->ws_offset, m->dsX, m->dsy,
+                             m->ds_count, m->ds_cap, st);
+        }
+    }
     enq_ns(h, 1, 1, st);
     r = enq_df_div_loop(h, capturing);
     if (r) return r;
@@ -347,7 +418,7 @@ int run_initial_ns(sphgpu_scene* h, int build_mode) {
         cudaMemcpyAsync(h->d.pos_s, h->d.pos, sizeof(float4) * n, cudaMemcpyDeviceToDevice, h->stream);
         cudaMemcpyAsync(h->d.vel_s, h->d.vel, sizeof(float4) * n, cudaMemcpyDeviceToDevice, h->stream);
         cudaMemcpyAsync(h->d.gid_s, h->d.gid, sizeof(int) * n, cudaMemcpyDeviceToDevice, h->stream);
-        cudaMemcpyAsync(h->d.kwarm_s, h->d.kwarm, sizeof(float) * n, cudaMemcpyDeviceToDevice, h->stream);
+        cudaMemcpyAsync(h->d.hist_s, h->d.hist, sizeof(float4) * n, cudaMemcpyDeviceToDevice, h->stream);
     }
     enq_ns(h, 0, build_mode, h->stream);
     h->in_staging = false;
@@ -440,7 +511,8 @@ int enq_steps(sphgpu_scene* h, int solver, int nsteps) {
         for (int s = 0; s < nsteps; ++s) {
             if (h->use_graphs && !h->prof.on) {
                 cudaGraphExec_t ex;
-                int key = (h->P.warm_start && h->have_kwarm ? 1 : 0) | (h->record_ksum ? 2 : 0) | (h->P.cfl ? 4 : 0);
+                int key = (h->mlp ? h->ws_mode : 0) | (h->record_ksum ? 4 : 0) | (h->P.cfl ? 8 : 0) |
+                           (h->ws_mode == 2 ? (h->ws_offset << 4) : 0);
                 int r = graph_for(h, key, &ex, df_graph_build);
                 if (r) return r;
                 CK(cudaGraphLaunch(ex, h->stream));
@@ -450,6 +522,7 @@ int enq_steps(sphgpu_scene* h, int solver, int nsteps) {
                 prof_collect(h);
             }
             h->frame++;
+            if (h->mlp && h->ws_mode == 2) h->ws_offset = (h->ws_offset + 1) % h->ws_every;
         }
         return 0;
     }
@@ -557,6 +630,8 @@ int sphgpu_create(const SphParams* p, int device, int max_fluid, sphgpu_t* out) 
     h->ncap = p->max_neighbours;
     h->g = make_grid(*p);
     fill_solver_const(h);
+    mlp_init_attributes();
+    ws_init_attributes();
     int r = alloc_scene(h);
     if (r) {
         free_scene(h);
@@ -850,7 +925,7 @@ int sphgpu_set_fluid(sphgpu_t h, const char* field, const float* in) {
             CK(cudaMemcpyAsync(d.pos_s, d.pos, sizeof(float4) * n, cudaMemcpyDeviceToDevice, h->stream));
             CK(cudaMemcpyAsync(d.vel_s, d.vel, sizeof(float4) * n, cudaMemcpyDeviceToDevice, h->stream));
             CK(cudaMemcpyAsync(d.gid_s, d.gid, sizeof(int) * n, cudaMemcpyDeviceToDevice, h->stream));
-            CK(cudaMemcpyAsync(d.kwarm_s, d.kwarm, sizeof(float) * n, cudaMemcpyDeviceToDevice, h->stream));
+            CK(cudaMemcpyAsync(d.hist_s, d.hist, sizeof(float4) * n, cudaMemcpyDeviceToDevice, h->stream));
             h->in_staging = true;
         }
         CK(cudaStreamSynchronize(h->stream));
@@ -874,7 +949,7 @@ int sphgpu_set_fluid(sphgpu_t h, const char* field, const float* in) {
             CK(cudaMemcpy(d.pos_s, d.pos, sizeof(float4) * n, cudaMemcpyDeviceToDevice));
             CK(cudaMemcpy(d.vel_s, d.vel, sizeof(float4) * n, cudaMemcpyDeviceToDevice));
             CK(cudaMemcpy(d.gid_s, d.gid, sizeof(int) * n, cudaMemcpyDeviceToDevice));
-            CK(cudaMemcpy(d.kwarm_s, d.kwarm, sizeof(float) * n, cudaMemcpyDeviceToDevice));
+            CK(cudaMemcpy(d.hist_s, d.hist, sizeof(float4) * n, cudaMemcpyDeviceToDevice));
             h->in_staging = true;
         }
         return n;
@@ -882,7 +957,7 @@ int sphgpu_set_fluid(sphgpu_t h, const char* field, const float* in) {
     float* dst = nullptr;
     if (f == "density") dst = d.rho;
     else if (f == "DFalpha") dst = d.alpha;
-    else if (f == "kappa_warm") { dst = d.kwarm; h->have_kwarm = true; invalidate_graphs(h); }
+    else if (f == "kappa_warm") dst = d.kwarm;
     else if (f == "kappa_sum") dst = d.ksum;
     else { h->err = "field not settable: " + f; return SPHGPU_EINVAL; }
     std::vector<int> order;
@@ -934,9 +1009,11 @@ int sphgpu_stage(sphgpu_t h, const char* name, SphStepStats* stats) {
     } else if (s == "DF_constantDensitySolverSecond") {
         if (h->in_staging) { h->err = "run neighbourSearch first"; return SPHGPU_EINVAL; }
         if (h->P.cfl) launch_cfl(d, h->cap, h->P.cfl_factor, h->P.particle_d, h->P.dt_max, h->P.dt_min, st);
-        int warm = h->P.warm_start && h->have_kwarm;
-        launch_df_forces(d, h->c, h->cap, warm, st);
-        if (warm) launch_df_warm_correction(d, h->c, h->cap, st);
+        launch_df_forces(d, h->c, h->cap, 0, st);
+        if (h->mlp && h->ws_mode == 1) {
+            launch_ws_features(d, h->c, h->mlp->m, 1, h->P.dt_max, h->alpha_ref, nullptr, h->cap, st);
+            launch_df_warm_correction(d, h->c, h->cap, st);
+        }
         r = enq_df_density_loop(h, false);
         if (r) return r;
         // integrate into staging (the reference updates positions in place)
@@ -1070,6 +1147,248 @@ int sphgpu_last_error(sphgpu_t h, char* buf, int len) {
     strncpy(buf, h->err.c_str(), len - 1);
     buf[len - 1] = 0;
     return (int)h->err.size();
+}
+
+// ---------------- learned warm start ----------------
+
+int sphgpu_mlp_create(int device, int dataset_cap, uint64_t seed, sphgpu_mlp_t* out) {
+    if (!out || dataset_cap < 0) return SPHGPU_EINVAL;
+    *out = nullptr;
+    if (cudaSetDevice(device) != cudaSuccess) return SPHGPU_ECUDA;
+    sphgpu_mlp* m = new sphgpu_mlp();
+    m->device = device;
+    cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking);
+    MlpDev& d = m->m;
+    bool ok = cudaMalloc(&d.master, sizeof(float) * MLP_NPARAM_PAD) == cudaSuccess &&
+              cudaMalloc(&d.grad, sizeof(float) * MLP_NPARAM_PAD) == cudaSuccess &&
+              cudaMalloc(&d.adam_m, sizeof(float) * MLP_NPARAM_PAD) == cudaSuccess &&
+              cudaMalloc(&d.adam_v, sizeof(float) * MLP_NPARAM_PAD) == cudaSuccess &&
+              cudaMalloc(&d.w_bf16, sizeof(__nv_bfloat16) * MLP_NPARAM_PAD) == cudaSuccess &&
+              cudaMalloc(&d.loss, sizeof(float)) == cudaSuccess &&
+              cudaMalloc(&d.norm, sizeof(float) * (2 * MLP_IN + 2)) == cudaSuccess &&
+              cudaMalloc(&m->ds_count, sizeof(int)) == cudaSuccess &&
+              cudaMalloc(&m->dsX, sizeof(float) * MLP_IN * ((size_t)dataset_cap + 1)) == cudaSuccess &&
+              cudaMalloc(&m->dsy, sizeof(float) * ((size_t)dataset_cap + 1)) == cudaSuccess;
+    if (!ok) {
+        sphgpu_mlp_destroy(m);
+        return SPHGPU_ENOMEM;
+    }
+    m->ds_cap = dataset_cap;
+    // Xavier-uniform initial weights, zero biases (host RNG, seeded)
+    std::vector<float> w(MLP_NPARAM_PAD, 0.f);
+    uint64_t x = seed * 6364136223846793005ull + 1442695040888963407ull;
+    auto uni = [&]() {
+        x ^= x << 13; x ^= x >> 7; x ^= x << 17;
+        return (double)(x >> 11) * (1.0 / 9007199254740992.0);
+    };
+    auto fill = [&](int off, int fan_in, int fan_out) {
+        const double a = std::sqrt(6.0 / (fan_in + fan_out));
+        for (int i = 0; i < fan_in * fan_out; ++i) w[off + i] = (float)((2 * uni() - 1) * a);
+    };
+    fill(MLP_OFF_W1, MLP_IN, MLP_H);
+    fill(MLP_OFF_W2, MLP_H, MLP_H);
+    fill(MLP_OFF_W3, MLP_H, 1);
+    std::vector<float> norm(2 * MLP_IN + 2, 0.f);
+    for (int i = 0; i < MLP_IN; ++i) norm[MLP_IN + i] = 1.f;
+    norm[2 * MLP_IN + 1] = 1.f;
+    cudaMemcpy(d.master, w.data(), sizeof(float) * MLP_NPARAM_PAD, cudaMemcpyHostToDevice);
+    cudaMemset(d.grad, 0, sizeof(float) * MLP_NPARAM_PAD);
+    cudaMemset(d.adam_m, 0, sizeof(float) * MLP_NPARAM_PAD);
+    cudaMemset(d.adam_v, 0, sizeof(float) * MLP_NPARAM_PAD);
+    cudaMemcpy(d.norm, norm.data(), sizeof(float) * norm.size(), cudaMemcpyHostToDevice);
+    cudaMemset(m->ds_count, 0, sizeof(int));
+    mlp_init_attributes();
+    launch_mlp_sync_bf16(d, m->stream);
+    if (cudaStreamSynchronize(m->stream) != cudaSuccess) {
+        sphgpu_mlp_destroy(m);
+        return SPHGPU_ECUDA;
+    }
+    *out = m;
+    return 0;
+}
+
+int sphgpu_mlp_destroy(sphgpu_mlp_t m) {
+    if (!m) return SPHGPU_EINVAL;
+    cudaSetDevice(m->device);
+    MlpDev& d = m->m;
+    void* ptrs[] = {d.master, d.grad, d.adam_m, d.adam_v, d.w_bf16, d.loss, d.norm, m->ds_count, m->dsX, m->dsy};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (m->stream) cudaStreamDestroy(m->stream);
+    delete m;
+    return 0;
+}
+
+int sphgpu_mlp_set_params(sphgpu_mlp_t m, const float* params) {
+    if (!m || !params) return SPHGPU_EINVAL;
+    cudaSetDevice(m->device);
+    if (cudaMemcpy(m->m.master, params, sizeof(float) * MLP_NPARAM, cudaMemcpyHostToDevice) != cudaSuccess)
+        return SPHGPU_ECUDA;
+    launch_mlp_sync_bf16(m->m, m->stream);
+    return cudaStreamSynchronize(m->stream) == cudaSuccess ? 0 : SPHGPU_ECUDA;
+}
+
+int sphgpu_mlp_get_params(sphgpu_mlp_t m, float* params) {
+    if (!m || !params) return SPHGPU_EINVAL;
+    cudaSetDevice(m->device);
+    return cudaMemcpy(params, m->m.master, sizeof(float) * MLP_NPARAM, cudaMemcpyDeviceToHost) == cudaSuccess
+               ? MLP_NPARAM : SPHGPU_ECUDA;
+}
+
+int sphgpu_mlp_set_norm(sphgpu_mlp_t m, const float* norm) {
+    if (!m || !norm) return SPHGPU_EINVAL;
+    cudaSetDevice(m->device);
+    return cudaMemcpy(m->m.norm, norm, sizeof(float) * (2 * MLP_IN + 2), cudaMemcpyHostToDevice) == cudaSuccess
+               ? 0 : SPHGPU_ECUDA;
+}
+
+int sphgpu_mlp_get_norm(sphgpu_mlp_t m, float* norm) {
+    if (!m || !norm) return SPHGPU_EINVAL;
+    cudaSetDevice(m->device);
+    return cudaMemcpy(norm, m->m.norm, sizeof(float) * (2 * MLP_IN + 2), cudaMemcpyDeviceToHost) == cudaSuccess
+               ? 0 : SPHGPU_ECUDA;
+}
+
+int sphgpu_mlp_dataset_size(sphgpu_mlp_t m) {
+    if (!m) return SPHGPU_EINVAL;
+    cudaSetDevice(m->device);
+    int n = 0;
+    if (cudaMemcpy(&n, m->ds_count, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return SPHGPU_ECUDA;
+    return std::min(n, m->ds_cap);
+}
+
+int sphgpu_mlp_dataset_set(sphgpu_mlp_t m, const float* X, const float* y, int n) {
+    if (!m || n < 0 || n > m->ds_cap || (n && (!X || !y))) return SPHGPU_EINVAL;
+    cudaSetDevice(m->device);
+    if (n) {
+        if (cudaMemcpy(m->dsX, X, sizeof(float) * MLP_IN * (size_t)n, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(m->dsy, y, sizeof(float) * n, cudaMemcpyHostToDevice) != cudaSuccess)
+            return SPHGPU_ECUDA;
+    }
+    return cudaMemcpy(m->ds_count, &n, sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess ? 0 : SPHGPU_ECUDA;
+}
+
+int sphgpu_mlp_dataset_get(sphgpu_mlp_t m, float* X, float* y, int max_n) {
+    if (!m || max_n < 0) return SPHGPU_EINVAL;
+    int n = std::min(sphgpu_mlp_dataset_size(m), max_n);
+    if (n < 0) return n;
+    if (n && X && cudaMemcpy(X, m->dsX, sizeof(float) * MLP_IN * (size_t)n, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return SPHGPU_ECUDA;
+    if (n && y && cudaMemcpy(y, m->dsy, sizeof(float) * n, cudaMemcpyDeviceToHost) != cudaSuccess) return SPHGPU_ECUDA;
+    return n;
+}
+
+// Train for `epochs` passes over the dataset in mini-batches of `batch` rows
+// (dataset order; shuffle it first with sphgpu_mlp_dataset_shuffle), Adam at
+// learning rate lr.  loss_per_epoch[e] = mean squared error (normalised
+// labels) of epoch e.
+int sphgpu_mlp_train(sphgpu_mlp_t m, int epochs, int batch, float lr, float* loss_per_epoch) {
+    if (!m || epochs < 0 || batch <= 0) return SPHGPU_EINVAL;
+    cudaSetDevice(m->device);
+    const int n = sphgpu_mlp_dataset_size(m);
+    if (n <= 0) { m->err = "empty dataset"; return SPHGPU_EINVAL; }
+    for (int e = 0; e < epochs; ++e) {
+        cudaMemsetAsync(m->m.loss, 0, sizeof(float), m->stream);
+        for (int b0 = 0; b0 < n; b0 += batch) {
+            const int bsz = std::min(batch, n - b0);
+            launch_mlp_train_batch(m->m, m->dsX, m->dsy, n, b0, bsz, 1.f / (float)bsz, m->stream);
+            launch_mlp_adam(m->m, lr, ++m->adam_t, m->stream);
+        }
+        float l = 0;
+        if (cudaMemcpyAsync(&l, m->m.loss, sizeof(float), cudaMemcpyDeviceToHost, m->stream) != cudaSuccess ||
+            cudaStreamSynchronize(m->stream) != cudaSuccess)
+            return SPHGPU_ECUDA;
+        if (loss_per_epoch) loss_per_epoch[e] = l / (float)n;
+    }
+    return cudaGetLastError() == cudaSuccess ? 0 : SPHGPU_ECUDA;
+}
+
+// Shuffle the dataset rows (host permutation from a seeded RNG, device gather).
+int sphgpu_mlp_dataset_shuffle(sphgpu_mlp_t m, uint64_t seed) {
+    if (!m) return SPHGPU_EINVAL;
+    const int n = sphgpu_mlp_dataset_size(m);
+    if (n <= 1) return 0;
+    std::vector<float> X((size_t)n * MLP_IN), y(n), X2((size_t)n * MLP_IN), y2(n);
+    if (sphgpu_mlp_dataset_get(m, X.data(), y.data(), n) != n) return SPHGPU_ECUDA;
+    std::vector<int> perm(n);
+    std::iota(perm.begin(), perm.end(), 0);
+    uint64_t x = seed * 0x9E3779B97F4A7C15ull + 7;
+    for (int i = n - 1; i > 0; --i) {
+        x ^= x << 13; x ^= x >> 7; x ^= x << 17;
+        std::swap(perm[i], perm[(int)(x % (uint64_t)(i + 1))]);
+    }
+    for (int i = 0; i < n; ++i) {
+        memcpy(&X2[(size_t)i * MLP_IN], &X[(size_t)perm[i] * MLP_IN], sizeof(float) * MLP_IN);
+        y2[i] = y[perm[i]];
+    }
+    return sphgpu_mlp_dataset_set(m, X2.data(), y2.data(), n);
+}
+
+// Gradient of the mean squared error over (X, y) (host arrays, n rows, one
+// mini-batch) w.r.t. the FP32 parameter vector; no update.  For checking the
+// backward kernels against a CPU restatement.
+int sphgpu_mlp_gradient(sphgpu_mlp_t m, const float* X, const float* y, int n, float* grad, float* loss) {
+    if (!m || !X || !y || n <= 0 || !grad) return SPHGPU_EINVAL;
+    cudaSetDevice(m->device);
+    float *dX = nullptr, *dy = nullptr;
+    if (cudaMalloc(&dX, sizeof(float) * MLP_IN * (size_t)n) != cudaSuccess ||
+        cudaMalloc(&dy, sizeof(float) * n) != cudaSuccess) {
+        cudaFree(dX);
+        return SPHGPU_ENOMEM;
+    }
+    cudaMemcpy(dX, X, sizeof(float) * MLP_IN * (size_t)n, cudaMemcpyHostToDevice);
+    cudaMemcpy(dy, y, sizeof(float) * n, cudaMemcpyHostToDevice);
+    cudaMemsetAsync(m->m.grad, 0, sizeof(float) * MLP_NPARAM_PAD, m->stream);
+    cudaMemsetAsync(m->m.loss, 0, sizeof(float), m->stream);
+    launch_mlp_train_batch(m->m, dX, dy, n, 0, n, 1.f / (float)n, m->stream);
+    cudaMemcpyAsync(grad, m->m.grad, sizeof(float) * MLP_NPARAM, cudaMemcpyDeviceToHost, m->stream);
+    float l = 0;
+    cudaMemcpyAsync(&l, m->m.loss, sizeof(float), cudaMemcpyDeviceToHost, m->stream);
+    cudaMemsetAsync(m->m.grad, 0, sizeof(float) * MLP_NPARAM_PAD, m->stream);
+    cudaError_t e = cudaStreamSynchronize(m->stream);
+    cudaFree(dX);
+    cudaFree(dy);
+    if (loss) *loss = l / (float)n;
+    return e == cudaSuccess ? 0 : SPHGPU_ECUDA;
+}
+
+int sphgpu_mlp_predict(sphgpu_mlp_t m, const float* X, float* y, int n) {
+    if (!m || !X || !y || n < 0) return SPHGPU_EINVAL;
+    if (!n) return 0;
+    cudaSetDevice(m->device);
+    float *dX = nullptr, *dy = nullptr;
+    if (cudaMalloc(&dX, sizeof(float) * MLP_IN * (size_t)n) != cudaSuccess ||
+        cudaMalloc(&dy, sizeof(float) * n) != cudaSuccess) {
+        cudaFree(dX);
+        return SPHGPU_ENOMEM;
+    }
+    cudaMemcpy(dX, X, sizeof(float) * MLP_IN * (size_t)n, cudaMemcpyHostToDevice);
+    launch_mlp_predict(m->m, dX, dy, n, m->stream);
+    cudaMemcpyAsync(y, dy, sizeof(float) * n, cudaMemcpyDeviceToHost, m->stream);
+    cudaError_t e = cudaStreamSynchronize(m->stream);
+    cudaFree(dX);
+    cudaFree(dy);
+    return e == cudaSuccess ? 0 : SPHGPU_ECUDA;
+}
+
+// Attach a network to a scene: mode 0 detaches, 1 applies the learned warm
+// start every DFSPH step, 2 records (features, converged stiffness) of every
+// `record_every`-th particle of every step into the network's dataset.
+int sphgpu_attach_warm_start(sphgpu_t h, sphgpu_mlp_t m, int mode, int record_every) {
+    if (!h || mode < 0 || mode > 2 || (mode && !m) || (mode == 2 && record_every <= 0)) return SPHGPU_EINVAL;
+    cudaSetDevice(h->device);
+    if (mode && m->device != h->device) { h->err = "network and scene on different devices"; return SPHGPU_EINVAL; }
+    if (mode == 2 && !h->recX) {
+        if (dalloc(h, &h->recX, (size_t)h->cap * MLP_IN) || dalloc(h, &h->recY, (size_t)h->cap)) return SPHGPU_ENOMEM;
+    }
+    h->mlp = mode ? m : nullptr;
+    h->ws_mode = mode;
+    h->ws_every = record_every > 0 ? record_every : 1;
+    h->ws_offset = 0;
+    h->P.warm_start = mode == 1;
+    if (mode != 1) cudaMemsetAsync(h->d.kwarm, 0, sizeof(float) * h->cap, h->stream);
+    invalidate_graphs(h);
+    return cudaStreamSynchronize(h->stream) == cudaSuccess ? 0 : SPHGPU_ECUDA;
 }
 
 // Internal controls used by the Python host layer (not part of the

@@ -44,7 +44,7 @@ __global__ void __launch_bounds__(NT) k_hash(DevScene s, GridGeom g, float3 smin
             s.pos_s[i] = p;
             s.vel_s[i] = v;
             s.gid_s[i] = s.gid[i];
-            if (s.kwarm_s) s.kwarm_s[i] = s.kwarm[i];
+            s.hist_s[i] = s.hist[i];
         } else {
             p = s.pos_s[i];
         }
@@ -78,7 +78,7 @@ __global__ void __launch_bounds__(NT) k_scatter(DevScene s) {
 
 // For sorted slot q: its particle i, its cell range [a, b); its final place is
 // a + #{particles of the cell with larger global index}.
-__global__ void __launch_bounds__(NT) k_rank_reorder(DevScene s, int dead_key, int carry_kwarm) {
+__global__ void __launch_bounds__(NT) k_rank_reorder(DevScene s, int dead_key, int carry_hist) {
     const int n = s.st->pad0;
     int q = blockIdx.x * NT + threadIdx.x;
     if (q >= n) return;
@@ -96,7 +96,7 @@ __global__ void __launch_bounds__(NT) k_rank_reorder(DevScene s, int dead_key, i
     s.pv[2 * p + 1] = v;
     s.pk[p] = make_float4(x.x, x.y, x.z, 0.f);
     s.gid[p] = my;
-    if (carry_kwarm) s.kwarm[p] = s.kwarm_s[i];
+    if (carry_hist) s.hist[p] = s.hist_s[i];
 }
 
 __global__ void k_count_active(DevScene s, int dead_key) {
@@ -294,10 +294,10 @@ void launch_hash(const DevScene& s, const GridGeom& g, const float* smin, const 
                                                           make_float3(smax[0], smax[1], smax[2]), integrate);
 }
 
-void launch_scatter_reorder(const DevScene& s, const GridGeom& g, int n_old, int carry_kwarm, cudaStream_t st) {
+void launch_scatter_reorder(const DevScene& s, const GridGeom& g, int n_old, int carry_hist, cudaStream_t st) {
     int nb = nblk(n_old > 0 ? n_old : 1, NT);
     k_scatter<<<nb, NT, 0, st>>>(s);
-    k_rank_reorder<<<nb, NT, 0, st>>>(s, g.nkeys - 1, carry_kwarm);
+    k_rank_reorder<<<nb, NT, 0, st>>>(s, g.nkeys - 1, carry_hist);
 }
 
 void launch_count_active(const DevScene& s, const GridGeom& g, cudaStream_t st) {

@@ -45,12 +45,14 @@ struct DevScene {
     float* aux0;        // rho_adv (DFSPH density loop), aii (IISPH)
     float* aux1;        // divergence deviation (DFSPH), IISPH rho_adv, PCISPH rho*
     float4* aux4;       // IISPH d_ii / sum d_ij p_j, PCISPH predicted position
-    float* kwarm;       // predicted initial kappa (learned warm start)
+    float* kwarm;       // predicted initial kappa (learned warm start), 0 otherwise
+    float4* hist;       // warm-start history: (khat, predicted error, divergence term) of the last step
+    float2* wsbuf;      // this step's (predicted error, divergence term)
     // staging (unsorted) copies used by the reorder
     float4* pos_s;
     float4* vel_s;
     int* gid_s;
-    float* kwarm_s;
+    float4* hist_s;
     int* key;
     int* slot;
     int* tmp;

@@ -1,0 +1,441 @@
+// sph_mlp.cu -- learned warm start for the DFSPH constant-density loop.
+//
+// The network (16 -> 64 -> 64 -> 1, GELU) predicts, per particle, the
+// dimensionless stiffness khat = kappa_sum * dt^2 / (rho0 * alpha) that the
+// density loop (DFSPH.cpp:566-700) applies over all of its iterations.  The
+// prediction is applied once before the loop as a pressure-velocity
+// correction of the same form as DFSPH.cpp:674; the unmodified loop then
+// runs to the same tolerance, so the network only changes where the loop
+// starts, and the gain is counted in iterations.
+//
+// GEMMs run on the tensor cores with mma.sync.m16n8k16 (BF16 operands, FP32
+// accumulation): a 128-row tile per 4-warp block, each warp owning 32 rows.
+// Training (forward + backward of a mini-batch, FP32 gradient atomics) and
+// Adam (FP32 master weights, BF16 copies for the GEMMs) are separate
+// kernels; inference is fused into the per-particle feature sweep.
+#include <cuda_bf16.h>
+
+#include "sph_kernels.cuh"
+#include "sph_mlp.cuh"
+
+namespace {
+
+constexpr int TR = 128;  // rows per block tile (4 warps x 32)
+
+__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.f + erff(z * 0.70710678118654752f)); }
+__device__ __forceinline__ float gelu_d(float z) {
+    return 0.5f * (1.f + erff(z * 0.70710678118654752f)) + z * expf(-0.5f * z * z) * 0.39894228040143268f;
+}
+
+__device__ __forceinline__ uint32_t pack2(__nv_bfloat16 lo, __nv_bfloat16 hi) {
+    return (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
+}
+
+__device__ __forceinline__ void mma16816(float c[4], const uint32_t a[4], const uint32_t b[2]) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// One 16x8 output tile accumulated over K (multiple of 16):
+//   C(m0.., n0..) += sum_k A(m, k) B(k, n)
+// with A(m, k) = A[m*am + k*ak] and B(k, n) = B[k*bk + n*bn] (BF16, shared
+// memory).  Fragment layout of m16n8k16 (PTX ISA): g = lane/4, t = lane%4.
+__device__ __forceinline__ void tile_mma(float c[4], const __nv_bfloat16* A, int am, int ak, const __nv_bfloat16* B,
+                                         int bk, int bn, int m0, int n0, int K) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    for (int k0 = 0; k0 < K; k0 += 16) {
+        uint32_t a[4], b[2];
+        const int r0 = m0 + g, r1 = m0 + g + 8, ka = k0 + 2 * t;
+        a[0] = pack2(A[r0 * am + ka * ak], A[r0 * am + (ka + 1) * ak]);
+        a[1] = pack2(A[r1 * am + ka * ak], A[r1 * am + (ka + 1) * ak]);
+        a[2] = pack2(A[r0 * am + (ka + 8) * ak], A[r0 * am + (ka + 9) * ak]);
+        a[3] = pack2(A[r1 * am + (ka + 8) * ak], A[r1 * am + (ka + 9) * ak]);
+        const int n = n0 + g;
+        b[0] = pack2(B[ka * bk + n * bn], B[(ka + 1) * bk + n * bn]);
+        b[1] = pack2(B[(ka + 8) * bk + n * bn], B[(ka + 9) * bk + n * bn]);
+        mma16816(c, a, b);
+    }
+}
+
+struct FwdSmem {
+    __nv_bfloat16 X[TR * MLP_IN];
+    __nv_bfloat16 W1[MLP_IN * MLP_H];
+    __nv_bfloat16 W2[MLP_H * MLP_H];
+    __nv_bfloat16 H1[TR * MLP_H];
+    float Z1[TR * MLP_H];
+    float Z2[TR * MLP_H];
+    float W3[MLP_H], b1[MLP_H], b2[MLP_H];
+    float b3;
+};
+
+struct TrainSmem {
+    FwdSmem f;
+    __nv_bfloat16 dZ2[TR * MLP_H];
+    __nv_bfloat16 dZ1[TR * MLP_H];
+    float g[TR];
+};
+
+// weights into shared memory (BF16 GEMM copies, FP32 biases)
+__device__ __forceinline__ void load_weights(const MlpDev& m, FwdSmem& S) {
+    for (int i = threadIdx.x; i < MLP_IN * MLP_H; i += blockDim.x) S.W1[i] = m.w_bf16[MLP_OFF_W1 + i];
+    for (int i = threadIdx.x; i < MLP_H * MLP_H; i += blockDim.x) S.W2[i] = m.w_bf16[MLP_OFF_W2 + i];
+    for (int i = threadIdx.x; i < MLP_H; i += blockDim.x) {
+        S.W3[i] = __bfloat162float(m.w_bf16[MLP_OFF_W3 + i]);
+        S.b1[i] = m.master[MLP_OFF_B1 + i];
+        S.b2[i] = m.master[MLP_OFF_B2 + i];
+    }
+    if (threadIdx.x == 0) S.b3 = m.master[MLP_OFF_B3];
+}
+
+// Forward pass of the warp's 32 rows (S.X filled, weights loaded):
+// Z1, H1 (BF16), Z2 in shared memory; returns y for row lane of the warp.
+__device__ __forceinline__ float forward_rows(FwdSmem& S) {
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    const int r0 = w * 32;
+    // layer 1: Z1 = X W1 + b1   (K = 16)
+    for (int mt = 0; mt < 2; ++mt)
+        for (int nt = 0; nt < MLP_H / 8; ++nt) {
+            float c[4] = {0.f, 0.f, 0.f, 0.f};
+            tile_mma(c, S.X, MLP_IN, 1, S.W1, MLP_H, 1, r0 + mt * 16, nt * 8, MLP_IN);
+            const int ra = r0 + mt * 16 + g, col = nt * 8 + 2 * t;
+            const float z[4] = {c[0] + S.b1[col], c[1] + S.b1[col + 1], c[2] + S.b1[col], c[3] + S.b1[col + 1]};
+            S.Z1[ra * MLP_H + col] = z[0];
+            S.Z1[ra * MLP_H + col + 1] = z[1];
+            S.Z1[(ra + 8) * MLP_H + col] = z[2];
+            S.Z1[(ra + 8) * MLP_H + col + 1] = z[3];
+            S.H1[ra * MLP_H + col] = __float2bfloat16_rn(gelu(z[0]));
+            S.H1[ra * MLP_H + col + 1] = __float2bfloat16_rn(gelu(z[1]));
+            S.H1[(ra + 8) * MLP_H + col] = __float2bfloat16_rn(gelu(z[2]));
+            S.H1[(ra + 8) * MLP_H + col + 1] = __float2bfloat16_rn(gelu(z[3]));
+        }
+    __syncwarp();
+    // layer 2: Z2 = H1 W2 + b2   (K = 64)
+    for (int mt = 0; mt < 2; ++mt)
+        for (int nt = 0; nt < MLP_H / 8; ++nt) {
+            float c[4] = {0.f, 0.f, 0.f, 0.f};
+            tile_mma(c, S.H1, MLP_H, 1, S.W2, MLP_H, 1, r0 + mt * 16, nt * 8, MLP_H);
+            const int ra = r0 + mt * 16 + g, col = nt * 8 + 2 * t;
+            S.Z2[ra * MLP_H + col] = c[0] + S.b2[col];
+            S.Z2[ra * MLP_H + col + 1] = c[1] + S.b2[col + 1];
+            S.Z2[(ra + 8) * MLP_H + col] = c[2] + S.b2[col];
+            S.Z2[(ra + 8) * MLP_H + col + 1] = c[3] + S.b2[col + 1];
+        }
+    __syncwarp();
+    // layer 3: y = gelu(Z2) W3 + b3 (row = lane), FP32
+    const int row = r0 + lane;
+    float y = S.b3;
+#pragma unroll 8
+    for (int j = 0; j < MLP_H; ++j) y = fmaf(gelu(S.Z2[row * MLP_H + j]), S.W3[j], y);
+    return y;
+}
+
+// ---------------- training ----------------
+
+// one 128-row tile of a mini-batch: forward, MSE gradient, backward, and FP32
+// atomics into m.grad.  inv_total = 1 / (rows in the mini-batch).
+__global__ void __launch_bounds__(TR) k_mlp_train(MlpDev m, const float* X, const float* y, int n, int b0, int bsz,
+                                                 float inv_total) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    TrainSmem& S = *reinterpret_cast<TrainSmem*>(smraw);
+    const int tile0 = b0 + blockIdx.x * TR;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    load_weights(m, S.f);
+    const float* nrm = m.norm;
+    for (int i = threadIdx.x; i < TR * MLP_IN; i += TR) {
+        const int r = i / MLP_IN, c = i % MLP_IN;
+        const int row = tile0 + r;
+        float v = 0.f;
+        if (row < b0 + bsz && row < n) v = (X[(size_t)row * MLP_IN + c] - nrm[c]) * nrm[MLP_IN + c];
+        S.f.X[i] = __float2bfloat16_rn(v);
+    }
+    __syncthreads();
+    const float yhat = forward_rows(S.f);
+    const int myrow = tile0 + w * 32 + lane;
+    const bool valid = myrow < b0 + bsz && myrow < n;
+    const float target = valid ? (y[myrow] - nrm[2 * MLP_IN]) * nrm[2 * MLP_IN + 1] : 0.f;
+    const float err = valid ? yhat - target : 0.f;
+    const float gr = 2.f * err * inv_total;  // dL/dy, L = mean (y - t)^2
+    S.g[w * 32 + lane] = gr;
+    // loss
+    float se = err * err;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) se += __shfl_down_sync(0xffffffffu, se, o);
+    if (lane == 0) atomicAdd(m.loss, se);
+    __syncwarp();
+    // output layer: dW3_j = sum_r g_r gelu(Z2_rj), db3 = sum g; dZ2 = g W3_j gelu'(Z2)
+    const int r0 = w * 32;
+    for (int j = lane; j < MLP_H; j += 32) {
+        float s3 = 0.f, sb = 0.f;
+        for (int r = 0; r < 32; ++r) {
+            const float z = S.f.Z2[(r0 + r) * MLP_H + j];
+            const float gg = S.g[r0 + r];
+            s3 = fmaf(gg, gelu(z), s3);
+            const float dz = gg * S.f.W3[j] * gelu_d(z);
+            sb += dz;
+            S.dZ2[(r0 + r) * MLP_H + j] = __float2bfloat16_rn(dz);
+        }
+        atomicAdd(&m.grad[MLP_OFF_W3 + j], s3);
+        atomicAdd(&m.grad[MLP_OFF_B2 + j], sb);
+    }
+    if (lane == 0) {
+        float sg = 0.f;
+        for (int r = 0; r < 32; ++r) sg += S.g[r0 + r];
+        atomicAdd(&m.grad[MLP_OFF_B3], sg);
+    }
+    __syncwarp();
+    // dH1 = dZ2 W2^T, dZ1 = dH1 * gelu'(Z1)   (B(k=j2, n=j1) = W2[j1][j2])
+    for (int mt = 0; mt < 2; ++mt)
+        for (int nt = 0; nt < MLP_H / 8; ++nt) {
+            float c[4] = {0.f, 0.f, 0.f, 0.f};
+            tile_mma(c, S.dZ2, MLP_H, 1, S.f.W2, 1, MLP_H, r0 + mt * 16, nt * 8, MLP_H);
+            const int ra = r0 + mt * 16 + g, col = nt * 8 + 2 * t;
+            S.dZ1[ra * MLP_H + col] = __float2bfloat16_rn(c[0] * gelu_d(S.f.Z1[ra * MLP_H + col]));
+            S.dZ1[ra * MLP_H + col + 1] = __float2bfloat16_rn(c[1] * gelu_d(S.f.Z1[ra * MLP_H + col + 1]));
+            S.dZ1[(ra + 8) * MLP_H + col] = __float2bfloat16_rn(c[2] * gelu_d(S.f.Z1[(ra + 8) * MLP_H + col]));
+            S.dZ1[(ra + 8) * MLP_H + col + 1] =
+                __float2bfloat16_rn(c[3] * gelu_d(S.f.Z1[(ra + 8) * MLP_H + col + 1]));
+        }
+    __syncthreads();
+    // db1 (from the BF16 dZ1 the GEMMs use)
+    for (int j = threadIdx.x; j < MLP_H; j += TR) {
+        float sb = 0.f;
+        for (int r = 0; r < TR; ++r) sb += __bfloat162float(S.dZ1[r * MLP_H + j]);
+        atomicAdd(&m.grad[MLP_OFF_B1 + j], sb);
+    }
+    // dW2 = H1^T dZ2 (64 x 64, K = 128 rows): 4 x 8 tiles, 8 per warp
+    for (int tt = w; tt < 32; tt += 4) {
+        const int mt = tt / 8, nt = tt % 8;
+        float c[4] = {0.f, 0.f, 0.f, 0.f};
+        tile_mma(c, S.f.H1, 1, MLP_H, S.dZ2, MLP_H, 1, mt * 16, nt * 8, TR);
+        const int ra = mt * 16 + g, col = nt * 8 + 2 * t;
+        atomicAdd(&m.grad[MLP_OFF_W2 + ra * MLP_H + col], c[0]);
+        atomicAdd(&m.grad[MLP_OFF_W2 + ra * MLP_H + col + 1], c[1]);
+        atomicAdd(&m.grad[MLP_OFF_W2 + (ra + 8) * MLP_H + col], c[2]);
+        atomicAdd(&m.grad[MLP_OFF_W2 + (ra + 8) * MLP_H + col + 1], c[3]);
+    }
+    // dW1 = X^T dZ1 (16 x 64, K = 128): 1 x 8 tiles, 2 per warp
+    for (int nt = w; nt < 8; nt += 4) {
+        float c[4] = {0.f, 0.f, 0.f, 0.f};
+        tile_mma(c, S.f.X, 1, MLP_IN, S.dZ1, MLP_H, 1, 0, nt * 8, TR);
+        const int ra = g, col = nt * 8 + 2 * t;
+        atomicAdd(&m.grad[MLP_OFF_W1 + ra * MLP_H + col], c[0]);
+        atomicAdd(&m.grad[MLP_OFF_W1 + ra * MLP_H + col + 1], c[1]);
+        atomicAdd(&m.grad[MLP_OFF_W1 + (ra + 8) * MLP_H + col], c[2]);
+        atomicAdd(&m.grad[MLP_OFF_W1 + (ra + 8) * MLP_H + col + 1], c[3]);
+    }
+}
+
+// Adam on the FP32 master weights, BF16 copies for the GEMMs, gradient reset
+__global__ void k_mlp_adam(MlpDev m, float lr, float bc1, float bc2) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= MLP_NPARAM) return;
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    const float gr = m.grad[i];
+    const float mm = b1 * m.adam_m[i] + (1.f - b1) * gr;
+    const float vv = b2 * m.adam_v[i] + (1.f - b2) * gr * gr;
+    m.adam_m[i] = mm;
+    m.adam_v[i] = vv;
+    const float w = m.master[i] - lr * (mm / bc1) / (sqrtf(vv / bc2) + eps);
+    m.master[i] = w;
+    m.w_bf16[i] = __float2bfloat16_rn(w);
+    m.grad[i] = 0.f;
+}
+
+__global__ void k_mlp_sync(MlpDev m) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < MLP_NPARAM) m.w_bf16[i] = __float2bfloat16_rn(m.master[i]);
+}
+
+__global__ void __launch_bounds__(TR) k_mlp_predict(MlpDev m, const float* X, float* y, int n) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    FwdSmem& S = *reinterpret_cast<FwdSmem*>(smraw);
+    const int tile0 = blockIdx.x * TR;
+    load_weights(m, S);
+    const float* nrm = m.norm;
+    for (int i = threadIdx.x; i < TR * MLP_IN; i += TR) {
+        const int r = i / MLP_IN, c = i % MLP_IN;
+        const int row = tile0 + r;
+        const float v = row < n ? (X[(size_t)row * MLP_IN + c] - nrm[c]) * nrm[MLP_IN + c] : 0.f;
+        S.X[i] = __float2bfloat16_rn(v);
+    }
+    __syncthreads();
+    const float yh = forward_rows(S);
+    const int row = tile0 + threadIdx.x;
+    if (row < n) y[row] = yh / nrm[2 * MLP_IN + 1] + nrm[2 * MLP_IN];
+}
+
+}  // namespace
+
+static size_t smem_train() { return sizeof(TrainSmem); }
+static size_t smem_fwd() { return sizeof(FwdSmem); }
+
+void mlp_init_attributes() {
+    cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_train());
+    cudaFuncSetAttribute(k_mlp_predict, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_fwd());
+}
+
+void launch_mlp_train_batch(const MlpDev& m, const float* X, const float* y, int n, int b0, int bsz, float inv_total,
+                            cudaStream_t st) {
+    const int blocks = (bsz + TR - 1) / TR;
+    k_mlp_train<<<blocks, TR, smem_train(), st>>>(m, X, y, n, b0, bsz, inv_total);
+}
+
+void launch_mlp_adam(const MlpDev& m, float lr, int t, cudaStream_t st) {
+    const float bc1 = 1.f - powf(0.9f, (float)t), bc2 = 1.f - powf(0.999f, (float)t);
+    k_mlp_adam<<<(MLP_NPARAM + 255) / 256, 256, 0, st>>>(m, lr, bc1, bc2);
+}
+
+void launch_mlp_sync_bf16(const MlpDev& m, cudaStream_t st) { k_mlp_sync<<<(MLP_NPARAM + 255) / 256, 256, 0, st>>>(m); }
+
+void launch_mlp_predict(const MlpDev& m, const float* X, float* y, int n, cudaStream_t st) {
+    if (n > 0) k_mlp_predict<<<(n + TR - 1) / TR, TR, smem_fwd(), st>>>(m, X, y, n);
+}
+
+// ===================== warm-start kernels on a scene =====================
+namespace {
+
+// Per-particle features (16, FP32) from the state after the non-pressure
+// forces (v_adv known) and before the density loop, plus the prediction.
+//  0 neighbour count / 32             8  |a_adv| dt^2 / d
+//  1 (rho - rho0)/rho0 * 100          9  boundary-neighbour fraction
+//  2 dt * Drho/Dt / rho0 * 100        10 log(alpha / alpha_ref)
+//  3 (max(rho_adv0, rho0) - rho0)/rho0 * 100   11 neighbour mean of khat_prev
+//  4 khat of the previous step        12 dt / dt_max
+//  5 feature 3 of the previous step   13 |sum_j m gradW_ij| d / rho0
+//  6 feature 2 of the previous step   14 v_y dt / d
+//  7 |v| dt / d                       15 1
+__device__ __forceinline__ void ws_features(const DevScene& s, const SolverConst& c, int p, float dt, float dt_max,
+                                            float alpha_ref, float x[MLP_IN], float& pred, float& divt) {
+    const float4 pa = s.pv[2 * p];
+    const float4 va = s.pv[2 * p + 1];
+    const int cnt = s.ncount[p];
+    const size_t stride = (size_t)c.stride;
+    float acc = 0.f, ax = 0.f, ay = 0.f, az = 0.f, kp = 0.f;
+    int nb = 0, nfl = 0;
+    for (int k = 0; k < cnt; ++k) {
+        const unsigned e = (unsigned)ell_get(s.nbr, stride, p, k);
+        const bool bnd = (e & BND_FLAG) != 0u;
+        const unsigned j = e & BND_MASK;
+        float4 pb, vb;
+        ld_record32((bnd ? s.bpv : s.pv) + 2 * (size_t)j, pb, vb);
+        const float m = bnd ? c.rho0 * pb.w : c.fm0;
+        const float xx = pa.x - pb.x, xy = pa.y - pb.y, xz = pa.z - pb.z;
+        const float f = grad_over_r(c.k, xx * xx + xy * xy + xz * xz);
+        acc = fmaf((xx * (va.x - vb.x) + xy * (va.y - vb.y) + xz * (va.z - vb.z)) * f, m, acc);
+        ax = fmaf(xx * f, m, ax);
+        ay = fmaf(xy * f, m, ay);
+        az = fmaf(xz * f, m, az);
+        if (bnd) ++nb;
+        else { kp += s.hist[j].x; ++nfl; }
+    }
+    const float rho0 = c.rho0, rho = s.rho[p], d = c.dpart;
+    const float4 hp = s.hist[p];
+    const float4 a = s.acc[p];
+    const float4 v = s.vel[p];
+    divt = dt * acc / rho0 * 100.f;
+    const float dadv = fmaxf(fmaf(acc, dt, rho), rho0);
+    pred = (dadv - rho0) / rho0 * 100.f;
+    x[0] = cnt * (1.f / 32.f);
+    x[1] = (rho - rho0) / rho0 * 100.f;
+    x[2] = divt;
+    x[3] = pred;
+    x[4] = hp.x;
+    x[5] = hp.y;
+    x[6] = hp.z;
+    x[7] = sqrtf(v.x * v.x + v.y * v.y + v.z * v.z) * dt / d;
+    x[8] = sqrtf(a.x * a.x + a.y * a.y + a.z * a.z) * dt * dt / d;
+    x[9] = cnt ? (float)nb / (float)cnt : 0.f;
+    x[10] = logf(fmaxf(s.alpha[p], 1e-30f) / alpha_ref);
+    x[11] = nfl ? kp / (float)nfl : 0.f;
+    x[12] = dt / dt_max;
+    x[13] = sqrtf(ax * ax + ay * ay + az * az) * d / rho0;
+    x[14] = v.y * dt / d;
+    x[15] = 1.f;
+}
+
+// features -> network -> kwarm (and, when recording, the features of the step)
+template <int INFER>
+__global__ void __launch_bounds__(TR) k_ws_features(DevScene s, SolverConst c, MlpDev m, float dt_max,
+                                                   float alpha_ref, float* Xout) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    FwdSmem& S = *reinterpret_cast<FwdSmem*>(smraw);
+    const int n = s.st->n_active;
+    const int p = blockIdx.x * TR + threadIdx.x;
+    const float dt = *s.dt;
+    float x[MLP_IN];
+    float pred = 0.f, divt = 0.f;
+    if (p < n) {
+        ws_features(s, c, p, dt, dt_max, alpha_ref, x, pred, divt);
+        s.wsbuf[p] = make_float2(pred, divt);
+        if (Xout)
+            for (int i = 0; i < MLP_IN; ++i) Xout[(size_t)p * MLP_IN + i] = x[i];
+    } else {
+        for (int i = 0; i < MLP_IN; ++i) x[i] = 0.f;
+    }
+    if (!INFER) return;
+    load_weights(m, S);
+    const float* nrm = m.norm;
+    for (int i = 0; i < MLP_IN; ++i) S.X[threadIdx.x * MLP_IN + i] = __float2bfloat16_rn((x[i] - nrm[i]) * nrm[MLP_IN + i]);
+    __syncthreads();
+    const float yn = forward_rows(S);
+    if (p < n) {
+        const float khat = yn / nrm[2 * MLP_IN + 1] + nrm[2 * MLP_IN];
+        // kappa = khat * rho0 * alpha / dt^2; negative predictions are not applied
+        const float kw = fmaxf(khat, 0.f) * c.rho0 * s.alpha[p] / (dt * dt);
+        s.kwarm[p] = kw;
+        s.pk[p].w = kw / s.rho[p];  // read by the warm-correction sweep
+    }
+}
+
+// after the density loop: the step's total stiffness (warm + loop) as khat,
+// history for the next step's features, and the training label
+__global__ void k_ws_post(DevScene s, SolverConst c, float* yout) {
+    const int n = s.st->n_active;
+    const int p = blockIdx.x * TR + threadIdx.x;
+    if (p >= n) return;
+    const float dt = *s.dt;
+    const float ktot = s.ksum[p] + s.kwarm[p];  // kwarm is 0 unless the warm start ran
+    const float khat = ktot * dt * dt / (c.rho0 * s.alpha[p]);
+    const float2 w = s.wsbuf[p];
+    s.hist[p] = make_float4(khat, w.x, w.y, 0.f);
+    if (yout) yout[p] = khat;
+    s.ksum[p] = 0.f;
+}
+
+// append every `every`-th particle (from `offset`) of the step to the dataset
+__global__ void k_ws_append(const float* X, const float* y, int n_max, const int* n_act, int every, int offset,
+                            float* dsX, float* dsy, int* ds_count, int ds_cap) {
+    const int n = *n_act;
+    const int i = blockIdx.x * TR + threadIdx.x;
+    const int p = offset + i * every;
+    if (p >= n || p >= n_max) return;
+    const int slot = atomicAdd(ds_count, 1);
+    if (slot >= ds_cap) return;
+    for (int k = 0; k < MLP_IN; ++k) dsX[(size_t)slot * MLP_IN + k] = X[(size_t)p * MLP_IN + k];
+    dsy[slot] = y[p];
+}
+}  // namespace
+
+void ws_init_attributes() {
+    cudaFuncSetAttribute(k_ws_features<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(FwdSmem));
+}
+
+void launch_ws_features(const DevScene& s, const SolverConst& c, const MlpDev& m, int infer, float dt_max,
+                        float alpha_ref, float* Xout, int n_max, cudaStream_t st) {
+    const int blocks = (n_max + TR - 1) / TR;
+    if (infer) k_ws_features<1><<<blocks, TR, sizeof(FwdSmem), st>>>(s, c, m, dt_max, alpha_ref, Xout);
+    else k_ws_features<0><<<blocks, TR, 0, st>>>(s, c, m, dt_max, alpha_ref, Xout);
+}
+
+void launch_ws_post(const DevScene& s, const SolverConst& c, float* yout, int n_max, cudaStream_t st) {
+    k_ws_post<<<(n_max + TR - 1) / TR, TR, 0, st>>>(s, c, yout);
+}
+
+void launch_ws_append(const float* X, const float* y, int n_max, const int* n_act, int every, int offset, float* dsX,
+                      float* dsy, int* ds_count, int ds_cap, cudaStream_t st) {
+    const int cnt = (n_max + every - 1) / every + 1;
+    k_ws_append<<<(cnt + TR - 1) / TR, TR, 0, st>>>(X, y, n_max, n_act, every, offset, dsX, dsy, ds_count, ds_cap);
+}

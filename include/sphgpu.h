@@ -190,6 +190,32 @@ void* sphgpu_stream(sphgpu_t h);
 int sphgpu_profile(sphgpu_t h, int enable);
 int sphgpu_profile_read(sphgpu_t h, char* names, int name_len, double* ms, int* launches, int cap);
 
+/* ---------------- learned warm start (no reference counterpart) ----------------
+ * A BF16 MLP (16 -> 64 -> 64 -> 1, GELU; FP32 master weights) that predicts the
+ * per-particle stiffness the DFSPH constant-density loop (DFSPH.cpp:566-700)
+ * converges to, applied once before the unmodified loop.  Parameter vector
+ * (FP32, SPHGPU_MLP_NPARAM): W1[16][64] b1[64] W2[64][64] b2[64] W3[64] b3.
+ * norm[34]: feature mean[16], 1/std[16], label mean, 1/std. */
+#define SPHGPU_MLP_NPARAM 5313
+typedef struct sphgpu_mlp* sphgpu_mlp_t;
+int sphgpu_mlp_create(int device, int dataset_cap, uint64_t seed, sphgpu_mlp_t* out);
+int sphgpu_mlp_destroy(sphgpu_mlp_t m);
+int sphgpu_mlp_set_params(sphgpu_mlp_t m, const float* params);
+int sphgpu_mlp_get_params(sphgpu_mlp_t m, float* params);
+int sphgpu_mlp_set_norm(sphgpu_mlp_t m, const float* norm);
+int sphgpu_mlp_get_norm(sphgpu_mlp_t m, float* norm);
+int sphgpu_mlp_dataset_size(sphgpu_mlp_t m);
+int sphgpu_mlp_dataset_set(sphgpu_mlp_t m, const float* X, const float* y, int n);
+int sphgpu_mlp_dataset_get(sphgpu_mlp_t m, float* X, float* y, int max_n);
+int sphgpu_mlp_dataset_shuffle(sphgpu_mlp_t m, uint64_t seed);
+int sphgpu_mlp_train(sphgpu_mlp_t m, int epochs, int batch, float lr, float* loss_per_epoch);
+int sphgpu_mlp_gradient(sphgpu_mlp_t m, const float* X, const float* y, int n, float* grad, float* loss);
+int sphgpu_mlp_predict(sphgpu_mlp_t m, const float* X, float* y, int n);
+/* mode 0: detach; 1: apply the warm start every DFSPH step; 2: record
+ * (features, converged stiffness) of every record_every-th particle into the
+ * network's dataset (plain solver, no warm start). */
+int sphgpu_attach_warm_start(sphgpu_t h, sphgpu_mlp_t m, int mode, int record_every);
+
 /* Copy of the last error message. */
 int sphgpu_last_error(sphgpu_t h, char* buf, int len);
 
