@@ -27,7 +27,7 @@ void ws_init_attributes();
 void launch_ws_features(const DevScene& s, const SolverConst& c, const MlpDev& m, int infer, float dt_max,
                         float alpha_ref, float* Xout, int n_max, cudaStream_t st);
 void launch_ws_post(const DevScene& s, const SolverConst& c, float* yout, int n_max, cudaStream_t st);
-void launch_ws_append(const float* X, const float* y, int n_max, const int* n_act, int every, int offset, float* dsX,
+void launch_ws_append(const float* X, const float* y, int n_max, const int* n_act, int every, int* offset, float* dsX,
                       float* dsy, int* ds_count, int ds_cap, cudaStream_t st);
 
 namespace {
@@ -400,7 +400,7 @@ int enq_df_step(sphgpu_scene* h, bool capturing) {
         launch(h, "ws_post", st, [&] { launch_ws_post(d, h->c, ws == 2 ? h->recY : nullptr, h->cap, st); });
         if (ws == 2) {
             sphgpu_mlp* m = h->mlp;
-            launch_ws_append(h->recX, h->recY, h->cap, &d.st->n_active, h->ws_every, h->ws_offset, m->dsX, m->dsy,
+            launch_ws_append(h->recX, h->recY, h->cap, &d.st->n_active, h->ws_every, &d.st->pad2, m->dsX, m->dsy,
                              m->ds_count, m->ds_cap, st);
         }
     }
@@ -511,8 +511,7 @@ int enq_steps(sphgpu_scene* h, int solver, int nsteps) {
         for (int s = 0; s < nsteps; ++s) {
             if (h->use_graphs && !h->prof.on) {
                 cudaGraphExec_t ex;
-                int key = (h->mlp ? h->ws_mode : 0) | (h->record_ksum ? 4 : 0) | (h->P.cfl ? 8 : 0) |
-                           (h->ws_mode == 2 ? (h->ws_offset << 4) : 0);
+                int key = (h->mlp ? h->ws_mode : 0) | (h->record_ksum ? 4 : 0) | (h->P.cfl ? 8 : 0);
                 int r = graph_for(h, key, &ex, df_graph_build);
                 if (r) return r;
                 CK(cudaGraphLaunch(ex, h->stream));
@@ -522,7 +521,6 @@ int enq_steps(sphgpu_scene* h, int solver, int nsteps) {
                 prof_collect(h);
             }
             h->frame++;
-            if (h->mlp && h->ws_mode == 2) h->ws_offset = (h->ws_offset + 1) % h->ws_every;
         }
         return 0;
     }
@@ -1385,6 +1383,7 @@ int sphgpu_attach_warm_start(sphgpu_t h, sphgpu_mlp_t m, int mode, int record_ev
     h->ws_mode = mode;
     h->ws_every = record_every > 0 ? record_every : 1;
     h->ws_offset = 0;
+    cudaMemsetAsync(&h->d.st->pad2, 0, sizeof(int), h->stream);
     h->P.warm_start = mode == 1;
     if (mode != 1) cudaMemsetAsync(h->d.kwarm, 0, sizeof(float) * h->cap, h->stream);
     invalidate_graphs(h);

@@ -22,6 +22,8 @@ struct DevStats {
     float dt;              // current step length
     float pad1;
     unsigned ticket[4];    // last-block tickets of the reductions
+    int pad2;              // warm-start recording: sampling offset
+    int pad3;
 };
 
 // Per-scene device pointers passed to every kernel by value.

@@ -406,17 +406,19 @@ __global__ void k_ws_post(DevScene s, SolverConst c, float* yout) {
 }
 
 // append every `every`-th particle (from `offset`) of the step to the dataset
-__global__ void k_ws_append(const float* X, const float* y, int n_max, const int* n_act, int every, int offset,
+__global__ void k_ws_append(const float* X, const float* y, int n_max, const int* n_act, int every, const int* offset,
                             float* dsX, float* dsy, int* ds_count, int ds_cap) {
     const int n = *n_act;
     const int i = blockIdx.x * TR + threadIdx.x;
-    const int p = offset + i * every;
+    const int p = *offset + i * every;
     if (p >= n || p >= n_max) return;
     const int slot = atomicAdd(ds_count, 1);
     if (slot >= ds_cap) return;
     for (int k = 0; k < MLP_IN; ++k) dsX[(size_t)slot * MLP_IN + k] = X[(size_t)p * MLP_IN + k];
     dsy[slot] = y[p];
 }
+// the sampling offset advances by one particle per recorded step
+__global__ void k_ws_advance(int* offset, int every) { *offset = (*offset + 1) % every; }
 }  // namespace
 
 void ws_init_attributes() {
@@ -434,8 +436,9 @@ void launch_ws_post(const DevScene& s, const SolverConst& c, float* yout, int n_
     k_ws_post<<<(n_max + TR - 1) / TR, TR, 0, st>>>(s, c, yout);
 }
 
-void launch_ws_append(const float* X, const float* y, int n_max, const int* n_act, int every, int offset, float* dsX,
+void launch_ws_append(const float* X, const float* y, int n_max, const int* n_act, int every, int* offset, float* dsX,
                       float* dsy, int* ds_count, int ds_cap, cudaStream_t st) {
     const int cnt = (n_max + every - 1) / every + 1;
     k_ws_append<<<(cnt + TR - 1) / TR, TR, 0, st>>>(X, y, n_max, n_act, every, offset, dsX, dsy, ds_count, ds_cap);
+    k_ws_advance<<<1, 1, 0, st>>>(offset, every);
 }
