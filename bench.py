@@ -70,10 +70,19 @@ def parse():
     ap.add_argument("--settle", type=int, default=300,
                     help="untimed steps before warm-up, so the timed window is in the collapsing flow "
                          "(t ~ 0.5 s) rather than the first steps from rest")
+    ap.add_argument("--no-warm-start", action="store_true", help="skip the learned warm-start arm")
+    ap.add_argument("--train-seeds", default="1,2", help="jitter seeds of the training runs")
+    ap.add_argument("--train-steps", type=int, default=350, help="recorded plain steps per training seed")
+    ap.add_argument("--train-every", type=int, default=175, help="record every n-th particle per step")
     ap.add_argument("--no-graphs", action="store_true",
                     help="host-driven solver loops instead of CUDA graphs (for ncu: kernels inside graphs "
                          "with conditional nodes cannot be profiled)")
     return ap.parse_args()
+
+
+def workload_seed(scale, seed):
+    from graphics_b200.scene import dam_break
+    return dam_break((scale, scale, scale), 0.01, (4.0, 2.0, 2.0), seed=seed)
 
 
 def workload(scale):
@@ -234,9 +243,23 @@ def run_ours(args):
         g.debug_set("use_graphs", 0)
     stream = torch.cuda.ExternalStream(g.lib.sphgpu_stream(g.h), device=torch.device("cuda", local))
 
+    # learned warm start: train on plain runs of other jitter seeds (untimed)
+    net, train_info = None, None
+    if not args.no_warm_start:
+        from graphics_b200.warmstart import train_for_scenes
+        t0 = time.perf_counter()
+        seeds = [int(x) for x in args.train_seeds.split(",") if x]
+        net, losses = train_for_scenes(lambda sd: workload_seed(args.scale, sd), seeds, settle=0,
+                                       record_steps=args.train_steps, every=args.train_every, epochs=20, lr=1e-3,
+                                       batch=8192, device=local, dataset_cap=4_200_000, **SOLVER_KW)
+        train_info = {"seeds": seeds, "samples": net.dataset_size(), "epochs": 20, "lr": 1e-3,
+                      "loss_first": float(losses[0]), "loss_last": float(losses[-1]),
+                      "seconds": round(time.perf_counter() - t0, 1)}
+
     # settle into the flow, then warm up (also builds the step graph)
     if args.settle > 0:
         g.step("dfsph", args.settle)
+    settle_pos, settle_vel = g.get("position"), g.get("velocity")
     g.step("dfsph", max(args.warmup, 1))
 
     def barrier():
@@ -263,6 +286,7 @@ def run_ours(args):
         barrier()
     ms = e0.elapsed_time(e1)
     end_pos = g.get("position")
+    st_plain = st
     ms_max = ms
     if dist:
         t = torch.tensor([ms], device="cuda")
@@ -275,6 +299,39 @@ def run_ours(args):
     it_div = st["total_iter_divergence"] / args.steps
     launches = args.steps * 13 + 2 * (st["total_iter_density"] + st["total_iter_divergence"])
 
+    # learned warm start on the same window: restore the settled state, warm
+    # up with the network attached (builds the per-particle history), time K
+    warm = None
+    if net is not None:
+        from graphics_b200.warmstart import attach
+        g.set("position", settle_pos)
+        g.set("velocity", settle_vel)
+        attach(g, net, 1)
+        g.step("dfsph", max(args.warmup, 1))
+        barrier()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        g.step_async("dfsph", args.steps)
+        f1.record(stream)
+        stw = g.synchronize()
+        barrier()
+        wms = f0.elapsed_time(f1)
+        if dist:
+            t = torch.tensor([wms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            wms = float(t.item())
+        wval = stw["n_fluid"] * args.steps * world / (wms / 1e3)
+        warm = {"value": wval, "unit": UNIT, "ms_per_step": wms / args.steps,
+                "iterations_per_step": {"density": stw["total_iter_density"] / args.steps,
+                                        "divergence": stw["total_iter_divergence"] / args.steps},
+                "speedup_vs_plain": wval / value,
+                "iteration_ratio": (st_plain["total_iter_density"] / max(stw["total_iter_density"], 1)),
+                "last_step": {"err_density": stw["err_density"], "status": stw["status"]},
+                "training": train_info,
+                "network": "16-64-64-1 GELU, BF16 weights/activations in mma.sync GEMMs, FP32 accumulate"}
+        attach(g, None, 0)
+        g.set("position", end_pos)  # continue from the plain run's state
+
     # per-kernel durations: the same kernels as individual launches bracketed
     # by CUDA events (host-driven loops), right after the timed region
     hbm, peak_kind = peaks()
@@ -283,7 +340,7 @@ def run_ours(args):
         roof, kern = profile_kernels(g, args, hbm, peak_kind)
     e2e = None
     return run_tail(args, g, sc, st, value, ms_max, it_rho, it_div, launches, roof, kern, clk, world, rank, dist,
-                    barrier, torch, snap_pos, snap_vel, end_pos)
+                    barrier, torch, snap_pos, snap_vel, end_pos, warm)
 
 
 def profile_kernels(g, args, hbm, peak_kind):
@@ -324,7 +381,7 @@ def profile_kernels(g, args, hbm, peak_kind):
 
 
 def run_tail(args, g, sc, st, value, ms_max, it_rho, it_div, launches, roof, kern, clk, world, rank, dist,
-             barrier, torch, snap_pos, snap_vel, end_pos):
+             barrier, torch, snap_pos, snap_vel, end_pos, warm):
     # end to end through the C ABI with pinned host buffers: the same K steps,
     # replayed from the snapshot taken before the timed region
     e2e = None
@@ -364,6 +421,7 @@ def run_tail(args, g, sc, st, value, ms_max, it_rho, it_div, launches, roof, ker
                 "iterations_per_step": {"density": it_rho, "divergence": it_div},
                 "last_step": {"err_density": st["err_density"], "err_divergence": st["err_divergence"],
                               "dt": st["dt"], "status": st["status"], "neighbour_overflow": st["neighbour_overflow"]},
+                "warm_start": warm,
                 "roofline": roof, "kernels": kern, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
                 "clocks": clk.summary()}
         print(json.dumps(line))
