@@ -59,6 +59,7 @@ struct SolverConst {
     float fm_ph[4];    // per phase mass
     float alpha_ph[4]; // per phase viscosity alpha
     int nphase;
+    float ws_scale;    // applied fraction of the predicted warm-start stiffness
     int cap;           // neighbour cap
     int stride;        // ELL column stride (>= fluid capacity)
 };

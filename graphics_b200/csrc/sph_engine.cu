@@ -208,6 +208,7 @@ void fill_solver_const(sphgpu_scene* h) {
     c.wc_B = c.rho0 * P.soundSpeed_cs * P.soundSpeed_cs / P.wc_gamma;
     c.cap = h->ncap;
     c.stride = h->stride;
+    c.ws_scale = P.ws_scale;
     // alpha of an interior particle of the ideal cubic lattice (spacing d),
     // the normalisation of the warm-start feature log(alpha / alpha_ref)
     {
@@ -601,6 +602,7 @@ int sphgpu_params_default(SphParams* p) {
     p->ii_min_iter = 2;
     p->ii_max_iter = 100;
     p->warm_start = 0;
+    p->ws_scale = 0.5f;
     return 0;
 }
 

@@ -384,7 +384,7 @@ __global__ void __launch_bounds__(TR) k_ws_features(DevScene s, SolverConst c, M
     if (p < n) {
         const float khat = yn / nrm[2 * MLP_IN + 1] + nrm[2 * MLP_IN];
         // kappa = khat * rho0 * alpha / dt^2; negative predictions are not applied
-        const float kw = fmaxf(khat, 0.f) * c.rho0 * s.alpha[p] / (dt * dt);
+        const float kw = c.ws_scale * fmaxf(khat, 0.f) * c.rho0 * s.alpha[p] / (dt * dt);
         s.kwarm[p] = kw;
         s.pk[p].w = kw / s.rho[p];  // read by the warm-correction sweep
     }

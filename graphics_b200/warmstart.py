@@ -169,7 +169,7 @@ def train_for_scenes(make_scene, seeds, settle, record_steps, every, epochs=20, 
             g.step("dfsph", settle)
         record(g, net, record_steps, every)
         g.close()
-    net.fit_normalisation()
     net.shuffle(7)
+    net.fit_normalisation()
     losses = net.train(epochs=epochs, batch=batch, lr=lr)
     return net, losses

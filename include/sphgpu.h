@@ -92,7 +92,11 @@ typedef struct SphParams {
     int ii_min_iter, ii_max_iter;
     /* learned warm start for the DFSPH density solve (0 = plain method) */
     int warm_start;
-    int reserved[7];
+    /* fraction of the predicted stiffness applied before the loop: the loop
+     * only pushes particles apart (rho_adv >= rho0 clamp, DFSPH.cpp:620-623),
+     * so an over-prediction cannot be undone and is kept below 1 */
+    float ws_scale;
+    int reserved[6];
 } SphParams;
 
 /* Per-step statistics (replaces m_EC and the CALL_TIME log rows). */
