@@ -409,9 +409,10 @@ __global__ void k_ws_post(DevScene s, SolverConst c, float* yout) {
 __global__ void k_ws_append(const float* X, const float* y, int n_max, const int* n_act, int every, const int* offset,
                             float* dsX, float* dsy, int* ds_count, int ds_cap) {
     const int n = *n_act;
-    const int i = blockIdx.x * TR + threadIdx.x;
-    const int p = *offset + i * every;
-    if (p >= n || p >= n_max) return;
+    const long long i = (long long)blockIdx.x * TR + threadIdx.x;
+    const long long pl = (long long)*offset + i * (long long)every;
+    if (pl < 0 || pl >= n || pl >= n_max) return;
+    const int p = (int)pl;
     const int slot = atomicAdd(ds_count, 1);
     if (slot >= ds_cap) return;
     for (int k = 0; k < MLP_IN; ++k) dsX[(size_t)slot * MLP_IN + k] = X[(size_t)p * MLP_IN + k];
@@ -438,7 +439,8 @@ void launch_ws_post(const DevScene& s, const SolverConst& c, float* yout, int n_
 
 void launch_ws_append(const float* X, const float* y, int n_max, const int* n_act, int every, int* offset, float* dsX,
                       float* dsy, int* ds_count, int ds_cap, cudaStream_t st) {
-    const int cnt = (n_max + every - 1) / every + 1;
-    k_ws_append<<<(cnt + TR - 1) / TR, TR, 0, st>>>(X, y, n_max, n_act, every, offset, dsX, dsy, ds_count, ds_cap);
+    const long long cnt = ((long long)n_max + every - 1) / every + 1;
+    k_ws_append<<<(int)((cnt + TR - 1) / TR), TR, 0, st>>>(X, y, n_max, n_act, every, offset, dsX, dsy, ds_count,
+                                                          ds_cap);
     k_ws_advance<<<1, 1, 0, st>>>(offset, every);
 }
