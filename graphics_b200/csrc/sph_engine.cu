@@ -382,9 +382,9 @@ int enq_df_step(sphgpu_scene* h, bool capturing) {
         launch(h, "cfl", st, [&] { launch_cfl(d, h->cap, h->P.cfl_factor, h->P.particle_d, h->P.dt_max, h->P.dt_min, st); });
     const int ws = h->mlp ? h->ws_mode : 0;
     launch(h, "df_forces", st, [&] { launch_df_forces(d, h->c, h->cap, 0, st); });
-    if (ws == 1) {
+    if (ws == 1 || ws == 3) {
         launch(h, "ws_features_infer", st, [&] {
-            launch_ws_features(d, h->c, h->mlp->m, 1, h->P.dt_max, h->alpha_ref, nullptr, h->cap, st);
+            launch_ws_features(d, h->c, h->mlp->m, ws == 1 ? 1 : 2, h->P.dt_max, h->alpha_ref, nullptr, h->cap, st);
         });
         launch(h, "df_warm", st, [&] { launch_df_warm_correction(d, h->c, h->cap, st); });
     } else if (ws == 2) {
@@ -876,6 +876,12 @@ int sphgpu_get_fluid(sphgpu_t h, const char* field, float* out) {
     else if (f == "DFkappaV") src = d.kappav;
     else if (f == "kappa_sum") src = d.ksum;
     else if (f == "kappa_warm") src = d.kwarm;
+    else if (f == "ws_hist") {
+        CK(cudaMemcpy2D(d.vadv, sizeof(float4), d.hist, sizeof(float4), sizeof(float4), n, cudaMemcpyDeviceToDevice));
+        src = d.vadv;
+        f4 = true;
+        comps = 3;
+    }
     else if (f == "density_adv") src = d.aux0;
     else if (f == "divergenceDeviation") src = d.aux1;
     else if (f == "presure") src = d.kr;
@@ -1375,7 +1381,7 @@ int sphgpu_mlp_predict(sphgpu_mlp_t m, const float* X, float* y, int n) {
 // start every DFSPH step, 2 records (features, converged stiffness) of every
 // `record_every`-th particle of every step into the network's dataset.
 int sphgpu_attach_warm_start(sphgpu_t h, sphgpu_mlp_t m, int mode, int record_every) {
-    if (!h || mode < 0 || mode > 2 || (mode && !m) || (mode == 2 && record_every <= 0)) return SPHGPU_EINVAL;
+    if (!h || mode < 0 || mode > 3 || (mode && !m) || (mode == 2 && record_every <= 0)) return SPHGPU_EINVAL;
     cudaSetDevice(h->device);
     if (mode && m->device != h->device) { h->err = "network and scene on different devices"; return SPHGPU_EINVAL; }
     if (mode == 2 && !h->recX) {
@@ -1386,8 +1392,8 @@ int sphgpu_attach_warm_start(sphgpu_t h, sphgpu_mlp_t m, int mode, int record_ev
     h->ws_every = record_every > 0 ? record_every : 1;
     h->ws_offset = 0;
     cudaMemsetAsync(&h->d.st->pad2, 0, sizeof(int), h->stream);
-    h->P.warm_start = mode == 1;
-    if (mode != 1) cudaMemsetAsync(h->d.kwarm, 0, sizeof(float) * h->cap, h->stream);
+    h->P.warm_start = mode == 1 || mode == 3;
+    if (mode != 1 && mode != 3) cudaMemsetAsync(h->d.kwarm, 0, sizeof(float) * h->cap, h->stream);
     invalidate_graphs(h);
     return cudaStreamSynchronize(h->stream) == cudaSuccess ? 0 : SPHGPU_ECUDA;
 }

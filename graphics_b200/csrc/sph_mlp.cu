@@ -357,6 +357,8 @@ __device__ __forceinline__ void ws_features(const DevScene& s, const SolverConst
 }
 
 // features -> network -> kwarm (and, when recording, the features of the step)
+// INFER 0: features only; 1: network; 2: previous step's stiffness (the
+// classic warm start, as a comparison for the network)
 template <int INFER>
 __global__ void __launch_bounds__(TR) k_ws_features(DevScene s, SolverConst c, MlpDev m, float dt_max,
                                                    float alpha_ref, float* Xout) {
@@ -376,6 +378,14 @@ __global__ void __launch_bounds__(TR) k_ws_features(DevScene s, SolverConst c, M
         for (int i = 0; i < MLP_IN; ++i) x[i] = 0.f;
     }
     if (!INFER) return;
+    if (INFER == 2) {
+        if (p < n) {
+            const float kw = c.ws_scale * fmaxf(x[4], 0.f) * c.rho0 * s.alpha[p] / (dt * dt);
+            s.kwarm[p] = kw;
+            s.pk[p].w = kw / s.rho[p];
+        }
+        return;
+    }
     load_weights(m, S);
     const float* nrm = m.norm;
     for (int i = 0; i < MLP_IN; ++i) S.X[threadIdx.x * MLP_IN + i] = __float2bfloat16_rn((x[i] - nrm[i]) * nrm[MLP_IN + i]);
@@ -429,7 +439,8 @@ void ws_init_attributes() {
 void launch_ws_features(const DevScene& s, const SolverConst& c, const MlpDev& m, int infer, float dt_max,
                         float alpha_ref, float* Xout, int n_max, cudaStream_t st) {
     const int blocks = (n_max + TR - 1) / TR;
-    if (infer) k_ws_features<1><<<blocks, TR, sizeof(FwdSmem), st>>>(s, c, m, dt_max, alpha_ref, Xout);
+    if (infer == 1) k_ws_features<1><<<blocks, TR, sizeof(FwdSmem), st>>>(s, c, m, dt_max, alpha_ref, Xout);
+    else if (infer == 2) k_ws_features<2><<<blocks, TR, 0, st>>>(s, c, m, dt_max, alpha_ref, Xout);
     else k_ws_features<0><<<blocks, TR, 0, st>>>(s, c, m, dt_max, alpha_ref, Xout);
 }
 

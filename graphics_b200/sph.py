@@ -25,7 +25,7 @@ from ._lib import SphParams, SphStepStats, SphGpuError
 
 SOLVERS = {"wcsph": _lib.WCSPH, "pcisph": _lib.PCISPH, "iisph_m": _lib.IISPH_M, "dfsph": _lib.DFSPH}
 
-VEC_FIELDS = ("position", "velocity", "vel_adv", "acce_adv", "acceleration")
+VEC_FIELDS = ("position", "velocity", "vel_adv", "acce_adv", "acceleration", "ws_hist")
 
 
 def _fptr(a):

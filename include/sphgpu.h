@@ -217,7 +217,8 @@ int sphgpu_mlp_gradient(sphgpu_mlp_t m, const float* X, const float* y, int n, f
 int sphgpu_mlp_predict(sphgpu_mlp_t m, const float* X, float* y, int n);
 /* mode 0: detach; 1: apply the warm start every DFSPH step; 2: record
  * (features, converged stiffness) of every record_every-th particle into the
- * network's dataset (plain solver, no warm start). */
+ * network's dataset (plain solver, no warm start); 3: the classic warm start
+ * (previous step's stiffness, no network) for comparison. */
 int sphgpu_attach_warm_start(sphgpu_t h, sphgpu_mlp_t m, int mode, int record_every);
 
 /* Copy of the last error message. */
