@@ -1,8 +1,11 @@
 // sph_mlp.cu -- learned warm start for the DFSPH constant-density loop.
 //
-// The network (16 -> 64 -> 64 -> 1, GELU) predicts, per particle, the
-// dimensionless stiffness khat = kappa_sum * dt^2 / (rho0 * alpha) that the
-// density loop (DFSPH.cpp:566-700) applies over all of its iterations.  The
+// The network (16 -> 64 -> 64 -> 1, GELU) predicts, per particle, the total
+// stiffness kappa_sum that the density loop (DFSPH.cpp:566-700) applies over
+// all of its iterations.  kappa ~ p / rho (the loop's velocity update
+// dt sum m (k_i/rho_i + k_j/rho_j) gradW is the pressure acceleration with
+// p/rho^2 = kappa/rho), so it is set by the flow (about g times depth) and
+// does not scale with the step length, which makes it a stable target.  The
 // prediction is applied once before the loop as a pressure-velocity
 // correction of the same form as DFSPH.cpp:674; the unmodified loop then
 // runs to the same tolerance, so the network only changes where the loop
@@ -302,8 +305,8 @@ namespace {
 //  0 neighbour count / 32             8  |a_adv| dt^2 / d
 //  1 (rho - rho0)/rho0 * 100          9  boundary-neighbour fraction
 //  2 dt * Drho/Dt / rho0 * 100        10 log(alpha / alpha_ref)
-//  3 (max(rho_adv0, rho0) - rho0)/rho0 * 100   11 neighbour mean of khat_prev
-//  4 khat of the previous step        12 dt / dt_max
+//  3 (max(rho_adv0, rho0) - rho0)/rho0 * 100   11 neighbour mean of feature 4
+//  4 kappa_sum of the previous step/10 12 dt / dt_max
 //  5 feature 3 of the previous step   13 |sum_j m gradW_ij| d / rho0
 //  6 feature 2 of the previous step   14 v_y dt / d
 //  7 |v| dt / d                       15 1
@@ -342,14 +345,14 @@ __device__ __forceinline__ void ws_features(const DevScene& s, const SolverConst
     x[1] = (rho - rho0) / rho0 * 100.f;
     x[2] = divt;
     x[3] = pred;
-    x[4] = hp.x;
+    x[4] = hp.x * 0.1f;
     x[5] = hp.y;
     x[6] = hp.z;
     x[7] = sqrtf(v.x * v.x + v.y * v.y + v.z * v.z) * dt / d;
     x[8] = sqrtf(a.x * a.x + a.y * a.y + a.z * a.z) * dt * dt / d;
     x[9] = cnt ? (float)nb / (float)cnt : 0.f;
     x[10] = logf(fmaxf(s.alpha[p], 1e-30f) / alpha_ref);
-    x[11] = nfl ? kp / (float)nfl : 0.f;
+    x[11] = nfl ? 0.1f * kp / (float)nfl : 0.f;
     x[12] = dt / dt_max;
     x[13] = sqrtf(ax * ax + ay * ay + az * az) * d / rho0;
     x[14] = v.y * dt / d;
@@ -380,7 +383,7 @@ __global__ void __launch_bounds__(TR) k_ws_features(DevScene s, SolverConst c, M
     if (!INFER) return;
     if (INFER == 2) {
         if (p < n) {
-            const float kw = c.ws_scale * fmaxf(x[4], 0.f) * c.rho0 * s.alpha[p] / (dt * dt);
+            const float kw = c.ws_scale * fmaxf(s.hist[p].x, 0.f);
             s.kwarm[p] = kw;
             s.pk[p].w = kw / s.rho[p];
         }
@@ -392,26 +395,24 @@ __global__ void __launch_bounds__(TR) k_ws_features(DevScene s, SolverConst c, M
     __syncthreads();
     const float yn = forward_rows(S);
     if (p < n) {
-        const float khat = yn / nrm[2 * MLP_IN + 1] + nrm[2 * MLP_IN];
-        // kappa = khat * rho0 * alpha / dt^2; negative predictions are not applied
-        const float kw = c.ws_scale * fmaxf(khat, 0.f) * c.rho0 * s.alpha[p] / (dt * dt);
+        const float kpred = yn / nrm[2 * MLP_IN + 1] + nrm[2 * MLP_IN];
+        // negative predictions are not applied (the loop only adds pressure)
+        const float kw = c.ws_scale * fmaxf(kpred, 0.f);
         s.kwarm[p] = kw;
         s.pk[p].w = kw / s.rho[p];  // read by the warm-correction sweep
     }
 }
 
-// after the density loop: the step's total stiffness (warm + loop) as khat,
-// history for the next step's features, and the training label
+// after the density loop: the step's total stiffness (warm + loop), history
+// for the next step's features, and the training label
 __global__ void k_ws_post(DevScene s, SolverConst c, float* yout) {
     const int n = s.st->n_active;
     const int p = blockIdx.x * TR + threadIdx.x;
     if (p >= n) return;
-    const float dt = *s.dt;
     const float ktot = s.ksum[p] + s.kwarm[p];  // kwarm is 0 unless the warm start ran
-    const float khat = ktot * dt * dt / (c.rho0 * s.alpha[p]);
     const float2 w = s.wsbuf[p];
-    s.hist[p] = make_float4(khat, w.x, w.y, 0.f);
-    if (yout) yout[p] = khat;
+    s.hist[p] = make_float4(ktot, w.x, w.y, 0.f);
+    if (yout) yout[p] = ktot;
     s.ksum[p] = 0.f;
 }
 

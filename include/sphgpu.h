@@ -196,8 +196,8 @@ int sphgpu_profile_read(sphgpu_t h, char* names, int name_len, double* ms, int* 
 
 /* ---------------- learned warm start (no reference counterpart) ----------------
  * A BF16 MLP (16 -> 64 -> 64 -> 1, GELU; FP32 master weights) that predicts the
- * per-particle stiffness the DFSPH constant-density loop (DFSPH.cpp:566-700)
- * converges to, applied once before the unmodified loop.  Parameter vector
+ * per-particle total stiffness kappa the DFSPH constant-density loop
+ * (DFSPH.cpp:566-700) applies, applied once before the unmodified loop.  Parameter vector
  * (FP32, SPHGPU_MLP_NPARAM): W1[16][64] b1[64] W2[64][64] b2[64] W3[64] b3.
  * norm[34]: feature mean[16], 1/std[16], label mean, 1/std. */
 #define SPHGPU_MLP_NPARAM 5313
