@@ -602,7 +602,7 @@ int sphgpu_params_default(SphParams* p) {
     p->ii_min_iter = 2;
     p->ii_max_iter = 100;
     p->warm_start = 0;
-    p->ws_scale = 0.5f;
+    p->ws_scale = 1.0f;
     return 0;
 }
 
