@@ -331,10 +331,19 @@ __global__ void __launch_bounds__(NT) k_cfl(DevScene s, float cfl, float d, floa
         last = atomicAdd(&s.st->ticket[2], 1u) == gridDim.x - 1;
     }
     __syncthreads();
-    if (last && threadIdx.x == 0) {
-        __threadfence();
+    if (!last) return;
+    __threadfence();
+    // the last block reduces the block maxima with all its threads
+    double vm = 0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += NT) vm = fmax(vm, ((volatile double*)s.partial)[i]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) vm = fmax(vm, __shfl_down_sync(0xffffffffu, vm, o));
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = vm;
+    __syncthreads();
+    if (threadIdx.x == 0) {
         double vmax = 0;
-        for (int i = 0; i < (int)gridDim.x; ++i) vmax = fmax(vmax, ((volatile double*)s.partial)[i]);
+        for (int i = 0; i < NT / 32; ++i) vmax = fmax(vmax, sh[i]);
         double dt = vmax > 0 ? (double)cfl * (double)d / vmax : (double)dt_max;
         if (dt > dt_max) dt = dt_max;
         if (dt < dt_min) dt = dt_min;
