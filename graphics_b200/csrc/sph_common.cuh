@@ -86,6 +86,21 @@ __device__ __forceinline__ float grad_over_r(const KerConst& k, float len2) {
     return q <= 1.f ? fin : fout;
 }
 
+// W(r) and -W'(r)/r of the single-h spline from r^2 (one rsqrt, no
+// division): the forms of ker_W / ker_W_grad (SphBase.h:840-889) used where
+// the result is summed (densities, alpha), relative error a few ulp.
+__device__ __forceinline__ void kernel_pair(const KerConst& k, float len2, float& w, float& f) {
+    const float inv_r = rsqrtf(len2);
+    const float q = len2 * inv_r * k.inv_h;
+    const float t = 2.f - q;
+    const float win = k.theta * fmaf(q * q, fmaf(0.75f, q, -1.5f), 1.f);
+    const float wout = k.theta * 0.25f * t * t * t;
+    w = q <= 1.f ? win : wout;
+    const float fin = k.g_in * fmaf(-2.25f, q, 3.f);
+    const float fout = k.g_out * t * t * inv_r;
+    f = q <= 1.f ? fin : fout;
+}
+
 // per-pair-h spline with range check, SphBase.h:855-871
 __device__ __forceinline__ float ker_W_h(float r, float h) {
     float q = r / h, qm2 = 2.f - q;

@@ -254,6 +254,7 @@ int alloc_scene(sphgpu_scene* h) {
     r |= dalloc(h, &d.key, n); r |= dalloc(h, &d.slot, n); r |= dalloc(h, &d.tmp, n);
     r |= dalloc(h, &d.cell_count, (size_t)h->g.nkeys + 1);
     r |= dalloc(h, &d.cell_start, (size_t)h->g.nkeys + 1);
+    r |= dalloc(h, &d.cstart2, (size_t)h->g.nkeys + 1);
     r |= dalloc(h, &d.bcell_start, (size_t)h->g.nkeys + 1);
     r |= dalloc(h, &d.nbr, (size_t)h->stride * ((h->ncap + 3) / 4) * 4);
     r |= dalloc(h, &d.ncount, n);
@@ -285,7 +286,7 @@ void free_scene(sphgpu_scene* h) {
     void* ptrs[] = {d.pos, d.vel, d.gid, d.rho, d.alpha, d.vadv, d.pv, d.pk, d.bpv, d.kappav, d.acc, d.kr, d.kappa, d.ksum, d.aux0,
                     d.aux1, d.aux4, d.kwarm, d.hist, d.wsbuf, d.pos_s, d.vel_s, d.gid_s, d.hist_s, d.key, d.slot, d.tmp,
                     h->recX, h->recY,
-                    d.cell_count, d.cell_start, d.bcell_start, d.nbr, d.ncount, d.partial, d.st,
+                    d.cell_count, d.cell_start, d.bcell_start, d.cstart2, d.nbr, d.ncount, d.partial, d.st,
                     d.bpos, d.bvel, d.bgid, h->cub_tmp};
     for (void* p : ptrs)
         if (p) cudaFree(p);

@@ -106,6 +106,13 @@ __global__ void k_count_active(DevScene s, int dead_key) {
     s.st->n_active = act;
 }
 
+// interleaved {fluid start, boundary start} per cell key: one 8-byte load
+// per cell bound in the neighbour-list kernel
+__global__ void k_merge_starts(DevScene s, int nk) {
+    const int k = blockIdx.x * NT + threadIdx.x;
+    if (k <= nk) s.cstart2[k] = make_int2(s.cell_start[k], s.bcell_start[k]);
+}
+
 // mode 0: neighbour lists only; 1: + DFSPH rho and alpha
 // (DF_constantDensitySolverFirst, DFSPH.cpp:84-193); 2: + WCSPH rho and Tait
 // pressure (WcSph::wc_computePressure, WcSph.cpp:99-153).
@@ -119,6 +126,8 @@ __global__ void __launch_bounds__(128) k_build(DevScene s, GridGeom g, SolverCon
         const float4 pa = s.pos[p];
         const int ph = phase_of(pa);
         const float fm0 = c.fm_ph[ph], rho0 = c.rho0_ph[ph];
+        const float4* __restrict__ P = s.pos;
+        const float4* __restrict__ BP = s.bpos;
         const int cx = cell_coord(pa.x, g.min[0], g.divisor);
         const int cy = cell_coord(pa.y, g.min[1], g.divisor);
         const int cz = cell_coord(pa.z, g.min[2], g.divisor);
@@ -131,27 +140,26 @@ __global__ void __launch_bounds__(128) k_build(DevScene s, GridGeom g, SolverCon
                 for (int dx = -1; dx <= 1; ++dx) {
                     int x = cx + dx, y = cy + dy, z = cz + dz;
                     if (!cell_inside(g, x, y, z)) continue;
-                    int key = cell_key(g, x, y, z);
-                    int a = s.cell_start[key], b = s.cell_start[key + 1];
-                    for (int q = a; q < b; ++q) {
-                        if (q == p) continue;
-                        float4 pb = s.pos[q];
-                        float len2 = dis_square_rn(pa.x, pa.y, pa.z, pb.x, pb.y, pb.z);
-                        if (len2 < c.h2cut) {
+                    const int key = cell_key(g, x, y, z);
+                    const int2 s0 = __ldg(s.cstart2 + key), s1 = __ldg(s.cstart2 + key + 1);
+                    for (int q = s0.x; q < s1.x; ++q) {
+                        const float4 pb = __ldg(P + q);
+                        const float len2 = dis_square_rn(pa.x, pa.y, pa.z, pb.x, pb.y, pb.z);
+                        if (len2 < c.h2cut && q != p) {
                             if (cnt < cap) {
                                 out[ell_index(stride, p, cnt)] = q;
                                 ++cnt;
                                 if (MODE != 0) {
-                                    float dis = sqrtf(len2);
-                                    density += fm0 * ker_W(c.k, dis);
+                                    float w, f;
+                                    kernel_pair(c.k, len2, w, f);
+                                    density = fmaf(fm0, w, density);
                                     if (MODE == 1) {
-                                        float gs = -ker_Wg(c.k, dis);
-                                        float f = gs / dis;
-                                        a1x += (pa.x - pb.x) * f * fm0;
-                                        a1y += (pa.y - pb.y) * f * fm0;
-                                        a1z += (pa.z - pb.z) * f * fm0;
-                                        float t = gs * fm0;
-                                        a2 = (float)((double)a2 + (double)t * (double)t);
+                                        const float fm = f * fm0;
+                                        a1x = fmaf(pa.x - pb.x, fm, a1x);
+                                        a1y = fmaf(pa.y - pb.y, fm, a1y);
+                                        a1z = fmaf(pa.z - pb.z, fm, a1z);
+                                        const float t = fm * sqrtf(len2);  // |gradW| m
+                                        a2 = fmaf(t, t, a2);
                                     }
                                 }
                             } else {
@@ -159,24 +167,23 @@ __global__ void __launch_bounds__(128) k_build(DevScene s, GridGeom g, SolverCon
                             }
                         }
                     }
-                    int ba = s.bcell_start[key], bb = s.bcell_start[key + 1];
-                    for (int q = ba; q < bb; ++q) {
-                        float4 pb = s.bpos[q];
-                        float len2 = dis_square_rn(pa.x, pa.y, pa.z, pb.x, pb.y, pb.z);
+                    for (int q = s0.y; q < s1.y; ++q) {
+                        const float4 pb = __ldg(BP + q);
+                        const float len2 = dis_square_rn(pa.x, pa.y, pa.z, pb.x, pb.y, pb.z);
                         if (len2 < c.h2cut) {
                             if (cnt < cap) {
                                 out[ell_index(stride, p, cnt)] = q | (int)BND_FLAG;
                                 ++cnt;
                                 if (MODE != 0) {
-                                    float dis = sqrtf(len2);
-                                    float vol = pb.w;
-                                    density += rho0 * vol * ker_W(c.k, dis);
+                                    float w, f;
+                                    kernel_pair(c.k, len2, w, f);
+                                    const float mb = rho0 * pb.w;
+                                    density = fmaf(mb, w, density);
                                     if (MODE == 1) {
-                                        float gs = -ker_Wg(c.k, dis);
-                                        float f = gs / dis;
-                                        a1x += (pa.x - pb.x) * f * rho0 * vol;
-                                        a1y += (pa.y - pb.y) * f * rho0 * vol;
-                                        a1z += (pa.z - pb.z) * f * rho0 * vol;
+                                        const float fm = f * mb;
+                                        a1x = fmaf(pa.x - pb.x, fm, a1x);
+                                        a1y = fmaf(pa.y - pb.y, fm, a1y);
+                                        a1z = fmaf(pa.z - pb.z, fm, a1z);
                                     }
                                 }
                             } else {
@@ -302,6 +309,7 @@ void launch_scatter_reorder(const DevScene& s, const GridGeom& g, int n_old, int
 
 void launch_count_active(const DevScene& s, const GridGeom& g, cudaStream_t st) {
     k_count_active<<<1, 1, 0, st>>>(s, g.nkeys - 1);
+    k_merge_starts<<<nblk(g.nkeys + 1, NT), NT, 0, st>>>(s, g.nkeys);
 }
 
 void launch_build(const DevScene& s, const GridGeom& g, const SolverConst& c, int mode, int n_max, cudaStream_t st) {

@@ -60,6 +60,7 @@ struct DevScene {
     int* tmp;
     int* cell_count;    // nkeys + 1
     int* cell_start;    // nkeys + 1
+    int2* cstart2;      // nkeys + 1: {fluid start, boundary start} per cell key
     // neighbour lists (ELL, column-major)
     int* nbr;
     int* ncount;
