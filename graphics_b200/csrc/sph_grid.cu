@@ -119,9 +119,9 @@ __global__ void k_merge_starts(DevScene s, int nk) {
 template <int MODE>
 __global__ void __launch_bounds__(128) k_build(DevScene s, GridGeom g, SolverConst c) {
     const int n = s.st->n_active;
-    int p = blockIdx.x * 128 + threadIdx.x;
+    const int p = blockIdx.x * 128 + threadIdx.x;
     int cnt = 0, over = 0;
-    bool act = p < n;
+    const bool act = p < n;
     if (act) {
         const float4 pa = s.pos[p];
         const int ph = phase_of(pa);
@@ -131,14 +131,26 @@ __global__ void __launch_bounds__(128) k_build(DevScene s, GridGeom g, SolverCon
         const int cx = cell_coord(pa.x, g.min[0], g.divisor);
         const int cy = cell_coord(pa.y, g.min[1], g.divisor);
         const int cz = cell_coord(pa.z, g.min[2], g.divisor);
-        float density = ker_W(c.k, 0.f) * fm0;
-        float a1x = 0.f, a1y = 0.f, a1z = 0.f, a2 = 0.f;
         int* out = s.nbr;
-        const int stride = c.stride, cap = c.cap;
-        for (int dz = -1; dz <= 1; ++dz)
-            for (int dy = -1; dy <= 1; ++dy)
+        const size_t stride = (size_t)c.stride;
+        const int cap = c.cap;
+        // distances to the faces of the own cell, for skipping neighbour cells
+        // that lie beyond the cut (with a margin, so only cells that provably
+        // hold no neighbour are skipped; the candidate test itself is exact)
+        const float hc = 1.f / g.divisor;
+        const float lo_x = pa.x - (g.min[0] + cx * hc), hi_x = (g.min[0] + (cx + 1) * hc) - pa.x;
+        const float lo_y = pa.y - (g.min[1] + cy * hc), hi_y = (g.min[1] + (cy + 1) * hc) - pa.y;
+        const float lo_z = pa.z - (g.min[2] + cz * hc), hi_z = (g.min[2] + (cz + 1) * hc) - pa.z;
+        const float cull = c.h2cut * 1.001f + 1e-12f;
+        // phase 1: candidate scan in the reference's order, append indices
+        for (int dz = -1; dz <= 1; ++dz) {
+            const float gz = dz < 0 ? fmaxf(lo_z, 0.f) : (dz > 0 ? fmaxf(hi_z, 0.f) : 0.f);
+            for (int dy = -1; dy <= 1; ++dy) {
+                const float gy = dy < 0 ? fmaxf(lo_y, 0.f) : (dy > 0 ? fmaxf(hi_y, 0.f) : 0.f);
                 for (int dx = -1; dx <= 1; ++dx) {
-                    int x = cx + dx, y = cy + dy, z = cz + dz;
+                    const float gx = dx < 0 ? fmaxf(lo_x, 0.f) : (dx > 0 ? fmaxf(hi_x, 0.f) : 0.f);
+                    if (gx * gx + gy * gy + gz * gz > cull) continue;
+                    const int x = cx + dx, y = cy + dy, z = cz + dz;
                     if (!cell_inside(g, x, y, z)) continue;
                     const int key = cell_key(g, x, y, z);
                     const int2 s0 = __ldg(s.cstart2 + key), s1 = __ldg(s.cstart2 + key + 1);
@@ -146,64 +158,57 @@ __global__ void __launch_bounds__(128) k_build(DevScene s, GridGeom g, SolverCon
                         const float4 pb = __ldg(P + q);
                         const float len2 = dis_square_rn(pa.x, pa.y, pa.z, pb.x, pb.y, pb.z);
                         if (len2 < c.h2cut && q != p) {
-                            if (cnt < cap) {
-                                out[ell_index(stride, p, cnt)] = q;
-                                ++cnt;
-                                if (MODE != 0) {
-                                    float w, f;
-                                    kernel_pair(c.k, len2, w, f);
-                                    density = fmaf(fm0, w, density);
-                                    if (MODE == 1) {
-                                        const float fm = f * fm0;
-                                        a1x = fmaf(pa.x - pb.x, fm, a1x);
-                                        a1y = fmaf(pa.y - pb.y, fm, a1y);
-                                        a1z = fmaf(pa.z - pb.z, fm, a1z);
-                                        const float t = fm * sqrtf(len2);  // |gradW| m
-                                        a2 = fmaf(t, t, a2);
-                                    }
-                                }
-                            } else {
-                                ++over;
-                            }
+                            if (cnt < cap) out[ell_index(stride, p, cnt++)] = q;
+                            else ++over;
                         }
                     }
                     for (int q = s0.y; q < s1.y; ++q) {
                         const float4 pb = __ldg(BP + q);
                         const float len2 = dis_square_rn(pa.x, pa.y, pa.z, pb.x, pb.y, pb.z);
                         if (len2 < c.h2cut) {
-                            if (cnt < cap) {
-                                out[ell_index(stride, p, cnt)] = q | (int)BND_FLAG;
-                                ++cnt;
-                                if (MODE != 0) {
-                                    float w, f;
-                                    kernel_pair(c.k, len2, w, f);
-                                    const float mb = rho0 * pb.w;
-                                    density = fmaf(mb, w, density);
-                                    if (MODE == 1) {
-                                        const float fm = f * mb;
-                                        a1x = fmaf(pa.x - pb.x, fm, a1x);
-                                        a1y = fmaf(pa.y - pb.y, fm, a1y);
-                                        a1z = fmaf(pa.z - pb.z, fm, a1z);
-                                    }
-                                }
-                            } else {
-                                ++over;
-                            }
+                            if (cnt < cap) out[ell_index(stride, p, cnt++)] = q | (int)BND_FLAG;
+                            else ++over;
                         }
                     }
                 }
+            }
+        }
         s.ncount[p] = cnt;
-        if (MODE == 1) {
-            s.rho[p] = density;
-            float al = a1x * a1x + a1y * a1y + a1z * a1z + a2;
-            if (al < 1.0e-6f) al = 1.0e-6f;
-            s.alpha[p] = density / al;
-        } else if (MODE == 2) {
-            s.rho[p] = density;
-            // Tait, WcSph.cpp:142-146 (NEGLECT_NEGATIVE_PRESSURE)
-            float pr = c.wc_B * (powf(density / rho0, c.wc_gamma) - 1.f);
-            if (pr < 0.f) pr = 0.f;
-            s.kr[p] = pr;
+        if (MODE != 0) {
+            // phase 2: rho and alpha over the stored list (all lanes busy)
+            float density = ker_W(c.k, 0.f) * fm0;
+            float a1x = 0.f, a1y = 0.f, a1z = 0.f, a2 = 0.f;
+            for (int k = 0; k < cnt; ++k) {
+                const unsigned e = (unsigned)out[ell_index(stride, p, k)];
+                const bool bnd = (e & BND_FLAG) != 0u;
+                const float4 pb = __ldg((bnd ? BP : P) + (e & BND_MASK));
+                const float xx = pa.x - pb.x, xy = pa.y - pb.y, xz = pa.z - pb.z;
+                const float len2 = dis_square_rn(pa.x, pa.y, pa.z, pb.x, pb.y, pb.z);
+                float w, f;
+                kernel_pair(c.k, len2, w, f);
+                const float m = bnd ? rho0 * pb.w : fm0;
+                density = fmaf(m, w, density);
+                if (MODE == 1) {
+                    const float fm = f * m;
+                    a1x = fmaf(xx, fm, a1x);
+                    a1y = fmaf(xy, fm, a1y);
+                    a1z = fmaf(xz, fm, a1z);
+                    const float t = bnd ? 0.f : fm * sqrtf(len2);  // |gradW| m, fluid only (DFSPH.cpp:161)
+                    a2 = fmaf(t, t, a2);
+                }
+            }
+            if (MODE == 1) {
+                s.rho[p] = density;
+                float al = a1x * a1x + a1y * a1y + a1z * a1z + a2;
+                if (al < 1.0e-6f) al = 1.0e-6f;
+                s.alpha[p] = density / al;
+            } else {
+                s.rho[p] = density;
+                // Tait, WcSph.cpp:142-146 (NEGLECT_NEGATIVE_PRESSURE)
+                float pr = c.wc_B * (powf(density / rho0, c.wc_gamma) - 1.f);
+                if (pr < 0.f) pr = 0.f;
+                s.kr[p] = pr;
+            }
         }
     }
     __shared__ int sh[4];
