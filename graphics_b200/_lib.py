@@ -30,7 +30,7 @@ class SphParams(C.Structure):
                 ("wc_gamma", C.c_float), ("pci_min_iter", C.c_int), ("pci_max_iter", C.c_int),
                 ("ii_omega", C.c_float), ("ii_eta_rel", C.c_float), ("ii_min_iter", C.c_int),
                 ("ii_max_iter", C.c_int), ("warm_start", C.c_int), ("ws_scale", C.c_float),
-                ("reserved", C.c_int * 6)]
+                ("ii_compat", C.c_int), ("reserved", C.c_int * 5)]
 
 
 class SphStepStats(C.Structure):

@@ -96,6 +96,7 @@ struct sphgpu_scene {
     float* recY = nullptr;  // [cap] labels
     float alpha_ref = 1.f;
     long long total_removed = 0;  // gid stays a permutation of [0, n) while 0
+    int last_solver = -1;         // solver of the last step (carried-state validity)
 };
 
 namespace {
@@ -251,6 +252,9 @@ int alloc_scene(sphgpu_scene* h) {
     r |= dalloc(h, &d.aux4, n); r |= dalloc(h, &d.kwarm, n); r |= dalloc(h, &d.hist, n); r |= dalloc(h, &d.wsbuf, n);
     r |= dalloc(h, &d.pos_s, n); r |= dalloc(h, &d.vel_s, n); r |= dalloc(h, &d.gid_s, n);
     r |= dalloc(h, &d.hist_s, n);
+    r |= dalloc(h, &d.cA, n); r |= dalloc(h, &d.cB, n); r |= dalloc(h, &d.cC, n);
+    r |= dalloc(h, &d.cA_s, n); r |= dalloc(h, &d.cB_s, n); r |= dalloc(h, &d.cC_s, n);
+    r |= dalloc(h, &d.ap, n); r |= dalloc(h, &d.pl2, n);
     r |= dalloc(h, &d.key, n); r |= dalloc(h, &d.slot, n); r |= dalloc(h, &d.tmp, n);
     r |= dalloc(h, &d.cell_count, (size_t)h->g.nkeys + 1);
     r |= dalloc(h, &d.cell_start, (size_t)h->g.nkeys + 1);
@@ -270,6 +274,7 @@ int alloc_scene(sphgpu_scene* h) {
     cudaMemsetAsync(d.kwarm, 0, sizeof(float) * n, h->stream);
     cudaMemsetAsync(d.hist, 0, sizeof(float4) * n, h->stream);
     cudaMemsetAsync(d.hist_s, 0, sizeof(float4) * n, h->stream);
+    for (float4* c4 : {d.cA, d.cB, d.cC, d.cA_s, d.cB_s, d.cC_s, d.ap}) cudaMemsetAsync(c4, 0, sizeof(float4) * n, h->stream);
     // CUB scan scratch
     cub::DeviceScan::ExclusiveSum(nullptr, h->cub_bytes, d.cell_count, d.cell_start, h->g.nkeys + 1, h->stream);
     if (cudaMalloc(&h->cub_tmp, h->cub_bytes + 16) != cudaSuccess) return SPHGPU_ENOMEM;
@@ -285,6 +290,7 @@ void free_scene(sphgpu_scene* h) {
     DevScene& d = h->d;
     void* ptrs[] = {d.pos, d.vel, d.gid, d.rho, d.alpha, d.vadv, d.pv, d.pk, d.bpv, d.kappav, d.acc, d.kr, d.kappa, d.ksum, d.aux0,
                     d.aux1, d.aux4, d.kwarm, d.hist, d.wsbuf, d.pos_s, d.vel_s, d.gid_s, d.hist_s, d.key, d.slot, d.tmp,
+                    d.cA, d.cB, d.cC, d.cA_s, d.cB_s, d.cC_s, d.ap, d.pl2,
                     h->recX, h->recY,
                     d.cell_count, d.cell_start, d.bcell_start, d.cstart2, d.nbr, d.ncount, d.partial, d.st,
                     d.bpos, d.bvel, d.bgid, h->cub_tmp};
@@ -298,7 +304,7 @@ void free_scene(sphgpu_scene* h) {
 
 // ---------------- step building blocks ----------------
 
-void enq_ns(sphgpu_scene* h, int integrate, int build_mode, cudaStream_t st) {
+void enq_ns(sphgpu_scene* h, int integrate, int build_mode, cudaStream_t st, int carry = 1) {
     DevScene& d = h->d;
     cudaMemsetAsync(d.cell_count, 0, sizeof(int) * ((size_t)h->g.nkeys + 1), st);
     launch(h, "hash", st, [&] { launch_hash(d, h->g, h->P.spaceMin, h->P.spaceMax, integrate, h->cap, st); });
@@ -306,7 +312,7 @@ void enq_ns(sphgpu_scene* h, int integrate, int build_mode, cudaStream_t st) {
         size_t b = h->cub_bytes;
         cub::DeviceScan::ExclusiveSum(h->cub_tmp, b, d.cell_count, d.cell_start, h->g.nkeys + 1, st);
     });
-    launch(h, "reorder", st, [&] { launch_scatter_reorder(d, h->g, h->cap, 1, st); });
+    launch(h, "reorder", st, [&] { launch_scatter_reorder(d, h->g, h->cap, carry, st); });
     launch_count_active(d, h->g, st);
     launch(h, build_mode == 1 ? "build_first" : (build_mode == 2 ? "build_pressure" : "build"), st,
            [&] { launch_build(d, h->g, h->c, build_mode, h->cap, st); });
@@ -413,16 +419,106 @@ int enq_df_step(sphgpu_scene* h, bool capturing) {
     return 0;
 }
 
-int run_initial_ns(sphgpu_scene* h, int build_mode) {
-    if (!h->in_staging) {
-        // state is in the sorted arrays: stage it (copy) so the sort sees it
-        int n = h->h_stats->n_active;
-        cudaMemcpyAsync(h->d.pos_s, h->d.pos, sizeof(float4) * n, cudaMemcpyDeviceToDevice, h->stream);
-        cudaMemcpyAsync(h->d.vel_s, h->d.vel, sizeof(float4) * n, cudaMemcpyDeviceToDevice, h->stream);
-        cudaMemcpyAsync(h->d.gid_s, h->d.gid, sizeof(int) * n, cudaMemcpyDeviceToDevice, h->stream);
-        cudaMemcpyAsync(h->d.hist_s, h->d.hist, sizeof(float4) * n, cudaMemcpyDeviceToDevice, h->stream);
+// The sorted arrays hold the state: copy it, with the carried per-particle
+// state, into the staging arrays the next sort reads.
+void stage_from_sorted(sphgpu_scene* h, int n) {
+    DevScene& d = h->d;
+    cudaStream_t st = h->stream;
+    cudaMemcpyAsync(d.pos_s, d.pos, sizeof(float4) * n, cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(d.vel_s, d.vel, sizeof(float4) * n, cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(d.gid_s, d.gid, sizeof(int) * n, cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(d.hist_s, d.hist, sizeof(float4) * n, cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(d.cA_s, d.cA, sizeof(float4) * n, cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(d.cB_s, d.cB, sizeof(float4) * n, cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(d.cC_s, d.cC, sizeof(float4) * n, cudaMemcpyDeviceToDevice, st);
+}
+
+// PciSph::pci_updateDelta (PciSph.cpp:133-162), in float as the reference
+// evaluates it: delta of a prototype particle with a full neighbourhood on
+// the lattice of spacing spacing_r, divided by dt^2.
+float pci_delta(const SphParams& P, const KerConst& k) {
+    const float sp = P.spacing_r, hs = P.smoothRadius_h, dt = P.dt;
+    const int n = (int)std::ceil(hs / sp);
+    float gs[3] = {0.f, 0.f, 0.f}, g2 = 0.f;
+    auto wg = [&](float r) {
+        float q = r / k.h, qm2 = 2 - q;
+        return q <= 1 ? k.thetah * (3 * q - 2.25f * q * q) : k.thetah * 0.75f * qm2 * qm2;
+    };
+    for (int z = -n; z <= n; ++z)
+        for (int y = -n; y <= n; ++y)
+            for (int x = -n; x <= n; ++x) {
+                if (!x && !y && !z) continue;
+                const float vf[3] = {(float)x * sp, (float)y * sp, (float)z * sp};
+                const float dis = std::sqrt(vf[0] * vf[0] + vf[1] * vf[1] + vf[2] * vf[2]);
+                if (dis < hs) {
+                    const float grad = -wg(dis);
+                    for (int c = 0; c < 3; ++c) gs[c] += vf[c] * (grad / dis);
+                    g2 += grad * grad;
+                }
+            }
+    const float v0 = (float)std::pow((double)sp, 3);
+    const float beta = 2 * v0 * v0;
+    const float delta = -1 / (beta * (-(gs[0] * gs[0] + gs[1] * gs[1] + gs[2] * gs[2]) - g2));
+    return delta / (dt * dt);
+}
+
+// One PCISPH step (PciSph::sphStep, PciSph.cpp:31-94): the state enters and
+// leaves in the staging arrays, like WCSPH.
+int enq_pci_step(sphgpu_scene* h, bool capturing) {
+    DevScene& d = h->d;
+    cudaStream_t st = h->stream;
+    const SphParams& P = h->P;
+    launch_step_begin(d, st);
+    enq_ns(h, 0, 0, st, 4);
+    const float delta = pci_delta(P, h->c.k);
+    launch(h, "pci_force_except", st, [&] { launch_pci_force_except(d, h->c, h->cap, st); });
+    launch_df_loop_reset(d, 0, st);
+    int r = enq_loop(h, capturing, [&](cudaStream_t s2, unsigned long long hd, int use) {
+        launch(h, "pci_density", s2, [&] { launch_pci_density(d, h->c, delta, h->cap, s2); });
+        launch(h, "pci_pressure", s2, [&] {
+            launch_pci_pressure(d, h->c, P.densityErro_eta, P.pci_min_iter, P.pci_max_iter, hd, use, h->cap, s2);
+        });
+    });
+    if (r) return r;
+    launch(h, "pci_finish", st, [&] { launch_pci_finish(d, h->cap, st); });
+    CK(cudaMemcpyAsync(h->h_stats, d.st, sizeof(DevStats), cudaMemcpyDeviceToHost, st));
+    return 0;
+}
+
+// One IISPH_M step (IISph_M::sphStep, IISph_M.cpp:10-75): phases solved in
+// turn, each with its own Jacobi loop.
+int enq_ii_step(sphgpu_scene* h, bool capturing) {
+    DevScene& d = h->d;
+    cudaStream_t st = h->stream;
+    const SphParams& P = h->P;
+    launch_step_begin(d, st);
+    enq_ns(h, 0, 0, st, 2 | 4 | 8);
+    launch(h, "ii_force_except", st, [&] { launch_ii_force_except(d, h->c, h->cap, st); });
+    const int nph = (int)h->rho0_ph.size();
+    for (int ph = 0; ph < nph; ++ph) {
+        launch_ii_phase_begin(d, st);
+        launch(h, "ii_density", st, [&] { launch_ii_density(d, h->c, ph, h->cap, st); });
+        launch(h, "ii_aii", st, [&] { launch_ii_aii(d, h->c, ph, h->cap, st); });
+        int r = enq_loop(h, capturing, [&](cudaStream_t s2, unsigned long long hd, int use) {
+            launch(h, "ii_sum", s2, [&] { launch_ii_sum(d, h->c, ph, h->cap, s2); });
+            launch(h, "ii_press", s2, [&] {
+                launch_ii_press(d, h->c, ph, (double)P.ii_omega, (double)P.ii_eta_rel, P.ii_min_iter, P.ii_max_iter,
+                                P.ii_compat, hd, use, h->cap, s2);
+            });
+        });
+        if (r) return r;
     }
-    enq_ns(h, 0, build_mode, h->stream);
+    launch(h, "ii_force", st, [&] { launch_ii_force(d, h->c, P.ii_compat, h->cap, st); });
+    CK(cudaMemcpyAsync(h->h_stats, d.st, sizeof(DevStats), cudaMemcpyDeviceToHost, st));
+    return 0;
+}
+
+int pci_graph_build(sphgpu_scene* h, bool cap) { return enq_pci_step(h, cap); }
+int ii_graph_build(sphgpu_scene* h, bool cap) { return enq_ii_step(h, cap); }
+
+int run_initial_ns(sphgpu_scene* h, int build_mode) {
+    if (!h->in_staging) stage_from_sorted(h, h->h_stats->n_active);  // the sort reads staging
+    enq_ns(h, 0, build_mode, h->stream, 1 | 2 | 4 | 8);
     h->in_staging = false;
     h->ns_valid = build_mode == 1;
     CK(cudaMemcpyAsync(h->h_stats, h->d.st, sizeof(DevStats), cudaMemcpyDeviceToHost, h->stream));
@@ -492,9 +588,9 @@ void fill_stats(sphgpu_scene* h, SphStepStats* o, int steps) {
 }
 
 int enq_steps(sphgpu_scene* h, int solver, int nsteps) {
-    if (solver != SPHGPU_DFSPH && solver != SPHGPU_WCSPH) {
-        h->err = "solver not available in this build";
-        return SPHGPU_ENOTIMPL;
+    if (solver != SPHGPU_DFSPH && solver != SPHGPU_WCSPH && solver != SPHGPU_PCISPH && solver != SPHGPU_IISPH_M) {
+        h->err = "unknown solver";
+        return SPHGPU_EINVAL;
     }
     if (h->h_stats->n_active <= 0 && h->n_total <= 0) {
         h->err = "no fluid particles";
@@ -505,6 +601,33 @@ int enq_steps(sphgpu_scene* h, int solver, int nsteps) {
         return SPHGPU_ENOTIMPL;
     }
     launch_call_begin(h->d, h->stream);
+    if (solver == SPHGPU_PCISPH || solver == SPHGPU_IISPH_M) {
+        if (h->last_solver != solver && h->last_solver >= 0) {
+            // entering from another solver: the carried state starts as the
+            // reference's fresh particles (the last density, zeros)
+            launch_carry_init(h->d, h->c, h->in_staging ? 1 : 0, h->cap, h->stream);
+        }
+        if (!h->in_staging) stage_from_sorted(h, h->cap);
+        h->last_solver = solver;
+        for (int s = 0; s < nsteps; ++s) {
+            if (h->use_graphs && !h->prof.on) {
+                cudaGraphExec_t ex;
+                const int key = solver == SPHGPU_PCISPH ? 100 : 200;
+                int r = graph_for(h, key, &ex, solver == SPHGPU_PCISPH ? pci_graph_build : ii_graph_build);
+                if (r) return r;
+                CK(cudaGraphLaunch(ex, h->stream));
+            } else {
+                int r = solver == SPHGPU_PCISPH ? enq_pci_step(h, false) : enq_ii_step(h, false);
+                if (r) return r;
+                prof_collect(h);
+            }
+            h->frame++;
+        }
+        h->in_staging = true;
+        h->ns_valid = false;
+        return 0;
+    }
+    h->last_solver = solver;
     if (solver == SPHGPU_DFSPH) {
         if (!h->ns_valid) {
             int r = run_initial_ns(h, 1);
@@ -528,12 +651,7 @@ int enq_steps(sphgpu_scene* h, int solver, int nsteps) {
     }
     // WCSPH: NS + density/pressure (fused), forces + integrate into staging
     for (int s = 0; s < nsteps; ++s) {
-        if (!h->in_staging) {
-            int n = h->cap;
-            cudaMemcpyAsync(h->d.pos_s, h->d.pos, sizeof(float4) * n, cudaMemcpyDeviceToDevice, h->stream);
-            cudaMemcpyAsync(h->d.vel_s, h->d.vel, sizeof(float4) * n, cudaMemcpyDeviceToDevice, h->stream);
-            cudaMemcpyAsync(h->d.gid_s, h->d.gid, sizeof(int) * n, cudaMemcpyDeviceToDevice, h->stream);
-        }
+        if (!h->in_staging) stage_from_sorted(h, h->cap);
         launch_step_begin(h->d, h->stream);
         enq_ns(h, 0, 2, h->stream);
         launch(h, "wc_force", h->stream, [&] { launch_wc_force(h->d, h->c, h->cap, h->stream); });
@@ -754,6 +872,8 @@ int sphgpu_add_fluid(sphgpu_t h, int n, const float* xyz, const float* vel, floa
     int phase = (int)h->rho0_ph.size();
     // bring the existing particles into staging in reference order
     std::vector<float4> P(cur + n), V(cur + n);
+    std::vector<float4> carried[3];
+    for (auto& c4 : carried) c4.assign(cur + n, make_float4(0.f, 0.f, 0.f, 0.f));
     if (cur > 0) {
         std::vector<int> gid;
         int m;
@@ -764,16 +884,30 @@ int sphgpu_add_fluid(sphgpu_t h, int n, const float* xyz, const float* vel, floa
         std::vector<int> order;
         ref_order(gid, order);
         for (int k = 0; k < m; ++k) { P[k] = tp[order[k]]; V[k] = tv[order[k]]; }
+        // carried PCISPH / IISPH_M state follows its particles
+        const float4* srcs[3] = {h->in_staging ? h->d.cA_s : h->d.cA, h->in_staging ? h->d.cB_s : h->d.cB,
+                                 h->in_staging ? h->d.cC_s : h->d.cC};
+        for (int a = 0; a < 3; ++a) {
+            std::vector<float4> t(m);
+            CK(cudaMemcpy(t.data(), srcs[a], sizeof(float4) * m, cudaMemcpyDeviceToHost));
+            for (int k = 0; k < m; ++k) carried[a][k] = t[order[k]];
+        }
     }
     for (int i = 0; i < n; ++i) {
         P[cur + i] = make_float4(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], int_bits_as_float(phase));
         V[cur + i] = vel ? make_float4(vel[3 * i], vel[3 * i + 1], vel[3 * i + 2], 0.f) : make_float4(0, 0, 0, 0);
+        // a new particle's density is its rest density (as the reference's
+        // scene setup leaves it before the first step)
+        carried[1][cur + i] = make_float4(0.f, 0.f, 0.f, rho0);
     }
     std::vector<int> G(cur + n);
     std::iota(G.begin(), G.end(), 0);
     CK(cudaMemcpy(h->d.pos_s, P.data(), sizeof(float4) * (cur + n), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(h->d.vel_s, V.data(), sizeof(float4) * (cur + n), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(h->d.gid_s, G.data(), sizeof(int) * (cur + n), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->d.cA_s, carried[0].data(), sizeof(float4) * (cur + n), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->d.cB_s, carried[1].data(), sizeof(float4) * (cur + n), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->d.cC_s, carried[2].data(), sizeof(float4) * (cur + n), cudaMemcpyHostToDevice));
     h->h_stats->n_active = cur + n;
     CK(cudaMemcpy(&h->d.st->n_active, &h->h_stats->n_active, sizeof(int), cudaMemcpyHostToDevice));
     h->rho0_ph.push_back(rho0);
@@ -870,7 +1004,19 @@ int sphgpu_get_fluid(sphgpu_t h, const char* field, float* out) {
         f4 = true;
         comps = 3;
     }
-    else if (f == "acce_adv" || f == "acceleration") { src = d.acc; f4 = true; comps = 3; }
+    else if (f == "acce_adv" || f == "acceleration" || f == "acce_presure") { src = d.acc; f4 = true; comps = 3; }
+    else if (f == "acce_pressure") { src = d.ap; f4 = true; comps = 3; }
+    else if (f == "pos_prediction") { src = d.aux4; f4 = true; comps = 3; }
+    else if (f == "dii") { src = d.cB; f4 = true; comps = 3; }
+    else if (f == "sum_dijpj") { src = d.cC; f4 = true; comps = 3; }
+    else if (f == "ii_vel_adv") { src = d.cA; f4 = true; comps = 3; }
+    else if (f == "aii" || f == "p_l") {
+        std::vector<float4> t(n);
+        CK(cudaMemcpy(t.data(), f == "aii" ? d.cC : d.cA, sizeof(float4) * n, cudaMemcpyDeviceToHost));
+        for (int k = 0; k < n; ++k) out[k] = t[order[k]].w;
+        return n;
+    }
+    else if (f == "rho_adv") src = d.aux1;
     else if (f == "density") src = d.rho;
     else if (f == "DFalpha") src = d.alpha;
     else if (f == "DFkappa") src = d.kappa;
@@ -929,10 +1075,7 @@ int sphgpu_set_fluid(sphgpu_t h, const char* field, const float* in) {
             // the sorted arrays are the state: stage them so the next search
             // rebuilds lists, rho/alpha and the packed sweep records
             h->ns_valid = false;
-            CK(cudaMemcpyAsync(d.pos_s, d.pos, sizeof(float4) * n, cudaMemcpyDeviceToDevice, h->stream));
-            CK(cudaMemcpyAsync(d.vel_s, d.vel, sizeof(float4) * n, cudaMemcpyDeviceToDevice, h->stream));
-            CK(cudaMemcpyAsync(d.gid_s, d.gid, sizeof(int) * n, cudaMemcpyDeviceToDevice, h->stream));
-            CK(cudaMemcpyAsync(d.hist_s, d.hist, sizeof(float4) * n, cudaMemcpyDeviceToDevice, h->stream));
+            stage_from_sorted(h, n);
             h->in_staging = true;
         }
         CK(cudaStreamSynchronize(h->stream));
@@ -953,13 +1096,26 @@ int sphgpu_set_fluid(sphgpu_t h, const char* field, const float* in) {
             // positions changed: lists and rho/alpha must be rebuilt
             h->ns_valid = false;
             // the sorted arrays are the state; stage them for the next sort
-            CK(cudaMemcpy(d.pos_s, d.pos, sizeof(float4) * n, cudaMemcpyDeviceToDevice));
-            CK(cudaMemcpy(d.vel_s, d.vel, sizeof(float4) * n, cudaMemcpyDeviceToDevice));
-            CK(cudaMemcpy(d.gid_s, d.gid, sizeof(int) * n, cudaMemcpyDeviceToDevice));
-            CK(cudaMemcpy(d.hist_s, d.hist, sizeof(float4) * n, cudaMemcpyDeviceToDevice));
+            stage_from_sorted(h, n);
+            CK(cudaStreamSynchronize(h->stream));
             h->in_staging = true;
         }
         return n;
+    }
+    if (f == "density") {
+        // the density the PCISPH / IISPH_M non-pressure forces read is the
+        // carried one (previous step): keep it in step with rho
+        bool stg = h->in_staging;
+        std::vector<int> g2;
+        int n2;
+        if (download_gid(h, g2, n2, stg)) return SPHGPU_ECUDA;
+        std::vector<int> o2;
+        ref_order(g2, o2);
+        float4* cb = stg ? d.cB_s : d.cB;
+        std::vector<float4> t(n2);
+        CK(cudaMemcpy(t.data(), cb, sizeof(float4) * n2, cudaMemcpyDeviceToHost));
+        for (int k = 0; k < n2; ++k) t[o2[k]].w = in[k];
+        CK(cudaMemcpy(cb, t.data(), sizeof(float4) * n2, cudaMemcpyHostToDevice));
     }
     float* dst = nullptr;
     if (f == "density") dst = d.rho;

@@ -78,7 +78,7 @@ __global__ void __launch_bounds__(NT) k_scatter(DevScene s) {
 
 // For sorted slot q: its particle i, its cell range [a, b); its final place is
 // a + #{particles of the cell with larger global index}.
-__global__ void __launch_bounds__(NT) k_rank_reorder(DevScene s, int dead_key, int carry_hist) {
+__global__ void __launch_bounds__(NT) k_rank_reorder(DevScene s, int dead_key, int carry) {
     const int n = s.st->pad0;
     int q = blockIdx.x * NT + threadIdx.x;
     if (q >= n) return;
@@ -96,7 +96,10 @@ __global__ void __launch_bounds__(NT) k_rank_reorder(DevScene s, int dead_key, i
     s.pv[2 * p + 1] = v;
     s.pk[p] = make_float4(x.x, x.y, x.z, 0.f);
     s.gid[p] = my;
-    if (carry_hist) s.hist[p] = s.hist_s[i];
+    if (carry & 1) s.hist[p] = s.hist_s[i];
+    if (carry & 2) s.cA[p] = s.cA_s[i];
+    if (carry & 4) s.cB[p] = s.cB_s[i];
+    if (carry & 8) s.cC[p] = s.cC_s[i];
 }
 
 __global__ void k_count_active(DevScene s, int dead_key) {
@@ -306,10 +309,10 @@ void launch_hash(const DevScene& s, const GridGeom& g, const float* smin, const 
                                                           make_float3(smax[0], smax[1], smax[2]), integrate);
 }
 
-void launch_scatter_reorder(const DevScene& s, const GridGeom& g, int n_old, int carry_hist, cudaStream_t st) {
+void launch_scatter_reorder(const DevScene& s, const GridGeom& g, int n_old, int carry, cudaStream_t st) {
     int nb = nblk(n_old > 0 ? n_old : 1, NT);
     k_scatter<<<nb, NT, 0, st>>>(s);
-    k_rank_reorder<<<nb, NT, 0, st>>>(s, g.nkeys - 1, carry_hist);
+    k_rank_reorder<<<nb, NT, 0, st>>>(s, g.nkeys - 1, carry);
 }
 
 void launch_count_active(const DevScene& s, const GridGeom& g, cudaStream_t st) {

@@ -24,6 +24,13 @@ struct DevStats {
     unsigned ticket[4];    // last-block tickets of the reductions
     int pad2;              // warm-start recording: sampling offset
     int pad3;
+    // PCISPH / IISPH_M loop state
+    int pci_emax_bits;     // max relative density error of the iteration (float bits)
+    int ii_iter;           // iterations of the current phase's pressure loop
+    int ii_num;            // particles of the current phase
+    int pad4;
+    double ii_sum_cum;     // running sums of the reference's bookkeeping
+    double ii_nb_cum;
 };
 
 // Per-scene device pointers passed to every kernel by value.
@@ -44,9 +51,9 @@ struct DevScene {
     float* kappa;       // DFkappa of the last density iteration
     float* kappav;      // DFkappaV of the last divergence iteration
     float* ksum;        // summed kappa over the density loop (warm-start label)
-    float* aux0;        // rho_adv (DFSPH density loop), aii (IISPH)
-    float* aux1;        // divergence deviation (DFSPH), IISPH rho_adv, PCISPH rho*
-    float4* aux4;       // IISPH d_ii / sum d_ij p_j, PCISPH predicted position
+    float* aux0;        // rho_adv (DFSPH density loop)
+    float* aux1;        // divergence deviation (DFSPH), rho_adv (IISPH_M)
+    float4* aux4;       // PCISPH predicted position; scratch for transfers
     float* kwarm;       // predicted initial kappa (learned warm start), 0 otherwise
     float4* hist;       // warm-start history: (khat, predicted error, divergence term) of the last step
     float2* wsbuf;      // this step's (predicted error, divergence term)
@@ -55,6 +62,16 @@ struct DevScene {
     float4* vel_s;
     int* gid_s;
     float4* hist_s;
+    // PCISPH / IISPH_M: carried per-particle state (sorted and staging) and
+    // loop scratch
+    float4* cA;         // IISPH_M: (v_adv, p_l)
+    float4* cB;         // (d_ii, rho); PCISPH: w = rho of the previous step
+    float4* cC;         // IISPH_M: (sum_j d_ij p_j, a_ii)
+    float4* cA_s;
+    float4* cB_s;
+    float4* cC_s;
+    float4* ap;         // PCISPH pressure acceleration
+    float* pl2;         // IISPH_M previous Jacobi iterate
     int* key;
     int* slot;
     int* tmp;
@@ -80,7 +97,8 @@ struct DevScene {
 // ---- neighbour search (sph_grid.cu) ----
 void launch_hash(const DevScene& s, const GridGeom& g, const float* smin, const float* smax, int integrate,
                  int n_old, cudaStream_t st);
-void launch_scatter_reorder(const DevScene& s, const GridGeom& g, int n_old, int carry_kwarm, cudaStream_t st);
+// carry: bit 0 hist, bit 1 cA, bit 2 cB, bit 3 cC (staging -> sorted)
+void launch_scatter_reorder(const DevScene& s, const GridGeom& g, int n_old, int carry, cudaStream_t st);
 void launch_count_active(const DevScene& s, const GridGeom& g, cudaStream_t st);
 // mode 0: lists only; 1: lists + DFSPH rho/alpha; 2: lists + WCSPH rho/pressure
 void launch_build(const DevScene& s, const GridGeom& g, const SolverConst& c, int mode, int n_max, cudaStream_t st);
@@ -107,3 +125,22 @@ void launch_call_begin(const DevScene& s, cudaStream_t st);
 
 // ---- WCSPH (sph_wcsph.cu) ----
 void launch_wc_force(const DevScene& s, const SolverConst& c, int n_max, cudaStream_t st);
+
+// ---- PCISPH / IISPH_M (sph_pci_ii.cu) ----
+void launch_pci_force_except(const DevScene& s, const SolverConst& c, int n_max, cudaStream_t st);
+void launch_pci_density(const DevScene& s, const SolverConst& c, float delta, int n_max, cudaStream_t st);
+void launch_pci_pressure(const DevScene& s, const SolverConst& c, float eta, int min_it, int max_it,
+                         unsigned long long cond_handle, int use_handle, int n_max, cudaStream_t st);
+void launch_pci_finish(const DevScene& s, int n_max, cudaStream_t st);
+void launch_ii_force_except(const DevScene& s, const SolverConst& c, int n_max, cudaStream_t st);
+void launch_ii_phase_begin(const DevScene& s, cudaStream_t st);
+void launch_ii_density(const DevScene& s, const SolverConst& c, int phase, int n_max, cudaStream_t st);
+void launch_ii_aii(const DevScene& s, const SolverConst& c, int phase, int n_max, cudaStream_t st);
+void launch_ii_sum(const DevScene& s, const SolverConst& c, int phase, int n_max, cudaStream_t st);
+void launch_ii_press(const DevScene& s, const SolverConst& c, int phase, double omega, double eta_rel, int min_it,
+                     int max_it, int compat, unsigned long long cond_handle, int use_handle, int n_max,
+                     cudaStream_t st);
+void launch_ii_force(const DevScene& s, const SolverConst& c, int compat, int n_max, cudaStream_t st);
+// carried state of particles coming from another solver: cB = (0, rho), cA = cC = 0
+// (staging: rho = the phase's rest density)
+void launch_carry_init(const DevScene& s, const SolverConst& c, int staging, int n_max, cudaStream_t st);

@@ -25,7 +25,8 @@ from ._lib import SphParams, SphStepStats, SphGpuError
 
 SOLVERS = {"wcsph": _lib.WCSPH, "pcisph": _lib.PCISPH, "iisph_m": _lib.IISPH_M, "dfsph": _lib.DFSPH}
 
-VEC_FIELDS = ("position", "velocity", "vel_adv", "acce_adv", "acceleration", "ws_hist")
+VEC_FIELDS = ("position", "velocity", "vel_adv", "acce_adv", "acceleration", "ws_hist", "acce_pressure",
+              "pos_prediction", "dii", "sum_dijpj", "ii_vel_adv", "acce_presure")
 
 
 def _fptr(a):
@@ -465,13 +466,38 @@ class WcSph(SphBase):
 
 
 class PciSph(SphBase):
-    """PCISPH (PciSph.h, PciSph.cpp)."""
+    """PCISPH (PciSph.h, PciSph.cpp): predict-correct loop on the maximum
+    density error, m_TH.densityErro_eta, between m_minIterations and
+    m_maxIterations iterations (PciSph.h:35)."""
     SOLVER = "pcisph"
+
+    def __init__(self, device=0):
+        super().__init__(device)
+        self.m_minIterations = 3
+        self.m_maxIterations = 10
+
+    def _params(self):
+        p = super()._params()
+        p.pci_min_iter = int(self.m_minIterations)
+        p.pci_max_iter = int(self.m_maxIterations)
+        return p
 
 
 class IISph_M(SphBase):
-    """IISPH, multiphase (IISph_M.h, IISph_M.cpp)."""
+    """IISPH, multiphase (IISph_M.h, IISph_M.cpp): relaxed Jacobi (omega 0.5)
+    per phase to the average density error 0.001 rho0 (IISph_M.cpp:285).
+    `ii_compat` selects the reference's loop bookkeeping / integration
+    (see SphParams.ii_compat in include/sphgpu.h)."""
     SOLVER = "iisph_m"
+
+    def __init__(self, device=0, ii_compat=0):
+        super().__init__(device)
+        self.ii_compat = ii_compat
+
+    def _params(self):
+        p = super()._params()
+        p.ii_compat = int(self.ii_compat)
+        return p
 
 
 class DFSPH(SphBase):

@@ -96,7 +96,16 @@ typedef struct SphParams {
      * only pushes particles apart (rho_adv >= rho0 clamp, DFSPH.cpp:620-623),
      * so an over-prediction cannot be undone and is kept below 1 */
     float ws_scale;
-    int reserved[6];
+    /* IISPH_M reproductions of the reference's loop bookkeeping (0 = the
+     * method as published; bits may be combined):
+     *   1  running error sums never reset between iterations, and the
+     *      two-iteration minimum counted in particle updates
+     *      (IISph_M.cpp:283-284, 350)
+     *   2  velocity update v += a_p dt without the advection acceleration,
+     *      as updateFluids built with -DIISPH does (SphBase.cpp:387-389);
+     *      otherwise v = v_adv + a_p dt */
+    int ii_compat;
+    int reserved[5];
 } SphParams;
 
 /* Per-step statistics (replaces m_EC and the CALL_TIME log rows). */

@@ -40,7 +40,8 @@ class OrcParams(C.Structure):
         ("cfl", C.c_int), ("cfl_factor", C.c_double), ("dt_max", C.c_double), ("dt_min", C.c_double),
         ("wc_gamma", C.c_double),
         ("pci_eta", C.c_double), ("pci_min_iter", C.c_int), ("pci_max_iter", C.c_int),
-        ("ii_omega", C.c_double), ("ii_eta_rel", C.c_double), ("ii_min_iter", C.c_int), ("ii_max_iter", C.c_int)]
+        ("ii_omega", C.c_double), ("ii_eta_rel", C.c_double), ("ii_min_iter", C.c_int), ("ii_max_iter", C.c_int),
+        ("ii_compat", C.c_int)]
 
 
 def build():
@@ -60,7 +61,7 @@ def default_params(scene=None, **kw):
              df_div_goal_abs=2.5, df_div_goal_rel=1e-3, df_div_min_iter=1, df_div_max_iter=30,
              cfl=0, cfl_factor=0.4, dt_max=5e-3, dt_min=1e-6, wc_gamma=7.0,
              pci_eta=0.01, pci_min_iter=3, pci_max_iter=10,
-             ii_omega=0.5, ii_eta_rel=1e-3, ii_min_iter=2, ii_max_iter=100)
+             ii_omega=0.5, ii_eta_rel=1e-3, ii_min_iter=2, ii_max_iter=100, ii_compat=0)
     if scene is not None:
         p.update(spacing_r=scene.spacing_r, smoothRadius_h=scene.smooth_radius,
                  spaceMin=scene.space_min, spaceMax=scene.space_max)
@@ -103,6 +104,9 @@ class Oracle:
             self._ps = _fill(RefParams, self.p)
             self.h = self.lib.ref_create(C.byref(self._ps), LOG_DIR.encode())
             self.cap = 48
+            if self.h and solver == "pcisph":
+                self.lib.ref_set_iter_limits(self.h, int(self.p.get("pci_min_iter", 3)),
+                                             int(self.p.get("pci_max_iter", 10)))
         if not self.h:
             raise RuntimeError("oracle creation failed")
         self.nfluid_phases = 0
@@ -149,10 +153,16 @@ class Oracle:
             lib.orc_stats.argtypes = [vp, ip, dp, dp, ip]
             lib.orc_set_solid.argtypes = [vp, i, cp, dp]
             lib.orc_set_solid.restype = i
+            lib.orc_pci_delta.argtypes = [vp]
+            lib.orc_pci_delta.restype = d
         else:
             lib.ref_error_counts.argtypes = [vp, ip, ip]
             lib.ref_frame.restype = i
             lib.ref_frame.argtypes = [vp]
+            lib.ref_set_iter_limits.restype = i
+            lib.ref_set_iter_limits.argtypes = [vp, i, i]
+            lib.ref_set_threads.restype = None
+            lib.ref_set_threads.argtypes = [i]
         cls._libs[name] = lib
         return lib
 
@@ -275,6 +285,14 @@ class Oracle:
 
     def threads(self):
         return self._f("threads")()
+
+    def pci_delta(self):
+        """PCISPH delta / dt^2 of the last pci_updateDelta (port only)."""
+        return float(self.lib.orc_pci_delta(self.h))
+
+    def set_threads(self, n):
+        """OpenMP threads of the compiled reference (process-wide)."""
+        self.lib.ref_set_threads(int(n))
 
 
 def make_scene_oracle(scene, kind="port", solver="dfsph", f64=False, visc_alpha=0.0, solid_visc=0.0, **kw):

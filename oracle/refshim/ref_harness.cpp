@@ -53,6 +53,11 @@ public:
         m_TH.spaceMax = vec_t(real_t(p.spaceMax[0]), real_t(p.spaceMax[1]), real_t(p.spaceMax[2]));
         m_TH.enable_vortex = 0;
         ker_update_numbers();
+#ifdef REF_TAG_pcisph
+        /* PciSph() leaves the pci_updateDelta cache keys uninitialised
+         * (PciSph.h:35,63); start from values that force the computation. */
+        pci_last_dt = pci_last_sp = pci_last_h = real_t(-1);
+#endif
     }
 
     int stage(const std::string& s) {
@@ -256,6 +261,19 @@ public:
     static void ref_set_dt_impl(void* hh, double dt) { static_cast<RefHarness*>(hh)->m_TH.dt = real_t(dt); }
     static int ref_frame_impl(void* hh) { return static_cast<RefHarness*>(hh)->m_TH.frameNumber; }
     static void ref_set_frame_impl(void* hh, int f) { static_cast<RefHarness*>(hh)->m_TH.frameNumber = f; }
+    /* PCISPH loop bounds m_minIterations / m_maxIterations (PciSph.h:35);
+     * returns -1 for the other solvers */
+    static int ref_set_iter_limits_impl(void* hh, int mn, int mx) {
+#ifdef REF_TAG_pcisph
+        RefHarness* h = static_cast<RefHarness*>(hh);
+        h->m_minIterations = mn;
+        h->m_maxIterations = mx;
+        return 0;
+#else
+        (void)hh; (void)mn; (void)mx;
+        return -1;
+#endif
+    }
     static double ref_kernel_impl(void* hh, int grad, double r) {
         RefHarness* h = static_cast<RefHarness*>(hh);
         return grad ? double(h->ker_W_grad(real_t(r))) : double(h->ker_W(real_t(r)));
@@ -289,4 +307,9 @@ void ref_set_dt(void* hh, double dt) { RefHarness::ref_set_dt_impl(hh, dt); }
 int ref_frame(void* hh) { return RefHarness::ref_frame_impl(hh); }
 void ref_set_frame(void* hh, int f) { RefHarness::ref_set_frame_impl(hh, f); }
 double ref_kernel(void* hh, int grad, double r) { return RefHarness::ref_kernel_impl(hh, grad, r); }
+int ref_set_iter_limits(void* hh, int mn, int mx) { return RefHarness::ref_set_iter_limits_impl(hh, mn, mx); }
+/* SphBase::SphBase sets the OpenMP thread count to omp_get_num_procs()
+ * (SphBase.cpp:242-243); this overrides it (1 thread makes the racy loops of
+ * IISph_M.cpp:315-351 deterministic) */
+void ref_set_threads(int n) { omp_set_num_threads(n); }
 }  // extern "C"

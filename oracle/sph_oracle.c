@@ -78,6 +78,7 @@ typedef struct OrcParams {
     double wc_gamma;      /* Tait exponent, reference 7 (WcSph.h:34) */
     double pci_eta; int pci_min_iter, pci_max_iter; /* PciSph.h:35 */
     double ii_omega, ii_eta_rel; int ii_min_iter, ii_max_iter;
+    int ii_compat;        /* IISPH_M reference-compatibility bits (sph_oracle_pci_ii.inc) */
 } OrcParams;
 
 typedef struct { int t, i; } PIdx; /* PartIdx, SphBase.h:596-617 */
@@ -89,7 +90,7 @@ typedef struct {
     real *density, *DFalpha, *DFalpha2, *DFkappa, *DFkappaV, *density_adv, *divdev, *presure;
     /* PCISPH / IISPH */
     real *pos_pred, *acce_pressure, *dii, *sum_dijpj, *adv_vel, *acce_presure;
-    real *aii, *rho_adv, *p_l;
+    real *aii, *rho_adv, *p_l, *p_l2;
     int *nnum; PIdx *nidx; real *ndis; /* neighbour lists, cap entries each */
     PIdx *next;
 } OrcFluid;
@@ -121,7 +122,8 @@ typedef struct {
     /* last-step statistics */
     int it_density, it_div, it_pci, it_ii;
     double err_density, err_div, err_pci, err_ii;
-    double pci_delta;
+    real pci_delta, pci_last_dt, pci_last_sp, pci_last_h, pci_last_delta;
+    int pci_init;
 } OrcScene;
 
 /* ---------------- kernels, SphBase.h:808-889 ---------------- */
@@ -340,7 +342,7 @@ static void copy_fluid_particle(OrcFluid* F, int dst, int src) {
     CP3(pos) CP3(vel) CP3(vel_adv) CP3(acce_adv) CP3(acceleration) CP3(DFalpha1) CP3(n_surf)
     CP3(pos_pred) CP3(acce_pressure) CP3(dii) CP3(sum_dijpj) CP3(adv_vel) CP3(acce_presure)
     CP1(density) CP1(DFalpha) CP1(DFalpha2) CP1(DFkappa) CP1(DFkappaV) CP1(density_adv) CP1(divdev)
-    CP1(presure) CP1(aii) CP1(rho_adv) CP1(p_l)
+    CP1(presure) CP1(aii) CP1(rho_adv) CP1(p_l) CP1(p_l2)
 #undef CP3
 #undef CP1
 }
@@ -910,7 +912,7 @@ static void free_fluid(OrcFluid* F) {
     real* arrs[] = {F->pos, F->vel, F->vel_adv, F->acce_adv, F->acceleration, F->DFalpha1, F->n_surf,
                     F->density, F->DFalpha, F->DFalpha2, F->DFkappa, F->DFkappaV, F->density_adv, F->divdev,
                     F->presure, F->pos_pred, F->acce_pressure, F->dii, F->sum_dijpj, F->adv_vel,
-                    F->acce_presure, F->aii, F->rho_adv, F->p_l, F->ndis};
+                    F->acce_presure, F->aii, F->rho_adv, F->p_l, F->p_l2, F->ndis};
     for (size_t i = 0; i < sizeof(arrs) / sizeof(arrs[0]); ++i) free(arrs[i]);
     free(F->nnum); free(F->nidx); free(F->next);
 }
@@ -957,7 +959,7 @@ int orc_add_fluid(void* h, int n, const double* xyz, const double* vel, double d
     ALLOC3(F->adv_vel, n); ALLOC3(F->acce_presure, n);
     ALLOC1(F->density, n); ALLOC1(F->DFalpha, n); ALLOC1(F->DFalpha2, n); ALLOC1(F->DFkappa, n);
     ALLOC1(F->DFkappaV, n); ALLOC1(F->density_adv, n); ALLOC1(F->divdev, n); ALLOC1(F->presure, n);
-    ALLOC1(F->aii, n); ALLOC1(F->rho_adv, n); ALLOC1(F->p_l, n);
+    ALLOC1(F->aii, n); ALLOC1(F->rho_adv, n); ALLOC1(F->p_l, n); ALLOC1(F->p_l2, n);
     F->nnum = (int*)calloc((size_t)n + 1, sizeof(int));
     F->nidx = (PIdx*)calloc((size_t)n * s->P.cap + 1, sizeof(PIdx));
     F->ndis = (real*)calloc((size_t)n * s->P.cap + 1, sizeof(real));
@@ -1090,6 +1092,7 @@ void orc_stats(void* h, int* iters, double* errs, double* dt, int* frame) {
 }
 
 void orc_set_dt(void* h, double dt) { ((OrcScene*)h)->P.dt = dt; }
+double orc_pci_delta(void* h) { return (double)((OrcScene*)h)->pci_delta; }
 void orc_set_frame(void* h, int f) { ((OrcScene*)h)->frame = f; }
 
 double orc_kernel(void* h, int grad, double r) {

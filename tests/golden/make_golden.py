@@ -9,6 +9,17 @@ oracle/_ref/) on small seeded scenes and records its outputs:
   step_dfsph.npz    state after 3 DFSPH runOneStep() calls (reference
                     bookkeeping: float error sums, goals 1e-4 / 2.5)
   step_wcsph.npz    state after 3 WcSph runOneStep() calls
+  settled_column.npz  input state for the PCISPH / IISPH_M fixtures: a
+                    10 x 20 x 10 column after 300 DFSPH steps of the CPU
+                    restatement (a raw lattice next to the walls starts
+                    ~8 % over rest density in the corners; PCISPH and IISPH
+                    resolve that in one step and blow up, so they start
+                    from a settled state)
+  step_pcisph.npz   PciSph::sphStep x 3 from the settled column, two phases
+                    (rest densities 1000 below, 3000 above)
+  step_iisphm.npz   IISph_M::sphStep x 3 from the same state, run with one
+                    OpenMP thread (the reference's pressure loop races on
+                    p_l and on its error sums, IISph_M.cpp:320-350)
 Run in the build container (the reference tree must be present):
     python tests/golden/make_golden.py
 """
@@ -22,7 +33,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
-from graphics_b200.scene import small_dam_break  # noqa: E402
+from graphics_b200.scene import Scene, rayleigh_taylor, small_dam_break  # noqa: E402
 from oracle import make_scene_oracle  # noqa: E402
 
 SCENE = dict(n=(12, 12, 12), r=0.025, seed=7)
@@ -30,8 +41,44 @@ DF_KW = dict(float_err=1, df_density_max_iter=1000000, nu=1e-3, dt=1e-3)
 WC_KW = dict(dt=2.5e-4, soundSpeed_cs=18.708287, nu=0.0)
 
 
+COLUMN = dict(counts=(10, 20, 10), r=0.025, box=(0.5, 1.25, 0.5), seed=1)
+PCI_KW = dict(dt=1e-3, densityErro_eta=5e-3, pci_min_iter=3, pci_max_iter=50, soundSpeed_cs=20.0, nu=1e-3)
+II_KW = dict(dt=1e-3, nu=1e-3, soundSpeed_cs=20.0)
+MULTI_VISC = dict(visc_alpha=0.02, solid_visc=0.01)
+
+
 def scene():
     return small_dam_break(SCENE["n"], r=SCENE["r"], seed=SCENE["seed"])
+
+
+def column_scene(state=None, rho=(1000.0, 3000.0)):
+    """The column of settled_column.npz: walls of rayleigh_taylor(COLUMN),
+    fluid state from the fixture, phase 1 above the median height."""
+    sc = rayleigh_taylor(COLUMN["counts"], COLUMN["r"], COLUMN["box"], seed=COLUMN["seed"])
+    if state is None:
+        state = np.load(os.path.join(HERE, "settled_column.npz"))
+    pos, vel = state["position"], state["velocity"]
+    kw = dict(sc.__dict__)
+    kw.update(fluid_pos=pos.astype(np.float32), fluid_vel=vel.astype(np.float32),
+              phase=(pos[:, 1] > np.median(pos[:, 1])).astype(np.int32), rho0_phases=list(rho))
+    return Scene(**kw)
+
+
+def make_settled_column():
+    sc = rayleigh_taylor(COLUMN["counts"], COLUMN["r"], COLUMN["box"], seed=COLUMN["seed"], rho_heavy=1000.0)
+    sc.phase = None
+    o = make_scene_oracle(sc, kind="port", dt=1e-3, nu=1e-3, df_div_goal_abs=0.0, df_div_goal_rel=1e-3,
+                          df_div_max_iter=100, **MULTI_VISC)
+    for _ in range(300):
+        o.stage("df_step")
+    assert o.n_fluid() == sc.n_fluid
+    st = dict(position=o.get("position").astype(np.float32), velocity=o.get("velocity").astype(np.float32))
+    np.savez_compressed(os.path.join(HERE, "settled_column.npz"), **st)
+    o.close()
+    return st
+
+
+MULTI_FIELDS = ("position", "velocity", "density", "presure")
 
 
 def main():
@@ -63,6 +110,25 @@ def main():
     np.savez_compressed(os.path.join(HERE, "step_wcsph.npz"),
                         **{f: o.get(f).astype(np.float32) for f in
                            ("position", "velocity", "density", "presure", "acceleration")})
+    o.close()
+    state = make_settled_column()
+    col = column_scene(state)
+    o = make_scene_oracle(col, kind="reference", solver="pcisph", **MULTI_VISC, **PCI_KW)
+    for _ in range(3):
+        o.stage("runOneStep")
+    np.savez_compressed(os.path.join(HERE, "step_pcisph.npz"),
+                        **{"%s_%d" % (f, k): o.get(f, k).astype(np.float32)
+                           for k in range(2) for f in MULTI_FIELDS + ("acceleration", "acce_pressure")})
+    o.close()
+
+    o = make_scene_oracle(col, kind="reference", solver="iisphm", **MULTI_VISC, **II_KW)
+    o.set_threads(1)
+    for _ in range(3):
+        o.stage("runOneStep")
+    np.savez_compressed(os.path.join(HERE, "step_iisphm.npz"),
+                        **{"%s_%d" % (f, k): o.get(f, k).astype(np.float32)
+                           for k in range(2)
+                           for f in MULTI_FIELDS + ("dii", "aii", "rho_adv", "sum_dijpj", "acce_presure")})
     o.close()
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):

@@ -110,3 +110,63 @@ def test_fp64_restatement_close_to_fp32():
         o.stage("DF_constantDensitySolverFirst")
     ra, rb = a.get("density"), b.get("density")
     assert np.max(np.abs(ra - rb) / rb) < 1e-5
+
+
+def _golden_module():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("make_golden", os.path.join(GOLD, "make_golden.py"))
+    m = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(m)
+    return m
+
+
+def test_pcisph_steps_match_golden():
+    """PciSph::sphStep x 3 (two phases) reproduced bit for bit."""
+    mg = _golden_module()
+    g = np.load(os.path.join(GOLD, "step_pcisph.npz"))
+    o = make_scene_oracle(mg.column_scene(), **mg.MULTI_VISC, **mg.PCI_KW)
+    for _ in range(3):
+        o.stage("pci_step")
+    for key in g.files:
+        f, k = key.rsplit("_", 1)
+        np.testing.assert_array_equal(o.get(f, int(k)).astype(np.float32), g[key], err_msg=key)
+
+
+def test_iisphm_steps_match_golden():
+    """IISph_M::sphStep x 3 (two phases, one thread) reproduced bit for bit
+    with the reference's bookkeeping, integration and in-place sweep
+    (ii_compat = 1 | 2 | 4)."""
+    mg = _golden_module()
+    g = np.load(os.path.join(GOLD, "step_iisphm.npz"))
+    o = make_scene_oracle(mg.column_scene(), ii_compat=7, **mg.MULTI_VISC, **mg.II_KW)
+    for _ in range(3):
+        o.stage("ii_step")
+    for key in g.files:
+        f, k = key.rsplit("_", 1)
+        np.testing.assert_array_equal(o.get(f, int(k)).astype(np.float32), g[key], err_msg=key)
+
+
+def test_pci_delta_known_answer():
+    """PCISPH delta (PciSph.cpp:133-162) against the lattice sums in FP64:
+    delta = 1 / (2 v0^2 (|sum gradW|^2 + sum |gradW|^2)) / dt^2."""
+    p = default_params(spacing_r=0.05, smoothRadius_h=0.1, dt=1e-3)
+    o = Oracle(p)
+    o.stage("pci_updateDelta")
+    h = 0.05
+    th = 1 / np.pi / h ** 4
+    g = np.zeros(3)
+    g2 = 0.0
+    r = np.arange(-2, 3)
+    for z in r:
+        for y in r:
+            for x in r:
+                v = np.array([x, y, z], float) * 0.05
+                d = np.linalg.norm(v)
+                if d == 0 or d >= 0.1:
+                    continue
+                q = d / h
+                w = th * (3 * q - 2.25 * q * q) if q <= 1 else th * 0.75 * (2 - q) ** 2
+                g += v * (-w / d)
+                g2 += w * w
+    want = 1.0 / (2 * (0.05 ** 3) ** 2 * (g @ g + g2)) / 1e-6
+    assert abs(o.pci_delta() - want) / want < 1e-5
