@@ -85,7 +85,9 @@ SIGNATURES = {
     "sphgpu_mlp_gradient": (_i, [_vp, _fp, _fp, _i, _fp, _fp]),
     "sphgpu_mlp_predict": (_i, [_vp, _fp, _fp, _i]),
     "sphgpu_attach_warm_start": (_i, [_vp, _vp, _i, _i]),
+    "sphgpu_cfl_dt_noalloc": (_i, [_vp, _i, _i, _f, _f, _f, _f, _vp, _vp, _vp]),
 }
+NOALLOC_MAX_N = 8388608
 MLP_NPARAM = 5313
 MLP_IN = 16
 EXTRA = {"sphgpu_debug_set": (_i, [_vp, _cp, _i])}

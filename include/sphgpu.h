@@ -171,7 +171,12 @@ int sphgpu_step_host(sphgpu_t h, int solver, const float* xyz, const float* vel,
 /* Fluid fields in reference order (phase by phase, each in insertion order).
  * field: "position","velocity" (n*3); "density","DFalpha","DFkappa",
  * "DFkappaV","density_adv","divergenceDeviation","presure" (n);
- * "vel_adv","acce_adv","acceleration" (n*3).  Returns the count written. */
+ * "vel_adv","acce_adv","acceleration" (n*3);
+ * PCISPH: "pos_prediction","acce_pressure" (n*3);
+ * IISPH_M: "dii","sum_dijpj","ii_vel_adv","acce_presure" (n*3),
+ *          "aii","p_l","rho_adv" (n).  Returns the count written.
+ * set: "position","velocity","density" (the density the next PCISPH /
+ * IISPH_M step's non-pressure forces read), "DFalpha". */
 int sphgpu_get_fluid(sphgpu_t h, const char* field, float* out);
 int sphgpu_set_fluid(sphgpu_t h, const char* field, const float* in);
 int sphgpu_get_boundary(sphgpu_t h, const char* field, float* out); /* "position","volume" */
@@ -232,6 +237,31 @@ int sphgpu_attach_warm_start(sphgpu_t h, sphgpu_mlp_t m, int mode, int record_ev
 
 /* Copy of the last error message. */
 int sphgpu_last_error(sphgpu_t h, char* buf, int len);
+
+/* CFL time step from velocities that already live on the device, without
+ * allocating anything (no counterpart in the reference, whose dt is fixed).
+ * It is the in-step rule of sphgpu_step with cfl != 0:
+ *   vmax = max |v| in FP64,  dt = clamp(cfl_factor * d / vmax, dt_min, dt_max)
+ * (dt_max when vmax = 0), for callers that step their own particle arrays
+ * and may not allocate device memory between steps: hosts that hand all
+ * device memory to one pool up front, or run under a fixed memory budget.
+ *   vel       device pointer to n records of `stride` floats (x, y, z first;
+ *             stride >= 3, e.g. 4 for float4)
+ *   dt_out    device pointer to one float, written with dt
+ *   vmax_out  device pointer to one double (or NULL), written with vmax
+ *   stream    cudaStream_t to run on (NULL: the legacy default stream)
+ * The scratch is a file-scope device array of one FP64 partial per block of
+ * 2048 velocities (32 KB) plus a ticket that is zero at load time and that
+ * every call leaves at zero, so n is limited to SPHGPU_NOALLOC_MAX_N;
+ * larger n is rejected with SPHGPU_EINVAL before any GPU work.  The first
+ * call on a device (with that device current) looks up the scratch address
+ * once (cudaGetSymbolAddress); make it before any stream capture.  All calls
+ * on one device share the scratch: calls that overlap in time (other
+ * streams, other threads) race on it and must be serialised by the caller.
+ * Returns 0, SPHGPU_EINVAL or SPHGPU_ECUDA. */
+#define SPHGPU_NOALLOC_MAX_N 8388608
+int sphgpu_cfl_dt_noalloc(const float* vel, int n, int stride, float cfl_factor, float d, float dt_max,
+                          float dt_min, float* dt_out, double* vmax_out, void* stream);
 
 #ifdef __cplusplus
 }
