@@ -329,6 +329,16 @@ def run_ours(args):
                 "last_step": {"err_density": stw["err_density"], "status": stw["status"]},
                 "training": train_info,
                 "network": "16-64-64-1 GELU, BF16 weights/activations in mma.sync GEMMs, FP32 accumulate"}
+        if args.profile_steps > 0:
+            # per-kernel durations of the warm-start step (individual launches)
+            g.profile(True)
+            g.step("dfsph", args.profile_steps)
+            prof = g.profile_read()
+            g.profile(False)
+            g.synchronize()
+            warm["kernels"] = {k: {"launches": c, "avg_us": round(1e3 * t / max(c, 1), 2),
+                                   "us_per_step": round(1e3 * t / args.profile_steps, 1)}
+                               for k, (t, c) in prof.items()}
         attach(g, None, 0)
         g.set("position", end_pos)  # continue from the plain run's state
 

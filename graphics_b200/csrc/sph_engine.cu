@@ -25,7 +25,9 @@
 void mlp_init_attributes();
 void ws_init_attributes();
 void launch_ws_features(const DevScene& s, const SolverConst& c, const MlpDev& m, int infer, float dt_max,
-                        float alpha_ref, float* Xout, int n_max, cudaStream_t st);
+                        float alpha_ref, float* Xout, __nv_bfloat16* xn, int n_max, cudaStream_t st);
+void launch_ws_infer(const DevScene& s, const SolverConst& c, const MlpDev& m, const __nv_bfloat16* xn, int n_max,
+                     int sm_count, cudaStream_t st);
 void launch_ws_post(const DevScene& s, const SolverConst& c, float* yout, int n_max, cudaStream_t st);
 void launch_ws_append(const float* X, const float* y, int n_max, const int* n_act, int every, int* offset, float* dsX,
                       float* dsy, int* ds_count, int ds_cap, cudaStream_t st);
@@ -94,6 +96,8 @@ struct sphgpu_scene {
     int ws_offset = 0;
     float* recX = nullptr;  // [cap][16] features of the step being recorded
     float* recY = nullptr;  // [cap] labels
+    __nv_bfloat16* xn = nullptr;  // [cap][16] normalised features for the network (mode 1)
+    int sm_count = 148;
     float alpha_ref = 1.f;
     long long total_removed = 0;  // gid stays a permutation of [0, n) while 0
     int last_solver = -1;         // solver of the last step (carried-state validity)
@@ -291,7 +295,7 @@ void free_scene(sphgpu_scene* h) {
     void* ptrs[] = {d.pos, d.vel, d.gid, d.rho, d.alpha, d.vadv, d.pv, d.pk, d.bpv, d.kappav, d.acc, d.kr, d.kappa, d.ksum, d.aux0,
                     d.aux1, d.aux4, d.kwarm, d.hist, d.wsbuf, d.pos_s, d.vel_s, d.gid_s, d.hist_s, d.key, d.slot, d.tmp,
                     d.cA, d.cB, d.cC, d.cA_s, d.cB_s, d.cC_s, d.ap, d.pl2,
-                    h->recX, h->recY,
+                    h->recX, h->recY, h->xn,
                     d.cell_count, d.cell_start, d.bcell_start, d.cstart2, d.nbr, d.ncount, d.partial, d.st,
                     d.bpos, d.bvel, d.bgid, h->cub_tmp};
     for (void* p : ptrs)
@@ -390,13 +394,16 @@ int enq_df_step(sphgpu_scene* h, bool capturing) {
     const int ws = h->mlp ? h->ws_mode : 0;
     launch(h, "df_forces", st, [&] { launch_df_forces(d, h->c, h->cap, 0, st); });
     if (ws == 1 || ws == 3) {
-        launch(h, "ws_features_infer", st, [&] {
-            launch_ws_features(d, h->c, h->mlp->m, ws == 1 ? 1 : 2, h->P.dt_max, h->alpha_ref, nullptr, h->cap, st);
+        launch(h, "ws_features", st, [&] {
+            launch_ws_features(d, h->c, h->mlp->m, ws == 1 ? 1 : 2, h->P.dt_max, h->alpha_ref, nullptr, h->xn, h->cap,
+                               st);
         });
+        if (ws == 1)
+            launch(h, "ws_infer", st, [&] { launch_ws_infer(d, h->c, h->mlp->m, h->xn, h->cap, h->sm_count, st); });
         launch(h, "df_warm", st, [&] { launch_df_warm_correction(d, h->c, h->cap, st); });
     } else if (ws == 2) {
         launch(h, "ws_features", st, [&] {
-            launch_ws_features(d, h->c, h->mlp->m, 0, h->P.dt_max, h->alpha_ref, h->recX, h->cap, st);
+            launch_ws_features(d, h->c, h->mlp->m, 0, h->P.dt_max, h->alpha_ref, h->recX, nullptr, h->cap, st);
         });
     }
     const int rec = h->record_ksum;
@@ -745,6 +752,7 @@ int sphgpu_create(const SphParams* p, int device, int max_fluid, sphgpu_t* out) 
         return SPHGPU_ECUDA;
     }
     h->cap = max_fluid;
+    cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, device);
     h->stride = roundup(max_fluid, 32);
     h->ncap = p->max_neighbours;
     h->g = make_grid(*p);
@@ -1010,6 +1018,15 @@ int sphgpu_get_fluid(sphgpu_t h, const char* field, float* out) {
     else if (f == "dii") { src = d.cB; f4 = true; comps = 3; }
     else if (f == "sum_dijpj") { src = d.cC; f4 = true; comps = 3; }
     else if (f == "ii_vel_adv") { src = d.cA; f4 = true; comps = 3; }
+    else if (f == "ws_features") {
+        // normalised BF16 network inputs of the last warm-start step (n*16)
+        if (!h->xn) { h->err = "no learned warm start attached"; return SPHGPU_EINVAL; }
+        std::vector<__nv_bfloat16> t((size_t)n * MLP_IN);
+        CK(cudaMemcpy(t.data(), h->xn, sizeof(__nv_bfloat16) * t.size(), cudaMemcpyDeviceToHost));
+        for (int k = 0; k < n; ++k)
+            for (int i = 0; i < MLP_IN; ++i) out[(size_t)k * MLP_IN + i] = __bfloat162float(t[(size_t)order[k] * MLP_IN + i]);
+        return n;
+    }
     else if (f == "aii" || f == "p_l") {
         std::vector<float4> t(n);
         CK(cudaMemcpy(t.data(), f == "aii" ? d.cC : d.cA, sizeof(float4) * n, cudaMemcpyDeviceToHost));
@@ -1174,7 +1191,8 @@ int sphgpu_stage(sphgpu_t h, const char* name, SphStepStats* stats) {
         if (h->P.cfl) launch_cfl(d, h->cap, h->P.cfl_factor, h->P.particle_d, h->P.dt_max, h->P.dt_min, st);
         launch_df_forces(d, h->c, h->cap, 0, st);
         if (h->mlp && h->ws_mode == 1) {
-            launch_ws_features(d, h->c, h->mlp->m, 1, h->P.dt_max, h->alpha_ref, nullptr, h->cap, st);
+            launch_ws_features(d, h->c, h->mlp->m, 1, h->P.dt_max, h->alpha_ref, nullptr, h->xn, h->cap, st);
+            launch_ws_infer(d, h->c, h->mlp->m, h->xn, h->cap, h->sm_count, st);
             launch_df_warm_correction(d, h->c, h->cap, st);
         }
         r = enq_df_density_loop(h, false);
@@ -1543,6 +1561,10 @@ int sphgpu_attach_warm_start(sphgpu_t h, sphgpu_mlp_t m, int mode, int record_ev
     if (mode && m->device != h->device) { h->err = "network and scene on different devices"; return SPHGPU_EINVAL; }
     if (mode == 2 && !h->recX) {
         if (dalloc(h, &h->recX, (size_t)h->cap * MLP_IN) || dalloc(h, &h->recY, (size_t)h->cap)) return SPHGPU_ENOMEM;
+    }
+    if (mode == 1 && !h->xn) {
+        if (dalloc(h, &h->xn, (size_t)h->cap * MLP_IN)) return SPHGPU_ENOMEM;
+        cudaMemsetAsync(h->xn, 0, sizeof(__nv_bfloat16) * (size_t)h->cap * MLP_IN, h->stream);
     }
     h->mlp = mode ? m : nullptr;
     h->ws_mode = mode;

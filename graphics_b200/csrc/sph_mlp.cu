@@ -359,47 +359,140 @@ __device__ __forceinline__ void ws_features(const DevScene& s, const SolverConst
     x[15] = 1.f;
 }
 
-// features -> network -> kwarm (and, when recording, the features of the step)
-// INFER 0: features only; 1: network; 2: previous step's stiffness (the
-// classic warm start, as a comparison for the network)
+// features of the step (and, when recording, their FP32 copy); INFER 0:
+// features only; 1: also the normalised BF16 features the inference kernel
+// reads; 2: previous step's stiffness (the classic warm start, as a
+// comparison for the network)
 template <int INFER>
 __global__ void __launch_bounds__(TR) k_ws_features(DevScene s, SolverConst c, MlpDev m, float dt_max,
-                                                   float alpha_ref, float* Xout) {
-    extern __shared__ __align__(16) unsigned char smraw[];
-    FwdSmem& S = *reinterpret_cast<FwdSmem*>(smraw);
+                                                   float alpha_ref, float* Xout, __nv_bfloat16* xn) {
     const int n = s.st->n_active;
     const int p = blockIdx.x * TR + threadIdx.x;
+    if (p >= n) return;
     const float dt = *s.dt;
     float x[MLP_IN];
     float pred = 0.f, divt = 0.f;
-    if (p < n) {
-        ws_features(s, c, p, dt, dt_max, alpha_ref, x, pred, divt);
-        s.wsbuf[p] = make_float2(pred, divt);
-        if (Xout)
-            for (int i = 0; i < MLP_IN; ++i) Xout[(size_t)p * MLP_IN + i] = x[i];
-    } else {
-        for (int i = 0; i < MLP_IN; ++i) x[i] = 0.f;
-    }
-    if (!INFER) return;
-    if (INFER == 2) {
-        if (p < n) {
-            const float kw = c.ws_scale * fmaxf(s.hist[p].x, 0.f);
-            s.kwarm[p] = kw;
-            s.pk[p].w = kw / s.rho[p];
-        }
-        return;
-    }
-    load_weights(m, S);
-    const float* nrm = m.norm;
-    for (int i = 0; i < MLP_IN; ++i) S.X[threadIdx.x * MLP_IN + i] = __float2bfloat16_rn((x[i] - nrm[i]) * nrm[MLP_IN + i]);
-    __syncthreads();
-    const float yn = forward_rows(S);
-    if (p < n) {
-        const float kpred = yn / nrm[2 * MLP_IN + 1] + nrm[2 * MLP_IN];
-        // negative predictions are not applied (the loop only adds pressure)
-        const float kw = c.ws_scale * fmaxf(kpred, 0.f);
+    ws_features(s, c, p, dt, dt_max, alpha_ref, x, pred, divt);
+    s.wsbuf[p] = make_float2(pred, divt);
+    if (Xout)
+        for (int i = 0; i < MLP_IN; ++i) Xout[(size_t)p * MLP_IN + i] = x[i];
+    if (INFER == 1) {
+        const float* nrm = m.norm;
+        uint32_t u[MLP_IN / 2];
+#pragma unroll
+        for (int i = 0; i < MLP_IN / 2; ++i)
+            u[i] = pack2(__float2bfloat16_rn((x[2 * i] - nrm[2 * i]) * nrm[MLP_IN + 2 * i]),
+                         __float2bfloat16_rn((x[2 * i + 1] - nrm[2 * i + 1]) * nrm[MLP_IN + 2 * i + 1]));
+        uint4* dst = reinterpret_cast<uint4*>(xn + (size_t)p * MLP_IN);
+        dst[0] = make_uint4(u[0], u[1], u[2], u[3]);
+        dst[1] = make_uint4(u[4], u[5], u[6], u[7]);
+    } else if (INFER == 2) {
+        const float kw = c.ws_scale * fmaxf(s.hist[p].x, 0.f);
         s.kwarm[p] = kw;
-        s.pk[p].w = kw / s.rho[p];  // read by the warm-correction sweep
+        s.pk[p].w = kw / s.rho[p];
+    }
+}
+
+// Inference of the warm-start network over the normalised features, on the
+// tensor cores with every activation in registers: each warp runs 2 x 16
+// rows; the layer-1 accumulator fragments (m16n8, FP32) are biased, passed
+// through GELU, rounded to BF16 and re-packed as the A fragments of layer 2
+// (m16k16: the C tiles of columns 16kk..16kk+7 and 16kk+8..16kk+15 form the
+// A fragment of k-step kk); layer 3 (64 -> 1) is a per-thread dot product
+// over the thread's accumulator columns, finished with two quad shuffles.
+// Weights sit in shared memory as pre-packed per-lane B fragments.
+struct InferSmem {
+    uint2 w1f[8 * 32];       // [n-tile][lane]
+    uint2 w2f[4 * 8 * 32];   // [k-step][n-tile][lane]
+    float b1[MLP_H], b2[MLP_H], w3[MLP_H];
+    float b3;
+    float y[TR];
+};
+
+__global__ void __launch_bounds__(TR) k_ws_infer(DevScene s, SolverConst c, MlpDev m, const __nv_bfloat16* xn) {
+    __shared__ InferSmem S;
+    const __nv_bfloat16* W = m.w_bf16;
+    for (int i = threadIdx.x; i < 8 * 32; i += TR) {
+        const int nt = i >> 5, lane = i & 31, g = lane >> 2, t = lane & 3, col = nt * 8 + g;
+        const __nv_bfloat16* w1 = W + MLP_OFF_W1;
+        S.w1f[i] = make_uint2(pack2(w1[(2 * t) * MLP_H + col], w1[(2 * t + 1) * MLP_H + col]),
+                              pack2(w1[(2 * t + 8) * MLP_H + col], w1[(2 * t + 9) * MLP_H + col]));
+    }
+    for (int i = threadIdx.x; i < 4 * 8 * 32; i += TR) {
+        const int kk = i >> 8, nt = (i >> 5) & 7, lane = i & 31, g = lane >> 2, t = lane & 3;
+        const int k = 16 * kk + 2 * t, col = nt * 8 + g;
+        const __nv_bfloat16* w2 = W + MLP_OFF_W2;
+        S.w2f[i] = make_uint2(pack2(w2[k * MLP_H + col], w2[(k + 1) * MLP_H + col]),
+                              pack2(w2[(k + 8) * MLP_H + col], w2[(k + 9) * MLP_H + col]));
+    }
+    for (int i = threadIdx.x; i < MLP_H; i += TR) {
+        S.b1[i] = m.master[MLP_OFF_B1 + i];
+        S.b2[i] = m.master[MLP_OFF_B2 + i];
+        S.w3[i] = __bfloat162float(W[MLP_OFF_W3 + i]);
+    }
+    if (threadIdx.x == 0) S.b3 = m.master[MLP_OFF_B3];
+    __syncthreads();
+    const int n = s.st->n_active;
+    const float* nrm = m.norm;
+    const float ysd = nrm[2 * MLP_IN + 1], ymean = nrm[2 * MLP_IN];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    for (int base = blockIdx.x * TR; base < n; base += gridDim.x * TR) {
+        for (int mt = 0; mt < 2; ++mt) {
+            const int rt = w * 32 + mt * 16;  // tile row offset inside the block's 128 rows
+            const int r0 = base + rt + g, r1 = r0 + 8;
+            const uint32_t* x0 = reinterpret_cast<const uint32_t*>(xn + (size_t)min(r0, n - 1) * MLP_IN);
+            const uint32_t* x1 = reinterpret_cast<const uint32_t*>(xn + (size_t)min(r1, n - 1) * MLP_IN);
+            const uint32_t a[4] = {__ldg(x0 + t), __ldg(x1 + t), __ldg(x0 + 4 + t), __ldg(x1 + 4 + t)};
+            uint32_t h[4][4];
+#pragma unroll
+            for (int nt = 0; nt < 8; ++nt) {
+                float cc[4] = {0.f, 0.f, 0.f, 0.f};
+                const uint2 b = S.w1f[nt * 32 + lane];
+                const uint32_t bb[2] = {b.x, b.y};
+                mma16816(cc, a, bb);
+                const int col = nt * 8 + 2 * t;
+                const uint32_t u01 = pack2(__float2bfloat16_rn(gelu(cc[0] + S.b1[col])),
+                                           __float2bfloat16_rn(gelu(cc[1] + S.b1[col + 1])));
+                const uint32_t u23 = pack2(__float2bfloat16_rn(gelu(cc[2] + S.b1[col])),
+                                           __float2bfloat16_rn(gelu(cc[3] + S.b1[col + 1])));
+                h[nt >> 1][(nt & 1) * 2] = u01;
+                h[nt >> 1][(nt & 1) * 2 + 1] = u23;
+            }
+            float y0 = 0.f, y1 = 0.f;
+#pragma unroll
+            for (int nt = 0; nt < 8; ++nt) {
+                float cc[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+                for (int kk = 0; kk < 4; ++kk) {
+                    const uint2 b = S.w2f[(kk * 8 + nt) * 32 + lane];
+                    const uint32_t bb[2] = {b.x, b.y};
+                    mma16816(cc, h[kk], bb);
+                }
+                const int col = nt * 8 + 2 * t;
+                y0 = fmaf(gelu(cc[0] + S.b2[col]), S.w3[col], y0);
+                y0 = fmaf(gelu(cc[1] + S.b2[col + 1]), S.w3[col + 1], y0);
+                y1 = fmaf(gelu(cc[2] + S.b2[col]), S.w3[col], y1);
+                y1 = fmaf(gelu(cc[3] + S.b2[col + 1]), S.w3[col + 1], y1);
+            }
+            y0 += __shfl_xor_sync(0xffffffffu, y0, 1);
+            y0 += __shfl_xor_sync(0xffffffffu, y0, 2);
+            y1 += __shfl_xor_sync(0xffffffffu, y1, 1);
+            y1 += __shfl_xor_sync(0xffffffffu, y1, 2);
+            if (t == 0) {
+                S.y[rt + g] = y0 + S.b3;
+                S.y[rt + g + 8] = y1 + S.b3;
+            }
+        }
+        __syncwarp();
+        const int p = base + threadIdx.x;
+        if (p < n) {
+            const float kpred = S.y[threadIdx.x] / ysd + ymean;
+            // negative predictions are not applied (the loop only adds pressure)
+            const float kw = c.ws_scale * fmaxf(kpred, 0.f);
+            s.kwarm[p] = kw;
+            s.pk[p].w = kw / s.rho[p];  // read by the warm-correction sweep
+        }
+        __syncwarp();
     }
 }
 
@@ -433,16 +526,22 @@ __global__ void k_ws_append(const float* X, const float* y, int n_max, const int
 __global__ void k_ws_advance(int* offset, int every) { *offset = (*offset + 1) % every; }
 }  // namespace
 
-void ws_init_attributes() {
-    cudaFuncSetAttribute(k_ws_features<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(FwdSmem));
-}
+void ws_init_attributes() {}
 
 void launch_ws_features(const DevScene& s, const SolverConst& c, const MlpDev& m, int infer, float dt_max,
-                        float alpha_ref, float* Xout, int n_max, cudaStream_t st) {
+                        float alpha_ref, float* Xout, __nv_bfloat16* xn, int n_max, cudaStream_t st) {
     const int blocks = (n_max + TR - 1) / TR;
-    if (infer == 1) k_ws_features<1><<<blocks, TR, sizeof(FwdSmem), st>>>(s, c, m, dt_max, alpha_ref, Xout);
-    else if (infer == 2) k_ws_features<2><<<blocks, TR, 0, st>>>(s, c, m, dt_max, alpha_ref, Xout);
-    else k_ws_features<0><<<blocks, TR, 0, st>>>(s, c, m, dt_max, alpha_ref, Xout);
+    if (infer == 1) k_ws_features<1><<<blocks, TR, 0, st>>>(s, c, m, dt_max, alpha_ref, Xout, xn);
+    else if (infer == 2) k_ws_features<2><<<blocks, TR, 0, st>>>(s, c, m, dt_max, alpha_ref, Xout, xn);
+    else k_ws_features<0><<<blocks, TR, 0, st>>>(s, c, m, dt_max, alpha_ref, Xout, xn);
+}
+
+void launch_ws_infer(const DevScene& s, const SolverConst& c, const MlpDev& m, const __nv_bfloat16* xn, int n_max,
+                     int sm_count, cudaStream_t st) {
+    int blocks = (n_max + TR - 1) / TR;
+    const int cap = sm_count * 8;  // persistent: each block packs the weights once
+    if (blocks > cap) blocks = cap;
+    k_ws_infer<<<blocks, TR, 0, st>>>(s, c, m, xn);
 }
 
 void launch_ws_post(const DevScene& s, const SolverConst& c, float* yout, int n_max, cudaStream_t st) {

@@ -171,10 +171,10 @@ class GpuScene:
     # -- fields --
     def get(self, field):
         n = self.n_fluid
-        comps = 3 if field in VEC_FIELDS else 1
+        comps = 3 if field in VEC_FIELDS else (_lib.MLP_IN if field == "ws_features" else 1)
         out = np.zeros(max(n, 1) * comps, dtype=np.float32)
         m = self._check(self.lib.sphgpu_get_fluid(self.h, field.encode(), _fptr(out)), "get " + field)
-        return out[:m * comps].reshape(m, 3) if comps == 3 else out[:m]
+        return out[:m * comps].reshape(m, comps) if comps > 1 else out[:m]
 
     def set(self, field, values):
         v = np.ascontiguousarray(values, dtype=np.float32).ravel()
@@ -184,7 +184,7 @@ class GpuScene:
         comps = 3 if field == "position" else 1
         out = np.zeros(max(self.nb, 1) * comps, dtype=np.float32)
         m = self._check(self.lib.sphgpu_get_boundary(self.h, field.encode(), _fptr(out)), "get_boundary")
-        return out[:m * comps].reshape(m, 3) if comps == 3 else out[:m]
+        return out[:m * comps].reshape(m, comps) if comps > 1 else out[:m]
 
     def neighbours(self):
         """(counts[n], t[n,cap], i[n,cap]) in the reference's PartIdx encoding."""

@@ -174,7 +174,9 @@ int sphgpu_step_host(sphgpu_t h, int solver, const float* xyz, const float* vel,
  * "vel_adv","acce_adv","acceleration" (n*3);
  * PCISPH: "pos_prediction","acce_pressure" (n*3);
  * IISPH_M: "dii","sum_dijpj","ii_vel_adv","acce_presure" (n*3),
- *          "aii","p_l","rho_adv" (n).  Returns the count written.
+ *          "aii","p_l","rho_adv" (n);
+ * learned warm start: "kappa_warm" (n), "ws_features" (n*16, the network's
+ * normalised inputs of the last step).  Returns the count written.
  * set: "position","velocity","density" (the density the next PCISPH /
  * IISPH_M step's non-pressure forces read), "DFalpha". */
 int sphgpu_get_fluid(sphgpu_t h, const char* field, float* out);

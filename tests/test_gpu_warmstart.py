@@ -89,3 +89,26 @@ def test_warm_start_saves_iterations_at_same_tolerance():
         assert st["err_density"] <= 1e-4 and not (st["status"] & 1)
         g.close()
     assert its[1] < its[2], its
+
+
+def test_scene_inference_kernel_matches_oracle():
+    """The in-step inference kernel (register-fragment MLP over the
+    normalised BF16 features) against the FP64 oracle on the same inputs."""
+    from graphics_b200.scene import small_dam_break
+    from graphics_b200.sph import scene_to_gpu
+    from graphics_b200.warmstart import attach
+    rng = np.random.default_rng(7)
+    net = _net()
+    w, norm = _random_state(rng)
+    net.set_params(w)
+    net.set_norm(norm)
+    g = scene_to_gpu(small_dam_break((16, 16, 16), 0.025, seed=3), dt=1e-3, ws_scale=1.0)
+    attach(g, net, 1)
+    g.step("dfsph", 2)
+    xn = g.get("ws_features")
+    kw = g.get("kappa_warm")
+    ident = np.concatenate([np.zeros(NIN), np.ones(NIN), norm[2 * NIN:]]).astype(np.float64)
+    ko = np.maximum(orc_predict(w, ident, xn.astype(np.float32)), 0.0)
+    assert xn.shape == (g.n_fluid, NIN) and np.all(np.isfinite(xn))
+    assert np.max(np.abs(kw - ko)) <= 2e-3 * np.max(np.abs(ko)) + 1e-5
+    g.close()
