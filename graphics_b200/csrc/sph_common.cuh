@@ -2,7 +2,7 @@
 //
 // Data layout in HBM (all fluid arrays in cell-sorted order, rebuilt every
 // neighbour search):
-//   pos   float4 (x, y, z, phase as int bits)   16 B/particle
+//   pos   float4 (x, y, z, phase | scene << 4 as int bits)   16 B/particle
 //   vel   float4 (vx, vy, vz, 0)                16 B/particle
 //   gid   int   global fluid index (phase-major insertion order; the
 //               reference's m_Fluids[k].fluidParticles[i] order)
@@ -31,7 +31,9 @@ struct GridGeom {
     float divisor;     // 1/h
     int num[3];        // cells per axis
     int nb[3];         // 4x4x4 bricks per axis
-    int nkeys;         // nb.x*nb.y*nb.z*64 + 1 (last key: removed particles)
+    int nkeys;         // keys of the whole key space + 1 (last key: removed particles)
+    int key0, key1;    // this grid's keys are [key0, key1) (a batch packs one grid per scene)
+    float smin[3], smax[3];  // m_TH.spaceMin / spaceMax (outside-particle removal)
 };
 
 // Kernel constants of the reference's single-h cubic spline
@@ -127,14 +129,17 @@ __device__ __forceinline__ int morton2x3(int x, int y, int z) {
 
 __device__ __forceinline__ int cell_key(const GridGeom& g, int cx, int cy, int cz) {
     int b = ((cz >> 2) * g.nb[1] + (cy >> 2)) * g.nb[0] + (cx >> 2);
-    return b * 64 + morton2x3(cx & 3, cy & 3, cz & 3);
+    return g.key0 + b * 64 + morton2x3(cx & 3, cy & 3, cz & 3);
 }
 
 __device__ __forceinline__ bool cell_inside(const GridGeom& g, int cx, int cy, int cz) {
     return cx >= 0 && cy >= 0 && cz >= 0 && cx < g.num[0] && cy < g.num[1] && cz < g.num[2];
 }
 
-__device__ __forceinline__ int phase_of(float4 p) { return __float_as_int(p.w); }
+// pos.w holds the fluid phase (4 bits) and, in a batch, the scene index
+// above them; the bits travel with the particle through every reorder
+__device__ __forceinline__ int phase_of(float4 p) { return __float_as_int(p.w) & 15; }
+__device__ __forceinline__ int scene_of(float4 p) { return __float_as_int(p.w) >> 4; }
 
 // One 32-byte record in a single 256-bit load (sm_100 ld.global.v8; the
 // address must be 32-byte aligned, which the packed pv/bpv arrays are).

@@ -86,8 +86,8 @@ __global__ void __launch_bounds__(NT) k_df_forces(DevScene s, SolverConst c, int
     const int p = blockIdx.x * NT + threadIdx.x;
     int zero = 0;
     if (p < n) {
-        const float dt = *s.dt;
         const float4 pa = s.pos[p];
+        const float dt = dt_of(s, pa);
         const float4 va = s.vel[p];
         const float rhoa = s.rho[p];
         const float fm0 = c.fm0, rho0 = c.rho0;
@@ -182,9 +182,9 @@ __global__ void __launch_bounds__(NT) k_df_dens_a(DevScene s, SolverConst c, int
     const int n = s.st->n_active;
     const int p = blockIdx.x * NT + threadIdx.x;
     double mine = 0.0;
-    if (p < n) {
-        const float dt = *s.dt;
+    if (p < n && scene_active(s, s.pv[2 * p])) {
         const float4 pa = s.pv[2 * p];
+        const float dt = dt_of(s, pa);
         const float4 va = s.pv[2 * p + 1];
         const float rho0 = c.rho0;
         const float acc = div_sweep(s, c, p, pa, va);
@@ -199,6 +199,7 @@ __global__ void __launch_bounds__(NT) k_df_dens_a(DevScene s, SolverConst c, int
         s.aux0[p] = dadv;
         mine = (double)dadv;
     }
+    if (s.nscenes > 1) return;  // a batch reduces per scene (k_batch_decide)
     __shared__ double sh[NT / 32];
     double bs = block_sum_double<NT>(mine, sh);
     double tot;
@@ -216,8 +217,8 @@ __global__ void __launch_bounds__(NT) k_df_vupdate(DevScene s, SolverConst c, do
                                                    int use_handle) {
     const int n = s.st->n_active;
     const int p = blockIdx.x * NT + threadIdx.x;
-    if (p < n) {
-        const float dt = *s.dt;
+    if (p < n && scene_active(s, s.pv[2 * p])) {
+        const float dt = dt_of(s, s.pv[2 * p]);
         const float4 pa = s.pk[p];
         float4 va = s.pv[2 * p + 1];
         const float ka = pa.w;
@@ -257,7 +258,7 @@ __global__ void __launch_bounds__(NT) k_df_vupdate(DevScene s, SolverConst c, do
         s.pv[2 * p + 1] = va;
         if (DIV) s.vel[p] = va;  // velocity = vel_adv (DFSPH.cpp:909)
     }
-    if (DECIDE && blockIdx.x == 0 && threadIdx.x == 0) {
+    if (DECIDE && s.nscenes <= 1 && blockIdx.x == 0 && threadIdx.x == 0) {
         // convergence decision of the iteration that just finished
         int it;
         int cont;
@@ -288,9 +289,9 @@ __global__ void __launch_bounds__(NT) k_df_div_a(DevScene s, SolverConst c) {
     const int n = s.st->n_active;
     const int p = blockIdx.x * NT + threadIdx.x;
     double mine = 0.0;
-    if (p < n) {
-        const float dt = *s.dt;
+    if (p < n && scene_active(s, s.pv[2 * p])) {
         const float4 pa = s.pv[2 * p];
+        const float dt = dt_of(s, pa);
         const float4 va = s.pv[2 * p + 1];
         float dd = div_sweep(s, c, p, pa, va);
         const float rho = s.rho[p];
@@ -301,6 +302,7 @@ __global__ void __launch_bounds__(NT) k_df_div_a(DevScene s, SolverConst c) {
         s.aux1[p] = dd;
         mine = (double)dd;
     }
+    if (s.nscenes > 1) return;  // a batch reduces per scene (k_batch_decide)
     __shared__ double sh[NT / 32];
     double bs = block_sum_double<NT>(mine, sh);
     double tot;

@@ -101,6 +101,12 @@ struct sphgpu_scene {
     float alpha_ref = 1.f;
     long long total_removed = 0;  // gid stays a permutation of [0, n) while 0
     int last_solver = -1;         // solver of the last step (carried-state validity)
+    // batch of independent scenes (nscenes > 1): one grid per scene in one key space
+    int nscenes = 1;
+    std::vector<GridGeom> sgeom;  // per scene (key ranges, boxes)
+    int last_scene = 0;           // scenes receive their fluid in order
+    GridGeom* d_geom = nullptr;
+    void* d_batch = nullptr;      // one allocation holding the BatchDev arrays
 };
 
 namespace {
@@ -176,6 +182,9 @@ GridGeom make_grid(const SphParams& P) {
         g.nb[i] = (g.num[i] + 3) / 4;
     }
     g.nkeys = g.nb[0] * g.nb[1] * g.nb[2] * 64 + 1;
+    g.key0 = 0;
+    g.key1 = g.nkeys - 1;
+    for (int i = 0; i < 3; ++i) { g.smin[i] = P.spaceMin[i]; g.smax[i] = P.spaceMax[i]; }
     return g;
 }
 
@@ -300,6 +309,8 @@ void free_scene(sphgpu_scene* h) {
                     d.bpos, d.bvel, d.bgid, h->cub_tmp};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    if (h->d_geom) cudaFree(h->d_geom);
+    if (h->d_batch) cudaFree(h->d_batch);
     if (h->h_stats) cudaFreeHost(h->h_stats);
     if (h->h_cont) cudaFreeHost(h->h_cont);
     for (auto& kv : h->graphs) cudaGraphExecDestroy(kv.second);
@@ -311,13 +322,14 @@ void free_scene(sphgpu_scene* h) {
 void enq_ns(sphgpu_scene* h, int integrate, int build_mode, cudaStream_t st, int carry = 1) {
     DevScene& d = h->d;
     cudaMemsetAsync(d.cell_count, 0, sizeof(int) * ((size_t)h->g.nkeys + 1), st);
-    launch(h, "hash", st, [&] { launch_hash(d, h->g, h->P.spaceMin, h->P.spaceMax, integrate, h->cap, st); });
+    launch(h, "hash", st, [&] { launch_hash(d, h->g, integrate, h->cap, st); });
     launch(h, "scan", st, [&] {
         size_t b = h->cub_bytes;
         cub::DeviceScan::ExclusiveSum(h->cub_tmp, b, d.cell_count, d.cell_start, h->g.nkeys + 1, st);
     });
     launch(h, "reorder", st, [&] { launch_scatter_reorder(d, h->g, h->cap, carry, st); });
     launch_count_active(d, h->g, st);
+    if (h->nscenes > 1) launch_batch_count(d, h->nscenes, st);
     launch(h, build_mode == 1 ? "build_first" : (build_mode == 2 ? "build_pressure" : "build"), st,
            [&] { launch_build(d, h->g, h->c, build_mode, h->cap, st); });
 }
@@ -360,12 +372,18 @@ int enq_df_density_loop(sphgpu_scene* h, bool capturing) {
     DevScene& d = h->d;
     const SphParams& P = h->P;
     launch_df_loop_reset(d, 0, h->stream);
+    if (h->nscenes > 1) launch_batch_loop_reset(d, h->nscenes, 0, h->stream);
     return enq_loop(h, capturing, [&](cudaStream_t st, unsigned long long hd, int use) {
         launch(h, "df_density_a", st, [&] { launch_df_dens_a(d, h->c, h->cap, h->record_ksum, st); });
         launch(h, "df_density_b", st, [&] {
             launch_df_dens_b(d, h->c, h->cap, P.df_density_goal, P.df_density_min_iter, P.df_density_max_iter, hd,
                              use, st);
         });
+        if (h->nscenes > 1)
+            launch(h, "batch_decide", st, [&] {
+                launch_batch_decide(d, h->c, 0, h->nscenes, 0.0, P.df_density_goal, P.df_density_min_iter,
+                                    P.df_density_max_iter, hd, use, st);
+            });
     });
 }
 
@@ -373,12 +391,18 @@ int enq_df_div_loop(sphgpu_scene* h, bool capturing) {
     DevScene& d = h->d;
     const SphParams& P = h->P;
     launch_df_loop_reset(d, 1, h->stream);
+    if (h->nscenes > 1) launch_batch_loop_reset(d, h->nscenes, 1, h->stream);
     return enq_loop(h, capturing, [&](cudaStream_t st, unsigned long long hd, int use) {
         launch(h, "df_div_a", st, [&] { launch_df_div_a(d, h->c, h->cap, st); });
         launch(h, "df_div_b", st, [&] {
             launch_df_div_b(d, h->c, h->cap, P.df_div_goal_abs, P.df_div_goal_rel, P.df_div_min_iter,
                             P.df_div_max_iter, hd, use, st);
         });
+        if (h->nscenes > 1)
+            launch(h, "batch_decide", st, [&] {
+                launch_batch_decide(d, h->c, 1, h->nscenes, P.df_div_goal_abs, P.df_div_goal_rel, P.df_div_min_iter,
+                                    P.df_div_max_iter, hd, use, st);
+            });
     });
 }
 
@@ -389,7 +413,11 @@ int enq_df_step(sphgpu_scene* h, bool capturing) {
     DevScene& d = h->d;
     cudaStream_t st = h->stream;
     launch_step_begin(d, st);
-    if (h->P.cfl)
+    if (h->P.cfl && h->nscenes > 1)
+        launch(h, "cfl", st, [&] {
+            launch_batch_cfl(d, h->nscenes, h->P.cfl_factor, h->P.particle_d, h->P.dt_max, h->P.dt_min, st);
+        });
+    else if (h->P.cfl)
         launch(h, "cfl", st, [&] { launch_cfl(d, h->cap, h->P.cfl_factor, h->P.particle_d, h->P.dt_max, h->P.dt_min, st); });
     const int ws = h->mlp ? h->ws_mode : 0;
     launch(h, "df_forces", st, [&] { launch_df_forces(d, h->c, h->cap, 0, st); });
@@ -607,7 +635,12 @@ int enq_steps(sphgpu_scene* h, int solver, int nsteps) {
         h->err = "DFSPH path supports one fluid phase";
         return SPHGPU_ENOTIMPL;
     }
+    if (h->nscenes > 1 && (solver != SPHGPU_DFSPH || (h->mlp && h->ws_mode))) {
+        h->err = "a batch of scenes runs the plain DFSPH solver";
+        return SPHGPU_ENOTIMPL;
+    }
     launch_call_begin(h->d, h->stream);
+    if (h->nscenes > 1) launch_batch_call_begin(h->d, h->nscenes, h->stream);
     if (solver == SPHGPU_PCISPH || solver == SPHGPU_IISPH_M) {
         if (h->last_solver != solver && h->last_solver >= 0) {
             // entering from another solver: the carried state starts as the
@@ -732,12 +765,19 @@ int sphgpu_params_default(SphParams* p) {
     return 0;
 }
 
-int sphgpu_create(const SphParams* p, int device, int max_fluid, sphgpu_t* out) {
-    if (!p || !out || max_fluid <= 0) return SPHGPU_EINVAL;
+// One scene (nscenes == 1, box from p) or a batch of nscenes scenes with
+// boxes smin/smax[3 * scene]: one grid per scene, key ranges back to back.
+static int create_impl(const SphParams* p, int device, int max_fluid, int nscenes, const float* smin,
+                       const float* smax, sphgpu_t* out) {
+    if (!p || !out || max_fluid <= 0 || nscenes <= 0) return SPHGPU_EINVAL;
     if (p->max_neighbours <= 0 || p->max_neighbours > 128) return SPHGPU_EINVAL;
     if (!(p->smoothRadius_h > 0) || !(p->particle_d > 0) || !(p->spacing_r > 0)) return SPHGPU_EINVAL;
-    for (int i = 0; i < 3; ++i)
-        if (!(p->spaceMax[i] > p->spaceMin[i])) return SPHGPU_EINVAL;
+    for (int sc = 0; sc < nscenes; ++sc)
+        for (int i = 0; i < 3; ++i) {
+            const float lo = nscenes > 1 ? smin[3 * sc + i] : p->spaceMin[i];
+            const float hi = nscenes > 1 ? smax[3 * sc + i] : p->spaceMax[i];
+            if (!(hi > lo)) return SPHGPU_EINVAL;
+        }
     *out = nullptr;
     sphgpu_scene* h = new sphgpu_scene();
     h->P = *p;
@@ -755,11 +795,59 @@ int sphgpu_create(const SphParams* p, int device, int max_fluid, sphgpu_t* out) 
     cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, device);
     h->stride = roundup(max_fluid, 32);
     h->ncap = p->max_neighbours;
-    h->g = make_grid(*p);
+    h->nscenes = nscenes;
+    if (nscenes == 1) {
+        h->g = make_grid(*p);
+    } else {
+        int off = 0;
+        for (int sc = 0; sc < nscenes; ++sc) {
+            SphParams q = *p;
+            for (int i = 0; i < 3; ++i) { q.spaceMin[i] = smin[3 * sc + i]; q.spaceMax[i] = smax[3 * sc + i]; }
+            GridGeom g = make_grid(q);
+            g.key0 = off;
+            g.key1 = off + g.nkeys - 1;
+            off = g.key1;
+            h->sgeom.push_back(g);
+        }
+        h->g = h->sgeom[0];
+        h->g.key0 = 0;
+        h->g.key1 = off;
+        h->g.nkeys = off + 1;  // one key space; its last key holds removed particles
+        for (auto& g : h->sgeom) g.nkeys = h->g.nkeys;
+    }
     fill_solver_const(h);
     mlp_init_attributes();
     ws_init_attributes();
     int r = alloc_scene(h);
+    if (!r && nscenes > 1) {
+        // per-scene state: grids, then one block for the BatchDev arrays
+        const size_t S = (size_t)nscenes;
+        const size_t bytes = S * (sizeof(float) + 7 * sizeof(int) + 3 * sizeof(double)) + 256;
+        if (cudaMalloc((void**)&h->d_geom, S * sizeof(GridGeom)) != cudaSuccess ||
+            cudaMalloc(&h->d_batch, bytes) != cudaSuccess) {
+            r = SPHGPU_ENOMEM;
+        } else {
+            cudaMemcpy(h->d_geom, h->sgeom.data(), S * sizeof(GridGeom), cudaMemcpyHostToDevice);
+            cudaMemset(h->d_batch, 0, bytes);
+            char* q = (char*)h->d_batch;
+            BatchDev& b = h->d.b;
+            b.err_density = (double*)q; q += S * sizeof(double);
+            b.err_div = (double*)q; q += S * sizeof(double);
+            b.vmax = (double*)q; q += S * sizeof(double);
+            b.dt = (float*)q; q += S * sizeof(float);
+            b.active = (int*)q; q += S * sizeof(int);
+            b.it_density = (int*)q; q += S * sizeof(int);
+            b.it_div = (int*)q; q += S * sizeof(int);
+            b.total_it_density = (int*)q; q += S * sizeof(int);
+            b.total_it_div = (int*)q; q += S * sizeof(int);
+            b.n = (int*)q; q += S * sizeof(int);
+            b.status = (unsigned*)q;
+            b.geom = h->d_geom;
+            std::vector<float> dts(S, p->dt);
+            cudaMemcpy(b.dt, dts.data(), S * sizeof(float), cudaMemcpyHostToDevice);
+        }
+    }
+    h->d.nscenes = nscenes;
     if (r) {
         free_scene(h);
         delete h;
@@ -767,6 +855,10 @@ int sphgpu_create(const SphParams* p, int device, int max_fluid, sphgpu_t* out) 
     }
     *out = h;
     return 0;
+}
+
+int sphgpu_create(const SphParams* p, int device, int max_fluid, sphgpu_t* out) {
+    return create_impl(p, device, max_fluid, 1, nullptr, nullptr, out);
 }
 
 int sphgpu_destroy(sphgpu_t h) {
@@ -797,14 +889,22 @@ int sphgpu_set_params(sphgpu_t h, const SphParams* p) {
     invalidate_graphs(h);
     float dt = p->dt;
     CK(cudaMemcpyAsync(h->d.dt, &dt, sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    if (h->nscenes > 1) {
+        std::vector<float> dts(h->nscenes, dt);
+        CK(cudaMemcpy(h->d.b.dt, dts.data(), sizeof(float) * h->nscenes, cudaMemcpyHostToDevice));
+    }
     CK(cudaStreamSynchronize(h->stream));
     return 0;
 }
 
-int sphgpu_set_boundary(sphgpu_t h, int n, const float* xyz, const int* solid_id, const float* volume) {
+// Boundary particles of all scenes (scene == NULL: the single scene).
+static int set_boundary_impl(sphgpu_t h, int n, const float* xyz, const int* solid_id, const int* scene, const float* volume) {
     if (!h || n < 0 || (n > 0 && !xyz)) return SPHGPU_EINVAL;
     cudaSetDevice(h->device);
     DevScene& d = h->d;
+    if (scene)
+        for (int i = 0; i < n; ++i)
+            if (scene[i] < 0 || scene[i] >= h->nscenes) { h->err = "boundary scene index out of range"; return SPHGPU_EINVAL; }
     if (d.bpos) { cudaFree(d.bpos); cudaFree(d.bvel); cudaFree(d.bgid); cudaFree(d.bpv); d.bpos = nullptr; }
     h->nb = n;
     d.nb = n;
@@ -812,22 +912,42 @@ int sphgpu_set_boundary(sphgpu_t h, int n, const float* xyz, const int* solid_id
     for (int i = 0; i < n; ++i) bp[i] = make_float4(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], volume ? volume[i] : 0.f);
     if (dalloc(h, &d.bpos, n) || dalloc(h, &d.bvel, n) || dalloc(h, &d.bgid, n) || dalloc(h, &d.bpv, 2 * (size_t)n))
         return SPHGPU_ENOMEM;
+    // cell keys on the device, each particle with its scene's grid
     std::vector<int> keys(n);
-    int* dkeys = nullptr;
-    if (dalloc(h, &dkeys, n)) return SPHGPU_ENOMEM;
-    CK(cudaMemcpy(d.bpos, bp.data(), sizeof(float4) * n, cudaMemcpyHostToDevice));
-    launch_boundary_keys(d.bpos, n, h->g, dkeys, h->stream);
-    CK(cudaStreamSynchronize(h->stream));
-    CK(cudaMemcpy(keys.data(), dkeys, sizeof(int) * n, cudaMemcpyDeviceToHost));
-    cudaFree(dkeys);
+    {
+        std::vector<int> ord(n);
+        std::iota(ord.begin(), ord.end(), 0);
+        if (scene) std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return scene[a] < scene[b]; });
+        std::vector<float4> tmp(n);
+        for (int i = 0; i < n; ++i) tmp[i] = bp[ord[i]];
+        int* dkeys = nullptr;
+        if (dalloc(h, &dkeys, n)) return SPHGPU_ENOMEM;
+        CK(cudaMemcpy(d.bpos, tmp.data(), sizeof(float4) * n, cudaMemcpyHostToDevice));
+        for (int a = 0; a < n;) {
+            int b = a;
+            const int sc = scene ? scene[ord[a]] : 0;
+            while (b < n && (scene ? scene[ord[b]] : 0) == sc) ++b;
+            const GridGeom& G = h->nscenes > 1 ? h->sgeom[sc] : h->g;
+            launch_boundary_keys(d.bpos + a, b - a, G, dkeys + a, h->stream);
+            a = b;
+        }
+        CK(cudaStreamSynchronize(h->stream));
+        std::vector<int> k2(n);
+        CK(cudaMemcpy(k2.data(), dkeys, sizeof(int) * n, cudaMemcpyDeviceToHost));
+        cudaFree(dkeys);
+        for (int i = 0; i < n; ++i) keys[ord[i]] = k2[i];
+    }
     // reference insertion rank: solids in order, each in index order (the
-    // caller's order, grouped by solid id)
+    // caller's order, grouped by solid id; in a batch, by scene first)
     std::vector<int> rank(n);
     {
         std::vector<int> ord(n);
         std::iota(ord.begin(), ord.end(), 0);
-        if (solid_id)
-            std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return solid_id[a] < solid_id[b]; });
+        std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) {
+            const int sa = scene ? scene[a] : 0, sb = scene ? scene[b] : 0;
+            if (sa != sb) return sa < sb;
+            return solid_id ? solid_id[a] < solid_id[b] : false;
+        });
         for (int i = 0; i < n; ++i) rank[ord[i]] = i;
     }
     for (int i = 0; i < n; ++i)
@@ -856,7 +976,12 @@ int sphgpu_set_boundary(sphgpu_t h, int n, const float* xyz, const int* solid_id
     CK(cudaMemcpy(d.bgid, h->bgid_h.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(d.bcell_start, start.data(), sizeof(int) * (h->g.nkeys + 1), cudaMemcpyHostToDevice));
     if (!volume) {
-        launch_boundary_volume(d, h->g, h->P.particle_d, h->c.h2cut, h->ncap, h->stream);
+        // each scene's walls with its own grid: its sorted range is contiguous
+        for (int sc = 0; sc < h->nscenes; ++sc) {
+            const GridGeom& G = h->nscenes > 1 ? h->sgeom[sc] : h->g;
+            launch_boundary_volume(d, G, h->P.particle_d, h->c.h2cut, h->ncap, start[G.key0], start[G.key1],
+                                   h->stream);
+        }
         CK(cudaStreamSynchronize(h->stream));
     }
     // packed {(x, y, z, volume), velocity} records for the sweeps
@@ -870,14 +995,39 @@ int sphgpu_set_boundary(sphgpu_t h, int n, const float* xyz, const int* solid_id
     return 0;
 }
 
-int sphgpu_add_fluid(sphgpu_t h, int n, const float* xyz, const float* vel, float rho0, float visc_alpha) {
+int sphgpu_set_boundary(sphgpu_t h, int n, const float* xyz, const int* solid_id, const float* volume) {
+    if (h && h->nscenes > 1) { h->err = "a batch takes its walls through sphgpu_batch_set_boundary"; return SPHGPU_EINVAL; }
+    return set_boundary_impl(h, n, xyz, solid_id, nullptr, volume);
+}
+
+// Append fluid particles: a new phase of the single scene (scene == NULL),
+// or, in a batch, particles of the given scenes (all in phase 0; the global
+// index order is scene by scene, each scene in the caller's order).
+static int add_fluid_impl(sphgpu_t h, int n, const float* xyz, const float* vel, float rho0, float visc_alpha,
+                          const int* scene) {
     if (!h || n <= 0 || !xyz || !(rho0 > 0)) return SPHGPU_EINVAL;
-    if (h->rho0_ph.size() >= 4) { h->err = "at most 4 fluid phases"; return SPHGPU_EINVAL; }
+    if (!scene && h->rho0_ph.size() >= 4) { h->err = "at most 4 fluid phases"; return SPHGPU_EINVAL; }
+    if (scene && !h->rho0_ph.empty() && (h->rho0_ph[0] != rho0 || h->alpha_ph[0] != visc_alpha)) {
+        h->err = "the scenes of a batch share one rest density and viscosity";
+        return SPHGPU_EINVAL;
+    }
+    std::vector<int> sord;  // batch: particles grouped by scene, stable
+    if (scene) {
+        for (int i = 0; i < n; ++i)
+            if (scene[i] < 0 || scene[i] >= h->nscenes) { h->err = "scene index out of range"; return SPHGPU_EINVAL; }
+        sord.resize(n);
+        std::iota(sord.begin(), sord.end(), 0);
+        std::stable_sort(sord.begin(), sord.end(), [&](int a, int b) { return scene[a] < scene[b]; });
+        if (scene[sord[0]] < h->last_scene) {
+            h->err = "batch fluid must be added scene by scene in increasing order";
+            return SPHGPU_EINVAL;
+        }
+    }
     cudaSetDevice(h->device);
     CK(cudaStreamSynchronize(h->stream));
     int cur = h->h_stats->n_active;
     if (cur + n > h->cap) { h->err = "fluid capacity exceeded"; return SPHGPU_EINVAL; }
-    int phase = (int)h->rho0_ph.size();
+    int phase = scene ? 0 : (int)h->rho0_ph.size();
     // bring the existing particles into staging in reference order
     std::vector<float4> P(cur + n), V(cur + n);
     std::vector<float4> carried[3];
@@ -901,12 +1051,14 @@ int sphgpu_add_fluid(sphgpu_t h, int n, const float* xyz, const float* vel, floa
             for (int k = 0; k < m; ++k) carried[a][k] = t[order[k]];
         }
     }
-    for (int i = 0; i < n; ++i) {
-        P[cur + i] = make_float4(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], int_bits_as_float(phase));
-        V[cur + i] = vel ? make_float4(vel[3 * i], vel[3 * i + 1], vel[3 * i + 2], 0.f) : make_float4(0, 0, 0, 0);
+    for (int k = 0; k < n; ++k) {
+        const int i = scene ? sord[k] : k;
+        const int w = phase | (scene ? scene[i] << 4 : 0);
+        P[cur + k] = make_float4(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], int_bits_as_float(w));
+        V[cur + k] = vel ? make_float4(vel[3 * i], vel[3 * i + 1], vel[3 * i + 2], 0.f) : make_float4(0, 0, 0, 0);
         // a new particle's density is its rest density (as the reference's
         // scene setup leaves it before the first step)
-        carried[1][cur + i] = make_float4(0.f, 0.f, 0.f, rho0);
+        carried[1][cur + k] = make_float4(0.f, 0.f, 0.f, rho0);
     }
     std::vector<int> G(cur + n);
     std::iota(G.begin(), G.end(), 0);
@@ -918,15 +1070,25 @@ int sphgpu_add_fluid(sphgpu_t h, int n, const float* xyz, const float* vel, floa
     CK(cudaMemcpy(h->d.cC_s, carried[2].data(), sizeof(float4) * (cur + n), cudaMemcpyHostToDevice));
     h->h_stats->n_active = cur + n;
     CK(cudaMemcpy(&h->d.st->n_active, &h->h_stats->n_active, sizeof(int), cudaMemcpyHostToDevice));
-    h->rho0_ph.push_back(rho0);
-    h->alpha_ph.push_back(visc_alpha);
-    h->phase_n.push_back(n);
+    if (!scene || h->rho0_ph.empty()) {
+        h->rho0_ph.push_back(rho0);
+        h->alpha_ph.push_back(visc_alpha);
+        h->phase_n.push_back(n);
+    } else {
+        h->phase_n[0] += n;
+    }
+    if (scene) h->last_scene = scene[sord[n - 1]];
     h->n_total = cur + n;
     fill_solver_const(h);
     invalidate_graphs(h);
     h->in_staging = true;
     h->ns_valid = false;
     return phase;
+}
+
+int sphgpu_add_fluid(sphgpu_t h, int n, const float* xyz, const float* vel, float rho0, float visc_alpha) {
+    if (h && h->nscenes > 1) { h->err = "a batch takes its fluid through sphgpu_batch_add_fluid"; return SPHGPU_EINVAL; }
+    return add_fluid_impl(h, n, xyz, vel, rho0, visc_alpha, nullptr);
 }
 
 int sphgpu_num_fluid(sphgpu_t h) {
@@ -1166,6 +1328,7 @@ int sphgpu_get_boundary(sphgpu_t h, const char* field, float* out) {
 
 int sphgpu_stage(sphgpu_t h, const char* name, SphStepStats* stats) {
     if (!h || !name) return SPHGPU_EINVAL;
+    if (h->nscenes > 1) { h->err = "stages are for single scenes"; return SPHGPU_EINVAL; }
     cudaSetDevice(h->device);
     h->err.clear();
     std::string s(name);
@@ -1199,7 +1362,7 @@ int sphgpu_stage(sphgpu_t h, const char* name, SphStepStats* stats) {
         if (r) return r;
         // integrate into staging (the reference updates positions in place)
         cudaMemsetAsync(d.cell_count, 0, sizeof(int) * ((size_t)h->g.nkeys + 1), st);
-        launch_hash(d, h->g, h->P.spaceMin, h->P.spaceMax, 1, h->cap, st);
+        launch_hash(d, h->g, 1, h->cap, st);
         h->in_staging = true;
         h->ns_valid = false;
     } else if (s == "DF_divergenceFreeSolver") {
@@ -1278,6 +1441,7 @@ int sphgpu_get_neighbours(sphgpu_t h, int* counts, int* t, int* idx) {
 }
 
 int sphgpu_get_cells(sphgpu_t h, long long* cell) {
+    if (h && h->nscenes > 1) { h->err = "reference cell indices are for single scenes"; return SPHGPU_EINVAL; }
     if (!h || !cell) return SPHGPU_EINVAL;
     cudaSetDevice(h->device);
     std::vector<float> p(3 * (size_t)std::max(1, h->h_stats->n_active));
@@ -1575,6 +1739,97 @@ int sphgpu_attach_warm_start(sphgpu_t h, sphgpu_mlp_t m, int mode, int record_ev
     if (mode != 1 && mode != 3) cudaMemsetAsync(h->d.kwarm, 0, sizeof(float) * h->cap, h->stream);
     invalidate_graphs(h);
     return cudaStreamSynchronize(h->stream) == cudaSuccess ? 0 : SPHGPU_ECUDA;
+}
+
+// ---- batch of independent scenes ----
+int sphgpu_batch_create(const SphParams* p, int nscenes, const float* space_min, const float* space_max, int device,
+                        int max_fluid, sphgpu_t* out) {
+    if (nscenes < 1 || !space_min || !space_max) return SPHGPU_EINVAL;
+    if (nscenes == 1) {
+        SphParams q = *p;
+        for (int i = 0; i < 3; ++i) { q.spaceMin[i] = space_min[i]; q.spaceMax[i] = space_max[i]; }
+        return create_impl(&q, device, max_fluid, 1, nullptr, nullptr, out);
+    }
+    return create_impl(p, device, max_fluid, nscenes, space_min, space_max, out);
+}
+
+int sphgpu_batch_num_scenes(sphgpu_t h) { return h ? h->nscenes : SPHGPU_EINVAL; }
+
+int sphgpu_batch_set_boundary(sphgpu_t h, int n, const float* xyz, const int* scene) {
+    if (!h || (n > 0 && !scene)) return SPHGPU_EINVAL;
+    return set_boundary_impl(h, n, xyz, nullptr, h->nscenes > 1 ? scene : nullptr, nullptr);
+}
+
+int sphgpu_batch_add_fluid(sphgpu_t h, int n, const float* xyz, const float* vel, const int* scene, float rho0,
+                           float visc_alpha) {
+    if (!h || (n > 0 && !scene)) return SPHGPU_EINVAL;
+    return add_fluid_impl(h, n, xyz, vel, rho0, visc_alpha, h->nscenes > 1 ? scene : nullptr);
+}
+
+int sphgpu_batch_stats(sphgpu_t h, SphStepStats* out, int cap) {
+    if (!h || !out || cap <= 0) return SPHGPU_EINVAL;
+    cudaSetDevice(h->device);
+    CK(cudaStreamSynchronize(h->stream));
+    if (h->nscenes == 1) {
+        fill_stats(h, out, 0);
+        return 1;
+    }
+    const int S = h->nscenes;
+    const BatchDev& b = h->d.b;
+    std::vector<double> ed(S), ev(S);
+    std::vector<float> dt(S);
+    std::vector<int> itd(S), itv(S), ttd(S), ttv(S), nn(S);
+    std::vector<unsigned> stt(S);
+    CK(cudaMemcpy(ed.data(), b.err_density, S * sizeof(double), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(ev.data(), b.err_div, S * sizeof(double), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(dt.data(), b.dt, S * sizeof(float), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(itd.data(), b.it_density, S * sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(itv.data(), b.it_div, S * sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(ttd.data(), b.total_it_density, S * sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(ttv.data(), b.total_it_div, S * sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(nn.data(), b.n, S * sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(stt.data(), b.status, S * sizeof(unsigned), cudaMemcpyDeviceToHost));
+    const int m = std::min(cap, S);
+    for (int i = 0; i < m; ++i) {
+        SphStepStats& o = out[i];
+        memset(&o, 0, sizeof(o));
+        o.n_fluid = nn[i];
+        o.iter_density = itd[i];
+        o.iter_divergence = itv[i];
+        o.err_density = ed[i];
+        o.err_divergence = ev[i];
+        o.dt = dt[i];
+        o.status = stt[i];
+        o.total_iter_density = ttd[i];
+        o.total_iter_divergence = ttv[i];
+    }
+    return m;
+}
+
+int sphgpu_batch_scene_range(sphgpu_t h, int scene, int* first, int* count) {
+    if (!h || scene < 0 || scene >= h->nscenes || !first || !count) return SPHGPU_EINVAL;
+    cudaSetDevice(h->device);
+    CK(cudaStreamSynchronize(h->stream));
+    if (h->nscenes == 1) { *first = 0; *count = h->h_stats->n_active; return 0; }
+    std::vector<int> nn(h->nscenes);
+    if (h->in_staging && !h->ns_valid && h->frame == 0) {
+        // before the first step: counts as added
+        std::vector<float4> P(h->h_stats->n_active);
+        CK(cudaMemcpy(P.data(), h->d.pos_s, sizeof(float4) * P.size(), cudaMemcpyDeviceToHost));
+        std::fill(nn.begin(), nn.end(), 0);
+        for (auto& q : P) {
+            int w;
+            memcpy(&w, &q.w, sizeof w);
+            nn[w >> 4]++;
+        }
+    } else {
+        CK(cudaMemcpy(nn.data(), h->d.b.n, sizeof(int) * h->nscenes, cudaMemcpyDeviceToHost));
+    }
+    int f = 0;
+    for (int i = 0; i < scene; ++i) f += nn[i];
+    *first = f;
+    *count = nn[scene];
+    return 0;
 }
 
 // Internal controls used by the Python host layer (not part of the

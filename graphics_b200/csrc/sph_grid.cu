@@ -24,7 +24,7 @@
 namespace {
 constexpr int NT = 256;
 
-__global__ void __launch_bounds__(NT) k_hash(DevScene s, GridGeom g, float3 smin, float3 smax, int integrate) {
+__global__ void __launch_bounds__(NT) k_hash(DevScene s, GridGeom g, int integrate) {
     const int n = s.st->n_active;
     if (blockIdx.x == 0 && threadIdx.x == 0) s.st->pad0 = n;  // staged count
     int i = blockIdx.x * NT + threadIdx.x;
@@ -34,8 +34,8 @@ __global__ void __launch_bounds__(NT) k_hash(DevScene s, GridGeom g, float3 smin
         if (integrate) {
             // Second loop 2.4: velocity = vel_adv; position += velocity*dt
             // (DFSPH.cpp:705-715), in round-to-nearest float ops.
-            float dt = *s.dt;
             p = s.pos[i];
+            const float dt = dt_of(s, p);
             v = s.pv[2 * i + 1];  // v_adv of the density loop
             p.x = __fadd_rn(p.x, __fmul_rn(v.x, dt));
             p.y = __fadd_rn(p.y, __fmul_rn(v.y, dt));
@@ -48,15 +48,17 @@ __global__ void __launch_bounds__(NT) k_hash(DevScene s, GridGeom g, float3 smin
         } else {
             p = s.pos_s[i];
         }
+        // the particle's scene grid (the only grid unless this is a batch)
+        const GridGeom G = s.nscenes > 1 ? s.b.geom[scene_of(p)] : g;
         // SphFluid::removeOutsideParts test (SphBase.cpp:34-44, Vec23.h:193-194)
-        bool in = smin.x <= p.x && smin.y <= p.y && smin.z <= p.z && p.x <= smax.x && p.y <= smax.y &&
-                  p.z <= smax.z;
+        bool in = G.smin[0] <= p.x && G.smin[1] <= p.y && G.smin[2] <= p.z && p.x <= G.smax[0] &&
+                  p.y <= G.smax[1] && p.z <= G.smax[2];
         int key = g.nkeys - 1;
         if (in) {
-            int cx = cell_coord(p.x, g.min[0], g.divisor);
-            int cy = cell_coord(p.y, g.min[1], g.divisor);
-            int cz = cell_coord(p.z, g.min[2], g.divisor);
-            if (cell_inside(g, cx, cy, cz)) key = cell_key(g, cx, cy, cz);
+            int cx = cell_coord(p.x, G.min[0], G.divisor);
+            int cy = cell_coord(p.y, G.min[1], G.divisor);
+            int cz = cell_coord(p.z, G.min[2], G.divisor);
+            if (cell_inside(G, cx, cy, cz)) key = cell_key(G, cx, cy, cz);
             else removed = 1;
         } else {
             removed = 1;
@@ -131,19 +133,20 @@ __global__ void __launch_bounds__(128) k_build(DevScene s, GridGeom g, SolverCon
         const float fm0 = c.fm_ph[ph], rho0 = c.rho0_ph[ph];
         const float4* __restrict__ P = s.pos;
         const float4* __restrict__ BP = s.bpos;
-        const int cx = cell_coord(pa.x, g.min[0], g.divisor);
-        const int cy = cell_coord(pa.y, g.min[1], g.divisor);
-        const int cz = cell_coord(pa.z, g.min[2], g.divisor);
+        const GridGeom G = s.nscenes > 1 ? s.b.geom[scene_of(pa)] : g;
+        const int cx = cell_coord(pa.x, G.min[0], G.divisor);
+        const int cy = cell_coord(pa.y, G.min[1], G.divisor);
+        const int cz = cell_coord(pa.z, G.min[2], G.divisor);
         int* out = s.nbr;
         const size_t stride = (size_t)c.stride;
         const int cap = c.cap;
         // distances to the faces of the own cell, for skipping neighbour cells
         // that lie beyond the cut (with a margin, so only cells that provably
         // hold no neighbour are skipped; the candidate test itself is exact)
-        const float hc = 1.f / g.divisor;
-        const float lo_x = pa.x - (g.min[0] + cx * hc), hi_x = (g.min[0] + (cx + 1) * hc) - pa.x;
-        const float lo_y = pa.y - (g.min[1] + cy * hc), hi_y = (g.min[1] + (cy + 1) * hc) - pa.y;
-        const float lo_z = pa.z - (g.min[2] + cz * hc), hi_z = (g.min[2] + (cz + 1) * hc) - pa.z;
+        const float hc = 1.f / G.divisor;
+        const float lo_x = pa.x - (G.min[0] + cx * hc), hi_x = (G.min[0] + (cx + 1) * hc) - pa.x;
+        const float lo_y = pa.y - (G.min[1] + cy * hc), hi_y = (G.min[1] + (cy + 1) * hc) - pa.y;
+        const float lo_z = pa.z - (G.min[2] + cz * hc), hi_z = (G.min[2] + (cz + 1) * hc) - pa.z;
         const float cull = c.h2cut * 1.001f + 1e-12f;
         // phase 1: candidate scan in the reference's order, append indices
         for (int dz = -1; dz <= 1; ++dz) {
@@ -154,8 +157,8 @@ __global__ void __launch_bounds__(128) k_build(DevScene s, GridGeom g, SolverCon
                     const float gx = dx < 0 ? fmaxf(lo_x, 0.f) : (dx > 0 ? fmaxf(hi_x, 0.f) : 0.f);
                     if (gx * gx + gy * gy + gz * gz > cull) continue;
                     const int x = cx + dx, y = cy + dy, z = cz + dz;
-                    if (!cell_inside(g, x, y, z)) continue;
-                    const int key = cell_key(g, x, y, z);
+                    if (!cell_inside(G, x, y, z)) continue;
+                    const int key = cell_key(G, x, y, z);
                     const int2 s0 = __ldg(s.cstart2 + key), s1 = __ldg(s.cstart2 + key + 1);
                     for (int q = s0.x; q < s1.x; ++q) {
                         const float4 pb = __ldg(P + q);
@@ -239,9 +242,10 @@ __global__ void k_boundary_keys(const float4* bpos, int nb, GridGeom g, int* key
 // (SphBase.cpp:766-813) with only boundary particles in the grid:
 // V_b = 1 / (W(0, d) + sum over the (capped) boundary neighbour list of
 // W(dis, (d_a + d_b)/2)).
-__global__ void __launch_bounds__(128) k_boundary_volume(DevScene s, GridGeom g, float dpart, float h2cut, int cap) {
-    int p = blockIdx.x * 128 + threadIdx.x;
-    if (p >= s.nb) return;
+__global__ void __launch_bounds__(128) k_boundary_volume(DevScene s, GridGeom g, float dpart, float h2cut, int cap,
+                                                         int b0, int b1) {
+    int p = b0 + blockIdx.x * 128 + threadIdx.x;
+    if (p >= b1) return;
     float4 pa = s.bpos[p];
     int cx = cell_coord(pa.x, g.min[0], g.divisor);
     int cy = cell_coord(pa.y, g.min[1], g.divisor);
@@ -303,10 +307,8 @@ void launch_from_ref_order(const float* src3, const int* gid, int n, float4* dst
 }
 
 
-void launch_hash(const DevScene& s, const GridGeom& g, const float* smin, const float* smax, int integrate,
-                 int n_old, cudaStream_t st) {
-    k_hash<<<nblk(n_old > 0 ? n_old : 1, NT), NT, 0, st>>>(s, g, make_float3(smin[0], smin[1], smin[2]),
-                                                          make_float3(smax[0], smax[1], smax[2]), integrate);
+void launch_hash(const DevScene& s, const GridGeom& g, int integrate, int n_old, cudaStream_t st) {
+    k_hash<<<nblk(n_old > 0 ? n_old : 1, NT), NT, 0, st>>>(s, g, integrate);
 }
 
 void launch_scatter_reorder(const DevScene& s, const GridGeom& g, int n_old, int carry, cudaStream_t st) {
@@ -331,7 +333,7 @@ void launch_boundary_keys(const float4* bpos, int nb, const GridGeom& g, int* ke
     if (nb > 0) k_boundary_keys<<<nblk(nb, NT), NT, 0, st>>>(bpos, nb, g, keys);
 }
 
-void launch_boundary_volume(const DevScene& s, const GridGeom& g, float dpart, float h2cut, int cap,
+void launch_boundary_volume(const DevScene& s, const GridGeom& g, float dpart, float h2cut, int cap, int b0, int b1,
                             cudaStream_t st) {
-    if (s.nb > 0) k_boundary_volume<<<nblk(s.nb, 128), 128, 0, st>>>(s, g, dpart, h2cut, cap);
+    if (b1 > b0) k_boundary_volume<<<nblk(b1 - b0, 128), 128, 0, st>>>(s, g, dpart, h2cut, cap, b0, b1);
 }

@@ -33,6 +33,23 @@ struct DevStats {
     double ii_nb_cum;
 };
 
+// Per-scene state of a batch (many independent scenes in one set of
+// arrays): each scene converges and picks its time step on its own.
+struct BatchDev {
+    const GridGeom* geom;  // [nscenes] grid of each scene (its key range)
+    float* dt;             // [nscenes] step length
+    int* active;           // [nscenes] 1 while the scene's current loop runs
+    int* it_density;       // [nscenes] iterations of the last density / divergence loop
+    int* it_div;
+    int* total_it_density; // [nscenes] summed over the steps of the current call
+    int* total_it_div;
+    int* n;                // [nscenes] active particles
+    unsigned* status;      // [nscenes] status bits
+    double* err_density;   // [nscenes]
+    double* err_div;
+    double* vmax;
+};
+
 // Per-scene device pointers passed to every kernel by value.
 struct DevScene {
     // fluid, cell-sorted
@@ -92,11 +109,22 @@ struct DevScene {
     double* partial;    // >= number of blocks of a particle launch
     DevStats* st;
     float* dt;          // == &st->dt
+    // batch of independent scenes (nscenes > 1); scene index in pos.w
+    int nscenes;
+    BatchDev b;
 };
 
+// step length of the particle's scene
+__device__ __forceinline__ float dt_of(const DevScene& s, float4 pa) {
+    return s.nscenes > 1 ? s.b.dt[scene_of(pa)] : *s.dt;
+}
+// in a batch: is the particle's scene still iterating its current loop?
+__device__ __forceinline__ bool scene_active(const DevScene& s, float4 pa) {
+    return s.nscenes <= 1 || s.b.active[scene_of(pa)] != 0;
+}
+
 // ---- neighbour search (sph_grid.cu) ----
-void launch_hash(const DevScene& s, const GridGeom& g, const float* smin, const float* smax, int integrate,
-                 int n_old, cudaStream_t st);
+void launch_hash(const DevScene& s, const GridGeom& g, int integrate, int n_old, cudaStream_t st);
 // carry: bit 0 hist, bit 1 cA, bit 2 cB, bit 3 cC (staging -> sorted)
 void launch_scatter_reorder(const DevScene& s, const GridGeom& g, int n_old, int carry, cudaStream_t st);
 void launch_count_active(const DevScene& s, const GridGeom& g, cudaStream_t st);
@@ -105,7 +133,8 @@ void launch_build(const DevScene& s, const GridGeom& g, const SolverConst& c, in
 void launch_to_ref_order(const float4* src, const int* gid, int n, float* dst3, cudaStream_t st);
 void launch_from_ref_order(const float* src3, const int* gid, int n, float4* dst, cudaStream_t st);
 void launch_boundary_keys(const float4* bpos, int nb, const GridGeom& g, int* keys, cudaStream_t st);
-void launch_boundary_volume(const DevScene& s, const GridGeom& g, float dpart, float h2cut, int cap,
+// boundary particles [b0, b1) (one scene of a batch, or all)
+void launch_boundary_volume(const DevScene& s, const GridGeom& g, float dpart, float h2cut, int cap, int b0, int b1,
                             cudaStream_t st);
 
 // ---- DFSPH (sph_dfsph.cu) ----
@@ -122,6 +151,15 @@ void launch_df_loop_reset(const DevScene& s, int which, cudaStream_t st);
 void launch_cfl(const DevScene& s, int n_max, float cfl, float d, float dt_max, float dt_min, cudaStream_t st);
 void launch_step_begin(const DevScene& s, cudaStream_t st);
 void launch_call_begin(const DevScene& s, cudaStream_t st);
+
+// ---- batch of scenes (sph_batch.cu) ----
+void launch_batch_loop_reset(const DevScene& s, int nscenes, int which, cudaStream_t st);
+void launch_batch_decide(const DevScene& s, const SolverConst& c, int which, int nscenes, double goal_abs,
+                         double goal_rel, int min_it, int max_it, unsigned long long cond_handle, int use_handle,
+                         cudaStream_t st);
+void launch_batch_cfl(const DevScene& s, int nscenes, float cfl, float d, float dt_max, float dt_min, cudaStream_t st);
+void launch_batch_call_begin(const DevScene& s, int nscenes, cudaStream_t st);
+void launch_batch_count(const DevScene& s, int nscenes, cudaStream_t st);
 
 // ---- WCSPH (sph_wcsph.cu) ----
 void launch_wc_force(const DevScene& s, const SolverConst& c, int n_max, cudaStream_t st);

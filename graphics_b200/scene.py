@@ -153,3 +153,22 @@ def small_dam_break(n=(10, 10, 10), r=0.025, box=None, seed=0):
     if box is None:
         box = (4 * n[0] * r, 2 * n[1] * r, 2 * n[2] * r)
     return dam_break(n, r, box, seed=seed)
+
+
+def config_batched_dfsph(nscenes=64, seed=0, r=0.01, n_min=1e4, n_max=2e5):
+    """Independent dam breaks of uneven size for a batch: N_i drawn
+    log-uniformly from [n_min, n_max], block aspect ratios uniform in
+    [0.5, 2] per axis (normalised so the lattice holds about N_i particles),
+    each block in its own walled box twice its length along x."""
+    rng = np.random.default_rng(seed)
+    scenes = []
+    d = 2.0 * r
+    for i in range(nscenes):
+        n = float(np.exp(rng.uniform(np.log(n_min), np.log(n_max))))
+        a = rng.uniform(0.5, 2.0, 3)
+        a = a / np.prod(a) ** (1.0 / 3.0)
+        counts = tuple(max(2, int(round(n ** (1.0 / 3.0) * a[k]))) for k in range(3))
+        box = (2.0 * counts[0] * d, counts[1] * d, counts[2] * d)
+        scenes.append(dam_break(counts, r, box, seed=seed * 1000 + i))
+    return scenes
+

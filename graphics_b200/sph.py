@@ -224,6 +224,70 @@ class GpuScene:
         self._check(self.lib.sphgpu_debug_set(self.h, key.encode(), int(value)), "debug_set " + key)
 
 
+class GpuBatch(GpuScene):
+    """Many independent DFSPH scenes in one handle (sphgpu_batch_*): one
+    set of arrays, per-scene boxes, CFL steps and loop convergence."""
+
+    def __init__(self, params, space_min, space_max, max_fluid, device=0):
+        self.lib = _lib.load()
+        self.params = params
+        smin = np.ascontiguousarray(space_min, dtype=np.float32).reshape(-1, 3)
+        smax = np.ascontiguousarray(space_max, dtype=np.float32).reshape(-1, 3)
+        self.nscenes = len(smin)
+        h = C.c_void_p()
+        rc = self.lib.sphgpu_batch_create(C.byref(params), self.nscenes, _fptr(smin), _fptr(smax), int(device),
+                                          int(max_fluid), C.byref(h))
+        if rc:
+            raise SphGpuError(rc, "sphgpu_batch_create failed (is a CUDA device present?)")
+        self.h = h
+        self.nb = 0
+
+    def set_boundary(self, pos, scene):
+        pos = np.ascontiguousarray(pos, dtype=np.float32)
+        sc = np.ascontiguousarray(scene, dtype=np.int32)
+        self._check(self.lib.sphgpu_batch_set_boundary(self.h, len(pos), _fptr(pos),
+                                                       sc.ctypes.data_as(C.POINTER(C.c_int))), "batch_set_boundary")
+        self.nb = len(pos)
+
+    def add_fluid(self, pos, vel, scene, rho0=1000.0, visc_alpha=0.0):
+        pos = np.ascontiguousarray(pos, dtype=np.float32)
+        vel = np.ascontiguousarray(vel, dtype=np.float32)
+        sc = np.ascontiguousarray(scene, dtype=np.int32)
+        return self._check(self.lib.sphgpu_batch_add_fluid(self.h, len(pos), _fptr(pos), _fptr(vel),
+                                                           sc.ctypes.data_as(C.POINTER(C.c_int)), float(rho0),
+                                                           float(visc_alpha)), "batch_add_fluid")
+
+    def scene_stats(self):
+        out = (SphStepStats * self.nscenes)()
+        m = self._check(self.lib.sphgpu_batch_stats(self.h, out, self.nscenes), "batch_stats")
+        return [out[i].as_dict() for i in range(m)]
+
+    def scene_range(self, k):
+        a, b = C.c_int(), C.c_int()
+        self._check(self.lib.sphgpu_batch_scene_range(self.h, int(k), C.byref(a), C.byref(b)), "batch_scene_range")
+        return a.value, b.value
+
+    def get_scene(self, field, k):
+        a, n = self.scene_range(k)
+        return self.get(field)[a:a + n]
+
+
+def batch_to_gpu(scenes, device=0, max_fluid=None, **params):
+    """GpuBatch holding a list of graphics_b200.scene.Scene (one phase each,
+    same particle size and rest density), walls as each scene's static solid."""
+    p = params_for_scene(scenes[0], **params)
+    smin = np.array([sc.space_min for sc in scenes], np.float32)
+    smax = np.array([sc.space_max for sc in scenes], np.float32)
+    n = sum(sc.n_fluid for sc in scenes)
+    b = GpuBatch(p, smin, smax, max_fluid or n, device=device)
+    b.set_boundary(np.concatenate([sc.boundary_pos for sc in scenes]),
+                   np.concatenate([np.full(len(sc.boundary_pos), k, np.int32) for k, sc in enumerate(scenes)]))
+    b.add_fluid(np.concatenate([sc.fluid_pos for sc in scenes]), np.concatenate([sc.fluid_vel for sc in scenes]),
+                np.concatenate([np.full(sc.n_fluid, k, np.int32) for k, sc in enumerate(scenes)]),
+                rho0=scenes[0].rho0)
+    return b
+
+
 def scene_to_gpu(scene, device=0, max_fluid=None, **params):
     """GpuScene holding a graphics_b200.scene.Scene (walls as one static solid)."""
     p = params_for_scene(scene, **params)

@@ -240,6 +240,30 @@ int sphgpu_attach_warm_start(sphgpu_t h, sphgpu_mlp_t m, int mode, int record_ev
 /* Copy of the last error message. */
 int sphgpu_last_error(sphgpu_t h, char* buf, int len);
 
+/* ---------------- batch of independent scenes (no reference counterpart) ----------------
+ * Many DFSPH scenes of uneven size in one handle: one set of arrays, one
+ * neighbour search and one launch per sweep for all of them, each scene with
+ * its own box and grid, its own CFL step and its own loop convergence (a
+ * converged scene stops iterating while the others continue).  All scenes
+ * share the SphParams (kernel, rest density, goals); space_min/space_max
+ * give each scene's box (3 floats per scene).  The handle is used with the
+ * ordinary calls (sphgpu_step, sphgpu_get_fluid, ...); fluid is returned
+ * scene by scene (see sphgpu_batch_scene_range).  Plain DFSPH only. */
+int sphgpu_batch_create(const SphParams* p, int nscenes, const float* space_min, const float* space_max, int device,
+                        int max_fluid, sphgpu_t* out);
+int sphgpu_batch_num_scenes(sphgpu_t h);
+/* walls of every scene: scene[i] = scene index of boundary particle i */
+int sphgpu_batch_set_boundary(sphgpu_t h, int n, const float* xyz, const int* scene);
+/* fluid particles with their scene indices (scenes in increasing order
+ * across calls; one rest density and viscosity for the whole batch) */
+int sphgpu_batch_add_fluid(sphgpu_t h, int n, const float* xyz, const float* vel, const int* scene, float rho0,
+                           float visc_alpha);
+/* per-scene statistics of the last step (iterations, errors, dt, status);
+ * returns the number of scenes written (<= cap) */
+int sphgpu_batch_stats(sphgpu_t h, SphStepStats* out, int cap);
+/* the scene's particles are [first, first + count) of sphgpu_get_fluid's output */
+int sphgpu_batch_scene_range(sphgpu_t h, int scene, int* first, int* count);
+
 /* CFL time step from velocities that already live on the device, without
  * allocating anything (no counterpart in the reference, whose dt is fixed).
  * It is the in-step rule of sphgpu_step with cfl != 0:
