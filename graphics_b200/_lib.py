@@ -86,6 +86,7 @@ SIGNATURES = {
     "sphgpu_mlp_predict": (_i, [_vp, _fp, _fp, _i]),
     "sphgpu_attach_warm_start": (_i, [_vp, _vp, _i, _i]),
     "sphgpu_cfl_dt_noalloc": (_i, [_vp, _i, _i, _f, _f, _f, _f, _vp, _vp, _vp]),
+    "sphgpu_autotune": (_i, [_vp, _i, _i, _cp, _i]),
     "sphgpu_batch_create": (_i, [C.POINTER(SphParams), _i, _fp, _fp, _i, _i, C.POINTER(_vp)]),
     "sphgpu_batch_num_scenes": (_i, [_vp]),
     "sphgpu_batch_set_boundary": (_i, [_vp, _i, _fp, _ip]),

@@ -29,6 +29,7 @@ constexpr int NT = 128;
 
 // last-block FP64 reduction of per-block partials; returns true in the
 // thread that holds the total (thread 0 of the last block).
+template <int BS>
 __device__ __forceinline__ bool finish_sum(double* partial, unsigned* ticket, double v, double* total) {
     __shared__ bool last;
     if (threadIdx.x == 0) {
@@ -40,10 +41,10 @@ __device__ __forceinline__ bool finish_sum(double* partial, unsigned* ticket, do
     __syncthreads();
     if (!last) return false;
     __threadfence();
-    __shared__ double sh[NT / 32];
+    __shared__ double sh[BS / 32];
     double acc = 0;
-    for (int i = threadIdx.x; i < (int)gridDim.x; i += NT) acc += ((volatile double*)partial)[i];
-    double tot = block_sum_double<NT>(acc, sh);
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += BS) acc += ((volatile double*)partial)[i];
+    double tot = block_sum_double<BS>(acc, sh);
     if (threadIdx.x == 0) {
         *total = tot;
         *ticket = 0u;
@@ -81,9 +82,10 @@ __global__ void k_loop_reset(DevScene s, int which) {
 }
 
 // non-pressure accelerations (gravity + viscosity) and v_adv
-__global__ void __launch_bounds__(NT) k_df_forces(DevScene s, SolverConst c, int warm) {
+template <int BS>
+__global__ void __launch_bounds__(BS) k_df_forces(DevScene s, SolverConst c, int warm) {
     const int n = s.st->n_active;
-    const int p = blockIdx.x * NT + threadIdx.x;
+    const int p = blockIdx.x * BS + threadIdx.x;
     int zero = 0;
     if (p < n) {
         const float4 pa = s.pos[p];
@@ -178,9 +180,10 @@ __device__ __forceinline__ float div_sweep(const DevScene& s, const SolverConst&
 }
 
 // density loop, part A: rho_adv, kappa, FP64 sum of rho_adv
-__global__ void __launch_bounds__(NT) k_df_dens_a(DevScene s, SolverConst c, int record) {
+template <int BS>
+__global__ void __launch_bounds__(BS) k_df_dens_a(DevScene s, SolverConst c, int record) {
     const int n = s.st->n_active;
-    const int p = blockIdx.x * NT + threadIdx.x;
+    const int p = blockIdx.x * BS + threadIdx.x;
     double mine = 0.0;
     if (p < n && scene_active(s, s.pv[2 * p])) {
         const float4 pa = s.pv[2 * p];
@@ -200,10 +203,10 @@ __global__ void __launch_bounds__(NT) k_df_dens_a(DevScene s, SolverConst c, int
         mine = (double)dadv;
     }
     if (s.nscenes > 1) return;  // a batch reduces per scene (k_batch_decide)
-    __shared__ double sh[NT / 32];
-    double bs = block_sum_double<NT>(mine, sh);
+    __shared__ double sh[BS / 32];
+    double bs = block_sum_double<BS>(mine, sh);
     double tot;
-    if (finish_sum(s.partial, &s.st->ticket[0], bs, &tot)) {
+    if (finish_sum<BS>(s.partial, &s.st->ticket[0], bs, &tot)) {
         s.st->err_density = (tot / (double)n - (double)c.rho0) / (double)c.rho0;
     }
 }
@@ -211,12 +214,12 @@ __global__ void __launch_bounds__(NT) k_df_dens_a(DevScene s, SolverConst c, int
 // density/divergence loop, part B: v_adv update with k = kappa/rho
 // (DFSPH.cpp:647-693 / 840-883); then the loop decision.  Each neighbour
 // costs one 16-byte record (x, y, z, k) (pk; boundary: (x, y, z, volume)).
-template <int DIV, int DECIDE>
-__global__ void __launch_bounds__(NT) k_df_vupdate(DevScene s, SolverConst c, double goal_abs, double goal_rel,
+template <int BS, int DIV, int DECIDE>
+__global__ void __launch_bounds__(BS) k_df_vupdate(DevScene s, SolverConst c, double goal_abs, double goal_rel,
                                                    int min_it, int max_it, cudaGraphConditionalHandle h,
                                                    int use_handle) {
     const int n = s.st->n_active;
-    const int p = blockIdx.x * NT + threadIdx.x;
+    const int p = blockIdx.x * BS + threadIdx.x;
     if (p < n && scene_active(s, s.pv[2 * p])) {
         const float dt = dt_of(s, s.pv[2 * p]);
         const float4 pa = s.pk[p];
@@ -285,9 +288,10 @@ __global__ void __launch_bounds__(NT) k_df_vupdate(DevScene s, SolverConst c, do
 }
 
 // divergence loop, part A: Drho/Dt, clamp, kappa_v, FP64 sum
-__global__ void __launch_bounds__(NT) k_df_div_a(DevScene s, SolverConst c) {
+template <int BS>
+__global__ void __launch_bounds__(BS) k_df_div_a(DevScene s, SolverConst c) {
     const int n = s.st->n_active;
-    const int p = blockIdx.x * NT + threadIdx.x;
+    const int p = blockIdx.x * BS + threadIdx.x;
     double mine = 0.0;
     if (p < n && scene_active(s, s.pv[2 * p])) {
         const float4 pa = s.pv[2 * p];
@@ -303,10 +307,10 @@ __global__ void __launch_bounds__(NT) k_df_div_a(DevScene s, SolverConst c) {
         mine = (double)dd;
     }
     if (s.nscenes > 1) return;  // a batch reduces per scene (k_batch_decide)
-    __shared__ double sh[NT / 32];
-    double bs = block_sum_double<NT>(mine, sh);
+    __shared__ double sh[BS / 32];
+    double bs = block_sum_double<BS>(mine, sh);
     double tot;
-    if (finish_sum(s.partial, &s.st->ticket[1], bs, &tot)) s.st->err_div = tot / (double)n;
+    if (finish_sum<BS>(s.partial, &s.st->ticket[1], bs, &tot)) s.st->err_div = tot / (double)n;
 }
 
 // FP64 max |v| and the CFL step dt = clamp(cfl * d / vmax, dt_min, dt_max)
@@ -356,33 +360,42 @@ __global__ void __launch_bounds__(NT) k_cfl(DevScene s, float cfl, float d, floa
 }
 }  // namespace
 
-static inline int nblk(int n) { return (n > 0 ? n + NT - 1 : NT) / NT; }
+static inline int nblk(int n, int bs = NT) { return (n > 0 ? n + bs - 1 : bs) / bs; }
+
+// block size chosen at run time (the autotuner picks it per kernel class)
+#define DISPATCH_BS(bs, CALL)                       \
+    switch (bs) {                                   \
+        case 64: { constexpr int B = 64; CALL; break; }   \
+        case 256: { constexpr int B = 256; CALL; break; } \
+        default: { constexpr int B = 128; CALL; break; }  \
+    }
 
 void launch_step_begin(const DevScene& s, cudaStream_t st) { k_step_begin<<<1, 1, 0, st>>>(s); }
 void launch_call_begin(const DevScene& s, cudaStream_t st) { k_call_begin<<<1, 1, 0, st>>>(s); }
 void launch_df_loop_reset(const DevScene& s, int which, cudaStream_t st) { k_loop_reset<<<1, 1, 0, st>>>(s, which); }
 
-void launch_df_forces(const DevScene& s, const SolverConst& c, int n_max, int warm, cudaStream_t st) {
-    k_df_forces<<<nblk(n_max), NT, 0, st>>>(s, c, warm);
+void launch_df_forces(const DevScene& s, const SolverConst& c, int n_max, int warm, cudaStream_t st, int bs) {
+    DISPATCH_BS(bs, (k_df_forces<B><<<nblk(n_max, B), B, 0, st>>>(s, c, warm)));
 }
-void launch_df_dens_a(const DevScene& s, const SolverConst& c, int n_max, int record, cudaStream_t st) {
-    k_df_dens_a<<<nblk(n_max), NT, 0, st>>>(s, c, record);
+void launch_df_dens_a(const DevScene& s, const SolverConst& c, int n_max, int record, cudaStream_t st, int bs) {
+    DISPATCH_BS(bs, (k_df_dens_a<B><<<nblk(n_max, B), B, 0, st>>>(s, c, record)));
 }
 void launch_df_dens_b(const DevScene& s, const SolverConst& c, int n_max, double goal, int min_it, int max_it,
-                      unsigned long long cond_handle, int use_handle, cudaStream_t st) {
-    k_df_vupdate<0, 1><<<nblk(n_max), NT, 0, st>>>(s, c, 0.0, goal, min_it, max_it,
-                                                    (cudaGraphConditionalHandle)cond_handle, use_handle);
+                      unsigned long long cond_handle, int use_handle, cudaStream_t st, int bs) {
+    DISPATCH_BS(bs, (k_df_vupdate<B, 0, 1><<<nblk(n_max, B), B, 0, st>>>(
+                        s, c, 0.0, goal, min_it, max_it, (cudaGraphConditionalHandle)cond_handle, use_handle)));
 }
-void launch_df_warm_correction(const DevScene& s, const SolverConst& c, int n_max, cudaStream_t st) {
-    k_df_vupdate<0, 0><<<nblk(n_max), NT, 0, st>>>(s, c, 0.0, 0.0, 0, 0, (cudaGraphConditionalHandle)0, 0);
+void launch_df_warm_correction(const DevScene& s, const SolverConst& c, int n_max, cudaStream_t st, int bs) {
+    DISPATCH_BS(bs, (k_df_vupdate<B, 0, 0><<<nblk(n_max, B), B, 0, st>>>(s, c, 0.0, 0.0, 0, 0,
+                                                                         (cudaGraphConditionalHandle)0, 0)));
 }
-void launch_df_div_a(const DevScene& s, const SolverConst& c, int n_max, cudaStream_t st) {
-    k_df_div_a<<<nblk(n_max), NT, 0, st>>>(s, c);
+void launch_df_div_a(const DevScene& s, const SolverConst& c, int n_max, cudaStream_t st, int bs) {
+    DISPATCH_BS(bs, (k_df_div_a<B><<<nblk(n_max, B), B, 0, st>>>(s, c)));
 }
 void launch_df_div_b(const DevScene& s, const SolverConst& c, int n_max, double goal_abs, double goal_rel,
-                     int min_it, int max_it, unsigned long long cond_handle, int use_handle, cudaStream_t st) {
-    k_df_vupdate<1, 1><<<nblk(n_max), NT, 0, st>>>(s, c, goal_abs, goal_rel, min_it, max_it,
-                                                 (cudaGraphConditionalHandle)cond_handle, use_handle);
+                     int min_it, int max_it, unsigned long long cond_handle, int use_handle, cudaStream_t st, int bs) {
+    DISPATCH_BS(bs, (k_df_vupdate<B, 1, 1><<<nblk(n_max, B), B, 0, st>>>(
+                        s, c, goal_abs, goal_rel, min_it, max_it, (cudaGraphConditionalHandle)cond_handle, use_handle)));
 }
 void launch_cfl(const DevScene& s, int n_max, float cfl, float d, float dt_max, float dt_min, cudaStream_t st) {
     k_cfl<<<nblk(n_max), NT, 0, st>>>(s, cfl, d, dt_max, dt_min);

@@ -101,6 +101,10 @@ struct sphgpu_scene {
     float alpha_ref = 1.f;
     long long total_removed = 0;  // gid stays a permutation of [0, n) while 0
     int last_solver = -1;         // solver of the last step (carried-state validity)
+    // block sizes per kernel class (sphgpu_autotune picks them by measurement)
+    struct Tune {
+        int forces = 128, sweep_a = 128, sweep_b = 128, build = 128;
+    } tune;
     // batch of independent scenes (nscenes > 1): one grid per scene in one key space
     int nscenes = 1;
     std::vector<GridGeom> sgeom;  // per scene (key ranges, boxes)
@@ -331,7 +335,7 @@ void enq_ns(sphgpu_scene* h, int integrate, int build_mode, cudaStream_t st, int
     launch_count_active(d, h->g, st);
     if (h->nscenes > 1) launch_batch_count(d, h->nscenes, st);
     launch(h, build_mode == 1 ? "build_first" : (build_mode == 2 ? "build_pressure" : "build"), st,
-           [&] { launch_build(d, h->g, h->c, build_mode, h->cap, st); });
+           [&] { launch_build(d, h->g, h->c, build_mode, h->cap, st, h->tune.build); });
 }
 
 // Jacobi loop: a conditional WHILE node while capturing, host-driven otherwise.
@@ -374,10 +378,11 @@ int enq_df_density_loop(sphgpu_scene* h, bool capturing) {
     launch_df_loop_reset(d, 0, h->stream);
     if (h->nscenes > 1) launch_batch_loop_reset(d, h->nscenes, 0, h->stream);
     return enq_loop(h, capturing, [&](cudaStream_t st, unsigned long long hd, int use) {
-        launch(h, "df_density_a", st, [&] { launch_df_dens_a(d, h->c, h->cap, h->record_ksum, st); });
+        launch(h, "df_density_a", st,
+               [&] { launch_df_dens_a(d, h->c, h->cap, h->record_ksum, st, h->tune.sweep_a); });
         launch(h, "df_density_b", st, [&] {
             launch_df_dens_b(d, h->c, h->cap, P.df_density_goal, P.df_density_min_iter, P.df_density_max_iter, hd,
-                             use, st);
+                             use, st, h->tune.sweep_b);
         });
         if (h->nscenes > 1)
             launch(h, "batch_decide", st, [&] {
@@ -393,10 +398,10 @@ int enq_df_div_loop(sphgpu_scene* h, bool capturing) {
     launch_df_loop_reset(d, 1, h->stream);
     if (h->nscenes > 1) launch_batch_loop_reset(d, h->nscenes, 1, h->stream);
     return enq_loop(h, capturing, [&](cudaStream_t st, unsigned long long hd, int use) {
-        launch(h, "df_div_a", st, [&] { launch_df_div_a(d, h->c, h->cap, st); });
+        launch(h, "df_div_a", st, [&] { launch_df_div_a(d, h->c, h->cap, st, h->tune.sweep_a); });
         launch(h, "df_div_b", st, [&] {
             launch_df_div_b(d, h->c, h->cap, P.df_div_goal_abs, P.df_div_goal_rel, P.df_div_min_iter,
-                            P.df_div_max_iter, hd, use, st);
+                            P.df_div_max_iter, hd, use, st, h->tune.sweep_b);
         });
         if (h->nscenes > 1)
             launch(h, "batch_decide", st, [&] {
@@ -420,7 +425,7 @@ int enq_df_step(sphgpu_scene* h, bool capturing) {
     else if (h->P.cfl)
         launch(h, "cfl", st, [&] { launch_cfl(d, h->cap, h->P.cfl_factor, h->P.particle_d, h->P.dt_max, h->P.dt_min, st); });
     const int ws = h->mlp ? h->ws_mode : 0;
-    launch(h, "df_forces", st, [&] { launch_df_forces(d, h->c, h->cap, 0, st); });
+    launch(h, "df_forces", st, [&] { launch_df_forces(d, h->c, h->cap, 0, st, h->tune.forces); });
     if (ws == 1 || ws == 3) {
         launch(h, "ws_features", st, [&] {
             launch_ws_features(d, h->c, h->mlp->m, ws == 1 ? 1 : 2, h->P.dt_max, h->alpha_ref, nullptr, h->xn, h->cap,
@@ -428,7 +433,7 @@ int enq_df_step(sphgpu_scene* h, bool capturing) {
         });
         if (ws == 1)
             launch(h, "ws_infer", st, [&] { launch_ws_infer(d, h->c, h->mlp->m, h->xn, h->cap, h->sm_count, st); });
-        launch(h, "df_warm", st, [&] { launch_df_warm_correction(d, h->c, h->cap, st); });
+        launch(h, "df_warm", st, [&] { launch_df_warm_correction(d, h->c, h->cap, st, h->tune.sweep_b); });
     } else if (ws == 2) {
         launch(h, "ws_features", st, [&] {
             launch_ws_features(d, h->c, h->mlp->m, 0, h->P.dt_max, h->alpha_ref, h->recX, nullptr, h->cap, st);
@@ -1739,6 +1744,65 @@ int sphgpu_attach_warm_start(sphgpu_t h, sphgpu_mlp_t m, int mode, int record_ev
     if (mode != 1 && mode != 3) cudaMemsetAsync(h->d.kwarm, 0, sizeof(float) * h->cap, h->stream);
     invalidate_graphs(h);
     return cudaStreamSynchronize(h->stream) == cudaSuccess ? 0 : SPHGPU_ECUDA;
+}
+
+// ---- autotuner ----
+// Measures the DFSPH step kernels at 64, 128 and 256 threads per block on the
+// handle's own scene (steps_per_candidate real steps each, timed per kernel
+// with CUDA events) and keeps, per kernel class, the fastest block size.
+// The scene advances by 3 * steps_per_candidate steps.  report (optional)
+// receives a JSON summary.
+int sphgpu_autotune(sphgpu_t h, int solver, int steps_per_candidate, char* report, int report_len) {
+    if (!h || steps_per_candidate <= 0) return SPHGPU_EINVAL;
+    if (solver != SPHGPU_DFSPH) { h->err = "the autotuner covers the DFSPH step"; return SPHGPU_ENOTIMPL; }
+    cudaSetDevice(h->device);
+    const int cands[3] = {64, 128, 256};
+    const char* cls[4] = {"forces", "sweep_a", "sweep_b", "build"};
+    double best_t[4] = {1e30, 1e30, 1e30, 1e30};
+    int best_b[4] = {128, 128, 128, 128};
+    std::string rep = "{\"candidates\": {";
+    const bool was_on = h->prof.on;
+    for (int ci = 0; ci < 3; ++ci) {
+        const int b = cands[ci];
+        h->tune.forces = h->tune.sweep_a = h->tune.sweep_b = h->tune.build = b;
+        h->prof.on = true;
+        h->prof.acc.clear();
+        int r = sphgpu_step(h, solver, steps_per_candidate, nullptr);
+        if (r < 0 && r != SPHGPU_EMAXITER) { h->prof.on = was_on; return r; }
+        auto avg = [&](std::initializer_list<const char*> names) {
+            double t = 0;
+            int n = 0;
+            for (const char* nm : names) {
+                auto it = h->prof.acc.find(nm);
+                if (it != h->prof.acc.end()) { t += it->second.first; n += it->second.second; }
+            }
+            return n ? t / n : 1e30;
+        };
+        const double t[4] = {avg({"df_forces"}), avg({"df_density_a", "df_div_a"}), avg({"df_density_b", "df_div_b"}),
+                             avg({"build_first"})};
+        char buf[256];
+        snprintf(buf, sizeof buf, "%s\"%d\": {\"forces\": %.2f, \"sweep_a\": %.2f, \"sweep_b\": %.2f, \"build\": %.2f}",
+                 ci ? ", " : "", b, 1e3 * t[0], 1e3 * t[1], 1e3 * t[2], 1e3 * t[3]);
+        rep += buf;
+        for (int k = 0; k < 4; ++k)
+            if (t[k] < best_t[k]) { best_t[k] = t[k]; best_b[k] = b; }
+    }
+    h->prof.on = was_on;
+    h->prof.acc.clear();
+    h->tune.forces = best_b[0];
+    h->tune.sweep_a = best_b[1];
+    h->tune.sweep_b = best_b[2];
+    h->tune.build = best_b[3];
+    invalidate_graphs(h);
+    char buf[256];
+    snprintf(buf, sizeof buf, "}, \"chosen\": {\"%s\": %d, \"%s\": %d, \"%s\": %d, \"%s\": %d}}", cls[0], best_b[0],
+             cls[1], best_b[1], cls[2], best_b[2], cls[3], best_b[3]);
+    rep += buf;
+    if (report && report_len > 0) {
+        strncpy(report, rep.c_str(), report_len - 1);
+        report[report_len - 1] = 0;
+    }
+    return 0;
 }
 
 // ---- batch of independent scenes ----

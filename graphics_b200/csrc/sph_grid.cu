@@ -121,10 +121,10 @@ __global__ void k_merge_starts(DevScene s, int nk) {
 // mode 0: neighbour lists only; 1: + DFSPH rho and alpha
 // (DF_constantDensitySolverFirst, DFSPH.cpp:84-193); 2: + WCSPH rho and Tait
 // pressure (WcSph::wc_computePressure, WcSph.cpp:99-153).
-template <int MODE>
-__global__ void __launch_bounds__(128) k_build(DevScene s, GridGeom g, SolverConst c) {
+template <int MODE, int BS>
+__global__ void __launch_bounds__(BS) k_build(DevScene s, GridGeom g, SolverConst c) {
     const int n = s.st->n_active;
-    const int p = blockIdx.x * 128 + threadIdx.x;
+    const int p = blockIdx.x * BS + threadIdx.x;
     int cnt = 0, over = 0;
     const bool act = p < n;
     if (act) {
@@ -217,10 +217,10 @@ __global__ void __launch_bounds__(128) k_build(DevScene s, GridGeom g, SolverCon
             }
         }
     }
-    __shared__ int sh[4];
-    int tot = block_sum_int<128>(act ? cnt : 0, sh);
-    int ov = block_sum_int<128>(over, sh);
-    int mx = block_max_int<128>(act ? cnt : 0, sh);
+    __shared__ int sh[BS / 32];
+    int tot = block_sum_int<BS>(act ? cnt : 0, sh);
+    int ov = block_sum_int<BS>(over, sh);
+    int mx = block_max_int<BS>(act ? cnt : 0, sh);
     if (threadIdx.x == 0) {
         if (tot) atomicAdd(&s.st->nbr_total, (unsigned long long)tot);
         if (ov) { atomicAdd(&s.st->overflow, ov); atomicOr(&s.st->status, 8u); }
@@ -322,11 +322,20 @@ void launch_count_active(const DevScene& s, const GridGeom& g, cudaStream_t st) 
     k_merge_starts<<<nblk(g.nkeys + 1, NT), NT, 0, st>>>(s, g.nkeys);
 }
 
-void launch_build(const DevScene& s, const GridGeom& g, const SolverConst& c, int mode, int n_max, cudaStream_t st) {
-    int nb = nblk(n_max > 0 ? n_max : 1, 128);
-    if (mode == 0) k_build<0><<<nb, 128, 0, st>>>(s, g, c);
-    else if (mode == 1) k_build<1><<<nb, 128, 0, st>>>(s, g, c);
-    else k_build<2><<<nb, 128, 0, st>>>(s, g, c);
+template <int BS>
+static void launch_build_bs(const DevScene& s, const GridGeom& g, const SolverConst& c, int mode, int n_max,
+                            cudaStream_t st) {
+    const int nb = nblk(n_max > 0 ? n_max : 1, BS);
+    if (mode == 0) k_build<0, BS><<<nb, BS, 0, st>>>(s, g, c);
+    else if (mode == 1) k_build<1, BS><<<nb, BS, 0, st>>>(s, g, c);
+    else k_build<2, BS><<<nb, BS, 0, st>>>(s, g, c);
+}
+
+void launch_build(const DevScene& s, const GridGeom& g, const SolverConst& c, int mode, int n_max, cudaStream_t st,
+                  int bs) {
+    if (bs == 64) launch_build_bs<64>(s, g, c, mode, n_max, st);
+    else if (bs == 256) launch_build_bs<256>(s, g, c, mode, n_max, st);
+    else launch_build_bs<128>(s, g, c, mode, n_max, st);
 }
 
 void launch_boundary_keys(const float4* bpos, int nb, const GridGeom& g, int* keys, cudaStream_t st) {

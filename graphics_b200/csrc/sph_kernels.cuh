@@ -129,7 +129,8 @@ void launch_hash(const DevScene& s, const GridGeom& g, int integrate, int n_old,
 void launch_scatter_reorder(const DevScene& s, const GridGeom& g, int n_old, int carry, cudaStream_t st);
 void launch_count_active(const DevScene& s, const GridGeom& g, cudaStream_t st);
 // mode 0: lists only; 1: lists + DFSPH rho/alpha; 2: lists + WCSPH rho/pressure
-void launch_build(const DevScene& s, const GridGeom& g, const SolverConst& c, int mode, int n_max, cudaStream_t st);
+void launch_build(const DevScene& s, const GridGeom& g, const SolverConst& c, int mode, int n_max, cudaStream_t st,
+                  int bs = 128);
 void launch_to_ref_order(const float4* src, const int* gid, int n, float* dst3, cudaStream_t st);
 void launch_from_ref_order(const float* src3, const int* gid, int n, float4* dst, cudaStream_t st);
 void launch_boundary_keys(const float4* bpos, int nb, const GridGeom& g, int* keys, cudaStream_t st);
@@ -139,14 +140,16 @@ void launch_boundary_volume(const DevScene& s, const GridGeom& g, float dpart, f
 
 // ---- DFSPH (sph_dfsph.cu) ----
 void launch_df_first(const DevScene& s, const SolverConst& c, int n_max, cudaStream_t st);
-void launch_df_forces(const DevScene& s, const SolverConst& c, int n_max, int warm, cudaStream_t st);
-void launch_df_dens_a(const DevScene& s, const SolverConst& c, int n_max, int record, cudaStream_t st);
+// bs: threads per block (64, 128 or 256; the autotuner's choice)
+void launch_df_forces(const DevScene& s, const SolverConst& c, int n_max, int warm, cudaStream_t st, int bs = 128);
+void launch_df_dens_a(const DevScene& s, const SolverConst& c, int n_max, int record, cudaStream_t st, int bs = 128);
 void launch_df_dens_b(const DevScene& s, const SolverConst& c, int n_max, double goal, int min_it, int max_it,
-                      unsigned long long cond_handle, int use_handle, cudaStream_t st);
-void launch_df_div_a(const DevScene& s, const SolverConst& c, int n_max, cudaStream_t st);
+                      unsigned long long cond_handle, int use_handle, cudaStream_t st, int bs = 128);
+void launch_df_div_a(const DevScene& s, const SolverConst& c, int n_max, cudaStream_t st, int bs = 128);
 void launch_df_div_b(const DevScene& s, const SolverConst& c, int n_max, double goal_abs, double goal_rel,
-                     int min_it, int max_it, unsigned long long cond_handle, int use_handle, cudaStream_t st);
-void launch_df_warm_correction(const DevScene& s, const SolverConst& c, int n_max, cudaStream_t st);
+                     int min_it, int max_it, unsigned long long cond_handle, int use_handle, cudaStream_t st,
+                     int bs = 128);
+void launch_df_warm_correction(const DevScene& s, const SolverConst& c, int n_max, cudaStream_t st, int bs = 128);
 void launch_df_loop_reset(const DevScene& s, int which, cudaStream_t st);
 void launch_cfl(const DevScene& s, int n_max, float cfl, float d, float dt_max, float dt_min, cudaStream_t st);
 void launch_step_begin(const DevScene& s, cudaStream_t st);

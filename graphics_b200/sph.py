@@ -204,6 +204,14 @@ class GpuScene:
         return out[:m]
 
     # -- profiling --
+    def autotune(self, solver="dfsph", steps=3):
+        """Pick block sizes per kernel class by measurement (sphgpu_autotune);
+        advances the scene by 3 * steps steps.  Returns the JSON report."""
+        import json
+        buf = C.create_string_buffer(4096)
+        self._check(self.lib.sphgpu_autotune(self.h, SOLVERS.get(solver, solver), int(steps), buf, 4096), "autotune")
+        return json.loads(buf.value.decode())
+
     def profile(self, on=True):
         self._check(self.lib.sphgpu_profile(self.h, int(on)), "profile")
 

@@ -240,6 +240,13 @@ int sphgpu_attach_warm_start(sphgpu_t h, sphgpu_mlp_t m, int mode, int record_ev
 /* Copy of the last error message. */
 int sphgpu_last_error(sphgpu_t h, char* buf, int len);
 
+/* Autotuner (no reference counterpart): times the DFSPH step kernels at 64,
+ * 128 and 256 threads per block on this scene (steps_per_candidate real
+ * steps per candidate; the scene advances by 3x that) and keeps the fastest
+ * block size per kernel class (forces, sweep A, sweep B, neighbour build).
+ * report (may be NULL) receives a JSON summary of the timings. */
+int sphgpu_autotune(sphgpu_t h, int solver, int steps_per_candidate, char* report, int report_len);
+
 /* ---------------- batch of independent scenes (no reference counterpart) ----------------
  * Many DFSPH scenes of uneven size in one handle: one set of arrays, one
  * neighbour search and one launch per sweep for all of them, each scene with

@@ -55,3 +55,21 @@ def test_batch_scenes_converge_independently():
     n = sum(b.scene_range(k)[1] for k in range(len(scenes)))
     assert n == b.n_fluid
     b.close()
+
+
+def test_autotune_picks_block_sizes_and_keeps_results():
+    """The autotuner times 64/128/256 threads per block and keeps a valid
+    choice; stepping with it gives the same iteration counts and states as
+    the default block sizes (the per-particle arithmetic does not depend on
+    the block size)."""
+    sc = small_dam_break((16, 16, 16), 0.025, seed=4)
+    g1, g2 = scene_to_gpu(sc, **KW), scene_to_gpu(sc, **KW)
+    rep = g1.autotune("dfsph", 1)
+    assert set(rep["chosen"]) == {"forces", "sweep_a", "sweep_b", "build"}
+    assert all(v in (64, 128, 256) for v in rep["chosen"].values())
+    g2.step("dfsph", 3)  # g1 advanced 3 steps while tuning
+    s1, s2 = g1.step("dfsph", 4), g2.step("dfsph", 4)
+    assert s1["total_iter_density"] == s2["total_iter_density"]
+    assert np.max(np.abs(g1.get("position") - g2.get("position"))) <= 1e-5
+    g1.close()
+    g2.close()
