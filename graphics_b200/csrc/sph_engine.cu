@@ -1161,6 +1161,22 @@ int sphgpu_get_fluid(sphgpu_t h, const char* field, float* out) {
         CK(cudaStreamSynchronize(h->stream));
         return n;
     }
+    if (f == "phase" || f == "scene") {
+        // fluid phase (or batch scene) index of each particle, as floats
+        std::vector<int> gid;
+        int n;
+        if (download_gid(h, gid, n, h->in_staging)) return SPHGPU_ECUDA;
+        std::vector<int> order;
+        ref_order(gid, order);
+        std::vector<float4> t(n);
+        CK(cudaMemcpy(t.data(), h->in_staging ? h->d.pos_s : h->d.pos, sizeof(float4) * n, cudaMemcpyDeviceToHost));
+        for (int k = 0; k < n; ++k) {
+            int w;
+            memcpy(&w, &t[order[k]].w, sizeof w);
+            out[k] = (float)(f == "phase" ? (w & 15) : (w >> 4));
+        }
+        return n;
+    }
     std::vector<int> gid;
     int n;
     if (download_gid(h, gid, n, staging)) return SPHGPU_ECUDA;

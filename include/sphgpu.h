@@ -176,7 +176,9 @@ int sphgpu_step_host(sphgpu_t h, int solver, const float* xyz, const float* vel,
  * IISPH_M: "dii","sum_dijpj","ii_vel_adv","acce_presure" (n*3),
  *          "aii","p_l","rho_adv" (n);
  * learned warm start: "kappa_warm" (n), "ws_features" (n*16, the network's
- * normalised inputs of the last step).  Returns the count written.
+ * normalised inputs of the last step);
+ * "phase" (n, fluid phase index), "scene" (n, batch scene index).
+ * Returns the count written.
  * set: "position","velocity","density" (the density the next PCISPH /
  * IISPH_M step's non-pressure forces read), "DFalpha". */
 int sphgpu_get_fluid(sphgpu_t h, const char* field, float* out);

@@ -1,0 +1,161 @@
+/*
+ * sphgpu_solver.hpp -- C++ drop-in for the reference's solver classes.
+ *
+ * GpuSolver<Base, Solver> derives from one of the reference's solver classes
+ * (WcSph, PciSph, IISph_M, DFSPH; PciSph.h:30, IISph_M.h:22, DFSPH.h:10) and
+ * overrides its step, virtual void sphStep() (SphBase.h:420), with one call
+ * into the C ABI of include/sphgpu.h.  A reference scene switches to the GPU
+ * by changing its base class:
+ *
+ *     class mySPH : public DFSPH                           // CPU (reference)
+ *     class mySPH : public GpuSolver<DFSPH, SPHGPU_DFSPH>  // GPU (sm_100a)
+ *
+ * setupScene(), stepEvent(), runOneStep() (SphBase.cpp:348-354) and the
+ * particle arrays m_Fluids / m_Solids (SphBase.h:660-661) keep their meaning:
+ * before the first step the scene is uploaded (walls as static solids, one
+ * phase per SphFluid); after every step positions, velocities and densities
+ * are written back into m_Fluids[k].fluidParticles, with particles that left
+ * [spaceMin, spaceMax] removed as SphFluid::removeOutsideParts does
+ * (SphBase.cpp:26-48).  If stepEvent() changes the number of particles of a
+ * phase, the scene is uploaded again before the next step.  m_EC receives
+ * the step's zero-distance and neighbour-overflow counts (SphBase.h:586-602).
+ *
+ * Header only; needs the reference's class declarations included first and
+ * links against libsphgpu.so.
+ */
+#ifndef SPHGPU_SOLVER_HPP_
+#define SPHGPU_SOLVER_HPP_
+
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "sphgpu.h"
+
+template <class Base, int Solver>
+class GpuSolver : public Base {
+public:
+    GpuSolver() { sphgpu_params_default(&gpu_params_); }
+    ~GpuSolver() override {
+        if (gpu_) sphgpu_destroy(gpu_);
+    }
+
+    /* Solver controls that m_TH does not hold (loop goals and caps, CFL,
+     * neighbour cap); defaults are sphgpu_params_default()'s.  Changes take
+     * effect at the next upload. */
+    SphParams& gpuParams() { return gpu_params_; }
+    /* Statistics of the last step (iterations, errors, dt, status). */
+    const SphStepStats& gpuStats() const { return stats_; }
+    /* CUDA device the scene runs on (set before the first step). */
+    void setGpuDevice(int d) { device_ = d; }
+
+protected:
+    void sphStep() override {
+        if (!gpu_ || host_layout_changed()) upload();
+        int rc = sphgpu_step(gpu_, Solver, 1, &stats_);
+        if (rc < 0 && rc != SPHGPU_EMAXITER) fail("sphgpu_step", rc);
+        this->m_EC.zeroDis += stats_.zero_distance;
+        this->m_EC.tooManyNeigb += stats_.neighbour_overflow;
+        download();
+    }
+
+private:
+    sphgpu_t gpu_ = nullptr;
+    SphParams gpu_params_;
+    SphStepStats stats_ = {};
+    int device_ = 0;
+    std::vector<size_t> counts_;  // per phase, as last written to m_Fluids
+
+    void fail(const char* what, int rc) {
+        char buf[512] = {0};
+        if (gpu_) sphgpu_last_error(gpu_, buf, sizeof buf);
+        throw std::runtime_error(std::string(what) + " failed (" + std::to_string(rc) + "): " + buf);
+    }
+
+    bool host_layout_changed() const {
+        if (counts_.size() != this->m_Fluids.size()) return true;
+        for (size_t k = 0; k < counts_.size(); ++k)
+            if (counts_[k] != this->m_Fluids[k].fluidParticles.size()) return true;
+        return false;
+    }
+
+    void upload() {
+        if (gpu_) { sphgpu_destroy(gpu_); gpu_ = nullptr; }
+        SphParams p = gpu_params_;
+        p.spacing_r = (float)this->m_TH.spacing_r;
+        p.smoothRadius_h = (float)this->m_TH.smoothRadius_h;
+        p.dt = (float)this->m_TH.dt;
+        for (int i = 0; i < 3; ++i) {
+            p.gravity[i] = (float)this->m_TH.gravity_g[i];
+            p.spaceMin[i] = (float)this->m_TH.spaceMin[i];
+            p.spaceMax[i] = (float)this->m_TH.spaceMax[i];
+        }
+        p.soundSpeed_cs = (float)this->m_TH.soundSpeed_cs;
+        p.nu = (float)this->m_TH.nu;
+        p.densityErro_eta = (float)this->m_TH.densityErro_eta;
+        int total = 0;
+        for (auto& f : this->m_Fluids) {
+            total += (int)f.fluidParticles.size();
+            if (!f.fluidParticles.empty()) p.particle_d = (float)f.fluidParticles[0].d;
+        }
+        if (!this->m_Solids.empty()) p.boundary_visc = (float)this->m_Solids[0].viscosity_alpha;
+        int rc = sphgpu_create(&p, device_, total > 0 ? total : 1, &gpu_);
+        if (rc) fail("sphgpu_create", rc);
+        std::vector<float> xyz, vel;
+        std::vector<int> sid;
+        for (size_t k = 0; k < this->m_Solids.size(); ++k)
+            for (auto& q : this->m_Solids[k].boundaryParticles) {
+                for (int c = 0; c < 3; ++c) xyz.push_back((float)q.position[c]);
+                sid.push_back((int)k);
+            }
+        rc = sphgpu_set_boundary(gpu_, (int)sid.size(), xyz.data(), sid.data(), nullptr);
+        if (rc) fail("sphgpu_set_boundary", rc);
+        counts_.clear();
+        for (auto& f : this->m_Fluids) {
+            xyz.clear();
+            vel.clear();
+            for (auto& q : f.fluidParticles)
+                for (int c = 0; c < 3; ++c) {
+                    xyz.push_back((float)q.position[c]);
+                    vel.push_back((float)q.velocity[c]);
+                }
+            counts_.push_back(f.fluidParticles.size());
+            if (f.fluidParticles.empty()) continue;
+            rc = sphgpu_add_fluid(gpu_, (int)f.fluidParticles.size(), xyz.data(), vel.data(),
+                                  (float)f.restDensity_rho0, (float)f.viscosity_alpha);
+            if (rc < 0) fail("sphgpu_add_fluid", rc);
+        }
+    }
+
+    void download() {
+        const int n = sphgpu_num_fluid(gpu_);
+        if (n < 0) fail("sphgpu_num_fluid", n);
+        std::vector<float> xyz(3 * (size_t)n), vel(3 * (size_t)n), rho((size_t)n), ph((size_t)n);
+        int rc = sphgpu_get_fluid(gpu_, "position", xyz.data());
+        if (rc >= 0) rc = sphgpu_get_fluid(gpu_, "velocity", vel.data());
+        if (rc >= 0) rc = sphgpu_get_fluid(gpu_, "density", rho.data());
+        if (rc >= 0) rc = sphgpu_get_fluid(gpu_, "phase", ph.data());
+        if (rc < 0) fail("sphgpu_get_fluid", rc);
+        // reference order: phase by phase, each in index order; removed
+        // particles are gone, so each phase keeps its first survivors
+        size_t i = 0;
+        for (size_t k = 0; k < this->m_Fluids.size(); ++k) {
+            auto& parts = this->m_Fluids[k].fluidParticles;
+            size_t m = 0;
+            while (i + m < (size_t)n && (size_t)ph[i + m] == k) ++m;
+            if (m < parts.size()) parts.resize(m);
+            for (size_t j = 0; j < m; ++j) {
+                auto& q = parts[j];
+                for (int c = 0; c < 3; ++c) {
+                    q.position[c] = xyz[3 * (i + j) + c];
+                    q.velocity[c] = vel[3 * (i + j) + c];
+                }
+                q.density = rho[i + j];
+            }
+            counts_[k] = parts.size();
+            i += m;
+        }
+    }
+};
+
+#endif /* SPHGPU_SOLVER_HPP_ */

@@ -34,6 +34,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF = os.environ.get("SPH_REFERENCE_SOURCE", "/root/reference/Source")
+ROOT = os.path.dirname(HERE)
 OUT = os.path.join(HERE, "_ref")
 SRC = os.path.join(OUT, "src")
 SHIM = os.path.join(HERE, "refshim")
@@ -159,6 +160,21 @@ def main():
             if real == "double":
                 cmd.insert(1, "-DREF_REAL_DOUBLE")
             jobs.append((so, cmd))
+    # the C++ drop-in check: a scene class derived from the reference's DFSPH
+    # switched to the GPU through include/sphgpu_solver.hpp (links libsphgpu.so)
+    lib = os.path.join(ROOT, "graphics_b200", "libsphgpu.so")
+    if os.path.exists(lib):
+        exe = os.path.join(OUT, "dropin_dfsph")
+        deps = [os.path.join(SHIM, "dropin_main.cpp"), os.path.join(ROOT, "include", "sphgpu_solver.hpp"),
+                os.path.join(ROOT, "include", "sphgpu.h"), os.path.join(SRC, "DFSPH.cpp"),
+                os.path.join(SRC, "SphBase.cpp"), os.path.join(SRC, "SphBase.h"), lib]
+        if not (os.path.exists(exe) and all(os.path.getmtime(exe) >= os.path.getmtime(d) for d in deps)):
+            jobs.append((exe, ["g++", "-std=c++17", "-O2", "-fopenmp", "-w", "-DREF_SOLVER_HEADER=\"DFSPH.h\"",
+                               "-DREF_SOLVER_CLASS=DFSPH", "-DREF_SPHGPU_SOLVER=SPHGPU_DFSPH", "-I" + SRC,
+                               "-I" + SHIM, "-I" + os.path.join(ROOT, "include"),
+                               os.path.join(SHIM, "dropin_main.cpp"), os.path.join(SRC, "SphBase.cpp"),
+                               os.path.join(SRC, "DFSPH.cpp"), "-L" + os.path.dirname(lib), "-lsphgpu",
+                               "-Wl,-rpath,$ORIGIN/../../graphics_b200", "-o", exe]))
     procs = [(so, subprocess.Popen(cmd, stderr=subprocess.PIPE)) for so, cmd in jobs]
     rc = 0
     for so, p in procs:
