@@ -40,7 +40,7 @@ SRC = os.path.join(OUT, "src")
 SHIM = os.path.join(HERE, "refshim")
 
 FILES = ["SphBase.h", "SphBase.cpp", "Vec23.h", "DFSPH.h", "DFSPH.cpp", "WcSph.h",
-         "WcSph.cpp", "PciSph.h", "PciSph.cpp", "IISph_M.h", "IISph_M.cpp"]
+         "WcSph.cpp", "PciSph.h", "PciSph.cpp", "IISph_M.h", "IISph_M.cpp", "IISph.h", "IISph.cpp"]
 
 # (anchor line in SphBase.h, text inserted after it).  The anchors are the last
 # member of FluidParticle (SphBase.h:117), of BoundaryParticle (SphBase.h:198)
@@ -87,6 +87,7 @@ SOLVERS = {
     "wcsph": ("WcSph.cpp", "WcSph.h", "WcSph", []),
     "pcisph": ("PciSph.cpp", "PciSph.h", "PciSph", ["-DPREDICTION_PCISPH"]),
     "iisphm": ("IISph_M.cpp", "IISph_M.h", "IISph_M", ["-DIISPH"]),
+    "iisph": ("IISph.cpp", "IISph.h", "IISph", ["-DIISPH"]),
 }
 
 

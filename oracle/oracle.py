@@ -41,7 +41,10 @@ class OrcParams(C.Structure):
         ("wc_gamma", C.c_double),
         ("pci_eta", C.c_double), ("pci_min_iter", C.c_int), ("pci_max_iter", C.c_int),
         ("ii_omega", C.c_double), ("ii_eta_rel", C.c_double), ("ii_min_iter", C.c_int), ("ii_max_iter", C.c_int),
-        ("ii_compat", C.c_int)]
+        ("ii_compat", C.c_int),
+        ("iv_kvisc", C.c_double), ("iv_kvisc_b", C.c_double), ("iv_cv_goal", C.c_double),
+        ("iv_div_goal", C.c_double), ("iv_cv_min_iter", C.c_int), ("iv_cv_max_iter", C.c_int),
+        ("iv_div_min_iter", C.c_int), ("iv_div_max_iter", C.c_int)]
 
 
 def build():
@@ -61,7 +64,9 @@ def default_params(scene=None, **kw):
              df_div_goal_abs=2.5, df_div_goal_rel=1e-3, df_div_min_iter=1, df_div_max_iter=30,
              cfl=0, cfl_factor=0.4, dt_max=5e-3, dt_min=1e-6, wc_gamma=7.0,
              pci_eta=0.01, pci_min_iter=3, pci_max_iter=10,
-             ii_omega=0.5, ii_eta_rel=1e-3, ii_min_iter=2, ii_max_iter=100, ii_compat=0)
+             ii_omega=0.5, ii_eta_rel=1e-3, ii_min_iter=2, ii_max_iter=100, ii_compat=0,
+             iv_kvisc=0.1, iv_kvisc_b=0.1, iv_cv_goal=1e-4, iv_div_goal=1e-3, iv_cv_min_iter=3,
+             iv_cv_max_iter=100, iv_div_min_iter=2, iv_div_max_iter=50)
     if scene is not None:
         p.update(spacing_r=scene.spacing_r, smoothRadius_h=scene.smooth_radius,
                  spaceMin=scene.space_min, spaceMax=scene.space_max)
@@ -85,7 +90,7 @@ class Oracle:
     """One scene in either back end.
 
     kind:  "port" (restatement) or "reference" (compiled reference)
-    solver: for "reference": dfsph | dfsph_capped | wcsph | pcisph | iisphm
+    solver: for "reference": dfsph | dfsph_capped | wcsph | pcisph | iisphm | iisph
     f64:   double-precision build
     """
 
@@ -155,6 +160,8 @@ class Oracle:
             lib.orc_set_solid.restype = i
             lib.orc_pci_delta.argtypes = [vp]
             lib.orc_pci_delta.restype = d
+            lib.orc_vf_stats.argtypes = [vp, ip, dp]
+            lib.orc_vf_stats.restype = None
         else:
             lib.ref_error_counts.argtypes = [vp, ip, ip]
             lib.ref_frame.restype = i
@@ -163,6 +170,10 @@ class Oracle:
             lib.ref_set_iter_limits.argtypes = [vp, i, i]
             lib.ref_set_threads.restype = None
             lib.ref_set_threads.argtypes = [i]
+            lib.ref_vf_iters.restype = i
+            lib.ref_vf_iters.argtypes = [vp, ip, ip]
+            lib.ref_set_solid.restype = i
+            lib.ref_set_solid.argtypes = [vp, i, cp, dp]
         cls._libs[name] = lib
         return lib
 
@@ -215,7 +226,7 @@ class Oracle:
             raise KeyError(field)
         vec = field in ("position", "velocity", "vel_adv", "acce_adv", "acceleration", "DFalpha1", "n",
                         "pos_prediction", "acce_pressure", "dii", "sum_dijpj", "advectionVelocity",
-                        "acce_presure", "advectionAcceleration")
+                        "acce_presure", "advectionAcceleration", "DF_alpha1", "VF_alpha1")
         return out[:3 * n].reshape(n, 3) if vec else out[:n]
 
     def set(self, field, values, k=0):
@@ -289,6 +300,29 @@ class Oracle:
     def pci_delta(self):
         """PCISPH delta / dt^2 of the last pci_updateDelta (port only)."""
         return float(self.lib.orc_pci_delta(self.h))
+
+    def vf_iters(self):
+        """IISph: (divergence-free, constant-volume) iterations.  Reference
+        build: m_TH.dF_iteration / cV_iteration accumulated since the last
+        call (each loop adds its iterations - 1; read and reset).  Port: the
+        iterations of the last loops, summed over phases."""
+        if self.kind == "port":
+            return self.vf_stats()[0]
+        a, b = C.c_int(), C.c_int()
+        self.lib.ref_vf_iters(self.h, C.byref(a), C.byref(b))
+        return a.value, b.value
+
+    def vf_stats(self):
+        """Port only: ((it_div, it_cv), (err_div, err_cv)) of the last IISph loops."""
+        it = (C.c_int * 2)()
+        er = (C.c_double * 2)()
+        self.lib.orc_vf_stats(self.h, it, er)
+        return (it[0], it[1]), (er[0], er[1])
+
+    def set_solid(self, field, values, k=0):
+        v = np.ascontiguousarray(values, dtype=np.float64).ravel()
+        if self._f("set_solid")(self.h, k, field.encode(), self._dp(v)) != 0:
+            raise KeyError(field)
 
     def set_threads(self, n):
         """OpenMP threads of the compiled reference (process-wide)."""

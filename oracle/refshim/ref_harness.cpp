@@ -58,6 +58,13 @@ public:
          * (PciSph.h:35,63); start from values that force the computation. */
         pci_last_dt = pci_last_sp = pci_last_h = real_t(-1);
 #endif
+#ifdef REF_TAG_iisph
+        /* IISph: the temperature / melting update (SphBase::updateTemperature,
+         * run by IISph::sphStep when m_TH.phaseTransition, IISph.cpp:74-76)
+         * is off, as in the reference's own demo scene (Demo-mySPH.h:49). */
+        m_TH.phaseTransition = false;
+        m_TH.dF_iteration = m_TH.cV_iteration = 0;  // uninitialised members (SphBase.h)
+#endif
     }
 
     int stage(const std::string& s) {
@@ -84,6 +91,13 @@ public:
         if (s == "ii_computePressure") { ii_computePressure(); return 0; }
         if (s == "ii_computeForcePressure") { ii_computeForcePressure(); return 0; }
 #endif
+#ifdef REF_TAG_iisph
+        if (s == "DF_prepareAttribute") { DF_prepareAttribute(); return 0; }
+        if (s == "VF_prepareAttribute") { VF_prepareAttribute(); return 0; }
+        if (s == "advectionStep") { advectionStep(); return 0; }
+        if (s == "VF_divergenceFreeSolver") { VF_divergenceFreeSolver(); return 0; }
+        if (s == "VF_constantVolumeSolver") { VF_constantVolumeSolver(); return 0; }
+#endif
         return -1;
     }
 
@@ -97,6 +111,10 @@ public:
         SCAL(aii) SCAL(rho_adv) SCAL(p_l) SCAL(d) SCAL(sphDensity) SCAL(advectionDensity)
         SCAL(restDensity) SCAL(presure) SCAL(mass) SCAL(density) SCAL(density_adv)
         SCAL(DFalpha) SCAL(DFalpha2) SCAL(DFkappa) SCAL(DFkappaV) SCAL(divergenceDeviation)
+        SCAL(restVolume) SCAL(beta) SCAL(kinematicViscosity) SCAL(temperature) SCAL(temperatureNext)
+        SCAL(DF_alpha) SCAL(DF_alpha2) SCAL(VF_gamma) SCAL(VF_sphVolume) SCAL(VF_advectionVolume)
+        SCAL(VF_alpha) SCAL(VF_alpha2) SCAL(VF_kappa) SCAL(VF_kappaV) SCAL(VF_divergenceDeviation)
+        VEC(DF_alpha1) VEC(VF_alpha1)
 #ifdef PREDICTION_PCISPH
         VEC(acce_pressure) VEC(pos_prediction)
 #endif
@@ -105,6 +123,9 @@ public:
     static int solidField(BoundPart& p, const char* f, real_t** ptr) {
         VEC(position) VEC(velocity) VEC(force) VEC(singleVelocity)
         SCAL(volume) SCAL(kerSumFromSelf) SCAL(d) SCAL(restDensity) SCAL(sphDensity)
+        SCAL(mass) SCAL(kinematicViscosity) SCAL(DF_alpha) SCAL(VF_gamma) SCAL(VF_sphVolume)
+        SCAL(VF_advectionVolume) SCAL(VF_alpha) SCAL(VF_alpha2) SCAL(VF_kappa) SCAL(VF_kappaV)
+        SCAL(VF_divergenceDeviation)
         return -1;
 #undef SCAL
 #undef VEC
@@ -158,6 +179,12 @@ public:
         FluidParticle p = FluidParticle();
         p.d = real_t(d);
         p.restDensity = real_t(rho0);
+        /* IISph reads beta (restDensity = rho0 * beta, IISph.cpp:109-110) and the
+         * temperature; a value-initialised particle has beta = 0.  The
+         * reference's demo scene sets beta = 1 at 0 degrees C
+         * (Demo-mySPH.h:90-93). */
+        p.beta = real_t(1);
+        p.temperature = p.temperatureNext = real_t(273.15);
         /* WcSph::wc_computePressure reads the neighbours' density before it is
          * first computed (WcSph.cpp:131, for the surface normal); start from
          * the rest density so that read is finite. */
@@ -274,6 +301,32 @@ public:
         return -1;
 #endif
     }
+    /* IISph iteration counters m_TH.dF_iteration / cV_iteration (each loop
+     * adds its iterations - 1, IISph.cpp:1449, 794); read and reset.
+     * Returns -1 for the other solvers. */
+    static int ref_vf_iters_impl(void* hh, int* df, int* cv) {
+#ifdef REF_TAG_iisph
+        RefHarness* h = static_cast<RefHarness*>(hh);
+        *df = int(h->m_TH.dF_iteration);
+        *cv = int(h->m_TH.cV_iteration);
+        h->m_TH.dF_iteration = 0;
+        h->m_TH.cV_iteration = 0;
+        return 0;
+#else
+        (void)hh; *df = *cv = 0;
+        return -1;
+#endif
+    }
+    static int ref_set_solid_impl(void* hh, int k, const char* field, const double* in) {
+        RefHarness* h = static_cast<RefHarness*>(hh);
+        auto& v = h->m_Solids[k].boundaryParticles;
+        for (size_t i = 0; i < v.size(); ++i) {
+            real_t* p; int c = RefHarness::solidField(v[i], field, &p);
+            if (c < 0) return -1;
+            for (int j = 0; j < c; ++j) p[j] = real_t(in[i * c + j]);
+        }
+        return 0;
+    }
     static double ref_kernel_impl(void* hh, int grad, double r) {
         RefHarness* h = static_cast<RefHarness*>(hh);
         return grad ? double(h->ker_W_grad(real_t(r))) : double(h->ker_W(real_t(r)));
@@ -308,6 +361,8 @@ int ref_frame(void* hh) { return RefHarness::ref_frame_impl(hh); }
 void ref_set_frame(void* hh, int f) { RefHarness::ref_set_frame_impl(hh, f); }
 double ref_kernel(void* hh, int grad, double r) { return RefHarness::ref_kernel_impl(hh, grad, r); }
 int ref_set_iter_limits(void* hh, int mn, int mx) { return RefHarness::ref_set_iter_limits_impl(hh, mn, mx); }
+int ref_vf_iters(void* hh, int* df, int* cv) { return RefHarness::ref_vf_iters_impl(hh, df, cv); }
+int ref_set_solid(void* hh, int k, const char* field, const double* in) { return RefHarness::ref_set_solid_impl(hh, k, field, in); }
 /* SphBase::SphBase sets the OpenMP thread count to omp_get_num_procs()
  * (SphBase.cpp:242-243); this overrides it (1 thread makes the racy loops of
  * IISph_M.cpp:315-351 deterministic) */

@@ -19,6 +19,9 @@
  *   - WCSPH: Tait pressure and forces              WcSph.cpp:23-462
  *   - PCISPH predict/correct loop                  PciSph.cpp:98-505
  *   - IISPH multiphase (IISph_M)                   IISph_M.cpp:10-684
+ *   - IISph, volume form (divergence-free and
+ *     constant-volume loops, per-pair h)           IISph.cpp:14-545, 546-815,
+ *                                                  1219-1570
  *
  * Arithmetic follows the reference expression by expression (evaluation order,
  * float/double promotions of std::pow), so that with `real` = float and no FMA
@@ -79,6 +82,12 @@ typedef struct OrcParams {
     double pci_eta; int pci_min_iter, pci_max_iter; /* PciSph.h:35 */
     double ii_omega, ii_eta_rel; int ii_min_iter, ii_max_iter;
     int ii_compat;        /* IISPH_M reference-compatibility bits (sph_oracle_pci_ii.inc) */
+    /* IISph (volume form, sph_oracle_iisph.inc): FluidParticle /
+     * BoundaryParticle::kinematicViscosity (SphBase.h:100,181, default 0.1)
+     * and the loop bounds of IISph.cpp:550-555 (goal 1e-4, min 3, max 100)
+     * and :1223-1227 (goal 1e-3, min 2, max 50) */
+    double iv_kvisc, iv_kvisc_b, iv_cv_goal, iv_div_goal;
+    int iv_cv_min_iter, iv_cv_max_iter, iv_div_min_iter, iv_div_max_iter;
 } OrcParams;
 
 typedef struct { int t, i; } PIdx; /* PartIdx, SphBase.h:596-617 */
@@ -91,6 +100,12 @@ typedef struct {
     /* PCISPH / IISPH */
     real *pos_pred, *acce_pressure, *dii, *sum_dijpj, *adv_vel, *acce_presure;
     real *aii, *rho_adv, *p_l, *p_l2;
+    /* IISph (volume form): per-phase beta (SphBase.h:98; restDensity =
+     * rho0 * beta) and per-particle state */
+    real beta;
+    real *adv_acc, *VF_alpha1;
+    real *sphDensity, *VF_gamma, *VF_sphVolume, *VF_advVol, *VF_alpha, *VF_alpha2, *VF_kappa, *VF_kappaV,
+        *VF_divdev;
     int *nnum; PIdx *nidx; real *ndis; /* neighbour lists, cap entries each */
     PIdx *next;
 } OrcFluid;
@@ -99,6 +114,8 @@ typedef struct {
     int n, rigid;
     real d, visc_alpha, rho0;
     real *pos, *vel, *svel, *volume, *kerSumFromSelf, *force;
+    /* IISph (volume form) per-particle state */
+    real *mass, *VF_gamma, *VF_sphVolume, *VF_advVol, *VF_alpha, *VF_alpha2, *VF_kappa, *VF_kappaV, *VF_divdev;
     int *nnum; PIdx *nidx; real *ndis;
     PIdx *next;
 } OrcSolid;
@@ -124,6 +141,8 @@ typedef struct {
     double err_density, err_div, err_pci, err_ii;
     real pci_delta, pci_last_dt, pci_last_sp, pci_last_h, pci_last_delta;
     int pci_init;
+    int it_iv_div, it_iv_cv;
+    double err_iv_div, err_iv_cv;
 } OrcScene;
 
 /* ---------------- kernels, SphBase.h:808-889 ---------------- */
@@ -343,6 +362,8 @@ static void copy_fluid_particle(OrcFluid* F, int dst, int src) {
     CP3(pos_pred) CP3(acce_pressure) CP3(dii) CP3(sum_dijpj) CP3(adv_vel) CP3(acce_presure)
     CP1(density) CP1(DFalpha) CP1(DFalpha2) CP1(DFkappa) CP1(DFkappaV) CP1(density_adv) CP1(divdev)
     CP1(presure) CP1(aii) CP1(rho_adv) CP1(p_l) CP1(p_l2)
+    CP3(adv_acc) CP3(VF_alpha1) CP1(sphDensity) CP1(VF_gamma) CP1(VF_sphVolume) CP1(VF_advVol) CP1(VF_alpha)
+    CP1(VF_alpha2) CP1(VF_kappa) CP1(VF_kappaV) CP1(VF_divdev)
 #undef CP3
 #undef CP1
 }
@@ -885,6 +906,7 @@ static void wc_step(OrcScene* s) {
 }
 
 #include "sph_oracle_pci_ii.inc"
+#include "sph_oracle_iisph.inc"
 
 /* ---------------- C interface ---------------- */
 
@@ -912,7 +934,9 @@ static void free_fluid(OrcFluid* F) {
     real* arrs[] = {F->pos, F->vel, F->vel_adv, F->acce_adv, F->acceleration, F->DFalpha1, F->n_surf,
                     F->density, F->DFalpha, F->DFalpha2, F->DFkappa, F->DFkappaV, F->density_adv, F->divdev,
                     F->presure, F->pos_pred, F->acce_pressure, F->dii, F->sum_dijpj, F->adv_vel,
-                    F->acce_presure, F->aii, F->rho_adv, F->p_l, F->p_l2, F->ndis};
+                    F->acce_presure, F->aii, F->rho_adv, F->p_l, F->p_l2, F->ndis,
+                    F->adv_acc, F->VF_alpha1, F->sphDensity, F->VF_gamma, F->VF_sphVolume, F->VF_advVol,
+                    F->VF_alpha, F->VF_alpha2, F->VF_kappa, F->VF_kappaV, F->VF_divdev};
     for (size_t i = 0; i < sizeof(arrs) / sizeof(arrs[0]); ++i) free(arrs[i]);
     free(F->nnum); free(F->nidx); free(F->next);
 }
@@ -923,6 +947,8 @@ void orc_destroy(void* h) {
     for (int k = 0; k < s->ns; ++k) {
         OrcSolid* S = &s->S[k];
         free(S->pos); free(S->vel); free(S->svel); free(S->volume); free(S->kerSumFromSelf); free(S->force);
+        free(S->mass); free(S->VF_gamma); free(S->VF_sphVolume); free(S->VF_advVol); free(S->VF_alpha);
+        free(S->VF_alpha2); free(S->VF_kappa); free(S->VF_kappaV); free(S->VF_divdev);
         free(S->nnum); free(S->nidx); free(S->ndis); free(S->next);
     }
     free(s->gridFirst);
@@ -937,6 +963,9 @@ int orc_add_solid(void* h, int n, const double* xyz, double d, double visc_alpha
     S->n = n; S->rigid = 1; S->d = (real)d; S->visc_alpha = (real)visc_alpha; S->rho0 = (real)rho0;
     ALLOC3(S->pos, n); ALLOC3(S->vel, n); ALLOC3(S->svel, n); ALLOC3(S->force, n);
     ALLOC1(S->volume, n); ALLOC1(S->kerSumFromSelf, n);
+    ALLOC1(S->mass, n); ALLOC1(S->VF_gamma, n); ALLOC1(S->VF_sphVolume, n); ALLOC1(S->VF_advVol, n);
+    ALLOC1(S->VF_alpha, n); ALLOC1(S->VF_alpha2, n); ALLOC1(S->VF_kappa, n); ALLOC1(S->VF_kappaV, n);
+    ALLOC1(S->VF_divdev, n);
     S->nnum = (int*)calloc((size_t)n + 1, sizeof(int));
     S->nidx = (PIdx*)calloc((size_t)n * s->P.cap + 1, sizeof(PIdx));
     S->ndis = (real*)calloc((size_t)n * s->P.cap + 1, sizeof(real));
@@ -960,6 +989,11 @@ int orc_add_fluid(void* h, int n, const double* xyz, const double* vel, double d
     ALLOC1(F->density, n); ALLOC1(F->DFalpha, n); ALLOC1(F->DFalpha2, n); ALLOC1(F->DFkappa, n);
     ALLOC1(F->DFkappaV, n); ALLOC1(F->density_adv, n); ALLOC1(F->divdev, n); ALLOC1(F->presure, n);
     ALLOC1(F->aii, n); ALLOC1(F->rho_adv, n); ALLOC1(F->p_l, n); ALLOC1(F->p_l2, n);
+    F->beta = 1;
+    ALLOC3(F->adv_acc, n); ALLOC3(F->VF_alpha1, n);
+    ALLOC1(F->sphDensity, n); ALLOC1(F->VF_gamma, n); ALLOC1(F->VF_sphVolume, n); ALLOC1(F->VF_advVol, n);
+    ALLOC1(F->VF_alpha, n); ALLOC1(F->VF_alpha2, n); ALLOC1(F->VF_kappa, n); ALLOC1(F->VF_kappaV, n);
+    ALLOC1(F->VF_divdev, n);
     F->nnum = (int*)calloc((size_t)n + 1, sizeof(int));
     F->nidx = (PIdx*)calloc((size_t)n * s->P.cap + 1, sizeof(PIdx));
     F->ndis = (real*)calloc((size_t)n * s->P.cap + 1, sizeof(real));
@@ -987,6 +1021,7 @@ int orc_stage(void* h, const char* name) {
     if (!strcmp(name, "wc_computePressure")) { wc_pressure(s); return 0; }
     if (!strcmp(name, "wc_computeForce")) { wc_force(s); return 0; }
     if (!strcmp(name, "wc_step")) { wc_step(s); return 0; }
+    if (orc_stage_iisph(s, name) == 0) return 0;
     return orc_stage_pci_ii(s, name);
 }
 
@@ -1000,6 +1035,10 @@ static int fluid_field(OrcFluid* F, const char* f, real** p) {
     V1("density", density) V1("DFalpha", DFalpha) V1("DFalpha2", DFalpha2) V1("DFkappa", DFkappa)
     V1("DFkappaV", DFkappaV) V1("density_adv", density_adv) V1("divergenceDeviation", divdev)
     V1("presure", presure) V1("aii", aii) V1("rho_adv", rho_adv) V1("p_l", p_l)
+    V3("advectionAcceleration", adv_acc) V3("VF_alpha1", VF_alpha1) V1("sphDensity", sphDensity)
+    V1("VF_gamma", VF_gamma) V1("VF_sphVolume", VF_sphVolume) V1("VF_advectionVolume", VF_advVol)
+    V1("VF_alpha", VF_alpha) V1("VF_alpha2", VF_alpha2) V1("VF_kappa", VF_kappa) V1("VF_kappaV", VF_kappaV)
+    V1("VF_divergenceDeviation", VF_divdev)
 #undef V3
 #undef V1
     return -1;
@@ -1029,6 +1068,15 @@ int orc_get_solid(void* h, int k, const char* field, double* out) {
     else if (!strcmp(field, "force")) { p = S->force; c = 3; }
     else if (!strcmp(field, "volume")) { p = S->volume; c = 1; }
     else if (!strcmp(field, "kerSumFromSelf")) { p = S->kerSumFromSelf; c = 1; }
+    else if (!strcmp(field, "mass")) { p = S->mass; c = 1; }
+    else if (!strcmp(field, "VF_gamma")) { p = S->VF_gamma; c = 1; }
+    else if (!strcmp(field, "VF_sphVolume")) { p = S->VF_sphVolume; c = 1; }
+    else if (!strcmp(field, "VF_advectionVolume")) { p = S->VF_advVol; c = 1; }
+    else if (!strcmp(field, "VF_alpha")) { p = S->VF_alpha; c = 1; }
+    else if (!strcmp(field, "VF_alpha2")) { p = S->VF_alpha2; c = 1; }
+    else if (!strcmp(field, "VF_kappa")) { p = S->VF_kappa; c = 1; }
+    else if (!strcmp(field, "VF_kappaV")) { p = S->VF_kappaV; c = 1; }
+    else if (!strcmp(field, "VF_divergenceDeviation")) { p = S->VF_divdev; c = 1; }
     else return -1;
     for (long i = 0; i < (long)c * S->n; ++i) out[i] = (double)p[i];
     return 0;
@@ -1089,6 +1137,14 @@ void orc_stats(void* h, int* iters, double* errs, double* dt, int* frame) {
     iters[0] = s->it_density; iters[1] = s->it_div; iters[2] = s->it_pci; iters[3] = s->it_ii;
     errs[0] = s->err_density; errs[1] = s->err_div; errs[2] = s->err_pci; errs[3] = s->err_ii;
     *dt = s->P.dt; *frame = s->frame;
+}
+
+/* IISph (volume form): iterations and errors of the last divergence-free and
+ * constant-volume loops (summed over phases) */
+void orc_vf_stats(void* h, int* iters, double* errs) {
+    OrcScene* s = (OrcScene*)h;
+    iters[0] = s->it_iv_div; iters[1] = s->it_iv_cv;
+    errs[0] = s->err_iv_div; errs[1] = s->err_iv_cv;
 }
 
 void orc_set_dt(void* h, double dt) { ((OrcScene*)h)->P.dt = dt; }

@@ -20,8 +20,13 @@ oracle/_ref/) on small seeded scenes and records its outputs:
   step_iisphm.npz   IISph_M::sphStep x 3 from the same state, run with one
                     OpenMP thread (the reference's pressure loop races on
                     p_l and on its error sums, IISph_M.cpp:320-350)
+  step_iisph.npz    IISph::sphStep x 3 (volume form) from the same state and
+                    phases, one OpenMP thread (its error sums run under
+                    `omp critical` in thread order, IISph.cpp:785,1437),
+                    with the boundary particles' own loop state
 Run in the build container (the reference tree must be present):
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            # all fixtures
+    python tests/golden/make_golden.py step_iisph # one of them
 """
 import os
 import sys
@@ -79,9 +84,28 @@ def make_settled_column():
 
 
 MULTI_FIELDS = ("position", "velocity", "density", "presure")
+IV_FIELDS = ("position", "velocity", "sphDensity", "VF_gamma", "VF_sphVolume", "VF_alpha", "VF_kappa",
+             "VF_kappaV", "VF_advectionVolume", "acce_presure")
+IV_SOLID_FIELDS = ("VF_gamma", "VF_sphVolume", "VF_alpha", "VF_kappa", "VF_kappaV")
+
+
+def make_step_iisph():
+    col = column_scene()
+    o = make_scene_oracle(col, kind="reference", solver="iisph", **MULTI_VISC, **II_KW)
+    o.set_threads(1)
+    for _ in range(3):
+        o.stage("runOneStep")
+    out = {"%s_%d" % (f, k): o.get(f, k).astype(np.float32) for k in range(2) for f in IV_FIELDS}
+    out.update({"solid_%s" % f: o.get_solid(f).astype(np.float32) for f in IV_SOLID_FIELDS})
+    np.savez_compressed(os.path.join(HERE, "step_iisph.npz"), **out)
+    o.close()
 
 
 def main():
+    if len(sys.argv) > 1:
+        for name in sys.argv[1:]:
+            globals()["make_" + name]()
+        return
     sc = scene()
     o = make_scene_oracle(sc, kind="reference", solver="dfsph", **DF_KW)
     o.stage("neighbourSearch")
@@ -130,6 +154,7 @@ def main():
                            for k in range(2)
                            for f in MULTI_FIELDS + ("dii", "aii", "rho_adv", "sum_dijpj", "acce_presure")})
     o.close()
+    make_step_iisph()
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))
