@@ -11,7 +11,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libsphgpu.so")
 
 OK, EINVAL, ENOMEM, ECUDA, EMAXITER, ENAN, ENEIGHBOUR_OVERFLOW, EOUT_OF_DOMAIN, ENOTIMPL = 0, -1, -2, -3, -4, -5, -6, -7, -8
-WCSPH, PCISPH, IISPH_M, DFSPH = 0, 1, 2, 3
+WCSPH, PCISPH, IISPH_M, DFSPH, IISPH = 0, 1, 2, 3, 4
 STATUS_MAXITER_DENSITY, STATUS_MAXITER_DIVERGENCE, STATUS_NAN = 1, 2, 4
 STATUS_NEIGHBOUR_OVERFLOW, STATUS_OUT_OF_DOMAIN, STATUS_ZERO_DISTANCE = 8, 16, 32
 
@@ -30,7 +30,10 @@ class SphParams(C.Structure):
                 ("wc_gamma", C.c_float), ("pci_min_iter", C.c_int), ("pci_max_iter", C.c_int),
                 ("ii_omega", C.c_float), ("ii_eta_rel", C.c_float), ("ii_min_iter", C.c_int),
                 ("ii_max_iter", C.c_int), ("warm_start", C.c_int), ("ws_scale", C.c_float),
-                ("ii_compat", C.c_int), ("reserved", C.c_int * 5)]
+                ("ii_compat", C.c_int),
+                ("iv_kvisc", C.c_float), ("iv_kvisc_b", C.c_float), ("iv_cv_goal", C.c_float),
+                ("iv_div_goal", C.c_float), ("iv_cv_min_iter", C.c_int), ("iv_cv_max_iter", C.c_int),
+                ("iv_div_min_iter", C.c_int), ("iv_div_max_iter", C.c_int), ("reserved", C.c_int * 5)]
 
 
 class SphStepStats(C.Structure):

@@ -64,6 +64,14 @@ struct SolverConst {
     float ws_scale;    // applied fraction of the predicted warm-start stiffness
     int cap;           // neighbour cap
     int stride;        // ELL column stride (>= fluid capacity)
+    // IISph (volume form, IISph.cpp): spline of the per-pair h = (d_a + d_b)/2
+    // (= d, one diameter for all particles), rest volume d^3, per-phase mass
+    // rho0 * beta * d^3 (beta = 1), kinematic viscosity of fluid / boundary
+    KerConst kd;
+    float iv_V;
+    float iv_m[4];
+    float iv_kv, iv_kvb;
+    int iv_multi_solid;  // 1 if the walls hold more than one solid (boundary lists then see the others)
 };
 
 // -------- cubic spline, SphBase.h:840-889 (single-h forms) --------
@@ -101,6 +109,19 @@ __device__ __forceinline__ void kernel_pair(const KerConst& k, float len2, float
     const float fin = k.g_in * fmaf(-2.25f, q, 3.f);
     const float fout = k.g_out * t * t * inv_r;
     f = q <= 1.f ? fin : fout;
+}
+
+// W(r) and -W'(r)/r evaluated as the reference does: r = sqrt(len2) and
+// q = r / h correctly rounded, so 2 - q is the reference's.  For sums whose
+// result can hinge on a single pair near the cut (a boundary particle with
+// one fluid neighbour), where the rsqrt form's few-ulp error in q becomes a
+// large relative error in (2 - q)^2.
+__device__ __forceinline__ void kernel_pair_rn(const KerConst& k, float len2, float& w, float& f) {
+    const float r = __fsqrt_rn(len2);
+    const float q = __fdiv_rn(r, k.h), qm2 = 2.f - q;
+    w = q <= 1.f ? k.theta * (1.f - 1.5f * q * q + 0.75f * q * q * q) : k.theta * (0.25f * qm2 * qm2 * qm2);
+    const float g = q <= 1.f ? k.thetah * (3.f * q - 2.25f * q * q) : k.thetah * 0.75f * qm2 * qm2;
+    f = __fdiv_rn(-g, r);
 }
 
 // per-pair-h spline with range check, SphBase.h:855-871

@@ -88,6 +88,7 @@ struct sphgpu_scene {
     std::vector<int> bgid_h;
     std::vector<int> bsolid_h;
     int nb = 0;
+    int iv_multi_solid = 0;  // walls hold more than one solid id
     int record_ksum = 0;
     // learned warm start: 0 off, 1 apply the network, 2 record training data
     sphgpu_mlp* mlp = nullptr;
@@ -227,6 +228,21 @@ void fill_solver_const(sphgpu_scene* h) {
     c.cap = h->ncap;
     c.stride = h->stride;
     c.ws_scale = P.ws_scale;
+    // IISph: per-pair h = (d + d)/2 = d (SphBase.h:855-915 with one diameter)
+    {
+        const float hd = (P.particle_d + P.particle_d) / 2;
+        c.kd.h = hd;
+        c.kd.inv_h = 1.f / hd;
+        c.kd.theta = 1 / (float)M_PI / (hd * hd * hd);
+        c.kd.thetah = 1 / (float)M_PI / (hd * hd * hd) / hd;
+        c.kd.g_in = -c.kd.thetah / hd;
+        c.kd.g_out = -0.75f * c.kd.thetah;
+        c.iv_V = (float)std::pow((double)P.particle_d, 3);  // std::pow(d, vec_t::dim), IISph.cpp:109
+        for (int i = 0; i < 4; ++i) c.iv_m[i] = c.rho0_ph[i] * c.iv_V;  // rho0 * beta * V, beta = 1
+        c.iv_kv = P.iv_kvisc;
+        c.iv_kvb = P.iv_kvisc_b;
+        c.iv_multi_solid = h->iv_multi_solid;
+    }
     // alpha of an interior particle of the ideal cubic lattice (spacing d),
     // the normalisation of the warm-start feature log(alpha / alpha_ref)
     {
@@ -271,7 +287,7 @@ int alloc_scene(sphgpu_scene* h) {
     r |= dalloc(h, &d.hist_s, n);
     r |= dalloc(h, &d.cA, n); r |= dalloc(h, &d.cB, n); r |= dalloc(h, &d.cC, n);
     r |= dalloc(h, &d.cA_s, n); r |= dalloc(h, &d.cB_s, n); r |= dalloc(h, &d.cC_s, n);
-    r |= dalloc(h, &d.ap, n); r |= dalloc(h, &d.pl2, n);
+    r |= dalloc(h, &d.ap, n); r |= dalloc(h, &d.pl2, n); r |= dalloc(h, &d.ivs, n);
     r |= dalloc(h, &d.key, n); r |= dalloc(h, &d.slot, n); r |= dalloc(h, &d.tmp, n);
     r |= dalloc(h, &d.cell_count, (size_t)h->g.nkeys + 1);
     r |= dalloc(h, &d.cell_start, (size_t)h->g.nkeys + 1);
@@ -307,7 +323,8 @@ void free_scene(sphgpu_scene* h) {
     DevScene& d = h->d;
     void* ptrs[] = {d.pos, d.vel, d.gid, d.rho, d.alpha, d.vadv, d.pv, d.pk, d.bpv, d.kappav, d.acc, d.kr, d.kappa, d.ksum, d.aux0,
                     d.aux1, d.aux4, d.kwarm, d.hist, d.wsbuf, d.pos_s, d.vel_s, d.gid_s, d.hist_s, d.key, d.slot, d.tmp,
-                    d.cA, d.cB, d.cC, d.cA_s, d.cB_s, d.cC_s, d.ap, d.pl2,
+                    d.cA, d.cB, d.cC, d.cA_s, d.cB_s, d.cC_s, d.ap, d.pl2, d.ivs,
+                    d.bsid, d.bnbr, d.bncount, d.bivs, d.bivo,
                     h->recX, h->recY, h->xn,
                     d.cell_count, d.cell_start, d.bcell_start, d.cstart2, d.nbr, d.ncount, d.partial, d.st,
                     d.bpos, d.bvel, d.bgid, h->cub_tmp};
@@ -553,8 +570,80 @@ int enq_ii_step(sphgpu_scene* h, bool capturing) {
     return 0;
 }
 
+void invalidate_graphs(sphgpu_scene* h);
+
+// IISph boundary state (allocated on first use: other solvers never need it)
+int ensure_iv_boundary(sphgpu_scene* h) {
+    DevScene& d = h->d;
+    if (d.bivs || h->nb == 0) return 0;
+    const int nb = h->nb;
+    d.bstride = roundup(nb, 32);
+    int r = dalloc(h, &d.bsid, nb) | dalloc(h, &d.bncount, nb) | dalloc(h, &d.bivs, nb) | dalloc(h, &d.bivo, nb) |
+            dalloc(h, &d.bnbr, (size_t)d.bstride * ((h->ncap + 3) / 4) * 4);
+    if (r) return SPHGPU_ENOMEM;
+    CK(cudaMemcpy(d.bsid, h->bsolid_h.data(), sizeof(int) * nb, cudaMemcpyHostToDevice));
+    CK(cudaMemset(d.bivs, 0, sizeof(float4) * nb));
+    CK(cudaMemset(d.bivo, 0, sizeof(float4) * nb));
+    CK(cudaMemset(d.bncount, 0, sizeof(int) * nb));
+    invalidate_graphs(h);
+    return 0;
+}
+
+// neighbour lists of fluid and boundary particles with IISph's
+// DF_prepareAttribute / VF_prepareAttribute terms (IISph.cpp:100-545); the
+// carried loop velocity (cA) and stiffnesses (cC) follow the reorder
+void enq_iv_prepare(sphgpu_scene* h, bool from_staging, cudaStream_t st) {
+    DevScene& d = h->d;
+    if (from_staging) enq_ns(h, 0, 3, st, 2 | 8);
+    else launch(h, "build_iisph", st, [&] { launch_build(d, h->g, h->c, 3, h->cap, st, h->tune.build); });
+    launch(h, "iv_boundary_build", st, [&] { launch_iv_boundary_build(d, h->g, h->c, h->tune.build, st); });
+}
+
+// the divergence-free (div = 1, IISph.cpp:1219-1456) or constant-volume
+// (div = 0, :546-815) loops, phase by phase
+int enq_iv_loops(sphgpu_scene* h, bool capturing, int div) {
+    DevScene& d = h->d;
+    const SphParams& P = h->P;
+    const double goal = (double)(div ? P.iv_div_goal : P.iv_cv_goal);  // real_t goals (float)
+    const int mn = div ? P.iv_div_min_iter : P.iv_cv_min_iter, mx = div ? P.iv_div_max_iter : P.iv_cv_max_iter;
+    const int nph = (int)h->rho0_ph.size();
+    for (int ph = 0; ph < nph; ++ph) {
+        launch_iv_phase_begin(d, h->stream);
+        launch(h, "iv_loop_init", h->stream, [&] { launch_iv_loop_init(d, ph, div, h->cap, h->stream); });
+        int r = enq_loop(h, capturing, [&](cudaStream_t s2, unsigned long long hd, int use) {
+            launch(h, div ? "iv_div_boundary" : "iv_cv_boundary", s2,
+                   [&] { launch_iv_boundary_sweep(d, h->c, div, h->tune.sweep_a, s2); });
+            launch(h, div ? "iv_div_a" : "iv_cv_a", s2,
+                   [&] { launch_iv_sweep_a(d, h->c, ph, div, h->cap, h->tune.sweep_a, s2); });
+            launch(h, div ? "iv_div_b" : "iv_cv_b", s2, [&] {
+                launch_iv_sweep_b(d, h->c, ph, div, goal, mn, mx, hd, use, h->cap, h->tune.sweep_b, s2);
+            });
+        });
+        if (r) return r;
+    }
+    return 0;
+}
+
+// One IISph step (IISph::sphStep, IISph.cpp:14-99): the state enters and
+// leaves in the staging arrays, like PCISPH and IISPH_M.
+int enq_iv_step(sphgpu_scene* h, bool capturing) {
+    DevScene& d = h->d;
+    cudaStream_t st = h->stream;
+    launch_step_begin(d, st);
+    enq_iv_prepare(h, true, st);
+    launch(h, "iv_forces", st, [&] { launch_iv_forces(d, h->c, h->cap, h->tune.forces, st); });
+    int r = enq_iv_loops(h, capturing, 1);
+    if (r) return r;
+    r = enq_iv_loops(h, capturing, 0);
+    if (r) return r;
+    launch(h, "iv_integrate", st, [&] { launch_iv_integrate(d, h->cap, st); });
+    CK(cudaMemcpyAsync(h->h_stats, d.st, sizeof(DevStats), cudaMemcpyDeviceToHost, st));
+    return 0;
+}
+
 int pci_graph_build(sphgpu_scene* h, bool cap) { return enq_pci_step(h, cap); }
 int ii_graph_build(sphgpu_scene* h, bool cap) { return enq_ii_step(h, cap); }
+int iv_graph_build(sphgpu_scene* h, bool cap) { return enq_iv_step(h, cap); }
 
 int run_initial_ns(sphgpu_scene* h, int build_mode) {
     if (!h->in_staging) stage_from_sorted(h, h->h_stats->n_active);  // the sort reads staging
@@ -628,7 +717,8 @@ void fill_stats(sphgpu_scene* h, SphStepStats* o, int steps) {
 }
 
 int enq_steps(sphgpu_scene* h, int solver, int nsteps) {
-    if (solver != SPHGPU_DFSPH && solver != SPHGPU_WCSPH && solver != SPHGPU_PCISPH && solver != SPHGPU_IISPH_M) {
+    if (solver != SPHGPU_DFSPH && solver != SPHGPU_WCSPH && solver != SPHGPU_PCISPH && solver != SPHGPU_IISPH_M &&
+        solver != SPHGPU_IISPH) {
         h->err = "unknown solver";
         return SPHGPU_EINVAL;
     }
@@ -646,7 +736,11 @@ int enq_steps(sphgpu_scene* h, int solver, int nsteps) {
     }
     launch_call_begin(h->d, h->stream);
     if (h->nscenes > 1) launch_batch_call_begin(h->d, h->nscenes, h->stream);
-    if (solver == SPHGPU_PCISPH || solver == SPHGPU_IISPH_M) {
+    if (solver == SPHGPU_PCISPH || solver == SPHGPU_IISPH_M || solver == SPHGPU_IISPH) {
+        if (solver == SPHGPU_IISPH) {
+            int r = ensure_iv_boundary(h);
+            if (r) return r;
+        }
         if (h->last_solver != solver && h->last_solver >= 0) {
             // entering from another solver: the carried state starts as the
             // reference's fresh particles (the last density, zeros)
@@ -657,12 +751,15 @@ int enq_steps(sphgpu_scene* h, int solver, int nsteps) {
         for (int s = 0; s < nsteps; ++s) {
             if (h->use_graphs && !h->prof.on) {
                 cudaGraphExec_t ex;
-                const int key = solver == SPHGPU_PCISPH ? 100 : 200;
-                int r = graph_for(h, key, &ex, solver == SPHGPU_PCISPH ? pci_graph_build : ii_graph_build);
+                const int key = solver == SPHGPU_PCISPH ? 100 : (solver == SPHGPU_IISPH_M ? 200 : 300);
+                int r = graph_for(h, key, &ex,
+                                  solver == SPHGPU_PCISPH ? pci_graph_build
+                                                          : (solver == SPHGPU_IISPH_M ? ii_graph_build : iv_graph_build));
                 if (r) return r;
                 CK(cudaGraphLaunch(ex, h->stream));
             } else {
-                int r = solver == SPHGPU_PCISPH ? enq_pci_step(h, false) : enq_ii_step(h, false);
+                int r = solver == SPHGPU_PCISPH ? enq_pci_step(h, false)
+                                                : (solver == SPHGPU_IISPH_M ? enq_ii_step(h, false) : enq_iv_step(h, false));
                 if (r) return r;
                 prof_collect(h);
             }
@@ -767,6 +864,14 @@ int sphgpu_params_default(SphParams* p) {
     p->ii_max_iter = 100;
     p->warm_start = 0;
     p->ws_scale = 1.0f;
+    p->iv_kvisc = 0.1f;
+    p->iv_kvisc_b = 0.1f;
+    p->iv_cv_goal = 1e-4f;
+    p->iv_div_goal = 1e-3f;
+    p->iv_cv_min_iter = 3;
+    p->iv_cv_max_iter = 100;
+    p->iv_div_min_iter = 2;
+    p->iv_div_max_iter = 50;
     return 0;
 }
 
@@ -911,6 +1016,10 @@ static int set_boundary_impl(sphgpu_t h, int n, const float* xyz, const int* sol
         for (int i = 0; i < n; ++i)
             if (scene[i] < 0 || scene[i] >= h->nscenes) { h->err = "boundary scene index out of range"; return SPHGPU_EINVAL; }
     if (d.bpos) { cudaFree(d.bpos); cudaFree(d.bvel); cudaFree(d.bgid); cudaFree(d.bpv); d.bpos = nullptr; }
+    for (void* q : {(void*)d.bsid, (void*)d.bnbr, (void*)d.bncount, (void*)d.bivs, (void*)d.bivo})
+        if (q) cudaFree(q);
+    d.bsid = d.bnbr = d.bncount = nullptr;
+    d.bivs = d.bivo = nullptr;
     h->nb = n;
     d.nb = n;
     std::vector<float4> bp(n);
@@ -976,6 +1085,10 @@ static int set_boundary_impl(sphgpu_t h, int n, const float* xyz, const int* sol
         start[keys[perm[i]] + 1]++;
     }
     for (int k = 0; k < h->g.nkeys; ++k) start[k + 1] += start[k];
+    h->iv_multi_solid = 0;
+    for (int i = 1; i < n; ++i)
+        if (h->bsolid_h[i] != h->bsolid_h[0]) h->iv_multi_solid = 1;
+    fill_solver_const(h);
     CK(cudaMemcpy(d.bpos, sp.data(), sizeof(float4) * n, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(d.bvel, sv.data(), sizeof(float4) * n, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(d.bgid, h->bgid_h.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
@@ -1195,7 +1308,33 @@ int sphgpu_get_fluid(sphgpu_t h, const char* field, float* out) {
         f4 = true;
         comps = 3;
     }
-    else if (f == "acce_adv" || f == "acceleration" || f == "acce_presure") { src = d.acc; f4 = true; comps = 3; }
+    else if (f == "acce_adv" || f == "acceleration" || (f == "acce_presure" && h->last_solver != SPHGPU_IISPH) ||
+             f == "advectionAcceleration") {
+        src = d.acc;
+        f4 = true;
+        comps = 3;
+    }
+    else if (f == "acce_presure") { src = d.ap; f4 = true; comps = 3; }
+    else if (f == "advectionVelocity") {
+        CK(cudaMemcpy2D(d.vadv, sizeof(float4), d.pv + 1, 2 * sizeof(float4), sizeof(float4), n,
+                        cudaMemcpyDeviceToDevice));
+        src = d.vadv;
+        f4 = true;
+        comps = 3;
+    }
+    else if (f == "sphDensity" || f == "VF_gamma" || f == "VF_sphVolume" || f == "VF_alpha") {
+        std::vector<float4> t(n);
+        CK(cudaMemcpy(t.data(), d.ivs, sizeof(float4) * n, cudaMemcpyDeviceToHost));
+        for (int k = 0; k < n; ++k) {
+            const float4& v = t[order[k]];
+            out[k] = f == "VF_gamma" ? v.x : (f == "VF_sphVolume" ? v.y : (f == "VF_alpha" ? v.z : v.w));
+        }
+        return n;
+    }
+    else if (f == "VF_kappa") src = d.kappa;
+    else if (f == "VF_kappaV") src = d.kappav;
+    else if (f == "VF_advectionVolume") src = d.aux0;
+    else if (f == "VF_divergenceDeviation") src = d.aux1;
     else if (f == "acce_pressure") { src = d.ap; f4 = true; comps = 3; }
     else if (f == "pos_prediction") { src = d.aux4; f4 = true; comps = 3; }
     else if (f == "dii") { src = d.cB; f4 = true; comps = 3; }
@@ -1338,11 +1477,27 @@ int sphgpu_get_boundary(sphgpu_t h, const char* field, float* out) {
     std::vector<float4> t(n);
     CK(cudaMemcpy(t.data(), h->d.bpos, sizeof(float4) * n, cudaMemcpyDeviceToHost));
     std::string f(field);
+    if (f != "position" && f != "volume") {
+        // IISph boundary loop state
+        static const char* names[8] = {"VF_gamma", "VF_sphVolume", "VF_alpha", nullptr,
+                                       "VF_kappa", "VF_kappaV", "VF_advectionVolume", "VF_divergenceDeviation"};
+        int which = -1;
+        for (int i = 0; i < 8; ++i)
+            if (names[i] && f == names[i]) which = i;
+        if (which < 0) { h->err = "unknown boundary field"; return SPHGPU_EINVAL; }
+        if (!h->d.bivs) { h->err = "no IISph boundary state (run an IISph step first)"; return SPHGPU_EINVAL; }
+        CK(cudaMemcpy(t.data(), which < 4 ? h->d.bivs : h->d.bivo, sizeof(float4) * n, cudaMemcpyDeviceToHost));
+        for (int i = 0; i < n; ++i) {
+            const float4& v = t[i];
+            const int c = which & 3;
+            out[h->bgid_h[i]] = c == 0 ? v.x : (c == 1 ? v.y : (c == 2 ? v.z : v.w));
+        }
+        return n;
+    }
     for (int i = 0; i < n; ++i) {
         int k = h->bgid_h[i];
         if (f == "position") { out[3 * k] = t[i].x; out[3 * k + 1] = t[i].y; out[3 * k + 2] = t[i].z; }
-        else if (f == "volume") out[k] = t[i].w;
-        else { h->err = "unknown boundary field"; return SPHGPU_EINVAL; }
+        else out[k] = t[i].w;
     }
     return n;
 }
@@ -1390,6 +1545,19 @@ int sphgpu_stage(sphgpu_t h, const char* name, SphStepStats* stats) {
         if (h->in_staging) { h->err = "run neighbourSearch first"; return SPHGPU_EINVAL; }
         r = enq_df_div_loop(h, false);
         if (r) return r;
+    } else if (s == "VF_prepareAttribute") {
+        if ((r = ensure_iv_boundary(h))) return r;
+        enq_iv_prepare(h, h->in_staging, st);
+        h->in_staging = false;
+        h->ns_valid = false;
+    } else if (s == "advectionStep" || s == "VF_divergenceFreeSolver" || s == "VF_constantVolumeSolver" ||
+               s == "iv_updateFluids") {
+        if (h->in_staging || (h->nb > 0 && !d.bivs)) { h->err = "run VF_prepareAttribute first"; return SPHGPU_EINVAL; }
+        if (s == "advectionStep") launch_iv_forces(d, h->c, h->cap, h->tune.forces, st);
+        else if (s == "iv_updateFluids") {
+            launch_iv_integrate(d, h->cap, st);
+            h->in_staging = true;
+        } else if ((r = enq_iv_loops(h, false, s == "VF_divergenceFreeSolver"))) return r;
     } else if (s == "wc_computeForce") {
         if (h->in_staging) { h->err = "run neighbourSearch first"; return SPHGPU_EINVAL; }
         launch_wc_force(d, h->c, h->cap, st);

@@ -120,7 +120,8 @@ __global__ void k_merge_starts(DevScene s, int nk) {
 
 // mode 0: neighbour lists only; 1: + DFSPH rho and alpha
 // (DF_constantDensitySolverFirst, DFSPH.cpp:84-193); 2: + WCSPH rho and Tait
-// pressure (WcSph::wc_computePressure, WcSph.cpp:99-153).
+// pressure (WcSph::wc_computePressure, WcSph.cpp:99-153); 3: + IISph
+// sphDensity, gamma, sphVolume and alpha (IISph.cpp:100-402).
 template <int MODE, int BS>
 __global__ void __launch_bounds__(BS) k_build(DevScene s, GridGeom g, SolverConst c) {
     const int n = s.st->n_active;
@@ -180,7 +181,40 @@ __global__ void __launch_bounds__(BS) k_build(DevScene s, GridGeom g, SolverCons
             }
         }
         s.ncount[p] = cnt;
-        if (MODE != 0) {
+        if (MODE == 3) {
+            // IISph: sphDensity (DF_prepareAttribute, IISph.cpp:127-170) and
+            // VF_prepareAttribute (IISph.cpp:309-402) over the stored list,
+            // per-pair h = (d_a + d_b)/2 = d (one diameter for all particles)
+            const float Va = c.iv_V, ma = c.iv_m[ph], rda = rho0;
+            const float w0 = c.kd.theta;  // W(0, d)
+            float density = w0 * ma;
+            float gamma = Va * w0;
+            float sphv = (float)((double)w0 * (double)Va * (double)Va);
+            float a1x = 0.f, a1y = 0.f, a1z = 0.f, a2 = 0.f;
+            for (int k = 0; k < cnt; ++k) {
+                const unsigned e = (unsigned)out[ell_index(stride, p, k)];
+                const bool bnd = (e & BND_FLAG) != 0u;
+                const float4 pb = __ldg((bnd ? BP : P) + (e & BND_MASK));
+                const float xx = pa.x - pb.x, xy = pa.y - pb.y, xz = pa.z - pb.z;
+                const float len2 = dis_square_rn(pa.x, pa.y, pa.z, pb.x, pb.y, pb.z);
+                float w, f;
+                kernel_pair_rn(c.kd, len2, w, f);
+                const float Vb = bnd ? pb.w : Va;
+                density = fmaf(bnd ? rda * Vb : c.iv_m[phase_of(pb)], w, density);
+                gamma = fmaf(Vb, w, gamma);
+                sphv = fmaf(Va * Vb, w, sphv);
+                const float fv = f * Vb;
+                a1x = fmaf(xx, fv, a1x);
+                a1y = fmaf(xy, fv, a1y);
+                a1z = fmaf(xz, fv, a1z);
+                // V_b^2 |gradW|^2 / m_b: fluid neighbours only (boundary terms
+                // belong to dynamic solids, IISph.cpp:386-393)
+                if (!bnd) a2 = fmaf(fv * fv, len2 / c.iv_m[phase_of(pb)], a2);
+            }
+            float al = ((a1x * a1x + a1y * a1y + a1z * a1z) / ma + a2) / gamma;
+            if (al < 1.0e-10f) al = 1.0e-10f;
+            s.ivs[p] = make_float4(gamma, sphv, 1.f / al, density);
+        } else if (MODE != 0) {
             // phase 2: rho and alpha over the stored list (all lanes busy)
             float density = ker_W(c.k, 0.f) * fm0;
             float a1x = 0.f, a1y = 0.f, a1z = 0.f, a2 = 0.f;
@@ -328,7 +362,8 @@ static void launch_build_bs(const DevScene& s, const GridGeom& g, const SolverCo
     const int nb = nblk(n_max > 0 ? n_max : 1, BS);
     if (mode == 0) k_build<0, BS><<<nb, BS, 0, st>>>(s, g, c);
     else if (mode == 1) k_build<1, BS><<<nb, BS, 0, st>>>(s, g, c);
-    else k_build<2, BS><<<nb, BS, 0, st>>>(s, g, c);
+    else if (mode == 2) k_build<2, BS><<<nb, BS, 0, st>>>(s, g, c);
+    else k_build<3, BS><<<nb, BS, 0, st>>>(s, g, c);
 }
 
 void launch_build(const DevScene& s, const GridGeom& g, const SolverConst& c, int mode, int n_max, cudaStream_t st,

@@ -87,8 +87,9 @@ struct DevScene {
     float4* cA_s;
     float4* cB_s;
     float4* cC_s;
-    float4* ap;         // PCISPH pressure acceleration
+    float4* ap;         // PCISPH pressure acceleration; IISph acce_presure
     float* pl2;         // IISPH_M previous Jacobi iterate
+    float4* ivs;        // IISph: (VF_gamma, VF_sphVolume, VF_alpha, sphDensity)
     int* key;
     int* slot;
     int* tmp;
@@ -104,6 +105,14 @@ struct DevScene {
     int* bcell_start;   // nkeys + 1
     int* bgid;          // boundary reference index (solid-major)
     int nb;
+    // IISph boundary particles: their own per-step neighbour lists (fluid
+    // entries, ELL4 with stride bstride) and loop state
+    int* bsid;          // solid of each sorted boundary particle
+    int* bnbr;
+    int* bncount;
+    float4* bivs;       // (VF_gamma, VF_sphVolume, VF_alpha, kappa/gamma of the current loop)
+    float4* bivo;       // (VF_kappa, VF_kappaV, VF_advectionVolume, VF_divergenceDeviation)
+    int bstride;
     int cap_fluid;      // fluid array capacity
     // reductions
     double* partial;    // >= number of blocks of a particle launch
@@ -128,7 +137,8 @@ void launch_hash(const DevScene& s, const GridGeom& g, int integrate, int n_old,
 // carry: bit 0 hist, bit 1 cA, bit 2 cB, bit 3 cC (staging -> sorted)
 void launch_scatter_reorder(const DevScene& s, const GridGeom& g, int n_old, int carry, cudaStream_t st);
 void launch_count_active(const DevScene& s, const GridGeom& g, cudaStream_t st);
-// mode 0: lists only; 1: lists + DFSPH rho/alpha; 2: lists + WCSPH rho/pressure
+// mode 0: lists only; 1: lists + DFSPH rho/alpha; 2: lists + WCSPH rho/pressure;
+// 3: lists + IISph VF_prepareAttribute / sphDensity (ivs)
 void launch_build(const DevScene& s, const GridGeom& g, const SolverConst& c, int mode, int n_max, cudaStream_t st,
                   int bs = 128);
 void launch_to_ref_order(const float4* src, const int* gid, int n, float* dst3, cudaStream_t st);
@@ -182,6 +192,21 @@ void launch_ii_press(const DevScene& s, const SolverConst& c, int phase, double 
                      int max_it, int compat, unsigned long long cond_handle, int use_handle, int n_max,
                      cudaStream_t st);
 void launch_ii_force(const DevScene& s, const SolverConst& c, int compat, int n_max, cudaStream_t st);
+// ---- IISph, volume form (sph_iisph.cu) ----
+// boundary particles' neighbour lists and VF_prepareAttribute terms
+void launch_iv_boundary_build(const DevScene& s, const GridGeom& g, const SolverConst& c, int bs, cudaStream_t st);
+// advectionStep (gravity + viscosity); loop velocities start from the carried ones
+void launch_iv_forces(const DevScene& s, const SolverConst& c, int n_max, int bs, cudaStream_t st);
+void launch_iv_phase_begin(const DevScene& s, cudaStream_t st);
+// loop velocity of phase `phase`: v (div) or v + a dt (constant volume); counts the phase
+void launch_iv_loop_init(const DevScene& s, int phase, int div, int n_max, cudaStream_t st);
+void launch_iv_boundary_sweep(const DevScene& s, const SolverConst& c, int div, int bs, cudaStream_t st);
+void launch_iv_sweep_a(const DevScene& s, const SolverConst& c, int phase, int div, int n_max, int bs, cudaStream_t st);
+void launch_iv_sweep_b(const DevScene& s, const SolverConst& c, int phase, int div, double goal, int min_it,
+                       int max_it, unsigned long long cond_handle, int use_handle, int n_max, int bs, cudaStream_t st);
+// acce_presure, v += acce_presure dt, x += v dt into the staging arrays (carried: v_adv)
+void launch_iv_integrate(const DevScene& s, int n_max, cudaStream_t st);
+
 // carried state of particles coming from another solver: cB = (0, rho), cA = cC = 0
 // (staging: rho = the phase's rest density)
 void launch_carry_init(const DevScene& s, const SolverConst& c, int staging, int n_max, cudaStream_t st);

@@ -23,10 +23,12 @@ import numpy as np
 from . import _lib
 from ._lib import SphParams, SphStepStats, SphGpuError
 
-SOLVERS = {"wcsph": _lib.WCSPH, "pcisph": _lib.PCISPH, "iisph_m": _lib.IISPH_M, "dfsph": _lib.DFSPH}
+SOLVERS = {"wcsph": _lib.WCSPH, "pcisph": _lib.PCISPH, "iisph_m": _lib.IISPH_M, "dfsph": _lib.DFSPH,
+           "iisph": _lib.IISPH}
 
 VEC_FIELDS = ("position", "velocity", "vel_adv", "acce_adv", "acceleration", "ws_hist", "acce_pressure",
-              "pos_prediction", "dii", "sum_dijpj", "ii_vel_adv", "acce_presure")
+              "pos_prediction", "dii", "sum_dijpj", "ii_vel_adv", "acce_presure", "advectionAcceleration",
+              "advectionVelocity")
 
 
 def _fptr(a):
@@ -569,6 +571,30 @@ class IISph_M(SphBase):
     def _params(self):
         p = super()._params()
         p.ii_compat = int(self.ii_compat)
+        return p
+
+
+class IISph(SphBase):
+    """IISph, the volume form (IISph.h, IISph.cpp): per-pair kernel h,
+    boundary particles with their own divergence / volume error, a
+    divergence-free loop (goal 1e-3 on mean(div) dt, 2..51 iterations) and a
+    constant-volume loop (goal 1e-4 on the mean relative volume error,
+    3..101 iterations), v += acce_presure dt (-DIISPH).  The particles'
+    kinematic viscosity (FluidParticle / BoundaryParticle::kinematicViscosity,
+    0.1) is `kinematicViscosity` / `boundaryKinematicViscosity`; the
+    temperature update (m_TH.phaseTransition) is off, as in the reference's
+    demo scene."""
+    SOLVER = "iisph"
+
+    def __init__(self, device=0):
+        super().__init__(device)
+        self.kinematicViscosity = 0.1
+        self.boundaryKinematicViscosity = 0.1
+
+    def _params(self):
+        p = super()._params()
+        p.iv_kvisc = float(self.kinematicViscosity)
+        p.iv_kvisc_b = float(self.boundaryKinematicViscosity)
         return p
 
 

@@ -13,6 +13,7 @@
  *   WcSph::sphStep                         WcSph.h:50;  WcSph.cpp:23-96
  *   PciSph::sphStep                        PciSph.h:39; PciSph.cpp:31-94
  *   IISph_M::sphStep                       IISph_M.h:35; IISph_M.cpp:10-75
+ *   IISph::sphStep (volume form)           IISph.h:35;   IISph.cpp:14-99
  *   SphBase::neighbourSearch               SphBase.h:673; SphBase.cpp:849-960
  *   m_Fluids / m_Solids particle arrays    SphBase.h:650-651, getters :513-541
  *   m_TH thresholds                        SphBase.h:546-583
@@ -27,7 +28,7 @@
 extern "C" {
 #endif
 
-#define SPHGPU_ABI_VERSION 1
+#define SPHGPU_ABI_VERSION 2
 
 /* error codes */
 #define SPHGPU_OK 0
@@ -45,6 +46,7 @@ extern "C" {
 #define SPHGPU_PCISPH 1  /* PciSph  */
 #define SPHGPU_IISPH_M 2 /* IISph_M */
 #define SPHGPU_DFSPH 3   /* DFSPH   */
+#define SPHGPU_IISPH 4   /* IISph: divergence-free + constant-volume loops, per-pair h */
 
 /* step status bits (SphStepStats.status) */
 #define SPHGPU_STATUS_MAXITER_DENSITY 1u
@@ -105,17 +107,30 @@ typedef struct SphParams {
      *      as updateFluids built with -DIISPH does (SphBase.cpp:387-389);
      *      otherwise v = v_adv + a_p dt */
     int ii_compat;
+    /* IISph, volume form (IISph.cpp): kinematic viscosity of fluid and of
+     * boundary particles [0.1, FluidParticle / BoundaryParticle::
+     * kinematicViscosity, SphBase.h:100,181]; constant-volume loop: goal on
+     * the mean relative volume error, min / max iterations [1e-4, 3, 100,
+     * IISph.cpp:550-555]; divergence-free loop: goal on mean(div) * dt,
+     * min / max [1e-3, 2, 50, IISph.cpp:1223-1227].  A loop stops once its
+     * iteration count exceeds max (the reference breaks when it > max). */
+    float iv_kvisc, iv_kvisc_b;
+    float iv_cv_goal, iv_div_goal;
+    int iv_cv_min_iter, iv_cv_max_iter, iv_div_min_iter, iv_div_max_iter;
     int reserved[5];
 } SphParams;
 
 /* Per-step statistics (replaces m_EC and the CALL_TIME log rows). */
 typedef struct SphStepStats {
     int n_fluid;                 /* active fluid particles after the step */
-    int iter_density;            /* constant-density / pressure loop iterations */
-    int iter_divergence;         /* divergence-free loop iterations */
+    int iter_density;            /* constant-density / pressure loop iterations
+                                    (IISph: constant-volume, summed over phases) */
+    int iter_divergence;         /* divergence-free loop iterations (IISph: summed over phases) */
     int removed;                 /* particles removed (outside the domain) */
-    double err_density;          /* final FP64 error of the density loop */
-    double err_divergence;       /* final FP64 error of the divergence loop */
+    double err_density;          /* final FP64 error of the density loop (IISph: mean
+                                    relative volume error, last phase) */
+    double err_divergence;       /* final FP64 error of the divergence loop (IISph:
+                                    mean divergence * dt, last phase) */
     double dt;                   /* step length used */
     uint32_t status;             /* SPHGPU_STATUS_* bits */
     int neighbour_overflow;      /* pairs dropped by the cap (m_EC.tooManyNeigb) */
@@ -175,6 +190,9 @@ int sphgpu_step_host(sphgpu_t h, int solver, const float* xyz, const float* vel,
  * PCISPH: "pos_prediction","acce_pressure" (n*3);
  * IISPH_M: "dii","sum_dijpj","ii_vel_adv","acce_presure" (n*3),
  *          "aii","p_l","rho_adv" (n);
+ * IISph: "advectionAcceleration","advectionVelocity","acce_presure" (n*3),
+ *        "sphDensity","VF_gamma","VF_sphVolume","VF_alpha","VF_kappa",
+ *        "VF_kappaV","VF_advectionVolume","VF_divergenceDeviation" (n);
  * learned warm start: "kappa_warm" (n), "ws_features" (n*16, the network's
  * normalised inputs of the last step);
  * "phase" (n, fluid phase index), "scene" (n, batch scene index).
@@ -183,7 +201,10 @@ int sphgpu_step_host(sphgpu_t h, int solver, const float* xyz, const float* vel,
  * IISPH_M step's non-pressure forces read), "DFalpha". */
 int sphgpu_get_fluid(sphgpu_t h, const char* field, float* out);
 int sphgpu_set_fluid(sphgpu_t h, const char* field, const float* in);
-int sphgpu_get_boundary(sphgpu_t h, const char* field, float* out); /* "position","volume" */
+/* Boundary fields in reference order (solid by solid): "position" (n*3),
+ * "volume"; after an IISph step also "VF_gamma","VF_sphVolume","VF_alpha",
+ * "VF_kappa","VF_kappaV","VF_advectionVolume","VF_divergenceDeviation". */
+int sphgpu_get_boundary(sphgpu_t h, const char* field, float* out);
 
 /* Stage-level entry points (parity tests run "given state S, call stage X"):
  *   "neighbourSearch"                 grid + neighbour lists (+ rho/alpha)
@@ -192,6 +213,11 @@ int sphgpu_get_boundary(sphgpu_t h, const char* field, float* out); /* "position
  *   "DF_constantDensitySolverSecond"  forces+density loop+integrate (:195-738)
  *   "DF_divergenceFreeSolver"         divergence loop       (:740-1024)
  *   "wc_computePressure", "wc_computeForce"                 (WcSph.cpp:99-462)
+ *   IISph: "VF_prepareAttribute" (neighbour lists of fluid and boundary
+ *   particles, sphDensity, gamma, sphVolume, alpha; IISph.cpp:100-545),
+ *   "advectionStep" (:1505-1570), "VF_divergenceFreeSolver" (:1219-1456),
+ *   "VF_constantVolumeSolver" (:546-815), "iv_updateFluids"
+ *   (SphBase.cpp:377-402 with -DIISPH)
  */
 int sphgpu_stage(sphgpu_t h, const char* name, SphStepStats* stats);
 

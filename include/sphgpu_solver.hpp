@@ -2,7 +2,8 @@
  * sphgpu_solver.hpp -- C++ drop-in for the reference's solver classes.
  *
  * GpuSolver<Base, Solver> derives from one of the reference's solver classes
- * (WcSph, PciSph, IISph_M, DFSPH; PciSph.h:30, IISph_M.h:22, DFSPH.h:10) and
+ * (WcSph, PciSph, IISph_M, IISph, DFSPH; PciSph.h:30, IISph_M.h:22,
+ * IISph.h:22, DFSPH.h:10) and
  * overrides its step, virtual void sphStep() (SphBase.h:420), with one call
  * into the C ABI of include/sphgpu.h.  A reference scene switches to the GPU
  * by changing its base class:
@@ -14,7 +15,8 @@
  * particle arrays m_Fluids / m_Solids (SphBase.h:660-661) keep their meaning:
  * before the first step the scene is uploaded (walls as static solids, one
  * phase per SphFluid); after every step positions, velocities and densities
- * are written back into m_Fluids[k].fluidParticles, with particles that left
+ * (IISph: sphDensity) are written back into m_Fluids[k].fluidParticles,
+ * with particles that left
  * [spaceMin, spaceMax] removed as SphFluid::removeOutsideParts does
  * (SphBase.cpp:26-48).  If stepEvent() changes the number of particles of a
  * phase, the scene is uploaded again before the next step.  m_EC receives
@@ -99,6 +101,11 @@ private:
             if (!f.fluidParticles.empty()) p.particle_d = (float)f.fluidParticles[0].d;
         }
         if (!this->m_Solids.empty()) p.boundary_visc = (float)this->m_Solids[0].viscosity_alpha;
+        // IISph reads the particles' kinematic viscosity (SphBase.h:100,181)
+        for (auto& f : this->m_Fluids)
+            if (!f.fluidParticles.empty()) { p.iv_kvisc = (float)f.fluidParticles[0].kinematicViscosity; break; }
+        for (auto& s : this->m_Solids)
+            if (!s.boundaryParticles.empty()) { p.iv_kvisc_b = (float)s.boundaryParticles[0].kinematicViscosity; break; }
         int rc = sphgpu_create(&p, device_, total > 0 ? total : 1, &gpu_);
         if (rc) fail("sphgpu_create", rc);
         std::vector<float> xyz, vel;
@@ -133,7 +140,7 @@ private:
         std::vector<float> xyz(3 * (size_t)n), vel(3 * (size_t)n), rho((size_t)n), ph((size_t)n);
         int rc = sphgpu_get_fluid(gpu_, "position", xyz.data());
         if (rc >= 0) rc = sphgpu_get_fluid(gpu_, "velocity", vel.data());
-        if (rc >= 0) rc = sphgpu_get_fluid(gpu_, "density", rho.data());
+        if (rc >= 0) rc = sphgpu_get_fluid(gpu_, Solver == SPHGPU_IISPH ? "sphDensity" : "density", rho.data());
         if (rc >= 0) rc = sphgpu_get_fluid(gpu_, "phase", ph.data());
         if (rc < 0) fail("sphgpu_get_fluid", rc);
         // reference order: phase by phase, each in index order; removed
@@ -150,7 +157,8 @@ private:
                     q.position[c] = xyz[3 * (i + j) + c];
                     q.velocity[c] = vel[3 * (i + j) + c];
                 }
-                q.density = rho[i + j];
+                if constexpr (Solver == SPHGPU_IISPH) q.sphDensity = rho[i + j];
+                else q.density = rho[i + j];
             }
             counts_[k] = parts.size();
             i += m;

@@ -161,21 +161,24 @@ def main():
             if real == "double":
                 cmd.insert(1, "-DREF_REAL_DOUBLE")
             jobs.append((so, cmd))
-    # the C++ drop-in check: a scene class derived from the reference's DFSPH
-    # switched to the GPU through include/sphgpu_solver.hpp (links libsphgpu.so)
+    # the C++ drop-in checks: scene classes derived from the reference's DFSPH
+    # and IISph switched to the GPU through include/sphgpu_solver.hpp (links
+    # libsphgpu.so)
     lib = os.path.join(ROOT, "graphics_b200", "libsphgpu.so")
-    if os.path.exists(lib):
-        exe = os.path.join(OUT, "dropin_dfsph")
+    for tag, cls, cpp, defs in (("dfsph", "DFSPH", "DFSPH.cpp", []), ("iisph", "IISph", "IISph.cpp", ["-DIISPH"])):
+        if not os.path.exists(lib):
+            break
+        exe = os.path.join(OUT, "dropin_" + tag)
         deps = [os.path.join(SHIM, "dropin_main.cpp"), os.path.join(ROOT, "include", "sphgpu_solver.hpp"),
-                os.path.join(ROOT, "include", "sphgpu.h"), os.path.join(SRC, "DFSPH.cpp"),
+                os.path.join(ROOT, "include", "sphgpu.h"), os.path.join(SRC, cpp),
                 os.path.join(SRC, "SphBase.cpp"), os.path.join(SRC, "SphBase.h"), lib]
         if not (os.path.exists(exe) and all(os.path.getmtime(exe) >= os.path.getmtime(d) for d in deps)):
-            jobs.append((exe, ["g++", "-std=c++17", "-O2", "-fopenmp", "-w", "-DREF_SOLVER_HEADER=\"DFSPH.h\"",
-                               "-DREF_SOLVER_CLASS=DFSPH", "-DREF_SPHGPU_SOLVER=SPHGPU_DFSPH", "-I" + SRC,
-                               "-I" + SHIM, "-I" + os.path.join(ROOT, "include"),
-                               os.path.join(SHIM, "dropin_main.cpp"), os.path.join(SRC, "SphBase.cpp"),
-                               os.path.join(SRC, "DFSPH.cpp"), "-L" + os.path.dirname(lib), "-lsphgpu",
-                               "-Wl,-rpath,$ORIGIN/../../graphics_b200", "-o", exe]))
+            jobs.append((exe, ["g++", "-std=c++17", "-O2", "-fopenmp", "-w", "-DREF_SOLVER_HEADER=\"%s.h\"" % cls,
+                               "-DREF_SOLVER_CLASS=" + cls, "-DREF_SPHGPU_SOLVER=SPHGPU_" + tag.upper(),
+                               "-I" + SRC, "-I" + SHIM, "-I" + os.path.join(ROOT, "include")] + defs +
+                         [os.path.join(SHIM, "dropin_main.cpp"), os.path.join(SRC, "SphBase.cpp"),
+                          os.path.join(SRC, cpp), "-L" + os.path.dirname(lib), "-lsphgpu",
+                          "-Wl,-rpath,$ORIGIN/../../graphics_b200", "-o", exe]))
     procs = [(so, subprocess.Popen(cmd, stderr=subprocess.PIPE)) for so, cmd in jobs]
     rc = 0
     for so, p in procs:

@@ -12,7 +12,8 @@
  *          visc_alpha, boundary_visc, d, density_goal, div_goal_rel;
  *          then fluid positions[nf*3], velocities[nf*3], boundary positions[nb*3]
  * out.bin: int32 n, frame, total density iterations; float32 positions[n*3],
- *          velocities[n*3], densities[n] (m_Fluids[0] after the steps) */
+ *          velocities[n*3], densities[n] (m_Fluids[0] after the steps;
+ *          IISph: sphDensity) */
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -82,7 +83,11 @@ public:
         std::vector<float> x, v, r;
         for (auto& q : parts) {
             for (int c = 0; c < 3; ++c) { x.push_back((float)q.position[c]); v.push_back((float)q.velocity[c]); }
+#if REF_SPHGPU_SOLVER == SPHGPU_IISPH
+            r.push_back((float)q.sphDensity);
+#else
             r.push_back((float)q.density);
+#endif
         }
         fwrite(x.data(), sizeof(float), x.size(), f);
         fwrite(v.data(), sizeof(float), v.size(), f);

@@ -29,7 +29,12 @@ def test_params_default_and_struct_sizes():
     p = _lib.SphParams()
     assert lib.sphgpu_params_default(ctypes.byref(p)) == 0
     assert p.max_neighbours == 48 and p.df_density_min_iter == 2 and abs(p.df_div_goal_abs - 2.5) < 1e-12
-    assert lib.sphgpu_abi_version() == 1
+    # fields after the DFSPH controls: a layout mismatch of the ctypes mirror
+    # would read other fields' bytes here
+    assert p.ii_max_iter == 100 and abs(p.ws_scale - 1.0) < 1e-7
+    assert (p.iv_cv_min_iter, p.iv_cv_max_iter, p.iv_div_min_iter, p.iv_div_max_iter) == (3, 100, 2, 50)
+    assert abs(p.iv_kvisc - 0.1) < 1e-7 and abs(p.iv_cv_goal - 1e-4) < 1e-10 and abs(p.iv_div_goal - 1e-3) < 1e-9
+    assert lib.sphgpu_abi_version() == 2
 
 
 def test_create_without_gpu_fails_loudly():
