@@ -52,6 +52,14 @@ ALG_BYTES = {
     "build_first": lambda nb: 16 + 4 + 4 * nb + 4 + 4,                     # pos | list,cnt,rho,alpha
     "hash": lambda nb: 16 + 16 + 4 + 16 + 16 + 4 + 4 + 4,                  # pos,vadv,gid | pos_s,vel_s,gid_s,key,slot
     "reorder": lambda nb: 4 + 4 + 4 + 16 + 16 + 4 + 16 + 16 + 4 + 4 + 4,  # scatter + rank-reorder
+    # IISph (volume form) loop sweeps: A reads pv (pos, v_adv), ivs (gamma,
+    # sphVolume, alpha), count, list and writes kappa, V_adv / div, pk.w;
+    # B reads pk, pos (phase), v_adv, count, list and writes v_adv (+ vel in
+    # the divergence loop)
+    "iv_cv_a": lambda nb: 16 + 16 + 16 + 4 + 4 * nb + 4 + 4 + 4,
+    "iv_cv_b": lambda nb: 16 + 16 + 16 + 4 + 4 * nb + 16,
+    "iv_div_a": lambda nb: 16 + 16 + 16 + 4 + 4 * nb + 4 + 4 + 4,
+    "iv_div_b": lambda nb: 16 + 16 + 16 + 4 + 4 * nb + 16 + 16,
 }
 
 
@@ -71,6 +79,8 @@ def parse():
                     help="untimed steps before warm-up, so the timed window is in the collapsing flow "
                          "(t ~ 0.5 s) rather than the first steps from rest")
     ap.add_argument("--no-warm-start", action="store_true", help="skip the learned warm-start arm")
+    ap.add_argument("--no-iisph", action="store_true",
+                    help="skip the IISph (volume form) arm timed on the same settled state")
     ap.add_argument("--train-seeds", default="1,2", help="jitter seeds of the training runs")
     ap.add_argument("--train-steps", type=int, default=350, help="recorded plain steps per training seed")
     ap.add_argument("--train-every", type=int, default=175, help="record every n-th particle per step")
@@ -357,9 +367,66 @@ def run_ours(args):
         attach(g, None, 0)
         g.set("position", end_pos)  # continue from the plain run's state
 
-    e2e = None
+    iisph = None
+    if not args.no_iisph:
+        iisph = run_iisph_arm(args, g, sc, settle_pos, settle_vel, st_plain["dt"], barrier, stream, dist, world,
+                              torch)
+        g.set("position", end_pos)
+
     return run_tail(args, g, sc, st, value, ms_max, it_rho, it_div, launches, roof, kern, clk, world, rank, dist,
-                    barrier, torch, snap_pos, snap_vel, end_pos, warm)
+                    barrier, torch, snap_pos, snap_vel, end_pos, warm, iisph)
+
+
+def run_iisph_arm(args, g, sc, settle_pos, settle_vel, dt, barrier, stream, dist, world, torch):
+    """The reference's IISph class (volume form: divergence-free and
+    constant-volume loops, boundary particles with their own loop state) on
+    the settled state of the same scene: fixed dt = the plain run's last CFL
+    step (IISph has no CFL rule), the particles' kinematic viscosity = nu.
+    (The reference's default 0.1 m^2/s belongs to its demo's 0.3 m
+    particles; explicit viscosity at d = 0.02 m needs 10 nu dt / h^2 << 1.)"""
+    from graphics_b200.sph import params_for_scene
+    nu = SOLVER_KW["nu"]
+    g.set_params(params_for_scene(sc, **{**SOLVER_KW, "cfl": 0, "dt": dt, "iv_kvisc": nu, "iv_kvisc_b": nu}))
+    g.set("position", settle_pos)
+    g.set("velocity", settle_vel)
+    g.step("iisph", max(args.warmup, 1))
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push("timed_iisph")
+    e0.record(stream)
+    g.step_async("iisph", args.steps)
+    e1.record(stream)
+    st = g.synchronize()
+    torch.cuda.nvtx.range_pop()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    out = {"solver": "IISph (IISph.cpp, volume form)", "value": st["n_fluid"] * args.steps * world / (ms / 1e3),
+           "unit": UNIT, "ms_per_step": ms / args.steps, "dt": dt, "kinematic_viscosity": nu,
+           "iterations_per_step": {"constant_volume": st["total_iter_density"] / args.steps,
+                                   "divergence_free": st["total_iter_divergence"] / args.steps},
+           "last_step": {"err_volume": st["err_density"], "err_divergence": st["err_divergence"],
+                         "status": st["status"]}}
+    if args.profile_steps > 0:
+        g.profile(True)
+        g.step("iisph", args.profile_steps)
+        prof = g.profile_read()
+        g.profile(False)
+        st_p = g.synchronize()
+        nb = st_p["mean_neighbours"]
+        kern = {}
+        for k, (tot_ms, cnt) in prof.items():
+            ent = {"launches": cnt, "avg_us": round(1e3 * tot_ms / max(cnt, 1), 2),
+                   "us_per_step": round(1e3 * tot_ms / args.profile_steps, 1)}
+            if k in ALG_BYTES:
+                ent["gbs"] = round(ALG_BYTES[k](nb) * st_p["n_fluid"] / (tot_ms / cnt / 1e3) / 1e9, 1)
+            kern[k] = ent
+        out["kernels"] = kern
+    g.set_params(params_for_scene(sc, **SOLVER_KW))
+    return out
 
 
 def profile_kernels(g, args, hbm, peak_kind):
@@ -402,7 +469,7 @@ def profile_kernels(g, args, hbm, peak_kind):
 
 
 def run_tail(args, g, sc, st, value, ms_max, it_rho, it_div, launches, roof, kern, clk, world, rank, dist,
-             barrier, torch, snap_pos, snap_vel, end_pos, warm):
+             barrier, torch, snap_pos, snap_vel, end_pos, warm, iisph=None):
     # end to end through the C ABI with pinned host buffers: the same K steps,
     # replayed from the snapshot taken before the timed region
     e2e = None
@@ -411,6 +478,7 @@ def run_tail(args, g, sc, st, value, ms_max, it_rho, it_div, launches, roof, ker
         pos, vel = snap_pos, snap_vel
         po = torch.empty((n, 3), dtype=torch.float32, pin_memory=True).numpy()
         vo = torch.empty((n, 3), dtype=torch.float32, pin_memory=True).numpy()
+        g.step_host("dfsph", pos, vel, po, vo)  # untimed: builds the step graph (the inputs stay the snapshot)
         barrier()
         t0 = time.perf_counter()
         for _ in range(args.steps):
@@ -442,7 +510,7 @@ def run_tail(args, g, sc, st, value, ms_max, it_rho, it_div, launches, roof, ker
                 "iterations_per_step": {"density": it_rho, "divergence": it_div},
                 "last_step": {"err_density": st["err_density"], "err_divergence": st["err_divergence"],
                               "dt": st["dt"], "status": st["status"], "neighbour_overflow": st["neighbour_overflow"]},
-                "warm_start": warm,
+                "warm_start": warm, "iisph": iisph,
                 "roofline": roof, "kernels": kern, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
                 "clocks": clk.summary()}
         print(json.dumps(line))
