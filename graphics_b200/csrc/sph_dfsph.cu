@@ -125,7 +125,9 @@ __global__ void __launch_bounds__(BS) k_df_forces(DevScene s, SolverConst c, int
             }
         }
         s.acc[p] = make_float4(ax, ay, az, 0.f);
-        s.pv[2 * p + 1] = make_float4(va.x + ax * dt, va.y + ay * dt, va.z + az * dt, 0.f);
+        // w: the previous step's predicted stiffness (warm-start history),
+        // which the feature sweep then reads with the neighbour's record
+        s.pv[2 * p + 1] = make_float4(va.x + ax * dt, va.y + ay * dt, va.z + az * dt, s.hist[p].x);
         if (warm) {
             // learned warm start: the predicted stiffness is applied once before
             // the Jacobi loop as a pressure-velocity correction of the form of

@@ -23,6 +23,7 @@
 
 // warm-start kernels (sph_mlp.cu)
 void mlp_init_attributes();
+int mlp_train_blocks(int rows);
 void ws_init_attributes();
 void launch_ws_features(const DevScene& s, const SolverConst& c, const MlpDev& m, int infer, float dt_max,
                         float alpha_ref, float* Xout, __nv_bfloat16* xn, int n_max, cudaStream_t st);
@@ -59,6 +60,7 @@ struct sphgpu_mlp {
     int* ds_count = nullptr;
     int ds_cap = 0;
     int adam_t = 0;
+    int gpart_blocks = 0;  // capacity of m.gpart in training tiles
     std::string err;
 };
 
@@ -1745,7 +1747,8 @@ int sphgpu_mlp_destroy(sphgpu_mlp_t m) {
     if (!m) return SPHGPU_EINVAL;
     cudaSetDevice(m->device);
     MlpDev& d = m->m;
-    void* ptrs[] = {d.master, d.grad, d.adam_m, d.adam_v, d.w_bf16, d.loss, d.norm, m->ds_count, m->dsX, m->dsy};
+    void* ptrs[] = {d.master, d.grad, d.adam_m, d.adam_v, d.w_bf16, d.loss, d.norm, d.gpart, m->ds_count, m->dsX,
+                    m->dsy};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (m->stream) cudaStreamDestroy(m->stream);
@@ -1816,11 +1819,28 @@ int sphgpu_mlp_dataset_get(sphgpu_mlp_t m, float* X, float* y, int max_n) {
 // (dataset order; shuffle it first with sphgpu_mlp_dataset_shuffle), Adam at
 // learning rate lr.  loss_per_epoch[e] = mean squared error (normalised
 // labels) of epoch e.
+// per-tile gradient slots for mini-batches of up to `rows` rows
+static int mlp_ensure_gpart(sphgpu_mlp_t m, int rows) {
+    const int blocks = mlp_train_blocks(rows);
+    if (blocks <= m->gpart_blocks) return 0;
+    if (m->m.gpart) cudaFree(m->m.gpart);
+    m->m.gpart = nullptr;
+    m->gpart_blocks = 0;
+    if (cudaMalloc(&m->m.gpart, sizeof(float) * ((size_t)blocks * MLP_NPARAM_PAD + blocks)) != cudaSuccess) {
+        m->m.gpart = nullptr;
+        m->err = "cudaMalloc failed (training gradient slots)";
+        return SPHGPU_ENOMEM;
+    }
+    m->gpart_blocks = blocks;
+    return 0;
+}
+
 int sphgpu_mlp_train(sphgpu_mlp_t m, int epochs, int batch, float lr, float* loss_per_epoch) {
     if (!m || epochs < 0 || batch <= 0) return SPHGPU_EINVAL;
     cudaSetDevice(m->device);
     const int n = sphgpu_mlp_dataset_size(m);
     if (n <= 0) { m->err = "empty dataset"; return SPHGPU_EINVAL; }
+    if (int r = mlp_ensure_gpart(m, std::min(batch, n))) return r;
     for (int e = 0; e < epochs; ++e) {
         cudaMemsetAsync(m->m.loss, 0, sizeof(float), m->stream);
         for (int b0 = 0; b0 < n; b0 += batch) {
@@ -1869,6 +1889,11 @@ int sphgpu_mlp_gradient(sphgpu_mlp_t m, const float* X, const float* y, int n, f
         cudaMalloc(&dy, sizeof(float) * n) != cudaSuccess) {
         cudaFree(dX);
         return SPHGPU_ENOMEM;
+    }
+    if (int r = mlp_ensure_gpart(m, n)) {
+        cudaFree(dX);
+        cudaFree(dy);
+        return r;
     }
     cudaMemcpy(dX, X, sizeof(float) * MLP_IN * (size_t)n, cudaMemcpyHostToDevice);
     cudaMemcpy(dy, y, sizeof(float) * n, cudaMemcpyHostToDevice);

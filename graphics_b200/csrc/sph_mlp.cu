@@ -79,6 +79,8 @@ struct TrainSmem {
     __nv_bfloat16 dZ2[TR * MLP_H];
     __nv_bfloat16 dZ1[TR * MLP_H];
     float g[TR];
+    float pw3[TR / 32][MLP_H], pb2[TR / 32][MLP_H];  // per-warp partials
+    float pb3[TR / 32], ploss[TR / 32];
 };
 
 // weights into shared memory (BF16 GEMM copies, FP32 biases)
@@ -137,8 +139,9 @@ __device__ __forceinline__ float forward_rows(FwdSmem& S) {
 
 // ---------------- training ----------------
 
-// one 128-row tile of a mini-batch: forward, MSE gradient, backward, and FP32
-// atomics into m.grad.  inv_total = 1 / (rows in the mini-batch).
+// one 128-row tile of a mini-batch: forward, MSE gradient, backward; the
+// tile's gradient goes to its own slot of m.gpart (k_mlp_reduce sums the
+// slots in order).  inv_total = 1 / (rows in the mini-batch).
 __global__ void __launch_bounds__(TR) k_mlp_train(MlpDev m, const float* X, const float* y, int n, int b0, int bsz,
                                                  float inv_total) {
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -162,11 +165,12 @@ __global__ void __launch_bounds__(TR) k_mlp_train(MlpDev m, const float* X, cons
     const float err = valid ? yhat - target : 0.f;
     const float gr = 2.f * err * inv_total;  // dL/dy, L = mean (y - t)^2
     S.g[w * 32 + lane] = gr;
+    float* gp = m.gpart + (size_t)blockIdx.x * MLP_NPARAM_PAD;
     // loss
     float se = err * err;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) se += __shfl_down_sync(0xffffffffu, se, o);
-    if (lane == 0) atomicAdd(m.loss, se);
+    if (lane == 0) S.ploss[w] = se;
     __syncwarp();
     // output layer: dW3_j = sum_r g_r gelu(Z2_rj), db3 = sum g; dZ2 = g W3_j gelu'(Z2)
     const int r0 = w * 32;
@@ -180,13 +184,13 @@ __global__ void __launch_bounds__(TR) k_mlp_train(MlpDev m, const float* X, cons
             sb += dz;
             S.dZ2[(r0 + r) * MLP_H + j] = __float2bfloat16_rn(dz);
         }
-        atomicAdd(&m.grad[MLP_OFF_W3 + j], s3);
-        atomicAdd(&m.grad[MLP_OFF_B2 + j], sb);
+        S.pw3[w][j] = s3;
+        S.pb2[w][j] = sb;
     }
     if (lane == 0) {
         float sg = 0.f;
         for (int r = 0; r < 32; ++r) sg += S.g[r0 + r];
-        atomicAdd(&m.grad[MLP_OFF_B3], sg);
+        S.pb3[w] = sg;
     }
     __syncwarp();
     // dH1 = dZ2 W2^T, dZ1 = dH1 * gelu'(Z1)   (B(k=j2, n=j1) = W2[j1][j2])
@@ -202,11 +206,24 @@ __global__ void __launch_bounds__(TR) k_mlp_train(MlpDev m, const float* X, cons
                 __float2bfloat16_rn(c[3] * gelu_d(S.f.Z1[(ra + 8) * MLP_H + col + 1]));
         }
     __syncthreads();
+    // the warps' W3 / b2 / b3 / loss partials, in warp order
+    for (int j = threadIdx.x; j < MLP_H; j += TR) {
+        float a = 0.f, b = 0.f;
+        for (int v = 0; v < TR / 32; ++v) { a += S.pw3[v][j]; b += S.pb2[v][j]; }
+        gp[MLP_OFF_W3 + j] = a;
+        gp[MLP_OFF_B2 + j] = b;
+    }
+    if (threadIdx.x == 0) {
+        float a = 0.f, l = 0.f;
+        for (int v = 0; v < TR / 32; ++v) { a += S.pb3[v]; l += S.ploss[v]; }
+        gp[MLP_OFF_B3] = a;
+        m.gpart[(size_t)gridDim.x * MLP_NPARAM_PAD + blockIdx.x] = l;
+    }
     // db1 (from the BF16 dZ1 the GEMMs use)
     for (int j = threadIdx.x; j < MLP_H; j += TR) {
         float sb = 0.f;
         for (int r = 0; r < TR; ++r) sb += __bfloat162float(S.dZ1[r * MLP_H + j]);
-        atomicAdd(&m.grad[MLP_OFF_B1 + j], sb);
+        gp[MLP_OFF_B1 + j] = sb;
     }
     // dW2 = H1^T dZ2 (64 x 64, K = 128 rows): 4 x 8 tiles, 8 per warp
     for (int tt = w; tt < 32; tt += 4) {
@@ -214,20 +231,36 @@ __global__ void __launch_bounds__(TR) k_mlp_train(MlpDev m, const float* X, cons
         float c[4] = {0.f, 0.f, 0.f, 0.f};
         tile_mma(c, S.f.H1, 1, MLP_H, S.dZ2, MLP_H, 1, mt * 16, nt * 8, TR);
         const int ra = mt * 16 + g, col = nt * 8 + 2 * t;
-        atomicAdd(&m.grad[MLP_OFF_W2 + ra * MLP_H + col], c[0]);
-        atomicAdd(&m.grad[MLP_OFF_W2 + ra * MLP_H + col + 1], c[1]);
-        atomicAdd(&m.grad[MLP_OFF_W2 + (ra + 8) * MLP_H + col], c[2]);
-        atomicAdd(&m.grad[MLP_OFF_W2 + (ra + 8) * MLP_H + col + 1], c[3]);
+        gp[MLP_OFF_W2 + ra * MLP_H + col] = c[0];
+        gp[MLP_OFF_W2 + ra * MLP_H + col + 1] = c[1];
+        gp[MLP_OFF_W2 + (ra + 8) * MLP_H + col] = c[2];
+        gp[MLP_OFF_W2 + (ra + 8) * MLP_H + col + 1] = c[3];
     }
     // dW1 = X^T dZ1 (16 x 64, K = 128): 1 x 8 tiles, 2 per warp
     for (int nt = w; nt < 8; nt += 4) {
         float c[4] = {0.f, 0.f, 0.f, 0.f};
         tile_mma(c, S.f.X, 1, MLP_IN, S.dZ1, MLP_H, 1, 0, nt * 8, TR);
         const int ra = g, col = nt * 8 + 2 * t;
-        atomicAdd(&m.grad[MLP_OFF_W1 + ra * MLP_H + col], c[0]);
-        atomicAdd(&m.grad[MLP_OFF_W1 + ra * MLP_H + col + 1], c[1]);
-        atomicAdd(&m.grad[MLP_OFF_W1 + (ra + 8) * MLP_H + col], c[2]);
-        atomicAdd(&m.grad[MLP_OFF_W1 + (ra + 8) * MLP_H + col + 1], c[3]);
+        gp[MLP_OFF_W1 + ra * MLP_H + col] = c[0];
+        gp[MLP_OFF_W1 + ra * MLP_H + col + 1] = c[1];
+        gp[MLP_OFF_W1 + (ra + 8) * MLP_H + col] = c[2];
+        gp[MLP_OFF_W1 + (ra + 8) * MLP_H + col + 1] = c[3];
+    }
+}
+
+// gradient of the mini-batch = the tiles' gradients summed in tile order;
+// the batch's squared error is added to m.loss (one thread, in order)
+__global__ void k_mlp_reduce(MlpDev m, int blocks) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < MLP_NPARAM) {
+        float a = 0.f;
+        for (int b = 0; b < blocks; ++b) a += m.gpart[(size_t)b * MLP_NPARAM_PAD + i];
+        m.grad[i] = a;
+    }
+    if (i == 0) {
+        float l = 0.f;
+        for (int b = 0; b < blocks; ++b) l += m.gpart[(size_t)blocks * MLP_NPARAM_PAD + b];
+        *m.loss += l;
     }
 }
 
@@ -280,10 +313,13 @@ void mlp_init_attributes() {
     cudaFuncSetAttribute(k_mlp_predict, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_fwd());
 }
 
+int mlp_train_blocks(int bsz) { return (bsz + TR - 1) / TR; }
+
 void launch_mlp_train_batch(const MlpDev& m, const float* X, const float* y, int n, int b0, int bsz, float inv_total,
                             cudaStream_t st) {
-    const int blocks = (bsz + TR - 1) / TR;
+    const int blocks = mlp_train_blocks(bsz);
     k_mlp_train<<<blocks, TR, smem_train(), st>>>(m, X, y, n, b0, bsz, inv_total);
+    k_mlp_reduce<<<(MLP_NPARAM + 255) / 256, 256, 0, st>>>(m, blocks);
 }
 
 void launch_mlp_adam(const MlpDev& m, float lr, int t, cudaStream_t st) {
@@ -332,7 +368,7 @@ __device__ __forceinline__ void ws_features(const DevScene& s, const SolverConst
         ay = fmaf(xy * f, m, ay);
         az = fmaf(xz * f, m, az);
         if (bnd) ++nb;
-        else { kp += s.hist[j].x; ++nfl; }
+        else { kp += vb.w; ++nfl; }  // the neighbour's history, carried in its record (k_df_forces)
     }
     const float rho0 = c.rho0, rho = s.rho[p], d = c.dpart;
     const float4 hp = s.hist[p];
@@ -509,21 +545,29 @@ __global__ void k_ws_post(DevScene s, SolverConst c, float* yout) {
     s.ksum[p] = 0.f;
 }
 
-// append every `every`-th particle (from `offset`) of the step to the dataset
+// append every `every`-th particle (from `offset`) of the step to the dataset,
+// sample i of the step at slot ds_count + i (the order of the particles, so
+// recording is run-to-run deterministic)
 __global__ void k_ws_append(const float* X, const float* y, int n_max, const int* n_act, int every, const int* offset,
-                            float* dsX, float* dsy, int* ds_count, int ds_cap) {
+                            float* dsX, float* dsy, const int* ds_count, int ds_cap) {
     const int n = *n_act;
     const long long i = (long long)blockIdx.x * TR + threadIdx.x;
     const long long pl = (long long)*offset + i * (long long)every;
     if (pl < 0 || pl >= n || pl >= n_max) return;
     const int p = (int)pl;
-    const int slot = atomicAdd(ds_count, 1);
+    const long long slot = (long long)*ds_count + i;
     if (slot >= ds_cap) return;
     for (int k = 0; k < MLP_IN; ++k) dsX[(size_t)slot * MLP_IN + k] = X[(size_t)p * MLP_IN + k];
     dsy[slot] = y[p];
 }
-// the sampling offset advances by one particle per recorded step
-__global__ void k_ws_advance(int* offset, int every) { *offset = (*offset + 1) % every; }
+// after the append: the dataset count grows by the step's samples and the
+// sampling offset advances by one particle per recorded step
+__global__ void k_ws_advance(int* offset, int every, const int* n_act, int n_max, int* ds_count, int ds_cap) {
+    const int n = min(*n_act, n_max), o = *offset;
+    const long long cnt = n > o ? ((long long)n - o + every - 1) / every : 0;
+    *ds_count = (int)min((long long)*ds_count + cnt, (long long)ds_cap);
+    *offset = (o + 1) % every;
+}
 }  // namespace
 
 void ws_init_attributes() {}
@@ -553,5 +597,5 @@ void launch_ws_append(const float* X, const float* y, int n_max, const int* n_ac
     const long long cnt = ((long long)n_max + every - 1) / every + 1;
     k_ws_append<<<(int)((cnt + TR - 1) / TR), TR, 0, st>>>(X, y, n_max, n_act, every, offset, dsX, dsy, ds_count,
                                                           ds_cap);
-    k_ws_advance<<<1, 1, 0, st>>>(offset, every);
+    k_ws_advance<<<1, 1, 0, st>>>(offset, every, n_act, n_max, ds_count, ds_cap);
 }

@@ -19,7 +19,10 @@
 
 struct MlpDev {
     float* master;          // FP32 parameters (Adam updates these)
-    float* grad;            // FP32 gradient accumulator
+    float* grad;            // FP32 gradient of the last mini-batch
+    float* gpart;           // [blocks][MLP_NPARAM_PAD] per-block gradients and
+                            // [blocks] squared errors (after them): summed in a
+                            // fixed order, so training is run-to-run deterministic
     float* adam_m;
     float* adam_v;
     __nv_bfloat16* w_bf16;  // BF16 copies of W1, W2, W3 used by the GEMMs
