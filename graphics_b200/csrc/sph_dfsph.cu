@@ -100,18 +100,13 @@ __global__ void __launch_bounds__(BS) k_df_forces(DevScene s, SolverConst c, int
         const size_t stride = (size_t)c.stride;
         for (int k = 0; k < cnt; ++k) {
             const unsigned e = (unsigned)ell_get(s.nbr, stride, p, k);
+            // one 32-byte record per neighbour: {(x, y, z, rho), v} or, for
+            // a boundary particle, {(x, y, z, volume), v}
             float4 pb, vb;
-            float m;
-            if (e & BND_FLAG) {
-                const unsigned b = e & BND_MASK;
-                pb = s.bpos[b];
-                vb = s.bvel[b];
-                m = rho0 * pb.w / rhoa;  // (frho0*volume)/fa.density, DFSPH.cpp:1353
-            } else {
-                pb = s.pos[e];
-                vb = s.vel[e];
-                m = fm0 / s.rho[e];      // fm0/fb.density, DFSPH.cpp:1265
-            }
+            const bool bnd = (e & BND_FLAG) != 0u;
+            ld_record32((bnd ? s.bpv : s.prv) + 2 * (size_t)(e & BND_MASK), pb, vb);
+            const float m = bnd ? rho0 * pb.w / rhoa   // (frho0*volume)/fa.density, DFSPH.cpp:1353
+                                : fm0 / pb.w;          // fm0/fb.density, DFSPH.cpp:1265
             const float xx = pa.x - pb.x, xy = pa.y - pb.y, xz = pa.z - pb.z;
             const float len2 = xx * xx + xy * xy + xz * xz;
             if (len2 == 0.f) { ++zero; continue; }
@@ -261,7 +256,10 @@ __global__ void __launch_bounds__(BS) k_df_vupdate(DevScene s, SolverConst c, do
         va.y = fmaf(-dy, dt, va.y);
         va.z = fmaf(-dz, dt, va.z);
         s.pv[2 * p + 1] = va;
-        if (DIV) s.vel[p] = va;  // velocity = vel_adv (DFSPH.cpp:909)
+        if (DIV) {
+            s.vel[p] = va;  // velocity = vel_adv (DFSPH.cpp:909)
+            s.prv[2 * p + 1] = va;
+        }
     }
     if (DECIDE && s.nscenes <= 1 && blockIdx.x == 0 && threadIdx.x == 0) {
         // convergence decision of the iteration that just finished

@@ -282,7 +282,7 @@ int alloc_scene(sphgpu_scene* h) {
     r |= dalloc(h, &d.pos, n); r |= dalloc(h, &d.vel, n); r |= dalloc(h, &d.gid, n);
     r |= dalloc(h, &d.rho, n); r |= dalloc(h, &d.alpha, n); r |= dalloc(h, &d.vadv, n);
     r |= dalloc(h, &d.acc, n); r |= dalloc(h, &d.kr, n); r |= dalloc(h, &d.kappa, n); r |= dalloc(h, &d.kappav, n);
-    r |= dalloc(h, &d.pv, 2 * (size_t)n); r |= dalloc(h, &d.pk, n);
+    r |= dalloc(h, &d.pv, 2 * (size_t)n); r |= dalloc(h, &d.pk, n); r |= dalloc(h, &d.prv, 2 * (size_t)n);
     r |= dalloc(h, &d.ksum, n); r |= dalloc(h, &d.aux0, n); r |= dalloc(h, &d.aux1, n);
     r |= dalloc(h, &d.aux4, n); r |= dalloc(h, &d.kwarm, n); r |= dalloc(h, &d.hist, n); r |= dalloc(h, &d.wsbuf, n);
     r |= dalloc(h, &d.pos_s, n); r |= dalloc(h, &d.vel_s, n); r |= dalloc(h, &d.gid_s, n);
@@ -323,7 +323,7 @@ int alloc_scene(sphgpu_scene* h) {
 
 void free_scene(sphgpu_scene* h) {
     DevScene& d = h->d;
-    void* ptrs[] = {d.pos, d.vel, d.gid, d.rho, d.alpha, d.vadv, d.pv, d.pk, d.bpv, d.kappav, d.acc, d.kr, d.kappa, d.ksum, d.aux0,
+    void* ptrs[] = {d.pos, d.vel, d.gid, d.rho, d.alpha, d.vadv, d.pv, d.pk, d.prv, d.bpv, d.kappav, d.acc, d.kr, d.kappa, d.ksum, d.aux0,
                     d.aux1, d.aux4, d.kwarm, d.hist, d.wsbuf, d.pos_s, d.vel_s, d.gid_s, d.hist_s, d.key, d.slot, d.tmp,
                     d.cA, d.cB, d.cC, d.cA_s, d.cB_s, d.cC_s, d.ap, d.pl2, d.ivs,
                     d.bsid, d.bnbr, d.bncount, d.bivs, d.bivo,
@@ -1469,6 +1469,9 @@ int sphgpu_set_fluid(sphgpu_t h, const char* field, const float* in) {
     std::vector<float> t(n);
     for (int k = 0; k < n; ++k) t[order[k]] = in[k];
     CK(cudaMemcpy(dst, t.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
+    if (dst == d.rho && n)  // the force kernel's record carries rho too
+        CK(cudaMemcpy2D(reinterpret_cast<char*>(d.prv) + 3 * sizeof(float), 2 * sizeof(float4), d.rho, sizeof(float),
+                        sizeof(float), n, cudaMemcpyDeviceToDevice));
     return n;
 }
 

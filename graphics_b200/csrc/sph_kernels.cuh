@@ -62,6 +62,9 @@ struct DevScene {
     float4* pv;         // 2 per particle: {position, loop velocity} -- the one
                         // 32-byte record the A sweeps gather per neighbour
     float4* pk;         // (x, y, z, kappa/rho) -- the record the B sweeps gather
+    float4* prv;        // 2 per particle: {(x, y, z, rho), velocity} -- the record the
+                        // DFSPH force kernel gathers (position and rho from the list
+                        // build, velocity from the reorder / divergence sweep)
     float4* bpv;        // 2 per boundary particle: {(x,y,z,volume), velocity}
     float4* acc;        // a_adv (DFSPH) / acceleration (WCSPH) / pressure accel (PCISPH, IISPH)
     float* kr;          // kappa/rho (DFSPH), pressure (WCSPH/PCISPH/IISPH)
