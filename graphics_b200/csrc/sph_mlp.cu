@@ -25,9 +25,23 @@ namespace {
 
 constexpr int TR = 128;  // rows per block tile (4 warps x 32)
 
-__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.f + erff(z * 0.70710678118654752f)); }
+// GELU in its tanh form, 0.5 z (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3))),
+// with the hardware tanh (PTX tanh.approx.f32, relative error about 2^-11,
+// below the BF16 rounding the activations take next); the same form in
+// training, inference and the CPU restatement (oracle/mlp_oracle.py)
+__device__ __forceinline__ float tanh_hw(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float gelu(float z) {
+    const float u = 0.7978845608028654f * fmaf(0.044715f * z, z * z, z);
+    return 0.5f * z * (1.f + tanh_hw(u));
+}
 __device__ __forceinline__ float gelu_d(float z) {
-    return 0.5f * (1.f + erff(z * 0.70710678118654752f)) + z * expf(-0.5f * z * z) * 0.39894228040143268f;
+    const float z2 = z * z;
+    const float t = tanh_hw(0.7978845608028654f * fmaf(0.044715f * z, z2, z));
+    return 0.5f * (1.f + t) + 0.5f * z * (1.f - t * t) * 0.7978845608028654f * fmaf(0.134145f, z2, 1.f);
 }
 
 __device__ __forceinline__ uint32_t pack2(__nv_bfloat16 lo, __nv_bfloat16 hi) {

@@ -1,6 +1,6 @@
 """CPU restatement of the warm-start network (TEST INFRASTRUCTURE ONLY).
 
-numpy FP64 forward and backward of the 16 -> 64 -> 64 -> 1 GELU network of
+numpy FP64 forward and backward of the 16 -> 64 -> 64 -> 1 GELU (tanh form) network of
 graphics_b200/csrc/sph_mlp.cu, with the same normalisation and, when
 `bf16=True`, BF16 rounding at the points where the GPU kernels round (GEMM
 operands: inputs, W1, W2, W3, H1, dZ2, dZ1).  Used to check the GPU forward
@@ -18,9 +18,6 @@ OFF_W3 = OFF_B2 + NH
 OFF_B3 = OFF_W3 + NH
 NPARAM = OFF_B3 + 1
 
-_erf = np.vectorize(math.erf)
-
-
 def bf16(x):
     """Round to the nearest BF16 value (ties to even), returned as float64."""
     a = np.asarray(x, np.float32).copy().view(np.uint32)
@@ -28,12 +25,17 @@ def bf16(x):
     return a.view(np.float32).astype(np.float64)
 
 
+_C = math.sqrt(2.0 / math.pi)
+
+
 def gelu(z):
-    return 0.5 * z * (1.0 + _erf(z / math.sqrt(2.0)))
+    """GELU, tanh form: 0.5 z (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3)))."""
+    return 0.5 * z * (1.0 + np.tanh(_C * (z + 0.044715 * z ** 3)))
 
 
 def gelu_d(z):
-    return 0.5 * (1.0 + _erf(z / math.sqrt(2.0))) + z * np.exp(-0.5 * z * z) / math.sqrt(2 * math.pi)
+    t = np.tanh(_C * (z + 0.044715 * z ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * z * (1.0 - t * t) * _C * (1.0 + 3 * 0.044715 * z ** 2)
 
 
 def unpack(w):
