@@ -51,7 +51,7 @@ ALG_BYTES = {
     "df_forces": lambda nb: 16 + 16 + 4 + 4 + 4 * nb + 16 + 16,            # pos,vel,rho,cnt,list | acc,vadv
     "build_first": lambda nb: 16 + 4 + 4 * nb + 4 + 4 + 16,                # pos | list,cnt,rho,alpha,(pos,rho) record
     "hash": lambda nb: 16 + 16 + 4 + 16 + 16 + 4 + 4 + 4,                  # pos,vadv,gid | pos_s,vel_s,gid_s,key,slot
-    "reorder": lambda nb: 4 + 4 + 4 + 16 + 16 + 4 + 16 + 16 + 4 + 4 + 4,  # scatter + rank-reorder
+    "reorder": lambda nb: 4 + 4 + 4 + 16 + 16 + 4 + 16 + 16 + 4 + 4 + 4 + 16,  # scatter + rank-reorder (+ v record)
     # IISph (volume form) loop sweeps: A reads pv (pos, v_adv), ivs (gamma,
     # sphVolume, alpha), count, list and writes kappa, V_adv / div, pk.w;
     # B reads pk, pos (phase), v_adv, count, list and writes v_adv (+ vel in
