@@ -2,8 +2,8 @@
  * sphgpu_solver.hpp -- C++ drop-in for the reference's solver classes.
  *
  * GpuSolver<Base, Solver> derives from one of the reference's solver classes
- * (WcSph, PciSph, IISph_M, IISph, DFSPH; PciSph.h:30, IISph_M.h:22,
- * IISph.h:22, DFSPH.h:10) and
+ * (WcSph, PciSph, IISph_M, IISph, DFSPH; WcSph.h:24, PciSph.h:31,
+ * IISph_M.h:10, IISph.h:10, DFSPH.h:10) and
  * overrides its step, virtual void sphStep() (SphBase.h:420), with one call
  * into the C ABI of include/sphgpu.h.  A reference scene switches to the GPU
  * by changing its base class:
@@ -101,6 +101,12 @@ private:
             if (!f.fluidParticles.empty()) p.particle_d = (float)f.fluidParticles[0].d;
         }
         if (!this->m_Solids.empty()) p.boundary_visc = (float)this->m_Solids[0].viscosity_alpha;
+        // solver constants the reference keeps in the solver object
+        if constexpr (Solver == SPHGPU_WCSPH) p.wc_gamma = (float)this->m_DensityPower_gamma;  // WcSph.h:34
+        if constexpr (Solver == SPHGPU_PCISPH) {  // PciSph.h:35
+            p.pci_min_iter = this->m_minIterations;
+            p.pci_max_iter = this->m_maxIterations;
+        }
         // IISph reads the particles' kinematic viscosity (SphBase.h:100,181)
         for (auto& f : this->m_Fluids)
             if (!f.fluidParticles.empty()) { p.iv_kvisc = (float)f.fluidParticles[0].kinematicViscosity; break; }

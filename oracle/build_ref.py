@@ -161,11 +161,14 @@ def main():
             if real == "double":
                 cmd.insert(1, "-DREF_REAL_DOUBLE")
             jobs.append((so, cmd))
-    # the C++ drop-in checks: scene classes derived from the reference's DFSPH
-    # and IISph switched to the GPU through include/sphgpu_solver.hpp (links
-    # libsphgpu.so)
+    # the C++ drop-in checks: scene classes derived from each of the
+    # reference's solver classes, switched to the GPU through
+    # include/sphgpu_solver.hpp (links libsphgpu.so)
     lib = os.path.join(ROOT, "graphics_b200", "libsphgpu.so")
-    for tag, cls, cpp, defs in (("dfsph", "DFSPH", "DFSPH.cpp", []), ("iisph", "IISph", "IISph.cpp", ["-DIISPH"])):
+    for tag, cls, cpp, defs in (("dfsph", "DFSPH", "DFSPH.cpp", []), ("iisph", "IISph", "IISph.cpp", ["-DIISPH"]),
+                                ("wcsph", "WcSph", "WcSph.cpp", []),
+                                ("pcisph", "PciSph", "PciSph.cpp", ["-DPREDICTION_PCISPH"]),
+                                ("iisph_m", "IISph_M", "IISph_M.cpp", ["-DIISPH"])):
         if not os.path.exists(lib):
             break
         exe = os.path.join(OUT, "dropin_" + tag)

@@ -9,7 +9,8 @@
  *
  * in.bin:  int32 nf, nb, steps; float32 spacing_r, smoothRadius_h, dt,
  *          gravity[3], spaceMin[3], spaceMax[3], soundSpeed_cs, nu, rho0,
- *          visc_alpha, boundary_visc, d, density_goal, div_goal_rel;
+ *          visc_alpha, boundary_visc, d, density_goal, div_goal_rel,
+ *          densityErro_eta;
  *          then fluid positions[nf*3], velocities[nf*3], boundary positions[nb*3]
  * out.bin: int32 n, frame, total density iterations; float32 positions[n*3],
  *          velocities[n*3], densities[n] (m_Fluids[0] after the steps;
@@ -43,6 +44,7 @@ public:
         m_TH.spaceMax = vec_t(q[9], q[10], q[11]);
         m_TH.soundSpeed_cs = q[12];
         m_TH.nu = q[13];
+        m_TH.densityErro_eta = q[20];  // PciSph's loop goal (uninitialised in ThresholdsBase)
         const float rho0 = q[14], visc = q[15], bvisc = q[16], d = q[17];
         gpuParams().df_density_goal = q[18];
         gpuParams().df_div_goal_abs = 0.0;

@@ -1,10 +1,10 @@
-"""The C++ drop-in (include/sphgpu_solver.hpp): a scene class derived from
-the reference's own DFSPH (or IISph) class (compiled from its sources by
-oracle/build_ref.py into oracle/_ref/dropin_dfsph, dropin_iisph) switched to
-the GPU by changing its base class to GpuSolver<DFSPH, SPHGPU_DFSPH> (or
-GpuSolver<IISph, SPHGPU_IISPH>).  Stepped with the reference's runOneStep(),
+"""The C++ drop-in (include/sphgpu_solver.hpp): for each of the reference's
+solver classes (DFSPH, IISph, WcSph, PciSph, IISph_M), a scene class derived
+from it (compiled from the reference's sources by oracle/build_ref.py into
+oracle/_ref/dropin_<solver>) switched to the GPU by changing its base class
+to GpuSolver<Class, SPHGPU_...>.  Stepped with the reference's runOneStep(),
 it must give the states the GPU path gives through the Python mirror for the
-same scene and parameters."""
+same scene and parameters, bit for bit."""
 import os
 import struct
 import subprocess
@@ -22,7 +22,8 @@ REF = os.path.join(ROOT, "oracle", "_ref")
 
 def _write(path, sc, steps, kw):
     p = [sc.spacing_r, sc.smooth_radius, kw["dt"], 0.0, -9.81, 0.0, *sc.space_min, *sc.space_max,
-         kw["soundSpeed_cs"], kw["nu"], sc.rho0, 0.0, 0.0, sc.d, kw["df_density_goal"], kw["df_div_goal_rel"], 0.0]
+         kw["soundSpeed_cs"], kw["nu"], sc.rho0, 0.0, 0.0, sc.d, kw["df_density_goal"], kw["df_div_goal_rel"],
+         kw["densityErro_eta"]]
     with open(path, "wb") as f:
         f.write(struct.pack("3i", sc.n_fluid, len(sc.boundary_pos), steps))
         f.write(np.asarray(p, np.float32).tobytes())
@@ -38,22 +39,41 @@ def _read(path):
     return n, frame, iters, a[:3 * n].reshape(n, 3), a[3 * n:6 * n].reshape(n, 3), a[6 * n:7 * n]
 
 
-@pytest.mark.parametrize("solver,dt", [("dfsph", 1e-3), ("iisph", 2.5e-4)])
-def test_cpp_dropin_subclass_matches_gpu_path(tmp_path, solver, dt):
+def _settled_column():
+    """The settled column of tests/golden/settled_column.npz as one phase
+    (the pressure-projection solvers start from a settled state)."""
+    import importlib.util
+    from graphics_b200.scene import Scene
+    gold = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "make_golden.py")
+    spec = importlib.util.spec_from_file_location("make_golden", gold)
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    col = mg.column_scene(rho=(1000.0, 1000.0))
+    kw = dict(col.__dict__)
+    kw.update(phase=None, rho0_phases=(1000.0,))
+    return Scene(**kw)
+
+
+@pytest.mark.parametrize("solver,dt,cs", [("dfsph", 1e-3, 100.0), ("iisph", 2.5e-4, 100.0),
+                                          ("wcsph", 2.5e-4, 18.708287), ("pcisph", 1e-3, 20.0),
+                                          ("iisph_m", 1e-3, 20.0)])
+def test_cpp_dropin_subclass_matches_gpu_path(tmp_path, solver, dt, cs):
     exe = os.path.join(REF, "dropin_" + solver)
     if not os.path.exists(exe):
         pytest.skip("drop-in check not built (needs the reference sources)")
-    sc = small_dam_break((12, 12, 12), 0.025, seed=5)
-    kw = dict(dt=dt, soundSpeed_cs=100.0, nu=1e-3, df_density_goal=1e-4, df_div_goal_rel=1e-3)
+    sc = small_dam_break((12, 12, 12), 0.025, seed=5) if solver in ("dfsph", "iisph") else _settled_column()
+    kw = dict(dt=dt, soundSpeed_cs=cs, nu=1e-3, df_density_goal=1e-4, df_div_goal_rel=1e-3, densityErro_eta=0.01)
     steps = 5
     _write(tmp_path / "in.bin", sc, steps, kw)
     r = subprocess.run([exe, str(tmp_path / "in.bin"), str(tmp_path / "out.bin")], cwd=tmp_path,
                        capture_output=True, timeout=300)
     assert r.returncode == 0, r.stderr.decode()[-2000:]
     n, frame, iters, x, v, rho = _read(tmp_path / "out.bin")
-    assert frame == steps and n <= sc.n_fluid and iters >= 2 * steps
+    assert frame == steps and n <= sc.n_fluid
+    if solver != "wcsph":
+        assert iters >= 2 * steps
     g = scene_to_gpu(sc, df_div_goal_abs=0.0, df_div_max_iter=100, **kw)
-    st = g.step(solver, steps)
+    g.step(solver, steps)
     assert g.n_fluid == n
     assert np.array_equal(g.get("position"), x)
     assert np.array_equal(g.get("velocity"), v)
