@@ -68,6 +68,10 @@ SIGNATURES = {
     "sphgpu_set_fluid": (_i, [_vp, _cp, _fp]),
     "sphgpu_get_boundary": (_i, [_vp, _cp, _fp]),
     "sphgpu_stage": (_i, [_vp, _cp, C.POINTER(SphStepStats)]),
+    "sphgpu_write_pos": (_i, [_vp, _cp, _i, _cp, _cp]),
+    "sphgpu_read_pos": (C.c_longlong, [_cp, _fp, C.c_longlong, _cp, _i, _ip]),
+    "sphgpu_save_snapshot": (_i, [_vp, _cp]),
+    "sphgpu_load_snapshot": (_i, [_cp, _i, C.POINTER(_vp)]),
     "sphgpu_get_neighbours": (_i, [_vp, _ip, _ip, _ip]),
     "sphgpu_get_cells": (_i, [_vp, C.POINTER(C.c_longlong)]),
     "sphgpu_stream": (_vp, [_vp]),

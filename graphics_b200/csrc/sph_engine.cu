@@ -2125,3 +2125,235 @@ int sphgpu_debug_set(sphgpu_t h, const char* key, int value) {
 }
 
 }  // extern "C"
+
+// ======================= output and restart =======================
+namespace {
+
+// a float4 field in reference order from the sorted or the staging copy
+int ref_order_field(sphgpu_scene* h, const float4* sorted, const float4* staging, std::vector<float4>& out) {
+    std::vector<int> gid;
+    int n;
+    if (download_gid(h, gid, n, h->in_staging)) return SPHGPU_ECUDA;
+    std::vector<int> order;
+    ref_order(gid, order);
+    std::vector<float4> t(n);
+    if (n) CK(cudaMemcpy(t.data(), h->in_staging ? staging : sorted, sizeof(float4) * n, cudaMemcpyDeviceToHost));
+    out.resize(n);
+    for (int k = 0; k < n; ++k) out[k] = t[order[k]];
+    return 0;
+}
+
+const char SNAP_MAGIC[8] = {'S', 'P', 'H', 'G', 'P', 'U', 'S', '1'};
+
+template <class T>
+bool put(FILE* f, const T* p, size_t n) { return n == 0 || fwrite(p, sizeof(T), n, f) == n; }
+template <class T>
+bool get(FILE* f, T* p, size_t n) { return n == 0 || fread(p, sizeof(T), n, f) == n; }
+
+}  // namespace
+
+extern "C" {
+
+// .pos file of one fluid phase in the reference's format (write_fluid_particles,
+// fUtility.h:254-303): four text lines, then per particle the chosen
+// components in the reference's fixed order, as float32.
+int sphgpu_write_pos(sphgpu_t h, const char* path, int phase, const char* components, const char* log_name) {
+    if (!h || !path || phase < 0) return SPHGPU_EINVAL;
+    cudaSetDevice(h->device);
+    std::string comp = components ? components : "position";
+    static const char* order[] = {"position", "velocity", "color", "density", "presure", "acceleration"};
+    std::vector<std::string> use;
+    for (const char* o : order)
+        if (comp.find(o) != std::string::npos) use.push_back(o);
+    if (use.empty()) { h->err = "no known component in '" + comp + "'"; return SPHGPU_EINVAL; }
+    for (auto& u : use)
+        if (u == "color") { h->err = "particle colours are not part of the GPU state"; return SPHGPU_EINVAL; }
+    int n = sphgpu_num_fluid(h);
+    if (n < 0) return n;
+    std::vector<float> ph(n);
+    int r = sphgpu_get_fluid(h, "phase", ph.data());
+    if (r < 0) return r;
+    std::vector<std::vector<float>> cols;
+    std::vector<int> width;
+    for (auto& u : use) {
+        const int w = (u == "density" || u == "presure") ? 1 : 3;
+        std::vector<float> v((size_t)n * w);
+        const char* f = u.c_str();
+        if (u == "density" && h->last_solver == SPHGPU_IISPH) f = "sphDensity";
+        if (u == "acceleration") f = h->last_solver == SPHGPU_IISPH ? "acce_presure" : "acceleration";
+        if ((r = sphgpu_get_fluid(h, f, v.data())) < 0) return r;
+        cols.push_back(std::move(v));
+        width.push_back(w);
+    }
+    std::vector<int> mine;
+    for (int i = 0; i < n; ++i)
+        if ((int)ph[i] == phase) mine.push_back(i);
+    FILE* fo = fopen(path, "wb");
+    if (!fo) { h->err = std::string("cannot open ") + path; return SPHGPU_EINVAL; }
+    std::string mask = "<";
+    for (auto& u : use) mask += " " + u + " ";
+    mask += ">";
+    fprintf(fo, "for parameters and scene info, please refer to \"%s\"\n", log_name ? log_name : "");
+    fprintf(fo, "components writed: %s\n", mask.c_str());
+    fprintf(fo, "%d (frame number), fluid index: %d\n", h->frame, phase);
+    fprintf(fo, "%zu (num particles)\n", mine.size());
+    bool ok = true;
+    for (int i : mine)
+        for (size_t c = 0; c < cols.size(); ++c) ok = ok && put(fo, &cols[c][(size_t)i * width[c]], width[c]);
+    ok = (fclose(fo) == 0) && ok;
+    if (!ok) { h->err = std::string("write failed: ") + path; return SPHGPU_EINVAL; }
+    return (int)mine.size();
+}
+
+// read_fluid_particles (fUtility.h:486-510): the header's component mask and
+// frame number, and the packed float32 records
+long long sphgpu_read_pos(const char* path, float* out, long long max_floats, char* mask, int mask_len, int* frame) {
+    if (!path) return SPHGPU_EINVAL;
+    FILE* f = fopen(path, "rb");
+    if (!f) return SPHGPU_EINVAL;
+    char l1[512], l2[512], l3[512], l4[512];
+    if (!fgets(l1, sizeof l1, f) || !fgets(l2, sizeof l2, f) || !fgets(l3, sizeof l3, f) || !fgets(l4, sizeof l4, f)) {
+        fclose(f);
+        return SPHGPU_EINVAL;
+    }
+    long long num = atoll(l4);
+    std::string m(l2);
+    const size_t colon = m.find(':');
+    std::string msk = colon == std::string::npos ? m : m.substr(colon + 1);
+    while (!msk.empty() && (msk.back() == '\n' || msk.back() == '\r')) msk.pop_back();
+    while (!msk.empty() && msk.front() == ' ') msk.erase(msk.begin());
+    int per = 0;  // floats per particle (get_part_size, fUtility.h:56-66)
+    if (msk.find("position") != std::string::npos) per += 3;
+    if (msk.find("velocity") != std::string::npos) per += 3;
+    if (msk.find("color") != std::string::npos) per += 4;
+    if (msk.find("density") != std::string::npos) per += 1;
+    if (msk.find("presure") != std::string::npos) per += 1;
+    if (msk.find("acceleration") != std::string::npos) per += 3;
+    if (msk.find("dt") != std::string::npos) per += 1;
+    if (mask && mask_len > 0) {
+        strncpy(mask, msk.c_str(), (size_t)mask_len - 1);
+        mask[mask_len - 1] = 0;
+    }
+    if (frame) *frame = atoi(l3);
+    const long long total = num * per;
+    if (out) {
+        if (total > max_floats) { fclose(f); return SPHGPU_EINVAL; }
+        if (!get(f, out, (size_t)total)) { fclose(f); return SPHGPU_EINVAL; }
+    }
+    fclose(f);
+    return num;
+}
+
+// Snapshot for checkpoint / resume: parameters, walls, every fluid particle
+// with the state the solvers carry between steps, the frame and the clock.
+int sphgpu_save_snapshot(sphgpu_t h, const char* path) {
+    if (!h || !path) return SPHGPU_EINVAL;
+    if (h->nscenes > 1) { h->err = "snapshots are for single scenes"; return SPHGPU_EINVAL; }
+    cudaSetDevice(h->device);
+    CK(cudaStreamSynchronize(h->stream));
+    DevScene& d = h->d;
+    std::vector<float4> P, V, Hs, A, B, C;
+    int r = ref_order_field(h, d.pos, d.pos_s, P);
+    if (!r) r = ref_order_field(h, d.vel, d.vel_s, V);
+    if (!r) r = ref_order_field(h, d.hist, d.hist_s, Hs);
+    if (!r) r = ref_order_field(h, d.cA, d.cA_s, A);
+    if (!r) r = ref_order_field(h, d.cB, d.cB_s, B);
+    if (!r) r = ref_order_field(h, d.cC, d.cC_s, C);
+    if (r) return r;
+    const int nb = h->nb;
+    std::vector<float4> bp(nb), bref(nb);
+    std::vector<int> sid(nb);
+    if (nb) CK(cudaMemcpy(bp.data(), d.bpos, sizeof(float4) * nb, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < nb; ++i) {
+        bref[h->bgid_h[i]] = bp[i];
+        sid[h->bgid_h[i]] = h->bsolid_h[i];
+    }
+    float dt = 0.f;
+    CK(cudaMemcpy(&dt, d.dt, sizeof(float), cudaMemcpyDeviceToHost));
+    FILE* f = fopen(path, "wb");
+    if (!f) { h->err = std::string("cannot open ") + path; return SPHGPU_EINVAL; }
+    const int hdr[8] = {SPHGPU_ABI_VERSION, (int)sizeof(SphParams), h->cap, nb, (int)P.size(),
+                        (int)h->rho0_ph.size(), h->frame, h->last_solver};
+    bool ok = put(f, SNAP_MAGIC, 8) && put(f, hdr, 8) && put(f, &h->P, 1) && put(f, &h->time, 1) && put(f, &dt, 1) &&
+              put(f, h->rho0_ph.data(), h->rho0_ph.size()) && put(f, h->alpha_ph.data(), h->alpha_ph.size()) &&
+              put(f, bref.data(), nb) && put(f, sid.data(), nb) && put(f, P.data(), P.size()) &&
+              put(f, V.data(), V.size()) && put(f, Hs.data(), Hs.size()) && put(f, A.data(), A.size()) &&
+              put(f, B.data(), B.size()) && put(f, C.data(), C.size());
+    ok = (fclose(f) == 0) && ok;
+    if (!ok) { h->err = std::string("write failed: ") + path; return SPHGPU_EINVAL; }
+    return 0;
+}
+
+int sphgpu_load_snapshot(const char* path, int device, sphgpu_t* out) {
+    if (!path || !out) return SPHGPU_EINVAL;
+    *out = nullptr;
+    FILE* f = fopen(path, "rb");
+    if (!f) return SPHGPU_EINVAL;
+    char magic[8];
+    int hdr[8];
+    SphParams P;
+    double time = 0;
+    float dt = 0;
+    bool ok = get(f, magic, 8) && memcmp(magic, SNAP_MAGIC, 8) == 0 && get(f, hdr, 8) &&
+              hdr[0] == SPHGPU_ABI_VERSION && hdr[1] == (int)sizeof(SphParams) && get(f, &P, 1) && get(f, &time, 1) &&
+              get(f, &dt, 1);
+    const int cap = ok ? hdr[2] : 0, nb = ok ? hdr[3] : 0, n = ok ? hdr[4] : 0, nph = ok ? hdr[5] : 0;
+    ok = ok && cap > 0 && nb >= 0 && n >= 0 && n <= cap && nph >= 0 && nph <= 4;
+    std::vector<float> rho0(nph), alpha(nph);
+    std::vector<float4> bref(nb), Pp(n), V(n), Hs(n), A(n), B(n), C(n);
+    std::vector<int> sid(nb);
+    ok = ok && get(f, rho0.data(), nph) && get(f, alpha.data(), nph) && get(f, bref.data(), nb) &&
+         get(f, sid.data(), nb) && get(f, Pp.data(), n) && get(f, V.data(), n) && get(f, Hs.data(), n) &&
+         get(f, A.data(), n) && get(f, B.data(), n) && get(f, C.data(), n);
+    fclose(f);
+    if (!ok) return SPHGPU_EINVAL;
+    sphgpu_t h = nullptr;
+    int r = sphgpu_create(&P, device, cap, &h);
+    if (r) return r;
+    std::vector<float> xyz(3 * (size_t)nb), vol(nb);
+    for (int i = 0; i < nb; ++i) {
+        xyz[3 * i] = bref[i].x; xyz[3 * i + 1] = bref[i].y; xyz[3 * i + 2] = bref[i].z;
+        vol[i] = bref[i].w;
+    }
+    if (nb && (r = sphgpu_set_boundary(h, nb, xyz.data(), sid.data(), vol.data())) < 0) { sphgpu_destroy(h); return r; }
+    // phases in order (the reference order is phase-major)
+    for (int ph = 0, a = 0; ph < nph; ++ph) {
+        int b = a;
+        int w;
+        while (b < n && (memcpy(&w, &Pp[b].w, sizeof w), (w & 15) == ph)) ++b;
+        std::vector<float> px(3 * (size_t)(b - a)), vx(3 * (size_t)(b - a));
+        for (int i = a; i < b; ++i) {
+            px[3 * (i - a)] = Pp[i].x; px[3 * (i - a) + 1] = Pp[i].y; px[3 * (i - a) + 2] = Pp[i].z;
+            vx[3 * (i - a)] = V[i].x; vx[3 * (i - a) + 1] = V[i].y; vx[3 * (i - a) + 2] = V[i].z;
+        }
+        if (b > a) r = add_fluid_impl(h, b - a, px.data(), vx.data(), rho0[ph], alpha[ph], nullptr);
+        else {
+            // a phase that lost all its particles keeps its slot and constants
+            h->rho0_ph.push_back(rho0[ph]);
+            h->alpha_ph.push_back(alpha[ph]);
+            h->phase_n.push_back(0);
+            fill_solver_const(h);
+            r = 0;
+        }
+        if (r < 0) { sphgpu_destroy(h); return r; }
+        a = b;
+    }
+    // carried per-particle state into the staging arrays (gid = reference index)
+    DevScene& d = h->d;
+    cudaError_t e = cudaSuccess;
+    if (n) {
+        e = cudaMemcpy(d.hist_s, Hs.data(), sizeof(float4) * n, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(d.cA_s, A.data(), sizeof(float4) * n, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(d.cB_s, B.data(), sizeof(float4) * n, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(d.cC_s, C.data(), sizeof(float4) * n, cudaMemcpyHostToDevice);
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(d.dt, &dt, sizeof(float), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) { sphgpu_destroy(h); return SPHGPU_ECUDA; }
+    h->frame = hdr[6];
+    h->last_solver = hdr[7];
+    h->time = time;
+    *out = h;
+    return 0;
+}
+
+}  // extern "C"

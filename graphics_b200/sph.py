@@ -17,6 +17,7 @@ arrays are exposed as numpy arrays in the reference's particle order.
 classes use it and tests/bench use it directly.
 """
 import ctypes as C
+import os
 
 import numpy as np
 
@@ -182,6 +183,35 @@ class GpuScene:
         v = np.ascontiguousarray(values, dtype=np.float32).ravel()
         self._check(self.lib.sphgpu_set_fluid(self.h, field.encode(), _fptr(v)), "set " + field)
 
+    # -- output and restart --
+    def write_pos(self, path, phase=0, components=("position",), log_name=""):
+        """The reference's .pos file of one fluid phase (sphgpu_write_pos)."""
+        rc = self.lib.sphgpu_write_pos(self.h, os.fspath(path).encode(), int(phase), " ".join(components).encode(),
+                                       log_name.encode())
+        return self._check(rc, "write_pos")
+
+    def save_snapshot(self, path):
+        """Checkpoint of the scene (sphgpu_save_snapshot)."""
+        self._check(self.lib.sphgpu_save_snapshot(self.h, os.fspath(path).encode()), "save_snapshot")
+
+    @classmethod
+    def load_snapshot(cls, path, device=0):
+        """A new scene continuing a saved one (sphgpu_load_snapshot)."""
+        lib = _lib.load()
+        h = C.c_void_p()
+        rc = lib.sphgpu_load_snapshot(os.fspath(path).encode(), int(device), C.byref(h))
+        if rc:
+            raise SphGpuError(rc, "sphgpu_load_snapshot failed")
+        g = cls.__new__(cls)
+        g.lib, g.h = lib, h
+        with open(path, "rb") as f:
+            f.read(8)
+            hdr = np.frombuffer(f.read(32), np.int32)
+            p = _lib.SphParams()
+            C.memmove(C.byref(p), f.read(C.sizeof(p)), C.sizeof(p))
+        g.params, g.nb = p, int(hdr[3])
+        return g
+
     def get_boundary(self, field):
         comps = 3 if field == "position" else 1
         out = np.zeros(max(self.nb, 1) * comps, dtype=np.float32)
@@ -296,6 +326,30 @@ def batch_to_gpu(scenes, device=0, max_fluid=None, **params):
                 np.concatenate([np.full(sc.n_fluid, k, np.int32) for k, sc in enumerate(scenes)]),
                 rho0=scenes[0].rho0)
     return b
+
+
+def read_pos(path):
+    """A .pos file in the reference's format (read_fluid_particles,
+    fUtility.h:486-510): (records as an (n, floats per particle) float32
+    array, component mask, frame number)."""
+    lib = _lib.load()
+    n = lib.sphgpu_read_pos(os.fspath(path).encode(), None, 0, None, 0, None)
+    if n < 0:
+        raise SphGpuError(int(n), "read_pos " + os.fspath(path))
+    mask = C.create_string_buffer(256)
+    frame = C.c_int()
+    size = os.path.getsize(path)
+    buf = np.zeros(max(size // 4, 1), np.float32)
+    n = lib.sphgpu_read_pos(os.fspath(path).encode(), _fptr(buf), len(buf), mask, 256, C.byref(frame))
+    if n < 0:
+        raise SphGpuError(int(n), "read_pos " + os.fspath(path))
+    per = 0
+    m = mask.value.decode()
+    for word, k in (("position", 3), ("velocity", 3), ("color", 4), ("density", 1), ("presure", 1),
+                    ("acceleration", 3), ("dt", 1)):
+        if word in m:
+            per += k
+    return buf[:n * per].reshape(n, per), m, frame.value
 
 
 def scene_to_gpu(scene, device=0, max_fluid=None, **params):

@@ -206,6 +206,32 @@ int sphgpu_set_fluid(sphgpu_t h, const char* field, const float* in);
  * "VF_kappa","VF_kappaV","VF_advectionVolume","VF_divergenceDeviation". */
 int sphgpu_get_boundary(sphgpu_t h, const char* field, float* out);
 
+/* Particle output in the reference's .pos format (write_fluid_particles,
+ * fUtility.h:254-303; Demo-Main.cpp:250-251 writes one file per phase and
+ * frame): line 1 names the scene log file (log_name), line 2 the components,
+ * line 3 the frame number and fluid index, line 4 the particle count, then
+ * per particle of fluid phase `phase`, in the reference's order, the chosen
+ * components as float32 in the reference's fixed component order: "position"
+ * (3), "velocity" (3), "density" (1), "presure" (1), "acceleration" (3);
+ * components = any of those words (NULL: "position", the reference's default
+ * WRITE_PARTICLE_position).  Returns the particle count written. */
+int sphgpu_write_pos(sphgpu_t h, const char* path, int phase, const char* components, const char* log_name);
+/* read_fluid_particles (fUtility.h:486-510): the particle count of a .pos
+ * file; with out != NULL also its records (max_floats = capacity of out in
+ * floats), the component mask line (mask, mask_len) and the frame number.
+ * Needs no GPU. */
+long long sphgpu_read_pos(const char* path, float* out, long long max_floats, char* mask, int mask_len, int* frame);
+
+/* Checkpoint / resume (no counterpart in the reference, whose restart is a
+ * .pos re-import): save a single scene -- parameters, walls with their
+ * volumes and solid ids, every fluid particle with the state the solvers
+ * carry between steps (warm-start history, PCISPH / IISPH_M / IISph carried
+ * values), frame and step length -- and load it into a new handle on
+ * `device`.  Stepping the loaded handle continues the saved run bit for bit.
+ * An attached warm-start network is not part of the snapshot. */
+int sphgpu_save_snapshot(sphgpu_t h, const char* path);
+int sphgpu_load_snapshot(const char* path, int device, sphgpu_t* out);
+
 /* Stage-level entry points (parity tests run "given state S, call stage X"):
  *   "neighbourSearch"                 grid + neighbour lists (+ rho/alpha)
  *   "DF_constantDensitySolverFirst"   rho, alpha            (DFSPH.cpp:84-193)
