@@ -14,6 +14,7 @@ OK, EINVAL, ENOMEM, ECUDA, EMAXITER, ENAN, ENEIGHBOUR_OVERFLOW, EOUT_OF_DOMAIN, 
 WCSPH, PCISPH, IISPH_M, DFSPH, IISPH = 0, 1, 2, 3, 4
 STATUS_MAXITER_DENSITY, STATUS_MAXITER_DIVERGENCE, STATUS_NAN = 1, 2, 4
 STATUS_NEIGHBOUR_OVERFLOW, STATUS_OUT_OF_DOMAIN, STATUS_ZERO_DISTANCE = 8, 16, 32
+STATUS_SOLID_OUTSIDE = 64
 
 _f3 = C.c_float * 3
 
@@ -48,6 +49,18 @@ class SphStepStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
 
 
+class SphRigidState(C.Structure):
+    """A rigid body's state as Bullet reports it (OpenGL column-major
+    transform, centre of mass, linear and angular velocity)."""
+    _fields_ = [("transform", C.c_float * 16), ("center_of_mass", _f3), ("linear_velocity", _f3),
+                ("angular_velocity", _f3)]
+
+
+# int fn(void* user, int nsolids, const int* solid_ids, const double* force,
+#        const double* torque, double dt, SphRigidState* states)
+RIGID_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double),
+                       C.POINTER(C.c_double), C.c_double, C.POINTER(SphRigidState))
+
 # every symbol include/sphgpu.h declares, with (restype, argtypes)
 _vp, _i, _f, _d = C.c_void_p, C.c_int, C.c_float, C.c_double
 _fp, _ip, _cp = C.POINTER(C.c_float), C.POINTER(C.c_int), C.c_char_p
@@ -72,6 +85,11 @@ SIGNATURES = {
     "sphgpu_read_pos": (C.c_longlong, [_cp, _fp, C.c_longlong, _cp, _i, _ip]),
     "sphgpu_save_snapshot": (_i, [_vp, _cp]),
     "sphgpu_load_snapshot": (_i, [_cp, _i, C.POINTER(_vp)]),
+    "sphgpu_set_solid_dynamic": (_i, [_vp, _i, _fp, C.POINTER(SphRigidState)]),
+    "sphgpu_set_rigid_callback": (_i, [_vp, RIGID_FN, _vp]),
+    "sphgpu_set_solid_state": (_i, [_vp, _i, C.POINTER(SphRigidState)]),
+    "sphgpu_get_solid_state": (_i, [_vp, _i, C.POINTER(SphRigidState)]),
+    "sphgpu_get_solid_force": (_i, [_vp, _i, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "sphgpu_get_neighbours": (_i, [_vp, _ip, _ip, _ip]),
     "sphgpu_get_cells": (_i, [_vp, C.POINTER(C.c_longlong)]),
     "sphgpu_stream": (_vp, [_vp]),

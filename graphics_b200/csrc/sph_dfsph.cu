@@ -101,10 +101,11 @@ __global__ void __launch_bounds__(BS) k_df_forces(DevScene s, SolverConst c, int
         for (int k = 0; k < cnt; ++k) {
             const unsigned e = (unsigned)ell_get(s.nbr, stride, p, k);
             // one 32-byte record per neighbour: {(x, y, z, rho), v} or, for
-            // a boundary particle, {(x, y, z, volume), v}
+            // a boundary particle, {(x, y, z, volume), singleVelocity +
+            // velocity} (DFSPH.cpp:1349)
             float4 pb, vb;
             const bool bnd = (e & BND_FLAG) != 0u;
-            ld_record32((bnd ? s.bpv : s.prv) + 2 * (size_t)(e & BND_MASK), pb, vb);
+            ld_record32((bnd ? s.bpf : s.prv) + 2 * (size_t)(e & BND_MASK), pb, vb);
             const float m = bnd ? rho0 * pb.w / rhoa   // (frho0*volume)/fa.density, DFSPH.cpp:1353
                                 : fm0 / pb.w;          // fm0/fb.density, DFSPH.cpp:1265
             const float xx = pa.x - pb.x, xy = pa.y - pb.y, xz = pa.z - pb.z;

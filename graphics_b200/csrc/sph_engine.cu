@@ -114,6 +114,19 @@ struct sphgpu_scene {
     int last_scene = 0;           // scenes receive their fluid in order
     GridGeom* d_geom = nullptr;
     void* d_batch = nullptr;      // one allocation holding the BatchDev arrays
+    // dynamic rigid solids (DFSPH): device data, the dense list of dynamic
+    // solids with their reference ranges, pinned exchange buffers
+    RigidDev R{};
+    std::vector<int> dyn_ids, dyn_r0, dyn_r1;
+    float* h_rstate = nullptr;    // [cap * 25] states (SphRigidState layout)
+    double* h_rout = nullptr;     // [cap * 6 + 1] joined force, torque; dt
+    int rigid_cap = 0;            // capacity of the per-solid arrays
+    void* sort_tmp = nullptr;
+    size_t sort_bytes = 0;
+    int sort_end_bit = 1;
+    sphgpu_rigid_fn rigid_fn = nullptr;
+    void* rigid_user = nullptr;
+    int rigid_fail = 0;
 };
 
 namespace {
@@ -321,6 +334,31 @@ int alloc_scene(sphgpu_scene* h) {
     return cudaStreamSynchronize(h->stream) == cudaSuccess ? 0 : SPHGPU_ECUDA;
 }
 
+// dynamic-solid state (the boundary returns to static walls)
+void free_rigid(sphgpu_scene* h) {
+    RigidDev& R = h->R;
+    DevScene& d = h->d;
+    void* ptrs[] = {R.x0, R.vol, R.dyn, R.sid, R.state, R.wpos, R.wvel, R.key_in, R.val_in, R.key_out, R.val_out,
+                    R.binv, R.out, R.partial, R.ticket, d.bforce, d.bks, h->sort_tmp};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (d.bpf && d.bpf != d.bpv) cudaFree(d.bpf);
+    d.bpf = d.bpv;
+    d.bforce = nullptr;
+    d.bks = nullptr;
+    if (h->h_rstate) cudaFreeHost(h->h_rstate);
+    if (h->h_rout) cudaFreeHost(h->h_rout);
+    h->h_rstate = nullptr;
+    h->h_rout = nullptr;
+    h->sort_tmp = nullptr;
+    h->sort_bytes = 0;
+    h->rigid_cap = 0;
+    R = RigidDev{};
+    h->dyn_ids.clear();
+    h->dyn_r0.clear();
+    h->dyn_r1.clear();
+}
+
 void free_scene(sphgpu_scene* h) {
     DevScene& d = h->d;
     void* ptrs[] = {d.pos, d.vel, d.gid, d.rho, d.alpha, d.vadv, d.pv, d.pk, d.prv, d.bpv, d.kappav, d.acc, d.kr, d.kappa, d.ksum, d.aux0,
@@ -332,6 +370,7 @@ void free_scene(sphgpu_scene* h) {
                     d.bpos, d.bvel, d.bgid, h->cub_tmp};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    free_rigid(h);
     if (h->d_geom) cudaFree(h->d_geom);
     if (h->d_batch) cudaFree(h->d_batch);
     if (h->h_stats) cudaFreeHost(h->h_stats);
@@ -341,6 +380,16 @@ void free_scene(sphgpu_scene* h) {
 }
 
 // ---------------- step building blocks ----------------
+
+// updatePaticles of every dynamic solid with the states in h_rstate, and the
+// re-sort of the whole boundary (SphWithBullet.cpp:212-221)
+void enq_boundary_update(sphgpu_scene* h, cudaStream_t st) {
+    if (!h->R.nd) return;
+    cudaMemcpyAsync(h->R.state, h->h_rstate, sizeof(float) * 25 * h->R.nd, cudaMemcpyHostToDevice, st);
+    launch(h, "rigid_place", st, [&] {
+        launch_rigid_place_sort(h->d, h->R, h->g, h->sort_tmp, h->sort_bytes, h->sort_end_bit, st);
+    });
+}
 
 void enq_ns(sphgpu_scene* h, int integrate, int build_mode, cudaStream_t st, int carry = 1) {
     DevScene& d = h->d;
@@ -353,6 +402,9 @@ void enq_ns(sphgpu_scene* h, int integrate, int build_mode, cudaStream_t st, int
     launch(h, "reorder", st, [&] { launch_scatter_reorder(d, h->g, h->cap, carry, st); });
     launch_count_active(d, h->g, st);
     if (h->nscenes > 1) launch_batch_count(d, h->nscenes, st);
+    if (h->R.nd)
+        launch(h, "rigid_volume", st,
+               [&] { launch_rigid_volume(d, h->R, h->g, h->P.particle_d, h->c.h2cut, h->ncap, st); });
     launch(h, build_mode == 1 ? "build_first" : (build_mode == 2 ? "build_pressure" : "build"), st,
            [&] { launch_build(d, h->g, h->c, build_mode, h->cap, st, h->tune.build); });
 }
@@ -433,10 +485,39 @@ int enq_df_div_loop(sphgpu_scene* h, bool capturing) {
 // The body of one DFSPH step after the first neighbour search
 // (DFSPH::sphStep, DFSPH.cpp:52-62), with the learned warm start when a
 // network is attached (ws_mode 1) or training-data recording (ws_mode 2).
+// Part 1: forces, the density loop and, with dynamic solids, their boundary
+// forces (copied to h_rout); part 2: updateSolids' particle update, the
+// neighbour search with rho/alpha, the divergence loop.  Without dynamic
+// solids one graph holds both; with them the rigid-body world runs on the
+// host between the two.
+int enq_df_part1(sphgpu_scene* h, bool capturing);
+int enq_df_part2(sphgpu_scene* h, bool capturing);
+
 int enq_df_step(sphgpu_scene* h, bool capturing) {
+    int r = enq_df_part1(h, capturing);
+    return r ? r : enq_df_part2(h, capturing);
+}
+
+// boundary forces of every dynamic solid and their FP64 joins -> h_rout
+void enq_rigid_forces(sphgpu_scene* h, cudaStream_t st) {
+    const int nd = h->R.nd;
+    if (!nd) return;
+    for (int i = 0; i < nd; ++i)
+        launch(h, "rigid_force", st, [&] {
+            launch_rigid_force(h->d, h->R, h->c, h->g, h->dyn_r0[i], h->dyn_r1[i], i, st);
+        });
+    cudaMemcpyAsync(h->h_rout, h->R.out, sizeof(double) * 6 * nd, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(h->h_rout + 6 * nd, h->d.dt, sizeof(float), cudaMemcpyDeviceToHost, st);
+}
+
+int enq_df_part1(sphgpu_scene* h, bool capturing) {
     DevScene& d = h->d;
     cudaStream_t st = h->stream;
     launch_step_begin(d, st);
+    // the boundary forces read the loop's summed stiffness; without the
+    // warm start (whose post-processing clears the sum) it restarts here
+    const bool dyn = h->R.nd > 0;
+    if (dyn && !(h->mlp && h->ws_mode)) cudaMemsetAsync(d.ksum, 0, sizeof(float) * h->cap, st);
     if (h->P.cfl && h->nscenes > 1)
         launch(h, "cfl", st, [&] {
             launch_batch_cfl(d, h->nscenes, h->P.cfl_factor, h->P.particle_d, h->P.dt_max, h->P.dt_min, st);
@@ -459,10 +540,11 @@ int enq_df_step(sphgpu_scene* h, bool capturing) {
         });
     }
     const int rec = h->record_ksum;
-    h->record_ksum = rec || ws != 0;
+    h->record_ksum = rec || ws != 0 || dyn;
     int r = enq_df_density_loop(h, capturing);
     h->record_ksum = rec;
     if (r) return r;
+    enq_rigid_forces(h, st);
     if (ws) {
         launch(h, "ws_post", st, [&] { launch_ws_post(d, h->c, ws == 2 ? h->recY : nullptr, h->cap, st); });
         if (ws == 2) {
@@ -471,8 +553,15 @@ int enq_df_step(sphgpu_scene* h, bool capturing) {
                              m->ds_count, m->ds_cap, st);
         }
     }
+    return 0;
+}
+
+int enq_df_part2(sphgpu_scene* h, bool capturing) {
+    DevScene& d = h->d;
+    cudaStream_t st = h->stream;
+    enq_boundary_update(h, st);
     enq_ns(h, 1, 1, st);
-    r = enq_df_div_loop(h, capturing);
+    int r = enq_df_div_loop(h, capturing);
     if (r) return r;
     CK(cudaMemcpyAsync(h->h_stats, d.st, sizeof(DevStats), cudaMemcpyDeviceToHost, st));
     return 0;
@@ -649,6 +738,7 @@ int iv_graph_build(sphgpu_scene* h, bool cap) { return enq_iv_step(h, cap); }
 
 int run_initial_ns(sphgpu_scene* h, int build_mode) {
     if (!h->in_staging) stage_from_sorted(h, h->h_stats->n_active);  // the sort reads staging
+    enq_boundary_update(h, h->stream);
     enq_ns(h, 0, build_mode, h->stream, 1 | 2 | 4 | 8);
     h->in_staging = false;
     h->ns_valid = build_mode == 1;
@@ -685,6 +775,30 @@ int graph_for(sphgpu_scene* h, int key, cudaGraphExec_t* out, int (*build)(sphgp
 }
 
 int df_graph_build(sphgpu_scene* h, bool cap) { return enq_df_step(h, cap); }
+int df1_graph_build(sphgpu_scene* h, bool cap) { return enq_df_part1(h, cap); }
+int df2_graph_build(sphgpu_scene* h, bool cap) { return enq_df_part2(h, cap); }
+
+// SphWithBullet::updateSolids' exchange with the rigid-body world: the
+// joined forces of the last step (h_rout, on the host once the stream is
+// synchronised) in, the new states (h_rstate) out
+int run_rigid_callback(sphgpu_scene* h) {
+    const int nd = h->R.nd;
+    if (!nd || !h->rigid_fn) return 0;
+    const double* f = h->h_rout;
+    std::vector<double> force(3 * nd), torque(3 * nd);
+    for (int i = 0; i < nd; ++i)
+        for (int c = 0; c < 3; ++c) {
+            force[3 * i + c] = f[6 * i + c];
+            torque[3 * i + c] = f[6 * i + 3 + c];
+        }
+    float dt;
+    memcpy(&dt, h->h_rout + 6 * nd, sizeof(float));
+    static_assert(sizeof(SphRigidState) == 25 * sizeof(float), "SphRigidState is 25 floats");
+    if (h->rigid_fn(h->rigid_user, nd, h->dyn_ids.data(), force.data(), torque.data(), (double)dt,
+                    reinterpret_cast<SphRigidState*>(h->h_rstate)))
+        h->rigid_fail = 1;
+    return 0;
+}
 
 void invalidate_graphs(sphgpu_scene* h) {
     for (auto& kv : h->graphs) cudaGraphExecDestroy(kv.second);
@@ -693,6 +807,7 @@ void invalidate_graphs(sphgpu_scene* h) {
 
 int status_to_rc(unsigned s) {
     if (s & SPHGPU_STATUS_NAN) return SPHGPU_ENAN;
+    if (s & SPHGPU_STATUS_SOLID_OUTSIDE) return SPHGPU_EOUT_OF_DOMAIN;
     if (s & (SPHGPU_STATUS_MAXITER_DENSITY | SPHGPU_STATUS_MAXITER_DIVERGENCE)) return SPHGPU_EMAXITER;
     return 0;
 }
@@ -736,6 +851,14 @@ int enq_steps(sphgpu_scene* h, int solver, int nsteps) {
         h->err = "a batch of scenes runs the plain DFSPH solver";
         return SPHGPU_ENOTIMPL;
     }
+    if (h->R.nd && solver != SPHGPU_DFSPH) {
+        h->err = "dynamic solids are coupled in the DFSPH step";
+        return SPHGPU_ENOTIMPL;
+    }
+    if (h->R.nd && h->record_ksum) {
+        h->err = "record_kappa_sum cannot be combined with dynamic solids";
+        return SPHGPU_EINVAL;
+    }
     launch_call_begin(h->d, h->stream);
     if (h->nscenes > 1) launch_batch_call_begin(h->d, h->nscenes, h->stream);
     if (solver == SPHGPU_PCISPH || solver == SPHGPU_IISPH_M || solver == SPHGPU_IISPH) {
@@ -777,17 +900,34 @@ int enq_steps(sphgpu_scene* h, int solver, int nsteps) {
             int r = run_initial_ns(h, 1);
             if (r) return r;
         }
+        const bool dyn = h->R.nd > 0;
         for (int s = 0; s < nsteps; ++s) {
+            const int key = (h->mlp ? h->ws_mode : 0) | (h->record_ksum ? 4 : 0) | (h->P.cfl ? 8 : 0);
             if (h->use_graphs && !h->prof.on) {
                 cudaGraphExec_t ex;
-                int key = (h->mlp ? h->ws_mode : 0) | (h->record_ksum ? 4 : 0) | (h->P.cfl ? 8 : 0);
-                int r = graph_for(h, key, &ex, df_graph_build);
+                int r = dyn ? graph_for(h, key | 16, &ex, df1_graph_build) : graph_for(h, key, &ex, df_graph_build);
                 if (r) return r;
                 CK(cudaGraphLaunch(ex, h->stream));
             } else {
-                int r = enq_df_step(h, false);
+                int r = dyn ? enq_df_part1(h, false) : enq_df_step(h, false);
                 if (r) return r;
                 prof_collect(h);
+            }
+            if (dyn) {
+                // the rigid-body world between the density loop and the
+                // neighbour search (DFSPH.cpp:52-56)
+                CK(cudaStreamSynchronize(h->stream));
+                run_rigid_callback(h);
+                if (h->use_graphs && !h->prof.on) {
+                    cudaGraphExec_t ex;
+                    int r = graph_for(h, key | 32, &ex, df2_graph_build);
+                    if (r) return r;
+                    CK(cudaGraphLaunch(ex, h->stream));
+                } else {
+                    int r = enq_df_part2(h, false);
+                    if (r) return r;
+                    prof_collect(h);
+                }
             }
             h->frame++;
         }
@@ -824,6 +964,102 @@ void ref_order(const std::vector<int>& gid, std::vector<int>& order) {
     std::sort(order.begin(), order.end(), [&](int a, int b) { return gid[a] < gid[b]; });
 }
 
+}  // namespace
+
+// ---- dynamic rigid solids ----
+namespace {
+// with a dynamic solid the boundary is re-sorted every step: refresh the
+// host copies of its order (reference index and solid of each sorted slot)
+int sync_boundary_order(sphgpu_scene* h) {
+    if (!h->R.nd || !h->nb) return 0;
+    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaMemcpy(h->bgid_h.data(), h->d.bgid, sizeof(int) * h->nb, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(h->bsolid_h.data(), h->d.bsid, sizeof(int) * h->nb, cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+int dyn_index(sphgpu_scene* h, int solid_id) {
+    for (size_t i = 0; i < h->dyn_ids.size(); ++i)
+        if (h->dyn_ids[i] == solid_id) return (int)i;
+    return -1;
+}
+
+// device arrays for the dynamic-solid path, on first use: the boundary in
+// reference order (world positions, static volumes), sort scratch, records
+int rigid_init(sphgpu_scene* h) {
+    if (h->R.x0) return 0;
+    DevScene& d = h->d;
+    RigidDev& R = h->R;
+    const int nb = h->nb;
+    R.nb = nb;
+    int r = dalloc(h, &R.x0, nb) | dalloc(h, &R.vol, nb) | dalloc(h, &R.dyn, nb) | dalloc(h, &R.sid, nb) |
+            dalloc(h, &R.wpos, nb) | dalloc(h, &R.wvel, nb) | dalloc(h, &R.key_in, nb) | dalloc(h, &R.val_in, nb) |
+            dalloc(h, &R.key_out, nb) | dalloc(h, &R.val_out, nb) | dalloc(h, &R.binv, nb) |
+            dalloc(h, &R.partial, 6 * ((size_t)nb / 128 + 2)) | dalloc(h, &d.bforce, nb) | dalloc(h, &d.bks, nb);
+    float4* bpf = nullptr;
+    r |= dalloc(h, &bpf, 2 * (size_t)nb);
+    if (!d.bsid) r |= dalloc(h, &d.bsid, nb);
+    if (r) return SPHGPU_ENOMEM;
+    d.bpf = bpf;
+    int bits = 1;
+    while (bits < 31 && (1ll << bits) <= (long long)(h->g.nkeys - 1)) ++bits;
+    h->sort_end_bit = bits;
+    h->sort_bytes = rigid_sort_bytes(nb, bits);
+    if (cudaMalloc(&h->sort_tmp, h->sort_bytes + 16) != cudaSuccess) return SPHGPU_ENOMEM;
+    // reference order from the sorted walls
+    std::vector<float4> bp(nb), x0(nb);
+    std::vector<float> vol(nb);
+    std::vector<int> dyn(nb, -1), sid(nb);
+    CK(cudaMemcpy(bp.data(), d.bpos, sizeof(float4) * nb, cudaMemcpyDeviceToHost));
+    for (int q = 0; q < nb; ++q) {
+        const int k = h->bgid_h[q];
+        x0[k] = make_float4(bp[q].x, bp[q].y, bp[q].z, 0.f);
+        vol[k] = bp[q].w;
+        sid[k] = h->bsolid_h[q];
+    }
+    CK(cudaMemcpy(R.x0, x0.data(), sizeof(float4) * nb, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(R.vol, vol.data(), sizeof(float) * nb, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(R.dyn, dyn.data(), sizeof(int) * nb, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(R.sid, sid.data(), sizeof(int) * nb, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d.bsid, h->bsolid_h.data(), sizeof(int) * nb, cudaMemcpyHostToDevice));
+    CK(cudaMemset(d.bforce, 0, sizeof(float4) * nb));
+    return 0;
+}
+
+// per-solid arrays with room for n dynamic solids
+int rigid_reserve(sphgpu_scene* h, int n) {
+    if (n <= h->rigid_cap) return 0;
+    const int cap = std::max(n, std::max(8, 2 * h->rigid_cap));
+    RigidDev& R = h->R;
+    float* st = nullptr;
+    double* out = nullptr;
+    unsigned* tk = nullptr;
+    float* hst = nullptr;
+    double* hout = nullptr;
+    if (dalloc(h, &st, 25 * (size_t)cap) || dalloc(h, &out, 6 * (size_t)cap) || dalloc(h, &tk, cap))
+        return SPHGPU_ENOMEM;
+    if (cudaMallocHost((void**)&hst, sizeof(float) * 25 * cap) != cudaSuccess ||
+        cudaMallocHost((void**)&hout, sizeof(double) * (6 * cap + 1)) != cudaSuccess)
+        return SPHGPU_ENOMEM;
+    memset(hst, 0, sizeof(float) * 25 * cap);
+    memset(hout, 0, sizeof(double) * (6 * cap + 1));
+    CK(cudaMemset(tk, 0, sizeof(unsigned) * cap));
+    CK(cudaMemset(out, 0, sizeof(double) * 6 * cap));
+    if (h->h_rstate) memcpy(hst, h->h_rstate, sizeof(float) * 25 * h->rigid_cap);
+    if (h->h_rout) memcpy(hout, h->h_rout, sizeof(double) * 6 * h->rigid_cap);
+    if (R.state) cudaFree(R.state);
+    if (R.out) cudaFree(R.out);
+    if (R.ticket) cudaFree(R.ticket);
+    if (h->h_rstate) cudaFreeHost(h->h_rstate);
+    if (h->h_rout) cudaFreeHost(h->h_rout);
+    R.state = st;
+    R.out = out;
+    R.ticket = tk;
+    h->h_rstate = hst;
+    h->h_rout = hout;
+    h->rigid_cap = cap;
+    return 0;
+}
 }  // namespace
 
 // ======================= C ABI =======================
@@ -1017,6 +1253,7 @@ static int set_boundary_impl(sphgpu_t h, int n, const float* xyz, const int* sol
     if (scene)
         for (int i = 0; i < n; ++i)
             if (scene[i] < 0 || scene[i] >= h->nscenes) { h->err = "boundary scene index out of range"; return SPHGPU_EINVAL; }
+    free_rigid(h);
     if (d.bpos) { cudaFree(d.bpos); cudaFree(d.bvel); cudaFree(d.bgid); cudaFree(d.bpv); d.bpos = nullptr; }
     for (void* q : {(void*)d.bsid, (void*)d.bnbr, (void*)d.bncount, (void*)d.bivs, (void*)d.bivo})
         if (q) cudaFree(q);
@@ -1028,6 +1265,7 @@ static int set_boundary_impl(sphgpu_t h, int n, const float* xyz, const int* sol
     for (int i = 0; i < n; ++i) bp[i] = make_float4(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], volume ? volume[i] : 0.f);
     if (dalloc(h, &d.bpos, n) || dalloc(h, &d.bvel, n) || dalloc(h, &d.bgid, n) || dalloc(h, &d.bpv, 2 * (size_t)n))
         return SPHGPU_ENOMEM;
+    d.bpf = d.bpv;
     // cell keys on the device, each particle with its scene's grid
     std::vector<int> keys(n);
     {
@@ -1234,6 +1472,12 @@ int sphgpu_synchronize(sphgpu_t h, SphStepStats* stats) {
     int rc = status_to_rc(h->h_stats->status);
     if (rc == SPHGPU_ENAN) h->err = "non-finite particle state";
     else if (rc == SPHGPU_EMAXITER) h->err = "solver loop reached its iteration cap";
+    else if (rc == SPHGPU_EOUT_OF_DOMAIN) h->err = "a dynamic solid left the grid";
+    if (h->rigid_fail) {
+        h->rigid_fail = 0;
+        h->err = "the rigid-body callback failed";
+        return SPHGPU_EINVAL;
+    }
     return rc;
 }
 
@@ -1478,10 +1722,35 @@ int sphgpu_set_fluid(sphgpu_t h, const char* field, const float* in) {
 int sphgpu_get_boundary(sphgpu_t h, const char* field, float* out) {
     if (!h || !field || !out) return SPHGPU_EINVAL;
     cudaSetDevice(h->device);
+    CK(cudaStreamSynchronize(h->stream));
     int n = h->nb;
     std::vector<float4> t(n);
     CK(cudaMemcpy(t.data(), h->d.bpos, sizeof(float4) * n, cudaMemcpyDeviceToHost));
     std::string f(field);
+    if (h->R.nd) {
+        if (int r = sync_boundary_order(h)) return r;
+        if (f == "velocity" || f == "force" || f == "kerSumFromSelf") {
+            if (f == "velocity") {
+                std::vector<float4> rec(2 * (size_t)n);
+                CK(cudaMemcpy(rec.data(), h->d.bpf, sizeof(float4) * 2 * n, cudaMemcpyDeviceToHost));
+                for (int i = 0; i < n; ++i) t[i] = rec[2 * (size_t)i + 1];
+            } else if (f == "force") {
+                CK(cudaMemcpy(t.data(), h->d.bforce, sizeof(float4) * n, cudaMemcpyDeviceToHost));
+            } else {
+                std::vector<float> ks(n);
+                CK(cudaMemcpy(ks.data(), h->d.bks, sizeof(float) * n, cudaMemcpyDeviceToHost));
+                for (int i = 0; i < n; ++i) out[h->bgid_h[i]] = ks[i];
+                return n;
+            }
+            for (int i = 0; i < n; ++i) {
+                const int k = h->bgid_h[i];
+                out[3 * k] = t[i].x;
+                out[3 * k + 1] = t[i].y;
+                out[3 * k + 2] = t[i].z;
+            }
+            return n;
+        }
+    }
     if (f != "position" && f != "volume") {
         // IISph boundary loop state
         static const char* names[8] = {"VF_gamma", "VF_sphVolume", "VF_alpha", nullptr,
@@ -1520,13 +1789,22 @@ int sphgpu_stage(sphgpu_t h, const char* name, SphStepStats* stats) {
     launch_step_begin(d, st);
     if (s == "neighbourSearch" || s == "DF_constantDensitySolverFirst" || s == "wc_computePressure") {
         int mode = s == "wc_computePressure" ? 2 : 1;
+        if (h->R.nd && mode != 1) { h->err = "dynamic solids are coupled in the DFSPH step"; return SPHGPU_ENOTIMPL; }
+        enq_boundary_update(h, st);
         if (h->in_staging) {
             enq_ns(h, 0, mode, st);
             h->in_staging = false;
         } else {
+            if (h->R.nd) {
+                launch_merge_starts(d, h->g, st);
+                launch_rigid_volume(d, h->R, h->g, h->P.particle_d, h->c.h2cut, h->ncap, st);
+            }
             launch_build(d, h->g, h->c, mode, h->cap, st);
         }
         h->ns_valid = mode == 1;
+    } else if (s == "updateSolids") {
+        CK(cudaStreamSynchronize(st));
+        run_rigid_callback(h);
     } else if (s == "DF_forceExceptPressure") {
         if (h->in_staging) { h->err = "run neighbourSearch first"; return SPHGPU_EINVAL; }
         launch_df_forces(d, h->c, h->cap, 0, st);
@@ -1539,8 +1817,15 @@ int sphgpu_stage(sphgpu_t h, const char* name, SphStepStats* stats) {
             launch_ws_infer(d, h->c, h->mlp->m, h->xn, h->cap, h->sm_count, st);
             launch_df_warm_correction(d, h->c, h->cap, st);
         }
+        const bool dyn = h->R.nd > 0;
+        if (dyn && !(h->mlp && h->ws_mode == 1)) cudaMemsetAsync(d.ksum, 0, sizeof(float) * h->cap, st);
+        const int rec = h->record_ksum;
+        h->record_ksum = rec || dyn;
         r = enq_df_density_loop(h, false);
+        h->record_ksum = rec;
         if (r) return r;
+        enq_rigid_forces(h, st);
+        if (dyn && h->mlp && h->ws_mode == 1) launch_ws_post(d, h->c, nullptr, h->cap, st);
         // integrate into staging (the reference updates positions in place)
         cudaMemsetAsync(d.cell_count, 0, sizeof(int) * ((size_t)h->g.nkeys + 1), st);
         launch_hash(d, h->g, 1, h->cap, st);
@@ -1584,6 +1869,7 @@ int sphgpu_get_neighbours(sphgpu_t h, int* counts, int* t, int* idx) {
     if (!h || !counts || !t || !idx) return SPHGPU_EINVAL;
     cudaSetDevice(h->device);
     if (h->in_staging) { h->err = "no neighbour lists (run neighbourSearch)"; return SPHGPU_EINVAL; }
+    if (int rs = sync_boundary_order(h)) return rs;
     std::vector<int> gid;
     int n;
     if (download_gid(h, gid, n, false)) return SPHGPU_ECUDA;
@@ -2112,6 +2398,103 @@ int sphgpu_batch_scene_range(sphgpu_t h, int scene, int* first, int* count) {
 // reference-facing surface): record the summed density-loop stiffness per
 // particle (training labels for the warm-start network), and switch CUDA
 // graphs off (host-driven loops).
+
+int sphgpu_set_solid_dynamic(sphgpu_t h, int solid_id, const float* inner_xyz, const SphRigidState* state) {
+    if (!h || !inner_xyz || !state) return SPHGPU_EINVAL;
+    if (h->nscenes > 1) { h->err = "dynamic solids are for single scenes"; return SPHGPU_EINVAL; }
+    cudaSetDevice(h->device);
+    CK(cudaStreamSynchronize(h->stream));
+    if (int rs = sync_boundary_order(h)) return rs;
+    // the solid's range in reference order (solids by id, each in insertion order)
+    std::vector<int> sid_ref(h->nb);
+    for (int q = 0; q < h->nb; ++q) sid_ref[h->bgid_h[q]] = h->bsolid_h[q];
+    int r0 = -1, r1 = -1;
+    for (int k = 0; k < h->nb; ++k)
+        if (sid_ref[k] == solid_id) {
+            if (r0 < 0) r0 = k;
+            r1 = k + 1;
+        }
+    if (r0 < 0) { h->err = "no boundary particle has this solid id"; return SPHGPU_EINVAL; }
+    int r = rigid_init(h);
+    if (r) return r;
+    int di = dyn_index(h, solid_id);
+    if (di < 0) {
+        if ((r = rigid_reserve(h, (int)h->dyn_ids.size() + 1))) return r;
+        di = (int)h->dyn_ids.size();
+        h->dyn_ids.push_back(solid_id);
+        h->dyn_r0.push_back(r0);
+        h->dyn_r1.push_back(r1);
+    }
+    RigidDev& R = h->R;
+    R.nd = (int)h->dyn_ids.size();
+    const int n = r1 - r0;
+    // body-frame positions, keeping kerSumFromSelf in .w
+    std::vector<float4> x0(n);
+    CK(cudaMemcpy(x0.data(), R.x0 + r0, sizeof(float4) * n, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < n; ++i) {
+        x0[i].x = inner_xyz[3 * i];
+        x0[i].y = inner_xyz[3 * i + 1];
+        x0[i].z = inner_xyz[3 * i + 2];
+    }
+    CK(cudaMemcpy(R.x0 + r0, x0.data(), sizeof(float4) * n, cudaMemcpyHostToDevice));
+    std::vector<int> dv(n, di);
+    CK(cudaMemcpy(R.dyn + r0, dv.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    memcpy(h->h_rstate + 25 * di, state, sizeof(SphRigidState));
+    // SphWithBullet::addSolid: updatePaticles, then prepareSolidPartWeight
+    enq_boundary_update(h, h->stream);
+    launch_rigid_prepare(h->d, R, h->g, h->P.particle_d, h->c.h2cut, h->ncap, h->stream);
+    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaGetLastError());
+    CK(cudaMemcpy(h->bgid_h.data(), h->d.bgid, sizeof(int) * h->nb, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(h->bsolid_h.data(), h->d.bsid, sizeof(int) * h->nb, cudaMemcpyDeviceToHost));
+    // the fluid lists hold the old boundary order: the next step searches anew
+    if (!h->in_staging) stage_from_sorted(h, h->h_stats->n_active);
+    h->in_staging = true;
+    h->ns_valid = false;
+    invalidate_graphs(h);
+    return 0;
+}
+
+int sphgpu_set_rigid_callback(sphgpu_t h, sphgpu_rigid_fn fn, void* user) {
+    if (!h) return SPHGPU_EINVAL;
+    h->rigid_fn = fn;
+    h->rigid_user = user;
+    return 0;
+}
+
+int sphgpu_set_solid_state(sphgpu_t h, int solid_id, const SphRigidState* state) {
+    if (!h || !state) return SPHGPU_EINVAL;
+    const int di = dyn_index(h, solid_id);
+    if (di < 0) { h->err = "not a dynamic solid"; return SPHGPU_EINVAL; }
+    cudaSetDevice(h->device);
+    CK(cudaStreamSynchronize(h->stream));
+    memcpy(h->h_rstate + 25 * di, state, sizeof(SphRigidState));
+    return 0;
+}
+
+int sphgpu_get_solid_state(sphgpu_t h, int solid_id, SphRigidState* state) {
+    if (!h || !state) return SPHGPU_EINVAL;
+    const int di = dyn_index(h, solid_id);
+    if (di < 0) { h->err = "not a dynamic solid"; return SPHGPU_EINVAL; }
+    cudaSetDevice(h->device);
+    CK(cudaStreamSynchronize(h->stream));
+    memcpy(state, h->h_rstate + 25 * di, sizeof(SphRigidState));
+    return 0;
+}
+
+int sphgpu_get_solid_force(sphgpu_t h, int solid_id, double force[3], double torque[3]) {
+    if (!h || !force || !torque) return SPHGPU_EINVAL;
+    const int di = dyn_index(h, solid_id);
+    if (di < 0) { h->err = "not a dynamic solid"; return SPHGPU_EINVAL; }
+    cudaSetDevice(h->device);
+    CK(cudaStreamSynchronize(h->stream));
+    for (int c = 0; c < 3; ++c) {
+        force[c] = h->h_rout[6 * di + c];
+        torque[c] = h->h_rout[6 * di + 3 + c];
+    }
+    return 0;
+}
+
 int sphgpu_debug_set(sphgpu_t h, const char* key, int value) {
     if (!h || !key) return SPHGPU_EINVAL;
     std::string k(key);
@@ -2249,6 +2632,7 @@ long long sphgpu_read_pos(const char* path, float* out, long long max_floats, ch
 int sphgpu_save_snapshot(sphgpu_t h, const char* path) {
     if (!h || !path) return SPHGPU_EINVAL;
     if (h->nscenes > 1) { h->err = "snapshots are for single scenes"; return SPHGPU_EINVAL; }
+    if (h->R.nd) { h->err = "snapshots hold static walls only"; return SPHGPU_EINVAL; }
     cudaSetDevice(h->device);
     CK(cudaStreamSynchronize(h->stream));
     DevScene& d = h->d;

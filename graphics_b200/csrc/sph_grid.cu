@@ -349,6 +349,10 @@ void launch_count_active(const DevScene& s, const GridGeom& g, cudaStream_t st) 
     k_merge_starts<<<nblk(g.nkeys + 1, NT), NT, 0, st>>>(s, g.nkeys);
 }
 
+void launch_merge_starts(const DevScene& s, const GridGeom& g, cudaStream_t st) {
+    k_merge_starts<<<nblk(g.nkeys + 1, NT), NT, 0, st>>>(s, g.nkeys);
+}
+
 template <int BS>
 static void launch_build_bs(const DevScene& s, const GridGeom& g, const SolverConst& c, int mode, int n_max,
                             cudaStream_t st) {

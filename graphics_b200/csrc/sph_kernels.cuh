@@ -66,6 +66,11 @@ struct DevScene {
                         // DFSPH force kernel gathers (position and rho from the list
                         // build, velocity from the reorder / divergence sweep)
     float4* bpv;        // 2 per boundary particle: {(x,y,z,volume), velocity}
+    float4* bpf;        // the record the DFSPH force kernel gathers for a boundary
+                        // particle: {(x,y,z,volume), singleVelocity + velocity}
+                        // (DFSPH.cpp:1349); the same array as bpv unless a solid
+                        // is dynamic (bpv then keeps singleVelocity = 0, which is
+                        // what the Jacobi loops read, DFSPH.cpp:615,822)
     float4* acc;        // a_adv (DFSPH) / acceleration (WCSPH) / pressure accel (PCISPH, IISPH)
     float* kr;          // kappa/rho (DFSPH), pressure (WCSPH/PCISPH/IISPH)
     float* kappa;       // DFkappa of the last density iteration
@@ -116,6 +121,10 @@ struct DevScene {
     float4* bivs;       // (VF_gamma, VF_sphVolume, VF_alpha, kappa/gamma of the current loop)
     float4* bivo;       // (VF_kappa, VF_kappaV, VF_advectionVolume, VF_divergenceDeviation)
     int bstride;
+    // dynamic rigid solids: boundary force of the last DFSPH step and
+    // kerSumFromSelf per sorted boundary particle
+    float4* bforce;
+    float* bks;
     int cap_fluid;      // fluid array capacity
     // reductions
     double* partial;    // >= number of blocks of a particle launch
@@ -124,6 +133,30 @@ struct DevScene {
     // batch of independent scenes (nscenes > 1); scene index in pos.w
     int nscenes;
     BatchDev b;
+};
+
+// Dynamic rigid solids (DFSPH): the boundary in reference order (solid by
+// solid, each in insertion order), the per-solid rigid states, and the
+// scratch of the per-step boundary re-sort and force reduction.
+struct RigidDev {
+    float4* x0;       // [nb] body-frame position (dynamic solid) or world position
+                      // (static solid); w = kerSumFromSelf
+    float* vol;       // [nb] current volume
+    int* dyn;         // [nb] dense index of the particle's dynamic solid, -1 if static
+    int* sid;         // [nb] solid id
+    float* state;     // [nd * 25] transform[16] (OpenGL, column-major), com[3],
+                      // linear velocity[3], angular velocity[3]
+    float4* wpos;     // [nb] placed position (w = kerSumFromSelf)
+    float4* wvel;     // [nb] rigid velocity of the placed particle
+    int* key_in;      // [nb] sort input (reversed reference order) and output
+    int* val_in;
+    int* key_out;
+    int* val_out;
+    int* binv;        // [nb] reference index -> sorted slot
+    double* out;      // [nd * 6] joined force and torque of the last step
+    double* partial;  // per-block partial sums, 6 per block
+    unsigned* ticket; // [nd] last-block tickets
+    int nb, nd;
 };
 
 // step length of the particle's scene
@@ -209,6 +242,25 @@ void launch_iv_sweep_b(const DevScene& s, const SolverConst& c, int phase, int d
                        int max_it, unsigned long long cond_handle, int use_handle, int n_max, int bs, cudaStream_t st);
 // acce_presure, v += acce_presure dt, x += v dt into the staging arrays (carried: v_adv)
 void launch_iv_integrate(const DevScene& s, int n_max, cudaStream_t st);
+
+// ---- dynamic rigid solids (sph_rigid.cu) ----
+// updatePaticles for every dynamic solid, cell keys, stable key sort of the
+// whole boundary (within a cell: descending reference index), gather into
+// the sorted arrays and the boundary cell table
+void launch_rigid_place_sort(const DevScene& s, const RigidDev& R, const GridGeom& g, void* sort_tmp,
+                             size_t sort_bytes, int end_bit, cudaStream_t st);
+size_t rigid_sort_bytes(int nb, int end_bit);
+// prepareSolidPartWeight over the boundary alone: kerSumFromSelf and volume
+void launch_rigid_prepare(const DevScene& s, const RigidDev& R, const GridGeom& g, float dpart, float h2cut, int cap,
+                          cudaStream_t st);
+// updateSolidPartWeight: volume = 1 / (kerSumFromSelf + other solids' terms)
+void launch_rigid_volume(const DevScene& s, const RigidDev& R, const GridGeom& g, float dpart, float h2cut, int cap,
+                         cudaStream_t st);
+// boundary force of dynamic solid di (reference range [r0, r1)) and its
+// joined force / torque (FP64)
+void launch_rigid_force(const DevScene& s, const RigidDev& R, const SolverConst& c, const GridGeom& g, int r0, int r1,
+                        int di, cudaStream_t st);
+void launch_merge_starts(const DevScene& s, const GridGeom& g, cudaStream_t st);
 
 // carried state of particles coming from another solver: cB = (0, rho), cA = cC = 0
 // (staging: rho = the phase's rest density)

@@ -106,6 +106,49 @@ def dam_break(counts, r, box, seed=0, jitter=0.1, layers=2, rho0=1000.0):
                  meta=dict(kind="dam_break", counts=tuple(counts), box=tuple(box), seed=seed))
 
 
+def box_surface(half, d):
+    """Boundary particles on the surface of the box [-half, half] (body
+    frame, float32): a lattice of n_a + 1 points per axis with n_a =
+    round(2 half_a / d) intervals, the points with an extreme index on some
+    axis -- one layer, as SphWithIO::makeCubeSampleParts samples a cube's
+    surface (SphWithIO.cpp:489-522)."""
+    n = [max(1, int(round(2.0 * half[a] / d))) for a in range(3)]
+    ax = [np.arange(n[a] + 1) for a in range(3)]
+    zz, yy, xx = np.meshgrid(ax[2], ax[1], ax[0], indexing="ij")
+    xx, yy, zz = xx.ravel(), yy.ravel(), zz.ravel()
+    surf = (xx == 0) | (xx == n[0]) | (yy == 0) | (yy == n[1]) | (zz == 0) | (zz == n[2])
+    pos = np.stack([-half[0] + xx[surf] * (2.0 * half[0] / n[0]),
+                    -half[1] + yy[surf] * (2.0 * half[1] / n[1]),
+                    -half[2] + zz[surf] * (2.0 * half[2] / n[2])], axis=1)
+    return pos.astype(np.float32)
+
+
+def floating_box(counts, r, box, body_half, body_center, seed=0, jitter=0.1, layers=2, rho0=1000.0):
+    """A walled tank whose lower part holds a fluid block of counts=(nx,ny,nz)
+    particles, with a box-shaped rigid body (one surface layer of boundary
+    particles, solid id 1; the walls are solid 0) at body_center; fluid
+    particles closer than d to the body's inside are left out.  The body's
+    body-frame particles and its placement are in meta["bodies"]."""
+    d = 2.0 * r
+    fluid = lattice_block(counts, r, jitter=jitter, seed=seed)
+    c = np.asarray(body_center, dtype=np.float64)
+    hb = np.asarray(body_half, dtype=np.float64)
+    keep = np.any(np.abs(fluid.astype(np.float64) - c) > hb + d, axis=1)
+    fluid = np.ascontiguousarray(fluid[keep])
+    walls = wall_shell(box, r, layers=layers)
+    inner = box_surface(body_half, d)
+    body = (inner + np.asarray(body_center, dtype=np.float32)).astype(np.float32)
+    margin = (layers + 0.5) * d
+    smin = tuple(float(-margin) for _ in range(3))
+    smax = tuple(float(box[a] + margin) for a in range(3))
+    sid = np.concatenate([np.zeros(len(walls), np.int32), np.ones(len(body), np.int32)])
+    return Scene(fluid_pos=fluid, fluid_vel=np.zeros_like(fluid), boundary_pos=np.concatenate([walls, body]), r=r,
+                 space_min=smin, space_max=smax, rho0=rho0, rho0_phases=(rho0,),
+                 meta=dict(kind="floating_box", counts=tuple(counts), box=tuple(box), seed=seed, solid_id=sid,
+                           bodies=[dict(solid_id=1, inner=inner, center=tuple(float(x) for x in body_center),
+                                        half=tuple(float(x) for x in body_half))]))
+
+
 def rayleigh_taylor(counts, r, box, seed=0, jitter=0.1, layers=2, rho_heavy=3000.0, rho_light=1000.0,
                     amplitude=0.02):
     """Two-phase column filling the box: phase 0 (light) below the interface

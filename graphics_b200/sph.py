@@ -212,8 +212,44 @@ class GpuScene:
         g.params, g.nb = p, int(hdr[3])
         return g
 
+    # -- dynamic rigid solids --
+    def set_solid_dynamic(self, solid_id, inner, state):
+        """Make solid `solid_id` a dynamic rigid body with body-frame
+        particle positions `inner` and a 25-value initial state
+        (sphgpu_set_solid_dynamic)."""
+        from .rigid import state_struct
+        inner = np.ascontiguousarray(inner, dtype=np.float32)
+        st = state_struct(state)
+        self._check(self.lib.sphgpu_set_solid_dynamic(self.h, int(solid_id), _fptr(inner), C.byref(st)),
+                    "set_solid_dynamic")
+
+    def set_rigid_world(self, world):
+        """Drive the dynamic solids with `world` (graphics_b200.rigid.RigidWorld
+        or any object with its gpu_callback()); None removes it."""
+        self._rigid_cb = None if world is None else world.gpu_callback()
+        fn = self._rigid_cb if self._rigid_cb is not None else _lib.RIGID_FN()
+        self._check(self.lib.sphgpu_set_rigid_callback(self.h, fn, None), "set_rigid_callback")
+
+    def set_solid_state(self, solid_id, state):
+        from .rigid import state_struct
+        st = state_struct(state)
+        self._check(self.lib.sphgpu_set_solid_state(self.h, int(solid_id), C.byref(st)), "set_solid_state")
+
+    def get_solid_state(self, solid_id):
+        from .rigid import state_array
+        st = _lib.SphRigidState()
+        self._check(self.lib.sphgpu_get_solid_state(self.h, int(solid_id), C.byref(st)), "get_solid_state")
+        return state_array(st)
+
+    def get_solid_force(self, solid_id):
+        """(force[3], torque[3]) of the last DFSPH step (rigidForceJoin)."""
+        f = (C.c_double * 3)()
+        t = (C.c_double * 3)()
+        self._check(self.lib.sphgpu_get_solid_force(self.h, int(solid_id), f, t), "get_solid_force")
+        return np.array(f[:]), np.array(t[:])
+
     def get_boundary(self, field):
-        comps = 3 if field == "position" else 1
+        comps = 3 if field in ("position", "velocity", "force") else 1
         out = np.zeros(max(self.nb, 1) * comps, dtype=np.float32)
         m = self._check(self.lib.sphgpu_get_boundary(self.h, field.encode(), _fptr(out)), "get_boundary")
         return out[:m * comps].reshape(m, comps) if comps > 1 else out[:m]
@@ -353,10 +389,11 @@ def read_pos(path):
 
 
 def scene_to_gpu(scene, device=0, max_fluid=None, **params):
-    """GpuScene holding a graphics_b200.scene.Scene (walls as one static solid)."""
+    """GpuScene holding a graphics_b200.scene.Scene (walls as one static
+    solid, or one per scene.meta["solid_id"] value)."""
     p = params_for_scene(scene, **params)
     g = GpuScene(p, max_fluid or scene.n_fluid, device=device)
-    g.set_boundary(scene.boundary_pos)
+    g.set_boundary(scene.boundary_pos, scene.meta.get("solid_id"))
     if scene.phase is None:
         g.add_fluid(scene.fluid_pos, scene.fluid_vel, rho0=scene.rho0)
     else:

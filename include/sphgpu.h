@@ -55,6 +55,7 @@ extern "C" {
 #define SPHGPU_STATUS_NEIGHBOUR_OVERFLOW 8u
 #define SPHGPU_STATUS_OUT_OF_DOMAIN 16u
 #define SPHGPU_STATUS_ZERO_DISTANCE 32u
+#define SPHGPU_STATUS_SOLID_OUTSIDE 64u  /* a dynamic solid's particle left the grid */
 
 typedef struct sphgpu_scene* sphgpu_t;
 
@@ -202,8 +203,11 @@ int sphgpu_step_host(sphgpu_t h, int solver, const float* xyz, const float* vel,
 int sphgpu_get_fluid(sphgpu_t h, const char* field, float* out);
 int sphgpu_set_fluid(sphgpu_t h, const char* field, const float* in);
 /* Boundary fields in reference order (solid by solid): "position" (n*3),
- * "volume"; after an IISph step also "VF_gamma","VF_sphVolume","VF_alpha",
- * "VF_kappa","VF_kappaV","VF_advectionVolume","VF_divergenceDeviation". */
+ * "volume"; with a dynamic solid also "velocity" (n*3, the rigid velocity
+ * updatePaticles gives), "force" (n*3, the last DFSPH step's boundary force)
+ * and "kerSumFromSelf"; after an IISph step also "VF_gamma","VF_sphVolume",
+ * "VF_alpha","VF_kappa","VF_kappaV","VF_advectionVolume",
+ * "VF_divergenceDeviation". */
 int sphgpu_get_boundary(sphgpu_t h, const char* field, float* out);
 
 /* Particle output in the reference's .pos format (write_fluid_particles,
@@ -232,12 +236,66 @@ long long sphgpu_read_pos(const char* path, float* out, long long max_floats, ch
 int sphgpu_save_snapshot(sphgpu_t h, const char* path);
 int sphgpu_load_snapshot(const char* path, int device, sphgpu_t* out);
 
+/* Dynamic rigid solids (DFSPH).  The reference couples rigid bodies to the
+ * fluid through Bullet (SphWithBullet::updateSolids, SphWithBullet.cpp:
+ * 180-224, called from DFSPH::sphStep, DFSPH.cpp:54): each step accumulates a
+ * force on every boundary particle (DFSPH.cpp:681-691, 723-737, 1334-1359),
+ * joins it per dynamic solid into a force and a torque about the centre of
+ * mass (SphSolid::rigidForceJoin, SphBase.cpp:131-143), lets Bullet advance
+ * the bodies, and moves the boundary particles with the new transforms
+ * (SphSolid::updatePaticles, SphBase.cpp:95-128) before the neighbour
+ * search.  Here the per-particle work runs on the device; the rigid-body
+ * world stays with the caller and exchanges one force, torque and state per
+ * solid and step. */
+
+/* The state Bullet reports for a rigid body (SphSolid::updatePaticles,
+ * SphWithBullet.cpp:302-317). */
+typedef struct SphRigidState {
+    float transform[16];       /* btTransform::getOpenGLMatrix: column-major, [12..14] = origin */
+    float center_of_mass[3];   /* btRigidBody::getCenterOfMassPosition */
+    float linear_velocity[3];
+    float angular_velocity[3];
+} SphRigidState;
+
+/* The rigid-body world's step (applyCentralForce / applyTorque /
+ * stepSimulation, SphWithBullet.cpp:185-210): called once per DFSPH step,
+ * after the density loop and before the neighbour search, on the thread that
+ * called sphgpu_step, with each dynamic solid's joined force and torque (3
+ * FP64 values per solid; solids in the order they were made dynamic) and the
+ * step length.  It advances the bodies and writes their new states into
+ * states[0 .. nsolids-1], which hold the current ones on entry.  A nonzero
+ * return makes the step call fail with SPHGPU_EINVAL once the step is done. */
+typedef int (*sphgpu_rigid_fn)(void* user, int nsolids, const int* solid_ids, const double* force,
+                               const double* torque, double dt, SphRigidState* states);
+
+/* Make solid `solid_id` (as given to sphgpu_set_boundary) a dynamic rigid
+ * body (SphSolid(dynamic = true, RIGIDBODY), SphBase.h:326-331): inner_xyz =
+ * the body-frame positions of its particles (SphSolid::innerPositions), 3
+ * floats per particle in the order set_boundary received them; state = its
+ * initial state.  As SphWithBullet::addSolid does (SphWithBullet.cpp:
+ * 101-136), the particles are placed at once and every boundary particle's
+ * kerSumFromSelf and volume recomputed (prepareSolidPartWeight).  Single
+ * scenes and the DFSPH solver. */
+int sphgpu_set_solid_dynamic(sphgpu_t h, int solid_id, const float* inner_xyz, const SphRigidState* state);
+/* fn = NULL removes the callback; the bodies then keep the state last set
+ * with sphgpu_set_solid_state, which moves the particles at the next step's
+ * updateSolids point (or the next "neighbourSearch" stage). */
+int sphgpu_set_rigid_callback(sphgpu_t h, sphgpu_rigid_fn fn, void* user);
+int sphgpu_set_solid_state(sphgpu_t h, int solid_id, const SphRigidState* state);
+int sphgpu_get_solid_state(sphgpu_t h, int solid_id, SphRigidState* state);
+/* rigidForceJoin of the last DFSPH step (or "DF_constantDensitySolverSecond"
+ * stage): the solid's total force and its torque about the centre of mass of
+ * its state at that step, summed in FP64. */
+int sphgpu_get_solid_force(sphgpu_t h, int solid_id, double force[3], double torque[3]);
+
 /* Stage-level entry points (parity tests run "given state S, call stage X"):
  *   "neighbourSearch"                 grid + neighbour lists (+ rho/alpha)
  *   "DF_constantDensitySolverFirst"   rho, alpha            (DFSPH.cpp:84-193)
  *   "DF_forceExceptPressure"          a_adv                 (DFSPH.cpp:1419-1475)
  *   "DF_constantDensitySolverSecond"  forces+density loop+integrate (:195-738)
  *   "DF_divergenceFreeSolver"         divergence loop       (:740-1024)
+ *   "updateSolids"                    the rigid callback on the last forces
+ *                                     (SphWithBullet.cpp:180-224)
  *   "wc_computePressure", "wc_computeForce"                 (WcSph.cpp:99-462)
  *   IISph: "VF_prepareAttribute" (neighbour lists of fluid and boundary
  *   particles, sphDensity, gamma, sphVolume, alpha; IISph.cpp:100-545),

@@ -9,8 +9,9 @@ the GPU machines; the built libraries travel there instead):
    the reference still hold.
 2. Augment the *copy* of SphBase.h with the particle / threshold members that
    the solver sources use but this revision of SphBase.h does not declare
-   (DFSPH.cpp, IISph_M.cpp and WcSph.cpp come from a later revision), a
-   `friend class RefHarness;` line, and an #ifdef around the real_t typedef.
+   (DFSPH.cpp, IISph_M.cpp and WcSph.cpp come from a later revision),
+   `friend class RefHarness;` / `friend class SphWithIO;` lines, and an
+   #ifdef around the real_t typedef.
    Each edit is inserted at a fixed anchor (AUGMENT); nothing else changes.
 3. Compile SphBase.cpp + one solver .cpp + oracle/refshim/ref_harness.cpp into
    one shared library per solver (DFSPH.h, IISph.h and IISph_M.h share the
@@ -58,6 +59,10 @@ AUGMENT = [
     # the oracle harness class reads private members (mg_NS, ker_* and
     # ker_update_numbers, SphBase.h:680-800)
     ("class SphBase{\n\npublic:\n", "    friend class RefHarness;\n", "after_anchor"),
+    # the test harness's updateSolids stand-in (refshim/SphWithIO.h) moves a
+    # dynamic solid with SphSolid::updatePaticles(com, transform, v, w), a
+    # protected member (SphBase.h:344-346)
+    ("class SphSolid : public SphObject  {\npublic:\n", "    friend class SphWithIO;\n", "after_anchor"),
     # the precision switch the reference describes at SphBase.h:37-40
     ("typedef float real_t;\n",
      "#ifdef REF_REAL_DOUBLE\ntypedef double real_t;\n#else\n", "wrap_typedef"),
@@ -149,7 +154,8 @@ def main():
         for real, suffix in (("float", ""), ("double", "_f64")):
             so = os.path.join(OUT, "libref_%s%s.so" % (tag, suffix))
             deps = [os.path.join(SRC, cpp), os.path.join(SRC, "SphBase.cpp"),
-                    os.path.join(SHIM, "ref_harness.cpp"), os.path.join(SRC, "SphBase.h")]
+                    os.path.join(SHIM, "ref_harness.cpp"), os.path.join(SHIM, "SphWithIO.h"),
+                    os.path.join(SRC, "SphBase.h")]
             if os.path.exists(so) and all(os.path.getmtime(so) >= os.path.getmtime(d) for d in deps):
                 continue
             cmd = ["g++", "-std=c++17", "-O3", "-fopenmp", "-fPIC", "-shared", "-w",
@@ -174,7 +180,8 @@ def main():
         exe = os.path.join(OUT, "dropin_" + tag)
         deps = [os.path.join(SHIM, "dropin_main.cpp"), os.path.join(ROOT, "include", "sphgpu_solver.hpp"),
                 os.path.join(ROOT, "include", "sphgpu.h"), os.path.join(SRC, cpp),
-                os.path.join(SRC, "SphBase.cpp"), os.path.join(SRC, "SphBase.h"), lib]
+                os.path.join(SRC, "SphBase.cpp"), os.path.join(SRC, "SphBase.h"), os.path.join(SHIM, "SphWithIO.h"),
+                lib]
         if not (os.path.exists(exe) and all(os.path.getmtime(exe) >= os.path.getmtime(d) for d in deps)):
             jobs.append((exe, ["g++", "-std=c++17", "-O2", "-fopenmp", "-w", "-DREF_SOLVER_HEADER=\"%s.h\"" % cls,
                                "-DREF_SOLVER_CLASS=" + cls, "-DREF_SPHGPU_SOLVER=SPHGPU_" + tag.upper(),

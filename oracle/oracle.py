@@ -328,14 +328,58 @@ class Oracle:
         """OpenMP threads of the compiled reference (process-wide)."""
         self.lib.ref_set_threads(int(n))
 
+    # -- dynamic rigid solids (SphWithBullet::updateSolids with a host world) --
+    def _rigid_sigs(self):
+        vp, dp, i = C.c_void_p, C.POINTER(C.c_double), C.c_int
+        pre = "orc_" if self.kind == "port" else "ref_"
+        for name, res, args in (("set_solid_dynamic", i, [vp, i, dp, dp]),
+                                ("set_rigid_callback", None, [vp, vp, vp]),
+                                ("rigid_force_join", i, [vp, i, dp, dp, dp]),
+                                ("rigid_error", i, [vp])):
+            f = getattr(self.lib, pre + name)
+            f.restype, f.argtypes = res, args
+
+    def set_solid_dynamic(self, k, inner, state):
+        """Solid k becomes a dynamic rigid body: body-frame positions inner
+        (n, 3), 25-value state (transform[16], com, v, w)."""
+        self._rigid_sigs()
+        inner = np.ascontiguousarray(inner, dtype=np.float64)
+        st = np.ascontiguousarray(state, dtype=np.float64)
+        if self._f("set_solid_dynamic")(self.h, int(k), self._dp(inner), self._dp(st)) != 0:
+            raise ValueError("set_solid_dynamic")
+
+    def set_rigid_world(self, world):
+        """Drive the dynamic solids with a graphics_b200.rigid.RigidWorld."""
+        self._rigid_sigs()
+        self._rigid_cb = world.double_callback()
+        self._f("set_rigid_callback")(self.h, C.cast(self._rigid_cb, C.c_void_p), None)
+
+    def rigid_force_join(self, k, com):
+        self._rigid_sigs()
+        c = np.ascontiguousarray(com, dtype=np.float64)
+        f, t = np.zeros(3), np.zeros(3)
+        self._f("rigid_force_join")(self.h, int(k), self._dp(c), self._dp(f), self._dp(t))
+        return f, t
+
+    def rigid_error(self):
+        self._rigid_sigs()
+        return self._f("rigid_error")(self.h)
+
 
 def make_scene_oracle(scene, kind="port", solver="dfsph", f64=False, visc_alpha=0.0, solid_visc=0.0, **kw):
     """Oracle holding `scene` (graphics_b200.scene.Scene): the walls are added
-    first as one static rigid solid (so its volumes come from boundary
-    neighbours only), then one fluid phase per rest density."""
+    first as static rigid solids (one, or one per scene.meta["solid_id"]
+    value; their volumes come from boundary neighbours only), then one fluid
+    phase per rest density."""
     p = default_params(scene, **kw)
     o = Oracle(p, kind=kind, solver=solver, f64=f64)
-    o.add_solid(scene.boundary_pos, scene.d, visc_alpha=solid_visc, rho0=scene.rho0, prepare=True)
+    sid = scene.meta.get("solid_id")
+    if sid is None:
+        o.add_solid(scene.boundary_pos, scene.d, visc_alpha=solid_visc, rho0=scene.rho0, prepare=True)
+    else:
+        # one solid per id, in id order (each addSolid prepares all solids)
+        for k in range(int(sid.max()) + 1):
+            o.add_solid(scene.boundary_pos[sid == k], scene.d, visc_alpha=solid_visc, rho0=scene.rho0, prepare=True)
     if scene.phase is None:
         o.add_fluid(scene.fluid_pos, scene.fluid_vel, d=scene.d, rho0=scene.rho0, visc_alpha=visc_alpha)
     else:

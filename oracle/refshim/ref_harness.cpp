@@ -74,6 +74,7 @@ public:
         if (s == "updateFluids") { updateFluids(); return 0; }
         if (s == "sphStep") { sphStep(); return 0; }
         if (s == "runOneStep") { runOneStep(); return 0; }
+        if (s == "updateSolids") { updateSolids(); return 0; }
 #if defined(REF_TAG_dfsph) || defined(REF_TAG_dfsph_capped)
         if (s == "DF_constantDensitySolverFirst") { DF_constantDensitySolverFirst(); return 0; }
         if (s == "DF_constantDensitySolverSecond") { DF_constantDensitySolverSecond(); return 0; }
@@ -327,6 +328,41 @@ public:
         }
         return 0;
     }
+    /* Dynamic rigid solid k (SphSolid::dynamic, SphBase.h:330) with body-frame
+     * positions inner (3n doubles, SphSolid::innerPositions) and initial
+     * state (25 doubles, see SphWithIO.h); placed at once, then
+     * prepareSolidPartWeight() recomputes every solid's kerSumFromSelf and
+     * volume, as SphWithBullet::addSolid does (SphWithBullet.cpp:131-135). */
+    static int ref_set_solid_dynamic_impl(void* hh, int k, const double* inner, const double* state) {
+        RefHarness* h = static_cast<RefHarness*>(hh);
+        if (k < 0 || k >= int(h->m_Solids.size())) return -1;
+        SphSolid& s = h->m_Solids[k];
+        s.dynamic = true;
+        s.type = SphSolid::RIGIDBODY;
+        s.innerPositions.resize(s.boundaryParticles.size());
+        for (size_t i = 0; i < s.innerPositions.size(); ++i)
+            s.innerPositions[i] = vec_t(real_t(inner[3 * i]), real_t(inner[3 * i + 1]), real_t(inner[3 * i + 2]));
+        h->setRigidState(k, state);
+        h->placeSolid(k);
+        h->prepareSolidPartWeight();
+        return 0;
+    }
+    static void ref_set_rigid_callback_impl(void* hh, void* fn, void* user) {
+        RefHarness* h = static_cast<RefHarness*>(hh);
+        h->rigid_fn = reinterpret_cast<RigidFn>(fn);
+        h->rigid_user = user;
+    }
+    static int ref_rigid_error_impl(void* hh) { return static_cast<RefHarness*>(hh)->rigid_err; }
+    /* SphSolid::rigidForceJoin of solid k about com (SphBase.cpp:131-143) */
+    static int ref_rigid_force_join_impl(void* hh, int k, const double* com, double* force, double* torque) {
+        RefHarness* h = static_cast<RefHarness*>(hh);
+        if (k < 0 || k >= int(h->m_Solids.size())) return -1;
+        vec_t f;
+        vec3_t t;
+        h->m_Solids[k].rigidForceJoin(vec_t(real_t(com[0]), real_t(com[1]), real_t(com[2])), f, t);
+        for (int c = 0; c < 3; ++c) { force[c] = double(f[c]); torque[c] = double(t[c]); }
+        return 0;
+    }
     static double ref_kernel_impl(void* hh, int grad, double r) {
         RefHarness* h = static_cast<RefHarness*>(hh);
         return grad ? double(h->ker_W_grad(real_t(r))) : double(h->ker_W(real_t(r)));
@@ -367,4 +403,12 @@ int ref_set_solid(void* hh, int k, const char* field, const double* in) { return
  * (SphBase.cpp:242-243); this overrides it (1 thread makes the racy loops of
  * IISph_M.cpp:315-351 deterministic) */
 void ref_set_threads(int n) { omp_set_num_threads(n); }
+int ref_set_solid_dynamic(void* hh, int k, const double* inner, const double* state) {
+    return RefHarness::ref_set_solid_dynamic_impl(hh, k, inner, state);
+}
+void ref_set_rigid_callback(void* hh, void* fn, void* user) { RefHarness::ref_set_rigid_callback_impl(hh, fn, user); }
+int ref_rigid_error(void* hh) { return RefHarness::ref_rigid_error_impl(hh); }
+int ref_rigid_force_join(void* hh, int k, const double* com, double* force, double* torque) {
+    return RefHarness::ref_rigid_force_join_impl(hh, k, com, force, torque);
+}
 }  // extern "C"

@@ -114,6 +114,15 @@ typedef struct {
     int n, rigid;
     real d, visc_alpha, rho0;
     real *pos, *vel, *svel, *volume, *kerSumFromSelf, *force;
+    /* dynamic rigid solid (SphSolid::dynamic, SphBase.h:330): body-frame
+     * positions (innerPositions, SphBase.h:336) and the rigid state the
+     * rigid-body world last reported: OpenGL column-major transform (float,
+     * as btTransform::getOpenGLMatrix writes it), centre of mass, linear and
+     * angular velocity (SphWithBullet.cpp:302-317) */
+    int dynamic;
+    real* inner;
+    float T[16];
+    real com[3], lin[3], ang[3];
     /* IISph (volume form) per-particle state */
     real *mass, *VF_gamma, *VF_sphVolume, *VF_advVol, *VF_alpha, *VF_alpha2, *VF_kappa, *VF_kappaV, *VF_divdev;
     int *nnum; PIdx *nidx; real *ndis;
@@ -143,6 +152,14 @@ typedef struct {
     int pci_init;
     int it_iv_div, it_iv_cv;
     double err_iv_div, err_iv_cv;
+    /* the rigid-body world that stands in for Bullet (SphWithBullet::
+     * updateSolids, SphWithBullet.cpp:180-224): per dynamic solid it receives
+     * the joined force and torque and returns the new state, 25 doubles
+     * (transform[16], com[3], linear[3], angular[3]); nonzero = failure */
+    int (*rigid_fn)(void* user, int nsolids, const int* ids, const double* force, const double* torque,
+                    double dt, double* states);
+    void* rigid_user;
+    int rigid_err;
 } OrcScene;
 
 /* ---------------- kernels, SphBase.h:808-889 ---------------- */
@@ -449,6 +466,77 @@ static void df_first(OrcScene* s) {
     }
 }
 
+/* Boundary reaction of the viscosity term, `rb.force -= tmp` of
+ * DF_fluidBoundExceptPressure (DFSPH.cpp:1334-1359), for fluid phase k.  The
+ * reference adds it inside its OpenMP particle loop without synchronisation,
+ * so with several threads its sums depend on the schedule; this serial pass
+ * gives the one-thread order (particle, then neighbour) with the same
+ * per-pair arithmetic as df_force_except_pressure. */
+static void df_visc_reaction(OrcScene* s, int k) {
+    const int cap = s->P.cap;
+    OrcFluid* F = &s->F[k];
+    real rho0 = F->rho0;
+    real hs = (real)s->P.smoothRadius_h, nu = (real)s->P.nu;
+    for (int i = 0; i < F->n; ++i) {
+        const real* pa = F->pos + 3 * (long)i;
+        const real* va = F->vel + 3 * (long)i;
+        const PIdx* L = F->nidx + (long)i * cap;
+        const real* D = F->ndis + (long)i * cap;
+        int n = F->nnum[i];
+        for (int j = 0; j < n; ++j) {
+            if (L[j].t <= 0) continue;
+            real dis = D[j];
+            if (dis == 0) continue;
+            OrcSolid* Sb = &s->S[L[j].t - 1];
+            const real* pb = Sb->pos + 3 * (long)L[j].i;
+            const real* sv = Sb->svel + 3 * (long)L[j].i;
+            const real* bv = Sb->vel + 3 * (long)L[j].i;
+            real* fb = Sb->force + 3 * (long)L[j].i;
+            real xab[3] = {pa[0] - pb[0], pa[1] - pb[1], pa[2] - pb[2]};
+            real vol = Sb->volume[L[j].i];
+            real s1 = -ker_W_grad(s, dis) / dis;
+            real pro = (va[0] - sv[0] - bv[0]) * xab[0] + (va[1] - sv[1] - bv[1]) * xab[1] +
+                       (va[2] - sv[2] - bv[2]) * xab[2];
+            if (pro < 0) {
+                real den = dis * dis + (real)0.01 * hs * hs;
+                for (int c = 0; c < 3; ++c) {
+                    real t = xab[c] * s1;
+                    t = t * pro; t = t / den; t = t * (rho0 * vol); t = t / F->density[i]; t = t * 10; t = t * nu;
+                    fb[c] = fb[c] - t;
+                }
+            }
+        }
+    }
+}
+
+/* Boundary reaction of one constant-density iteration, `p_b.force += acc_p`
+ * (DFSPH.cpp:681-691), in the reference's one-thread order; acc_p is the
+ * term the fluid particle's v_adv update subtracts (same arithmetic). */
+static void df_pressure_reaction(OrcScene* s, OrcFluid* F) {
+    const int cap = s->P.cap;
+    real rho0 = F->rho0;
+    for (int i = 0; i < F->n; ++i) {
+        const real* pa = F->pos + 3 * (long)i;
+        real ka = F->DFkappa[i] / F->density[i];
+        const PIdx* L = F->nidx + (long)i * cap;
+        const real* D = F->ndis + (long)i * cap;
+        int n = F->nnum[i];
+        for (int j = 0; j < n; ++j) {
+            if (L[j].t <= 0) continue;
+            OrcSolid* Sb = &s->S[L[j].t - 1];
+            const real* pb = Sb->pos + 3 * (long)L[j].i;
+            real* fb = Sb->force + 3 * (long)L[j].i;
+            real vol = Sb->volume[L[j].i];
+            real gs = -ker_W_grad(s, D[j]);
+            for (int c = 0; c < 3; ++c) {
+                real g = (pa[c] - pb[c]) * (gs / D[j]);
+                real accp = g * rho0 * vol * ka;
+                fb[c] += accp;
+            }
+        }
+    }
+}
+
 /* DF_forceExceptPressure + ii_fluidPartForceExceptPressure_fsame/_fdiff and
  * DF_fluidBoundExceptPressure, DFSPH.cpp:1246-1359, 1419-1475 */
 static void df_force_except_pressure(OrcScene* s) {
@@ -519,6 +607,7 @@ static void df_force_except_pressure(OrcScene* s) {
                 }
             }
         }
+        df_visc_reaction(s, k);
     }
     s->zeroDis += zero;
 }
@@ -610,6 +699,7 @@ static void df_second(OrcScene* s) {
                     }
                 }
             }
+            df_pressure_reaction(s, F);
             if (s->P.float_err) {
                 real fs = (real)sum;
                 errorRate = ((fs / num) - rho0) / rho0;
@@ -628,6 +718,15 @@ static void df_second(OrcScene* s) {
         remove_outside(s, F);
         if (it > s->it_density) s->it_density = it;
         if (errorRate > s->err_density || k == 0) s->err_density = errorRate;
+    }
+    /* acceleration-per-density sums -> forces, with the mass of phase 0
+     * (DFSPH.cpp:723-737) */
+    if (s->nf > 0) {
+        real fm0 = v0 * s->F[0].rho0;
+        for (int k = 0; k < s->ns; ++k) {
+            OrcSolid* S = &s->S[k];
+            for (long i = 0; i < 3L * S->n; ++i) S->force[i] = S->force[i] * fm0;
+        }
     }
 }
 
@@ -742,6 +841,84 @@ static void cfl_dt(OrcScene* s) {
     s->P.dt = (double)(float)dt;
 }
 
+/* SphSolid::updatePaticles(centerOfMass, tranform, linearVelocity,
+ * angularVelocity), SphBase.cpp:95-128 (3-D branch): position = transform *
+ * innerPosition with the homogeneous divide, velocity = v + w x (x - com). */
+static void solid_update_particles(OrcSolid* S) {
+    const float* t = S->T;
+    for (int i = 0; i < S->n; ++i) {
+        const real* p0 = S->inner + 3 * (long)i;
+        real* bp = S->pos + 3 * (long)i;
+        real* bv = S->vel + 3 * (long)i;
+        bp[0] = t[0] * p0[0] + t[4] * p0[1] + t[8] * p0[2] + t[12];
+        bp[1] = t[1] * p0[0] + t[5] * p0[1] + t[9] * p0[2] + t[13];
+        bp[2] = t[2] * p0[0] + t[6] * p0[1] + t[10] * p0[2] + t[14];
+        real alpha = t[3] * p0[0] + t[7] * p0[1] + t[11] * p0[2] + t[15];
+        bp[0] /= alpha; bp[1] /= alpha; bp[2] /= alpha;
+        real r[3] = {bp[0] - S->com[0], bp[1] - S->com[1], bp[2] - S->com[2]};
+        /* vec3::cross, Vec23.h:142-143 */
+        real w[3] = {S->ang[1] * r[2] - S->ang[2] * r[1], S->ang[2] * r[0] - S->ang[0] * r[2],
+                     S->ang[0] * r[1] - S->ang[1] * r[0]};
+        bv[0] = S->lin[0] + w[0]; bv[1] = S->lin[1] + w[1]; bv[2] = S->lin[2] + w[2];
+    }
+}
+
+/* SphSolid::rigidForceJoin, SphBase.cpp:131-143: total force and the torque
+ * about the centre of mass, summed in particle order. */
+static void rigid_force_join(const OrcSolid* S, const real* com, real* tf, real* tt) {
+    tf[0] = tf[1] = tf[2] = 0; tt[0] = tt[1] = tt[2] = 0;
+    for (int i = 0; i < S->n; ++i) {
+        const real* f = S->force + 3 * (long)i;
+        const real* x = S->pos + 3 * (long)i;
+        real r[3] = {x[0] - com[0], x[1] - com[1], x[2] - com[2]};
+        tf[0] += f[0]; tf[1] += f[1]; tf[2] += f[2];
+        tt[0] += r[1] * f[2] - r[2] * f[1];
+        tt[1] += r[2] * f[0] - r[0] * f[2];
+        tt[2] += r[0] * f[1] - r[1] * f[0];
+    }
+}
+
+static void solid_set_state(OrcSolid* S, const double* st) {
+    for (int c = 0; c < 16; ++c) S->T[c] = (float)st[c];
+    for (int c = 0; c < 3; ++c) {
+        S->com[c] = (real)(float)st[16 + c];
+        S->lin[c] = (real)(float)st[19 + c];
+        S->ang[c] = (real)(float)st[22 + c];
+    }
+}
+
+/* SphWithBullet::updateSolids, SphWithBullet.cpp:180-224, with the rigid-body
+ * world behind s->rigid_fn: join each dynamic solid's force and torque about
+ * its current centre of mass, let the world advance the bodies by dt, then
+ * move the boundary particles with the returned states.  Without a world the
+ * bodies keep their states. */
+static void update_solids(OrcScene* s) {
+    int ids[16], nd = 0;
+    double force[48], torque[48], states[16 * 25];
+    for (int k = 0; k < s->ns; ++k) {
+        OrcSolid* S = &s->S[k];
+        if (!S->dynamic) continue;
+        real tf[3], tt[3];
+        rigid_force_join(S, S->com, tf, tt);
+        for (int c = 0; c < 3; ++c) { force[3 * nd + c] = tf[c]; torque[3 * nd + c] = tt[c]; }
+        for (int c = 0; c < 16; ++c) states[25 * nd + c] = S->T[c];
+        for (int c = 0; c < 3; ++c) {
+            states[25 * nd + 16 + c] = S->com[c];
+            states[25 * nd + 19 + c] = S->lin[c];
+            states[25 * nd + 22 + c] = S->ang[c];
+        }
+        ids[nd++] = k;
+    }
+    if (!nd) return;
+    if (s->rigid_fn && s->rigid_fn(s->rigid_user, nd, ids, force, torque, (double)(real)s->P.dt, states))
+        s->rigid_err = 1;
+    for (int j = 0; j < nd; ++j) {
+        OrcSolid* S = &s->S[ids[j]];
+        solid_set_state(S, states + 25 * j);
+        solid_update_particles(S);
+    }
+}
+
 /* DFSPH::sphStep, DFSPH.cpp:45-62, followed by runOneStep's bookkeeping
  * (SphBase.cpp:348-354) */
 static void df_step(OrcScene* s) {
@@ -752,6 +929,7 @@ static void df_step(OrcScene* s) {
     }
     if (s->P.cfl) cfl_dt(s);
     df_second(s);
+    update_solids(s);
     neighbour_search(s, 1, 1, 0);
     update_solid_part_weight(s);
     df_first(s);
@@ -947,6 +1125,7 @@ void orc_destroy(void* h) {
     for (int k = 0; k < s->ns; ++k) {
         OrcSolid* S = &s->S[k];
         free(S->pos); free(S->vel); free(S->svel); free(S->volume); free(S->kerSumFromSelf); free(S->force);
+        free(S->inner);
         free(S->mass); free(S->VF_gamma); free(S->VF_sphVolume); free(S->VF_advVol); free(S->VF_alpha);
         free(S->VF_alpha2); free(S->VF_kappa); free(S->VF_kappaV); free(S->VF_divdev);
         free(S->nnum); free(S->nidx); free(S->ndis); free(S->next);
@@ -974,6 +1153,43 @@ int orc_add_solid(void* h, int n, const double* xyz, double d, double visc_alpha
     if (prepare) prepare_solid_part_weight(s);
     return s->ns - 1;
 }
+
+/* Make solid k a dynamic rigid body (SphSolid(dynamic=true, RIGIDBODY),
+ * SphBase.h:326): inner = its body-frame particle positions (3n), state = 25
+ * doubles (transform[16] OpenGL column-major, com[3], linear[3],
+ * angular[3]).  As SphWithBullet::addSolid does (SphWithBullet.cpp:
+ * 131-135), the particles are placed at once and every solid's
+ * kerSumFromSelf and volume recomputed (prepareSolidPartWeight). */
+int orc_set_solid_dynamic(void* h, int k, const double* inner, const double* state) {
+    OrcScene* s = (OrcScene*)h;
+    if (k < 0 || k >= s->ns) return -1;
+    OrcSolid* S = &s->S[k];
+    if (!S->inner) ALLOC3(S->inner, S->n);
+    for (long i = 0; i < 3L * S->n; ++i) S->inner[i] = (real)inner[i];
+    S->dynamic = 1;
+    solid_set_state(S, state);
+    solid_update_particles(S);
+    prepare_solid_part_weight(s);
+    return 0;
+}
+
+void orc_set_rigid_callback(void* h, void* fn, void* user) {
+    OrcScene* s = (OrcScene*)h;
+    s->rigid_fn = (int (*)(void*, int, const int*, const double*, const double*, double, double*))fn;
+    s->rigid_user = user;
+}
+
+/* rigidForceJoin of solid k about com (3 doubles); returns 0 */
+int orc_rigid_force_join(void* h, int k, const double* com, double* force, double* torque) {
+    OrcScene* s = (OrcScene*)h;
+    if (k < 0 || k >= s->ns) return -1;
+    real c[3] = {(real)com[0], (real)com[1], (real)com[2]}, tf[3], tt[3];
+    rigid_force_join(&s->S[k], c, tf, tt);
+    for (int i = 0; i < 3; ++i) { force[i] = tf[i]; torque[i] = tt[i]; }
+    return 0;
+}
+
+int orc_rigid_error(void* h) { return ((OrcScene*)h)->rigid_err; }
 
 int orc_add_fluid(void* h, int n, const double* xyz, const double* vel, double d, double rho0,
                   double visc_alpha, double tension) {
@@ -1017,6 +1233,7 @@ int orc_stage(void* h, const char* name) {
     if (!strcmp(name, "DF_divergenceFreeSolver")) { df_divergence_free(s); return 0; }
     if (!strcmp(name, "DF_forceExceptPressure")) { df_force_except_pressure(s); return 0; }
     if (!strcmp(name, "df_step")) { df_step(s); return 0; }
+    if (!strcmp(name, "updateSolids")) { update_solids(s); return 0; }
     if (!strcmp(name, "cfl_dt")) { cfl_dt(s); return 0; }
     if (!strcmp(name, "wc_computePressure")) { wc_pressure(s); return 0; }
     if (!strcmp(name, "wc_computeForce")) { wc_force(s); return 0; }

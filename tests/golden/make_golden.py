@@ -24,6 +24,12 @@ oracle/_ref/) on small seeded scenes and records its outputs:
                     phases, one OpenMP thread (its error sums run under
                     `omp critical` in thread order, IISph.cpp:785,1437),
                     with the boundary particles' own loop state
+  rigid_dfsph.npz   DFSPH runOneStep x 5 with a dynamic rigid box in a
+                    tank (rigid_scene), one OpenMP thread (the boundary
+                    forces are summed without synchronisation inside the
+                    parallel loops, DFSPH.cpp:689,1357): the force and torque
+                    handed to the rigid-body world each step, the body's
+                    final state, particle positions and volumes
 Run in the build container (the reference tree must be present):
     python tests/golden/make_golden.py            # all fixtures
     python tests/golden/make_golden.py step_iisph # one of them
@@ -38,7 +44,8 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
-from graphics_b200.scene import Scene, rayleigh_taylor, small_dam_break  # noqa: E402
+from graphics_b200.rigid import RigidBody, RigidWorld  # noqa: E402
+from graphics_b200.scene import Scene, floating_box, rayleigh_taylor, small_dam_break  # noqa: E402
 from oracle import make_scene_oracle  # noqa: E402
 
 SCENE = dict(n=(12, 12, 12), r=0.025, seed=7)
@@ -87,6 +94,50 @@ MULTI_FIELDS = ("position", "velocity", "density", "presure")
 IV_FIELDS = ("position", "velocity", "sphDensity", "VF_gamma", "VF_sphVolume", "VF_alpha", "VF_kappa",
              "VF_kappaV", "VF_advectionVolume", "acce_presure")
 IV_SOLID_FIELDS = ("VF_gamma", "VF_sphVolume", "VF_alpha", "VF_kappa", "VF_kappaV")
+
+
+# a 0.2 m box of density 500 pushed down and spun, half in the fluid of a
+# 0.8 m tank (1,940 fluid particles, 3,904 wall and 98 body particles)
+RIGID = dict(counts=(16, 8, 16), r=0.025, box=(0.8, 0.8, 0.8), half=(0.1, 0.1, 0.1), center=(0.4, 0.38, 0.4),
+             seed=3, density=500.0, q=(np.cos(0.02), 0.6 * np.sin(0.02), 0.0, 0.8 * np.sin(0.02)),
+             v=(0.0, -0.2, 0.05), w=(0.5, 0.0, 0.3))
+RIGID_KW = dict(float_err=1, df_density_max_iter=1000000, nu=1e-3, dt=1e-3)
+RIGID_STEPS = 5
+
+
+def rigid_scene():
+    c = RIGID
+    return floating_box(c["counts"], c["r"], c["box"], c["half"], c["center"], seed=c["seed"])
+
+
+def rigid_world(sc):
+    """The rigid-body world holding the scene's box (solid 1)."""
+    c, b = RIGID, sc.meta["bodies"][0]
+    w = RigidWorld()
+    w.add(b["solid_id"], RigidBody.box(c["density"], b["half"], b["center"], q=c["q"], v=c["v"], w=c["w"]))
+    return w
+
+
+def make_rigid_dfsph():
+    sc = rigid_scene()
+    o = make_scene_oracle(sc, kind="reference", solver="dfsph", **RIGID_KW)
+    o.set_threads(1)
+    w = rigid_world(sc)
+    b = sc.meta["bodies"][0]
+    o.set_solid_dynamic(b["solid_id"], b["inner"], w.state(b["solid_id"]))
+    o.set_rigid_world(w)
+    for _ in range(RIGID_STEPS):
+        o.stage("runOneStep")
+    assert o.rigid_error() == 0
+    out = dict(force=np.array([f for _, f, _, _ in w.log])[:, 0], torque=np.array([t for _, _, t, _ in w.log])[:, 0],
+               dt=np.array([d for *_, d in w.log]), state=w.state(b["solid_id"]),
+               body_position=o.get_solid("position", 1).astype(np.float32),
+               body_velocity=o.get_solid("velocity", 1).astype(np.float32),
+               wall_volume=o.get_solid("volume", 0).astype(np.float32),
+               body_volume=o.get_solid("volume", 1).astype(np.float32),
+               position=o.get("position").astype(np.float32), velocity=o.get("velocity").astype(np.float32))
+    np.savez_compressed(os.path.join(HERE, "rigid_dfsph.npz"), **out)
+    o.close()
 
 
 def make_step_iisph():
@@ -155,6 +206,7 @@ def main():
                            for f in MULTI_FIELDS + ("dii", "aii", "rho_adv", "sum_dijpj", "acce_presure")})
     o.close()
     make_step_iisph()
+    make_rigid_dfsph()
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -20,7 +20,7 @@ def make_pair(scene=None, visc_alpha=0.0, boundary_visc=0.0, cap=48, **kw):
     gp = params_for_scene(scene, max_neighbours=cap, boundary_visc=boundary_visc,
                           **{k: v for k, v in p.items() if k not in ("float_err",)})
     g = GpuScene(gp, scene.n_fluid)
-    g.set_boundary(scene.boundary_pos)
+    g.set_boundary(scene.boundary_pos, scene.meta.get("solid_id"))
     if scene.phase is None:
         g.add_fluid(scene.fluid_pos, scene.fluid_vel, rho0=scene.rho0, visc_alpha=visc_alpha)
     else:
