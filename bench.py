@@ -84,7 +84,7 @@ def parse():
     ap.add_argument("--train-seeds", default="1,2", help="jitter seeds of the training runs")
     ap.add_argument("--train-steps", type=int, default=350, help="recorded plain steps per training seed")
     ap.add_argument("--train-every", type=int, default=175, help="record every n-th particle per step")
-    ap.add_argument("--workload", default="dam_break_1m", choices=["dam_break_1m", "batched_64"],
+    ap.add_argument("--workload", default="dam_break_1m", choices=["dam_break_1m", "batched_64", "floating_box_1m"],
                     help="dam_break_1m: the headline 1M-particle DFSPH dam break; batched_64: 64 independent "
                          "dam breaks of 10k-200k particles in one batch")
     ap.add_argument("--no-graphs", action="store_true",
@@ -635,6 +635,219 @@ def run_batched(args):
         dist.destroy_process_group()
 
 
+# Dynamic rigid body: the DFSPH step with a 0.4 m box of density 500
+# floating half submerged in a 1 m deep pool filling the 4 x 2 x 2 m tank
+# (200 x 50 x 100 fluid lattice, r = 0.01 m, ~995k fluid particles after the
+# box's volume is cleared; 2,402 body and ~180k wall particles), the host
+# rigid-body world (graphics_b200.rigid) in the loop every step.
+RIGID_BODY = dict(half=(0.2, 0.2, 0.2), center=(2.0, 1.0, 1.0), density=500.0,
+                  q=(float(np.cos(0.05)), 0.0, 0.0, float(np.sin(0.05))))
+# Algorithmic bytes per boundary particle (every wall and body particle) of
+# the per-step boundary kernels, and per body particle of the force kernel:
+#   rigid_place  : place (x0, dyn -> wpos, wvel, key, slot, count = 64 B),
+#                  scatter (key, slot, cell start -> tmp = 16 B), in-cell
+#                  rank and gather (tmp, key, cell range, wpos, wvel, vol,
+#                  sid -> bpos, bks, bpv, bpf, bgid, bsid, binv = 156 B);
+#                  plus 12 B per cell key (count clear, scan read + write)
+#   rigid_volume : bpos, bsid, bks, bgid in; volume into bpos, bpv, bpf and
+#                  the reference-order copy (44 B)
+#   rigid_force  : binv, bpf record in, force out (52 B)
+RIGID_ALG = {"rigid_place": 236, "rigid_volume": 44, "rigid_force": 52}
+RIGID_ALG_PER_KEY = {"rigid_place": 12}
+
+
+def cell_keys(sc):
+    """Cell keys of the scene's grid (4x4x4 bricks of smoothRadius_h cells
+    over [spaceMin - 2h, spaceMax + 2h], as the library enumerates them)."""
+    h = np.float32(sc.smooth_radius)
+    lo, hi = np.float32(sc.space_min), np.float32(sc.space_max)
+    num = ((hi - lo + h * np.float32(2)) * (np.float32(1) / h)).astype(np.int64) + 2
+    return int(np.prod((num + 3) // 4) * 64 + 1)
+
+
+def rigid_workload(seed=0):
+    from graphics_b200.scene import floating_box
+    b = RIGID_BODY
+    return floating_box((200, 50, 100), 0.01, (4.0, 2.0, 2.0), b["half"], b["center"], seed=seed)
+
+
+def rigid_world(sc):
+    from graphics_b200.rigid import RigidBody, RigidWorld
+    b, m = RIGID_BODY, sc.meta["bodies"][0]
+    w = RigidWorld()
+    w.add(m["solid_id"], RigidBody.box(b["density"], b["half"], b["center"], q=b["q"]))
+    return w
+
+
+def cpu_rigid_sample(sc, budget, dt):
+    """The reference's DFSPH with the rigid stand-in of the oracle harness
+    (rigidForceJoin, the same host world, updatePaticles) on all host cores,
+    steps from rest until `budget` seconds."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import make_scene_oracle
+    t0 = time.perf_counter()
+    o = make_scene_oracle(sc, kind="reference", solver="dfsph_capped", nu=SOLVER_KW["nu"], dt=dt)
+    w = rigid_world(sc)
+    m = sc.meta["bodies"][0]
+    o.set_solid_dynamic(m["solid_id"], m["inner"], w.state(m["solid_id"]))
+    o.set_rigid_world(w)
+    setup = time.perf_counter() - t0
+    steps, t_run = 0, 0.0
+    while True:
+        t1 = time.perf_counter()
+        o.stage("runOneStep")
+        t_run += time.perf_counter() - t1
+        steps += 1
+        if t_run >= budget or steps >= 50:
+            break
+    cores = o.threads()
+    o.close()
+    return {"value": sc.n_fluid * steps / t_run, "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": "%d DFSPH step(s) of the %d-particle floating-box scene from rest at fixed dt=%.1e s with "
+                      "the dynamic box coupled every step (reference DFSPH.cpp + SphBase.cpp rigidForceJoin / "
+                      "updatePaticles via oracle/_ref, float, all threads; density loop FP64-summed and capped "
+                      "at 100), setup %.1f s untimed" % (steps, sc.n_fluid, dt, setup),
+            "seconds": t_run}
+
+
+def run_rigid(args):
+    """DFSPH with a dynamic rigid body (one GPU; the scene does not shard)."""
+    import torch
+    from graphics_b200.sph import scene_to_gpu
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world_n = int(os.environ.get("WORLD_SIZE", "1"))
+    torch.cuda.set_device(local)
+    sc = rigid_workload()
+    m = sc.meta["bodies"][0]
+    g = scene_to_gpu(sc, device=local, **SOLVER_KW)
+    if args.no_graphs:
+        g.debug_set("use_graphs", 0)
+    w = rigid_world(sc)
+    g.set_solid_dynamic(m["solid_id"], m["inner"], w.state(m["solid_id"]))
+    g.set_rigid_world(w)
+    stream = torch.cuda.ExternalStream(g.lib.sphgpu_stream(g.h), device=torch.device("cuda", local))
+    settle = min(args.settle, 150)
+    if settle:
+        g.step("dfsph", settle)
+    g.step("dfsph", max(args.warmup, 1))
+    import copy
+    snap_pos, snap_vel = g.get("position"), g.get("velocity")
+    body0 = copy.deepcopy(w.bodies[m["solid_id"]])
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        torch.cuda.nvtx.range_push("timed_rigid")  # lets an ncu launch list select the timed steps
+        e0.record(stream)
+        st = g.step("dfsph", args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
+    ms = e0.elapsed_time(e1)
+    n = st["n_fluid"]
+    value = n * args.steps / (ms / 1e3)
+    log = w.log[-args.steps:]
+    hbm, peak_kind = peaks()
+    # per-kernel durations (individual launches, CUDA events), next steps
+    g.profile(True)
+    g.step("dfsph", args.profile_steps)
+    prof = g.profile_read()
+    g.profile(False)
+    st_p = g.synchronize()
+    nbp = sc.n_boundary
+    nbody = len(m["inner"])
+    kern = {}
+    for k, (tot_ms, cnt) in prof.items():
+        ent = {"launches": cnt, "avg_us": round(1e3 * tot_ms / max(cnt, 1), 2),
+               "us_per_step": round(1e3 * tot_ms / args.profile_steps, 1)}
+        if k in RIGID_ALG:
+            units = nbody if k == "rigid_force" else nbp
+            b = RIGID_ALG[k] * units + RIGID_ALG_PER_KEY.get(k, 0) * cell_keys(sc)
+            ent["alg_bytes"] = b
+            ent["gbs"] = round(b / (tot_ms / cnt / 1e3) / 1e9, 1)
+        kern[k] = ent
+    dom = max((k for k in kern if k in RIGID_ALG), key=lambda k: kern[k]["us_per_step"])
+    roof = {"bound": "hbm", "kernel": dom, "achieved": kern[dom]["gbs"], "peak": hbm, "unit": "GB/s",
+            "frac": round(kern[dom]["gbs"] / hbm, 4), "traffic": None,
+            "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
+            "alg_bytes_per_boundary_particle": RIGID_ALG[dom] if dom != "rigid_force" else None,
+            "rigid_us_per_step": round(sum(kern[k]["us_per_step"] for k in kern if k in RIGID_ALG), 1)}
+    # the same state with the body held static (one more static solid)
+    bpos = g.get_boundary("position")
+    g.close()
+    from graphics_b200.sph import params_for_scene, GpuScene
+    g2 = GpuScene(params_for_scene(sc, **SOLVER_KW), sc.n_fluid, device=local)
+    g2.set_boundary(bpos, sc.meta["solid_id"])
+    g2.add_fluid(snap_pos, snap_vel, rho0=sc.rho0)
+    g2.step("dfsph", max(args.warmup, 1))
+    g2.set("position", snap_pos)
+    g2.set("velocity", snap_vel)
+    g2.step("dfsph", 0)
+    s2 = torch.cuda.ExternalStream(g2.lib.sphgpu_stream(g2.h), device=torch.device("cuda", local))
+    torch.cuda.synchronize()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(s2)
+    st2 = g2.step("dfsph", args.steps)
+    f1.record(s2)
+    torch.cuda.synchronize()
+    ms2 = f0.elapsed_time(f1)
+    g2.close()
+    # end to end: host positions/velocities in and out every step, the world
+    # in the loop, from the snapshot of the timed region's start
+    e2e = None
+    if args.e2e_steps > 0:
+        g3 = scene_to_gpu(sc, device=local, **SOLVER_KW)
+        w3 = rigid_world(sc)
+        w3.bodies[m["solid_id"]] = copy.deepcopy(body0)
+        g3.set_solid_dynamic(m["solid_id"], m["inner"], w3.state(m["solid_id"]))
+        g3.set_rigid_world(w3)
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+        pos, vel = pin(snap_pos), pin(snap_vel)
+        po, vo = pin(np.empty_like(snap_pos)), pin(np.empty_like(snap_vel))
+        g3.step_host("dfsph", pos, vel, po, vo)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            g3.step_host("dfsph", pos, vel, po, vo)
+            pos, po = po, pos
+            vel, vo = vo, vel
+        sec = time.perf_counter() - t0
+        e2e = {"value": n * args.steps / sec, "unit": UNIT, "h2d_bytes_per_step": int(n * 24),
+               "d2h_bytes_per_step": int(n * 24), "steps": args.steps,
+               "note": "sphgpu_step_host with the rigid world in the loop: pinned positions+velocities in, "
+                       "step, positions+velocities out"}
+        g3.close()
+    cpu = None
+    if rank == 0 and world_n == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_rigid_sample(sc, budget=args.cpu_budget, dt=st["dt"])
+        except Exception as e:
+            cpu = {"unavailable": str(e)}
+    if rank == 0:
+        F = np.array([f for _, f, _, _ in log])[:, 0]
+        line = {"metric": "DFSPH particle-steps/s with a dynamic rigid body coupled every step", "value": value,
+                "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded pool with a floating box)",
+                "config": {"workload": "dfsph_floating_box_%dk" % (sc.n_fluid // 1000), "n_fluid": sc.n_fluid,
+                           "n_boundary": nbp, "n_body_particles": nbody, "body": RIGID_BODY, "r": sc.r,
+                           "box": list(sc.meta["box"]), "settle_steps": settle, "cfl": 0.4,
+                           "dt_max": SOLVER_KW["dt_max"], "density_goal": 1e-4, "divergence_goal": 1e-3,
+                           "parallelism": "single", "l2": "inputs larger than L2"},
+                "iterations_per_step": {"density": st["total_iter_density"] / args.steps,
+                                        "divergence": st["total_iter_divergence"] / args.steps},
+                "static_body": {"ms_per_step": ms2 / args.steps,
+                                "iterations_per_step": {"density": st2["total_iter_density"] / args.steps,
+                                                        "divergence": st2["total_iter_divergence"] / args.steps},
+                                "note": "the same state with the box as a static solid"},
+                "body_force_last": F[-1].tolist(), "body_state_last": w.state(m["solid_id"])[16:22].tolist(),
+                "roofline": roof, "kernels": kern, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": int(round(sum(kern[k]["launches"] for k in kern) * args.steps
+                                          / max(args.profile_steps, 1))),
+                "clocks": clk.summary()}
+        print(json.dumps(line))
+
+
 def main():
     args = parse()
     SOLVER_KW["df_density_max_iter"] = args.max_iter
@@ -643,6 +856,8 @@ def main():
         run_reference(args)
     elif args.workload == "batched_64":
         run_batched(args)
+    elif args.workload == "floating_box_1m":
+        run_rigid(args)
     else:
         run_ours(args)
 

@@ -121,9 +121,6 @@ struct sphgpu_scene {
     float* h_rstate = nullptr;    // [cap * 25] states (SphRigidState layout)
     double* h_rout = nullptr;     // [cap * 6 + 1] joined force, torque; dt
     int rigid_cap = 0;            // capacity of the per-solid arrays
-    void* sort_tmp = nullptr;
-    size_t sort_bytes = 0;
-    int sort_end_bit = 1;
     sphgpu_rigid_fn rigid_fn = nullptr;
     void* rigid_user = nullptr;
     int rigid_fail = 0;
@@ -338,8 +335,8 @@ int alloc_scene(sphgpu_scene* h) {
 void free_rigid(sphgpu_scene* h) {
     RigidDev& R = h->R;
     DevScene& d = h->d;
-    void* ptrs[] = {R.x0, R.vol, R.dyn, R.sid, R.state, R.wpos, R.wvel, R.key_in, R.val_in, R.key_out, R.val_out,
-                    R.binv, R.out, R.partial, R.ticket, d.bforce, d.bks, h->sort_tmp};
+    void* ptrs[] = {R.x0, R.vol, R.dyn, R.sid, R.state, R.wpos, R.wvel, R.key, R.slot, R.tmp, R.cnt,
+                    R.binv, R.out, R.partial, R.ticket, d.bforce, d.bks};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (d.bpf && d.bpf != d.bpv) cudaFree(d.bpf);
@@ -350,8 +347,6 @@ void free_rigid(sphgpu_scene* h) {
     if (h->h_rout) cudaFreeHost(h->h_rout);
     h->h_rstate = nullptr;
     h->h_rout = nullptr;
-    h->sort_tmp = nullptr;
-    h->sort_bytes = 0;
     h->rigid_cap = 0;
     R = RigidDev{};
     h->dyn_ids.clear();
@@ -387,7 +382,7 @@ void enq_boundary_update(sphgpu_scene* h, cudaStream_t st) {
     if (!h->R.nd) return;
     cudaMemcpyAsync(h->R.state, h->h_rstate, sizeof(float) * 25 * h->R.nd, cudaMemcpyHostToDevice, st);
     launch(h, "rigid_place", st, [&] {
-        launch_rigid_place_sort(h->d, h->R, h->g, h->sort_tmp, h->sort_bytes, h->sort_end_bit, st);
+        launch_rigid_place_sort(h->d, h->R, h->g, h->cub_tmp, h->cub_bytes, st);
     });
 }
 
@@ -993,19 +988,14 @@ int rigid_init(sphgpu_scene* h) {
     const int nb = h->nb;
     R.nb = nb;
     int r = dalloc(h, &R.x0, nb) | dalloc(h, &R.vol, nb) | dalloc(h, &R.dyn, nb) | dalloc(h, &R.sid, nb) |
-            dalloc(h, &R.wpos, nb) | dalloc(h, &R.wvel, nb) | dalloc(h, &R.key_in, nb) | dalloc(h, &R.val_in, nb) |
-            dalloc(h, &R.key_out, nb) | dalloc(h, &R.val_out, nb) | dalloc(h, &R.binv, nb) |
-            dalloc(h, &R.partial, 6 * ((size_t)nb / 128 + 2)) | dalloc(h, &d.bforce, nb) | dalloc(h, &d.bks, nb);
+            dalloc(h, &R.wpos, nb) | dalloc(h, &R.wvel, nb) | dalloc(h, &R.key, nb) | dalloc(h, &R.slot, nb) |
+            dalloc(h, &R.tmp, nb) | dalloc(h, &R.cnt, (size_t)h->g.nkeys + 1) | dalloc(h, &R.binv, nb) |
+            dalloc(h, &R.partial, 6 * ((size_t)nb / 4 + 2)) | dalloc(h, &d.bforce, nb) | dalloc(h, &d.bks, nb);
     float4* bpf = nullptr;
     r |= dalloc(h, &bpf, 2 * (size_t)nb);
     if (!d.bsid) r |= dalloc(h, &d.bsid, nb);
     if (r) return SPHGPU_ENOMEM;
     d.bpf = bpf;
-    int bits = 1;
-    while (bits < 31 && (1ll << bits) <= (long long)(h->g.nkeys - 1)) ++bits;
-    h->sort_end_bit = bits;
-    h->sort_bytes = rigid_sort_bytes(nb, bits);
-    if (cudaMalloc(&h->sort_tmp, h->sort_bytes + 16) != cudaSuccess) return SPHGPU_ENOMEM;
     // reference order from the sorted walls
     std::vector<float4> bp(nb), x0(nb);
     std::vector<float> vol(nb);

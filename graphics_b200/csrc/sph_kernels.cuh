@@ -148,10 +148,10 @@ struct RigidDev {
                       // linear velocity[3], angular velocity[3]
     float4* wpos;     // [nb] placed position (w = kerSumFromSelf)
     float4* wvel;     // [nb] rigid velocity of the placed particle
-    int* key_in;      // [nb] sort input (reversed reference order) and output
-    int* val_in;
-    int* key_out;
-    int* val_out;
+    int* key;         // [nb] cell key of each placed particle (reference order)
+    int* slot;        // [nb] its arrival slot in the cell count
+    int* tmp;         // [nb] sorted slot -> reference index, before the in-cell rank
+    int* cnt;         // [nkeys + 1] particles per cell key
     int* binv;        // [nb] reference index -> sorted slot
     double* out;      // [nd * 6] joined force and torque of the last step
     double* partial;  // per-block partial sums, 6 per block
@@ -244,12 +244,12 @@ void launch_iv_sweep_b(const DevScene& s, const SolverConst& c, int phase, int d
 void launch_iv_integrate(const DevScene& s, int n_max, cudaStream_t st);
 
 // ---- dynamic rigid solids (sph_rigid.cu) ----
-// updatePaticles for every dynamic solid, cell keys, stable key sort of the
-// whole boundary (within a cell: descending reference index), gather into
-// the sorted arrays and the boundary cell table
-void launch_rigid_place_sort(const DevScene& s, const RigidDev& R, const GridGeom& g, void* sort_tmp,
-                             size_t sort_bytes, int end_bit, cudaStream_t st);
-size_t rigid_sort_bytes(int nb, int end_bit);
+// updatePaticles for every dynamic solid, then a counting sort of the whole
+// boundary by cell key (within a cell: descending reference index) into the
+// sorted arrays and the boundary cell table; scan_tmp / scan_bytes: CUB scan
+// scratch for nkeys + 1 entries
+void launch_rigid_place_sort(const DevScene& s, const RigidDev& R, const GridGeom& g, void* scan_tmp,
+                             size_t scan_bytes, cudaStream_t st);
 // prepareSolidPartWeight over the boundary alone: kerSumFromSelf and volume
 void launch_rigid_prepare(const DevScene& s, const RigidDev& R, const GridGeom& g, float dpart, float h2cut, int cap,
                           cudaStream_t st);

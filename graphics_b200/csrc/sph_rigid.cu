@@ -16,8 +16,9 @@
 // Here the rigid-body world stays on the host and exchanges only force,
 // torque and state per solid and step; everything per particle runs on the
 // device:
-//   k_rigid_force     per boundary particle of a dynamic solid: gathers its
-//                     fluid neighbours (the fluid particles whose capped list
+//   k_rigid_force     per boundary particle of a dynamic solid (one warp,
+//                     a lane per neighbour cell): gathers its fluid
+//                     neighbours (the fluid particles whose capped list
 //                     holds it), sums both reactions, and joins force and
 //                     torque per solid in FP64 (block partials summed in a
 //                     fixed order by the last block).  The pressure reaction
@@ -30,18 +31,18 @@
 //                     (transform in round-to-nearest float ops in the
 //                     reference's evaluation order) and the cell keys of the
 //                     whole boundary
-//   radix sort        stable sort of the keys, fed in reversed reference
-//                     order, so each cell lists its particles in descending
-//                     reference index -- the reference's linked-list order
-//   k_rigid_gather    sorted boundary arrays, inverse permutation
-//   k_bcell_bounds    boundary cell table (lower bound per key)
+//   counting sort     per-cell counts (k_rigid_place), exclusive scan into
+//                     the boundary cell table, scatter, then the in-cell rank
+//                     by descending reference index -- the reference's
+//                     linked-list order -- with the gather into the sorted
+//                     arrays and the inverse permutation (k_rigid_rank)
 //   k_rigid_volume    updateSolidPartWeight after the fluid sort: the
 //                     boundary particle's capped list in the reference's
 //                     order (fluid candidates count toward the cap; same-solid
 //                     particles are skipped, SphBase.cpp:922)
 //   k_rigid_prepare   prepareSolidPartWeight over the boundary alone
 //                     (kerSumFromSelf and volume), when a solid turns dynamic
-#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
 #include "sph_kernels.cuh"
 
@@ -87,14 +88,26 @@ __global__ void __launch_bounds__(NT) k_rigid_place(DevScene s, RigidDev R, Grid
         if (cell_inside(g, cx, cy, cz)) key = cell_key(g, cx, cy, cz);
     }
     if (key == g.nkeys - 1) atomicOr(&s.st->status, 64u);
-    R.key_in[R.nb - 1 - r] = key;
-    R.val_in[R.nb - 1 - r] = r;
+    R.key[r] = key;
+    R.slot[r] = atomicAdd(&R.cnt[key], 1);
 }
 
-__global__ void __launch_bounds__(NT) k_rigid_gather(DevScene s, RigidDev R) {
-    const int q = blockIdx.x * NT + threadIdx.x;
-    if (q >= R.nb) return;
-    const int r = R.val_out[q];
+__global__ void __launch_bounds__(NT) k_rigid_scatter(DevScene s, RigidDev R) {
+    const int r = blockIdx.x * NT + threadIdx.x;
+    if (r < R.nb) R.tmp[s.bcell_start[R.key[r]] + R.slot[r]] = r;
+}
+
+// sorted slot q holds reference particle tmp[q] of cell [a, b); its final
+// slot is a + #{particles of the cell with a larger reference index}
+__global__ void __launch_bounds__(NT) k_rigid_rank(DevScene s, RigidDev R) {
+    const int q0 = blockIdx.x * NT + threadIdx.x;
+    if (q0 >= R.nb) return;
+    const int r = R.tmp[q0];
+    const int key = R.key[r];
+    const int a = s.bcell_start[key], b = s.bcell_start[key + 1];
+    int rank = 0;
+    for (int j = a; j < b; ++j) rank += R.tmp[j] > r;
+    const int q = a + rank;
     const float4 p = R.wpos[r], v = R.wvel[r];
     const float vol = R.vol[r];
     const float4 pv = make_float4(p.x, p.y, p.z, vol);
@@ -107,18 +120,6 @@ __global__ void __launch_bounds__(NT) k_rigid_gather(DevScene s, RigidDev R) {
     s.bgid[q] = r;
     s.bsid[q] = R.sid[r];
     R.binv[r] = q;
-}
-
-__global__ void __launch_bounds__(256) k_bcell_bounds(DevScene s, RigidDev R, int nkeys) {
-    const int k = blockIdx.x * 256 + threadIdx.x;
-    if (k > nkeys) return;
-    int lo = 0, hi = R.nb;  // first sorted slot with key >= k
-    while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (R.key_out[mid] < k) lo = mid + 1;
-        else hi = mid;
-    }
-    s.bcell_start[k] = lo;
 }
 
 __device__ __forceinline__ void set_volume(DevScene& s, const RigidDev& R, int q, float vol) {
@@ -182,6 +183,24 @@ __global__ void __launch_bounds__(NT) k_rigid_volume(DevScene s, RigidDev R, Gri
     const int cz = cell_coord(pa.z, g.min[2], g.divisor);
     const float hp = (dpart + dpart) / 2;
     float sum = s.bks[q];
+    // no particle of another solid within the cut: the list adds nothing
+    bool other = false;
+    for (int dz = -1; dz <= 1 && !other; ++dz)
+        for (int dy = -1; dy <= 1 && !other; ++dy)
+            for (int dx = -1; dx <= 1 && !other; ++dx) {
+                const int x = cx + dx, y = cy + dy, z = cz + dz;
+                if (!cell_inside(g, x, y, z)) continue;
+                const int key = cell_key(g, x, y, z);
+                for (int b = s.bcell_start[key], e = s.bcell_start[key + 1]; b < e && !other; ++b) {
+                    if (s.bsid[b] == sid) continue;
+                    const float4 pb = s.bpos[b];
+                    other = dis_square_rn(pa.x, pa.y, pa.z, pb.x, pb.y, pb.z) < h2cut;
+                }
+            }
+    if (!other) {
+        set_volume(s, R, q, 1.f / sum);
+        return;
+    }
     int cnt = 0;
     for (int dz = -1; dz <= 1 && cnt < cap; ++dz)
         for (int dy = -1; dy <= 1 && cnt < cap; ++dy)
@@ -218,110 +237,125 @@ __global__ void __launch_bounds__(NT) k_rigid_volume(DevScene s, RigidDev R, Gri
 //   pressure (DFSPH.cpp:687-689), summed over the iterations:
 //     force += x f rho0 V_q (sum_it kappa_a) / rho_a
 // and force *= rho0 * spacing_r^3 (DFSPH.cpp:723-737).
+// One warp per boundary particle, lane l < 27 scanning cell l of the 27 (x
+// fastest); the lanes' sums meet in a fixed shuffle tree, the particles'
+// FP64 force and torque in fixed-order block and grid sums.
 template <int BS>
 __global__ void __launch_bounds__(BS) k_rigid_force(DevScene s, RigidDev R, SolverConst c, GridGeom g, int r0, int r1,
                                                     int di) {
-    const int r = r0 + blockIdx.x * BS + threadIdx.x;
-    double acc[6] = {0, 0, 0, 0, 0, 0};
+    constexpr int WPB = BS / 32;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int r = r0 + blockIdx.x * WPB + wid;
+    __shared__ double wsum[WPB][6];
     if (r < r1) {
         const int q = R.binv[r];
         const float4 pb = s.bpf[2 * q], vb = s.bpf[2 * q + 1];
         const float Vb = pb.w;
-        const int cx = cell_coord(pb.x, g.min[0], g.divisor);
-        const int cy = cell_coord(pb.y, g.min[1], g.divisor);
-        const int cz = cell_coord(pb.z, g.min[2], g.divisor);
-        const float den0 = 0.01f * c.hs * c.hs;
-        const float visc = 10.f * c.nu;
-        const size_t stride = (size_t)c.stride;
-        const int me = (int)((unsigned)q | BND_FLAG);
         float px = 0.f, py = 0.f, pz = 0.f, vx = 0.f, vy = 0.f, vz = 0.f;
-        for (int dz = -1; dz <= 1; ++dz)
-            for (int dy = -1; dy <= 1; ++dy)
-                for (int dx = -1; dx <= 1; ++dx) {
-                    const int x = cx + dx, y = cy + dy, z = cz + dz;
-                    if (!cell_inside(g, x, y, z)) continue;
-                    const int key = cell_key(g, x, y, z);
-                    const int a0 = s.cstart2[key].x, a1 = s.cstart2[key + 1].x;
-                    for (int a = a0; a < a1; ++a) {
-                        const float4 pa = s.pos[a];
-                        const float len2 = dis_square_rn(pa.x, pa.y, pa.z, pb.x, pb.y, pb.z);
-                        if (!(len2 < c.h2cut)) continue;
-                        const int cnt = s.ncount[a];
-                        if (cnt >= c.cap) {
-                            bool listed = false;
-                            for (int k = 0; k < cnt && !listed; ++k) listed = ell_get(s.nbr, stride, a, k) == me;
-                            if (!listed) continue;
-                        }
-                        if (len2 == 0.f) continue;  // the reference skips zero distances (DFSPH.cpp:1338-1342)
-                        const float xx = pa.x - pb.x, xy = pa.y - pb.y, xz = pa.z - pb.z;
-                        const float f = grad_over_r(c.k, len2);
-                        const float rhoa = s.rho[a];
-                        const float kap = (s.ksum[a] + s.kwarm[a]) / rhoa;
-                        const float tp = f * (c.rho0 * kap) * Vb;
-                        px = fmaf(xx, tp, px);
-                        py = fmaf(xy, tp, py);
-                        pz = fmaf(xz, tp, pz);
-                        const float4 va = s.vel[a];
-                        const float pro = (va.x - vb.x) * xx + (va.y - vb.y) * xy + (va.z - vb.z) * xz;
-                        if (pro < 0.f) {
-                            const float m = c.rho0 * Vb / rhoa;
-                            const float tv = f * pro / (len2 + den0) * m * visc;
-                            vx = fmaf(xx, tv, vx);
-                            vy = fmaf(xy, tv, vy);
-                            vz = fmaf(xz, tv, vz);
-                        }
+        if (lane < 27) {
+            const int x = cell_coord(pb.x, g.min[0], g.divisor) + lane % 3 - 1;
+            const int y = cell_coord(pb.y, g.min[1], g.divisor) + (lane / 3) % 3 - 1;
+            const int z = cell_coord(pb.z, g.min[2], g.divisor) + lane / 9 - 1;
+            if (cell_inside(g, x, y, z)) {
+                const int key = cell_key(g, x, y, z);
+                const int a0 = s.cstart2[key].x, a1 = s.cstart2[key + 1].x;
+                const float den0 = 0.01f * c.hs * c.hs;
+                const float visc = 10.f * c.nu;
+                const size_t stride = (size_t)c.stride;
+                const int me = (int)((unsigned)q | BND_FLAG);
+                for (int a = a0; a < a1; ++a) {
+                    const float4 pa = s.pos[a];
+                    const float len2 = dis_square_rn(pa.x, pa.y, pa.z, pb.x, pb.y, pb.z);
+                    if (!(len2 < c.h2cut)) continue;
+                    const int cnt = s.ncount[a];
+                    if (cnt >= c.cap) {
+                        bool listed = false;
+                        for (int k = 0; k < cnt && !listed; ++k) listed = ell_get(s.nbr, stride, a, k) == me;
+                        if (!listed) continue;
+                    }
+                    if (len2 == 0.f) continue;  // the reference skips zero distances (DFSPH.cpp:1338-1342)
+                    const float xx = pa.x - pb.x, xy = pa.y - pb.y, xz = pa.z - pb.z;
+                    const float f = grad_over_r(c.k, len2);
+                    const float rhoa = s.rho[a];
+                    const float kap = (s.ksum[a] + s.kwarm[a]) / rhoa;
+                    const float tp = f * (c.rho0 * kap) * Vb;
+                    px = fmaf(xx, tp, px);
+                    py = fmaf(xy, tp, py);
+                    pz = fmaf(xz, tp, pz);
+                    const float4 va = s.vel[a];
+                    const float pro = (va.x - vb.x) * xx + (va.y - vb.y) * xy + (va.z - vb.z) * xz;
+                    if (pro < 0.f) {
+                        const float m = c.rho0 * Vb / rhoa;
+                        const float tv = f * pro / (len2 + den0) * m * visc;
+                        vx = fmaf(xx, tv, vx);
+                        vy = fmaf(xy, tv, vy);
+                        vz = fmaf(xz, tv, vz);
                     }
                 }
-        const float fx = c.fm0 * (px - vx), fy = c.fm0 * (py - vy), fz = c.fm0 * (pz - vz);
-        s.bforce[q] = make_float4(fx, fy, fz, 0.f);
-        const float* st = R.state + 25 * di;
-        const double rx = (double)pb.x - st[16], ry = (double)pb.y - st[17], rz = (double)pb.z - st[18];
-        acc[0] = fx;
-        acc[1] = fy;
-        acc[2] = fz;
-        acc[3] = ry * fz - rz * fy;
-        acc[4] = rz * fx - rx * fz;
-        acc[5] = rx * fy - ry * fx;
-    }
-    __shared__ double sh[BS / 32];
-    double bs[6];
+            }
+        }
 #pragma unroll
-    for (int i = 0; i < 6; ++i) bs[i] = block_sum_double<BS>(acc[i], sh);
+        for (int o = 16; o > 0; o >>= 1) {
+            px += __shfl_down_sync(0xffffffffu, px, o);
+            py += __shfl_down_sync(0xffffffffu, py, o);
+            pz += __shfl_down_sync(0xffffffffu, pz, o);
+            vx += __shfl_down_sync(0xffffffffu, vx, o);
+            vy += __shfl_down_sync(0xffffffffu, vy, o);
+            vz += __shfl_down_sync(0xffffffffu, vz, o);
+        }
+        if (lane == 0) {
+            const float fx = c.fm0 * (px - vx), fy = c.fm0 * (py - vy), fz = c.fm0 * (pz - vz);
+            s.bforce[q] = make_float4(fx, fy, fz, 0.f);
+            const float* st = R.state + 25 * di;
+            const double rx = (double)pb.x - st[16], ry = (double)pb.y - st[17], rz = (double)pb.z - st[18];
+            wsum[wid][0] = fx;
+            wsum[wid][1] = fy;
+            wsum[wid][2] = fz;
+            wsum[wid][3] = ry * fz - rz * fy;
+            wsum[wid][4] = rz * fx - rx * fz;
+            wsum[wid][5] = rx * fy - ry * fx;
+        }
+    } else if (lane == 0) {
+        for (int i = 0; i < 6; ++i) wsum[wid][i] = 0.0;
+    }
+    __syncthreads();
     __shared__ bool last;
     if (threadIdx.x == 0) {
-        for (int i = 0; i < 6; ++i) R.partial[6 * (size_t)blockIdx.x + i] = bs[i];
+        for (int i = 0; i < 6; ++i) {
+            double b = 0.0;
+            for (int w = 0; w < WPB; ++w) b += wsum[w][i];
+            R.partial[6 * (size_t)blockIdx.x + i] = b;
+        }
         __threadfence();
         last = atomicAdd(&R.ticket[di], 1u) == gridDim.x - 1;
     }
     __syncthreads();
-    if (!last || threadIdx.x != 0) return;
+    if (!last) return;
     __threadfence();
-    double tot[6] = {0, 0, 0, 0, 0, 0};
-    for (int b = 0; b < (int)gridDim.x; ++b)
-        for (int i = 0; i < 6; ++i) tot[i] += ((volatile double*)R.partial)[6 * (size_t)b + i];
-    for (int i = 0; i < 6; ++i) R.out[6 * di + i] = tot[i];
-    R.ticket[di] = 0u;
+    // the last block: thread t sums blocks t, t + BS, ... in order, then a
+    // fixed tree over the threads
+    __shared__ double sh[BS / 32];
+    for (int i = 0; i < 6; ++i) {
+        double v = 0.0;
+        for (int b = threadIdx.x; b < (int)gridDim.x; b += BS) v += ((volatile double*)R.partial)[6 * (size_t)b + i];
+        const double tot = block_sum_double<BS>(v, sh);
+        if (threadIdx.x == 0) R.out[6 * di + i] = tot;
+    }
+    if (threadIdx.x == 0) R.ticket[di] = 0u;
 }
 }  // namespace
 
 static inline int nblk(int n, int bs) { return (n > 0 ? n + bs - 1 : bs) / bs; }
 
-size_t rigid_sort_bytes(int nb, int end_bit) {
-    size_t bytes = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, bytes, (const int*)nullptr, (int*)nullptr, (const int*)nullptr,
-                                    (int*)nullptr, nb, 0, end_bit);
-    return bytes;
-}
-
-void launch_rigid_place_sort(const DevScene& s, const RigidDev& R, const GridGeom& g, void* sort_tmp,
-                             size_t sort_bytes, int end_bit, cudaStream_t st) {
+void launch_rigid_place_sort(const DevScene& s, const RigidDev& R, const GridGeom& g, void* scan_tmp,
+                             size_t scan_bytes, cudaStream_t st) {
     if (R.nb <= 0) return;
+    cudaMemsetAsync(R.cnt, 0, sizeof(int) * ((size_t)g.nkeys + 1), st);
     k_rigid_place<<<nblk(R.nb, NT), NT, 0, st>>>(s, R, g);
-    size_t b = sort_bytes;
-    cub::DeviceRadixSort::SortPairs(sort_tmp, b, (const int*)R.key_in, R.key_out, (const int*)R.val_in, R.val_out,
-                                    R.nb, 0, end_bit, st);
-    k_rigid_gather<<<nblk(R.nb, NT), NT, 0, st>>>(s, R);
-    k_bcell_bounds<<<nblk(g.nkeys + 1, 256), 256, 0, st>>>(s, R, g.nkeys);
+    size_t b = scan_bytes;
+    cub::DeviceScan::ExclusiveSum(scan_tmp, b, R.cnt, s.bcell_start, g.nkeys + 1, st);
+    k_rigid_scatter<<<nblk(R.nb, NT), NT, 0, st>>>(s, R);
+    k_rigid_rank<<<nblk(R.nb, NT), NT, 0, st>>>(s, R);
 }
 
 void launch_rigid_prepare(const DevScene& s, const RigidDev& R, const GridGeom& g, float dpart, float h2cut, int cap,
@@ -336,5 +370,5 @@ void launch_rigid_volume(const DevScene& s, const RigidDev& R, const GridGeom& g
 
 void launch_rigid_force(const DevScene& s, const RigidDev& R, const SolverConst& c, const GridGeom& g, int r0, int r1,
                         int di, cudaStream_t st) {
-    if (r1 > r0) k_rigid_force<NT><<<nblk(r1 - r0, NT), NT, 0, st>>>(s, R, c, g, r0, r1, di);
+    if (r1 > r0) k_rigid_force<NT><<<nblk(r1 - r0, NT / 32), NT, 0, st>>>(s, R, c, g, r0, r1, di);
 }

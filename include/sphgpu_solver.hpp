@@ -22,6 +22,13 @@
  * phase, the scene is uploaded again before the next step.  m_EC receives
  * the step's zero-distance and neighbour-overflow counts (SphBase.h:586-602).
  *
+ * Dynamic rigid solids (SphSolid::dynamic, SphBase.h:330; DFSPH): uploaded
+ * with their innerPositions and the state gpuRigidState() gives; every step
+ * the library calls gpuRigidStep() with each dynamic solid's joined force
+ * and torque -- the exchange SphWithBullet::updateSolids has with Bullet
+ * (SphWithBullet.cpp:180-224, 302-317) -- and after the step the solids'
+ * boundaryParticles positions and velocities are written back.
+ *
  * Header only; needs the reference's class declarations included first and
  * links against libsphgpu.so.
  */
@@ -51,6 +58,31 @@ public:
     /* CUDA device the scene runs on (set before the first step). */
     void setGpuDevice(int d) { device_ = d; }
 
+    /* Rigid-body world of the dynamic solids.  gpuRigidState(k): solid k's
+     * state at upload; the default is the identity transform (its
+     * innerPositions are its positions under the identity, SphBase.h:
+     * 334-336) with the centre of mass at the particles' centroid, at rest.
+     * gpuRigidStep: apply force[3i..] and torque[3i..] to solid solids[i],
+     * advance the bodies by dt, write their new states into states[i] (which
+     * hold the current ones); the default keeps them.  A scene with Bullet
+     * overrides both with SphWithBullet.cpp:185-210's calls
+     * (applyCentralForce, applyTorque, stepSimulation, getOpenGLMatrix,
+     * getCenterOfMassPosition, getLinearVelocity, getAngularVelocity). */
+    virtual SphRigidState gpuRigidState(int solid) {
+        SphRigidState st = {};
+        st.transform[0] = st.transform[5] = st.transform[10] = st.transform[15] = 1.f;
+        const auto& in = this->m_Solids[solid].innerPositions;
+        double c[3] = {0, 0, 0};
+        for (auto& x : in)
+            for (int k = 0; k < 3; ++k) c[k] += x[k];
+        for (int k = 0; k < 3; ++k) st.center_of_mass[k] = in.empty() ? 0.f : (float)(c[k] / in.size());
+        return st;
+    }
+    virtual void gpuRigidStep(int n, const int* solids, const double* force, const double* torque, double dt,
+                              SphRigidState* states) {
+        (void)n; (void)solids; (void)force; (void)torque; (void)dt; (void)states;
+    }
+
 protected:
     void sphStep() override {
         if (!gpu_ || host_layout_changed()) upload();
@@ -59,6 +91,7 @@ protected:
         this->m_EC.zeroDis += stats_.zero_distance;
         this->m_EC.tooManyNeigb += stats_.neighbour_overflow;
         download();
+        download_solids();
     }
 
 private:
@@ -67,6 +100,16 @@ private:
     SphStepStats stats_ = {};
     int device_ = 0;
     std::vector<size_t> counts_;  // per phase, as last written to m_Fluids
+
+    static int rigid_trampoline(void* user, int n, const int* solids, const double* force, const double* torque,
+                                double dt, SphRigidState* states) {
+        try {
+            static_cast<GpuSolver*>(user)->gpuRigidStep(n, solids, force, torque, dt, states);
+            return 0;
+        } catch (...) {
+            return 1;  // the step call then fails with SPHGPU_EINVAL
+        }
+    }
 
     void fail(const char* what, int rc) {
         char buf[512] = {0};
@@ -137,6 +180,44 @@ private:
             rc = sphgpu_add_fluid(gpu_, (int)f.fluidParticles.size(), xyz.data(), vel.data(),
                                   (float)f.restDensity_rho0, (float)f.viscosity_alpha);
             if (rc < 0) fail("sphgpu_add_fluid", rc);
+        }
+        bool dyn = false;
+        for (size_t k = 0; k < this->m_Solids.size(); ++k) {
+            auto& s = this->m_Solids[k];
+            if (!s.dynamic) continue;
+            xyz.clear();
+            for (auto& x : s.innerPositions)
+                for (int c = 0; c < 3; ++c) xyz.push_back((float)x[c]);
+            const SphRigidState st = gpuRigidState((int)k);
+            rc = sphgpu_set_solid_dynamic(gpu_, (int)k, xyz.data(), &st);
+            if (rc) fail("sphgpu_set_solid_dynamic", rc);
+            dyn = true;
+        }
+        if (dyn) sphgpu_set_rigid_callback(gpu_, &GpuSolver::rigid_trampoline, this);
+    }
+
+    // dynamic solids' particles (reference order: solid by solid) back into
+    // m_Solids, as updatePaticles leaves them
+    void download_solids() {
+        bool dyn = false;
+        for (auto& s : this->m_Solids) dyn = dyn || s.dynamic;
+        if (!dyn) return;
+        size_t nb = 0;
+        for (auto& s : this->m_Solids) nb += s.boundaryParticles.size();
+        std::vector<float> x(3 * nb), v(3 * nb);
+        int rc = sphgpu_get_boundary(gpu_, "position", x.data());
+        if (rc >= 0) rc = sphgpu_get_boundary(gpu_, "velocity", v.data());
+        if (rc < 0) fail("sphgpu_get_boundary", rc);
+        size_t i = 0;
+        for (auto& s : this->m_Solids) {
+            for (auto& q : s.boundaryParticles) {
+                if (s.dynamic)
+                    for (int c = 0; c < 3; ++c) {
+                        q.position[c] = x[3 * i + c];
+                        q.velocity[c] = v[3 * i + c];
+                    }
+                ++i;
+            }
         }
     }
 

@@ -11,10 +11,18 @@
  *          gravity[3], spaceMin[3], spaceMax[3], soundSpeed_cs, nu, rho0,
  *          visc_alpha, boundary_visc, d, density_goal, div_goal_rel,
  *          densityErro_eta;
- *          then fluid positions[nf*3], velocities[nf*3], boundary positions[nb*3]
+ *          then fluid positions[nf*3], velocities[nf*3], boundary positions[nb*3];
+ *          optionally int32 nbody and, if nbody > 0, a dynamic rigid solid
+ *          (solid 1): float32 body-frame positions[nbody*3], centre of mass
+ *          at t = 0 [3], linear velocity [3], angular velocity about z --
+ *          a body in prescribed motion (translation plus rotation about z
+ *          through the centre of mass), which gpuRigidStep advances
  * out.bin: int32 n, frame, total density iterations; float32 positions[n*3],
  *          velocities[n*3], densities[n] (m_Fluids[0] after the steps;
- *          IISph: sphDensity) */
+ *          IISph: sphDensity); with a body also float32 its particles'
+ *          positions[nbody*3] and the force and torque (float64[6]) of the
+ *          last step */
+#include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -29,6 +37,37 @@ public:
     void stepEvent() override {}
 
     int iters = 0;
+    // prescribed motion of the dynamic body (solid 1)
+    int nbody = 0;
+    float com0[3] = {0, 0, 0}, lin[3] = {0, 0, 0}, wz = 0;
+    double t = 0;
+    double last_ft[6] = {0, 0, 0, 0, 0, 0};
+
+    SphRigidState body_state(double time) const {
+        SphRigidState s = {};
+        const double a = (double)wz * time, c = std::cos(a), sn = std::sin(a);
+        s.transform[0] = (float)c;
+        s.transform[1] = (float)sn;
+        s.transform[4] = (float)-sn;
+        s.transform[5] = (float)c;
+        s.transform[10] = 1.f;
+        s.transform[15] = 1.f;
+        for (int k = 0; k < 3; ++k) {
+            const float x = (float)((double)com0[k] + (double)lin[k] * time);
+            s.transform[12 + k] = x;
+            s.center_of_mass[k] = x;
+            s.linear_velocity[k] = lin[k];
+        }
+        s.angular_velocity[2] = wz;
+        return s;
+    }
+    SphRigidState gpuRigidState(int) override { return body_state(t); }
+    void gpuRigidStep(int n, const int*, const double* force, const double* torque, double dt,
+                      SphRigidState* states) override {
+        for (int k = 0; k < 3; ++k) { last_ft[k] = force[k]; last_ft[3 + k] = torque[k]; }
+        t += dt;
+        for (int i = 0; i < n; ++i) states[i] = body_state(t);
+    }
 
     void load(FILE* f, int& steps) {
         int32_t hdr[3];
@@ -65,6 +104,23 @@ public:
             s.innerPositions.push_back(b.position);
         }
         m_Solids.push_back(s);
+        int32_t nbd = 0;
+        if (fread(&nbd, sizeof nbd, 1, f) == 1 && nbd > 0) {
+            nbody = nbd;
+            std::vector<float> in(3 * (size_t)nbd);
+            float m[7];
+            if (fread(in.data(), sizeof(float), in.size(), f) != in.size() || fread(m, sizeof m, 1, f) != 1) exit(2);
+            for (int k = 0; k < 3; ++k) { com0[k] = m[k]; lin[k] = m[3 + k]; }
+            wz = m[6];
+            SphSolid body(true, SphSolid::RIGIDBODY, static_cast<real_t>(bvisc), 0);
+            for (int i = 0; i < nbd; ++i) {
+                const vec_t x0(in[3 * i], in[3 * i + 1], in[3 * i + 2]);
+                b.position = vec_t(x0[0] + com0[0], x0[1] + com0[1], x0[2] + com0[2]);
+                body.boundaryParticles.push_back(b);
+                body.innerPositions.push_back(x0);
+            }
+            m_Solids.push_back(body);
+        }
         SphFluid fl(static_cast<real_t>(rho0), static_cast<real_t>(visc), static_cast<real_t>(0));
         FluidParticle p = FluidParticle();
         p.d = d;
@@ -94,6 +150,13 @@ public:
         fwrite(x.data(), sizeof(float), x.size(), f);
         fwrite(v.data(), sizeof(float), v.size(), f);
         fwrite(r.data(), sizeof(float), r.size(), f);
+        if (nbody > 0) {
+            std::vector<float> bx;
+            for (auto& q : m_Solids[1].boundaryParticles)
+                for (int c = 0; c < 3; ++c) bx.push_back((float)q.position[c]);
+            fwrite(bx.data(), sizeof(float), bx.size(), f);
+            fwrite(last_ft, sizeof last_ft, 1, f);
+        }
     }
 };
 

@@ -79,3 +79,81 @@ def test_cpp_dropin_subclass_matches_gpu_path(tmp_path, solver, dt, cs):
     assert np.array_equal(g.get("velocity"), v)
     assert np.array_equal(g.get("sphDensity" if solver == "iisph" else "density"), rho)
     g.close()
+
+
+class _PrescribedWorld:
+    """A body in prescribed motion (translation + rotation about z through
+    the centre of mass), as the drop-in scene's gpuRigidStep advances it:
+    the same double arithmetic (math.sin/cos, the C library's) and float
+    rounding, so both sides hand the library identical states."""
+
+    def __init__(self, com0, lin, wz):
+        self.com0, self.lin, self.wz = [float(x) for x in com0], [float(x) for x in lin], float(wz)
+        self.t = 0.0
+        self.log = []
+
+    def state(self, _sid=1):
+        import math
+        a = self.wz * self.t
+        c, s = math.cos(a), math.sin(a)
+        st = np.zeros(25, np.float32)
+        st[0], st[1], st[4], st[5], st[10], st[15] = c, s, -s, c, 1.0, 1.0
+        for k in range(3):
+            x = np.float32(self.com0[k] + self.lin[k] * self.t)
+            st[12 + k] = st[16 + k] = x
+            st[19 + k] = self.lin[k]
+        st[24] = self.wz
+        return st
+
+    def step(self, ids, force, torque, dt):
+        self.log.append((np.array(force, np.float64), np.array(torque, np.float64)))
+        self.t += dt
+
+    def gpu_callback(self):
+        from graphics_b200.rigid import RigidWorld
+        return RigidWorld.gpu_callback(self)
+
+
+def test_cpp_dropin_dynamic_solid_matches_gpu_path(tmp_path):
+    """A DFSPH scene with a dynamic rigid solid (SphSolid(dynamic=true)) in
+    the C++ drop-in: upload of innerPositions and state, the rigid-body world
+    behind gpuRigidStep every step, the solid's particles written back into
+    m_Solids -- bit for bit what the Python path gives with the same world."""
+    exe = os.path.join(REF, "dropin_dfsph")
+    if not os.path.exists(exe):
+        pytest.skip("drop-in check not built (needs the reference sources)")
+    from graphics_b200.scene import floating_box
+    sc = floating_box((16, 8, 16), 0.025, (0.8, 0.8, 0.8), (0.1, 0.1, 0.1), (0.4, 0.38, 0.4), seed=3)
+    sid = sc.meta["solid_id"]
+    body = sc.meta["bodies"][0]
+    walls = sc.boundary_pos[sid == 0]
+    com0, lin, wz = np.float32(body["center"]), np.float32([0.0, -0.1, 0.05]), np.float32(0.8)
+    kw = dict(dt=1e-3, soundSpeed_cs=100.0, nu=1e-3, df_density_goal=1e-4, df_div_goal_rel=1e-3, densityErro_eta=0.01)
+    steps = 5
+    wsc = type(sc)(**{**sc.__dict__, "boundary_pos": walls, "meta": {}})
+    _write(tmp_path / "in.bin", wsc, steps, kw)
+    with open(tmp_path / "in.bin", "ab") as f:
+        f.write(struct.pack("i", len(body["inner"])))
+        f.write(np.ascontiguousarray(body["inner"], np.float32).tobytes())
+        f.write(np.concatenate([com0, lin, [wz]]).astype(np.float32).tobytes())
+    r = subprocess.run([exe, str(tmp_path / "in.bin"), str(tmp_path / "out.bin")], cwd=tmp_path,
+                       capture_output=True, timeout=300)
+    assert r.returncode == 0, r.stderr.decode()[-2000:]
+    n, frame, iters, x, v, rho = _read(tmp_path / "out.bin")
+    raw = open(tmp_path / "out.bin", "rb").read()[12 + 28 * n:]
+    nb = len(body["inner"])
+    bx = np.frombuffer(raw[:12 * nb], np.float32).reshape(nb, 3)
+    ft = np.frombuffer(raw[12 * nb:12 * nb + 48], np.float64)
+    g = scene_to_gpu(sc, df_div_goal_abs=0.0, df_div_max_iter=100, **kw)
+    w = _PrescribedWorld(com0, lin, wz)
+    g.set_solid_dynamic(1, body["inner"], w.state())
+    g.set_rigid_world(w)
+    g.step("dfsph", steps)
+    assert frame == steps and g.n_fluid == n
+    assert np.array_equal(g.get("position"), x)
+    assert np.array_equal(g.get("velocity"), v)
+    assert np.array_equal(g.get("density"), rho)
+    assert np.array_equal(g.get_boundary("position")[-nb:], bx)
+    assert np.array_equal(np.concatenate(w.log[-1]).ravel(), ft)
+    assert np.abs(ft).max() > 0
+    g.close()
