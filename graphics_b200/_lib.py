@@ -90,6 +90,16 @@ SIGNATURES = {
     "sphgpu_set_solid_state": (_i, [_vp, _i, C.POINTER(SphRigidState)]),
     "sphgpu_get_solid_state": (_i, [_vp, _i, C.POINTER(SphRigidState)]),
     "sphgpu_get_solid_force": (_i, [_vp, _i, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "sphgpu_surface_create": (_i, [C.POINTER(C.c_double), C.POINTER(C.c_double), _d, _d, _d, _i, C.POINTER(_vp)]),
+    "sphgpu_surface_destroy": (_i, [_vp]),
+    "sphgpu_surface_grid": (_i, [_vp, C.POINTER(C.c_double), _ip, C.POINTER(C.c_double)]),
+    "sphgpu_surface_field": (_i, [_vp, _i, _vp, _i, _i]),
+    "sphgpu_surface_get_field": (_i, [_vp, _fp]),
+    "sphgpu_surface_set_field": (_i, [_vp, _fp]),
+    "sphgpu_surface_mesh": (C.c_longlong, [_vp, _f, _i, _fp, C.c_longlong]),
+    "sphgpu_surface_stream": (_vp, [_vp]),
+    "sphgpu_surface_last_error": (_i, [_vp, _cp, _i]),
+    "sphgpu_mc_table": (_i, [_ip, C.POINTER(C.c_byte)]),
     "sphgpu_get_neighbours": (_i, [_vp, _ip, _ip, _ip]),
     "sphgpu_get_cells": (_i, [_vp, C.POINTER(C.c_longlong)]),
     "sphgpu_stream": (_vp, [_vp]),

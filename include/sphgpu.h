@@ -288,6 +288,48 @@ int sphgpu_get_solid_state(sphgpu_t h, int solid_id, SphRigidState* state);
  * its state at that step, summed in FP64. */
 int sphgpu_get_solid_force(sphgpu_t h, int solid_id, double force[3], double torque[3]);
 
+/* Surface reconstruction (the reference's surface_field and marchingCubes,
+ * driven by its re.c: surface_setup, surface_aniso, marchingCubes).
+ *
+ * sphgpu_surface_create: surface_field::surface_setup(min, max, r_p, r_h,
+ *   cell_size) (surface_field.cpp:8-41): the field grid spans
+ *   [min - 0.75 r_h, max + 0.75 r_h] with nodes every cell_size; particles
+ *   must lie in [min, max].
+ * sphgpu_surface_field: surface_isotro (aniso = 0, surface_field.cpp:43-75)
+ *   or surface_aniso (aniso = 1, :83-176) of n positions (3 floats each, host
+ *   memory, or device memory when on_device != 0).  Nodes hold the sum over
+ *   particles of det(G) W(|G (x - c)|) (W: the reference's cubic spline of
+ *   radius r_h times r_p^3).  SPHGPU_EOUT_OF_DOMAIN if a particle lies
+ *   outside the neighbour grid (the field is still computed).
+ * sphgpu_surface_get_field / set_field: the grid (x fastest, then y, z;
+ *   get_grid_min / get_grid_num / get_cell_size via sphgpu_surface_grid).
+ * sphgpu_surface_mesh: marchingCubes(result, iso, field, grid_min, grid_num,
+ *   cell) (marching_cubes.cpp:45-120): triangles of 9 floats (3 vertices)
+ *   into out (capacity max_tris triangles; NULL to count), in cube order (z,
+ *   y, x, x fastest); returns the triangle count.  ref_rows = 1 pairs the
+ *   node rows as the reference's row caches do (cube y spans rows
+ *   max(y-1, 0) and y, so its first row of cubes is flat and the mesh sits
+ *   one cell higher along y) and accumulates the cube corners' coordinates
+ *   as its loops do; ref_rows = 0 takes rows y and y + 1 and corners at
+ *   min + i * cell.  The case table is this library's (sphgpu_mc_table): it
+ *   cuts the same polygons out of every cube case as the reference's and
+ *   may split them along other diagonals.
+ * sphgpu_mc_table: that table (ntri[256]; tri[256 * 16] edge ids, -1 after
+ *   the last triangle; cube numbering of marching_cubes.cpp:9-31).  Needs no
+ *   GPU. */
+typedef struct sphgpu_surface* sphgpu_surface_t;
+int sphgpu_surface_create(const double* min3, const double* max3, double r_p, double r_h, double cell_size,
+                          int device, sphgpu_surface_t* out);
+int sphgpu_surface_destroy(sphgpu_surface_t s);
+int sphgpu_surface_grid(sphgpu_surface_t s, double* min3, int* num3, double* cell);
+int sphgpu_surface_field(sphgpu_surface_t s, int aniso, const float* xyz, int n, int on_device);
+int sphgpu_surface_get_field(sphgpu_surface_t s, float* out);
+int sphgpu_surface_set_field(sphgpu_surface_t s, const float* in);
+long long sphgpu_surface_mesh(sphgpu_surface_t s, float iso, int ref_rows, float* out, long long max_tris);
+void* sphgpu_surface_stream(sphgpu_surface_t s);
+int sphgpu_surface_last_error(sphgpu_surface_t s, char* buf, int len);
+int sphgpu_mc_table(int* ntri, signed char* tri);
+
 /* Stage-level entry points (parity tests run "given state S, call stage X"):
  *   "neighbourSearch"                 grid + neighbour lists (+ rho/alpha)
  *   "DF_constantDensitySolverFirst"   rho, alpha            (DFSPH.cpp:84-193)

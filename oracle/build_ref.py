@@ -17,7 +17,8 @@ the GPU machines; the built libraries travel there instead):
    one shared library per solver (DFSPH.h, IISph.h and IISph_M.h share the
    include guard II_SPH_H_, so each solver needs its own library):
        oracle/_ref/libref_dfsph.so, libref_wcsph.so, libref_pcisph.so,
-       libref_iisphm.so
+       libref_iisphm.so; and the surface reconstruction (surface_field.cpp,
+       marching_cubes.cpp) into libref_surface.so
    Two precisions: real_t=float (the reference as shipped, SphBase.h:40) and
    real_t=double (the typedef switch the reference itself describes,
    SphBase.h:37-39) -> suffix _f64.  A third DFSPH variant,
@@ -41,7 +42,8 @@ SRC = os.path.join(OUT, "src")
 SHIM = os.path.join(HERE, "refshim")
 
 FILES = ["SphBase.h", "SphBase.cpp", "Vec23.h", "DFSPH.h", "DFSPH.cpp", "WcSph.h",
-         "WcSph.cpp", "PciSph.h", "PciSph.cpp", "IISph_M.h", "IISph_M.cpp", "IISph.h", "IISph.cpp"]
+         "WcSph.cpp", "PciSph.h", "PciSph.cpp", "IISph_M.h", "IISph_M.cpp", "IISph.h", "IISph.cpp",
+         "surface_field.h", "surface_field.cpp", "marching_cubes.h", "marching_cubes.cpp"]
 
 # (anchor line in SphBase.h, text inserted after it).  The anchors are the last
 # member of FluidParticle (SphBase.h:117), of BoundaryParticle (SphBase.h:198)
@@ -66,6 +68,14 @@ AUGMENT = [
     # the precision switch the reference describes at SphBase.h:37-40
     ("typedef float real_t;\n",
      "#ifdef REF_REAL_DOUBLE\ntypedef double real_t;\n#else\n", "wrap_typedef"),
+]
+
+# Vec23.h's mat33(const vec3&, vec3&, vec3&) binds temporaries to non-const
+# references (an MSVC extension) where surface_field.cpp scales a matrix
+# (Vec23.h:399, 444); the copy takes const references.
+VEC_FIX = [
+    ("inline mat33( const vec3<_T>& a, vec3<_T>& b, vec3<_T>& c ): U(a), V(b), W(c) { }",
+     "inline mat33( const vec3<_T>& a, const vec3<_T>& b, const vec3<_T>& c ): U(a), V(b), W(c) { }"),
 ]
 
 # DFSPH.cpp's density loop (DFSPH.cpp:225-231, 566, 627-631, 696) sums the
@@ -142,6 +152,11 @@ def main():
         t = transcode(f)
         if f == "SphBase.h":
             t = augment(t)
+        if f == "Vec23.h":
+            for a, b in VEC_FIX:
+                if a not in t:
+                    raise SystemExit("Vec23.h anchor not found: %r" % a[:40])
+                t = t.replace(a, b, 1)
         write_if_changed(os.path.join(SRC, f), t)
         if f == "DFSPH.cpp":
             for old, new in DF_CAP:
@@ -167,6 +182,18 @@ def main():
             if real == "double":
                 cmd.insert(1, "-DREF_REAL_DOUBLE")
             jobs.append((so, cmd))
+    # surface reconstruction: surface_field.cpp (TNT / JAMA replaced by the
+    # stand-in refshim/jama_svd.h) and marching_cubes.cpp, which declares its
+    # tables extern and defines them static (-fpermissive) and calls memcpy
+    # without including <cstring>
+    for real, suffix in (("float", ""),):
+        so = os.path.join(OUT, "libref_surface%s.so" % suffix)
+        srcs = [os.path.join(SRC, "surface_field.cpp"), os.path.join(SRC, "marching_cubes.cpp"),
+                os.path.join(SHIM, "surface_harness.cpp")]
+        deps = srcs + [os.path.join(SRC, "SphBase.h"), os.path.join(SHIM, "jama_svd.h")]
+        if not (os.path.exists(so) and all(os.path.getmtime(so) >= os.path.getmtime(d) for d in deps)):
+            jobs.append((so, ["g++", "-std=c++17", "-O3", "-fPIC", "-shared", "-w", "-fpermissive", "-fopenmp",
+                              "-include", "cstring", "-I" + SHIM, "-I" + SRC] + srcs + ["-o", so]))
     # the C++ drop-in checks: scene classes derived from each of the
     # reference's solver classes, switched to the GPU through
     # include/sphgpu_solver.hpp (links libsphgpu.so)

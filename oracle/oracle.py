@@ -387,3 +387,78 @@ def make_scene_oracle(scene, kind="port", solver="dfsph", f64=False, visc_alpha=
             m = scene.phase == ph
             o.add_fluid(scene.fluid_pos[m], scene.fluid_vel[m], d=scene.d, rho0=rho, visc_alpha=visc_alpha)
     return o
+
+
+class RefSurface:
+    """The reference's surface_field and marchingCubes compiled from its
+    sources (oracle/_ref/libref_surface.so; TNT/JAMA replaced by the stand-in
+    refshim/jama_svd.h).  The reference keeps its spline constants in
+    function-local statics (surface_field.cpp:237-241, 255): one radius per
+    process.  surface_aniso prints a progress line every 1 % of the particles
+    and divides by n / 100, so it needs at least 100 particles."""
+
+    _lib = None
+
+    @classmethod
+    def load(cls):
+        if cls._lib is None:
+            name = os.path.join(REF_DIR, "libref_surface.so")
+            if not os.path.exists(name):
+                raise FileNotFoundError(name + " (run oracle/build_ref.py)")
+            lib = C.CDLL(name)
+            dp, fp, ip = C.POINTER(C.c_double), C.POINTER(C.c_float), C.POINTER(C.c_int)
+            lib.rsf_create.restype = C.c_void_p
+            lib.rsf_create.argtypes = [dp, dp, C.c_double, C.c_double, C.c_double]
+            lib.rsf_destroy.argtypes = [C.c_void_p]
+            lib.rsf_grid.argtypes = [C.c_void_p, dp, ip, dp]
+            lib.rsf_field.restype = C.c_longlong
+            lib.rsf_field.argtypes = [C.c_void_p, C.c_int, dp, C.c_int, fp]
+            lib.rsf_marching_cubes.restype = C.c_longlong
+            lib.rsf_marching_cubes.argtypes = [C.c_float, fp, fp, ip, C.c_float, fp, C.c_longlong]
+            cls._lib = lib
+        return cls._lib
+
+    def __init__(self, mn, mx, r_p, r_h, cell):
+        lib = self.load()
+        dp = C.POINTER(C.c_double)
+        a = np.asarray(mn, np.float64)
+        b = np.asarray(mx, np.float64)
+        self.h = lib.rsf_create(a.ctypes.data_as(dp), b.ctypes.data_as(dp), r_p, r_h, cell)
+        g = np.zeros(3)
+        n = np.zeros(3, np.int32)
+        c = C.c_double()
+        lib.rsf_grid(self.h, g.ctypes.data_as(dp), n.ctypes.data_as(C.POINTER(C.c_int)), C.byref(c))
+        self.grid_min, self.grid_num, self.cell = g, n, c.value
+
+    def field(self, positions, aniso=True):
+        lib = self.load()
+        p = np.ascontiguousarray(positions, np.float64)
+        out = np.zeros(int(np.prod(self.grid_num)), np.float32)
+        lib.rsf_field(self.h, int(aniso), p.ctypes.data_as(C.POINTER(C.c_double)), len(p),
+                      out.ctypes.data_as(C.POINTER(C.c_float)))
+        return out
+
+    @classmethod
+    def marching_cubes(cls, iso, field, grid_min, grid_num, cell, max_tris=None):
+        lib = cls.load()
+        f = np.ascontiguousarray(field, np.float32)
+        mn = np.asarray(grid_min, np.float32)
+        res = np.asarray(grid_num, np.int32)
+        fp = C.POINTER(C.c_float)
+        n = lib.rsf_marching_cubes(float(iso), f.ctypes.data_as(fp), mn.ctypes.data_as(fp),
+                                   res.ctypes.data_as(C.POINTER(C.c_int)), float(cell), None, 0)
+        out = np.zeros((max(n, 1), 3, 3), np.float32)
+        lib.rsf_marching_cubes(float(iso), f.ctypes.data_as(fp), mn.ctypes.data_as(fp),
+                               res.ctypes.data_as(C.POINTER(C.c_int)), float(cell), out.ctypes.data_as(fp), n)
+        return out[:n]
+
+    def close(self):
+        if self.h:
+            self.load().rsf_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
