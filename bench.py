@@ -84,7 +84,8 @@ def parse():
     ap.add_argument("--train-seeds", default="1,2", help="jitter seeds of the training runs")
     ap.add_argument("--train-steps", type=int, default=350, help="recorded plain steps per training seed")
     ap.add_argument("--train-every", type=int, default=175, help="record every n-th particle per step")
-    ap.add_argument("--workload", default="dam_break_1m", choices=["dam_break_1m", "batched_64", "floating_box_1m"],
+    ap.add_argument("--workload", default="dam_break_1m",
+                    choices=["dam_break_1m", "batched_64", "floating_box_1m", "surface_1m"],
                     help="dam_break_1m: the headline 1M-particle DFSPH dam break; batched_64: 64 independent "
                          "dam breaks of 10k-200k particles in one batch")
     ap.add_argument("--no-graphs", action="store_true",
@@ -848,6 +849,130 @@ def run_rigid(args):
         print(json.dumps(line))
 
 
+# Surface reconstruction: the reference's reconstruction driver (re.c:29,
+# 107, 112) on the 1M-particle dam-break block (100^3 jittered lattice,
+# r_p = 0.01 m): surface_setup(bbox, r_p, r_h = 2 r_p, cell = r_p / 4),
+# surface_aniso, marchingCubes at iso 0.5.  One "step" = field + mesh.
+SURF = dict(r_p=0.01, r_h=0.02, cell=0.0025, iso=0.5)
+# algorithmic bytes of the field kernel per launch: every node written once
+# (4 B), every (tile, particle) pair's record read once (centre + det, G,
+# box = 64 B) with its particle index (4 B)
+SURF_ALG_NODE, SURF_ALG_PAIR = 4, 68
+
+
+def cpu_surface_sample(pos, budget):
+    """The reference's surface_aniso + marchingCubes (oracle/_ref, one
+    thread: surface_aniso has no OpenMP) on a sub-block of the workload,
+    grown until it takes about `budget` seconds."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import RefSurface
+    lo = pos.min(0)
+    side, t_run, n = 10, 0.0, 0
+    while True:
+        m = np.all(pos < lo + side * 2 * SURF["r_p"], axis=1)
+        sub = pos[m].astype(np.float64)
+        rs = RefSurface(sub.min(0), sub.max(0), SURF["r_p"], SURF["r_h"], SURF["cell"])
+        t0 = time.perf_counter()
+        f = rs.field(sub, aniso=True)
+        tris = RefSurface.marching_cubes(SURF["iso"], f, rs.grid_min.astype(np.float32), rs.grid_num,
+                                         np.float32(rs.cell))
+        t_run = time.perf_counter() - t0
+        n = len(sub)
+        rs.close()
+        if t_run >= budget / 4 or side >= 100:
+            break
+        side = int(side * 1.6)
+    return {"value": n / t_run, "unit": "particles/s", "cores": 1, "kind": "reference",
+            "sample": "%d particles (a %d^3 corner of the block): surface_aniso + marchingCubes of the reference "
+                      "(oracle/_ref, float field, FP64 kernels; single-threaded as written), %d triangles"
+                      % (n, side, len(tris)),
+            "seconds": t_run}
+
+
+def run_surface(args):
+    """Surface reconstruction of the 1M-particle block (one GPU; a single
+    field does not shard)."""
+    import torch
+    from graphics_b200.scene import lattice_block
+    from graphics_b200.surface import surface_field
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    pos = lattice_block((args.scale,) * 3, SURF["r_p"], jitter=0.1, seed=0)
+    n = len(pos)
+    sf = surface_field(device=local)
+    sf.surface_setup(pos.min(0).astype(np.float64), pos.max(0).astype(np.float64), SURF["r_p"], SURF["r_h"],
+                     SURF["cell"])
+    dpos = torch.from_numpy(pos).to("cuda")
+    stream = torch.cuda.ExternalStream(sf.lib.sphgpu_surface_stream(sf.h), device=torch.device("cuda", local))
+    lib = sf.lib
+
+    def step():
+        rc = lib.sphgpu_surface_field(sf.h, 1, dpos.data_ptr(), n, 1)
+        assert rc == 0, rc
+        return lib.sphgpu_surface_mesh(sf.h, SURF["iso"], 0, None, 0)
+
+    for _ in range(max(args.warmup, 1)):
+        ntri = step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            ntri = step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    value = n * args.steps / (ms / 1e3)
+    # per-kernel durations: the field and mesh calls bracketed by events
+    f0, f1, f2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    tf = tm = 0.0
+    reps = max(args.profile_steps, 1)
+    for _ in range(reps):
+        f0.record(stream)
+        lib.sphgpu_surface_field(sf.h, 1, dpos.data_ptr(), n, 1)
+        f1.record(stream)
+        lib.sphgpu_surface_mesh(sf.h, SURF["iso"], 0, None, 0)
+        f2.record(stream)
+        torch.cuda.synchronize()
+        tf += f0.elapsed_time(f1)
+        tm += f1.elapsed_time(f2)
+    nodes = int(np.prod(sf.get_grid_num()))
+    # end to end: host positions in, host triangles out
+    e2e = None
+    if args.e2e_steps > 0:
+        pin = torch.from_numpy(pos).pin_memory().numpy()
+        out = torch.empty((ntri, 3, 3), dtype=torch.float32, pin_memory=True).numpy()
+        import ctypes as C
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            lib.sphgpu_surface_field(sf.h, 1, pin.ctypes.data, n, 0)
+            m = lib.sphgpu_surface_mesh(sf.h, SURF["iso"], 0, out.ctypes.data_as(C.POINTER(C.c_float)), ntri)
+        sec = time.perf_counter() - t0
+        e2e = {"value": n * args.steps / sec, "unit": "particles/s", "h2d_bytes_per_step": int(n * 12),
+               "d2h_bytes_per_step": int(m * 36), "steps": args.steps,
+               "note": "sphgpu_surface_field from host positions, sphgpu_surface_mesh into host memory"}
+    hbm, peak_kind = peaks()
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_surface_sample(pos, args.cpu_budget)
+        except Exception as e:
+            cpu = {"unavailable": str(e)}
+    if rank == 0:
+        line = {"metric": "surface reconstruction particles/s (anisotropic field + marching cubes)", "value": value,
+                "unit": "particles/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic (seeded jittered lattice block)",
+                "config": {"workload": "surface_aniso_block_%dk" % (n // 1000), "n_particles": n, **SURF,
+                           "grid_nodes": nodes, "grid": sf.get_grid_num().tolist(), "triangles": int(ntri),
+                           "parallelism": "single", "l2": "field %.1f GB > L2" % (nodes * 4 / 1e9)},
+                "kernels": {"field_ms": tf / reps, "mesh_ms": tm / reps},
+                "roofline": None, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": None, "clocks": clk.summary()}
+        print(json.dumps(line))
+    sf.close()
+
+
 def main():
     args = parse()
     SOLVER_KW["df_density_max_iter"] = args.max_iter
@@ -858,6 +983,8 @@ def main():
         run_batched(args)
     elif args.workload == "floating_box_1m":
         run_rigid(args)
+    elif args.workload == "surface_1m":
+        run_surface(args)
     else:
         run_ours(args)
 

@@ -549,6 +549,7 @@ struct sphgpu_surface {
     float* field = nullptr;
     // particles
     int pcap = 0;
+    float* xyz = nullptr;  // host positions staged on the device
     float4 *pos = nullptr, *rec0 = nullptr, *rec1 = nullptr, *rec2 = nullptr;
     int4 *blo = nullptr, *bhi = nullptr;
     int *key = nullptr, *slot = nullptr, *tmp = nullptr, *sorted = nullptr, *npair = nullptr, *poff = nullptr;
@@ -580,10 +581,11 @@ namespace {
         }                                                                                           \
     } while (0)
 
-bool g_table_ready = false;
+// the case table lives in each device's constant memory
+unsigned long long g_table_ready = 0;  // bit d: device d has it
 
 int ensure_table(sphgpu_surface* s) {
-    if (g_table_ready) return 0;
+    if (s->device < 64 && ((g_table_ready >> s->device) & 1ull)) return 0;
     signed char tri[256][16];
     unsigned char nt[256];
     mc_build_table(tri, nt);
@@ -591,7 +593,7 @@ int ensure_table(sphgpu_surface* s) {
     SCK(cudaMemcpyToSymbol(c_ntri, nt, sizeof nt));
     SCK(cudaMemcpyToSymbol(c_vert, kVert, sizeof kVert));
     SCK(cudaMemcpyToSymbol(c_edge, kEdge, sizeof kEdge));
-    g_table_ready = true;
+    if (s->device < 64) g_table_ready |= 1ull << s->device;
     return 0;
 }
 
@@ -625,7 +627,7 @@ int ensure_particles(sphgpu_surface* s, int n) {
     int r = salloc(s, &s->pos, cap) | salloc(s, &s->rec0, cap) | salloc(s, &s->rec1, cap) | salloc(s, &s->rec2, cap) |
             salloc(s, &s->blo, cap) | salloc(s, &s->bhi, cap) | salloc(s, &s->key, cap) | salloc(s, &s->slot, cap) |
             salloc(s, &s->tmp, cap) | salloc(s, &s->sorted, cap) | salloc(s, &s->npair, (size_t)cap + 1) |
-            salloc(s, &s->poff, (size_t)cap + 1);
+            salloc(s, &s->poff, (size_t)cap + 1) | salloc(s, &s->xyz, 3 * (size_t)cap);
     if (r) return SPHGPU_ENOMEM;
     s->pcap = cap;
     return 0;
@@ -783,7 +785,7 @@ int sphgpu_surface_create(const double* mn, const double* mx, double r_p, double
 int sphgpu_surface_destroy(sphgpu_surface_t s) {
     if (!s) return SPHGPU_EINVAL;
     cudaSetDevice(s->device);
-    void* ptrs[] = {s->field, s->pos, s->rec0, s->rec1, s->rec2, s->blo, s->bhi, s->key, s->slot, s->tmp, s->sorted,
+    void* ptrs[] = {s->field, s->xyz, s->pos, s->rec0, s->rec1, s->rec2, s->blo, s->bhi, s->key, s->slot, s->tmp, s->sorted,
                     s->npair, s->poff, s->pcnt, s->pstart, s->bad, s->ptile, s->ppart, s->ptile_s, s->ppart_s,
                     s->tstart, s->ntri, s->toff, s->tris, s->coords, s->tmpbuf};
     for (void* p : ptrs)
@@ -813,8 +815,7 @@ int sphgpu_surface_field(sphgpu_surface_t s, int aniso, const float* xyz, int n,
         if (on_device) {
             d = const_cast<float*>(xyz);
         } else {
-            if (ensure_tmp(s, sizeof(float) * 3 * (size_t)n)) return SPHGPU_ENOMEM;
-            d = (float*)s->tmpbuf;
+            d = s->xyz;
             SCK(cudaMemcpyAsync(d, xyz, sizeof(float) * 3 * (size_t)n, cudaMemcpyHostToDevice, s->stream));
         }
         k_pack_xyz<<<nblk(n, 256), 256, 0, s->stream>>>(d, n, s->pos);
@@ -880,9 +881,11 @@ long long sphgpu_surface_mesh(sphgpu_surface_t s, float iso, int ref_rows, float
                 h += cf;
             }
         } else {
+            // node i at min + i * cell from the float min and cell that
+            // marchingCubes receives, evaluated in double
             for (int i = 0; i + 1 < g[a]; ++i) {
-                lo[i] = (float)(s->gmin[a] + (double)i * s->cell);
-                hi[i] = (float)(s->gmin[a] + (double)(i + 1) * s->cell);
+                lo[i] = (float)((double)mnf[a] + (double)i * (double)cf);
+                hi[i] = (float)((double)mnf[a] + (double)(i + 1) * (double)cf);
             }
         }
     }

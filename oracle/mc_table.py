@@ -99,7 +99,8 @@ def edge_mask(case):
 
 def cube_extents(res, mn, cell, ref_rows):
     """Per axis, the low and high coordinate of cube i (float32): nodes at
-    mn + i * cell (computed in double), or with ref_rows the running float
+    mn + i * cell (float32 mn and cell, evaluated in double), or with
+    ref_rows the running float
     sums of the reference's loops (marching_cubes.cpp:53-66: x_max = x_min +
     cell per cube; y and z minima and maxima each summed)."""
     ext = []
@@ -117,8 +118,8 @@ def cube_extents(res, mn, cell, ref_rows):
                 h = f32(h + f32(cell))
         else:
             for i in range(n):
-                lo[i] = f32(float(mn[a]) + i * float(cell))
-                hi[i] = f32(float(mn[a]) + (i + 1) * float(cell))
+                lo[i] = f32(float(f32(mn[a])) + i * float(f32(cell)))
+                hi[i] = f32(float(f32(mn[a])) + (i + 1) * float(f32(cell)))
         ext.append((lo, hi))
     return ext
 

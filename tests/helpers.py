@@ -44,3 +44,33 @@ def elem_rel(a, b):
     a = np.asarray(a, np.float64)
     b = np.asarray(b, np.float64)
     return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-30))) if a.size else 0.0
+
+
+def closed_and_oriented(tris, tol):
+    """A triangle mesh (T, 3, 3) is closed and consistently oriented: after
+    welding vertices closer than tol (a cut edge's vertex is interpolated
+    from either end by the cubes that share the edge, so copies can differ by
+    an ulp), every directed side appears once and its reverse once."""
+    from scipy.spatial import cKDTree
+    pts = np.asarray(tris, np.float64).reshape(-1, 3)
+    parent = np.arange(len(pts))
+
+    def find(i):
+        while parent[i] != i:
+            parent[i] = parent[parent[i]]
+            i = parent[i]
+        return i
+
+    for i, j in cKDTree(pts).query_pairs(tol):
+        a, b = find(i), find(j)
+        if a != b:
+            parent[max(a, b)] = min(a, b)
+    lab = np.array([find(i) for i in range(len(pts))]).reshape(-1, 3)
+    sides = {}
+    for t in lab:
+        if len(set(t)) < 3:
+            continue  # a degenerate sliver (vertex on a node)
+        for k in range(3):
+            s = (t[k], t[(k + 1) % 3])
+            sides[s] = sides.get(s, 0) + 1
+    return all(v == 1 for v in sides.values()) and all((b, a) in sides for (a, b) in sides)

@@ -8,6 +8,7 @@ import pytest
 
 import mc_table as mt
 from graphics_b200.scene import lattice_block
+from helpers import closed_and_oriented
 
 pytestmark = pytest.mark.gpu
 REF = os.path.exists(os.path.join(os.path.dirname(__file__), "..", "oracle", "_ref", "libref_surface.so"))
@@ -100,7 +101,6 @@ def test_gpu_marching_cubes_vertices_are_the_references():
 def test_gpu_mesh_of_a_sphere_is_closed():
     from graphics_b200.surface import surface_field
     sf = surface_field()
-    n = 40
     sf.surface_setup((0, 0, 0), (1, 1, 1), R_P, R_H, 1.0 / 16)
     num = sf.get_grid_num()
     mn = sf.get_grid_min()
@@ -108,16 +108,9 @@ def test_gpu_mesh_of_a_sphere_is_closed():
     f = np.sqrt((x - 0.5) ** 2 + (y - 0.5) ** 2 + (z - 0.5) ** 2).astype(np.float32)
     sf.set_field(f)
     tris = sf.mesh(0.3).astype(np.float64)
-    key = lambda p: tuple(np.round(p, 6))
-    sides = {}
-    for t in tris:
-        for k in range(3):
-            s = (key(t[k]), key(t[(k + 1) % 3]))
-            sides[s] = sides.get(s, 0) + 1
-    assert all(v == 1 for v in sides.values()) and all((b, a) in sides for (a, b) in sides)
+    assert closed_and_oriented(tris, 1e-6)
     vol = np.einsum("ij,ij->i", tris[:, 0], np.cross(tris[:, 1], tris[:, 2])).sum() / 6.0
     assert abs(abs(vol) - 4 / 3 * np.pi * 0.3 ** 3) < 0.02 * 4 / 3 * np.pi * 0.3 ** 3
-    del n
 
 
 def test_isotropic_field_integral():

@@ -10,6 +10,7 @@ import pytest
 
 import mc_table as mt
 from graphics_b200.scene import lattice_block
+from helpers import closed_and_oriented
 
 REF = os.path.exists(os.path.join(os.path.dirname(__file__), "..", "oracle", "_ref", "libref_surface.so"))
 # one radius set for every reference call in the process (its spline
@@ -123,14 +124,7 @@ def test_restated_marching_cubes_closed_surface():
     z, y, x = np.meshgrid(ax, ax, ax, indexing="ij")
     f = np.sqrt(x * x + y * y + z * z).astype(np.float32)  # "in" = below iso: inside the sphere
     tris = mt.marching_cubes(f, (n, n, n), (0, 0, 0), 1.0, 1.0)
-    key = lambda p: tuple(np.round(p, 5))
-    sides = {}
-    for t in tris:
-        for k in range(3):
-            s = (key(t[k]), key(t[(k + 1) % 3]))
-            sides[s] = sides.get(s, 0) + 1
-    assert all(v == 1 for v in sides.values())
-    assert all((b, a) in sides for (a, b) in sides)
+    assert closed_and_oriented(tris, 1e-5)
     t = tris.astype(np.float64)
     vol = np.einsum("ij,ij->i", t[:, 0], np.cross(t[:, 1], t[:, 2])).sum() / 6.0
     assert abs(abs(vol) - 4 / 3 * np.pi * 8 ** 3) < 0.03 * 4 / 3 * np.pi * 8 ** 3
