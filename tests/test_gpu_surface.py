@@ -101,7 +101,7 @@ def test_gpu_marching_cubes_vertices_are_the_references():
 def test_gpu_mesh_of_a_sphere_is_closed():
     from graphics_b200.surface import surface_field
     sf = surface_field()
-    sf.surface_setup((0, 0, 0), (1, 1, 1), R_P, R_H, 1.0 / 16)
+    sf.surface_setup((0, 0, 0), (1, 1, 1), R_P, R_H, 1.0 / 32)
     num = sf.get_grid_num()
     mn = sf.get_grid_min()
     z, y, x = np.meshgrid(*[mn[a] + np.arange(num[a]) * sf.get_cell_size() for a in (2, 1, 0)], indexing="ij")
