@@ -21,18 +21,22 @@
 //                              det G and the node box the reference loops
 //                              over (its cell +- int(h_cell_num s_max), +1 on
 //                              the upper side, clamped to the grid)
-//   tile binning               the grid in 8x8x8-node tiles; every particle
+//   tile binning               the grid in 8x16x16-node tiles; every particle
 //                              is listed under each tile its box touches
 //                              (count, scan, emit, stable radix sort by tile:
 //                              within a tile in ascending particle order)
 //   k_sf_field                 one CTA per tile: its particles staged in
-//                              shared memory in chunks, each thread sums its
-//                              nodes' det G W(|G (x - c)|) over them in
-//                              particle order (no atomics: deterministic)
+//                              shared memory in chunks, each thread sums the
+//                              8 nodes of its x-row, det G W(|G (x - c)|),
+//                              over them in particle order (no atomics:
+//                              deterministic); along a row |G (x - c)|^2 is
+//                              a quadratic in the node index, so only the
+//                              nodes in its root interval are evaluated
 // The isotropic field is the same with G = I and the box +- h_cell_num.
 //
-// Marching cubes: k_mc_count (cube case -> triangle count from the case
-// table), exclusive scan, k_mc_emit (cut-edge vertices interpolated as
+// Marching cubes: k_mc_count (triangles per block of 256 cubes from the
+// case table), exclusive scan over the blocks, k_mc_emit (the block's cubes
+// again, an in-block scan, cut-edge vertices interpolated as
 // VertexInterp does, marching_cubes.cpp:39-40, in round-to-nearest float
 // ops; triangles in cube order z, y, x, each cube's in table order).  The
 // case table is built at start-up by mc_build_table() from first principles
@@ -51,9 +55,10 @@
 
 namespace {
 
-constexpr int TILE = 8;              // nodes per tile edge
-constexpr int TILE_N = TILE * TILE * TILE;
-constexpr int FT = 256;              // threads of the field kernel (2 nodes each)
+// field tiles: 8 (x) x 16 (y) x 16 (z) nodes, one thread per x-row of 8
+constexpr int TX = 8, TY = 16, TZ = 16;
+constexpr int FT = TY * TZ;          // threads of the field kernel
+constexpr int MCB = 256;             // cubes per marching-cubes block
 
 // ---------------- marching-cubes case table ----------------
 // Cube numbering of marching_cubes.cpp:9-31: vertex v at (x, y, z) bits
@@ -357,7 +362,8 @@ __global__ void __launch_bounds__(128) k_sf_kernel(SfParams P, const float4* pos
 // tiles a particle's box touches
 __device__ __forceinline__ int tile_span(int4 lo, int4 hi, int a) {
     const int l = (&lo.x)[a], h = (&hi.x)[a];
-    return h < l ? 0 : h / TILE - l / TILE + 1;
+    const int t = a == 0 ? TX : (a == 1 ? TY : TZ);
+    return h < l ? 0 : h / t - l / t + 1;
 }
 
 __global__ void k_sf_tile_count(const int4* box_lo, const int4* box_hi, int n, int* npair) {
@@ -374,9 +380,9 @@ __global__ void k_sf_tile_emit(SfParams P, const int4* box_lo, const int4* box_h
     const int4 lo = box_lo[i], hi = box_hi[i];
     if (hi.x < lo.x || hi.y < lo.y || hi.z < lo.z) return;
     int o = off[i];
-    for (int tz = lo.z / TILE; tz <= hi.z / TILE; ++tz)
-        for (int ty = lo.y / TILE; ty <= hi.y / TILE; ++ty)
-            for (int tx = lo.x / TILE; tx <= hi.x / TILE; ++tx) {
+    for (int tz = lo.z / TZ; tz <= hi.z / TZ; ++tz)
+        for (int ty = lo.y / TY; ty <= hi.y / TY; ++ty)
+            for (int tx = lo.x / TX; tx <= hi.x / TX; ++tx) {
                 ptile[o] = (tz * P.tiles[1] + ty) * P.tiles[0] + tx;
                 ppart[o] = i;
                 ++o;
@@ -401,66 +407,89 @@ __device__ __forceinline__ float sf_spline(const SfParams& P, float r) {
     return r < 0.5f * P.r_h ? fmaf(P.p3 * r, r * r, fmaf(P.p2, r * r, P.p1)) : P.p4 * hr * hr * hr;
 }
 
+// One CTA per tile, one thread per x-row of 8 nodes.  Along a row the
+// transformed offset u = G (x - c) is linear in the node index k, so
+// r^2(k) = |u0|^2 + 2 (u0.du) k + |du|^2 k^2 (du = G e_x cell, staged with the
+// particle) and r^2 <= r_h^2 holds on the interval between the quadratic's
+// roots (widened by one node each side); the nodes in it are tested directly
+// with r^2 from the polynomial in k.
 __global__ void __launch_bounds__(FT) k_sf_field(SfParams P, const int* tstart, const int* ppart, const float4* rec0,
                                                  const float4* rec1, const float4* rec2, const int4* box_lo,
                                                  const int4* box_hi, float* field) {
     const int t = blockIdx.x;
     const int tx = t % P.tiles[0], ty = (t / P.tiles[0]) % P.tiles[1], tz = t / (P.tiles[0] * P.tiles[1]);
-    __shared__ float4 s0[FT], s1[FT];
-    __shared__ float2 s2[FT];
+    __shared__ float4 s0[FT], s1[FT], s3[FT];
+    __shared__ float4 s2[FT];
     __shared__ int4 slo[FT], shi[FT];
-    int nid[2];
-    float acc[2] = {0.f, 0.f};
-    float px[2], py[2], pz[2];
-    bool valid[2];
-    for (int k = 0; k < 2; ++k) {
-        const int l = threadIdx.x + k * FT;
-        const int lx = l % TILE, ly = (l / TILE) % TILE, lz = l / (TILE * TILE);
-        const int x = tx * TILE + lx, y = ty * TILE + ly, z = tz * TILE + lz;
-        valid[k] = x < P.gnum[0] && y < P.gnum[1] && z < P.gnum[2];
-        nid[k] = valid[k] ? (z * P.gnum[1] + y) * P.gnum[0] + x : -1;
-        px[k] = P.gmin[0] + (float)x * P.cell;
-        py[k] = P.gmin[1] + (float)y * P.cell;
-        pz[k] = P.gmin[2] + (float)z * P.cell;
-    }
+    const int y = ty * TY + (int)(threadIdx.x % TY), z = tz * TZ + (int)(threadIdx.x / TY);
+    const int x0 = tx * TX;
+    const bool row = y < P.gnum[1] && z < P.gnum[2];
+    const int xlast = min(TX - 1, P.gnum[0] - 1 - x0);
+    const float px0 = P.gmin[0] + (float)x0 * P.cell;
+    const float py = P.gmin[1] + (float)y * P.cell, pz = P.gmin[2] + (float)z * P.cell;
+    const float rh = P.r_h, rh2 = P.r_h2, hh = 0.5f * P.r_h;
+    float acc[TX];
+#pragma unroll
+    for (int k = 0; k < TX; ++k) acc[k] = 0.f;
     const int a0 = tstart[t], a1 = tstart[t + 1];
-    const int lx0 = threadIdx.x % TILE, ly0 = (threadIdx.x / TILE) % TILE, lz0 = threadIdx.x / (TILE * TILE);
-    const int gx = tx * TILE + lx0, gy = ty * TILE + ly0;
-    const int gz0 = tz * TILE + lz0, gz1 = gz0 + FT / (TILE * TILE);
     for (int base = a0; base < a1; base += FT) {
         const int m = min(FT, a1 - base);
         __syncthreads();
         if ((int)threadIdx.x < m) {
             const int i = ppart[base + threadIdx.x];
+            const float4 g = rec1[i], g2 = rec2[i];
             s0[threadIdx.x] = rec0[i];
-            s1[threadIdx.x] = rec1[i];
-            const float4 r2 = rec2[i];
-            s2[threadIdx.x] = make_float2(r2.x, r2.y);
+            s1[threadIdx.x] = g;
+            const float dx = g.x * P.cell, dy = g.y * P.cell, dz = g.z * P.cell;
+            const float A = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            s2[threadIdx.x] = make_float4(g2.x, g2.y, 1.f / A, 0.f);
+            s3[threadIdx.x] = make_float4(dx, dy, dz, A);
             slo[threadIdx.x] = box_lo[i];
             shi[threadIdx.x] = box_hi[i];
         }
         __syncthreads();
+        if (!row) continue;
         for (int j = 0; j < m; ++j) {
-            const float4 c = s0[j], g = s1[j];
-            const float2 g2 = s2[j];
             const int4 lo = slo[j], hi = shi[j];
-            const bool inxy = gx >= lo.x && gx <= hi.x && gy >= lo.y && gy <= hi.y;
+            if (y < lo.y || y > hi.y || z < lo.z || z > hi.z) continue;
+            const int xa = max(lo.x - x0, 0), xb = min(hi.x - x0, xlast);
+            if (xa > xb) continue;
+            const float4 c = s0[j], g = s1[j], g2 = s2[j], du = s3[j];
+            const float vx = px0 - c.x, vy = py - c.y, vz = pz - c.z;
+            // G = [[gxx gxy gxz] [gxy gyy gyz] [gxz gyz gzz]]; u0 = G v
+            const float ux = fmaf(g.x, vx, fmaf(g.y, vy, g.z * vz));
+            const float uy = fmaf(g.y, vx, fmaf(g.w, vy, g2.x * vz));
+            const float uz = fmaf(g.z, vx, fmaf(g2.x, vy, g2.y * vz));
+            const float B = fmaf(ux, du.x, fmaf(uy, du.y, uz * du.z));
+            const float C0 = fmaf(ux, ux, fmaf(uy, uy, uz * uz));
+            const float disc = fmaf(B, B, -du.w * (C0 - rh2));
+            // min_k r^2 = r_h^2 - disc / |du|^2: the row misses the ellipsoid
+            // (kept when within rounding of touching it)
+            if (disc < -1e-5f * rh2 * du.w) continue;
+            const float sq = disc > 0.f ? disc * rsqrtf(disc) : 0.f;
+            const int ka = max(xa, (int)floorf((-B - sq) * g2.z) - 1);
+            const int kb = min(xb, (int)ceilf((-B + sq) * g2.z) + 1);
+            const float B2 = 2.f * B;
 #pragma unroll
-            for (int k = 0; k < 2; ++k) {
-                const int gz = k ? gz1 : gz0;
-                if (!(inxy && gz >= lo.z && gz <= hi.z && valid[k])) continue;
-                const float vx = px[k] - c.x, vy = py[k] - c.y, vz = pz[k] - c.z;
-                // G v with G = [[gxx gxy gxz] [gxy gyy gyz] [gxz gyz gzz]]
-                const float ux = fmaf(g.x, vx, fmaf(g.y, vy, g.z * vz));
-                const float uy = fmaf(g.y, vx, fmaf(g.w, vy, g2.x * vz));
-                const float uz = fmaf(g.z, vx, fmaf(g2.x, vy, g2.y * vz));
-                const float r2 = fmaf(ux, ux, fmaf(uy, uy, uz * uz));
-                if (r2 <= P.r_h2) acc[k] += c.w * sf_spline(P, sqrtf(r2));
+            for (int k = 0; k < TX; ++k) {
+                if (k < ka || k > kb) continue;
+                const float fk = (float)k;
+                const float r2 = fmaf(fmaf(du.w, fk, B2), fk, C0);
+                if (!(r2 <= rh2)) continue;
+                // ker_spline (surface_field.cpp:235-249), times the particle volume
+                const float r = r2 > 0.f ? r2 * rsqrtf(r2) : 0.f;
+                const float hr = rh - r;
+                const float w = r < hh ? fmaf(P.p3 * r, r2, fmaf(P.p2, r2, P.p1)) : P.p4 * hr * hr * hr;
+                acc[k] = fmaf(c.w, w, acc[k]);
             }
         }
     }
-    for (int k = 0; k < 2; ++k)
-        if (valid[k]) field[nid[k]] = acc[k];
+    if (row) {
+        const size_t base = ((size_t)z * P.gnum[1] + y) * P.gnum[0] + x0;
+#pragma unroll
+        for (int k = 0; k < TX; ++k)
+            if (k <= xlast) field[base + k] = acc[k];
+    }
 }
 
 // ---------------- marching cubes ----------------
@@ -493,32 +522,66 @@ __device__ __forceinline__ void mc_corners(const McParams& M, const float* f, lo
     }
 }
 
-__global__ void k_mc_count(McParams M, const float* f, long long ncubes, int* ntri) {
-    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= ncubes) return;
-    int x, y, z;
-    float v[8];
-    mc_corners(M, f, c, x, y, z, v);
+__device__ __forceinline__ int mc_case(const McParams& M, const float v[8]) {
     int cs = 0;
 #pragma unroll
     for (int k = 0; k < 8; ++k) cs |= (v[k] < M.iso) << k;
-    ntri[c] = c_ntri[cs];
+    return cs;
 }
 
-__global__ void k_mc_emit(McParams M, const float* f, long long ncubes, const int* ntri, const int* off,
-                          float* out) {
-    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= ncubes || ntri[c] == 0) return;
-    int x, y, z;
-    float v[8];
-    mc_corners(M, f, c, x, y, z, v);
-    int cs = 0;
+// pass 1: triangles per block of MCB consecutive cubes
+__global__ void __launch_bounds__(MCB) k_mc_count(McParams M, const float* f, long long ncubes, int* bcount) {
+    const long long c = (long long)blockIdx.x * MCB + threadIdx.x;
+    int n = 0;
+    if (c < ncubes) {
+        int x, y, z;
+        float v[8];
+        mc_corners(M, f, c, x, y, z, v);
+        n = c_ntri[mc_case(M, v)];
+    }
+    __shared__ int sh[MCB / 32];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) cs |= (v[k] < M.iso) << k;
+    for (int o = 16; o > 0; o >>= 1) n += __shfl_down_sync(0xffffffffu, n, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = n;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int t = 0;
+        for (int w = 0; w < MCB / 32; ++w) t += sh[w];
+        bcount[blockIdx.x] = t;
+    }
+}
+
+// pass 2: the block's cubes again, their offsets by an in-block scan after
+// the block's offset, triangles written in cube order
+__global__ void __launch_bounds__(MCB) k_mc_emit(McParams M, const float* f, long long ncubes, const int* boff,
+                                                 float* out) {
+    const long long c = (long long)blockIdx.x * MCB + threadIdx.x;
+    int x = 0, y = 0, z = 0, cs = 0, n = 0;
+    float v[8];
+    if (c < ncubes) {
+        mc_corners(M, f, c, x, y, z, v);
+        cs = mc_case(M, v);
+        n = c_ntri[cs];
+    }
+    // exclusive scan of n over the block (warp scans, then warp totals)
+    __shared__ int wsum[MCB / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int inc = n;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += t;
+    }
+    if (lane == 31) wsum[wid] = inc;
+    __syncthreads();
+    int before = 0;
+    for (int w = 0; w < wid; ++w) before += wsum[w];
+    if (n == 0) return;
+    const long long first = (long long)boff[blockIdx.x] + before + inc - n;
     const float lo[3] = {M.cx_lo[x], M.cy_lo[y], M.cz_lo[z]};
     const float hi[3] = {M.cx_hi[x], M.cy_hi[y], M.cz_hi[z]};
-    float* o = out + 9 * (long long)off[c];
-    for (int t = 0; t < 3 * ntri[c]; ++t) {
+    float* o = out + 9 * first;
+    for (int t = 0; t < 3 * n; ++t) {
         const int e = c_tri[cs][t];
         const int a = c_edge[e][0], b = c_edge[e][1];
         const float va = v[a], vb = v[b];
@@ -562,8 +625,8 @@ struct sphgpu_surface {
     int* tstart = nullptr;
     // marching cubes
     long long cubecap = 0, tricap = 0, ntris = 0;
-    int* ntri = nullptr;
-    int* toff = nullptr;
+    int* ntri = nullptr;  // triangles per block of MCB cubes
+    int* toff = nullptr;  // and the blocks' offsets
     float* tris = nullptr;
     float* coords = nullptr;  // 6 coordinate tables
     void* tmpbuf = nullptr;
@@ -735,7 +798,7 @@ int sphgpu_surface_create(const double* mn, const double* mx, double r_p, double
         P.gmin[a] = (float)s->gmin[a];
         P.gmin_d[a] = s->gmin[a];
         P.gnum[a] = s->gnum[a];
-        P.tiles[a] = (s->gnum[a] + TILE - 1) / TILE;
+        P.tiles[a] = (s->gnum[a] + (a == 0 ? TX : (a == 1 ? TY : TZ)) - 1) / (a == 0 ? TX : (a == 1 ? TY : TZ));
     }
     P.gdiv_d = 1.0 / cell_size;
     P.cell = (float)cell_size;
@@ -859,9 +922,10 @@ long long sphgpu_surface_mesh(sphgpu_surface_t s, float iso, int ref_rows, float
         s->err = "more than 2^31 - 1 cubes";
         return SPHGPU_EINVAL;
     }
-    if (ncubes > s->cubecap) {
-        if (salloc(s, &s->ntri, (size_t)ncubes) || salloc(s, &s->toff, (size_t)ncubes)) return SPHGPU_ENOMEM;
-        s->cubecap = ncubes;
+    const long long nblocks = (ncubes + MCB - 1) / MCB;
+    if (nblocks > s->cubecap) {
+        if (salloc(s, &s->ntri, (size_t)nblocks) || salloc(s, &s->toff, (size_t)nblocks)) return SPHGPU_ENOMEM;
+        s->cubecap = nblocks;
     }
     // cube extents per index: nodes at min + i * cell; with ref_rows the
     // reference's running float sums (marching_cubes.cpp:53-66)
@@ -900,22 +964,22 @@ long long sphgpu_surface_mesh(sphgpu_surface_t s, float iso, int ref_rows, float
     M.cy_hi = s->coords + 3 * (size_t)m;
     M.cz_lo = s->coords + 4 * (size_t)m;
     M.cz_hi = s->coords + 5 * (size_t)m;
-    k_mc_count<<<nblk(ncubes, 256), 256, 0, st>>>(M, s->field, ncubes, s->ntri);
+    k_mc_count<<<(int)nblocks, MCB, 0, st>>>(M, s->field, ncubes, s->ntri);
     size_t b = 0;
-    cub::DeviceScan::ExclusiveSum(nullptr, b, s->ntri, s->toff, (int)ncubes, st);
+    cub::DeviceScan::ExclusiveSum(nullptr, b, s->ntri, s->toff, (int)nblocks, st);
     if (int r = ensure_tmp(s, b)) return r;
-    cub::DeviceScan::ExclusiveSum(s->tmpbuf, b, s->ntri, s->toff, (int)ncubes, st);
+    cub::DeviceScan::ExclusiveSum(s->tmpbuf, b, s->ntri, s->toff, (int)nblocks, st);
     int last_off = 0;
     int last_n = 0;
-    SCK(cudaMemcpyAsync(&last_off, s->toff + ncubes - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
-    SCK(cudaMemcpyAsync(&last_n, s->ntri + ncubes - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SCK(cudaMemcpyAsync(&last_off, s->toff + nblocks - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SCK(cudaMemcpyAsync(&last_n, s->ntri + nblocks - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
     SCK(cudaStreamSynchronize(st));
     const long long total = (long long)last_off + last_n;  // < 2^31: 5 triangles per cube at most
     if (total > s->tricap) {
         if (salloc(s, &s->tris, 9 * (size_t)total)) return SPHGPU_ENOMEM;
         s->tricap = total;
     }
-    if (total > 0) k_mc_emit<<<nblk(ncubes, 256), 256, 0, st>>>(M, s->field, ncubes, s->ntri, s->toff, s->tris);
+    if (total > 0) k_mc_emit<<<(int)nblocks, MCB, 0, st>>>(M, s->field, ncubes, s->toff, s->tris);
     SCK(cudaGetLastError());
     SCK(cudaStreamSynchronize(st));
     s->ntris = total;
