@@ -34,9 +34,11 @@
 //                              nodes in its root interval are evaluated
 // The isotropic field is the same with G = I and the box +- h_cell_num.
 //
-// Marching cubes: k_mc_count (triangles per block of 256 cubes from the
-// case table), exclusive scan over the blocks, k_mc_emit (the block's cubes
-// again, an in-block scan, cut-edge vertices interpolated as
+// Marching cubes: k_mc_count (each thread 4 consecutive x-cubes: their case
+// bytes, and the triangles per block from the case table), exclusive scan
+// over the blocks, k_mc_emit (the block's case bytes again, an in-block
+// scan; cubes with triangles gather their corners; cut-edge vertices
+// interpolated as
 // VertexInterp does, marching_cubes.cpp:39-40, in round-to-nearest float
 // ops; triangles in cube order z, y, x, each cube's in table order).  The
 // case table is built at start-up by mc_build_table() from first principles
@@ -58,7 +60,8 @@ namespace {
 // field tiles: 8 (x) x 16 (y) x 16 (z) nodes, one thread per x-row of 8
 constexpr int TX = 8, TY = 16, TZ = 16;
 constexpr int FT = TY * TZ;          // threads of the field kernel
-constexpr int MCB = 256;             // cubes per marching-cubes block
+constexpr int MCB = 256;             // threads per marching-cubes block
+constexpr int MCX = 4;               // consecutive x-cubes per marching-cubes thread
 
 // ---------------- marching-cubes case table ----------------
 // Cube numbering of marching_cubes.cpp:9-31: vertex v at (x, y, z) bits
@@ -529,15 +532,43 @@ __device__ __forceinline__ int mc_case(const McParams& M, const float v[8]) {
     return cs;
 }
 
-// pass 1: triangles per block of MCB consecutive cubes
-__global__ void __launch_bounds__(MCB) k_mc_count(McParams M, const float* f, long long ncubes, int* bcount) {
-    const long long c = (long long)blockIdx.x * MCB + threadIdx.x;
+// A thread takes MCX consecutive cubes of one x-row (a group); groups are
+// numbered row by row, so group order is cube order.
+__device__ __forceinline__ void mc_group(const McParams& M, long long g, int gpr, int& x0, int& xe, int& y, int& z) {
+    const int ncx = M.res[0] - 1, ncy = M.res[1] - 1;
+    const long long r = g / gpr;
+    x0 = (int)(g % gpr) * MCX;
+    xe = min(x0 + MCX, ncx);
+    y = (int)(r % ncy);
+    z = (int)(r / ncy);
+}
+
+// pass 1: the case of every cube (one byte) and the triangles per block of
+// MCB groups; a group reads its 4 node rows once (MCX + 1 nodes each)
+__global__ void __launch_bounds__(MCB) k_mc_count(McParams M, const float* f, long long ngroups, int gpr,
+                                                  unsigned char* cases, int* bcount) {
+    const long long g = (long long)blockIdx.x * MCB + threadIdx.x;
     int n = 0;
-    if (c < ncubes) {
-        int x, y, z;
-        float v[8];
-        mc_corners(M, f, c, x, y, z, v);
-        n = c_ntri[mc_case(M, v)];
+    if (g < ngroups) {
+        int x0, xe, y, z;
+        mc_group(M, g, gpr, x0, xe, y, z);
+        const int ylo = M.ref_rows ? max(y - 1, 0) : y, yhi = M.ref_rows ? y : y + 1;
+        const long long plane = (long long)M.res[0] * M.res[1];
+        // rows of vertices 0, 1, 2, 3 (x low side; 4..7 are the same rows at x + 1)
+        const float* r0 = f + z * plane + (long long)ylo * M.res[0];
+        const float* r1 = f + (z + 1) * plane + (long long)ylo * M.res[0];
+        const float* r2 = f + (z + 1) * plane + (long long)yhi * M.res[0];
+        const float* r3 = f + z * plane + (long long)yhi * M.res[0];
+        int lo = (r0[x0] < M.iso) | ((r1[x0] < M.iso) << 1) | ((r2[x0] < M.iso) << 2) | ((r3[x0] < M.iso) << 3);
+        const long long c0 = ((long long)z * (M.res[1] - 1) + y) * (M.res[0] - 1);
+        for (int x = x0; x < xe; ++x) {
+            const int hi =
+                (r0[x + 1] < M.iso) | ((r1[x + 1] < M.iso) << 1) | ((r2[x + 1] < M.iso) << 2) | ((r3[x + 1] < M.iso) << 3);
+            const int cs = lo | (hi << 4);
+            cases[c0 + x] = (unsigned char)cs;
+            n += c_ntri[cs];
+            lo = hi;
+        }
     }
     __shared__ int sh[MCB / 32];
 #pragma unroll
@@ -551,19 +582,18 @@ __global__ void __launch_bounds__(MCB) k_mc_count(McParams M, const float* f, lo
     }
 }
 
-// pass 2: the block's cubes again, their offsets by an in-block scan after
-// the block's offset, triangles written in cube order
-__global__ void __launch_bounds__(MCB) k_mc_emit(McParams M, const float* f, long long ncubes, const int* boff,
-                                                 float* out) {
-    const long long c = (long long)blockIdx.x * MCB + threadIdx.x;
-    int x = 0, y = 0, z = 0, cs = 0, n = 0;
-    float v[8];
-    if (c < ncubes) {
-        mc_corners(M, f, c, x, y, z, v);
-        cs = mc_case(M, v);
-        n = c_ntri[cs];
+// pass 2: the cases again, offsets by an in-block scan after the block's
+// offset; only cubes with triangles gather their corners
+__global__ void __launch_bounds__(MCB) k_mc_emit(McParams M, const float* f, long long ngroups, int gpr,
+                                                 const unsigned char* cases, const int* boff, float* out) {
+    const long long g = (long long)blockIdx.x * MCB + threadIdx.x;
+    int x0 = 0, xe = 0, y = 0, z = 0, n = 0;
+    long long c0 = 0;
+    if (g < ngroups) {
+        mc_group(M, g, gpr, x0, xe, y, z);
+        c0 = ((long long)z * (M.res[1] - 1) + y) * (M.res[0] - 1);
+        for (int x = x0; x < xe; ++x) n += c_ntri[cases[c0 + x]];
     }
-    // exclusive scan of n over the block (warp scans, then warp totals)
     __shared__ int wsum[MCB / 32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     int inc = n;
@@ -577,22 +607,31 @@ __global__ void __launch_bounds__(MCB) k_mc_emit(McParams M, const float* f, lon
     int before = 0;
     for (int w = 0; w < wid; ++w) before += wsum[w];
     if (n == 0) return;
-    const long long first = (long long)boff[blockIdx.x] + before + inc - n;
-    const float lo[3] = {M.cx_lo[x], M.cy_lo[y], M.cz_lo[z]};
-    const float hi[3] = {M.cx_hi[x], M.cy_hi[y], M.cz_hi[z]};
-    float* o = out + 9 * first;
-    for (int t = 0; t < 3 * n; ++t) {
-        const int e = c_tri[cs][t];
-        const int a = c_edge[e][0], b = c_edge[e][1];
-        const float va = v[a], vb = v[b];
-        // VertexInterp (marching_cubes.cpp:39-40)
-        const float mu = __fdiv_rn(__fsub_rn(M.iso, va), __fsub_rn(vb, va));
+    long long first = (long long)boff[blockIdx.x] + before + inc - n;
+    for (int x = x0; x < xe; ++x) {
+        const int cs = cases[c0 + x];
+        const int nc = c_ntri[cs];
+        if (!nc) continue;
+        int cx, cy, cz;
+        float v[8];
+        mc_corners(M, f, c0 + x, cx, cy, cz, v);
+        const float lo[3] = {M.cx_lo[cx], M.cy_lo[cy], M.cz_lo[cz]};
+        const float hi[3] = {M.cx_hi[cx], M.cy_hi[cy], M.cz_hi[cz]};
+        float* o = out + 9 * first;
+        for (int t = 0; t < 3 * nc; ++t) {
+            const int e = c_tri[cs][t];
+            const int a = c_edge[e][0], b = c_edge[e][1];
+            const float va = v[a], vb = v[b];
+            // VertexInterp (marching_cubes.cpp:39-40)
+            const float mu = __fdiv_rn(__fsub_rn(M.iso, va), __fsub_rn(vb, va));
 #pragma unroll
-        for (int ax = 0; ax < 3; ++ax) {
-            const float pa = c_vert[a][ax] ? hi[ax] : lo[ax];
-            const float pb = c_vert[b][ax] ? hi[ax] : lo[ax];
-            o[3 * t + ax] = __fadd_rn(pa, __fmul_rn(mu, __fsub_rn(pb, pa)));
+            for (int ax = 0; ax < 3; ++ax) {
+                const float pa = c_vert[a][ax] ? hi[ax] : lo[ax];
+                const float pb = c_vert[b][ax] ? hi[ax] : lo[ax];
+                o[3 * t + ax] = __fadd_rn(pa, __fmul_rn(mu, __fsub_rn(pb, pa)));
+            }
         }
+        first += nc;
     }
 }
 
@@ -625,8 +664,10 @@ struct sphgpu_surface {
     int* tstart = nullptr;
     // marching cubes
     long long cubecap = 0, tricap = 0, ntris = 0;
-    int* ntri = nullptr;  // triangles per block of MCB cubes
+    int* ntri = nullptr;  // triangles per block of MCB cube groups
     int* toff = nullptr;  // and the blocks' offsets
+    unsigned char* cases = nullptr;  // case byte per cube
+    long long casecap = 0;
     float* tris = nullptr;
     float* coords = nullptr;  // 6 coordinate tables
     void* tmpbuf = nullptr;
@@ -850,7 +891,7 @@ int sphgpu_surface_destroy(sphgpu_surface_t s) {
     cudaSetDevice(s->device);
     void* ptrs[] = {s->field, s->xyz, s->pos, s->rec0, s->rec1, s->rec2, s->blo, s->bhi, s->key, s->slot, s->tmp, s->sorted,
                     s->npair, s->poff, s->pcnt, s->pstart, s->bad, s->ptile, s->ppart, s->ptile_s, s->ppart_s,
-                    s->tstart, s->ntri, s->toff, s->tris, s->coords, s->tmpbuf};
+                    s->tstart, s->ntri, s->toff, s->cases, s->tris, s->coords, s->tmpbuf};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -922,10 +963,16 @@ long long sphgpu_surface_mesh(sphgpu_surface_t s, float iso, int ref_rows, float
         s->err = "more than 2^31 - 1 cubes";
         return SPHGPU_EINVAL;
     }
-    const long long nblocks = (ncubes + MCB - 1) / MCB;
+    const int gpr = (g[0] - 1 + MCX - 1) / MCX;  // groups per x-row
+    const long long ngroups = (long long)gpr * (g[1] - 1) * (g[2] - 1);
+    const long long nblocks = (ngroups + MCB - 1) / MCB;
     if (nblocks > s->cubecap) {
         if (salloc(s, &s->ntri, (size_t)nblocks) || salloc(s, &s->toff, (size_t)nblocks)) return SPHGPU_ENOMEM;
         s->cubecap = nblocks;
+    }
+    if (ncubes > s->casecap) {
+        if (salloc(s, &s->cases, (size_t)ncubes)) return SPHGPU_ENOMEM;
+        s->casecap = ncubes;
     }
     // cube extents per index: nodes at min + i * cell; with ref_rows the
     // reference's running float sums (marching_cubes.cpp:53-66)
@@ -964,7 +1011,7 @@ long long sphgpu_surface_mesh(sphgpu_surface_t s, float iso, int ref_rows, float
     M.cy_hi = s->coords + 3 * (size_t)m;
     M.cz_lo = s->coords + 4 * (size_t)m;
     M.cz_hi = s->coords + 5 * (size_t)m;
-    k_mc_count<<<(int)nblocks, MCB, 0, st>>>(M, s->field, ncubes, s->ntri);
+    k_mc_count<<<(int)nblocks, MCB, 0, st>>>(M, s->field, ngroups, gpr, s->cases, s->ntri);
     size_t b = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, b, s->ntri, s->toff, (int)nblocks, st);
     if (int r = ensure_tmp(s, b)) return r;
@@ -979,7 +1026,7 @@ long long sphgpu_surface_mesh(sphgpu_surface_t s, float iso, int ref_rows, float
         if (salloc(s, &s->tris, 9 * (size_t)total)) return SPHGPU_ENOMEM;
         s->tricap = total;
     }
-    if (total > 0) k_mc_emit<<<(int)nblocks, MCB, 0, st>>>(M, s->field, ncubes, s->toff, s->tris);
+    if (total > 0) k_mc_emit<<<(int)nblocks, MCB, 0, st>>>(M, s->field, ngroups, gpr, s->cases, s->toff, s->tris);
     SCK(cudaGetLastError());
     SCK(cudaStreamSynchronize(st));
     s->ntris = total;
