@@ -18,7 +18,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
          "-I" + os.path.join(PKG, "..", "include")]
 SOURCES = ["sph_grid.cu", "sph_dfsph.cu", "sph_wcsph.cu", "sph_pci_ii.cu", "sph_iisph.cu", "sph_batch.cu", "sph_mlp.cu", "sph_engine.cu", "sph_noalloc.cu",
-           "sph_rigid.cu", "sph_surface.cu"]
+           "sph_rigid.cu", "sph_surface.cu", "sph_vortex.cu"]
 
 
 def _newer(dst, srcs):

@@ -121,6 +121,7 @@ struct sphgpu_scene {
     float* h_rstate = nullptr;    // [cap * 25] states (SphRigidState layout)
     double* h_rout = nullptr;     // [cap * 6 + 1] joined force, torque; dt
     int rigid_cap = 0;            // capacity of the per-solid arrays
+    int vort_last = 0;            // vorticity option of the last DFSPH step (its carried state in cA)
     sphgpu_rigid_fn rigid_fn = nullptr;
     void* rigid_user = nullptr;
     int rigid_fail = 0;
@@ -294,6 +295,7 @@ int alloc_scene(sphgpu_scene* h) {
     r |= dalloc(h, &d.acc, n); r |= dalloc(h, &d.kr, n); r |= dalloc(h, &d.kappa, n); r |= dalloc(h, &d.kappav, n);
     r |= dalloc(h, &d.pv, 2 * (size_t)n); r |= dalloc(h, &d.pk, n); r |= dalloc(h, &d.prv, 2 * (size_t)n);
     r |= dalloc(h, &d.ksum, n); r |= dalloc(h, &d.aux0, n); r |= dalloc(h, &d.aux1, n);
+    r |= dalloc(h, &d.vA, n); r |= dalloc(h, &d.vB, n);
     r |= dalloc(h, &d.aux4, n); r |= dalloc(h, &d.kwarm, n); r |= dalloc(h, &d.hist, n); r |= dalloc(h, &d.wsbuf, n);
     r |= dalloc(h, &d.pos_s, n); r |= dalloc(h, &d.vel_s, n); r |= dalloc(h, &d.gid_s, n);
     r |= dalloc(h, &d.hist_s, n);
@@ -356,7 +358,7 @@ void free_rigid(sphgpu_scene* h) {
 
 void free_scene(sphgpu_scene* h) {
     DevScene& d = h->d;
-    void* ptrs[] = {d.pos, d.vel, d.gid, d.rho, d.alpha, d.vadv, d.pv, d.pk, d.prv, d.bpv, d.kappav, d.acc, d.kr, d.kappa, d.ksum, d.aux0,
+    void* ptrs[] = {d.pos, d.vel, d.gid, d.rho, d.alpha, d.vadv, d.pv, d.pk, d.prv, d.bpv, d.kappav, d.acc, d.kr, d.kappa, d.ksum, d.vA, d.vB, d.aux0,
                     d.aux1, d.aux4, d.kwarm, d.hist, d.wsbuf, d.pos_s, d.vel_s, d.gid_s, d.hist_s, d.key, d.slot, d.tmp,
                     d.cA, d.cB, d.cC, d.cA_s, d.cB_s, d.cC_s, d.ap, d.pl2, d.ivs,
                     d.bsid, d.bnbr, d.bncount, d.bivs, d.bivo,
@@ -521,6 +523,11 @@ int enq_df_part1(sphgpu_scene* h, bool capturing) {
         launch(h, "cfl", st, [&] { launch_cfl(d, h->cap, h->P.cfl_factor, h->P.particle_d, h->P.dt_max, h->P.dt_min, st); });
     const int ws = h->mlp ? h->ws_mode : 0;
     launch(h, "df_forces", st, [&] { launch_df_forces(d, h->c, h->cap, 0, st, h->tune.forces); });
+    if (h->P.enable_vortex)
+        launch(h, "vortex", st, [&] {
+            launch_vortex_second(d, h->c, h->P.enable_vortex, h->P.vort_alpha, h->P.vort_zeta, h->P.vort_nu_t,
+                                 h->P.spacing_r, h->cap, st);
+        });
     if (ws == 1 || ws == 3) {
         launch(h, "ws_features", st, [&] {
             launch_ws_features(d, h->c, h->mlp->m, ws == 1 ? 1 : 2, h->P.dt_max, h->alpha_ref, nullptr, h->xn, h->cap,
@@ -555,9 +562,12 @@ int enq_df_part2(sphgpu_scene* h, bool capturing) {
     DevScene& d = h->d;
     cudaStream_t st = h->stream;
     enq_boundary_update(h, st);
-    enq_ns(h, 1, 1, st);
+    const int vort = h->P.enable_vortex ? 2 : 0;  // carry cA (w or n0) through the sort
+    enq_ns(h, 1 | vort, 1, st, 1 | vort);
     int r = enq_df_div_loop(h, capturing);
     if (r) return r;
+    if (h->P.enable_vortex == 3)
+        launch(h, "vortex", st, [&] { launch_vortex_after_div(d, h->c, h->P.spacing_r, h->cap, st); });
     CK(cudaMemcpyAsync(h->h_stats, d.st, sizeof(DevStats), cudaMemcpyDeviceToHost, st));
     return 0;
 }
@@ -850,6 +860,13 @@ int enq_steps(sphgpu_scene* h, int solver, int nsteps) {
         h->err = "dynamic solids are coupled in the DFSPH step";
         return SPHGPU_ENOTIMPL;
     }
+    if (solver == SPHGPU_DFSPH && h->P.enable_vortex) {
+        if (h->P.enable_vortex < 0 || h->P.enable_vortex > 3) { h->err = "enable_vortex is 0..3"; return SPHGPU_EINVAL; }
+        if (h->nscenes > 1 || (h->mlp && h->ws_mode)) {
+            h->err = "the vorticity options run in the plain single-scene DFSPH step";
+            return SPHGPU_ENOTIMPL;
+        }
+    }
     if (h->R.nd && h->record_ksum) {
         h->err = "record_kappa_sum cannot be combined with dynamic solids";
         return SPHGPU_EINVAL;
@@ -889,6 +906,7 @@ int enq_steps(sphgpu_scene* h, int solver, int nsteps) {
         h->ns_valid = false;
         return 0;
     }
+    const bool entering = h->last_solver != solver;
     h->last_solver = solver;
     if (solver == SPHGPU_DFSPH) {
         if (!h->ns_valid) {
@@ -896,8 +914,15 @@ int enq_steps(sphgpu_scene* h, int solver, int nsteps) {
             if (r) return r;
         }
         const bool dyn = h->R.nd > 0;
+        if (h->P.enable_vortex != h->vort_last || (h->P.enable_vortex && entering)) {
+            // a vorticity option starts from zero carried vectors
+            CK(cudaMemsetAsync(h->d.cA, 0, sizeof(float4) * h->cap, h->stream));
+            CK(cudaMemsetAsync(h->d.cA_s, 0, sizeof(float4) * h->cap, h->stream));
+            h->vort_last = h->P.enable_vortex;
+        }
         for (int s = 0; s < nsteps; ++s) {
-            const int key = (h->mlp ? h->ws_mode : 0) | (h->record_ksum ? 4 : 0) | (h->P.cfl ? 8 : 0);
+            const int key = (h->mlp ? h->ws_mode : 0) | (h->record_ksum ? 4 : 0) | (h->P.cfl ? 8 : 0) |
+                            (h->P.enable_vortex << 6);
             if (h->use_graphs && !h->prof.on) {
                 cudaGraphExec_t ex;
                 int r = dyn ? graph_for(h, key | 16, &ex, df1_graph_build) : graph_for(h, key, &ex, df_graph_build);
@@ -1551,6 +1576,10 @@ int sphgpu_get_fluid(sphgpu_t h, const char* field, float* out) {
         comps = 3;
     }
     else if (f == "acce_presure") { src = d.ap; f4 = true; comps = 3; }
+    // DFSPH vorticity options' vectors (see sph_vortex.cu)
+    else if (f == "omega" || f == "deltaVorticity") { src = d.vA; f4 = true; comps = 3; }
+    else if (f == "dOmega" || f == "psi") { src = d.vB; f4 = true; comps = 3; }
+    else if (f == "angular_velocity" || f == "n0Vorticity") { src = d.cA; f4 = true; comps = 3; }
     else if (f == "advectionVelocity") {
         CK(cudaMemcpy2D(d.vadv, sizeof(float4), d.pv + 1, 2 * sizeof(float4), sizeof(float4), n,
                         cudaMemcpyDeviceToDevice));
@@ -1782,7 +1811,7 @@ int sphgpu_stage(sphgpu_t h, const char* name, SphStepStats* stats) {
         if (h->R.nd && mode != 1) { h->err = "dynamic solids are coupled in the DFSPH step"; return SPHGPU_ENOTIMPL; }
         enq_boundary_update(h, st);
         if (h->in_staging) {
-            enq_ns(h, 0, mode, st);
+            enq_ns(h, 0, mode, st, h->P.enable_vortex ? 3 : 1);
             h->in_staging = false;
         } else {
             if (h->R.nd) {
@@ -1802,6 +1831,9 @@ int sphgpu_stage(sphgpu_t h, const char* name, SphStepStats* stats) {
         if (h->in_staging) { h->err = "run neighbourSearch first"; return SPHGPU_EINVAL; }
         if (h->P.cfl) launch_cfl(d, h->cap, h->P.cfl_factor, h->P.particle_d, h->P.dt_max, h->P.dt_min, st);
         launch_df_forces(d, h->c, h->cap, 0, st);
+        if (h->P.enable_vortex)
+            launch_vortex_second(d, h->c, h->P.enable_vortex, h->P.vort_alpha, h->P.vort_zeta, h->P.vort_nu_t,
+                                 h->P.spacing_r, h->cap, st);
         if (h->mlp && h->ws_mode == 1) {
             launch_ws_features(d, h->c, h->mlp->m, 1, h->P.dt_max, h->alpha_ref, nullptr, h->xn, h->cap, st);
             launch_ws_infer(d, h->c, h->mlp->m, h->xn, h->cap, h->sm_count, st);
@@ -1818,13 +1850,14 @@ int sphgpu_stage(sphgpu_t h, const char* name, SphStepStats* stats) {
         if (dyn && h->mlp && h->ws_mode == 1) launch_ws_post(d, h->c, nullptr, h->cap, st);
         // integrate into staging (the reference updates positions in place)
         cudaMemsetAsync(d.cell_count, 0, sizeof(int) * ((size_t)h->g.nkeys + 1), st);
-        launch_hash(d, h->g, 1, h->cap, st);
+        launch_hash(d, h->g, h->P.enable_vortex ? 3 : 1, h->cap, st);
         h->in_staging = true;
         h->ns_valid = false;
     } else if (s == "DF_divergenceFreeSolver") {
         if (h->in_staging) { h->err = "run neighbourSearch first"; return SPHGPU_EINVAL; }
         r = enq_df_div_loop(h, false);
         if (r) return r;
+        if (h->P.enable_vortex == 3) launch_vortex_after_div(d, h->c, h->P.spacing_r, h->cap, st);
     } else if (s == "VF_prepareAttribute") {
         if ((r = ensure_iv_boundary(h))) return r;
         enq_iv_prepare(h, h->in_staging, st);

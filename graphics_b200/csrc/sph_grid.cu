@@ -45,6 +45,7 @@ __global__ void __launch_bounds__(NT) k_hash(DevScene s, GridGeom g, int integra
             s.vel_s[i] = v;
             s.gid_s[i] = s.gid[i];
             s.hist_s[i] = s.hist[i];
+            if (integrate & 2) s.cA_s[i] = s.cA[i];  // DFSPH vorticity state carried through the sort
         } else {
             p = s.pos_s[i];
         }

@@ -76,6 +76,8 @@ struct DevScene {
     float* kappa;       // DFkappa of the last density iteration
     float* kappav;      // DFkappaV of the last divergence iteration
     float* ksum;        // summed kappa over the density loop (warm-start label)
+    float4* vA;         // DFSPH vorticity options: per-particle scratch vectors
+    float4* vB;
     float* aux0;        // rho_adv (DFSPH density loop)
     float* aux1;        // divergence deviation (DFSPH), rho_adv (IISPH_M)
     float4* aux4;       // PCISPH predicted position; scratch for transfers
@@ -242,6 +244,14 @@ void launch_iv_sweep_b(const DevScene& s, const SolverConst& c, int phase, int d
                        int max_it, unsigned long long cond_handle, int use_handle, int n_max, int bs, cudaStream_t st);
 // acce_presure, v += acce_presure dt, x += v dt into the staging arrays (carried: v_adv)
 void launch_iv_integrate(const DevScene& s, int n_max, cudaStream_t st);
+
+// ---- DFSPH vorticity options (sph_vortex.cu) ----
+// after the non-pressure forces: mode 1 TRRV, 2 micropolar (velocity and
+// v_adv refined), 3 the vorticity at the start of the step (into cA)
+void launch_vortex_second(const DevScene& s, const SolverConst& c, int mode, float alpha, float zeta, float nu_t,
+                          float spacing, int n_max, cudaStream_t st);
+// mode 3 after the divergence loop: stream-function correction of the velocity
+void launch_vortex_after_div(const DevScene& s, const SolverConst& c, float spacing, int n_max, cudaStream_t st);
 
 // ---- dynamic rigid solids (sph_rigid.cu) ----
 // updatePaticles for every dynamic solid, then a counting sort of the whole

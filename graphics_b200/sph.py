@@ -29,7 +29,7 @@ SOLVERS = {"wcsph": _lib.WCSPH, "pcisph": _lib.PCISPH, "iisph_m": _lib.IISPH_M, 
 
 VEC_FIELDS = ("position", "velocity", "vel_adv", "acce_adv", "acceleration", "ws_hist", "acce_pressure",
               "pos_prediction", "dii", "sum_dijpj", "ii_vel_adv", "acce_presure", "advectionAcceleration",
-              "advectionVelocity")
+              "advectionVelocity", "omega", "dOmega", "angular_velocity", "n0Vorticity", "deltaVorticity", "psi")
 
 
 def _fptr(a):

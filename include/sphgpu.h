@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define SPHGPU_ABI_VERSION 2
+#define SPHGPU_ABI_VERSION 3
 
 /* error codes */
 #define SPHGPU_OK 0
@@ -118,6 +118,14 @@ typedef struct SphParams {
     float iv_kvisc, iv_kvisc_b;
     float iv_cv_goal, iv_div_goal;
     int iv_cv_min_iter, iv_cv_max_iter, iv_div_min_iter, iv_div_max_iter;
+    /* DFSPH vorticity options, m_TH.enable_vortex (DFSPH.cpp:233-553,
+     * 913-1022): 0 off; 1 TRRV (vorticity, its transport dOmega, velocity
+     * refined through a Rankine vortex with weight vort_alpha = m_TH.alpha);
+     * 2 micropolar (angular velocity carried per particle, m_TH.zeta,
+     * m_TH.nu_t); 3 stream-function correction (vorticity lost over the step
+     * put back through a stream function).  Single fluid phase. */
+    int enable_vortex;
+    float vort_alpha, vort_zeta, vort_nu_t;
     int reserved[5];
 } SphParams;
 
@@ -196,6 +204,8 @@ int sphgpu_step_host(sphgpu_t h, int solver, const float* xyz, const float* vel,
  *        "VF_kappaV","VF_advectionVolume","VF_divergenceDeviation" (n);
  * learned warm start: "kappa_warm" (n), "ws_features" (n*16, the network's
  * normalised inputs of the last step);
+ * DFSPH vorticity options (n*3): "omega", "dOmega" (TRRV), "angular_velocity"
+ * (micropolar), "n0Vorticity", "deltaVorticity", "psi" (stream function);
  * "phase" (n, fluid phase index), "scene" (n, batch scene index).
  * Returns the count written.
  * set: "position","velocity","density" (the density the next PCISPH /

@@ -30,6 +30,13 @@ class RefParams(C.Structure):
                 ("spaceMin", _dbl3), ("spaceMax", _dbl3)]
 
 
+class RefParamsV(C.Structure):
+    """RefParams of the reference harness (RefParams + the vorticity
+    options; the restatement's OrcParams starts with the first part)."""
+    _fields_ = RefParams._fields_ + [("enable_vortex", C.c_int), ("alpha", C.c_double), ("zeta", C.c_double),
+                                     ("nu_t", C.c_double)]
+
+
 class OrcParams(C.Structure):
     """Mirror of OrcParams in sph_oracle.c."""
     _fields_ = RefParams._fields_ + [
@@ -106,7 +113,7 @@ class Oracle:
             self.cap = int(self.p.get("cap", 48))
         else:
             os.makedirs(LOG_DIR, exist_ok=True)
-            self._ps = _fill(RefParams, self.p)
+            self._ps = _fill(RefParamsV, self.p)
             self.h = self.lib.ref_create(C.byref(self._ps), LOG_DIR.encode())
             self.cap = 48
             if self.h and solver == "pcisph":

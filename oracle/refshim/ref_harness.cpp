@@ -30,6 +30,9 @@ struct RefParams {
     double nu;               /* m_TH.nu (viscosity of the DFSPH/IISPH_M force loops) */
     double th_h, th_r, th_bt; /* m_TH.h / r / bt (WCSPH surface tension, adhesion) */
     double spaceMin[3], spaceMax[3];
+    /* m_TH.enable_vortex / alpha / zeta / nu_t (DFSPH's vorticity options) */
+    int enable_vortex;
+    double alpha, zeta, nu_t;
 };
 }
 
@@ -51,7 +54,10 @@ public:
         m_TH.bt = real_t(p.th_bt);
         m_TH.spaceMin = vec_t(real_t(p.spaceMin[0]), real_t(p.spaceMin[1]), real_t(p.spaceMin[2]));
         m_TH.spaceMax = vec_t(real_t(p.spaceMax[0]), real_t(p.spaceMax[1]), real_t(p.spaceMax[2]));
-        m_TH.enable_vortex = 0;
+        m_TH.enable_vortex = p.enable_vortex;
+        m_TH.alpha = real_t(p.alpha);
+        m_TH.zeta = real_t(p.zeta);
+        m_TH.nu_t = real_t(p.nu_t);
         ker_update_numbers();
 #ifdef REF_TAG_pcisph
         /* PciSph() leaves the pci_updateDelta cache keys uninitialised
@@ -108,7 +114,8 @@ public:
 #define VEC(name) if (!strcmp(f, #name)) { *ptr = &p.name[0]; return 3; }
         VEC(position) VEC(velocity) VEC(advectionVelocity) VEC(advectionAcceleration)
         VEC(acce_presure) VEC(dii) VEC(sum_dijpj) VEC(n) VEC(acceleration)
-        VEC(DFalpha1) VEC(vel_adv) VEC(acce_adv)
+        VEC(DFalpha1) VEC(vel_adv) VEC(acce_adv) VEC(omega) VEC(angular_velocity) VEC(dOmega)
+        VEC(n0Vorticity) VEC(deltaVorticity) VEC(psi) VEC(vorticity)
         SCAL(aii) SCAL(rho_adv) SCAL(p_l) SCAL(d) SCAL(sphDensity) SCAL(advectionDensity)
         SCAL(restDensity) SCAL(presure) SCAL(mass) SCAL(density) SCAL(density_adv)
         SCAL(DFalpha) SCAL(DFalpha2) SCAL(DFkappa) SCAL(DFkappaV) SCAL(divergenceDeviation)

@@ -34,7 +34,7 @@ def test_params_default_and_struct_sizes():
     assert p.ii_max_iter == 100 and abs(p.ws_scale - 1.0) < 1e-7
     assert (p.iv_cv_min_iter, p.iv_cv_max_iter, p.iv_div_min_iter, p.iv_div_max_iter) == (3, 100, 2, 50)
     assert abs(p.iv_kvisc - 0.1) < 1e-7 and abs(p.iv_cv_goal - 1e-4) < 1e-10 and abs(p.iv_div_goal - 1e-3) < 1e-9
-    assert lib.sphgpu_abi_version() == 2
+    assert lib.sphgpu_abi_version() == 3
 
 
 def test_create_without_gpu_fails_loudly():
