@@ -233,7 +233,8 @@ class Oracle:
             raise KeyError(field)
         vec = field in ("position", "velocity", "vel_adv", "acce_adv", "acceleration", "DFalpha1", "n",
                         "pos_prediction", "acce_pressure", "dii", "sum_dijpj", "advectionVelocity",
-                        "acce_presure", "advectionAcceleration", "DF_alpha1", "VF_alpha1")
+                        "acce_presure", "advectionAcceleration", "DF_alpha1", "VF_alpha1", "omega",
+                        "angular_velocity", "dOmega", "n0Vorticity", "deltaVorticity", "psi", "vorticity")
         return out[:3 * n].reshape(n, 3) if vec else out[:n]
 
     def set(self, field, values, k=0):
