@@ -36,7 +36,8 @@ class SphParams(C.Structure):
                 ("iv_div_goal", C.c_float), ("iv_cv_min_iter", C.c_int), ("iv_cv_max_iter", C.c_int),
                 ("iv_div_min_iter", C.c_int), ("iv_div_max_iter", C.c_int),
                 ("enable_vortex", C.c_int), ("vort_alpha", C.c_float), ("vort_zeta", C.c_float),
-                ("vort_nu_t", C.c_float), ("reserved", C.c_int * 5)]
+                ("vort_nu_t", C.c_float), ("th_h", C.c_float), ("th_r", C.c_float), ("th_bt", C.c_float),
+                ("reserved", C.c_int * 5)]
 
 
 class SphStepStats(C.Structure):

@@ -57,6 +57,7 @@ struct SolverConst {
     float visc_alpha;  // phase 0 artificial viscosity (WCSPH)
     float bvisc;       // boundary viscosity alpha
     float wc_B, wc_gamma;
+    float th_h, th_r, th_bt;  // WCSPH surface tension / adhesion (m_TH.h, r, bt)
     float rho0_ph[4];  // per phase rest density
     float fm_ph[4];    // per phase mass
     float alpha_ph[4]; // per phase viscosity alpha

@@ -238,6 +238,9 @@ void fill_solver_const(sphgpu_scene* h) {
     c.bvisc = P.boundary_visc;
     c.wc_gamma = P.wc_gamma;
     c.wc_B = c.rho0 * P.soundSpeed_cs * P.soundSpeed_cs / P.wc_gamma;
+    c.th_h = P.th_h;
+    c.th_r = P.th_r;
+    c.th_bt = P.th_bt;
     c.cap = h->ncap;
     c.stride = h->stride;
     c.ws_scale = P.ws_scale;
@@ -958,7 +961,9 @@ int enq_steps(sphgpu_scene* h, int solver, int nsteps) {
         if (!h->in_staging) stage_from_sorted(h, h->cap);
         launch_step_begin(h->d, h->stream);
         enq_ns(h, 0, 2, h->stream);
-        launch(h, "wc_force", h->stream, [&] { launch_wc_force(h->d, h->c, h->cap, h->stream); });
+        const bool surf = h->P.th_h != 0.f || h->P.th_r != 0.f || h->P.th_bt != 0.f;
+        if (surf) launch(h, "wc_normal", h->stream, [&] { launch_wc_normal(h->d, h->c, h->cap, h->stream); });
+        launch(h, "wc_force", h->stream, [&] { launch_wc_force(h->d, h->c, h->cap, h->stream, surf); });
         h->in_staging = true;
         h->ns_valid = false;
         CK(cudaMemcpyAsync(h->h_stats, h->d.st, sizeof(DevStats), cudaMemcpyDeviceToHost, h->stream));
@@ -1873,7 +1878,9 @@ int sphgpu_stage(sphgpu_t h, const char* name, SphStepStats* stats) {
         } else if ((r = enq_iv_loops(h, false, s == "VF_divergenceFreeSolver"))) return r;
     } else if (s == "wc_computeForce") {
         if (h->in_staging) { h->err = "run neighbourSearch first"; return SPHGPU_EINVAL; }
-        launch_wc_force(d, h->c, h->cap, st);
+        const bool surf = h->P.th_h != 0.f || h->P.th_r != 0.f || h->P.th_bt != 0.f;
+        if (surf) launch_wc_normal(d, h->c, h->cap, st);
+        launch_wc_force(d, h->c, h->cap, st, surf);
         h->in_staging = true;
         h->ns_valid = false;
     } else {

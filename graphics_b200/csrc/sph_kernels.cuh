@@ -213,7 +213,9 @@ void launch_batch_call_begin(const DevScene& s, int nscenes, cudaStream_t st);
 void launch_batch_count(const DevScene& s, int nscenes, cudaStream_t st);
 
 // ---- WCSPH (sph_wcsph.cu) ----
-void launch_wc_force(const DevScene& s, const SolverConst& c, int n_max, cudaStream_t st);
+// surf: with surface tension and adhesion (the normals of launch_wc_normal in vA)
+void launch_wc_force(const DevScene& s, const SolverConst& c, int n_max, cudaStream_t st, bool surf = false);
+void launch_wc_normal(const DevScene& s, const SolverConst& c, int n_max, cudaStream_t st);
 
 // ---- PCISPH / IISPH_M (sph_pci_ii.cu) ----
 void launch_pci_force_except(const DevScene& s, const SolverConst& c, int n_max, cudaStream_t st);

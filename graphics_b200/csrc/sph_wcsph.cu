@@ -5,13 +5,42 @@
 // into the neighbour-list kernel (sph_grid.cu, mode 2); this file holds the
 // force pass, fused with the Euler-Cromer update (SphBase.cpp:377-402), which
 // writes the new state into the staging arrays that the next neighbour search
-// sorts.  Surface tension and adhesion (WcSph.cpp:188-211, 300-311) are not on
-// this path: they vanish for m_TH.r = m_TH.bt = 0, the plain method.
+// sorts.  Surface tension and adhesion (WcSph.cpp:188-211, 300-311) run when
+// m_TH.h, r or bt is set: k_wc_normal computes the surface normals
+// n_i = h sum_j m/rho_j gradW_ij over fluid neighbours from this step's
+// densities (the reference reads the neighbours' densities in the same loop
+// that writes them, WcSph.cpp:129-133, so its values depend on the thread
+// schedule), and the force kernel adds cohesion, curvature and adhesion.
 #include "sph_kernels.cuh"
 
 namespace {
 constexpr int NT = 128;
 
+// wc_computePressure's surface normal (WcSph.cpp:124-137) into vA
+__global__ void __launch_bounds__(NT) k_wc_normal(DevScene s, SolverConst c) {
+    const int n = s.st->n_active;
+    const int p = blockIdx.x * NT + threadIdx.x;
+    if (p >= n) return;
+    const float4 pa = s.pos[p];
+    const float fm0 = c.fm_ph[phase_of(pa)];
+    float nx = 0.f, ny = 0.f, nz = 0.f;
+    const int cnt = s.ncount[p];
+    const size_t stride = (size_t)c.stride;
+    for (int k = 0; k < cnt; ++k) {
+        const unsigned e = (unsigned)ell_get(s.nbr, stride, p, k);
+        if (e & BND_FLAG) continue;
+        const float4 pb = s.pos[e];
+        const float xx = pa.x - pb.x, xy = pa.y - pb.y, xz = pa.z - pb.z;
+        const float dis = sqrtf(xx * xx + xy * xy + xz * xz);
+        const float g = -ker_Wg(c.k, dis) / dis * (fm0 / s.rho[e]);
+        nx += xx * g;
+        ny += xy * g;
+        nz += xz * g;
+    }
+    s.vA[p] = make_float4(nx * c.th_h, ny * c.th_h, nz * c.th_h, 0.f);
+}
+
+template <bool SURF>
 __global__ void __launch_bounds__(NT) k_wc_force(DevScene s, SolverConst c) {
     const int n = s.st->n_active;
     const int p = blockIdx.x * NT + threadIdx.x;
@@ -52,6 +81,14 @@ __global__ void __launch_bounds__(NT) k_wc_force(DevScene s, SolverConst c) {
                     const float pi = -nu * pro / (len2 + den0);
                     acce += grad * (-rho0 * vol * pi);
                 }
+                if (SURF) {
+                    // adhesion (WcSph.cpp:300-311)
+                    const float h = c.th_h;
+                    float A = 0.f;
+                    if (2.f * dis > h && dis <= h)
+                        A = 0.007f / powf(h, 3.25f) * powf(-4.f * dis * dis / h + 6.f * dis - 2.f * h, 0.25f);
+                    acce += -c.th_bt * rho0 * vol * A / dis;
+                }
             } else {
                 pb = s.pos[e];
                 const float4 vb = s.vel[e];
@@ -70,6 +107,22 @@ __global__ void __launch_bounds__(NT) k_wc_force(DevScene s, SolverConst c) {
                         const float nu = 2.f * alpha * c.hs * c.cs / (ra + rb);
                         const float pi = -nu * pro / (len2 + den0);
                         acce += grad * (-fma * pi);
+                    }
+                    if (SURF) {
+                        // cohesion and curvature (WcSph.cpp:188-210), Kij with the
+                        // reference's rest density 1000
+                        const float h = c.th_h;
+                        const float Kij = 2.f * 1000.0f / (ra + rb);
+                        float C = 0.f;
+                        const float k9 = 32.0f / (3.14f * powf(h, 9.0f));
+                        if (2.f * dis > h && dis <= h) C = k9 * powf(h - dis, 3.0f) * powf(dis, 3.0f);
+                        else if (dis > 0.f && 2.f * dis <= h)
+                            C = k9 * (2.f * powf(h - dis, 3.0f) * powf(dis, 3.0f) - powf(h, 6.0f) / 64.0f);
+                        const float coh = -c.th_r * fma * C / dis;
+                        const float4 na = s.vA[p], nb = s.vA[e];
+                        ax += (xx * coh + (na.x - nb.x) * -c.th_r) * Kij;
+                        ay += (xy * coh + (na.y - nb.y) * -c.th_r) * Kij;
+                        az += (xz * coh + (na.z - nb.z) * -c.th_r) * Kij;
                     }
                 } else {
                     // wc_fluidPartForce_fdiff, WcSph.cpp:239-253
@@ -109,6 +162,10 @@ __global__ void __launch_bounds__(NT) k_wc_force(DevScene s, SolverConst c) {
 }
 }  // namespace
 
-void launch_wc_force(const DevScene& s, const SolverConst& c, int n_max, cudaStream_t st) {
-    k_wc_force<<<(n_max + NT - 1) / NT, NT, 0, st>>>(s, c);
+void launch_wc_force(const DevScene& s, const SolverConst& c, int n_max, cudaStream_t st, bool surf) {
+    if (surf) k_wc_force<true><<<(n_max + NT - 1) / NT, NT, 0, st>>>(s, c);
+    else k_wc_force<false><<<(n_max + NT - 1) / NT, NT, 0, st>>>(s, c);
+}
+void launch_wc_normal(const DevScene& s, const SolverConst& c, int n_max, cudaStream_t st) {
+    k_wc_normal<<<(n_max + NT - 1) / NT, NT, 0, st>>>(s, c);
 }

@@ -126,6 +126,11 @@ typedef struct SphParams {
      * put back through a stream function).  Single fluid phase. */
     int enable_vortex;
     float vort_alpha, vort_zeta, vort_nu_t;
+    /* WCSPH surface tension and adhesion (WcSph.cpp:188-211, 300-311):
+     * m_TH.h (the surface kernel's radius and the normal's scale), m_TH.r
+     * (cohesion and curvature), m_TH.bt (adhesion); all 0 = the plain
+     * method */
+    float th_h, th_r, th_bt;
     int reserved[5];
 } SphParams;
 

@@ -145,7 +145,13 @@ private:
         }
         if (!this->m_Solids.empty()) p.boundary_visc = (float)this->m_Solids[0].viscosity_alpha;
         // solver constants the reference keeps in the solver object
-        if constexpr (Solver == SPHGPU_WCSPH) p.wc_gamma = (float)this->m_DensityPower_gamma;  // WcSph.h:34
+        if constexpr (Solver == SPHGPU_WCSPH) {
+            p.wc_gamma = (float)this->m_DensityPower_gamma;  // WcSph.h:34
+            // surface tension and adhesion read m_TH.h / r / bt (WcSph.cpp:124-311)
+            p.th_h = (float)this->m_TH.h;
+            p.th_r = (float)this->m_TH.r;
+            p.th_bt = (float)this->m_TH.bt;
+        }
         if constexpr (Solver == SPHGPU_PCISPH) {  // PciSph.h:35
             p.pci_min_iter = this->m_minIterations;
             p.pci_max_iter = this->m_maxIterations;

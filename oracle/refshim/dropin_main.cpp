@@ -71,7 +71,7 @@ public:
 
     void load(FILE* f, int& steps) {
         int32_t hdr[3];
-        float q[21];
+        float q[24];
         if (fread(hdr, sizeof hdr, 1, f) != 1 || fread(q, sizeof q, 1, f) != 1) exit(2);
         const int nf = hdr[0], nb = hdr[1];
         steps = hdr[2];
@@ -84,6 +84,9 @@ public:
         m_TH.soundSpeed_cs = q[12];
         m_TH.nu = q[13];
         m_TH.densityErro_eta = q[20];  // PciSph's loop goal (uninitialised in ThresholdsBase)
+        m_TH.h = q[21];  // WcSph's surface tension and adhesion (uninitialised in ThresholdsBase)
+        m_TH.r = q[22];
+        m_TH.bt = q[23];
         const float rho0 = q[14], visc = q[15], bvisc = q[16], d = q[17];
         gpuParams().df_density_goal = q[18];
         gpuParams().df_div_goal_abs = 0.0;

@@ -951,28 +951,42 @@ static void wc_pressure(OrcScene* s) {
         real B = rho0 * cs * cs / gamma;
 #pragma omp parallel for
         for (int i = 0; i < F->n; ++i) {
-            const real* pa = F->pos + 3 * (long)i;
-            real ni[3] = {0, 0, 0};
             real density = wm0;
             const PIdx* L = F->nidx + (long)i * cap;
             const real* D = F->ndis + (long)i * cap;
             int n = F->nnum[i];
             for (int j = 0; j < n; ++j) {
-                if (L[j].t < 0) {
-                    const real* pb = fpos(s, L[j]);
-                    density += fm0 * ker_W(s, D[j]);
-                    real gs = -ker_W_grad(s, D[j]) / D[j];
-                    real rb = s->F[-L[j].t - 1].density[L[j].i];
-                    for (int c = 0; c < 3; ++c) ni[c] += (pa[c] - pb[c]) * gs * (fm0 / rb);
-                } else {
-                    density += rho0 * s->S[L[j].t - 1].volume[L[j].i] * ker_W(s, D[j]);
-                }
+                if (L[j].t < 0) density += fm0 * ker_W(s, D[j]);
+                else density += rho0 * s->S[L[j].t - 1].volume[L[j].i] * ker_W(s, D[j]);
             }
             F->density[i] = density;
-            for (int c = 0; c < 3; ++c) F->n_surf[3 * (long)i + c] = ni[c] * thh;
             real p = B * (POWR(density / rho0, gamma) - 1);
             if (p < 0) p = 0;
             F->presure[i] = p;
+        }
+    }
+    /* The surface normal n_i = h sum_j m/rho_j gradW_ij (WcSph.cpp:124-137)
+     * with this step's densities: the reference reads the neighbours'
+     * densities in the loop that writes them, so its value depends on the
+     * thread schedule (it vanishes for m_TH.h = 0, the plain method). */
+    for (int k = 0; k < s->nf; ++k) {
+        OrcFluid* F = &s->F[k];
+        real fm0 = F->rho0 * v0;
+#pragma omp parallel for
+        for (int i = 0; i < F->n; ++i) {
+            const real* pa = F->pos + 3 * (long)i;
+            real ni[3] = {0, 0, 0};
+            const PIdx* L = F->nidx + (long)i * cap;
+            const real* D = F->ndis + (long)i * cap;
+            int n = F->nnum[i];
+            for (int j = 0; j < n; ++j) {
+                if (L[j].t >= 0) continue;
+                const real* pb = fpos(s, L[j]);
+                real gs = -ker_W_grad(s, D[j]) / D[j];
+                real rb = s->F[-L[j].t - 1].density[L[j].i];
+                for (int c = 0; c < 3; ++c) ni[c] += (pa[c] - pb[c]) * gs * (fm0 / rb);
+            }
+            for (int c = 0; c < 3; ++c) F->n_surf[3 * (long)i + c] = ni[c] * thh;
         }
     }
 }

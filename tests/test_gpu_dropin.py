@@ -23,7 +23,7 @@ REF = os.path.join(ROOT, "oracle", "_ref")
 def _write(path, sc, steps, kw):
     p = [sc.spacing_r, sc.smooth_radius, kw["dt"], 0.0, -9.81, 0.0, *sc.space_min, *sc.space_max,
          kw["soundSpeed_cs"], kw["nu"], sc.rho0, 0.0, 0.0, sc.d, kw["df_density_goal"], kw["df_div_goal_rel"],
-         kw["densityErro_eta"]]
+         kw["densityErro_eta"], kw.get("th_h", 0.0), kw.get("th_r", 0.0), kw.get("th_bt", 0.0)]
     with open(path, "wb") as f:
         f.write(struct.pack("3i", sc.n_fluid, len(sc.boundary_pos), steps))
         f.write(np.asarray(p, np.float32).tobytes())
@@ -78,6 +78,34 @@ def test_cpp_dropin_subclass_matches_gpu_path(tmp_path, solver, dt, cs):
     assert np.array_equal(g.get("position"), x)
     assert np.array_equal(g.get("velocity"), v)
     assert np.array_equal(g.get("sphDensity" if solver == "iisph" else "density"), rho)
+    g.close()
+
+
+def test_cpp_dropin_wcsph_surface_terms(tmp_path):
+    """WcSph with m_TH.h / r / bt set in the scene (surface tension and
+    adhesion): the drop-in reads them from m_TH like the reference does."""
+    exe = os.path.join(REF, "dropin_wcsph")
+    if not os.path.exists(exe):
+        pytest.skip("drop-in check not built (needs the reference sources)")
+    sc = _settled_column()
+    kw = dict(dt=2.5e-4, soundSpeed_cs=18.708287, nu=1e-3, df_density_goal=1e-4, df_div_goal_rel=1e-3,
+              densityErro_eta=0.01, th_h=sc.smooth_radius, th_r=0.2, th_bt=1.0)
+    steps = 5
+    _write(tmp_path / "in.bin", sc, steps, kw)
+    r = subprocess.run([exe, str(tmp_path / "in.bin"), str(tmp_path / "out.bin")], cwd=tmp_path,
+                       capture_output=True, timeout=300)
+    assert r.returncode == 0, r.stderr.decode()[-2000:]
+    n, frame, _, x, v, rho = _read(tmp_path / "out.bin")
+    g = scene_to_gpu(sc, df_div_goal_abs=0.0, df_div_max_iter=100, **kw)
+    g.step("wcsph", steps)
+    assert frame == steps and g.n_fluid == n
+    assert np.array_equal(g.get("position"), x)
+    assert np.array_equal(g.get("velocity"), v)
+    assert np.array_equal(g.get("density"), rho)
+    plain = scene_to_gpu(sc, df_div_goal_abs=0.0, df_div_max_iter=100, **dict(kw, th_h=0.0, th_r=0.0, th_bt=0.0))
+    plain.step("wcsph", steps)
+    assert not np.array_equal(plain.get("velocity"), v)
+    plain.close()
     g.close()
 
 

@@ -178,6 +178,28 @@ def test_wcsph_pressure_force_and_steps():
     assert rel_err(g.get("position"), o.get("position"), scale=1.0) < 1e-6
 
 
+def test_wcsph_surface_tension_and_adhesion():
+    """m_TH.h / r / bt set (the reference's demo values): the surface
+    normal, cohesion, curvature and adhesion terms against the oracle's
+    force pass (itself bit-exact with the reference's), then steps."""
+    sc = small_dam_break((12, 12, 12), r=0.025, seed=7)
+    kw = dict(dt=2.5e-4, soundSpeed_cs=18.708287, th_h=sc.smooth_radius, th_r=0.2, th_bt=1.0)
+    sc, g, o = make_pair(sc, visc_alpha=0.01, boundary_visc=0.01, **kw)
+    g.stage("wc_computePressure")
+    for st in ("neighbourSearch", "updateSolidPartWeight", "wc_computePressure"):
+        o.stage(st)
+    assert elem_rel(g.get("density"), o.get("density")) < RTOL
+    g.stage("wc_computeForce")
+    o.stage("wc_computeForce")
+    assert rel_err(g.get("acceleration"), o.get("acceleration")) < 1e-4
+    sc, g, o = make_pair(sc, visc_alpha=0.01, boundary_visc=0.01, **kw)
+    for _ in range(3):
+        g.step("wcsph", 1)
+        o.stage("wc_step")
+    assert elem_rel(g.get("density"), o.get("density")) < 1e-4
+    assert rel_err(g.get("position"), o.get("position"), scale=1.0) < 1e-6
+
+
 def test_out_of_domain_particles_removed_with_status():
     sc = small_dam_break((8, 8, 8), r=0.025, seed=2)
     sc.fluid_pos[0] = np.array(sc.space_max) + 1.0  # outside

@@ -101,6 +101,36 @@ def test_restatement_equals_reference_build(solver, stage, kw):
         np.testing.assert_array_equal(a.get(f), b.get(f), err_msg=f)
 
 
+@pytest.mark.skipif(not REF, reason="reference build not present")
+def test_wcsph_surface_terms_equal_reference_build():
+    """Surface tension and adhesion on (m_TH.h = the smoothing radius,
+    m_TH.r = 0.2, m_TH.bt = 1: the reference's demo scene,
+    Demo-mySPH.h:42-44): the restatement's force pass against the
+    reference's, bit for bit.  The reference's wc_computePressure reads the
+    neighbours' densities in the loop that writes them (WcSph.cpp:129-133);
+    run twice on the same positions, its second pass reads this step's
+    densities throughout, which is the restatement's surface normal."""
+    sc = small_dam_break((9, 9, 9), r=0.025, seed=3)
+    kw = dict(WC_KW, th_h=sc.smooth_radius, th_r=0.2, th_bt=1.0, visc_alpha=0.01, solid_visc=0.01)
+    a = make_scene_oracle(sc, kind="port", **kw)
+    b = make_scene_oracle(sc, kind="reference", solver="wcsph", **kw)
+    for o in (a, b):
+        o.stage("neighbourSearch")
+        o.stage("updateSolidPartWeight")
+        o.stage("wc_computePressure")
+    b.stage("wc_computePressure")
+    np.testing.assert_array_equal(a.get("density"), b.get("density"))
+    a.stage("wc_computeForce")
+    b.stage("wc_computeForce")
+    acc = a.get("acceleration")
+    np.testing.assert_array_equal(acc, b.get("acceleration"))
+    # the surface terms are on: the same state without them gives another force
+    c = make_scene_oracle(sc, kind="port", **dict(kw, th_h=0.0, th_r=0.0, th_bt=0.0))
+    for st in ("neighbourSearch", "updateSolidPartWeight", "wc_computePressure", "wc_computeForce"):
+        c.stage(st)
+    assert np.abs(c.get("acceleration") - acc).max() > 1e-3 * np.abs(acc).max()
+
+
 def test_fp64_restatement_close_to_fp32():
     sc = scene()
     a = make_scene_oracle(sc, **DF_KW)
