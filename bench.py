@@ -916,6 +916,7 @@ def run_surface(args):
         ntri = step()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    k0 = sf.stats()[2]
     with ClockSampler(local) as clk:
         e0.record(stream)
         for _ in range(args.steps):
@@ -923,6 +924,7 @@ def run_surface(args):
         e1.record(stream)
         torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
+    npairs, ntiles, k1 = sf.stats()
     value = n * args.steps / (ms / 1e3)
     # per-kernel durations: the field and mesh calls bracketed by events
     f0, f1, f2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
@@ -953,6 +955,16 @@ def run_surface(args):
                "d2h_bytes_per_step": int(m * 36), "steps": args.steps,
                "note": "sphgpu_surface_field from host positions, sphgpu_surface_mesh into host memory"}
     hbm, peak_kind = peaks()
+    # the field kernel (the largest share of the step): its algorithmic bytes
+    # over its event-timed duration; bound by instruction issue in practice
+    # (every row of a tile tests every particle listed under the tile), so
+    # the HBM fraction is low by construction
+    field_bytes = nodes * SURF_ALG_NODE + npairs * SURF_ALG_PAIR
+    roof = {"kernel": "k_sf_field (+ per-particle kernels and tile binning of sphgpu_surface_field)",
+            "bound": "hbm", "achieved": field_bytes / (tf / reps * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
+            "traffic": None, "alg_bytes": int(field_bytes), "tile_pairs": int(npairs), "tiles": int(ntiles),
+            "peak_source": peak_kind}
+    roof["frac"] = roof["achieved"] / hbm
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         try:
@@ -968,7 +980,8 @@ def run_surface(args):
                            "grid_nodes": nodes, "grid": sf.get_grid_num().tolist(), "triangles": int(ntri),
                            "parallelism": "single", "l2": "field %.1f GB > L2" % (nodes * 4 / 1e9)},
                 "kernels": {"field_ms": tf / reps, "mesh_ms": tm / reps},
-                "roofline": None, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": None, "clocks": clk.summary()}
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(k1 - k0),
+                "clocks": clk.summary()}
         print(json.dumps(line))
     sf.close()
 

@@ -102,6 +102,7 @@ SIGNATURES = {
     "sphgpu_surface_mesh": (C.c_longlong, [_vp, _f, _i, _fp, C.c_longlong]),
     "sphgpu_surface_stream": (_vp, [_vp]),
     "sphgpu_surface_last_error": (_i, [_vp, _cp, _i]),
+    "sphgpu_surface_stats": (_i, [_vp, C.POINTER(C.c_longlong), _ip, C.POINTER(C.c_longlong)]),
     "sphgpu_mc_table": (_i, [_ip, C.POINTER(C.c_byte)]),
     "sphgpu_get_neighbours": (_i, [_vp, _ip, _ip, _ip]),
     "sphgpu_get_cells": (_i, [_vp, C.POINTER(C.c_longlong)]),

@@ -648,6 +648,8 @@ struct sphgpu_surface {
     int gnum[3] = {0, 0, 0};
     long long nnodes = 0;
     int ntiles = 0;
+    long long npairs = 0;    // (tile, particle) pairs of the last field
+    long long kernels = 0;   // this file's kernel launches, cumulative
     float* field = nullptr;
     // particles
     int pcap = 0;
@@ -751,6 +753,7 @@ int run_field(sphgpu_surface* s, int n, int aniso) {
     if (aniso && n > 0) {
         SCK(cudaMemsetAsync(s->pcnt, 0, sizeof(int) * ((size_t)pcells + 2), st));
         SCK(cudaMemsetAsync(s->bad, 0, sizeof(int), st));
+        s->kernels += 3;
         k_sf_key<<<nblk(n, 256), 256, 0, st>>>(P, s->pos, n, s->key, s->slot, s->pcnt, s->bad);
         size_t b = 0;
         cub::DeviceScan::ExclusiveSum(nullptr, b, s->pcnt, s->pstart, pcells + 2, st);
@@ -759,12 +762,14 @@ int run_field(sphgpu_surface* s, int n, int aniso) {
         k_sf_scatter<<<nblk(n, 256), 256, 0, st>>>(s->key, s->slot, s->pstart, n, s->tmp);
         k_sf_rank<<<nblk(n, 256), 256, 0, st>>>(s->key, s->pstart, s->tmp, n, s->sorted);
     }
+    s->kernels += n > 0;
     if (n > 0)
         k_sf_kernel<<<nblk(n, 128), 128, 0, st>>>(P, s->pos, n, s->sorted, s->pstart, aniso, s->rec0, s->rec1, s->rec2,
                                                     s->blo, s->bhi);
     // tile pairs
     long long npairs = 0;
     if (n > 0) {
+        ++s->kernels;
         k_sf_tile_count<<<nblk(n, 256), 256, 0, st>>>(s->blo, s->bhi, n, s->npair);
         SCK(cudaMemsetAsync(s->npair + n, 0, sizeof(int), st));
         size_t b = 0;
@@ -784,6 +789,7 @@ int run_field(sphgpu_surface* s, int n, int aniso) {
         s->paircap = cap;
     }
     if (npairs > 0) {
+        ++s->kernels;
         k_sf_tile_emit<<<nblk(n, 256), 256, 0, st>>>(P, s->blo, s->bhi, n, s->poff, s->ptile, s->ppart);
         int bits = 1;
         while (bits < 31 && (1ll << bits) <= (long long)s->ntiles) ++bits;
@@ -794,6 +800,8 @@ int run_field(sphgpu_surface* s, int n, int aniso) {
         cub::DeviceRadixSort::SortPairs(s->tmpbuf, b, s->ptile, s->ptile_s, s->ppart, s->ppart_s, (int)npairs, 0, bits,
                                         st);
     }
+    s->npairs = npairs;
+    s->kernels += 2;
     k_sf_tile_bounds<<<nblk((long long)s->ntiles + 1, 256), 256, 0, st>>>(s->ptile_s, npairs, s->ntiles, s->tstart);
     k_sf_field<<<s->ntiles, FT, 0, st>>>(P, s->tstart, s->ppart_s, s->rec0, s->rec1, s->rec2, s->blo, s->bhi,
                                           s->field);
@@ -922,6 +930,7 @@ int sphgpu_surface_field(sphgpu_surface_t s, int aniso, const float* xyz, int n,
             d = s->xyz;
             SCK(cudaMemcpyAsync(d, xyz, sizeof(float) * 3 * (size_t)n, cudaMemcpyHostToDevice, s->stream));
         }
+        ++s->kernels;
         k_pack_xyz<<<nblk(n, 256), 256, 0, s->stream>>>(d, n, s->pos);
     }
     int r = run_field(s, n, aniso);
@@ -1011,6 +1020,7 @@ long long sphgpu_surface_mesh(sphgpu_surface_t s, float iso, int ref_rows, float
     M.cy_hi = s->coords + 3 * (size_t)m;
     M.cz_lo = s->coords + 4 * (size_t)m;
     M.cz_hi = s->coords + 5 * (size_t)m;
+    ++s->kernels;
     k_mc_count<<<(int)nblocks, MCB, 0, st>>>(M, s->field, ngroups, gpr, s->cases, s->ntri);
     size_t b = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, b, s->ntri, s->toff, (int)nblocks, st);
@@ -1026,6 +1036,7 @@ long long sphgpu_surface_mesh(sphgpu_surface_t s, float iso, int ref_rows, float
         if (salloc(s, &s->tris, 9 * (size_t)total)) return SPHGPU_ENOMEM;
         s->tricap = total;
     }
+    s->kernels += total > 0;
     if (total > 0) k_mc_emit<<<(int)nblocks, MCB, 0, st>>>(M, s->field, ngroups, gpr, s->cases, s->toff, s->tris);
     SCK(cudaGetLastError());
     SCK(cudaStreamSynchronize(st));
@@ -1036,6 +1047,14 @@ long long sphgpu_surface_mesh(sphgpu_surface_t s, float iso, int ref_rows, float
 }
 
 void* sphgpu_surface_stream(sphgpu_surface_t s) { return s ? (void*)s->stream : nullptr; }
+
+int sphgpu_surface_stats(sphgpu_surface_t s, long long* n_pairs, int* n_tiles, long long* kernels) {
+    if (!s) return SPHGPU_EINVAL;
+    if (n_pairs) *n_pairs = s->npairs;
+    if (n_tiles) *n_tiles = s->ntiles;
+    if (kernels) *kernels = s->kernels;
+    return 0;
+}
 
 int sphgpu_surface_last_error(sphgpu_surface_t s, char* buf, int len) {
     if (!s || !buf || len <= 0) return SPHGPU_EINVAL;

@@ -97,6 +97,12 @@ class surface_field:
     def get_cell_size(self):
         return self.cell_size
 
+    def stats(self):
+        """(tile-particle pairs of the last field, tiles, kernel launches so far)."""
+        pairs, tiles, kern = C.c_longlong(), C.c_int(), C.c_longlong()
+        self.lib.sphgpu_surface_stats(self.h, C.byref(pairs), C.byref(tiles), C.byref(kern))
+        return pairs.value, tiles.value, kern.value
+
     def mesh(self, iso, ref_rows=False):
         """marchingCubes over the device field: (T, 3, 3) float32."""
         n = self.lib.sphgpu_surface_mesh(self.h, float(iso), int(bool(ref_rows)), None, 0)

@@ -343,6 +343,11 @@ int sphgpu_surface_set_field(sphgpu_surface_t s, const float* in);
 long long sphgpu_surface_mesh(sphgpu_surface_t s, float iso, int ref_rows, float* out, long long max_tris);
 void* sphgpu_surface_stream(sphgpu_surface_t s);
 int sphgpu_surface_last_error(sphgpu_surface_t s, char* buf, int len);
+/* Work counters (no reference counterpart): the (tile, particle) pairs of
+ * the last field (each particle listed under every 8 x 16 x 16-node tile its
+ * node box touches), the number of tiles, and this handle's kernel launches
+ * so far.  Any pointer may be NULL. */
+int sphgpu_surface_stats(sphgpu_surface_t s, long long* n_pairs, int* n_tiles, long long* kernels);
 int sphgpu_mc_table(int* ntri, signed char* tri);
 
 /* Stage-level entry points (parity tests run "given state S, call stage X"):
