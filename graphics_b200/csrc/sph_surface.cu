@@ -248,6 +248,7 @@ __global__ void __launch_bounds__(128) k_sf_kernel(SfParams P, const float4* pos
     float g[6] = {1.f, 0.f, 0.f, 1.f, 0.f, 1.f};
     float det = 1.f;
     double smax = 1.0;
+    double ext[3] = {-1.0, -1.0, -1.0};  // the ellipsoid's half-extents per axis (aniso only)
     if (aniso) {
         int cx, cy, cz;
         const int home = pcell(P, pi, cx, cy, cz);
@@ -336,6 +337,13 @@ __global__ void __launch_bounds__(128) k_sf_kernel(SfParams P, const float4* pos
             g[5] = (float)G[2][2];
             det = (float)(1.0 / (s[0] * s[1] * s[2]));
             smax = s[0];
+            // {x : |G (x - c)| <= r_h} = {c + V diag(s) V^T u : |u| <= r_h}:
+            // along axis a it reaches r_h |row a of V diag(s)|
+            for (int a = 0; a < 3; ++a) {
+                double e2 = 0.0;
+                for (int k = 0; k < 3; ++k) e2 += V[a][o[k]] * s[k] * V[a][o[k]] * s[k];
+                ext[a] = (double)P.r_h * sqrt(e2);
+            }
             cxr = pi.x + mx;
             cyr = pi.y + my;
             czr = pi.z + mz;
@@ -357,6 +365,15 @@ __global__ void __launch_bounds__(128) k_sf_kernel(SfParams P, const float4* pos
         const int c = (int)((cc[a] - P.gmin_d[a]) * P.gdiv_d);
         lo[a] = max(c - hw, 0);
         hi[a] = min(c + hw + 1, P.gnum[a] - 1);
+        // The reference's box bounds the ellipsoid's circumscribed sphere;
+        // nodes outside the ellipsoid add nothing (W = 0 beyond r_h), so the
+        // box is cut to the ellipsoid's axis-aligned extent, one node of
+        // margin each side (the field's own r <= r_h test decides within).
+        if (ext[a] >= 0.0) {
+            const double u = (cc[a] - P.gmin_d[a]) * P.gdiv_d, e = ext[a] * P.gdiv_d;
+            lo[a] = max(lo[a], (int)floor(u - e) - 1);
+            hi[a] = min(hi[a], (int)ceil(u + e) + 1);
+        }
     }
     box_lo[i] = make_int4(lo[0], lo[1], lo[2], 0);
     box_hi[i] = make_int4(hi[0], hi[1], hi[2], 0);
@@ -473,17 +490,23 @@ __global__ void __launch_bounds__(FT) k_sf_field(SfParams P, const int* tstart, 
             const int ka = max(xa, (int)floorf((-B - sq) * g2.z) - 1);
             const int kb = min(xb, (int)ceilf((-B + sq) * g2.z) + 1);
             const float B2 = 2.f * B;
+            // the row's two halves, each evaluated only when the interval
+            // reaches it (adjacent rows of a warp mostly agree)
 #pragma unroll
-            for (int k = 0; k < TX; ++k) {
-                if (k < ka || k > kb) continue;
-                const float fk = (float)k;
-                const float r2 = fmaf(fmaf(du.w, fk, B2), fk, C0);
-                if (!(r2 <= rh2)) continue;
-                // ker_spline (surface_field.cpp:235-249), times the particle volume
-                const float r = r2 > 0.f ? r2 * rsqrtf(r2) : 0.f;
-                const float hr = rh - r;
-                const float w = r < hh ? fmaf(P.p3 * r, r2, fmaf(P.p2, r2, P.p1)) : P.p4 * hr * hr * hr;
-                acc[k] = fmaf(c.w, w, acc[k]);
+            for (int half = 0; half < 2; ++half) {
+                if (half == 0 ? ka >= TX / 2 : kb < TX / 2) continue;
+#pragma unroll
+                for (int k = half * (TX / 2); k < (half + 1) * (TX / 2); ++k) {
+                    if (k < ka || k > kb) continue;
+                    const float fk = (float)k;
+                    const float r2 = fmaf(fmaf(du.w, fk, B2), fk, C0);
+                    if (!(r2 <= rh2)) continue;
+                    // ker_spline (surface_field.cpp:235-249), times the particle volume
+                    const float r = r2 > 0.f ? r2 * rsqrtf(r2) : 0.f;
+                    const float hr = rh - r;
+                    const float w = r < hh ? fmaf(P.p3 * r, r2, fmaf(P.p2, r2, P.p1)) : P.p4 * hr * hr * hr;
+                    acc[k] = fmaf(c.w, w, acc[k]);
+                }
             }
         }
     }
