@@ -146,7 +146,8 @@ class ClockSampler:
     def __init__(self, gpu_index):
         self.idx = gpu_index
         self.p = None
-        self.path = os.path.join(ROOT, "gpurun_out", "clocks_%d.csv" % gpu_index)
+        self.path = os.path.join(os.environ.get("SPH_BENCH_OUT", os.path.join(ROOT, "_bench_out")),
+                                 "clocks_%d.csv" % gpu_index)
 
     def __enter__(self):
         try:
