@@ -205,7 +205,8 @@ __global__ void __launch_bounds__(BS) k_df_dens_a(DevScene s, SolverConst c, int
     double bs = block_sum_double<BS>(mine, sh);
     double tot;
     if (finish_sum<BS>(s.partial, &s.st->ticket[0], bs, &tot)) {
-        s.st->err_density = (tot / (double)n - (double)c.rho0) / (double)c.rho0;
+        // no particle left (all removed): nothing to solve
+        s.st->err_density = n > 0 ? (tot / (double)n - (double)c.rho0) / (double)c.rho0 : 0.0;
     }
 }
 
@@ -311,7 +312,7 @@ __global__ void __launch_bounds__(BS) k_df_div_a(DevScene s, SolverConst c) {
     __shared__ double sh[BS / 32];
     double bs = block_sum_double<BS>(mine, sh);
     double tot;
-    if (finish_sum<BS>(s.partial, &s.st->ticket[1], bs, &tot)) s.st->err_div = tot / (double)n;
+    if (finish_sum<BS>(s.partial, &s.st->ticket[1], bs, &tot)) s.st->err_div = n > 0 ? tot / (double)n : 0.0;
 }
 
 // FP64 max |v| and the CFL step dt = clamp(cfl * d / vmax, dt_min, dt_max)

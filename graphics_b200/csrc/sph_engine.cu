@@ -1673,9 +1673,16 @@ int sphgpu_set_fluid(sphgpu_t h, const char* field, const float* in) {
     std::vector<int> gid;
     int n;
     bool staging = h->in_staging && (f == "position" || f == "velocity");
-    if (download_gid(h, gid, n, staging)) return SPHGPU_ECUDA;
+    const bool on_device = (f == "position" || f == "velocity") && h->total_removed == 0;
+    if (on_device) {
+        // reordered on the device: only the count is needed on the host
+        CK(cudaStreamSynchronize(h->stream));
+        n = h->h_stats->n_active;
+    } else if (download_gid(h, gid, n, staging)) {
+        return SPHGPU_ECUDA;
+    }
     DevScene& d = h->d;
-    if ((f == "position" || f == "velocity") && h->total_removed == 0) {
+    if (on_device) {
         float4* dst = f == "position" ? (staging ? d.pos_s : d.pos) : (staging ? d.vel_s : d.vel);
         float* tmp3 = (float*)d.aux4;
         CK(cudaMemcpyAsync(tmp3, in, sizeof(float) * 3 * (size_t)n, cudaMemcpyHostToDevice, h->stream));
