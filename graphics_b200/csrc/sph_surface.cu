@@ -421,6 +421,14 @@ __global__ void k_sf_tile_bounds(const int* tile_sorted, long long npairs, int n
     tstart[t] = (int)lo;
 }
 
+// PTX sqrt.approx (relative error within a few ulp; sqrt(0) = 0), for the
+// splat's distances, which only feed the spline
+__device__ __forceinline__ float sqrt_approx(float x) {
+    float y;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 // ker_spline (surface_field.cpp:235-249), times the particle volume
 __device__ __forceinline__ float sf_spline(const SfParams& P, float r) {
     const float hr = P.r_h - r;
@@ -501,10 +509,11 @@ __global__ void __launch_bounds__(FT) k_sf_field(SfParams P, const int* tstart, 
                     const float fk = (float)k;
                     const float r2 = fmaf(fmaf(du.w, fk, B2), fk, C0);
                     if (!(r2 <= rh2)) continue;
-                    // ker_spline (surface_field.cpp:235-249), times the particle volume
-                    const float r = r2 > 0.f ? r2 * rsqrtf(r2) : 0.f;
+                    // ker_spline (surface_field.cpp:235-249), times the particle
+                    // volume: p1 + r^2 (p2 + p3 r) inside h/2, p4 (h - r)^3 beyond
+                    const float r = sqrt_approx(r2);
                     const float hr = rh - r;
-                    const float w = r < hh ? fmaf(P.p3 * r, r2, fmaf(P.p2, r2, P.p1)) : P.p4 * hr * hr * hr;
+                    const float w = r < hh ? fmaf(fmaf(P.p3, r, P.p2), r2, P.p1) : (P.p4 * hr) * (hr * hr);
                     acc[k] = fmaf(c.w, w, acc[k]);
                 }
             }
