@@ -617,7 +617,10 @@ __global__ void __launch_bounds__(MCB) k_mc_count(McParams M, const float* f, lo
 // pass 2: the cases again, offsets by an in-block scan after the block's
 // offset; only cubes with triangles gather their corners
 __global__ void __launch_bounds__(MCB) k_mc_emit(McParams M, const float* f, long long ngroups, int gpr,
-                                                 const unsigned char* cases, const int* boff, float* out) {
+                                                 const unsigned char* cases, const int* bcount, const int* boff,
+                                                 float* out) {
+    // most blocks of cubes hold no surface: the whole block leaves at once
+    if (bcount[blockIdx.x] == 0) return;
     const long long g = (long long)blockIdx.x * MCB + threadIdx.x;
     int x0 = 0, xe = 0, y = 0, z = 0, n = 0;
     long long c0 = 0;
@@ -1069,7 +1072,8 @@ long long sphgpu_surface_mesh(sphgpu_surface_t s, float iso, int ref_rows, float
         s->tricap = total;
     }
     s->kernels += total > 0;
-    if (total > 0) k_mc_emit<<<(int)nblocks, MCB, 0, st>>>(M, s->field, ngroups, gpr, s->cases, s->toff, s->tris);
+    if (total > 0)
+        k_mc_emit<<<(int)nblocks, MCB, 0, st>>>(M, s->field, ngroups, gpr, s->cases, s->ntri, s->toff, s->tris);
     SCK(cudaGetLastError());
     SCK(cudaStreamSynchronize(st));
     s->ntris = total;
