@@ -74,3 +74,17 @@ def closed_and_oriented(tris, tol):
             s = (t[k], t[(k + 1) % 3])
             sides[s] = sides.get(s, 0) + 1
     return all(v == 1 for v in sides.values()) and all((b, a) in sides for (a, b) in sides)
+
+
+def build_surface_dropin(out_dir):
+    """Compile tests/cpp/surface_dropin_main.cpp against include/ and the
+    library; returns the executable's path."""
+    import os
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    exe = os.path.join(str(out_dir), "surface_dropin")
+    lib = os.path.join(root, "graphics_b200")
+    subprocess.run(["g++", "-std=c++17", "-O2", "-I" + os.path.join(root, "include"),
+                    os.path.join(root, "tests", "cpp", "surface_dropin_main.cpp"), "-L" + lib, "-lsphgpu",
+                    "-Wl,-rpath," + lib, "-o", exe], check=True, capture_output=True)
+    return exe

@@ -125,3 +125,34 @@ def test_isotropic_field_integral():
     assert abs(tot - len(pos) * R_P ** 3) < 0.01 * len(pos) * R_P ** 3
     sf.surface_aniso(pos)
     assert np.isfinite(sf.get_field()).all()
+
+
+def test_cpp_dropin_matches_python_path(tmp_path):
+    """include/sphgpu_surface.hpp driven as the reconstruction driver drives
+    surface_field and marchingCubes (tests/cpp/surface_dropin_main.cpp): the
+    same field and triangles as the Python mirror, bit for bit."""
+    import struct
+    import subprocess
+    from graphics_b200.surface import surface_field
+    from helpers import build_surface_dropin
+    exe = build_surface_dropin(tmp_path)
+    pos = blob(seed=4).astype(np.float32)
+    with open(tmp_path / "in.bin", "wb") as f:
+        f.write(struct.pack("i", len(pos)) + pos.tobytes())
+    r = subprocess.run([exe, str(tmp_path / "in.bin"), str(tmp_path / "f.bin"), str(tmp_path / "t.bin")],
+                       capture_output=True, timeout=300)
+    assert r.returncode == 0, r.stderr.decode()[-2000:]
+    raw = open(tmp_path / "f.bin", "rb").read()
+    num = np.frombuffer(raw[:12], np.int32)
+    field = np.frombuffer(raw[12:], np.float32)
+    tris = np.fromfile(tmp_path / "t.bin", np.float32).reshape(-1, 3, 3)
+    sf = surface_field()
+    p64 = pos.astype(np.float64)
+    sf.surface_setup(p64.min(0), p64.max(0), 0.01, 0.02, 0.005)
+    np.testing.assert_array_equal(sf.get_grid_num(), num)
+    sf.surface_aniso(pos)
+    np.testing.assert_array_equal(sf.get_field().ravel(), field)
+    g = sf.mesh(0.5)
+    assert len(g) > 100
+    np.testing.assert_array_equal(g, tris)
+    sf.close()

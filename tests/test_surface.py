@@ -128,3 +128,23 @@ def test_restated_marching_cubes_closed_surface():
     t = tris.astype(np.float64)
     vol = np.einsum("ij,ij->i", t[:, 0], np.cross(t[:, 1], t[:, 2])).sum() / 6.0
     assert abs(abs(vol) - 4 / 3 * np.pi * 8 ** 3) < 0.03 * 4 / 3 * np.pi * 8 ** 3
+
+
+def test_cpp_dropin_builds_and_reports_errors(tmp_path):
+    """include/sphgpu_surface.hpp compiles with the driver's calls
+    (tests/cpp/surface_dropin_main.cpp) and links against the library; on a
+    machine without a GPU its first call throws with the library's message."""
+    import struct
+    import subprocess
+    import torch
+    from helpers import build_surface_dropin
+    exe = build_surface_dropin(tmp_path)
+    if torch.cuda.is_available():
+        pytest.skip("the run itself is checked by tests/test_gpu_surface.py")
+    pos = blob().astype(np.float32)
+    with open(tmp_path / "in.bin", "wb") as f:
+        f.write(struct.pack("i", len(pos)) + pos.tobytes())
+    r = subprocess.run([exe, str(tmp_path / "in.bin"), str(tmp_path / "f.bin"), str(tmp_path / "t.bin")],
+                       capture_output=True, timeout=120)
+    assert r.returncode == 3
+    assert b"sphgpu_surface_create failed" in r.stderr
