@@ -40,27 +40,37 @@ UNIT = "particle-steps/s"
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM = 6650.0
 
-# Algorithmic bytes per fluid particle of each kernel class (compulsory
-# traffic: own-particle state and the neighbour index list; neighbour state
-# gathers are cache traffic and not counted).  nb = mean stored neighbours.
+# Algorithmic bytes per fluid particle of each kernel class, as the hot-path
+# byte model defines them (compulsory traffic: own-particle state in and out
+# and the 4-byte neighbour index list; gathers of neighbour state are cache
+# traffic and not counted; nb = mean stored neighbours):
+#   hash + cell id 24, integrate 64, counting sort 32, reindex 80, cell
+#   ranges 4, list build 20 + 4 nb, density + alpha 24 + 4 nb, forces + v_adv
+#   48 + 4 nb, Jacobi sweep A (rho_adv / Drho/Dt + kappa) 40 + 4 nb, Jacobi
+#   sweep B (v_adv update) 56 + 4 nb.
+# Fused kernels count the bytes of every stage they perform (the hash kernel
+# also integrates; the list build also sums rho and alpha).
 ALG_BYTES = {
-    "df_density_a": lambda nb: 16 + 16 + 4 + 4 + 4 + 4 * nb + 4 + 4 + 4,   # pos,vadv,rho,alpha,cnt,list | kr,kappa,rho_adv
-    "df_density_b": lambda nb: 16 + 16 + 4 + 4 + 4 * nb + 16,              # pos,vadv,kr,cnt,list | vadv
-    "df_div_a": lambda nb: 16 + 16 + 4 + 4 + 4 + 4 * nb + 4 + 4 + 4,
-    "df_div_b": lambda nb: 16 + 16 + 4 + 4 + 4 * nb + 16,
-    "df_forces": lambda nb: 16 + 16 + 4 + 4 + 4 * nb + 16 + 16,            # pos,vel,rho,cnt,list | acc,vadv
-    "build_first": lambda nb: 16 + 4 + 4 * nb + 4 + 4 + 16,                # pos | list,cnt,rho,alpha,(pos,rho) record
-    "hash": lambda nb: 16 + 16 + 4 + 16 + 16 + 4 + 4 + 4,                  # pos,vadv,gid | pos_s,vel_s,gid_s,key,slot
-    "reorder": lambda nb: 4 + 4 + 4 + 16 + 16 + 4 + 16 + 16 + 4 + 4 + 4 + 16,  # scatter + rank-reorder (+ v record)
-    # IISph (volume form) loop sweeps: A reads pv (pos, v_adv), ivs (gamma,
-    # sphVolume, alpha), count, list and writes kappa, V_adv / div, pk.w;
-    # B reads pk, pos (phase), v_adv, count, list and writes v_adv (+ vel in
-    # the divergence loop)
+    "df_density_a": lambda nb: 16 + 16 + 4 + 4 * nb + 4,
+    "df_density_b": lambda nb: 16 + 4 + 4 + 32 + 4 * nb,
+    "df_div_a": lambda nb: 16 + 16 + 4 + 4 * nb + 4,
+    "df_div_b": lambda nb: 16 + 4 + 4 + 32 + 4 * nb,
+    "df_forces": lambda nb: 32 + 4 * nb + 16,
+    "build_first": lambda nb: (16 + 4 + 4 * nb) + (16 + 4 * nb + 8),
+    "hash": lambda nb: 24 + 64,
+    "reorder": lambda nb: 32 + 80,
+    # IISph (volume form) loop sweeps (not in the byte model; own compulsory
+    # sets): A reads pv (pos, v_adv), ivs (gamma, sphVolume, alpha), count,
+    # list and writes kappa, V_adv / div, pk.w; B reads pk, pos (phase),
+    # v_adv, count, list and writes v_adv (+ vel in the divergence loop)
     "iv_cv_a": lambda nb: 16 + 16 + 16 + 4 + 4 * nb + 4 + 4 + 4,
     "iv_cv_b": lambda nb: 16 + 16 + 16 + 4 + 4 * nb + 16,
     "iv_div_a": lambda nb: 16 + 16 + 16 + 4 + 4 * nb + 4 + 4 + 4,
     "iv_div_b": lambda nb: 16 + 16 + 16 + 4 + 4 * nb + 16 + 16,
 }
+# cell ranges: 4 B per particle plus 8 B per cell key (count, start)
+SCAN_BYTES_PER_PARTICLE = 4
+SCAN_BYTES_PER_KEY = 8
 
 
 def parse():
@@ -81,6 +91,9 @@ def parse():
     ap.add_argument("--no-warm-start", action="store_true", help="skip the learned warm-start arm")
     ap.add_argument("--no-iisph", action="store_true",
                     help="skip the IISph (volume form) arm timed on the same settled state")
+    ap.add_argument("--no-subarms", action="store_true",
+                    help="skip the short GPU runs of the other configurations (2M warm start, 27k WCSPH, "
+                         "500k two-phase IISPH_M / PCISPH)")
     ap.add_argument("--train-seeds", default="1,2", help="jitter seeds of the training runs")
     ap.add_argument("--train-steps", type=int, default=350, help="recorded plain steps per training seed")
     ap.add_argument("--train-every", type=int, default=175, help="record every n-th particle per step")
@@ -118,16 +131,17 @@ SOLVER_KW = dict(cfl=1, cfl_factor=0.4, dt_max=2e-3, dt_min=1e-6, dt=2e-3, nu=1e
 SETTLE = [0]
 
 
-def config_dict(sc, extra=None):
-    d = {"workload": "dfsph_dam_break_%dk" % (sc.n_fluid // 1000), "n_fluid": sc.n_fluid,
-         "n_boundary": sc.n_boundary, "r": sc.r, "box": list(sc.meta["box"]), "cfl": 0.4,
-         "dt_max": SOLVER_KW["dt_max"], "settle_steps": SETTLE[0],
-         "density_goal": 1e-4, "divergence_goal": 1e-3, "max_iter": SOLVER_KW["df_density_max_iter"],
-         "div_max_iter": SOLVER_KW["df_div_max_iter"], "neighbour_cap": 48,
-         "l2": "inputs larger than L2 (neighbour lists %.0f MB + state)" % (sc.n_fluid * 48 * 4 / 1e6)}
-    if extra:
-        d.update(extra)
-    return d
+def config_dict(sc, world=1):
+    """The workload as both arms describe it (the reference arm prints the
+    same dictionary, so the two lines are for the same configuration)."""
+    return {"workload": "dfsph_dam_break_%dk" % (sc.n_fluid // 1000), "n_fluid": sc.n_fluid,
+            "n_boundary": sc.n_boundary, "r": sc.r, "box": list(sc.meta["box"]), "cfl": 0.4,
+            "dt_max": SOLVER_KW["dt_max"], "settle_steps": SETTLE[0],
+            "density_goal": 1e-4, "divergence_goal": 1e-3, "max_iter": SOLVER_KW["df_density_max_iter"],
+            "div_max_iter": SOLVER_KW["df_div_max_iter"], "neighbour_cap": 48,
+            "window": "the steps after settle_steps + warmup DFSPH steps from the seeded lattice",
+            "l2": "inputs larger than L2 (neighbour lists %.0f MB + state)" % (sc.n_fluid * 48 * 4 / 1e6),
+            "parallelism": "replicas x%d" % world if world > 1 else "single"}
 
 
 def peaks():
@@ -138,7 +152,20 @@ def peaks():
         return FALLBACK_HBM, "fallback"
 
 
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
 class ClockSampler:
+    """nvidia-smi samples (every 50 ms) of SM clock, power and throttle
+    reasons between start() and stop()."""
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -149,18 +176,18 @@ class ClockSampler:
         self.path = os.path.join(os.environ.get("SPH_BENCH_OUT", os.path.join(ROOT, "_bench_out")),
                                  "clocks_%d.csv" % gpu_index)
 
-    def __enter__(self):
+    def start(self):
         try:
             os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.f = open(self.path, "w")
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + self.QUERY,
-                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                       "--format=csv,noheader,nounits", "-lms", "50"], stdout=self.f,
                                       stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
         return self
 
-    def __exit__(self, *a):
+    def stop(self):
         if self.p:
             self.p.terminate()
             try:
@@ -169,7 +196,13 @@ class ClockSampler:
                 self.p.kill()
             self.f.close()
 
-    def summary(self):
+    def __enter__(self):
+        return self.start()
+
+    def __exit__(self, *a):
+        self.stop()
+
+    def summary(self, covers="the timed region"):
         if not self.p:
             return None
         sm, mx, reasons = [], 0.0, set()
@@ -188,16 +221,38 @@ class ClockSampler:
                     reasons.add(nm)
         if not sm:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm),
+                "covers": covers}
 
 
-def cpu_reference_sample(sc, budget, dt):
-    """Time the reference's own DFSPH (capped-bookkeeping build, OpenMP on all
-    host cores) on the same scene: steps from rest until `budget` seconds."""
+def window_dt(vel, d):
+    """The CFL step the GPU computes at the start of a step from these
+    velocities: clamp(0.4 d / max|v|, dt_min, dt_max) with an FP64 max."""
+    vmax = float(np.sqrt((np.asarray(vel, np.float64) ** 2).sum(1)).max()) if len(vel) else 0.0
+    dt = SOLVER_KW["cfl_factor"] * d / vmax if vmax > 0 else SOLVER_KW["dt_max"]
+    return float(np.float32(min(max(dt, SOLVER_KW["dt_min"]), SOLVER_KW["dt_max"])))
+
+
+def cpu_reference_window(sc, pos, vel, budget, max_steps, start_note):
+    """The reference's own DFSPH (oracle/_ref/libref_dfsph_capped.so: float,
+    OpenMP on every host core; DFSPH.cpp with only its loop bookkeeping
+    changed to an FP64 density mean and 100-iteration caps) from the GPU
+    window's start state, at a fixed dt equal to the GPU's first CFL step of
+    the window (the reference has no CFL rule).  The frame-0 neighbour
+    search and rho/alpha run untimed (the GPU did them at the end of the
+    previous step); then whole steps until `budget` seconds or `max_steps`."""
+    import dataclasses
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from oracle import make_scene_oracle
+    dt = window_dt(vel, sc.d)
     t0 = time.perf_counter()
-    o = make_scene_oracle(sc, kind="reference", solver="dfsph_capped", nu=SOLVER_KW["nu"], dt=dt)
+    sc2 = dataclasses.replace(sc, fluid_pos=np.ascontiguousarray(pos, np.float32),
+                              fluid_vel=np.ascontiguousarray(vel, np.float32))
+    o = make_scene_oracle(sc2, kind="reference", solver="dfsph_capped", nu=SOLVER_KW["nu"], dt=dt)
+    for name in ("neighbourSearch", "updateSolidPartWeight", "DF_constantDensitySolverFirst"):
+        o.stage(name)
+    o.set_frame(1)
+    o.df_iters()
     setup = time.perf_counter() - t0
     steps, t_run = 0, 0.0
     while True:
@@ -205,25 +260,53 @@ def cpu_reference_sample(sc, budget, dt):
         o.stage("runOneStep")
         t_run += time.perf_counter() - t1
         steps += 1
-        if t_run >= budget or steps >= 50:
+        if t_run >= budget or steps >= max_steps:
             break
+    it_d, it_v = o.df_iters()
     cores = o.threads()
-    rho = o.get("density")
+    rho = np.asarray(o.get("density"), np.float64)
     o.close()
-    return {"value": sc.n_fluid * steps / t_run, "unit": UNIT, "cores": cores, "kind": "reference",
-            "sample": "%d DFSPH step(s) of the %d-particle dam break from rest at fixed dt=%.1e s "
-                      "(reference DFSPH.cpp via oracle/_ref, float, density loop FP64-summed and capped at 100, "
-                      "divergence goal 0.1%% relative), setup %.1f s untimed" % (steps, sc.n_fluid, dt, setup),
-            "seconds": t_run, "mean_density": float(np.mean(rho))}
+    return {"value": sc.n_fluid * steps / t_run, "unit": UNIT, "cores": cores, "cpu_model": cpu_model(),
+            "kind": "reference", "dt": dt,
+            "iterations_per_step": {"density": it_d / steps, "divergence": it_v / steps},
+            "sample": "%d DFSPH step(s) of the %d-particle dam break from %s, fixed dt = %.4e s (the GPU "
+                      "window's first CFL step); reference DFSPH.cpp via oracle/_ref (float, density mean FP64 "
+                      "and loops capped at 100), %d OpenMP threads; setup %.1f s untimed"
+                      % (steps, sc.n_fluid, start_note, dt, cores, setup),
+            "seconds": round(t_run, 2), "mean_density_error": float(np.mean(rho) / sc.rho0 - 1.0)}
+
+
+def settle_on_gpu(sc, steps, device):
+    """The window's start state: `steps` DFSPH steps of the GPU path from the
+    seeded lattice (input preparation only; nothing here is timed)."""
+    from graphics_b200.sph import scene_to_gpu
+    g = scene_to_gpu(sc, device=device, **SOLVER_KW)
+    g.step("dfsph", steps)
+    pos, vel = g.get("position"), g.get("velocity")
+    g.close()
+    return pos, vel
 
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
     sc = workload(args.scale)
     try:
-        cb = cpu_reference_sample(sc, budget=max(30.0, args.cpu_budget * 2), dt=SOLVER_KW["dt_max"])
+        import torch
+        if not torch.cuda.is_available():
+            raise RuntimeError("no CUDA device for the window's start state")
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        pos, vel = settle_on_gpu(sc, SETTLE[0] + max(args.warmup, 1), int(os.environ.get("LOCAL_RANK", "0")))
+        note = ("the state after %d + %d DFSPH steps (settle + warm-up, the GPU arm's window start, "
+                "prepared untimed on the GPU)" % (SETTLE[0], max(args.warmup, 1)))
+    except Exception as e:
+        pos, vel = sc.fluid_pos, sc.fluid_vel
+        note = "rest (the window's start state could not be prepared: %s)" % e
+    try:
+        cb = cpu_reference_window(sc, pos, vel, budget=max(30.0, args.cpu_budget * 2), max_steps=args.steps,
+                                  start_note=note)
     except Exception as e:  # the reference build is missing
         print(json.dumps({"impl": "reference", "unavailable": "reference CPU build not loadable: %s" % e}))
         return
@@ -231,14 +314,12 @@ def run_reference(args):
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sc.n_fluid / v,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded dam break)", "config": config_dict(sc, {"parallelism": "cpu-openmp"}),
+            "data": "synthetic (seeded dam break)", "config": config_dict(sc, world),
             "cpu_baseline": cb, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
 
-def run_ours(args):
-    import torch
-
+def init_dist(torch):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -249,7 +330,38 @@ def run_ours(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
+    return world, rank, local, dist
 
+
+def timed_window(g, solver, steps, stream, torch, dist, nvtx=None):
+    """K steps of `solver` on `g`, bracketed by CUDA events on the scene's
+    stream (inputs resident); returns (max-over-ranks ms, stats)."""
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    if nvtx:
+        torch.cuda.nvtx.range_push(nvtx)
+    e0.record(stream)
+    g.step_async(solver, steps)
+    e1.record(stream)
+    st = g.synchronize()
+    if nvtx:
+        torch.cuda.nvtx.range_pop()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms, st
+
+
+def run_ours(args):
+    import torch
+    world, rank, local, dist = init_dist(torch)
     from graphics_b200.sph import scene_to_gpu
 
     sc = workload(args.scale)
@@ -268,7 +380,7 @@ def run_ours(args):
                                        record_steps=args.train_steps, every=args.train_every, epochs=20, lr=1e-3,
                                        batch=8192, device=local, dataset_cap=4_200_000, **SOLVER_KW)
         train_info = {"seeds": seeds, "samples": net.dataset_size(), "epochs": 20, "lr": 1e-3,
-                      "loss_first": float(losses[0]), "loss_last": float(losses[-1]),
+                      "loss_first": round(float(losses[0]), 4), "loss_last": round(float(losses[-1]), 4),
                       "seconds": round(time.perf_counter() - t0, 1)}
 
     # settle into the flow, then warm up (also builds the step graph)
@@ -277,13 +389,8 @@ def run_ours(args):
     settle_pos, settle_vel = g.get("position"), g.get("velocity")
     g.step("dfsph", max(args.warmup, 1))
 
-    def barrier():
-        if dist:
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    # snapshot of the state the timed region starts from; the end-to-end run
-    # replays the same steps from it through the host-buffer API
+    # snapshot of the state the timed region starts from; the end-to-end run,
+    # the FP64 check and the CPU baseline all start from it
     n0 = g.n_fluid
     snap_pos = torch.empty((n0, 3), dtype=torch.float32, pin_memory=True).numpy()
     snap_vel = torch.empty((n0, 3), dtype=torch.float32, pin_memory=True).numpy()
@@ -291,27 +398,12 @@ def run_ours(args):
     snap_vel[:] = g.get("velocity")
     g.set("position", snap_pos)  # same restaging the host-buffer path performs
     g.step("dfsph", 0)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    barrier()
-    with ClockSampler(local) as clk:
-        torch.cuda.nvtx.range_push("timed_plain")  # lets an ncu launch list select the timed steps
-        e0.record(stream)
-        g.step_async("dfsph", args.steps)
-        e1.record(stream)
-        st = g.synchronize()
-        torch.cuda.nvtx.range_pop()
-        barrier()
-    ms = e0.elapsed_time(e1)
+    clk = ClockSampler(local).start()
+    ms_max, st = timed_window(g, "dfsph", args.steps, stream, torch, dist, nvtx="timed_plain")
     end_pos = g.get("position")
     st_plain = st
-    ms_max = ms
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
     n_active = st["n_fluid"]
-    total_particle_steps = n_active * args.steps * world
-    value = total_particle_steps / (ms_max / 1e3)
+    value = n_active * args.steps * world / (ms_max / 1e3)
     it_rho = st["total_iter_density"] / args.steps
     it_div = st["total_iter_divergence"] / args.steps
     launches = args.steps * 13 + 2 * (st["total_iter_density"] + st["total_iter_divergence"])
@@ -322,7 +414,7 @@ def run_ours(args):
     hbm, peak_kind = peaks()
     kern, roof = {}, None
     if args.profile_steps > 0:
-        roof, kern = profile_kernels(g, args, hbm, peak_kind)
+        roof, kern = profile_kernels(g, args, hbm, peak_kind, sc)
 
     # learned warm start on the same window: restore the settled state, warm
     # up with the network attached (builds the per-particle history), time K
@@ -333,50 +425,135 @@ def run_ours(args):
         g.set("velocity", settle_vel)
         attach(g, net, 1)
         g.step("dfsph", max(args.warmup, 1))
-        barrier()
-        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.nvtx.range_push("timed_warm")
-        f0.record(stream)
-        g.step_async("dfsph", args.steps)
-        f1.record(stream)
-        stw = g.synchronize()
-        torch.cuda.nvtx.range_pop()
-        barrier()
-        wms = f0.elapsed_time(f1)
-        if dist:
-            t = torch.tensor([wms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            wms = float(t.item())
+        wms, stw = timed_window(g, "dfsph", args.steps, stream, torch, dist, nvtx="timed_warm")
         wval = stw["n_fluid"] * args.steps * world / (wms / 1e3)
-        warm = {"value": wval, "unit": UNIT, "ms_per_step": wms / args.steps,
+        warm = {"value": wval, "ms_per_step": round(wms / args.steps, 4),
+                "speedup_vs_plain": round(wval / value, 3),
                 "iterations_per_step": {"density": stw["total_iter_density"] / args.steps,
                                         "divergence": stw["total_iter_divergence"] / args.steps},
-                "speedup_vs_plain": wval / value,
-                "iteration_ratio": (st_plain["total_iter_density"] / max(stw["total_iter_density"], 1)),
-                "last_step": {"err_density": stw["err_density"], "status": stw["status"]},
-                "training": train_info,
-                "network": "16-64-64-1 GELU, BF16 weights/activations in mma.sync GEMMs, FP32 accumulate"}
+                "err_density_last": stw["err_density"], "status": stw["status"], "training": train_info,
+                "network": "16-64-64-1 GELU, BF16 weights/activations (mma.sync), FP32 accumulate"}
         if args.profile_steps > 0:
-            # per-kernel durations of the warm-start step (individual launches)
             g.profile(True)
             g.step("dfsph", args.profile_steps)
             prof = g.profile_read()
             g.profile(False)
             g.synchronize()
-            warm["kernels"] = {k: {"launches": c, "avg_us": round(1e3 * t / max(c, 1), 2),
-                                   "us_per_step": round(1e3 * t / args.profile_steps, 1)}
-                               for k, (t, c) in prof.items()}
+            warm["kernels_us_per_step"] = {k: round(1e3 * t / args.profile_steps, 1) for k, (t, c) in prof.items()}
         attach(g, None, 0)
         g.set("position", end_pos)  # continue from the plain run's state
 
+    e2e = run_e2e(args, g, snap_pos, snap_vel, end_pos, world, dist, torch)
+    clk.stop()
+
     iisph = None
     if not args.no_iisph:
-        iisph = run_iisph_arm(args, g, sc, settle_pos, settle_vel, st_plain["dt"], barrier, stream, dist, world,
-                              torch)
-        g.set("position", end_pos)
+        def barrier():
+            if dist:
+                dist.barrier()
+            torch.cuda.synchronize()
 
-    return run_tail(args, g, sc, st, value, ms_max, it_rho, it_div, launches, roof, kern, clk, world, rank, dist,
-                    barrier, torch, snap_pos, snap_vel, end_pos, warm, iisph)
+        iisph = run_iisph_arm(args, g, sc, settle_pos, settle_vel, st_plain["dt"], barrier, stream, dist,
+                              world, torch)
+
+    fp64 = cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            fp64 = fp64_window_check(sc, g, snap_pos, snap_vel)
+        except Exception as e:
+            fp64 = {"unavailable": str(e)}
+        try:
+            cpu = cpu_reference_window(sc, snap_pos, snap_vel, budget=args.cpu_budget, max_steps=args.steps,
+                                       start_note="the GPU window's start state (after %d + %d GPU steps)"
+                                                  % (args.settle, max(args.warmup, 1)))
+            cpu["gpu_window"] = {"dt_first_step": window_dt(snap_vel, sc.d), "dt_last_step": st_plain["dt"],
+                                 "iterations_per_step": {"density": it_rho, "divergence": it_div}}
+        except Exception as e:
+            cpu = {"unavailable": str(e)}
+    g.close()
+
+    subarms = {}
+    if not args.no_subarms and world == 1:
+        subarms = run_subarms(args, net, local, stream, torch)
+    if net is not None:
+        net.close()
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded dam break)",
+                "config": config_dict(sc, world),
+                "iterations_per_step": {"density": it_rho, "divergence": it_div},
+                "last_step": {"err_density": st["err_density"], "err_divergence": st["err_divergence"],
+                              "dt": st["dt"], "status": st["status"], "neighbour_overflow": st["neighbour_overflow"]},
+                "kernels": kern, "iisph": iisph, "roofline": roof, "fp64_check": fp64, "cpu_baseline": cpu,
+                "e2e": e2e, "gpu_launches": launches, "subarms": subarms, "warm_start": warm,
+                "clocks": clk.summary("the plain and warm-start timed windows, the kernel profile and the e2e "
+                                      "replay")}
+        print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+
+
+def run_e2e(args, g, snap_pos, snap_vel, end_pos, world, dist, torch):
+    """End to end through the C ABI with pinned host buffers: the same K
+    steps, replayed from the snapshot taken before the timed region."""
+    if args.e2e_steps <= 0:
+        return None
+    n = snap_pos.shape[0]
+    pos, vel = snap_pos.copy(), snap_vel.copy()
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+    pos, vel = pin(pos), pin(vel)
+    po = torch.empty((n, 3), dtype=torch.float32, pin_memory=True).numpy()
+    vo = torch.empty((n, 3), dtype=torch.float32, pin_memory=True).numpy()
+    g.step_host("dfsph", pos, vel, po, vo)  # untimed: builds the step graph (the inputs stay the snapshot)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        g.step_host("dfsph", pos, vel, po, vo)
+        pos, po = po, pos
+        vel, vo = vo, vel
+    sec = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([sec], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        sec = float(t.item())
+    return {"value": n * args.steps * world / sec, "unit": UNIT, "h2d_bytes_per_step": int(n * 24),
+            "d2h_bytes_per_step": int(n * 24), "steps": args.steps,
+            "same_trajectory_as_timed": bool(np.array_equal(pos, end_pos)),
+            "note": "sphgpu_step_host: pinned positions+velocities in, step, positions+velocities out"}
+
+
+def fp64_window_check(sc, g, pos, vel):
+    """The window's first step on the GPU against the FP64 build of the CPU
+    restatement (oracle/liboracle_f64.so) from the same state: the error of
+    the timed result against an FP64 oracle."""
+    import dataclasses
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import make_scene_oracle
+    g.set("position", pos)
+    g.set("velocity", vel)
+    st = g.step("dfsph", 1)
+    rg = g.get("density").astype(np.float64)
+    vg = g.get("velocity").astype(np.float64)
+    xg = g.get("position").astype(np.float64)
+    t0 = time.perf_counter()
+    sc2 = dataclasses.replace(sc, fluid_pos=np.ascontiguousarray(pos), fluid_vel=np.ascontiguousarray(vel))
+    o = make_scene_oracle(sc2, f64=True, **SOLVER_KW)
+    o.stage("df_step")
+    it, err, dt, _ = o.stats()
+    ro, vo, xo = o.get("density"), o.get("velocity"), o.get("position")
+    o.close()
+    vs = max(float(np.abs(vo).max()), 1e-30)
+    return {"oracle": "oracle/liboracle_f64.so (CPU restatement, FP64), same start state and CFL rule",
+            "max_rel_density": float(np.max(np.abs(rg - ro) / ro)),
+            "max_rel_velocity": float(np.max(np.abs(vg - vo)) / vs),
+            "max_abs_position_m": float(np.max(np.abs(xg - xo))),
+            "mean_density_error": {"gpu": float(np.mean(rg) / sc.rho0 - 1), "oracle_f64": float(np.mean(ro) / sc.rho0 - 1)},
+            "iterations": {"gpu": [st["iter_density"], st["iter_divergence"]], "oracle_f64": [it[0], it[1]]},
+            "dt": {"gpu": st["dt"], "oracle_f64": dt}, "oracle_seconds": round(time.perf_counter() - t0, 1)}
 
 
 def run_iisph_arm(args, g, sc, settle_pos, settle_vel, dt, barrier, stream, dist, world, torch):
@@ -421,8 +598,7 @@ def run_iisph_arm(args, g, sc, settle_pos, settle_vel, dt, barrier, stream, dist
         nb = st_p["mean_neighbours"]
         kern = {}
         for k, (tot_ms, cnt) in prof.items():
-            ent = {"launches": cnt, "avg_us": round(1e3 * tot_ms / max(cnt, 1), 2),
-                   "us_per_step": round(1e3 * tot_ms / args.profile_steps, 1)}
+            ent = {"n": cnt, "us": round(1e3 * tot_ms / max(cnt, 1), 1)}
             if k in ALG_BYTES:
                 ent["gbs"] = round(ALG_BYTES[k](nb) * st_p["n_fluid"] / (tot_ms / cnt / 1e3) / 1e9, 1)
             kern[k] = ent
@@ -431,24 +607,31 @@ def run_iisph_arm(args, g, sc, settle_pos, settle_vel, dt, barrier, stream, dist
     return out
 
 
-def profile_kernels(g, args, hbm, peak_kind):
+def profile_kernels(g, args, hbm, peak_kind, sc):
     g.profile(True)
     g.step("dfsph", args.profile_steps)
     prof = g.profile_read()
     g.profile(False)
     st_p = g.synchronize()
     nb = st_p["mean_neighbours"]
-    kern = {}
+    n = st_p["n_fluid"]
+    nkeys = cell_keys(sc)
+    kern, full = {}, {}
     for k, (tot_ms, cnt) in prof.items():
-        ent = {"total_ms": round(tot_ms, 4), "launches": cnt, "avg_us": round(1e3 * tot_ms / max(cnt, 1), 2)}
+        avg = tot_ms / max(cnt, 1)
+        ent = {"n": cnt, "us": round(1e3 * avg, 1)}
+        b = None
         if k in ALG_BYTES:
-            b = ALG_BYTES[k](nb) * st_p["n_fluid"]
-            ent["alg_bytes"] = int(b)
-            ent["gbs"] = round(b / (tot_ms / cnt / 1e3) / 1e9, 1)
+            b = ALG_BYTES[k](nb) * n
+        elif k == "scan":
+            b = SCAN_BYTES_PER_PARTICLE * n + SCAN_BYTES_PER_KEY * nkeys
+        if b is not None:
+            ent["gbs"] = round(b / (avg / 1e3) / 1e9, 1)
         kern[k] = ent
+        full[k] = (avg, b, tot_ms)
     # the dominant kernel: the largest share of the step among the kernels
     # with an algorithmic byte count
-    dom = max((k for k in kern if k in ALG_BYTES), key=lambda k: kern[k]["total_ms"])
+    dom = max((k for k in full if k in ALG_BYTES), key=lambda k: full[k][2])
     traffic = None
     tf = os.path.join(ROOT, "profiles", "dram_traffic_1m.json")
     if os.path.exists(tf):
@@ -456,69 +639,133 @@ def profile_kernels(g, args, hbm, peak_kind):
             traffic = json.load(open(tf)).get(dom)
         except Exception:
             traffic = None
-    roof = {"bound": "hbm", "kernel": dom, "achieved": kern[dom]["gbs"], "peak": hbm, "unit": "GB/s",
-            "frac": round(kern[dom]["gbs"] / hbm, 4), "traffic": traffic,
+    ach = full[dom][1] / (full[dom][0] / 1e3) / 1e9
+    roof = {"bound": "hbm", "kernel": dom, "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
+            "frac": round(ach / hbm, 4), "traffic": traffic,
+            "traffic_source": "ncu capture of this kernel (dram__bytes_read.sum + dram__bytes_write.sum), read "
+                              "from profiles/dram_traffic_1m.json, not measured in this run",
             "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
             "alg_bytes_per_particle": round(ALG_BYTES[dom](nb), 1), "mean_neighbours": round(nb, 2)}
-    # neighbour + density kernels (hash, scan, reorder, list build with rho/alpha)
-    ns_keys = [k for k in ("hash", "scan", "reorder", "build_first") if k in kern]
-    ns_ms = sum(kern[k]["total_ms"] / kern[k]["launches"] for k in ns_keys)
-    ns_bytes = sum(ALG_BYTES[k](nb) * st_p["n_fluid"] for k in ns_keys if k in ALG_BYTES)
-    roof["neighbour_density_group"] = {"kernels": ns_keys, "us_per_step": round(ns_ms * 1e3, 1),
-                                       "gbs": round(ns_bytes / (ns_ms / 1e3) / 1e9, 1),
-                                       "frac": round(ns_bytes / (ns_ms / 1e3) / 1e9 / hbm, 4)}
+    # neighbour + density kernels (hash with integration, cell ranges,
+    # counting sort + reindex, list build with rho/alpha)
+    ns_keys = [k for k in ("hash", "scan", "reorder", "build_first") if k in full]
+    ns_s = sum(full[k][0] for k in ns_keys) / 1e3
+    ns_bytes = sum(full[k][1] for k in ns_keys)
+    roof["neighbour_density_group"] = {"kernels": ns_keys, "us_per_step": round(ns_s * 1e6, 1),
+                                       "gbs": round(ns_bytes / ns_s / 1e9, 1),
+                                       "frac": round(ns_bytes / ns_s / 1e9 / hbm, 4)}
     return roof, kern
 
 
-def run_tail(args, g, sc, st, value, ms_max, it_rho, it_div, launches, roof, kern, clk, world, rank, dist,
-             barrier, torch, snap_pos, snap_vel, end_pos, warm, iisph=None):
-    # end to end through the C ABI with pinned host buffers: the same K steps,
-    # replayed from the snapshot taken before the timed region
-    e2e = None
-    if args.e2e_steps > 0:
-        n = snap_pos.shape[0]
-        pos, vel = snap_pos, snap_vel
-        po = torch.empty((n, 3), dtype=torch.float32, pin_memory=True).numpy()
-        vo = torch.empty((n, 3), dtype=torch.float32, pin_memory=True).numpy()
-        g.step_host("dfsph", pos, vel, po, vo)  # untimed: builds the step graph (the inputs stay the snapshot)
-        barrier()
-        t0 = time.perf_counter()
-        for _ in range(args.steps):
-            g.step_host("dfsph", pos, vel, po, vo)
-            pos, po = po, pos
-            vel, vo = vo, vel
-        t1 = time.perf_counter()
-        sec = t1 - t0
-        if dist:
-            t = torch.tensor([sec], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            sec = float(t.item())
-        e2e = {"value": n * args.steps * world / sec, "unit": UNIT, "h2d_bytes_per_step": int(n * 24),
-               "d2h_bytes_per_step": int(n * 24), "steps": args.steps,
-               "same_trajectory_as_timed": bool(np.array_equal(pos, end_pos)),
-               "note": "sphgpu_step_host: pinned positions+velocities in, step, positions+velocities out"}
+# ---- the other configurations, as short GPU runs inside the default bench ----
 
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        try:
-            cpu = cpu_reference_sample(sc, budget=args.cpu_budget, dt=st["dt"])
-        except Exception as e:
-            cpu = {"unavailable": str(e)}
-    if rank == 0:
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded dam break)",
-                "config": config_dict(sc, {"parallelism": "replicas x%d" % world if world > 1 else "single"}),
-                "iterations_per_step": {"density": it_rho, "divergence": it_div},
-                "last_step": {"err_density": st["err_density"], "err_divergence": st["err_divergence"],
-                              "dt": st["dt"], "status": st["status"], "neighbour_overflow": st["neighbour_overflow"]},
-                "warm_start": warm, "iisph": iisph,
-                "roofline": roof, "kernels": kern, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-                "clocks": clk.summary()}
-        print(json.dumps(line))
+# two-phase column (rest densities 1000 below, 3000 above): Monaghan
+# viscosity 0.02 in the fluid and 0.01 at the walls, fixed dt = 1e-3 s
+MULTI_KW = dict(dt=1e-3, nu=1e-3, soundSpeed_cs=20.0, cfl=0)
+MULTI_VISC = dict(visc_alpha=0.02, boundary_visc=0.01)
+IISPH_M_KW = dict(ii_omega=0.5, ii_eta_rel=5e-4, ii_min_iter=2, ii_max_iter=100, ii_compat=0)
+PCISPH_KW = dict(densityErro_eta=5e-3, pci_min_iter=3, pci_max_iter=50)
+# WCSPH dam break: Tait B = 50,000 Pa (c_s = sqrt(B gamma / rho0)), gamma 7,
+# Monaghan viscosity 0.01, fixed dt = 2.5e-4 s
+WCSPH_KW = dict(dt=2.5e-4, soundSpeed_cs=18.708287, wc_gamma=7.0, cfl=0)
+WCSPH_VISC = dict(visc_alpha=0.01, boundary_visc=0.01)
+
+
+def gpu_scene(sc, device, visc_alpha=0.0, boundary_visc=0.0, **kw):
+    from graphics_b200.sph import GpuScene, params_for_scene
+    g = GpuScene(params_for_scene(sc, boundary_visc=boundary_visc, **kw), sc.n_fluid, device=device)
+    g.set_boundary(sc.boundary_pos, sc.meta.get("solid_id"))
+    if sc.phase is None:
+        g.add_fluid(sc.fluid_pos, sc.fluid_vel, rho0=sc.rho0, visc_alpha=visc_alpha)
+    else:
+        for ph, rho in enumerate(sc.rho0_phases):
+            m = sc.phase == ph
+            g.add_fluid(sc.fluid_pos[m], sc.fluid_vel[m], rho0=rho, visc_alpha=visc_alpha)
+    return g
+
+
+def _stream(g, torch, device):
+    return torch.cuda.ExternalStream(g.lib.sphgpu_stream(g.h), device=torch.device("cuda", device))
+
+
+def subarm_warm_2m(args, net, device, torch):
+    """The learned warm start at 2,000,000 particles (200 x 100 x 100 block,
+    r = 0.008 m, the 1M dam break's box and goals), with the network trained
+    on plain runs of the 1M dam break: the same window (after settle +
+    warm-up steps) timed plain and with the warm start."""
+    from graphics_b200.scene import config_dfsph_2m
+    from graphics_b200.warmstart import attach
+    from graphics_b200.sph import scene_to_gpu
+    sc = config_dfsph_2m()
+    g = scene_to_gpu(sc, device=device, **SOLVER_KW)
+    s = _stream(g, torch, device)
+    g.step("dfsph", SETTLE[0])
+    pos, vel = g.get("position"), g.get("velocity")
+    g.step("dfsph", max(args.warmup, 1))
+    ms, st = timed_window(g, "dfsph", args.steps, s, torch, None)
+    out = {"config": "DFSPH dam break 2M (200x100x100, r=0.008), settle %d" % SETTLE[0],
+           "plain": {"value": st["n_fluid"] * args.steps / (ms / 1e3), "ms_per_step": round(ms / args.steps, 3),
+                     "iterations_per_step": st["total_iter_density"] / args.steps}}
+    if net is not None:
+        g.set("position", pos)
+        g.set("velocity", vel)
+        attach(g, net, 1)
+        g.step("dfsph", max(args.warmup, 1))
+        wms, sw = timed_window(g, "dfsph", args.steps, s, torch, None)
+        attach(g, None, 0)
+        out["warm"] = {"value": sw["n_fluid"] * args.steps / (wms / 1e3), "ms_per_step": round(wms / args.steps, 3),
+                       "iterations_per_step": sw["total_iter_density"] / args.steps,
+                       "err_density_last": sw["err_density"]}
+        out["speedup_vs_plain"] = round(out["warm"]["value"] / out["plain"]["value"], 3)
+        out["network"] = "the 1M-trained network (config 2 runs), features normalised as trained"
     g.close()
-    if dist:
-        dist.destroy_process_group()
+    return out
+
+
+def subarm_wcsph_27k(args, device, torch):
+    """The 27,000-particle WCSPH dam break (r = 0.025 m): 1,000 steps of
+    2.5e-4 s from the seeded lattice, all timed."""
+    from graphics_b200.scene import config_wcsph_27k
+    sc = config_wcsph_27k()
+    g = gpu_scene(sc, device, **WCSPH_VISC, **WCSPH_KW)
+    s = _stream(g, torch, device)
+    g.step("wcsph", 0)
+    ms, st = timed_window(g, "wcsph", 1000, s, torch, None)
+    rho = g.get("density").astype(np.float64)
+    g.close()
+    return {"config": "WCSPH dam break 27k (30^3, r=0.025), fixed dt 2.5e-4 s, 1000 steps from the lattice",
+            "value": st["n_fluid"] * 1000 / (ms / 1e3), "ms_per_step": round(ms / 1000, 4),
+            "mean_density_error_last": float(rho.mean() / sc.rho0 - 1.0), "status": st["status"]}
+
+
+def subarm_multiphase_500k(args, device, torch):
+    """The 500k two-phase Rayleigh-Taylor column: IISPH_M (relaxed Jacobi,
+    omega 0.5, 0.05 %) and PCISPH (0.5 %, at most 50 iterations), fixed dt =
+    1e-3 s; each timed over K steps after W warm-up steps from the lattice."""
+    from graphics_b200.scene import config_multiphase_500k
+    sc = config_multiphase_500k()
+    out = {"config": "two-phase column 500,094 (63x126x63, rho0 1000/3000), fixed dt 1e-3 s"}
+    for name, solver, kw in (("iisph_m", "iisph_m", IISPH_M_KW), ("pcisph", "pcisph", PCISPH_KW)):
+        g = gpu_scene(sc, device, **MULTI_VISC, **MULTI_KW, **kw)
+        s = _stream(g, torch, device)
+        g.step(solver, max(args.warmup, 1))
+        ms, st = timed_window(g, solver, args.steps, s, torch, None)
+        out[name] = {"value": st["n_fluid"] * args.steps / (ms / 1e3), "ms_per_step": round(ms / args.steps, 3),
+                     "iterations_per_step": st["total_iter_density"] / args.steps, "status": st["status"]}
+        g.close()
+    return out
+
+
+def run_subarms(args, net, device, stream, torch):
+    out = {}
+    for name, fn in (("config5_warm_start_2m", lambda: subarm_warm_2m(args, net, device, torch)),
+                     ("config1_wcsph_27k", lambda: subarm_wcsph_27k(args, device, torch)),
+                     ("config3_multiphase_500k", lambda: subarm_multiphase_500k(args, device, torch))):
+        try:
+            out[name] = fn()
+        except Exception as e:
+            out[name] = {"error": str(e)[:300]}
+    return out
 
 
 def lpt_shards(sizes, world):

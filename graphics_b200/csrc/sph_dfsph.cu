@@ -402,6 +402,3 @@ void launch_df_div_b(const DevScene& s, const SolverConst& c, int n_max, double 
 void launch_cfl(const DevScene& s, int n_max, float cfl, float d, float dt_max, float dt_min, cudaStream_t st) {
     k_cfl<<<nblk(n_max), NT, 0, st>>>(s, cfl, d, dt_max, dt_min);
 }
-void launch_df_first(const DevScene& s, const SolverConst& c, int n_max, cudaStream_t st) {
-    (void)s; (void)c; (void)n_max; (void)st;  // fused into the neighbour-list kernel (launch_build mode 1)
-}

@@ -187,7 +187,6 @@ void launch_boundary_volume(const DevScene& s, const GridGeom& g, float dpart, f
                             cudaStream_t st);
 
 // ---- DFSPH (sph_dfsph.cu) ----
-void launch_df_first(const DevScene& s, const SolverConst& c, int n_max, cudaStream_t st);
 // bs: threads per block (64, 128 or 256; the autotuner's choice)
 void launch_df_forces(const DevScene& s, const SolverConst& c, int n_max, int warm, cudaStream_t st, int bs = 128);
 void launch_df_dens_a(const DevScene& s, const SolverConst& c, int n_max, int record, cudaStream_t st, int bs = 128);

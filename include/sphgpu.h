@@ -462,9 +462,16 @@ int sphgpu_batch_scene_range(sphgpu_t h, int scene, int* first, int* count);
  * every call leaves at zero, so n is limited to SPHGPU_NOALLOC_MAX_N;
  * larger n is rejected with SPHGPU_EINVAL before any GPU work.  The first
  * call on a device (with that device current) looks up the scratch address
- * once (cudaGetSymbolAddress); make it before any stream capture.  All calls
+ * once (cudaGetSymbolAddress); make it before any stream capture.  The
+ * address is kept for the life of the process: after cudaDeviceReset on a
+ * device the library module is loaded anew and the kept address is stale,
+ * so do not use this entry point on a device that has been reset.  All calls
  * on one device share the scratch: calls that overlap in time (other
  * streams, other threads) race on it and must be serialised by the caller.
+ * A velocity with a non-finite component makes vmax and dt NaN (the step is
+ * not silently computed from the other particles); n = 0 gives vmax = 0 and
+ * dt = dt_max.  Launch errors are reported with cudaPeekAtLastError, so an
+ * earlier error of other work is returned as SPHGPU_ECUDA but not cleared.
  * Returns 0, SPHGPU_EINVAL or SPHGPU_ECUDA. */
 #define SPHGPU_NOALLOC_MAX_N 8388608
 int sphgpu_cfl_dt_noalloc(const float* vel, int n, int stride, float cfl_factor, float d, float dt_max,

@@ -18,6 +18,7 @@
 // error here; out_of_box() reports it).
 #pragma once
 
+#include <climits>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -81,6 +82,7 @@ public:
 private:
     const std::vector<float>& run(const std::vector<Vec3d>& position, int aniso) {
         if (!h_) throw std::runtime_error("surface_setup has not been called");
+        if (position.size() > (size_t)INT_MAX) throw std::runtime_error("surface_field: more than INT_MAX particles");
         std::vector<float> xyz(3 * position.size());
         for (size_t i = 0; i < position.size(); ++i)
             for (int c = 0; c < 3; ++c) xyz[3 * i + c] = (float)position[i][c];

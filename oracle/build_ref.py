@@ -1,6 +1,9 @@
 #!/usr/bin/env python3
 """Build the reference's own CPU solver code into oracle/_ref/ (test infrastructure).
 
+    python oracle/build_ref.py <reference Source/ directory>
+    (or SPH_REFERENCE_SOURCE=<dir> python oracle/build_ref.py)
+
 Recipe, run in the build container only (the reference tree is not present on
 the GPU machines; the built libraries travel there instead):
 
@@ -35,7 +38,8 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("SPH_REFERENCE_SOURCE", "/root/reference/Source")
+# the reference's Source/ directory: the first argument, else $SPH_REFERENCE_SOURCE
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SPH_REFERENCE_SOURCE", "")
 ROOT = os.path.dirname(HERE)
 OUT = os.path.join(HERE, "_ref")
 SRC = os.path.join(OUT, "src")
@@ -93,6 +97,14 @@ DF_CAP = [
      "\t\tdouble densitySum = 0;\n\t\tint maximumIteration = 50;"),
     ("\t\twhile (errorRate > errorRateGoal || currentIteration < minimumIteration)\n",
      "\t\twhile ((errorRate > errorRateGoal || currentIteration < minimumIteration) && currentIteration < REF_DF_MAXITER)\n"),
+    # iteration counts of both loops, summed for the harness to read
+    # (ref_df_iters); inserted on the loops' closing lines, so line numbers
+    # stay those of DFSPH.cpp
+    ("\t\t} //end of iteration\n",
+     "\t\t} { extern int ref_df_iter_count[2]; ref_df_iter_count[0] += currentIteration; } //end of iteration\n"),
+    ("\t\t} // end of the iteration\n\n\t\t/* loop particle 4 */",
+     "\t\t} { extern int ref_df_iter_count[2]; ref_df_iter_count[1] += currentIteration; } // end of the iteration"
+     "\n\n\t\t/* loop particle 4 */"),
 ]
 
 SOLVERS = {
@@ -144,8 +156,8 @@ def write_if_changed(dst, t):
 
 
 def main():
-    if not os.path.isdir(REF):
-        print("reference sources not present (%s); keeping prebuilt oracle/_ref" % REF)
+    if not REF or not os.path.isdir(REF):
+        print("reference sources not given or not present (%r); keeping prebuilt oracle/_ref" % REF)
         return 0
     os.makedirs(SRC, exist_ok=True)
     for f in FILES:

@@ -320,6 +320,14 @@ class Oracle:
         self.lib.ref_vf_iters(self.h, C.byref(a), C.byref(b))
         return a.value, b.value
 
+    def df_iters(self):
+        """Reference "dfsph_capped" build: (density, divergence) loop
+        iterations summed since the last call (read and reset)."""
+        a, b = C.c_int(), C.c_int()
+        if self.lib.ref_df_iters(C.byref(a), C.byref(b)) != 0:
+            raise RuntimeError("iteration counts exist in the dfsph_capped reference build only")
+        return a.value, b.value
+
     def vf_stats(self):
         """Port only: ((it_div, it_cv), (err_div, err_cv)) of the last IISph loops."""
         it = (C.c_int * 2)()

@@ -22,6 +22,10 @@
 #include <unistd.h>
 #include REF_SOLVER_HEADER
 
+#ifdef REF_TAG_dfsph_capped
+int ref_df_iter_count[2];  // written by the capped DFSPH loops
+#endif
+
 extern "C" {
 struct RefParams {
     double spacing_r, smoothRadius_h, dt;
@@ -325,6 +329,21 @@ public:
         return -1;
 #endif
     }
+    /* DFSPH "capped" build: density and divergence loop iterations summed
+     * since the last call (counted on the loops' closing lines by
+     * build_ref.py's edit of the copy); read and reset.  Returns -1 for the
+     * other builds. */
+    static int ref_df_iters_impl(int* dens, int* div) {
+#ifdef REF_TAG_dfsph_capped
+        *dens = ref_df_iter_count[0];
+        *div = ref_df_iter_count[1];
+        ref_df_iter_count[0] = ref_df_iter_count[1] = 0;
+        return 0;
+#else
+        *dens = *div = 0;
+        return -1;
+#endif
+    }
     static int ref_set_solid_impl(void* hh, int k, const char* field, const double* in) {
         RefHarness* h = static_cast<RefHarness*>(hh);
         auto& v = h->m_Solids[k].boundaryParticles;
@@ -405,6 +424,7 @@ void ref_set_frame(void* hh, int f) { RefHarness::ref_set_frame_impl(hh, f); }
 double ref_kernel(void* hh, int grad, double r) { return RefHarness::ref_kernel_impl(hh, grad, r); }
 int ref_set_iter_limits(void* hh, int mn, int mx) { return RefHarness::ref_set_iter_limits_impl(hh, mn, mx); }
 int ref_vf_iters(void* hh, int* df, int* cv) { return RefHarness::ref_vf_iters_impl(hh, df, cv); }
+int ref_df_iters(int* dens, int* div) { return RefHarness::ref_df_iters_impl(dens, div); }
 int ref_set_solid(void* hh, int k, const char* field, const double* in) { return RefHarness::ref_set_solid_impl(hh, k, field, in); }
 /* SphBase::SphBase sets the OpenMP thread count to omp_get_num_procs()
  * (SphBase.cpp:242-243); this overrides it (1 thread makes the racy loops of
