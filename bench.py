@@ -233,18 +233,19 @@ def window_dt(vel, d):
     return float(np.float32(min(max(dt, SOLVER_KW["dt_min"]), SOLVER_KW["dt_max"])))
 
 
-def cpu_reference_window(sc, pos, vel, budget, max_steps, start_note):
+def cpu_reference_window(sc, pos, vel, dts, budget, max_steps, start_note):
     """The reference's own DFSPH (oracle/_ref/libref_dfsph_capped.so: float,
     OpenMP on every host core; DFSPH.cpp with only its loop bookkeeping
     changed to an FP64 density mean and 100-iteration caps) from the GPU
-    window's start state, at a fixed dt equal to the GPU's first CFL step of
-    the window (the reference has no CFL rule).  The frame-0 neighbour
-    search and rho/alpha run untimed (the GPU did them at the end of the
-    previous step); then whole steps until `budget` seconds or `max_steps`."""
+    window's start state, step k at the GPU window's k-th CFL step dts[k]
+    (the reference has no CFL rule; its m_TH.dt is set before each step).
+    The frame-0 neighbour search and rho/alpha run untimed (the GPU did them
+    at the end of the previous step); then whole steps until `budget`
+    seconds or `max_steps`."""
     import dataclasses
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from oracle import make_scene_oracle
-    dt = window_dt(vel, sc.d)
+    dt = dts[0]
     t0 = time.perf_counter()
     sc2 = dataclasses.replace(sc, fluid_pos=np.ascontiguousarray(pos, np.float32),
                               fluid_vel=np.ascontiguousarray(vel, np.float32))
@@ -256,6 +257,7 @@ def cpu_reference_window(sc, pos, vel, budget, max_steps, start_note):
     setup = time.perf_counter() - t0
     steps, t_run = 0, 0.0
     while True:
+        o.set_dt(dts[steps % len(dts)])
         t1 = time.perf_counter()
         o.stage("runOneStep")
         t_run += time.perf_counter() - t1
@@ -266,25 +268,28 @@ def cpu_reference_window(sc, pos, vel, budget, max_steps, start_note):
     cores = o.threads()
     rho = np.asarray(o.get("density"), np.float64)
     o.close()
+    used = [dts[k % len(dts)] for k in range(steps)]
     return {"value": sc.n_fluid * steps / t_run, "unit": UNIT, "cores": cores, "cpu_model": cpu_model(),
-            "kind": "reference", "dt": dt,
+            "kind": "reference", "dt_first": used[0], "dt_mean": float(np.mean(used)),
             "iterations_per_step": {"density": it_d / steps, "divergence": it_v / steps},
-            "sample": "%d DFSPH step(s) of the %d-particle dam break from %s, fixed dt = %.4e s (the GPU "
-                      "window's first CFL step); reference DFSPH.cpp via oracle/_ref (float, density mean FP64 "
-                      "and loops capped at 100), %d OpenMP threads; setup %.1f s untimed"
-                      % (steps, sc.n_fluid, start_note, dt, cores, setup),
+            "sample": "%d DFSPH step(s) of the %d-particle dam break from %s, each at the GPU window's CFL step "
+                      "of the same index (%.3e..%.3e s); reference DFSPH.cpp via oracle/_ref (float, density "
+                      "mean FP64 and loops capped at 100), %d OpenMP threads; setup %.1f s untimed"
+                      % (steps, sc.n_fluid, start_note, min(used), max(used), cores, setup),
             "seconds": round(t_run, 2), "mean_density_error": float(np.mean(rho) / sc.rho0 - 1.0)}
 
 
-def settle_on_gpu(sc, steps, device):
-    """The window's start state: `steps` DFSPH steps of the GPU path from the
-    seeded lattice (input preparation only; nothing here is timed)."""
+def settle_on_gpu(sc, steps, device, window):
+    """The window's start state -- `steps` DFSPH steps of the GPU path from
+    the seeded lattice -- and the CFL steps of the `window` steps that follow
+    (input preparation only; nothing here is timed)."""
     from graphics_b200.sph import scene_to_gpu
     g = scene_to_gpu(sc, device=device, **SOLVER_KW)
     g.step("dfsph", steps)
     pos, vel = g.get("position"), g.get("velocity")
+    dts = [g.step("dfsph", 1)["dt"] for _ in range(window)]
     g.close()
-    return pos, vel
+    return pos, vel, dts
 
 
 def run_reference(args):
@@ -298,14 +303,16 @@ def run_reference(args):
         if not torch.cuda.is_available():
             raise RuntimeError("no CUDA device for the window's start state")
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-        pos, vel = settle_on_gpu(sc, SETTLE[0] + max(args.warmup, 1), int(os.environ.get("LOCAL_RANK", "0")))
+        pos, vel, dts = settle_on_gpu(sc, SETTLE[0] + max(args.warmup, 1), int(os.environ.get("LOCAL_RANK", "0")),
+                                      args.steps)
         note = ("the state after %d + %d DFSPH steps (settle + warm-up, the GPU arm's window start, "
                 "prepared untimed on the GPU)" % (SETTLE[0], max(args.warmup, 1)))
     except Exception as e:
         pos, vel = sc.fluid_pos, sc.fluid_vel
+        dts = [window_dt(vel, sc.d)]
         note = "rest (the window's start state could not be prepared: %s)" % e
     try:
-        cb = cpu_reference_window(sc, pos, vel, budget=max(30.0, args.cpu_budget * 2), max_steps=args.steps,
+        cb = cpu_reference_window(sc, pos, vel, dts, budget=max(30.0, args.cpu_budget * 2), max_steps=args.steps,
                                   start_note=note)
     except Exception as e:  # the reference build is missing
         print(json.dumps({"impl": "reference", "unavailable": "reference CPU build not loadable: %s" % e}))
@@ -458,15 +465,16 @@ def run_ours(args):
 
     fp64 = cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        dts = [window_dt(snap_vel, sc.d)]
         try:
-            fp64 = fp64_window_check(sc, g, snap_pos, snap_vel)
+            fp64, dts = fp64_window_check(sc, g, snap_pos, snap_vel, args.steps)
         except Exception as e:
             fp64 = {"unavailable": str(e)}
         try:
-            cpu = cpu_reference_window(sc, snap_pos, snap_vel, budget=args.cpu_budget, max_steps=args.steps,
+            cpu = cpu_reference_window(sc, snap_pos, snap_vel, dts, budget=args.cpu_budget, max_steps=args.steps,
                                        start_note="the GPU window's start state (after %d + %d GPU steps)"
                                                   % (args.settle, max(args.warmup, 1)))
-            cpu["gpu_window"] = {"dt_first_step": window_dt(snap_vel, sc.d), "dt_last_step": st_plain["dt"],
+            cpu["gpu_window"] = {"dt_mean": float(np.mean(dts)),
                                  "iterations_per_step": {"density": it_rho, "divergence": it_div}}
         except Exception as e:
             cpu = {"unavailable": str(e)}
@@ -526,10 +534,11 @@ def run_e2e(args, g, snap_pos, snap_vel, end_pos, world, dist, torch):
             "note": "sphgpu_step_host: pinned positions+velocities in, step, positions+velocities out"}
 
 
-def fp64_window_check(sc, g, pos, vel):
+def fp64_window_check(sc, g, pos, vel, window):
     """The window's first step on the GPU against the FP64 build of the CPU
     restatement (oracle/liboracle_f64.so) from the same state: the error of
-    the timed result against an FP64 oracle."""
+    the timed result against an FP64 oracle.  Also returns the CFL steps of
+    the window (the GPU replays it step by step from the same state)."""
     import dataclasses
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from oracle import make_scene_oracle
@@ -539,6 +548,7 @@ def fp64_window_check(sc, g, pos, vel):
     rg = g.get("density").astype(np.float64)
     vg = g.get("velocity").astype(np.float64)
     xg = g.get("position").astype(np.float64)
+    dts = [st["dt"]] + [g.step("dfsph", 1)["dt"] for _ in range(window - 1)]
     t0 = time.perf_counter()
     sc2 = dataclasses.replace(sc, fluid_pos=np.ascontiguousarray(pos), fluid_vel=np.ascontiguousarray(vel))
     o = make_scene_oracle(sc2, f64=True, **SOLVER_KW)
@@ -553,7 +563,7 @@ def fp64_window_check(sc, g, pos, vel):
             "max_abs_position_m": float(np.max(np.abs(xg - xo))),
             "mean_density_error": {"gpu": float(np.mean(rg) / sc.rho0 - 1), "oracle_f64": float(np.mean(ro) / sc.rho0 - 1)},
             "iterations": {"gpu": [st["iter_density"], st["iter_divergence"]], "oracle_f64": [it[0], it[1]]},
-            "dt": {"gpu": st["dt"], "oracle_f64": dt}, "oracle_seconds": round(time.perf_counter() - t0, 1)}
+            "dt": {"gpu": st["dt"], "oracle_f64": dt}, "oracle_seconds": round(time.perf_counter() - t0, 1)}, dts
 
 
 def run_iisph_arm(args, g, sc, settle_pos, settle_vel, dt, barrier, stream, dist, world, torch):
@@ -738,20 +748,46 @@ def subarm_wcsph_27k(args, device, torch):
             "mean_density_error_last": float(rho.mean() / sc.rho0 - 1.0), "status": st["status"]}
 
 
-def subarm_multiphase_500k(args, device, torch):
-    """The 500k two-phase Rayleigh-Taylor column: IISPH_M (relaxed Jacobi,
-    omega 0.5, 0.05 %) and PCISPH (0.5 %, at most 50 iterations), fixed dt =
-    1e-3 s; each timed over K steps after W warm-up steps from the lattice."""
+def settled_column_500k(device, steps=300):
+    """The 500k column settled under gravity: the reference's iterative
+    multiphase solvers do not hold a 126-layer column started from the
+    lattice at rest (PCISPH and IISPH_M reach their iteration caps in the
+    first steps, compress it past the neighbour cap and blow it apart, in
+    the CPU restatement as on the GPU), so, as the reference's own settled
+    column fixture is made, the column first settles as one fluid under
+    DFSPH (fixed dt 1e-3 s, `steps` steps); then the particles above the
+    perturbed interface become the heavy phase."""
+    import dataclasses
     from graphics_b200.scene import config_multiphase_500k
     sc = config_multiphase_500k()
-    out = {"config": "two-phase column 500,094 (63x126x63, rho0 1000/3000), fixed dt 1e-3 s"}
+    one = dataclasses.replace(sc, phase=None, rho0_phases=(sc.rho0,))
+    g = gpu_scene(one, device, **MULTI_VISC, **{**SOLVER_KW, "cfl": 0, "dt": 1e-3})
+    g.step("dfsph", steps)
+    pos, vel = g.get("position"), g.get("velocity")
+    g.close()
+    x, y, z = (pos[:, k].astype(np.float64) for k in range(3))
+    box = sc.meta["box"]
+    iface = box[1] / 2 + 0.02 * np.sin(2 * np.pi * x) * np.sin(2 * np.pi * z)
+    return dataclasses.replace(sc, fluid_pos=np.ascontiguousarray(pos), fluid_vel=np.ascontiguousarray(vel),
+                               phase=(y > iface).astype(np.int32))
+
+
+def subarm_multiphase_500k(args, device, torch):
+    """The 500k two-phase Rayleigh-Taylor column (settled first, see
+    settled_column_500k): IISPH_M (relaxed Jacobi, omega 0.5, 0.05 %) and
+    PCISPH (0.5 %, at most 50 iterations), fixed dt = 1e-3 s; each timed
+    over K steps after W warm-up steps."""
+    sc = settled_column_500k(device)
+    out = {"config": "two-phase column 500,094 (63x126x63, rho0 1000/3000), fixed dt 1e-3 s, from the column "
+                     "settled as one fluid (300 DFSPH steps)"}
     for name, solver, kw in (("iisph_m", "iisph_m", IISPH_M_KW), ("pcisph", "pcisph", PCISPH_KW)):
         g = gpu_scene(sc, device, **MULTI_VISC, **MULTI_KW, **kw)
         s = _stream(g, torch, device)
         g.step(solver, max(args.warmup, 1))
         ms, st = timed_window(g, solver, args.steps, s, torch, None)
         out[name] = {"value": st["n_fluid"] * args.steps / (ms / 1e3), "ms_per_step": round(ms / args.steps, 3),
-                     "iterations_per_step": st["total_iter_density"] / args.steps, "status": st["status"]}
+                     "iterations_per_step": st["total_iter_density"] / args.steps, "status": st["status"],
+                     "n_fluid": st["n_fluid"]}
         g.close()
     return out
 
@@ -760,7 +796,8 @@ def run_subarms(args, net, device, stream, torch):
     out = {}
     for name, fn in (("config5_warm_start_2m", lambda: subarm_warm_2m(args, net, device, torch)),
                      ("config1_wcsph_27k", lambda: subarm_wcsph_27k(args, device, torch)),
-                     ("config3_multiphase_500k", lambda: subarm_multiphase_500k(args, device, torch))):
+                     ("config3_multiphase_500k", lambda: subarm_multiphase_500k(args, device, torch)),
+                     ("config4_batched_64", lambda: subarm_batched_64(args, device, torch))):
         try:
             out[name] = fn()
         except Exception as e:
@@ -779,74 +816,44 @@ def lpt_shards(sizes, world):
     return [sorted(p) for p in parts]
 
 
-def run_batched(args):
-    """64 independent dam breaks (10k-200k particles, log-uniform) in one
-    batch per GPU: one neighbour search and one launch per sweep for all of
-    them, per-scene CFL step and loop convergence.  Multi-GPU: scenes sharded
-    over ranks (longest first), no data-path collective; value = all ranks'
-    particle-steps / max-over-ranks time."""
-    import torch
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
-    from graphics_b200.scene import config_batched_dfsph
+def batched_window(scenes, args, device, torch, dist, unbatched):
+    """One batch of independent dam breaks on this GPU: settle (at most 100
+    steps), the block-size autotuner, W warm-up steps, then K steps timed
+    with CUDA events (max over ranks).  Also: the per-kernel event times of
+    a few host-driven steps, whose sum against the graph-timed step gives
+    the launch overhead per step; with `unbatched`, the same scenes from the
+    same states stepped one single-scene handle after another."""
     from graphics_b200.sph import batch_to_gpu, scene_to_gpu
-    scenes_all = config_batched_dfsph(64, seed=0)
-    mine = lpt_shards([s.n_fluid for s in scenes_all], world)[rank]
-    scenes = [scenes_all[i] for i in mine]
-    b = batch_to_gpu(scenes, device=local, **SOLVER_KW)
-    stream = torch.cuda.ExternalStream(b.lib.sphgpu_stream(b.h), device=torch.device("cuda", local))
+    b = batch_to_gpu(scenes, device=device, **SOLVER_KW)
+    stream = torch.cuda.ExternalStream(b.lib.sphgpu_stream(b.h), device=torch.device("cuda", device))
     settle = min(args.settle, 100)
     if settle:
         b.step("dfsph", settle)
     tune = b.autotune("dfsph", 2)
     b.step("dfsph", max(args.warmup, 1))
-
-    def barrier():
-        if dist:
-            dist.barrier()
-        torch.cuda.synchronize()
-
     n0 = b.n_fluid
     snap = [(b.get_scene("position", k), b.get_scene("velocity", k)) for k in range(len(scenes))]
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    barrier()
-    with ClockSampler(local) as clk:
-        e0.record(stream)
-        b.step_async("dfsph", args.steps)
-        e1.record(stream)
-        st = b.synchronize()
-        barrier()
-    ms = e0.elapsed_time(e1)
+    ms, st = timed_window(b, "dfsph", args.steps, stream, torch, dist)
     per = b.scene_stats()
-    ms_max = ms
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
-        tot = torch.tensor([float(st["n_fluid"])], device="cuda")
-        dist.all_reduce(tot)
-        n_all = tot.item()
-    else:
-        n_all = st["n_fluid"]
-    value = n_all * args.steps / (ms_max / 1e3)
-    its = [p["total_iter_density"] / args.steps for p in per]
-    # the same scenes from the same states, one handle after another
+    its = [p_["total_iter_density"] / args.steps for p_ in per]
+    # kernel time per step (individual launches with events) on the next steps
+    b.profile(True)
+    nprof = 3
+    b.step("dfsph", nprof)
+    prof = b.profile_read()
+    b.profile(False)
+    stp = b.synchronize()
+    kern_ms = sum(t for t, c in prof.values()) / nprof
+    launches = sum(c for t, c in prof.values()) / nprof
+    b.close()
     unb = None
-    if world == 1 and rank == 0:
+    if unbatched:
         t_seq = 0.0
         for k, sc in enumerate(scenes):
-            g = scene_to_gpu(sc, device=local, **SOLVER_KW)
+            g = scene_to_gpu(sc, device=device, **SOLVER_KW)
             g.set("position", snap[k][0])
             g.set("velocity", snap[k][1])
-            s2 = torch.cuda.ExternalStream(g.lib.sphgpu_stream(g.h), device=torch.device("cuda", local))
+            s2 = torch.cuda.ExternalStream(g.lib.sphgpu_stream(g.h), device=torch.device("cuda", device))
             g.step("dfsph", 1)
             g.set("position", snap[k][0])
             g.set("velocity", snap[k][1])
@@ -862,6 +869,41 @@ def run_batched(args):
             g.close()
         unb = {"value": n0 * args.steps / (t_seq / 1e3), "unit": UNIT, "ms_per_step": t_seq / args.steps,
                "note": "the same scenes from the same states, one single-scene handle after another"}
+    it_prof = (stp["total_iter_density"] + stp["total_iter_divergence"]) / nprof
+    return {"ms": ms, "st": st, "n0": n0, "settle": settle, "tune": tune, "unbatched": unb,
+            "iterations_per_step": {"density_min": min(its), "density_max": max(its),
+                                    "density_mean": sum(its) / len(its)},
+            "launch_overhead": {"kernel_ms_per_step": round(kern_ms, 4),
+                                "launches_per_step": round(launches, 1),
+                                "loop_iterations_per_step": round(it_prof, 2),
+                                "note": "sum of the event-timed kernels of host-driven steps; against the graph-timed "
+                                        "ms_per_step (different steps, same flow) the difference is the launch and "
+                                        "dependency overhead of the graph's kernel nodes"}}
+
+
+def run_batched(args):
+    """64 independent dam breaks (10k-200k particles, log-uniform) in one
+    batch per GPU: one neighbour search and one launch per sweep for all of
+    them, per-scene CFL step and loop convergence.  Multi-GPU: scenes sharded
+    over ranks (longest first), no data-path collective; value = all ranks'
+    particle-steps / max-over-ranks time."""
+    import torch
+    world, rank, local, dist = init_dist(torch)
+    from graphics_b200.scene import config_batched_dfsph
+    scenes_all = config_batched_dfsph(64, seed=0)
+    mine = lpt_shards([s.n_fluid for s in scenes_all], world)[rank]
+    scenes = [scenes_all[i] for i in mine]
+    with ClockSampler(local) as clk:
+        r = batched_window(scenes, args, local, torch, dist, unbatched=(world == 1))
+    ms_max, st = r["ms"], r["st"]
+    if dist:
+        tot = torch.tensor([float(st["n_fluid"])], device="cuda")
+        dist.all_reduce(tot)
+        n_all = tot.item()
+    else:
+        n_all = st["n_fluid"]
+    value = n_all * args.steps / (ms_max / 1e3)
+    unb = r["unbatched"]
     if rank == 0:
         line = {"metric": "batched DFSPH particle-steps/s (64 independent scenes, 10k-200k particles each)",
                 "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -870,18 +912,34 @@ def run_batched(args):
                 "config": {"workload": "batched_dfsph_64", "n_scenes": len(scenes_all),
                            "n_fluid_total": int(sum(s.n_fluid for s in scenes_all)),
                            "n_boundary_total": int(sum(s.n_boundary for s in scenes_all)),
-                           "scenes_on_rank0": len(scenes), "r": 0.01, "settle_steps": settle,
+                           "scenes_on_rank0": len(scenes), "r": 0.01, "settle_steps": r["settle"],
                            "parallelism": "scene shards x%d (LPT)" % world if world > 1 else "single",
                            "l2": "inputs larger than L2"},
-                "iterations_per_step": {"density_min": min(its), "density_max": max(its),
-                                        "density_mean": sum(its) / len(its)},
-                "autotune": tune, "unbatched": unb,
+                "iterations_per_step": r["iterations_per_step"], "launch_overhead": r["launch_overhead"],
+                "autotune": r["tune"], "unbatched": unb,
                 "speedup_vs_unbatched": (value / unb["value"]) if unb else None,
-                "gpu_launches": None, "clocks": clk.summary()}
+                "gpu_launches": int(round(r["launch_overhead"]["launches_per_step"] * args.steps)),
+                "clocks": clk.summary()}
         print(json.dumps(line))
-    b.close()
     if dist:
         dist.destroy_process_group()
+
+
+def subarm_batched_64(args, device, torch):
+    """The batched configuration (64 independent dam breaks of 10k-200k
+    particles in one batch), compactly: value, the autotuner's choice, the
+    launch overhead per step and the speed-up over the same scenes stepped
+    one handle after another."""
+    from graphics_b200.scene import config_batched_dfsph
+    scenes = config_batched_dfsph(64, seed=0)
+    r = batched_window(scenes, args, device, torch, None, unbatched=True)
+    value = r["st"]["n_fluid"] * args.steps / (r["ms"] / 1e3)
+    unb = r["unbatched"]
+    return {"config": "64 dam breaks, %d fluid particles in all, settle %d" % (r["n0"], r["settle"]),
+            "value": value, "ms_per_step": round(r["ms"] / args.steps, 3),
+            "iterations_per_step": r["iterations_per_step"], "launch_overhead": r["launch_overhead"],
+            "autotune": r["tune"].get("chosen", r["tune"]),
+            "unbatched_value": unb["value"], "speedup_vs_unbatched": round(value / unb["value"], 3)}
 
 
 # Dynamic rigid body: the DFSPH step with a 0.4 m box of density 500

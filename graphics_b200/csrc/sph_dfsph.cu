@@ -81,7 +81,11 @@ __global__ void k_loop_reset(DevScene s, int which) {
     s.st->cont = 1;
 }
 
-// non-pressure accelerations (gravity + viscosity) and v_adv
+// non-pressure accelerations (gravity + viscosity) and v_adv.  The list is
+// read four entries at a time (one 16-byte load, the next group's issued
+// before the current group's record gathers) and each neighbour costs one
+// 32-byte record; the per-pair divisions become reciprocals (1/rho_i once
+// per particle, 1/rho_j and 1/(r^2 + 0.01 h^2) per pair).
 template <int BS>
 __global__ void __launch_bounds__(BS) k_df_forces(DevScene s, SolverConst c, int warm) {
     const int n = s.st->n_active;
@@ -92,32 +96,48 @@ __global__ void __launch_bounds__(BS) k_df_forces(DevScene s, SolverConst c, int
         const float dt = dt_of(s, pa);
         const float4 va = s.vel[p];
         const float rhoa = s.rho[p];
-        const float fm0 = c.fm0, rho0 = c.rho0;
+        const float fm0 = c.fm0;
+        const float bm = c.rho0 * __frcp_rn(rhoa);  // (frho0*volume)/fa.density = bm * volume, DFSPH.cpp:1353
         const float den0 = 0.01f * c.hs * c.hs;
         const float visc = 10.f * c.nu;
         float ax = c.gravity[0], ay = c.gravity[1], az = c.gravity[2];
         const int cnt = s.ncount[p];
+        const int ng = (cnt + 3) >> 2;
         const size_t stride = (size_t)c.stride;
-        for (int k = 0; k < cnt; ++k) {
-            const unsigned e = (unsigned)ell_get(s.nbr, stride, p, k);
-            // one 32-byte record per neighbour: {(x, y, z, rho), v} or, for
-            // a boundary particle, {(x, y, z, volume), singleVelocity +
-            // velocity} (DFSPH.cpp:1349)
-            float4 pb, vb;
-            const bool bnd = (e & BND_FLAG) != 0u;
-            ld_record32((bnd ? s.bpf : s.prv) + 2 * (size_t)(e & BND_MASK), pb, vb);
-            const float m = bnd ? rho0 * pb.w / rhoa   // (frho0*volume)/fa.density, DFSPH.cpp:1353
-                                : fm0 / pb.w;          // fm0/fb.density, DFSPH.cpp:1265
-            const float xx = pa.x - pb.x, xy = pa.y - pb.y, xz = pa.z - pb.z;
-            const float len2 = xx * xx + xy * xy + xz * xz;
-            if (len2 == 0.f) { ++zero; continue; }
-            const float pro = (va.x - vb.x) * xx + (va.y - vb.y) * xy + (va.z - vb.z) * xz;
-            if (pro < 0.f) {
-                const float f = grad_over_r(c.k, len2);
-                const float t = f * pro / (len2 + den0) * m * visc;
-                ax += xx * t;
-                ay += xy * t;
-                az += xz * t;
+        int4 nxt = ng ? ell_group(s.nbr, stride, p, 0) : make_int4(0, 0, 0, 0);
+        for (int gi = 0; gi < ng; ++gi) {
+            const int4 cur = nxt;
+            if (gi + 1 < ng) nxt = ell_group(s.nbr, stride, p, gi + 1);
+            const unsigned e[4] = {(unsigned)cur.x, (unsigned)cur.y, (unsigned)cur.z, (unsigned)cur.w};
+            // one 32-byte record per neighbour: {(x, y, z, rho), v} or, for a
+            // boundary particle, {(x, y, z, volume), singleVelocity + velocity}
+            // (DFSPH.cpp:1349); entries past the count read the particle's own
+            // record and are masked out
+            float4 pb[4], vb[4];
+            bool ok[4], bnd[4];
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                ok[t] = gi * 4 + t < cnt;
+                const unsigned u = ok[t] ? e[t] : (unsigned)p;
+                bnd[t] = (u & BND_FLAG) != 0u;
+                ld_record32((bnd[t] ? s.bpf : s.prv) + 2 * (size_t)(u & BND_MASK), pb[t], vb[t]);
+            }
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                const float m = bnd[t] ? bm * pb[t].w              // DFSPH.cpp:1353
+                                       : fm0 * __frcp_rn(pb[t].w);  // fm0/fb.density, DFSPH.cpp:1265
+                const float xx = pa.x - pb[t].x, xy = pa.y - pb[t].y, xz = pa.z - pb[t].z;
+                const float len2 = xx * xx + xy * xy + xz * xz;
+                const bool z0 = len2 == 0.f;  // zero distance: counted, no force (m_EC.zeroDis)
+                zero += ok[t] && z0;
+                const float pro = (va.x - vb[t].x) * xx + (va.y - vb[t].y) * xy + (va.z - vb[t].z) * xz;
+                if (ok[t] && !z0 && pro < 0.f) {
+                    const float f = grad_over_r(c.k, len2);
+                    const float tt = f * pro * __frcp_rn(len2 + den0) * m * visc;
+                    ax = fmaf(xx, tt, ax);
+                    ay = fmaf(xy, tt, ay);
+                    az = fmaf(xz, tt, az);
+                }
             }
         }
         s.acc[p] = make_float4(ax, ay, az, 0.f);

@@ -34,14 +34,20 @@ __device__ __forceinline__ float tanh_hw(float x) {
     asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
     return y;
 }
+// u = sqrt(2/pi) (z + 0.044715 z^3) = z (k0 + k1 z^2), k0 = sqrt(2/pi),
+// k1 = 0.044715 sqrt(2/pi); GELU = h + h tanh(u) with h = z / 2 (five FP32
+// operations and one tanh per activation: the inference kernel is bound by
+// this elementwise work, not by its GEMMs)
 __device__ __forceinline__ float gelu(float z) {
-    const float u = 0.7978845608028654f * fmaf(0.044715f * z, z * z, z);
-    return 0.5f * z * (1.f + tanh_hw(u));
+    const float u = z * fmaf(0.0356774081f, z * z, 0.7978845608f);
+    const float hz = 0.5f * z;
+    return fmaf(hz, tanh_hw(u), hz);
 }
+// d/dz: (1 + t) / 2 + (z / 2) (1 - t^2) (k0 + 3 k1 z^2)
 __device__ __forceinline__ float gelu_d(float z) {
     const float z2 = z * z;
-    const float t = tanh_hw(0.7978845608028654f * fmaf(0.044715f * z, z2, z));
-    return 0.5f * (1.f + t) + 0.5f * z * (1.f - t * t) * 0.7978845608028654f * fmaf(0.134145f, z2, 1.f);
+    const float t = tanh_hw(z * fmaf(0.0356774081f, z2, 0.7978845608f));
+    return fmaf(0.5f, t, 0.5f) + 0.5f * z * fmaf(-t, t, 1.f) * fmaf(0.1070322243f, z2, 0.7978845608f);
 }
 
 __device__ __forceinline__ uint32_t pack2(__nv_bfloat16 lo, __nv_bfloat16 hi) {
@@ -368,21 +374,37 @@ __device__ __forceinline__ void ws_features(const DevScene& s, const SolverConst
     const size_t stride = (size_t)c.stride;
     float acc = 0.f, ax = 0.f, ay = 0.f, az = 0.f, kp = 0.f;
     int nb = 0, nfl = 0;
-    for (int k = 0; k < cnt; ++k) {
-        const unsigned e = (unsigned)ell_get(s.nbr, stride, p, k);
-        const bool bnd = (e & BND_FLAG) != 0u;
-        const unsigned j = e & BND_MASK;
-        float4 pb, vb;
-        ld_record32((bnd ? s.bpv : s.pv) + 2 * (size_t)j, pb, vb);
-        const float m = bnd ? c.rho0 * pb.w : c.fm0;
-        const float xx = pa.x - pb.x, xy = pa.y - pb.y, xz = pa.z - pb.z;
-        const float f = grad_over_r(c.k, xx * xx + xy * xy + xz * xz);
-        acc = fmaf((xx * (va.x - vb.x) + xy * (va.y - vb.y) + xz * (va.z - vb.z)) * f, m, acc);
-        ax = fmaf(xx * f, m, ax);
-        ay = fmaf(xy * f, m, ay);
-        az = fmaf(xz * f, m, az);
-        if (bnd) ++nb;
-        else { kp += vb.w; ++nfl; }  // the neighbour's history, carried in its record (k_df_forces)
+    // four list entries per 16-byte load (the next group's issued before the
+    // current group's record gathers); entries past the count read the
+    // particle's own record and are masked out
+    const int ng = (cnt + 3) >> 2;
+    int4 nxt = ng ? ell_group(s.nbr, stride, p, 0) : make_int4(0, 0, 0, 0);
+    for (int gi = 0; gi < ng; ++gi) {
+        const int4 cur = nxt;
+        if (gi + 1 < ng) nxt = ell_group(s.nbr, stride, p, gi + 1);
+        const unsigned e4[4] = {(unsigned)cur.x, (unsigned)cur.y, (unsigned)cur.z, (unsigned)cur.w};
+        float4 pb[4], vb[4];
+        bool ok[4], bnd[4];
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            ok[t] = gi * 4 + t < cnt;
+            const unsigned u = ok[t] ? e4[t] : (unsigned)p;
+            bnd[t] = (u & BND_FLAG) != 0u;
+            ld_record32((bnd[t] ? s.bpv : s.pv) + 2 * (size_t)(u & BND_MASK), pb[t], vb[t]);
+        }
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            if (!ok[t]) continue;
+            const float m = bnd[t] ? c.rho0 * pb[t].w : c.fm0;
+            const float xx = pa.x - pb[t].x, xy = pa.y - pb[t].y, xz = pa.z - pb[t].z;
+            const float f = grad_over_r(c.k, xx * xx + xy * xy + xz * xz);
+            acc = fmaf((xx * (va.x - vb[t].x) + xy * (va.y - vb[t].y) + xz * (va.z - vb[t].z)) * f, m, acc);
+            ax = fmaf(xx * f, m, ax);
+            ay = fmaf(xy * f, m, ay);
+            az = fmaf(xz * f, m, az);
+            if (bnd[t]) ++nb;
+            else { kp += vb[t].w; ++nfl; }  // the neighbour's history, carried in its record (k_df_forces)
+        }
     }
     const float rho0 = c.rho0, rho = s.rho[p], d = c.dpart;
     const float4 hp = s.hist[p];

@@ -9,8 +9,8 @@ compiled reference by tests/test_oracle.py) on the same seeded inputs.
   Reference: SphBase.cpp:849-1089 (grid, neighbour search), DFSPH.cpp:84-193
   (rho, alpha), DFSPH.cpp:195-738 (the step).
 * 500,094-particle two-phase Rayleigh-Taylor column (rest densities 1000 /
-  3000): one PCISPH step (PciSph.cpp:98-129) and one IISPH_M step
-  (IISph_M.cpp:78-360) from the seeded lattice.
+  3000): one PCISPH step (PciSph.cpp:98-129) from the settled column and one
+  IISPH_M step (IISph_M.cpp:78-360) from the seeded lattice.
 * 27,000-particle WCSPH dam break, 1,000 steps of 2.5e-4 s
   (WcSph.cpp:23-153): trajectories part chaotically, so the runs are compared
   by mean density error and kinetic energy along the way.
@@ -97,24 +97,66 @@ def test_1m_settled_cells_neighbour_sets_rho_alpha(settled_1m):
     _check_ns(settled_1m, **DF_KW)
 
 
+def _sorted_keys(t, i, c):
+    live = np.arange(t.shape[1])[None, :] < c[:, None]
+    key = (t.astype(np.int64) << 32) | (i.astype(np.int64) & 0xffffffff)
+    key[~live] = np.iinfo(np.int64).max
+    key.sort(axis=1)
+    return key
+
+
 def test_1m_settled_dfsph_step(settled_1m):
     """One whole DFSPH step (CFL dt, density loop to 0.01 %, integration,
-    neighbour search, rho/alpha, divergence loop) from the settled state.
-    When the FP64 error sums of the two paths land on different sides of
-    the goal the iteration counts differ by one and the fields are held to
-    the size of one Jacobi correction instead."""
+    neighbour search, rho/alpha, divergence loop) from the settled state,
+    against the float oracle and its FP64 build.
+
+    The step's velocities come out of ~15-35 Jacobi iterations whose
+    stiffness is (rho_adv - rho0)/dt^2 alpha, which cancels in FP32: the GPU
+    must be as close to the float oracle as the float oracle is to its FP64
+    build (within a factor 2), or within 1e-4 of the largest speed.  The
+    densities at the end are summed over the neighbour lists of the new
+    positions; a position that moves by an ulp can take a pair across the
+    cut (and, where the 48-entry cap is full, change which neighbours are
+    kept), so densities are compared on the particles whose neighbour set
+    is the same in both paths -- those differ at most 1e-4 of all, and every
+    density outside the tolerance belongs to one of them."""
+    from oracle import make_scene_oracle
     _, g, o = make_pair(settled_1m, **DF_KW)
     st = g.step("dfsph", 1)
     o.stage("df_step")
+    p = dict(COMMON)
+    p.update(DF_KW)
+    od = make_scene_oracle(settled_1m, f64=True, **p)
+    od.stage("df_step")
     it, err, dt, _ = o.stats()
     assert abs(st["dt"] - dt) <= 1e-6 * dt
     assert abs(st["iter_density"] - it[0]) <= 1, (st["iter_density"], it[0])
     assert abs(st["iter_divergence"] - it[1]) <= 1, (st["iter_divergence"], it[1])
-    tol = RTOL if (st["iter_density"] == it[0] and st["iter_divergence"] == it[1]) else 1e-4
-    assert elem_rel(g.get("density"), o.get("density")) < tol
-    assert rel_err(g.get("velocity"), o.get("velocity")) < tol * 10
-    assert rel_err(g.get("position"), o.get("position"), scale=1.0) < 1e-6
     assert st["err_density"] <= 1e-4 and err[0] <= 1e-4
+    vg, vo, vd = g.get("velocity").astype(np.float64), o.get("velocity"), od.get("velocity")
+    vs = np.abs(vo).max()
+    d_gpu, d_f64 = np.abs(vg - vo).max() / vs, np.abs(vo - vd).max() / vs
+    assert d_gpu <= max(1e-4, 2 * d_f64), (d_gpu, d_f64)
+    # positions move by v dt: the same bound in metres
+    xg, xo, xd = g.get("position").astype(np.float64), o.get("position"), od.get("position")
+    x_gpu, x_f64 = np.abs(xg - xo).max(), np.abs(xo - xd).max()
+    assert x_gpu <= max(1e-6, 2 * x_f64), (x_gpu, x_f64)
+    gc, gt, gi = g.neighbours()
+    oc, ot, oi, _ = o.neighbours()
+    differ = np.any(_sorted_keys(gt, gi, gc) != _sorted_keys(ot, oi, oc), axis=1)
+    dc, dt_, di, _ = od.neighbours()
+    differ64 = np.any(_sorted_keys(ot, oi, oc) != _sorted_keys(dt_, di, dc), axis=1)
+    rg, ro, rd = g.get("density").astype(np.float64), o.get("density"), od.get("density")
+    e = np.abs(rg - ro) / ro
+    e64 = np.abs(ro - rd) / ro
+    tol = max(RTOL, 2 * e64[~differ & ~differ64].max())
+    print("1M step: iterations gpu %s oracle %s; velocity gpu-f32 %.3g f32-f64 %.3g; %d of %d particles with "
+          "a different neighbour set; density gpu-f32 %.3g (same sets) %.3g (all), f32-f64 %.3g"
+          % ((st["iter_density"], st["iter_divergence"]), tuple(it[:2]), d_gpu, d_f64, differ.sum(), len(e),
+             e[~differ].max(), e.max(), e64[~differ].max()))
+    assert differ.sum() <= 1e-4 * len(e)
+    assert e[~differ].max() <= tol
+    assert np.all(differ[e > tol])
 
 
 # ---- config 3: the two-phase column at 500k ----
@@ -147,11 +189,38 @@ def _close_as_float(g, o, od, field):
     assert d_gpu <= max(RTOL, 2 * d_f64), (field, d_gpu, d_f64)
 
 
-def test_500k_column_pcisph_step():
-    """PCISPH on the 500k column (0.5 % tolerance): one step with the
-    iteration count pinned to 5, so the comparison does not hinge on where
-    the max-error test falls."""
+@pytest.fixture(scope="module")
+def settled_column():
+    """The 500k column settled under gravity as one fluid (300 GPU DFSPH
+    steps of 1e-3 s), then the particles above the perturbed interface made
+    the heavy phase -- the way the reference's settled-column fixture is
+    made.  From the lattice at rest PCISPH does not hold the 126-layer
+    column (it reaches its iteration cap and blows the column apart, in the
+    CPU restatement as on the GPU), which makes a comparison of single
+    steps there ill-conditioned."""
     sc = config_multiphase_500k()
+    one = dataclasses.replace(sc, phase=None, rho0_phases=(sc.rho0,))
+    _, g, o = make_pair(one, **dict(DF_KW, cfl=0, dt=1e-3), visc_alpha=MULTI_VISC["visc_alpha"],
+                        boundary_visc=MULTI_VISC["boundary_visc"])
+    o.close()
+    g.step("dfsph", 300)
+    pos, vel = g.get("position"), g.get("velocity")
+    g.close()
+    assert len(pos) == sc.n_fluid and np.isfinite(pos).all()
+    x, y, z = (pos[:, k].astype(np.float64) for k in range(3))
+    iface = sc.meta["box"][1] / 2 + 0.02 * np.sin(2 * np.pi * x) * np.sin(2 * np.pi * z)
+    return dataclasses.replace(sc, fluid_pos=np.ascontiguousarray(pos), fluid_vel=np.ascontiguousarray(vel),
+                               phase=(y > iface).astype(np.int32))
+
+
+def test_500k_column_pcisph_step(settled_column):
+    """PCISPH on the settled 500k column (0.5 % tolerance): one step with
+    the iteration count pinned to 5, so the comparison does not hinge on
+    where the max-error test falls.  After the first iteration the density
+    is that of predicted positions moved by the pressure accelerations, so
+    it is held, like the pressures, to the float oracle's own distance from
+    its FP64 build."""
+    sc = settled_column
     kw = dict(II_KW, densityErro_eta=5e-3, pci_min_iter=5, pci_max_iter=5)
     _, g, o = make_pair(sc, **MULTI_VISC, **kw)
     od = _f64(sc, **kw)
@@ -159,11 +228,7 @@ def test_500k_column_pcisph_step():
     o.stage("pci_step")
     od.stage("pci_step")
     assert st["iter_density"] == 5 == o.stats()[0][2]
-    rho = _o(o, "density")
-    assert elem_rel(g.get("density"), rho) < RTOL
-    dp = np.abs(g.get("presure") - _o(o, "presure")).max()
-    assert dp <= 5 * o.pci_delta() * RTOL * rho.max()
-    for f in ("presure", "acceleration", "velocity"):
+    for f in ("density", "presure", "acceleration", "velocity"):
         _close_as_float(g, o, od, f)
     assert rel_err(g.get("position"), _o(o, "position"), scale=1.0) < 1e-6
 
