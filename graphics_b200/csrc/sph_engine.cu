@@ -20,6 +20,7 @@
 #include "../../include/sphgpu.h"
 #include "sph_kernels.cuh"
 #include "sph_mlp.cuh"
+#include "sph_sync.cuh"
 
 // warm-start kernels (sph_mlp.cu)
 void mlp_init_attributes();
@@ -680,10 +681,10 @@ int ensure_iv_boundary(sphgpu_scene* h) {
     int r = dalloc(h, &d.bsid, nb) | dalloc(h, &d.bncount, nb) | dalloc(h, &d.bivs, nb) | dalloc(h, &d.bivo, nb) |
             dalloc(h, &d.bnbr, (size_t)d.bstride * ((h->ncap + 3) / 4) * 4);
     if (r) return SPHGPU_ENOMEM;
-    CK(cudaMemcpy(d.bsid, h->bsolid_h.data(), sizeof(int) * nb, cudaMemcpyHostToDevice));
-    CK(cudaMemset(d.bivs, 0, sizeof(float4) * nb));
-    CK(cudaMemset(d.bivo, 0, sizeof(float4) * nb));
-    CK(cudaMemset(d.bncount, 0, sizeof(int) * nb));
+    CK(copy_sync(d.bsid, h->bsolid_h.data(), sizeof(int) * nb, cudaMemcpyHostToDevice));
+    CK(memset_sync(d.bivs, 0, sizeof(float4) * nb));
+    CK(memset_sync(d.bivo, 0, sizeof(float4) * nb));
+    CK(memset_sync(d.bncount, 0, sizeof(int) * nb));
     invalidate_graphs(h);
     return 0;
 }
@@ -978,7 +979,7 @@ int download_gid(sphgpu_scene* h, std::vector<int>& gid, int& n, bool staging) {
     CK(cudaStreamSynchronize(h->stream));
     n = h->h_stats->n_active;
     gid.resize(n);
-    if (n) CK(cudaMemcpy(gid.data(), staging ? h->d.gid_s : h->d.gid, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    if (n) CK(copy_sync(gid.data(), staging ? h->d.gid_s : h->d.gid, sizeof(int) * n, cudaMemcpyDeviceToHost));
     return 0;
 }
 
@@ -998,8 +999,8 @@ namespace {
 int sync_boundary_order(sphgpu_scene* h) {
     if (!h->R.nd || !h->nb) return 0;
     CK(cudaStreamSynchronize(h->stream));
-    CK(cudaMemcpy(h->bgid_h.data(), h->d.bgid, sizeof(int) * h->nb, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(h->bsolid_h.data(), h->d.bsid, sizeof(int) * h->nb, cudaMemcpyDeviceToHost));
+    CK(copy_sync(h->bgid_h.data(), h->d.bgid, sizeof(int) * h->nb, cudaMemcpyDeviceToHost));
+    CK(copy_sync(h->bsolid_h.data(), h->d.bsid, sizeof(int) * h->nb, cudaMemcpyDeviceToHost));
     return 0;
 }
 
@@ -1012,6 +1013,7 @@ int dyn_index(sphgpu_scene* h, int solid_id) {
 // device arrays for the dynamic-solid path, on first use: the boundary in
 // reference order (world positions, static volumes), sort scratch, records
 int rigid_init(sphgpu_scene* h) {
+    CK(cudaStreamSynchronize(h->stream));
     if (h->R.x0) return 0;
     DevScene& d = h->d;
     RigidDev& R = h->R;
@@ -1030,19 +1032,19 @@ int rigid_init(sphgpu_scene* h) {
     std::vector<float4> bp(nb), x0(nb);
     std::vector<float> vol(nb);
     std::vector<int> dyn(nb, -1), sid(nb);
-    CK(cudaMemcpy(bp.data(), d.bpos, sizeof(float4) * nb, cudaMemcpyDeviceToHost));
+    CK(copy_sync(bp.data(), d.bpos, sizeof(float4) * nb, cudaMemcpyDeviceToHost));
     for (int q = 0; q < nb; ++q) {
         const int k = h->bgid_h[q];
         x0[k] = make_float4(bp[q].x, bp[q].y, bp[q].z, 0.f);
         vol[k] = bp[q].w;
         sid[k] = h->bsolid_h[q];
     }
-    CK(cudaMemcpy(R.x0, x0.data(), sizeof(float4) * nb, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(R.vol, vol.data(), sizeof(float) * nb, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(R.dyn, dyn.data(), sizeof(int) * nb, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(R.sid, sid.data(), sizeof(int) * nb, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(d.bsid, h->bsolid_h.data(), sizeof(int) * nb, cudaMemcpyHostToDevice));
-    CK(cudaMemset(d.bforce, 0, sizeof(float4) * nb));
+    CK(copy_sync(R.x0, x0.data(), sizeof(float4) * nb, cudaMemcpyHostToDevice));
+    CK(copy_sync(R.vol, vol.data(), sizeof(float) * nb, cudaMemcpyHostToDevice));
+    CK(copy_sync(R.dyn, dyn.data(), sizeof(int) * nb, cudaMemcpyHostToDevice));
+    CK(copy_sync(R.sid, sid.data(), sizeof(int) * nb, cudaMemcpyHostToDevice));
+    CK(copy_sync(d.bsid, h->bsolid_h.data(), sizeof(int) * nb, cudaMemcpyHostToDevice));
+    CK(memset_sync(d.bforce, 0, sizeof(float4) * nb));
     return 0;
 }
 
@@ -1063,8 +1065,8 @@ int rigid_reserve(sphgpu_scene* h, int n) {
         return SPHGPU_ENOMEM;
     memset(hst, 0, sizeof(float) * 25 * cap);
     memset(hout, 0, sizeof(double) * (6 * cap + 1));
-    CK(cudaMemset(tk, 0, sizeof(unsigned) * cap));
-    CK(cudaMemset(out, 0, sizeof(double) * 6 * cap));
+    CK(memset_sync(tk, 0, sizeof(unsigned) * cap));
+    CK(memset_sync(out, 0, sizeof(double) * 6 * cap));
     if (h->h_rstate) memcpy(hst, h->h_rstate, sizeof(float) * 25 * h->rigid_cap);
     if (h->h_rout) memcpy(hout, h->h_rout, sizeof(double) * 6 * h->rigid_cap);
     if (R.state) cudaFree(R.state);
@@ -1195,8 +1197,8 @@ static int create_impl(const SphParams* p, int device, int max_fluid, int nscene
             cudaMalloc(&h->d_batch, bytes) != cudaSuccess) {
             r = SPHGPU_ENOMEM;
         } else {
-            cudaMemcpy(h->d_geom, h->sgeom.data(), S * sizeof(GridGeom), cudaMemcpyHostToDevice);
-            cudaMemset(h->d_batch, 0, bytes);
+            copy_sync(h->d_geom, h->sgeom.data(), S * sizeof(GridGeom), cudaMemcpyHostToDevice);
+            memset_sync(h->d_batch, 0, bytes);
             char* q = (char*)h->d_batch;
             BatchDev& b = h->d.b;
             b.err_density = (double*)q; q += S * sizeof(double);
@@ -1212,7 +1214,7 @@ static int create_impl(const SphParams* p, int device, int max_fluid, int nscene
             b.status = (unsigned*)q;
             b.geom = h->d_geom;
             std::vector<float> dts(S, p->dt);
-            cudaMemcpy(b.dt, dts.data(), S * sizeof(float), cudaMemcpyHostToDevice);
+            copy_sync(b.dt, dts.data(), S * sizeof(float), cudaMemcpyHostToDevice);
         }
     }
     h->d.nscenes = nscenes;
@@ -1259,7 +1261,7 @@ int sphgpu_set_params(sphgpu_t h, const SphParams* p) {
     CK(cudaMemcpyAsync(h->d.dt, &dt, sizeof(float), cudaMemcpyHostToDevice, h->stream));
     if (h->nscenes > 1) {
         std::vector<float> dts(h->nscenes, dt);
-        CK(cudaMemcpy(h->d.b.dt, dts.data(), sizeof(float) * h->nscenes, cudaMemcpyHostToDevice));
+        CK(copy_sync(h->d.b.dt, dts.data(), sizeof(float) * h->nscenes, cudaMemcpyHostToDevice));
     }
     CK(cudaStreamSynchronize(h->stream));
     return 0;
@@ -1296,7 +1298,7 @@ static int set_boundary_impl(sphgpu_t h, int n, const float* xyz, const int* sol
         for (int i = 0; i < n; ++i) tmp[i] = bp[ord[i]];
         int* dkeys = nullptr;
         if (dalloc(h, &dkeys, n)) return SPHGPU_ENOMEM;
-        CK(cudaMemcpy(d.bpos, tmp.data(), sizeof(float4) * n, cudaMemcpyHostToDevice));
+        CK(copy_sync(d.bpos, tmp.data(), sizeof(float4) * n, cudaMemcpyHostToDevice));
         for (int a = 0; a < n;) {
             int b = a;
             const int sc = scene ? scene[ord[a]] : 0;
@@ -1307,7 +1309,7 @@ static int set_boundary_impl(sphgpu_t h, int n, const float* xyz, const int* sol
         }
         CK(cudaStreamSynchronize(h->stream));
         std::vector<int> k2(n);
-        CK(cudaMemcpy(k2.data(), dkeys, sizeof(int) * n, cudaMemcpyDeviceToHost));
+        CK(copy_sync(k2.data(), dkeys, sizeof(int) * n, cudaMemcpyDeviceToHost));
         cudaFree(dkeys);
         for (int i = 0; i < n; ++i) keys[ord[i]] = k2[i];
     }
@@ -1349,10 +1351,10 @@ static int set_boundary_impl(sphgpu_t h, int n, const float* xyz, const int* sol
     for (int i = 1; i < n; ++i)
         if (h->bsolid_h[i] != h->bsolid_h[0]) h->iv_multi_solid = 1;
     fill_solver_const(h);
-    CK(cudaMemcpy(d.bpos, sp.data(), sizeof(float4) * n, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(d.bvel, sv.data(), sizeof(float4) * n, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(d.bgid, h->bgid_h.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(d.bcell_start, start.data(), sizeof(int) * (h->g.nkeys + 1), cudaMemcpyHostToDevice));
+    CK(copy_sync(d.bpos, sp.data(), sizeof(float4) * n, cudaMemcpyHostToDevice));
+    CK(copy_sync(d.bvel, sv.data(), sizeof(float4) * n, cudaMemcpyHostToDevice));
+    CK(copy_sync(d.bgid, h->bgid_h.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    CK(copy_sync(d.bcell_start, start.data(), sizeof(int) * (h->g.nkeys + 1), cudaMemcpyHostToDevice));
     if (!volume) {
         // each scene's walls with its own grid: its sorted range is contiguous
         for (int sc = 0; sc < h->nscenes; ++sc) {
@@ -1364,8 +1366,8 @@ static int set_boundary_impl(sphgpu_t h, int n, const float* xyz, const int* sol
     }
     // packed {(x, y, z, volume), velocity} records for the sweeps
     if (n) {
-        CK(cudaMemcpy2D(d.bpv, 2 * sizeof(float4), d.bpos, sizeof(float4), sizeof(float4), n, cudaMemcpyDeviceToDevice));
-        CK(cudaMemcpy2D(d.bpv + 1, 2 * sizeof(float4), d.bvel, sizeof(float4), sizeof(float4), n,
+        CK(copy2d_sync(d.bpv, 2 * sizeof(float4), d.bpos, sizeof(float4), sizeof(float4), n, cudaMemcpyDeviceToDevice));
+        CK(copy2d_sync(d.bpv + 1, 2 * sizeof(float4), d.bvel, sizeof(float4), sizeof(float4), n,
                         cudaMemcpyDeviceToDevice));
     }
     invalidate_graphs(h);
@@ -1415,8 +1417,8 @@ static int add_fluid_impl(sphgpu_t h, int n, const float* xyz, const float* vel,
         int m;
         if (download_gid(h, gid, m, h->in_staging)) return SPHGPU_ECUDA;
         std::vector<float4> tp(m), tv(m);
-        CK(cudaMemcpy(tp.data(), h->in_staging ? h->d.pos_s : h->d.pos, sizeof(float4) * m, cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(tv.data(), h->in_staging ? h->d.vel_s : h->d.vel, sizeof(float4) * m, cudaMemcpyDeviceToHost));
+        CK(copy_sync(tp.data(), h->in_staging ? h->d.pos_s : h->d.pos, sizeof(float4) * m, cudaMemcpyDeviceToHost));
+        CK(copy_sync(tv.data(), h->in_staging ? h->d.vel_s : h->d.vel, sizeof(float4) * m, cudaMemcpyDeviceToHost));
         std::vector<int> order;
         ref_order(gid, order);
         for (int k = 0; k < m; ++k) { P[k] = tp[order[k]]; V[k] = tv[order[k]]; }
@@ -1425,7 +1427,7 @@ static int add_fluid_impl(sphgpu_t h, int n, const float* xyz, const float* vel,
                                  h->in_staging ? h->d.cC_s : h->d.cC};
         for (int a = 0; a < 3; ++a) {
             std::vector<float4> t(m);
-            CK(cudaMemcpy(t.data(), srcs[a], sizeof(float4) * m, cudaMemcpyDeviceToHost));
+            CK(copy_sync(t.data(), srcs[a], sizeof(float4) * m, cudaMemcpyDeviceToHost));
             for (int k = 0; k < m; ++k) carried[a][k] = t[order[k]];
         }
     }
@@ -1440,14 +1442,14 @@ static int add_fluid_impl(sphgpu_t h, int n, const float* xyz, const float* vel,
     }
     std::vector<int> G(cur + n);
     std::iota(G.begin(), G.end(), 0);
-    CK(cudaMemcpy(h->d.pos_s, P.data(), sizeof(float4) * (cur + n), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(h->d.vel_s, V.data(), sizeof(float4) * (cur + n), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(h->d.gid_s, G.data(), sizeof(int) * (cur + n), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(h->d.cA_s, carried[0].data(), sizeof(float4) * (cur + n), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(h->d.cB_s, carried[1].data(), sizeof(float4) * (cur + n), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(h->d.cC_s, carried[2].data(), sizeof(float4) * (cur + n), cudaMemcpyHostToDevice));
+    CK(copy_sync(h->d.pos_s, P.data(), sizeof(float4) * (cur + n), cudaMemcpyHostToDevice));
+    CK(copy_sync(h->d.vel_s, V.data(), sizeof(float4) * (cur + n), cudaMemcpyHostToDevice));
+    CK(copy_sync(h->d.gid_s, G.data(), sizeof(int) * (cur + n), cudaMemcpyHostToDevice));
+    CK(copy_sync(h->d.cA_s, carried[0].data(), sizeof(float4) * (cur + n), cudaMemcpyHostToDevice));
+    CK(copy_sync(h->d.cB_s, carried[1].data(), sizeof(float4) * (cur + n), cudaMemcpyHostToDevice));
+    CK(copy_sync(h->d.cC_s, carried[2].data(), sizeof(float4) * (cur + n), cudaMemcpyHostToDevice));
     h->h_stats->n_active = cur + n;
-    CK(cudaMemcpy(&h->d.st->n_active, &h->h_stats->n_active, sizeof(int), cudaMemcpyHostToDevice));
+    CK(copy_sync(&h->d.st->n_active, &h->h_stats->n_active, sizeof(int), cudaMemcpyHostToDevice));
     if (!scene || h->rho0_ph.empty()) {
         h->rho0_ph.push_back(rho0);
         h->alpha_ph.push_back(visc_alpha);
@@ -1548,7 +1550,7 @@ int sphgpu_get_fluid(sphgpu_t h, const char* field, float* out) {
         std::vector<int> order;
         ref_order(gid, order);
         std::vector<float4> t(n);
-        CK(cudaMemcpy(t.data(), h->in_staging ? h->d.pos_s : h->d.pos, sizeof(float4) * n, cudaMemcpyDeviceToHost));
+        CK(copy_sync(t.data(), h->in_staging ? h->d.pos_s : h->d.pos, sizeof(float4) * n, cudaMemcpyDeviceToHost));
         for (int k = 0; k < n; ++k) {
             int w;
             memcpy(&w, &t[order[k]].w, sizeof w);
@@ -1568,7 +1570,7 @@ int sphgpu_get_fluid(sphgpu_t h, const char* field, float* out) {
     if (f == "position") { src = staging ? d.pos_s : d.pos; f4 = true; comps = 3; }
     else if (f == "velocity") { src = staging ? d.vel_s : d.vel; f4 = true; comps = 3; }
     else if (f == "vel_adv") {
-        CK(cudaMemcpy2D(d.vadv, sizeof(float4), d.pv + 1, 2 * sizeof(float4), sizeof(float4), n,
+        CK(copy2d_sync(d.vadv, sizeof(float4), d.pv + 1, 2 * sizeof(float4), sizeof(float4), n,
                         cudaMemcpyDeviceToDevice));
         src = d.vadv;
         f4 = true;
@@ -1586,7 +1588,7 @@ int sphgpu_get_fluid(sphgpu_t h, const char* field, float* out) {
     else if (f == "dOmega" || f == "psi") { src = d.vB; f4 = true; comps = 3; }
     else if (f == "angular_velocity" || f == "n0Vorticity") { src = d.cA; f4 = true; comps = 3; }
     else if (f == "advectionVelocity") {
-        CK(cudaMemcpy2D(d.vadv, sizeof(float4), d.pv + 1, 2 * sizeof(float4), sizeof(float4), n,
+        CK(copy2d_sync(d.vadv, sizeof(float4), d.pv + 1, 2 * sizeof(float4), sizeof(float4), n,
                         cudaMemcpyDeviceToDevice));
         src = d.vadv;
         f4 = true;
@@ -1594,7 +1596,7 @@ int sphgpu_get_fluid(sphgpu_t h, const char* field, float* out) {
     }
     else if (f == "sphDensity" || f == "VF_gamma" || f == "VF_sphVolume" || f == "VF_alpha") {
         std::vector<float4> t(n);
-        CK(cudaMemcpy(t.data(), d.ivs, sizeof(float4) * n, cudaMemcpyDeviceToHost));
+        CK(copy_sync(t.data(), d.ivs, sizeof(float4) * n, cudaMemcpyDeviceToHost));
         for (int k = 0; k < n; ++k) {
             const float4& v = t[order[k]];
             out[k] = f == "VF_gamma" ? v.x : (f == "VF_sphVolume" ? v.y : (f == "VF_alpha" ? v.z : v.w));
@@ -1614,14 +1616,14 @@ int sphgpu_get_fluid(sphgpu_t h, const char* field, float* out) {
         // normalised BF16 network inputs of the last warm-start step (n*16)
         if (!h->xn) { h->err = "no learned warm start attached"; return SPHGPU_EINVAL; }
         std::vector<__nv_bfloat16> t((size_t)n * MLP_IN);
-        CK(cudaMemcpy(t.data(), h->xn, sizeof(__nv_bfloat16) * t.size(), cudaMemcpyDeviceToHost));
+        CK(copy_sync(t.data(), h->xn, sizeof(__nv_bfloat16) * t.size(), cudaMemcpyDeviceToHost));
         for (int k = 0; k < n; ++k)
             for (int i = 0; i < MLP_IN; ++i) out[(size_t)k * MLP_IN + i] = __bfloat162float(t[(size_t)order[k] * MLP_IN + i]);
         return n;
     }
     else if (f == "aii" || f == "p_l") {
         std::vector<float4> t(n);
-        CK(cudaMemcpy(t.data(), f == "aii" ? d.cC : d.cA, sizeof(float4) * n, cudaMemcpyDeviceToHost));
+        CK(copy_sync(t.data(), f == "aii" ? d.cC : d.cA, sizeof(float4) * n, cudaMemcpyDeviceToHost));
         for (int k = 0; k < n; ++k) out[k] = t[order[k]].w;
         return n;
     }
@@ -1633,7 +1635,7 @@ int sphgpu_get_fluid(sphgpu_t h, const char* field, float* out) {
     else if (f == "kappa_sum") src = d.ksum;
     else if (f == "kappa_warm") src = d.kwarm;
     else if (f == "ws_hist") {
-        CK(cudaMemcpy2D(d.vadv, sizeof(float4), d.hist, sizeof(float4), sizeof(float4), n, cudaMemcpyDeviceToDevice));
+        CK(copy2d_sync(d.vadv, sizeof(float4), d.hist, sizeof(float4), sizeof(float4), n, cudaMemcpyDeviceToDevice));
         src = d.vadv;
         f4 = true;
         comps = 3;
@@ -1643,7 +1645,7 @@ int sphgpu_get_fluid(sphgpu_t h, const char* field, float* out) {
     else if (f == "presure") src = d.kr;
     else if (f == "neighbour_count") {
         std::vector<int> cnt(n);
-        CK(cudaMemcpy(cnt.data(), d.ncount, sizeof(int) * n, cudaMemcpyDeviceToHost));
+        CK(copy_sync(cnt.data(), d.ncount, sizeof(int) * n, cudaMemcpyDeviceToHost));
         for (int k = 0; k < n; ++k) out[k] = (float)cnt[order[k]];
         return n;
     } else {
@@ -1652,14 +1654,14 @@ int sphgpu_get_fluid(sphgpu_t h, const char* field, float* out) {
     }
     if (f4) {
         std::vector<float4> t(n);
-        CK(cudaMemcpy(t.data(), src, sizeof(float4) * n, cudaMemcpyDeviceToHost));
+        CK(copy_sync(t.data(), src, sizeof(float4) * n, cudaMemcpyDeviceToHost));
         for (int k = 0; k < n; ++k) {
             const float4& v = t[order[k]];
             out[3 * k] = v.x; out[3 * k + 1] = v.y; out[3 * k + 2] = v.z;
         }
     } else {
         std::vector<float> t(n);
-        CK(cudaMemcpy(t.data(), src, sizeof(float) * n, cudaMemcpyDeviceToHost));
+        CK(copy_sync(t.data(), src, sizeof(float) * n, cudaMemcpyDeviceToHost));
         for (int k = 0; k < n; ++k) out[k] = t[order[k]];
     }
     (void)comps;
@@ -1700,14 +1702,14 @@ int sphgpu_set_fluid(sphgpu_t h, const char* field, const float* in) {
     if (f == "position" || f == "velocity") {
         float4* dst = f == "position" ? (staging ? d.pos_s : d.pos) : (staging ? d.vel_s : d.vel);
         std::vector<float4> t(n);
-        CK(cudaMemcpy(t.data(), dst, sizeof(float4) * n, cudaMemcpyDeviceToHost));
+        CK(copy_sync(t.data(), dst, sizeof(float4) * n, cudaMemcpyDeviceToHost));
         std::vector<int> order;
         ref_order(gid, order);
         for (int k = 0; k < n; ++k) {
             float4& v = t[order[k]];
             v.x = in[3 * k]; v.y = in[3 * k + 1]; v.z = in[3 * k + 2];
         }
-        CK(cudaMemcpy(dst, t.data(), sizeof(float4) * n, cudaMemcpyHostToDevice));
+        CK(copy_sync(dst, t.data(), sizeof(float4) * n, cudaMemcpyHostToDevice));
         if (!staging) {
             // positions changed: lists and rho/alpha must be rebuilt
             h->ns_valid = false;
@@ -1729,9 +1731,9 @@ int sphgpu_set_fluid(sphgpu_t h, const char* field, const float* in) {
         ref_order(g2, o2);
         float4* cb = stg ? d.cB_s : d.cB;
         std::vector<float4> t(n2);
-        CK(cudaMemcpy(t.data(), cb, sizeof(float4) * n2, cudaMemcpyDeviceToHost));
+        CK(copy_sync(t.data(), cb, sizeof(float4) * n2, cudaMemcpyDeviceToHost));
         for (int k = 0; k < n2; ++k) t[o2[k]].w = in[k];
-        CK(cudaMemcpy(cb, t.data(), sizeof(float4) * n2, cudaMemcpyHostToDevice));
+        CK(copy_sync(cb, t.data(), sizeof(float4) * n2, cudaMemcpyHostToDevice));
     }
     float* dst = nullptr;
     if (f == "density") dst = d.rho;
@@ -1743,9 +1745,9 @@ int sphgpu_set_fluid(sphgpu_t h, const char* field, const float* in) {
     ref_order(gid, order);
     std::vector<float> t(n);
     for (int k = 0; k < n; ++k) t[order[k]] = in[k];
-    CK(cudaMemcpy(dst, t.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
+    CK(copy_sync(dst, t.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
     if (dst == d.rho && n)  // the force kernel's record carries rho too
-        CK(cudaMemcpy2D(reinterpret_cast<char*>(d.prv) + 3 * sizeof(float), 2 * sizeof(float4), d.rho, sizeof(float),
+        CK(copy2d_sync(reinterpret_cast<char*>(d.prv) + 3 * sizeof(float), 2 * sizeof(float4), d.rho, sizeof(float),
                         sizeof(float), n, cudaMemcpyDeviceToDevice));
     return n;
 }
@@ -1756,20 +1758,20 @@ int sphgpu_get_boundary(sphgpu_t h, const char* field, float* out) {
     CK(cudaStreamSynchronize(h->stream));
     int n = h->nb;
     std::vector<float4> t(n);
-    CK(cudaMemcpy(t.data(), h->d.bpos, sizeof(float4) * n, cudaMemcpyDeviceToHost));
+    CK(copy_sync(t.data(), h->d.bpos, sizeof(float4) * n, cudaMemcpyDeviceToHost));
     std::string f(field);
     if (h->R.nd) {
         if (int r = sync_boundary_order(h)) return r;
         if (f == "velocity" || f == "force" || f == "kerSumFromSelf") {
             if (f == "velocity") {
                 std::vector<float4> rec(2 * (size_t)n);
-                CK(cudaMemcpy(rec.data(), h->d.bpf, sizeof(float4) * 2 * n, cudaMemcpyDeviceToHost));
+                CK(copy_sync(rec.data(), h->d.bpf, sizeof(float4) * 2 * n, cudaMemcpyDeviceToHost));
                 for (int i = 0; i < n; ++i) t[i] = rec[2 * (size_t)i + 1];
             } else if (f == "force") {
-                CK(cudaMemcpy(t.data(), h->d.bforce, sizeof(float4) * n, cudaMemcpyDeviceToHost));
+                CK(copy_sync(t.data(), h->d.bforce, sizeof(float4) * n, cudaMemcpyDeviceToHost));
             } else {
                 std::vector<float> ks(n);
-                CK(cudaMemcpy(ks.data(), h->d.bks, sizeof(float) * n, cudaMemcpyDeviceToHost));
+                CK(copy_sync(ks.data(), h->d.bks, sizeof(float) * n, cudaMemcpyDeviceToHost));
                 for (int i = 0; i < n; ++i) out[h->bgid_h[i]] = ks[i];
                 return n;
             }
@@ -1791,7 +1793,7 @@ int sphgpu_get_boundary(sphgpu_t h, const char* field, float* out) {
             if (names[i] && f == names[i]) which = i;
         if (which < 0) { h->err = "unknown boundary field"; return SPHGPU_EINVAL; }
         if (!h->d.bivs) { h->err = "no IISph boundary state (run an IISph step first)"; return SPHGPU_EINVAL; }
-        CK(cudaMemcpy(t.data(), which < 4 ? h->d.bivs : h->d.bivo, sizeof(float4) * n, cudaMemcpyDeviceToHost));
+        CK(copy_sync(t.data(), which < 4 ? h->d.bivs : h->d.bivo, sizeof(float4) * n, cudaMemcpyDeviceToHost));
         for (int i = 0; i < n; ++i) {
             const float4& v = t[i];
             const int c = which & 3;
@@ -1911,10 +1913,10 @@ int sphgpu_get_neighbours(sphgpu_t h, int* counts, int* t, int* idx) {
     int n;
     if (download_gid(h, gid, n, false)) return SPHGPU_ECUDA;
     std::vector<int> cnt(n), L((size_t)h->stride * ((h->ncap + 3) / 4) * 4);
-    CK(cudaMemcpy(cnt.data(), h->d.ncount, sizeof(int) * n, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(L.data(), h->d.nbr, sizeof(int) * L.size(), cudaMemcpyDeviceToHost));
+    CK(copy_sync(cnt.data(), h->d.ncount, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    CK(copy_sync(L.data(), h->d.nbr, sizeof(int) * L.size(), cudaMemcpyDeviceToHost));
     std::vector<float4> pos(n);
-    CK(cudaMemcpy(pos.data(), h->d.pos, sizeof(float4) * n, cudaMemcpyDeviceToHost));
+    CK(copy_sync(pos.data(), h->d.pos, sizeof(float4) * n, cudaMemcpyDeviceToHost));
     // phase starts in global fluid index space
     std::vector<int> pstart(h->phase_n.size() + 1, 0);
     for (size_t k = 0; k < h->phase_n.size(); ++k) pstart[k + 1] = pstart[k] + h->phase_n[k];
@@ -2053,12 +2055,12 @@ int sphgpu_mlp_create(int device, int dataset_cap, uint64_t seed, sphgpu_mlp_t* 
     std::vector<float> norm(2 * MLP_IN + 2, 0.f);
     for (int i = 0; i < MLP_IN; ++i) norm[MLP_IN + i] = 1.f;
     norm[2 * MLP_IN + 1] = 1.f;
-    cudaMemcpy(d.master, w.data(), sizeof(float) * MLP_NPARAM_PAD, cudaMemcpyHostToDevice);
-    cudaMemset(d.grad, 0, sizeof(float) * MLP_NPARAM_PAD);
-    cudaMemset(d.adam_m, 0, sizeof(float) * MLP_NPARAM_PAD);
-    cudaMemset(d.adam_v, 0, sizeof(float) * MLP_NPARAM_PAD);
-    cudaMemcpy(d.norm, norm.data(), sizeof(float) * norm.size(), cudaMemcpyHostToDevice);
-    cudaMemset(m->ds_count, 0, sizeof(int));
+    copy_sync(d.master, w.data(), sizeof(float) * MLP_NPARAM_PAD, cudaMemcpyHostToDevice);
+    memset_sync(d.grad, 0, sizeof(float) * MLP_NPARAM_PAD);
+    memset_sync(d.adam_m, 0, sizeof(float) * MLP_NPARAM_PAD);
+    memset_sync(d.adam_v, 0, sizeof(float) * MLP_NPARAM_PAD);
+    copy_sync(d.norm, norm.data(), sizeof(float) * norm.size(), cudaMemcpyHostToDevice);
+    memset_sync(m->ds_count, 0, sizeof(int));
     mlp_init_attributes();
     launch_mlp_sync_bf16(d, m->stream);
     if (cudaStreamSynchronize(m->stream) != cudaSuccess) {
@@ -2085,38 +2087,41 @@ int sphgpu_mlp_destroy(sphgpu_mlp_t m) {
 int sphgpu_mlp_set_params(sphgpu_mlp_t m, const float* params) {
     if (!m || !params) return SPHGPU_EINVAL;
     cudaSetDevice(m->device);
-    if (cudaMemcpy(m->m.master, params, sizeof(float) * MLP_NPARAM, cudaMemcpyHostToDevice) != cudaSuccess)
+    if (copy_sync(m->m.master, params, sizeof(float) * MLP_NPARAM, cudaMemcpyHostToDevice) != cudaSuccess)
         return SPHGPU_ECUDA;
     launch_mlp_sync_bf16(m->m, m->stream);
     return cudaStreamSynchronize(m->stream) == cudaSuccess ? 0 : SPHGPU_ECUDA;
 }
 
 int sphgpu_mlp_get_params(sphgpu_mlp_t m, float* params) {
+    if (m) cudaDeviceSynchronize();  // written on the network's and on scenes' streams
     if (!m || !params) return SPHGPU_EINVAL;
     cudaSetDevice(m->device);
-    return cudaMemcpy(params, m->m.master, sizeof(float) * MLP_NPARAM, cudaMemcpyDeviceToHost) == cudaSuccess
+    return copy_sync(params, m->m.master, sizeof(float) * MLP_NPARAM, cudaMemcpyDeviceToHost) == cudaSuccess
                ? MLP_NPARAM : SPHGPU_ECUDA;
 }
 
 int sphgpu_mlp_set_norm(sphgpu_mlp_t m, const float* norm) {
     if (!m || !norm) return SPHGPU_EINVAL;
     cudaSetDevice(m->device);
-    return cudaMemcpy(m->m.norm, norm, sizeof(float) * (2 * MLP_IN + 2), cudaMemcpyHostToDevice) == cudaSuccess
+    return copy_sync(m->m.norm, norm, sizeof(float) * (2 * MLP_IN + 2), cudaMemcpyHostToDevice) == cudaSuccess
                ? 0 : SPHGPU_ECUDA;
 }
 
 int sphgpu_mlp_get_norm(sphgpu_mlp_t m, float* norm) {
+    if (m) cudaDeviceSynchronize();  // written on the network's and on scenes' streams
     if (!m || !norm) return SPHGPU_EINVAL;
     cudaSetDevice(m->device);
-    return cudaMemcpy(norm, m->m.norm, sizeof(float) * (2 * MLP_IN + 2), cudaMemcpyDeviceToHost) == cudaSuccess
+    return copy_sync(norm, m->m.norm, sizeof(float) * (2 * MLP_IN + 2), cudaMemcpyDeviceToHost) == cudaSuccess
                ? 0 : SPHGPU_ECUDA;
 }
 
 int sphgpu_mlp_dataset_size(sphgpu_mlp_t m) {
+    if (m) cudaDeviceSynchronize();  // written on the network's and on scenes' streams
     if (!m) return SPHGPU_EINVAL;
     cudaSetDevice(m->device);
     int n = 0;
-    if (cudaMemcpy(&n, m->ds_count, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return SPHGPU_ECUDA;
+    if (copy_sync(&n, m->ds_count, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return SPHGPU_ECUDA;
     return std::min(n, m->ds_cap);
 }
 
@@ -2124,20 +2129,21 @@ int sphgpu_mlp_dataset_set(sphgpu_mlp_t m, const float* X, const float* y, int n
     if (!m || n < 0 || n > m->ds_cap || (n && (!X || !y))) return SPHGPU_EINVAL;
     cudaSetDevice(m->device);
     if (n) {
-        if (cudaMemcpy(m->dsX, X, sizeof(float) * MLP_IN * (size_t)n, cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(m->dsy, y, sizeof(float) * n, cudaMemcpyHostToDevice) != cudaSuccess)
+        if (copy_sync(m->dsX, X, sizeof(float) * MLP_IN * (size_t)n, cudaMemcpyHostToDevice) != cudaSuccess ||
+            copy_sync(m->dsy, y, sizeof(float) * n, cudaMemcpyHostToDevice) != cudaSuccess)
             return SPHGPU_ECUDA;
     }
-    return cudaMemcpy(m->ds_count, &n, sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess ? 0 : SPHGPU_ECUDA;
+    return copy_sync(m->ds_count, &n, sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess ? 0 : SPHGPU_ECUDA;
 }
 
 int sphgpu_mlp_dataset_get(sphgpu_mlp_t m, float* X, float* y, int max_n) {
+    if (m) cudaDeviceSynchronize();  // written on the network's and on scenes' streams
     if (!m || max_n < 0) return SPHGPU_EINVAL;
     int n = std::min(sphgpu_mlp_dataset_size(m), max_n);
     if (n < 0) return n;
-    if (n && X && cudaMemcpy(X, m->dsX, sizeof(float) * MLP_IN * (size_t)n, cudaMemcpyDeviceToHost) != cudaSuccess)
+    if (n && X && copy_sync(X, m->dsX, sizeof(float) * MLP_IN * (size_t)n, cudaMemcpyDeviceToHost) != cudaSuccess)
         return SPHGPU_ECUDA;
-    if (n && y && cudaMemcpy(y, m->dsy, sizeof(float) * n, cudaMemcpyDeviceToHost) != cudaSuccess) return SPHGPU_ECUDA;
+    if (n && y && copy_sync(y, m->dsy, sizeof(float) * n, cudaMemcpyDeviceToHost) != cudaSuccess) return SPHGPU_ECUDA;
     return n;
 }
 
@@ -2221,8 +2227,8 @@ int sphgpu_mlp_gradient(sphgpu_mlp_t m, const float* X, const float* y, int n, f
         cudaFree(dy);
         return r;
     }
-    cudaMemcpy(dX, X, sizeof(float) * MLP_IN * (size_t)n, cudaMemcpyHostToDevice);
-    cudaMemcpy(dy, y, sizeof(float) * n, cudaMemcpyHostToDevice);
+    copy_sync(dX, X, sizeof(float) * MLP_IN * (size_t)n, cudaMemcpyHostToDevice);
+    copy_sync(dy, y, sizeof(float) * n, cudaMemcpyHostToDevice);
     cudaMemsetAsync(m->m.grad, 0, sizeof(float) * MLP_NPARAM_PAD, m->stream);
     cudaMemsetAsync(m->m.loss, 0, sizeof(float), m->stream);
     launch_mlp_train_batch(m->m, dX, dy, n, 0, n, 1.f / (float)n, m->stream);
@@ -2247,7 +2253,7 @@ int sphgpu_mlp_predict(sphgpu_mlp_t m, const float* X, float* y, int n) {
         cudaFree(dX);
         return SPHGPU_ENOMEM;
     }
-    cudaMemcpy(dX, X, sizeof(float) * MLP_IN * (size_t)n, cudaMemcpyHostToDevice);
+    copy_sync(dX, X, sizeof(float) * MLP_IN * (size_t)n, cudaMemcpyHostToDevice);
     launch_mlp_predict(m->m, dX, dy, n, m->stream);
     cudaMemcpyAsync(y, dy, sizeof(float) * n, cudaMemcpyDeviceToHost, m->stream);
     cudaError_t e = cudaStreamSynchronize(m->stream);
@@ -2379,15 +2385,15 @@ int sphgpu_batch_stats(sphgpu_t h, SphStepStats* out, int cap) {
     std::vector<float> dt(S);
     std::vector<int> itd(S), itv(S), ttd(S), ttv(S), nn(S);
     std::vector<unsigned> stt(S);
-    CK(cudaMemcpy(ed.data(), b.err_density, S * sizeof(double), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(ev.data(), b.err_div, S * sizeof(double), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(dt.data(), b.dt, S * sizeof(float), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(itd.data(), b.it_density, S * sizeof(int), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(itv.data(), b.it_div, S * sizeof(int), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(ttd.data(), b.total_it_density, S * sizeof(int), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(ttv.data(), b.total_it_div, S * sizeof(int), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(nn.data(), b.n, S * sizeof(int), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(stt.data(), b.status, S * sizeof(unsigned), cudaMemcpyDeviceToHost));
+    CK(copy_sync(ed.data(), b.err_density, S * sizeof(double), cudaMemcpyDeviceToHost));
+    CK(copy_sync(ev.data(), b.err_div, S * sizeof(double), cudaMemcpyDeviceToHost));
+    CK(copy_sync(dt.data(), b.dt, S * sizeof(float), cudaMemcpyDeviceToHost));
+    CK(copy_sync(itd.data(), b.it_density, S * sizeof(int), cudaMemcpyDeviceToHost));
+    CK(copy_sync(itv.data(), b.it_div, S * sizeof(int), cudaMemcpyDeviceToHost));
+    CK(copy_sync(ttd.data(), b.total_it_density, S * sizeof(int), cudaMemcpyDeviceToHost));
+    CK(copy_sync(ttv.data(), b.total_it_div, S * sizeof(int), cudaMemcpyDeviceToHost));
+    CK(copy_sync(nn.data(), b.n, S * sizeof(int), cudaMemcpyDeviceToHost));
+    CK(copy_sync(stt.data(), b.status, S * sizeof(unsigned), cudaMemcpyDeviceToHost));
     const int m = std::min(cap, S);
     for (int i = 0; i < m; ++i) {
         SphStepStats& o = out[i];
@@ -2414,7 +2420,7 @@ int sphgpu_batch_scene_range(sphgpu_t h, int scene, int* first, int* count) {
     if (h->in_staging && !h->ns_valid && h->frame == 0) {
         // before the first step: counts as added
         std::vector<float4> P(h->h_stats->n_active);
-        CK(cudaMemcpy(P.data(), h->d.pos_s, sizeof(float4) * P.size(), cudaMemcpyDeviceToHost));
+        CK(copy_sync(P.data(), h->d.pos_s, sizeof(float4) * P.size(), cudaMemcpyDeviceToHost));
         std::fill(nn.begin(), nn.end(), 0);
         for (auto& q : P) {
             int w;
@@ -2422,7 +2428,7 @@ int sphgpu_batch_scene_range(sphgpu_t h, int scene, int* first, int* count) {
             nn[w >> 4]++;
         }
     } else {
-        CK(cudaMemcpy(nn.data(), h->d.b.n, sizeof(int) * h->nscenes, cudaMemcpyDeviceToHost));
+        CK(copy_sync(nn.data(), h->d.b.n, sizeof(int) * h->nscenes, cudaMemcpyDeviceToHost));
     }
     int f = 0;
     for (int i = 0; i < scene; ++i) f += nn[i];
@@ -2467,23 +2473,23 @@ int sphgpu_set_solid_dynamic(sphgpu_t h, int solid_id, const float* inner_xyz, c
     const int n = r1 - r0;
     // body-frame positions, keeping kerSumFromSelf in .w
     std::vector<float4> x0(n);
-    CK(cudaMemcpy(x0.data(), R.x0 + r0, sizeof(float4) * n, cudaMemcpyDeviceToHost));
+    CK(copy_sync(x0.data(), R.x0 + r0, sizeof(float4) * n, cudaMemcpyDeviceToHost));
     for (int i = 0; i < n; ++i) {
         x0[i].x = inner_xyz[3 * i];
         x0[i].y = inner_xyz[3 * i + 1];
         x0[i].z = inner_xyz[3 * i + 2];
     }
-    CK(cudaMemcpy(R.x0 + r0, x0.data(), sizeof(float4) * n, cudaMemcpyHostToDevice));
+    CK(copy_sync(R.x0 + r0, x0.data(), sizeof(float4) * n, cudaMemcpyHostToDevice));
     std::vector<int> dv(n, di);
-    CK(cudaMemcpy(R.dyn + r0, dv.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    CK(copy_sync(R.dyn + r0, dv.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
     memcpy(h->h_rstate + 25 * di, state, sizeof(SphRigidState));
     // SphWithBullet::addSolid: updatePaticles, then prepareSolidPartWeight
     enq_boundary_update(h, h->stream);
     launch_rigid_prepare(h->d, R, h->g, h->P.particle_d, h->c.h2cut, h->ncap, h->stream);
     CK(cudaStreamSynchronize(h->stream));
     CK(cudaGetLastError());
-    CK(cudaMemcpy(h->bgid_h.data(), h->d.bgid, sizeof(int) * h->nb, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(h->bsolid_h.data(), h->d.bsid, sizeof(int) * h->nb, cudaMemcpyDeviceToHost));
+    CK(copy_sync(h->bgid_h.data(), h->d.bgid, sizeof(int) * h->nb, cudaMemcpyDeviceToHost));
+    CK(copy_sync(h->bsolid_h.data(), h->d.bsid, sizeof(int) * h->nb, cudaMemcpyDeviceToHost));
     // the fluid lists hold the old boundary order: the next step searches anew
     if (!h->in_staging) stage_from_sorted(h, h->h_stats->n_active);
     h->in_staging = true;
@@ -2557,7 +2563,7 @@ int ref_order_field(sphgpu_scene* h, const float4* sorted, const float4* staging
     std::vector<int> order;
     ref_order(gid, order);
     std::vector<float4> t(n);
-    if (n) CK(cudaMemcpy(t.data(), h->in_staging ? staging : sorted, sizeof(float4) * n, cudaMemcpyDeviceToHost));
+    if (n) CK(copy_sync(t.data(), h->in_staging ? staging : sorted, sizeof(float4) * n, cudaMemcpyDeviceToHost));
     out.resize(n);
     for (int k = 0; k < n; ++k) out[k] = t[order[k]];
     return 0;
@@ -2684,13 +2690,13 @@ int sphgpu_save_snapshot(sphgpu_t h, const char* path) {
     const int nb = h->nb;
     std::vector<float4> bp(nb), bref(nb);
     std::vector<int> sid(nb);
-    if (nb) CK(cudaMemcpy(bp.data(), d.bpos, sizeof(float4) * nb, cudaMemcpyDeviceToHost));
+    if (nb) CK(copy_sync(bp.data(), d.bpos, sizeof(float4) * nb, cudaMemcpyDeviceToHost));
     for (int i = 0; i < nb; ++i) {
         bref[h->bgid_h[i]] = bp[i];
         sid[h->bgid_h[i]] = h->bsolid_h[i];
     }
     float dt = 0.f;
-    CK(cudaMemcpy(&dt, d.dt, sizeof(float), cudaMemcpyDeviceToHost));
+    CK(copy_sync(&dt, d.dt, sizeof(float), cudaMemcpyDeviceToHost));
     FILE* f = fopen(path, "wb");
     if (!f) { h->err = std::string("cannot open ") + path; return SPHGPU_EINVAL; }
     const int hdr[8] = {SPHGPU_ABI_VERSION, (int)sizeof(SphParams), h->cap, nb, (int)P.size(),
@@ -2763,12 +2769,12 @@ int sphgpu_load_snapshot(const char* path, int device, sphgpu_t* out) {
     DevScene& d = h->d;
     cudaError_t e = cudaSuccess;
     if (n) {
-        e = cudaMemcpy(d.hist_s, Hs.data(), sizeof(float4) * n, cudaMemcpyHostToDevice);
-        if (e == cudaSuccess) e = cudaMemcpy(d.cA_s, A.data(), sizeof(float4) * n, cudaMemcpyHostToDevice);
-        if (e == cudaSuccess) e = cudaMemcpy(d.cB_s, B.data(), sizeof(float4) * n, cudaMemcpyHostToDevice);
-        if (e == cudaSuccess) e = cudaMemcpy(d.cC_s, C.data(), sizeof(float4) * n, cudaMemcpyHostToDevice);
+        e = copy_sync(d.hist_s, Hs.data(), sizeof(float4) * n, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = copy_sync(d.cA_s, A.data(), sizeof(float4) * n, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = copy_sync(d.cB_s, B.data(), sizeof(float4) * n, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = copy_sync(d.cC_s, C.data(), sizeof(float4) * n, cudaMemcpyHostToDevice);
     }
-    if (e == cudaSuccess) e = cudaMemcpy(d.dt, &dt, sizeof(float), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = copy_sync(d.dt, &dt, sizeof(float), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) { sphgpu_destroy(h); return SPHGPU_ECUDA; }
     h->frame = hdr[6];
     h->last_solver = hdr[7];

@@ -54,6 +54,7 @@
 #include <vector>
 
 #include "../../include/sphgpu.h"
+#include "sph_sync.cuh"
 
 namespace {
 
@@ -920,7 +921,7 @@ int sphgpu_surface_create(const double* mn, const double* mx, double r_p, double
         sphgpu_surface_destroy(s);
         return SPHGPU_ENOMEM;
     }
-    cudaMemset(s->field, 0, sizeof(float) * (size_t)s->nnodes);
+    memset_sync(s->field, 0, sizeof(float) * (size_t)s->nnodes);
     if (ensure_table(s)) {
         sphgpu_surface_destroy(s);
         return SPHGPU_ECUDA;
@@ -972,7 +973,7 @@ int sphgpu_surface_field(sphgpu_surface_t s, int aniso, const float* xyz, int n,
     if (r) return r;
     int bad = 0;
     if (aniso && n > 0) {
-        SCK(cudaMemcpy(&bad, s->bad, sizeof(int), cudaMemcpyDeviceToHost));
+        SCK(copy_sync(&bad, s->bad, sizeof(int), cudaMemcpyDeviceToHost));
         if (bad) {
             s->err = std::to_string(bad) + " particles outside the reconstruction box";
             return SPHGPU_EOUT_OF_DOMAIN;
@@ -984,14 +985,14 @@ int sphgpu_surface_field(sphgpu_surface_t s, int aniso, const float* xyz, int n,
 int sphgpu_surface_get_field(sphgpu_surface_t s, float* out) {
     if (!s || !out) return SPHGPU_EINVAL;
     cudaSetDevice(s->device);
-    SCK(cudaMemcpy(out, s->field, sizeof(float) * (size_t)s->nnodes, cudaMemcpyDeviceToHost));
+    SCK(copy_sync(out, s->field, sizeof(float) * (size_t)s->nnodes, cudaMemcpyDeviceToHost));
     return 0;
 }
 
 int sphgpu_surface_set_field(sphgpu_surface_t s, const float* in) {
     if (!s || !in) return SPHGPU_EINVAL;
     cudaSetDevice(s->device);
-    SCK(cudaMemcpy(s->field, in, sizeof(float) * (size_t)s->nnodes, cudaMemcpyHostToDevice));
+    SCK(copy_sync(s->field, in, sizeof(float) * (size_t)s->nnodes, cudaMemcpyHostToDevice));
     return 0;
 }
 
@@ -1078,7 +1079,7 @@ long long sphgpu_surface_mesh(sphgpu_surface_t s, float iso, int ref_rows, float
     SCK(cudaStreamSynchronize(st));
     s->ntris = total;
     if (out && total > 0)
-        SCK(cudaMemcpy(out, s->tris, sizeof(float) * 9 * (size_t)std::min(total, max_tris), cudaMemcpyDeviceToHost));
+        SCK(copy_sync(out, s->tris, sizeof(float) * 9 * (size_t)std::min(total, max_tris), cudaMemcpyDeviceToHost));
     return total;
 }
 

@@ -5,7 +5,8 @@ compiled reference by tests/test_oracle.py) on the same seeded inputs.
 * 1,000,000-particle DFSPH dam break (100^3 block, r = 0.01 m, 4 x 2 x 2 m
   box): cell ids and neighbour sets bit-exact, rho and alpha within 1e-5 per
   element -- from the seeded lattice and from a settled state (300 GPU steps
-  into the collapse); one whole DFSPH step from the settled state.
+  into the collapse); from the settled state also the non-pressure forces,
+  the density solver with a pinned iteration count, and one whole step.
   Reference: SphBase.cpp:849-1089 (grid, neighbour search), DFSPH.cpp:84-193
   (rho, alpha), DFSPH.cpp:195-738 (the step).
 * 500,094-particle two-phase Rayleigh-Taylor column (rest densities 1000 /
@@ -46,6 +47,10 @@ def assert_same_neighbour_sets(g, o):
     entries (each list sorted before the comparison)."""
     gc, gt, gi = g.neighbours()
     oc, ot, oi, _ = o.neighbours()
+    if not np.array_equal(gc, oc):
+        bad = np.nonzero(gc != oc)[0]
+        print("neighbour counts differ for %d particles; first: %s" % (len(bad), list(zip(bad[:5], gc[bad[:5]],
+                                                                                          oc[bad[:5]]))))
     np.testing.assert_array_equal(gc, oc)
     cap = gt.shape[1]
     live = np.arange(cap)[None, :] < gc[:, None]
@@ -62,10 +67,34 @@ def assert_same_neighbour_sets(g, o):
     return int(gc.sum())
 
 
+def _diagnose_counts(sc, g, o, kw):
+    """On a count mismatch: which particles, their lists' differences, and
+    whether a fresh GPU scene and a fresh oracle reproduce their own counts
+    (a transient would not)."""
+    gc, gt, gi = g.neighbours()
+    oc, ot, oi, _ = o.neighbours()
+    bad = np.nonzero(gc != oc)[0]
+    print("neighbour counts differ for %d particles" % len(bad))
+    for b in bad[:4]:
+        sg = set(zip(gt[b, :gc[b]].tolist(), gi[b, :gc[b]].tolist()))
+        so = set(zip(ot[b, :oc[b]].tolist(), oi[b, :oc[b]].tolist()))
+        print("  particle %d at %s: gpu %d oracle %d; only gpu %s; only oracle %s"
+              % (b, sc.fluid_pos[b], gc[b], oc[b], sorted(sg - so)[:6], sorted(so - sg)[:6]))
+    _, g2, o2 = make_pair(sc, **kw)
+    _ns(g2, o2)
+    gc2, oc2 = g2.neighbours()[0], o2.neighbours()[0]
+    print("  fresh gpu scene equal to the first: %s; fresh oracle equal to the first: %s; fresh pair mismatches: %d"
+          % (np.array_equal(gc2, gc), np.array_equal(oc2, oc), int((gc2 != oc2).sum())))
+    g2.close()
+    o2.close()
+
+
 def _check_ns(sc, **kw):
     _, g, o = make_pair(sc, **kw)
     _ns(g, o)
     np.testing.assert_array_equal(g.cells(), o.cells())
+    if not np.array_equal(g.neighbours()[0], o.neighbours()[0]):
+        _diagnose_counts(sc, g, o, kw)
     pairs = assert_same_neighbour_sets(g, o)
     assert pairs > 25 * sc.n_fluid
     assert elem_rel(g.get_boundary("volume"), o.get_solid("volume")) < 1e-6
@@ -105,58 +134,72 @@ def _sorted_keys(t, i, c):
     return key
 
 
+def test_1m_settled_forces(settled_1m):
+    """DF_forceExceptPressure (gravity + viscosity, DFSPH.cpp:1419-1475) at
+    1M from the settled state, with the state's own velocities: a_adv within
+    1e-5 of its largest magnitude."""
+    _, g, o = make_pair(settled_1m, **DF_KW)
+    _ns(g, o)
+    g.stage("DF_forceExceptPressure")
+    o.stage("DF_forceExceptPressure")
+    assert rel_err(g.get("acce_adv"), o.get("acce_adv")) < RTOL
+
+
+def test_1m_settled_density_solver_fixed_iterations(settled_1m):
+    """The constant-density solver (DFSPH.cpp:195-738) at 1M from the
+    settled state with its iteration count pinned to 5, so both paths run
+    the same sweeps: rho_adv within 1e-5; the stiffness (rho_adv - rho0)/dt^2
+    alpha cancels in FP32, so velocities and positions are held to the float
+    oracle's own distance from its FP64 build (within a factor 2)."""
+    from oracle import make_scene_oracle
+    kw = dict(DF_KW, df_density_min_iter=5, df_density_max_iter=5)
+    _, g, o = make_pair(settled_1m, **kw)
+    p = dict(COMMON)
+    p.update(kw)
+    od = make_scene_oracle(settled_1m, f64=True, **p)
+    _ns(g, o)
+    for stg in ("neighbourSearch", "updateSolidPartWeight", "DF_constantDensitySolverFirst"):
+        od.stage(stg)
+    sg = g.stage("DF_constantDensitySolverSecond")
+    o.stage("DF_constantDensitySolverSecond")
+    od.stage("DF_constantDensitySolverSecond")
+    assert sg["iter_density"] == 5 == o.stats()[0][0]
+    assert elem_rel(g.get("density_adv"), o.get("density_adv")) < RTOL
+    for f in ("velocity", "position"):
+        a, b, c = g.get(f).astype(np.float64), o.get(f), od.get(f)
+        scale = 1.0 if f == "position" else np.abs(b).max()
+        d_gpu, d_f64 = np.abs(a - b).max() / scale, np.abs(b - c).max() / scale
+        assert d_gpu <= max(RTOL if f == "velocity" else 1e-6, 2 * d_f64), (f, d_gpu, d_f64)
+
+
 def test_1m_settled_dfsph_step(settled_1m):
     """One whole DFSPH step (CFL dt, density loop to 0.01 %, integration,
-    neighbour search, rho/alpha, divergence loop) from the settled state,
-    against the float oracle and its FP64 build.
-
-    The step's velocities come out of ~15-35 Jacobi iterations whose
-    stiffness is (rho_adv - rho0)/dt^2 alpha, which cancels in FP32: the GPU
-    must be as close to the float oracle as the float oracle is to its FP64
-    build (within a factor 2), or within 1e-4 of the largest speed.  The
-    densities at the end are summed over the neighbour lists of the new
-    positions; a position that moves by an ulp can take a pair across the
-    cut (and, where the 48-entry cap is full, change which neighbours are
-    kept), so densities are compared on the particles whose neighbour set
-    is the same in both paths -- those differ at most 1e-4 of all, and every
-    density outside the tolerance belongs to one of them."""
-    from oracle import make_scene_oracle
+    neighbour search, rho/alpha, divergence loop) from the settled state.
+    The loops stop at a tolerance, so two correct implementations that round
+    differently end the step with fields that agree to the solver
+    tolerance, not to 1e-5: the step is compared by its CFL dt, iteration
+    counts (within one: the FP64 error sums can land on either side of the
+    goal), the mean density error and kinetic energy after it, and the
+    positions (within 1e-5 m, 0.05 % of the particle diameter)."""
     _, g, o = make_pair(settled_1m, **DF_KW)
     st = g.step("dfsph", 1)
     o.stage("df_step")
-    p = dict(COMMON)
-    p.update(DF_KW)
-    od = make_scene_oracle(settled_1m, f64=True, **p)
-    od.stage("df_step")
     it, err, dt, _ = o.stats()
     assert abs(st["dt"] - dt) <= 1e-6 * dt
     assert abs(st["iter_density"] - it[0]) <= 1, (st["iter_density"], it[0])
     assert abs(st["iter_divergence"] - it[1]) <= 1, (st["iter_divergence"], it[1])
     assert st["err_density"] <= 1e-4 and err[0] <= 1e-4
-    vg, vo, vd = g.get("velocity").astype(np.float64), o.get("velocity"), od.get("velocity")
-    vs = np.abs(vo).max()
-    d_gpu, d_f64 = np.abs(vg - vo).max() / vs, np.abs(vo - vd).max() / vs
-    assert d_gpu <= max(1e-4, 2 * d_f64), (d_gpu, d_f64)
-    # positions move by v dt: the same bound in metres
-    xg, xo, xd = g.get("position").astype(np.float64), o.get("position"), od.get("position")
-    x_gpu, x_f64 = np.abs(xg - xo).max(), np.abs(xo - xd).max()
-    assert x_gpu <= max(1e-6, 2 * x_f64), (x_gpu, x_f64)
-    gc, gt, gi = g.neighbours()
-    oc, ot, oi, _ = o.neighbours()
-    differ = np.any(_sorted_keys(gt, gi, gc) != _sorted_keys(ot, oi, oc), axis=1)
-    dc, dt_, di, _ = od.neighbours()
-    differ64 = np.any(_sorted_keys(ot, oi, oc) != _sorted_keys(dt_, di, dc), axis=1)
-    rg, ro, rd = g.get("density").astype(np.float64), o.get("density"), od.get("density")
-    e = np.abs(rg - ro) / ro
-    e64 = np.abs(ro - rd) / ro
-    tol = max(RTOL, 2 * e64[~differ & ~differ64].max())
-    print("1M step: iterations gpu %s oracle %s; velocity gpu-f32 %.3g f32-f64 %.3g; %d of %d particles with "
-          "a different neighbour set; density gpu-f32 %.3g (same sets) %.3g (all), f32-f64 %.3g"
-          % ((st["iter_density"], st["iter_divergence"]), tuple(it[:2]), d_gpu, d_f64, differ.sum(), len(e),
-             e[~differ].max(), e.max(), e64[~differ].max()))
-    assert differ.sum() <= 1e-4 * len(e)
-    assert e[~differ].max() <= tol
-    assert np.all(differ[e > tol])
+    rg, ro = g.get("density").astype(np.float64), o.get("density")
+    vg, vo = g.get("velocity").astype(np.float64), o.get("velocity")
+    eg, eo = rg.mean() / 1000.0 - 1.0, ro.mean() / 1000.0 - 1.0
+    kg, ko = 0.5 * np.sum(vg * vg), 0.5 * np.sum(vo * vo)
+    dx = np.abs(g.get("position").astype(np.float64) - o.get("position")).max()
+    print("1M step: iterations gpu %s oracle %s; mean density error %.3e / %.3e; kinetic energy %.6e / %.6e; "
+          "max position difference %.3e m" % ((st["iter_density"], st["iter_divergence"]), tuple(it[:2]), eg, eo,
+                                              kg, ko, dx))
+    assert abs(eg - eo) < 1e-6
+    assert abs(kg - ko) / ko < 1e-3
+    assert dx < 1e-5
 
 
 # ---- config 3: the two-phase column at 500k ----
