@@ -120,25 +120,21 @@ __global__ void k_merge_starts(DevScene s, int nk) {
     if (k <= nk) s.cstart2[k] = make_int2(s.cell_start[k], s.bcell_start[k]);
 }
 
-// Ints per thread of the shared-memory list staging: the first LROW entries
-// of a list (a multiple of 4, so rows start on 16-byte boundaries and the
-// rows of 8 consecutive threads fall on distinct bank quads); entries past
-// them (particles with more than LROW neighbours, near walls) go straight
-// to the global list.  36 of the cap's 48 keeps the rows small enough that
-// 10 blocks of 128 threads fit an SM with L1 to spare.
-constexpr int LROW = 36;
+// Ints per thread of the shared-memory list staging (>= the cap of 48, a
+// multiple of 4 so that every row starts on a 16-byte boundary; 52 also
+// spreads the rows of 8 consecutive threads over distinct bank quads).
+constexpr int LROW = 52;
 
 // mode 0: neighbour lists only; 1: + DFSPH rho and alpha
 // (DF_constantDensitySolverFirst, DFSPH.cpp:84-193); 2: + WCSPH rho and Tait
 // pressure (WcSph::wc_computePressure, WcSph.cpp:99-153); 3: + IISph
 // sphDensity, gamma, sphVolume and alpha (IISph.cpp:100-402).
 //
-// STAGED: a kept neighbour among the first LROW is one predicated
-// shared-memory store into the thread's row -- no divergent branch around a
-// global store in the candidate loop -- and that part of the list leaves in
-// 16-byte groups (a warp writes whole sectors); the rho/alpha pass reads it
-// back from shared memory.  Entries past LROW, and every entry when not
-// STAGED, go straight to the global ELL list.
+// STAGED (cap <= 48): a kept neighbour is one predicated shared-memory store
+// into the thread's row -- no divergent branch around a global store in the
+// candidate loop -- and the finished list leaves in 16-byte groups (a warp
+// writes whole sectors); the rho/alpha pass reads the list back from shared
+// memory.  Otherwise entries go straight to the global ELL list.
 template <int MODE, int BS, bool STAGED>
 __global__ void __launch_bounds__(BS) k_build(DevScene s, GridGeom g, SolverConst c) {
     extern __shared__ int4 list_smem[];
@@ -177,8 +173,7 @@ __global__ void __launch_bounds__(BS) k_build(DevScene s, GridGeom g, SolverCons
                         const bool hit = len2 < c.h2cut && q != p;
                         if (STAGED) {
                             // cnt counts every hit; the first `cap` are kept
-                            if (hit && cnt < LROW) row[cnt] = q;
-                            if (hit && cnt >= LROW && cnt < cap) out[ell_index(stride, p, cnt)] = q;
+                            if (hit && cnt < cap) row[cnt] = q;
                             cnt += hit;
                         } else if (hit) {
                             if (cnt < cap) out[ell_index(stride, p, cnt++)] = q;
@@ -190,8 +185,7 @@ __global__ void __launch_bounds__(BS) k_build(DevScene s, GridGeom g, SolverCons
                         const float len2 = dis_square_rn(pa.x, pa.y, pa.z, pb.x, pb.y, pb.z);
                         const bool hit = len2 < c.h2cut;
                         if (STAGED) {
-                            if (hit && cnt < LROW) row[cnt] = q | (int)BND_FLAG;
-                            if (hit && cnt >= LROW && cnt < cap) out[ell_index(stride, p, cnt)] = q | (int)BND_FLAG;
+                            if (hit && cnt < cap) row[cnt] = q | (int)BND_FLAG;
                             cnt += hit;
                         } else if (hit) {
                             if (cnt < cap) out[ell_index(stride, p, cnt++)] = q | (int)BND_FLAG;
@@ -208,8 +202,7 @@ __global__ void __launch_bounds__(BS) k_build(DevScene s, GridGeom g, SolverCons
             // read: every sweep masks them)
             const int4* r4 = reinterpret_cast<const int4*>(row);
             int4* o4 = reinterpret_cast<int4*>(out);
-            const int ngs = min(cnt, LROW);
-            for (int gi = 0; gi < ((ngs + 3) >> 2); ++gi) o4[(size_t)gi * stride + p] = r4[gi];
+            for (int gi = 0; gi < ((cnt + 3) >> 2); ++gi) o4[(size_t)gi * stride + p] = r4[gi];
         }
         s.ncount[p] = cnt;
         if (MODE == 3) {
@@ -223,7 +216,7 @@ __global__ void __launch_bounds__(BS) k_build(DevScene s, GridGeom g, SolverCons
             float sphv = (float)((double)w0 * (double)Va * (double)Va);
             float a1x = 0.f, a1y = 0.f, a1z = 0.f, a2 = 0.f;
             for (int k = 0; k < cnt; ++k) {
-                const unsigned e = (STAGED && k < LROW) ? (unsigned)row[k] : (unsigned)out[ell_index(stride, p, k)];
+                const unsigned e = STAGED ? (unsigned)row[k] : (unsigned)out[ell_index(stride, p, k)];
                 const bool bnd = (e & BND_FLAG) != 0u;
                 const float4 pb = __ldg((bnd ? BP : P) + (e & BND_MASK));
                 const float xx = pa.x - pb.x, xy = pa.y - pb.y, xz = pa.z - pb.z;
@@ -250,7 +243,7 @@ __global__ void __launch_bounds__(BS) k_build(DevScene s, GridGeom g, SolverCons
             float density = ker_W(c.k, 0.f) * fm0;
             float a1x = 0.f, a1y = 0.f, a1z = 0.f, a2 = 0.f;
             for (int k = 0; k < cnt; ++k) {
-                const unsigned e = (STAGED && k < LROW) ? (unsigned)row[k] : (unsigned)out[ell_index(stride, p, k)];
+                const unsigned e = STAGED ? (unsigned)row[k] : (unsigned)out[ell_index(stride, p, k)];
                 const bool bnd = (e & BND_FLAG) != 0u;
                 const float4 pb = __ldg((bnd ? BP : P) + (e & BND_MASK));
                 const float xx = pa.x - pb.x, xy = pa.y - pb.y, xz = pa.z - pb.z;
@@ -406,9 +399,9 @@ template <int BS>
 static void launch_build_bs(const DevScene& s, const GridGeom& g, const SolverConst& c, int mode, int n_max,
                             cudaStream_t st) {
     const int nb = nblk(n_max > 0 ? n_max : 1, BS);
-    // staging needs the rows to fit the default 48 KB of dynamic shared
-    // memory (64 and 128 threads per block)
-    if (BS * LROW * sizeof(int) <= 48 * 1024) launch_build_st<BS, true>(s, g, c, mode, nb, st);
+    // staging needs the cap to fit a row and the rows to fit the default
+    // 48 KB of dynamic shared memory (64 and 128 threads per block)
+    if (c.cap <= LROW - 4 && BS * LROW * sizeof(int) <= 48 * 1024) launch_build_st<BS, true>(s, g, c, mode, nb, st);
     else launch_build_st<BS, false>(s, g, c, mode, nb, st);
 }
 

@@ -152,7 +152,9 @@ def test_1m_settled_density_solver_fixed_iterations(settled_1m):
     alpha cancels in FP32, so velocities and positions are held to the float
     oracle's own distance from its FP64 build (within a factor 2)."""
     from oracle import make_scene_oracle
-    kw = dict(DF_KW, df_density_min_iter=5, df_density_max_iter=5)
+    # a fixed dt (the stage runs the loop at the scene's dt; the CFL rule
+    # belongs to the whole step)
+    kw = dict(DF_KW, cfl=0, dt=5e-4, df_density_min_iter=5, df_density_max_iter=5)
     _, g, o = make_pair(settled_1m, **kw)
     p = dict(COMMON)
     p.update(kw)
