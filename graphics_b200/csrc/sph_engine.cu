@@ -1511,15 +1511,61 @@ int sphgpu_step(sphgpu_t h, int solver, int nsteps, SphStepStats* stats) {
     return r;
 }
 
+// One step from and to host buffers.  When the device holds a sorted state
+// with valid lists (a DFSPH step ended there, no particle was ever removed),
+// the incoming state is compared with it on the device: velocities are
+// copied in, and only if a position differs are the positions staged for a
+// new neighbour search -- a caller that hands back the previous step's
+// output (the usual loop) pays for the transfers, not for a search.  The
+// transfers are stream-ordered, with one host synchronisation for the
+// comparison and one at the end.
 int sphgpu_step_host(sphgpu_t h, int solver, const float* xyz, const float* vel, float* xyz_out, float* vel_out,
                      SphStepStats* stats) {
     if (!h) return SPHGPU_EINVAL;
     int r = 0;
-    if (xyz && (r = sphgpu_set_fluid(h, "position", xyz)) < 0) return r;
-    if (vel && (r = sphgpu_set_fluid(h, "velocity", vel)) < 0) return r;
+    cudaSetDevice(h->device);
+    CK(cudaStreamSynchronize(h->stream));
+    const bool fast = xyz && vel && solver == SPHGPU_DFSPH && h->total_removed == 0 && !h->in_staging &&
+                      h->ns_valid && h->nscenes == 1 && h->R.nd == 0;
+    if (fast) {
+        DevScene& d = h->d;
+        const int n = h->h_stats->n_active;
+        float* tx = (float*)d.aux4;
+        float* tv = (float*)d.vadv;
+        CK(cudaMemcpyAsync(tx, xyz, sizeof(float) * 3 * (size_t)n, cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(tv, vel, sizeof(float) * 3 * (size_t)n, cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemsetAsync(&d.st->cont, 0, sizeof(int), h->stream));
+        launch_state_in(tx, tv, d.gid, n, d.pos, d.vel, d.prv, &d.st->cont, h->stream);
+        CK(cudaMemcpyAsync(h->h_cont, &d.st->cont, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        if (*h->h_cont) {
+            // a position changed: the sorted state is staged and searched again
+            launch_from_ref_order(tx, d.gid, n, d.pos, h->stream);
+            h->ns_valid = false;
+            stage_from_sorted(h, n);
+            h->in_staging = true;
+        }
+    } else {
+        if (xyz && (r = sphgpu_set_fluid(h, "position", xyz)) < 0) return r;
+        if (vel && (r = sphgpu_set_fluid(h, "velocity", vel)) < 0) return r;
+    }
     r = sphgpu_step(h, solver, 1, stats);
     if (r && r != SPHGPU_EMAXITER) return r;
     int r2 = 0;
+    if (h->total_removed == 0 && xyz_out && vel_out) {
+        // both outputs reordered on the device, copied out back to back
+        DevScene& d = h->d;
+        const int n = h->h_stats->n_active;
+        const bool stg = h->in_staging;
+        float* tx = (float*)d.aux4;
+        float* tv = (float*)d.vadv;
+        launch_to_ref_order(stg ? d.pos_s : d.pos, stg ? d.gid_s : d.gid, n, tx, h->stream);
+        launch_to_ref_order(stg ? d.vel_s : d.vel, stg ? d.gid_s : d.gid, n, tv, h->stream);
+        CK(cudaMemcpyAsync(xyz_out, tx, sizeof(float) * 3 * (size_t)n, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(vel_out, tv, sizeof(float) * 3 * (size_t)n, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        return r;
+    }
     if (xyz_out) r2 = sphgpu_get_fluid(h, "position", xyz_out) < 0 ? SPHGPU_ECUDA : 0;
     if (!r2 && vel_out) r2 = sphgpu_get_fluid(h, "velocity", vel_out) < 0 ? SPHGPU_ECUDA : 0;
     return r2 ? r2 : r;

@@ -344,6 +344,26 @@ __global__ void k_to_ref_order(const float4* src, const int* gid, int n, float* 
     dst3[g + 1] = v.y;
     dst3[g + 2] = v.z;
 }
+// A host step's incoming state (reference order) against the sorted state
+// whose lists are still valid: velocities go straight into the sorted
+// arrays (vel and the velocity half of the force kernel's record); a
+// position that differs from the device's sets *changed, and the caller
+// then stages the positions and searches again.
+__global__ void k_state_in(const float* xyz3, const float* vel3, const int* gid, int n, const float4* pos,
+                           float4* vel, float4* prv, int* changed) {
+    const int p = blockIdx.x * NT + threadIdx.x;
+    int diff = 0;
+    if (p < n) {
+        const size_t g = (size_t)gid[p] * 3;
+        const float4 x = pos[p];
+        diff = x.x != xyz3[g] || x.y != xyz3[g + 1] || x.z != xyz3[g + 2];
+        const float4 v = make_float4(vel3[g], vel3[g + 1], vel3[g + 2], 0.f);
+        vel[p] = v;
+        prv[2 * p + 1] = v;
+    }
+    if (__syncthreads_or(diff) && threadIdx.x == 0) atomicOr(changed, 1);
+}
+
 __global__ void k_from_ref_order(const float* src3, const int* gid, int n, float4* dst) {
     int p = blockIdx.x * NT + threadIdx.x;
     if (p >= n) return;
@@ -360,6 +380,10 @@ static inline int nblk(int n, int nt) { return (n + nt - 1) / nt; }
 
 void launch_to_ref_order(const float4* src, const int* gid, int n, float* dst3, cudaStream_t st) {
     if (n > 0) k_to_ref_order<<<nblk(n, NT), NT, 0, st>>>(src, gid, n, dst3);
+}
+void launch_state_in(const float* xyz3, const float* vel3, const int* gid, int n, const float4* pos, float4* vel,
+                     float4* prv, int* changed, cudaStream_t st) {
+    if (n > 0) k_state_in<<<nblk(n, NT), NT, 0, st>>>(xyz3, vel3, gid, n, pos, vel, prv, changed);
 }
 void launch_from_ref_order(const float* src3, const int* gid, int n, float4* dst, cudaStream_t st) {
     if (n > 0) k_from_ref_order<<<nblk(n, NT), NT, 0, st>>>(src3, gid, n, dst);

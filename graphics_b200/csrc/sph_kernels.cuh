@@ -181,6 +181,10 @@ void launch_build(const DevScene& s, const GridGeom& g, const SolverConst& c, in
                   int bs = 128);
 void launch_to_ref_order(const float4* src, const int* gid, int n, float* dst3, cudaStream_t st);
 void launch_from_ref_order(const float* src3, const int* gid, int n, float4* dst, cudaStream_t st);
+// host state (reference order) into a sorted state with valid lists:
+// velocities copied in, *changed set when a position differs
+void launch_state_in(const float* xyz3, const float* vel3, const int* gid, int n, const float4* pos, float4* vel,
+                     float4* prv, int* changed, cudaStream_t st);
 void launch_boundary_keys(const float4* bpos, int nb, const GridGeom& g, int* keys, cudaStream_t st);
 // boundary particles [b0, b1) (one scene of a batch, or all)
 void launch_boundary_volume(const DevScene& s, const GridGeom& g, float dpart, float h2cut, int cap, int b0, int b1,

@@ -240,3 +240,30 @@ def test_larger_scene_density_error_property():
         assert (st["err_density"] <= 1e-4) or (st["status"] & 1)
         assert st["n_fluid"] == sc.n_fluid
     assert np.isfinite(g.get("position")).all()
+
+
+def test_step_host_matches_device_steps():
+    """sphgpu_step_host (host buffers in and out) against the same steps on
+    the device state: handing back the previous output (lists still valid,
+    no new search), changing only velocities, and moving one particle
+    (positions staged and searched again) all give the device path's
+    result bit for bit."""
+    sc, g, o = make_pair(cfl=1)
+    sc2, ref, o2 = make_pair(cfl=1)
+    g.step("dfsph", 2)
+    ref.step("dfsph", 2)
+    pos, vel = g.get("position"), g.get("velocity")
+    po, vo = np.empty_like(pos), np.empty_like(vel)
+    for k in range(3):
+        if k == 1:
+            vel = vel * np.float32(0.5)
+            ref.set("velocity", vel)
+        if k == 2:
+            pos = pos.copy()
+            pos[7] += np.float32(0.001)
+            ref.set("position", pos)
+        g.step_host("dfsph", pos, vel, po, vo)
+        ref.step("dfsph", 1)
+        np.testing.assert_array_equal(po, ref.get("position"))
+        np.testing.assert_array_equal(vo, ref.get("velocity"))
+        pos, vel = po.copy(), vo.copy()
