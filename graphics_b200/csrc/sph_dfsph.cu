@@ -335,15 +335,22 @@ __global__ void __launch_bounds__(BS) k_df_div_a(DevScene s, SolverConst c) {
     if (finish_sum<BS>(s.partial, &s.st->ticket[1], bs, &tot)) s.st->err_div = n > 0 ? tot / (double)n : 0.0;
 }
 
-// FP64 max |v| and the CFL step dt = clamp(cfl * d / vmax, dt_min, dt_max)
+// FP64 max |v| and the CFL step dt = clamp(cfl * d / vmax, dt_min, dt_max).
+// Each thread takes CFL_ITEMS velocities and the maximum is taken over the
+// squared speeds, with one square root at the end: sqrt is correctly rounded
+// and monotone, so this is the maximum of the per-particle speeds exactly.
+constexpr int CFL_ITEMS = 8;
 __global__ void __launch_bounds__(NT) k_cfl(DevScene s, float cfl, float d, float dt_max, float dt_min) {
     const int n = s.st->n_active;
-    const int p = blockIdx.x * NT + threadIdx.x;
     double m = 0.0;
-    if (p < n) {
-        float4 v = s.vel[p];
-        double x = v.x, y = v.y, z = v.z;
-        m = sqrt(x * x + y * y + z * z);
+#pragma unroll
+    for (int k = 0; k < CFL_ITEMS; ++k) {
+        const int p = (blockIdx.x * CFL_ITEMS + k) * NT + threadIdx.x;
+        if (p < n) {
+            const float4 v = s.vel[p];
+            const double x = v.x, y = v.y, z = v.z;
+            m = fmax(m, x * x + y * y + z * z);
+        }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
@@ -372,6 +379,7 @@ __global__ void __launch_bounds__(NT) k_cfl(DevScene s, float cfl, float d, floa
     if (threadIdx.x == 0) {
         double vmax = 0;
         for (int i = 0; i < NT / 32; ++i) vmax = fmax(vmax, sh[i]);
+        vmax = sqrt(vmax);
         double dt = vmax > 0 ? (double)cfl * (double)d / vmax : (double)dt_max;
         if (dt > dt_max) dt = dt_max;
         if (dt < dt_min) dt = dt_min;
@@ -420,5 +428,5 @@ void launch_df_div_b(const DevScene& s, const SolverConst& c, int n_max, double 
                         s, c, goal_abs, goal_rel, min_it, max_it, (cudaGraphConditionalHandle)cond_handle, use_handle)));
 }
 void launch_cfl(const DevScene& s, int n_max, float cfl, float d, float dt_max, float dt_min, cudaStream_t st) {
-    k_cfl<<<nblk(n_max), NT, 0, st>>>(s, cfl, d, dt_max, dt_min);
+    k_cfl<<<nblk(n_max, NT * CFL_ITEMS), NT, 0, st>>>(s, cfl, d, dt_max, dt_min);
 }

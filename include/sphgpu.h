@@ -193,7 +193,11 @@ int sphgpu_synchronize(sphgpu_t h, SphStepStats* stats);
 
 /* Host-buffer round trip for one step (the drop-in path, where the host
  * arrays stay authoritative): upload xyz/vel (n*3 floats, reference order),
- * run one step, download positions and velocities into xyz_out/vel_out. */
+ * run one step, download positions and velocities into xyz_out/vel_out.
+ * When the device state ended a DFSPH step (lists valid, no particle ever
+ * removed), the upload is compared with it on the device: velocities are
+ * taken as given, and the neighbour search runs again only if a position
+ * differs -- handing back the previous output costs the transfers only. */
 int sphgpu_step_host(sphgpu_t h, int solver, const float* xyz, const float* vel, float* xyz_out,
                      float* vel_out, SphStepStats* stats);
 
