@@ -152,3 +152,95 @@ def test_scene_inference_kernel_matches_oracle():
     assert xn.shape == (g.n_fluid, NIN) and np.all(np.isfinite(xn))
     assert np.max(np.abs(kw - ko)) <= 2e-3 * np.max(np.abs(ko)) + 1e-5
     g.close()
+
+
+def _bf16(x):
+    a = np.asarray(x, np.float32).copy().view(np.uint32)
+    a = (a + (((a >> 16) & 1) + np.uint32(0x7FFF))) & np.uint32(0xFFFF0000)
+    return a.view(np.float32).astype(np.float64)
+
+
+def test_feature_gather_matches_cpu_restatement():
+    """The warm-start feature gather (k_ws_features) against a CPU
+    restatement of its 16 features from the same state: the neighbour lists,
+    densities, alpha and non-pressure accelerations of the CPU oracle from
+    the GPU's state after one warm-start step, the velocities and the
+    per-particle history (the last step's stiffness sum, predicted error and
+    divergence term) of the GPU.  The GPU hands the features over as the
+    network's BF16 inputs (identity normalisation here), so they agree to
+    BF16 rounding."""
+    from graphics_b200.scene import small_dam_break
+    from graphics_b200.sph import scene_to_gpu
+    from helpers import COMMON
+    from oracle import make_scene_oracle
+    from graphics_b200.warmstart import attach
+    rng = np.random.default_rng(11)
+    net = _net()
+    w, _ = _random_state(rng)
+    net.set_params(w * np.float32(0.2))
+    net.set_norm(np.concatenate([np.zeros(NIN), np.ones(NIN), [0.0, 1.0]]).astype(np.float32))
+    sc = small_dam_break((14, 14, 14), 0.025, seed=4)
+    kw = dict(cfl=0, dt=1e-3, dt_max=2e-3, nu=1e-3, ws_scale=1.0)
+    g = scene_to_gpu(sc, **kw)
+    attach(g, net, 1)
+    g.step("dfsph", 1)
+    pos, vel, hist = (g.get(f).astype(np.float64) for f in ("position", "velocity", "ws_hist"))
+    g.step("dfsph", 1)
+    feat = g.get("ws_features").astype(np.float64)
+    g.close()
+    # the CPU side of the second step's features, from the state after the first
+    p = dict(COMMON)
+    p.update(kw)
+    o = make_scene_oracle(sc, **{k: v for k, v in p.items() if k != "ws_scale"})
+    o.set("position", pos)
+    o.set("velocity", vel)
+    o.set_frame(0)
+    for stg in ("neighbourSearch", "updateSolidPartWeight", "DF_constantDensitySolverFirst", "DF_forceExceptPressure"):
+        o.stage(stg)
+    cnt, t, idx, _ = o.neighbours()
+    rho, alpha, a_adv, a1 = o.get("density"), o.get("DFalpha"), o.get("acce_adv"), o.get("DFalpha1")
+    vol = o.get_solid("volume")
+    o.close()
+    d, dt, rho0 = sc.d, kw["dt"], sc.rho0
+    m_f = rho0 * d ** 3
+    va = vel + a_adv * dt
+    live = np.arange(t.shape[1])[None, :] < cnt[:, None]
+    bnd = t > 0
+    j = np.where(live, idx, 0)
+    bpos = sc.boundary_pos.astype(np.float64)
+    xj = np.where(bnd[..., None], bpos[np.where(bnd, j, 0)], pos[np.where(bnd, 0, j)])
+    vj = np.where(bnd[..., None], 0.0, va[np.where(bnd, 0, j)])
+    mj = np.where(bnd, rho0 * vol[np.where(bnd, j, 0)], m_f)
+    xij = pos[:, None, :] - xj
+    r = np.linalg.norm(xij, axis=2)
+    r = np.where(live, r, 1.0)
+    q = r / d
+    sig = 1.0 / (np.pi * d ** 3)
+    dw = np.where(q <= 1, sig / d * (-3 * q + 2.25 * q * q), -sig / d * 0.75 * (2 - q) ** 2)
+    grad = (mj * dw / r)[..., None] * xij
+    acc = np.where(live, np.einsum("nkc,nkc->nk", grad, va[:, None, :] - vj), 0.0).sum(1)
+    nb = (live & bnd).sum(1)
+    nfl = (live & ~bnd).sum(1)
+    kp = np.where(live & ~bnd, hist[np.where(bnd, 0, j), 0], 0.0).sum(1)
+    # alpha of an interior particle of the ideal lattice (the feature's scale)
+    ii = np.array([(a, b, c) for a in range(-2, 3) for b in range(-2, 3) for c in range(-2, 3)], np.float64)
+    rr = d * np.linalg.norm(ii, axis=1)
+    rr = rr[(rr > 0) & (rr < 2 * d)]
+    qq = rr / d
+    W = lambda x: np.where(x <= 1, sig * (1 - 1.5 * x * x + 0.75 * x ** 3), sig * 0.25 * (2 - x) ** 3)
+    Wg = np.where(qq <= 1, sig / d * (3 * qq - 2.25 * qq * qq), sig / d * 0.75 * (2 - qq) ** 2)
+    alpha_ref = m_f * (W(0.0) + W(qq).sum()) / ((m_f * Wg) ** 2).sum()
+    divt = dt * acc / rho0 * 100
+    pred = (np.maximum(rho + acc * dt, rho0) - rho0) / rho0 * 100
+    x = np.stack([cnt / 32, (rho - rho0) / rho0 * 100, divt, pred, 0.1 * hist[:, 0], hist[:, 1], hist[:, 2],
+                  np.linalg.norm(vel, axis=1) * dt / d, np.linalg.norm(a_adv, axis=1) * dt * dt / d,
+                  np.where(cnt > 0, nb / np.maximum(cnt, 1), 0), np.log(np.maximum(alpha, 1e-30) / alpha_ref),
+                  np.where(nfl > 0, 0.1 * kp / np.maximum(nfl, 1), 0), np.full(len(cnt), dt / kw["dt_max"]),
+                  np.linalg.norm(a1, axis=1) * d / rho0, vel[:, 1] * dt / d, np.ones(len(cnt))], axis=1)
+    # two BF16 steps of the value, plus 0.2 % of the feature's range for the
+    # FP32 sums behind the differences rho - rho0 and the divergence term
+    ref = _bf16(x)
+    scale = np.abs(x).max(0) + 1e-12
+    excess = np.abs(feat - ref) - (2.0 ** -7 * np.abs(ref) + 2e-3 * scale)
+    assert np.all(excess <= 0), excess.max(0)
+    assert np.abs(x[:, 4]).max() > 0 and np.abs(x[:, 11]).max() > 0  # the history features are exercised
