@@ -77,6 +77,16 @@ struct sphgpu_scene {
     std::vector<int> phase_n;
     int n_total = 0;  // particles known to the host (before removals)
     bool ns_valid = false, in_staging = true;
+    // Sort bookkeeping for the getters.  A DFSPH step writes the
+    // non-pressure acceleration (and the vorticity vectors) and the density
+    // loop's per-particle results before its neighbour search re-sorts the
+    // particles, so after the step those arrays are in the previous sorted
+    // order -- the order the integration copied into the staging arrays
+    // (gid_s).  sorts counts the sorts enqueued; ep_acc / ep_loop / ep_vort
+    // hold the count at which each group was last written (the vorticity
+    // vectors of options 1 and 2 come before the sort, those of option 3
+    // after the divergence loop).
+    long sorts = 0, ep_acc = -2, ep_loop = -2, ep_vort = -2;
     int frame = 0;
     double time = 0;
     void* cub_tmp = nullptr;
@@ -749,6 +759,7 @@ int run_initial_ns(sphgpu_scene* h, int build_mode) {
     if (!h->in_staging) stage_from_sorted(h, h->h_stats->n_active);  // the sort reads staging
     enq_boundary_update(h, h->stream);
     enq_ns(h, 0, build_mode, h->stream, 1 | 2 | 4 | 8);
+    ++h->sorts;
     h->in_staging = false;
     h->ns_valid = build_mode == 1;
     CK(cudaMemcpyAsync(h->h_stats, h->d.st, sizeof(DevStats), cudaMemcpyDeviceToHost, h->stream));
@@ -904,6 +915,8 @@ int enq_steps(sphgpu_scene* h, int solver, int nsteps) {
                 if (r) return r;
                 prof_collect(h);
             }
+            // the step sorts first, then writes every per-particle result
+            h->ep_acc = h->ep_loop = ++h->sorts;
             h->frame++;
         }
         h->in_staging = true;
@@ -953,6 +966,9 @@ int enq_steps(sphgpu_scene* h, int solver, int nsteps) {
                     prof_collect(h);
                 }
             }
+            // forces and the density loop ran before the step's sort
+            h->ep_acc = h->ep_loop = h->sorts++;
+            h->ep_vort = h->P.enable_vortex == 3 ? h->sorts : h->sorts - 1;
             h->frame++;
         }
         return 0;
@@ -965,6 +981,7 @@ int enq_steps(sphgpu_scene* h, int solver, int nsteps) {
         const bool surf = h->P.th_h != 0.f || h->P.th_r != 0.f || h->P.th_bt != 0.f;
         if (surf) launch(h, "wc_normal", h->stream, [&] { launch_wc_normal(h->d, h->c, h->cap, h->stream); });
         launch(h, "wc_force", h->stream, [&] { launch_wc_force(h->d, h->c, h->cap, h->stream, surf); });
+        h->ep_acc = h->ep_loop = ++h->sorts;
         h->in_staging = true;
         h->ns_valid = false;
         CK(cudaMemcpyAsync(h->h_stats, h->d.st, sizeof(DevStats), cudaMemcpyDeviceToHost, h->stream));
@@ -1609,6 +1626,30 @@ int sphgpu_get_fluid(sphgpu_t h, const char* field, float* out) {
     if (download_gid(h, gid, n, staging)) return SPHGPU_ECUDA;
     std::vector<int> order;
     ref_order(gid, order);
+    // arrays written before the last sort are read through the order the
+    // integration staged (gid_s): order[k] becomes the slot the k-th particle
+    // held then
+    const bool acc_group = f == "acce_adv" || f == "acceleration" || f == "advectionAcceleration" ||
+                           (f == "acce_presure" && h->last_solver != SPHGPU_IISPH);
+    const bool vort_group = f == "omega" || f == "deltaVorticity" || f == "dOmega" || f == "psi";
+    const bool loop_group = f == "DFkappa" || f == "kappa_sum" || f == "kappa_warm" || f == "density_adv" ||
+                            f == "ws_features" || f == "VF_kappa" || f == "VF_advectionVolume";
+    const long ep = acc_group ? h->ep_acc : (loop_group ? h->ep_loop : (vort_group ? h->ep_vort : h->sorts));
+    if (!staging && ep == h->sorts - 1) {
+        const int ns = h->h_stats->pad0;
+        std::vector<int> gs(ns);
+        if (ns) CK(copy_sync(gs.data(), h->d.gid_s, sizeof(int) * ns, cudaMemcpyDeviceToHost));
+        int mx = 0;
+        for (int v : gs) mx = std::max(mx, v);
+        for (int v : gid) mx = std::max(mx, v);
+        std::vector<int> inv((size_t)mx + 1, -1);
+        for (int i = 0; i < ns; ++i) inv[gs[i]] = i;
+        for (int k = 0; k < n; ++k) {
+            const int o = inv[gid[order[k]]];
+            if (o < 0) { h->err = "field " + f + " has no value for a particle of the last sort"; return SPHGPU_EINVAL; }
+            order[k] = o;
+        }
+    }
     int comps = 1;
     const void* src = nullptr;
     bool f4 = false;
@@ -1872,6 +1913,7 @@ int sphgpu_stage(sphgpu_t h, const char* name, SphStepStats* stats) {
         enq_boundary_update(h, st);
         if (h->in_staging) {
             enq_ns(h, 0, mode, st, h->P.enable_vortex ? 3 : 1);
+            ++h->sorts;
             h->in_staging = false;
         } else {
             if (h->R.nd) {
@@ -1887,6 +1929,7 @@ int sphgpu_stage(sphgpu_t h, const char* name, SphStepStats* stats) {
     } else if (s == "DF_forceExceptPressure") {
         if (h->in_staging) { h->err = "run neighbourSearch first"; return SPHGPU_EINVAL; }
         launch_df_forces(d, h->c, h->cap, 0, st);
+        h->ep_acc = h->sorts;
     } else if (s == "DF_constantDensitySolverSecond") {
         if (h->in_staging) { h->err = "run neighbourSearch first"; return SPHGPU_EINVAL; }
         if (h->P.cfl) launch_cfl(d, h->cap, h->P.cfl_factor, h->P.particle_d, h->P.dt_max, h->P.dt_min, st);
@@ -1911,15 +1954,21 @@ int sphgpu_stage(sphgpu_t h, const char* name, SphStepStats* stats) {
         // integrate into staging (the reference updates positions in place)
         cudaMemsetAsync(d.cell_count, 0, sizeof(int) * ((size_t)h->g.nkeys + 1), st);
         launch_hash(d, h->g, h->P.enable_vortex ? 3 : 1, h->cap, st);
+        h->ep_acc = h->ep_loop = h->sorts;
+        if (h->P.enable_vortex == 1 || h->P.enable_vortex == 2) h->ep_vort = h->sorts;
         h->in_staging = true;
         h->ns_valid = false;
     } else if (s == "DF_divergenceFreeSolver") {
         if (h->in_staging) { h->err = "run neighbourSearch first"; return SPHGPU_EINVAL; }
         r = enq_df_div_loop(h, false);
         if (r) return r;
-        if (h->P.enable_vortex == 3) launch_vortex_after_div(d, h->c, h->P.spacing_r, h->cap, st);
+        if (h->P.enable_vortex == 3) {
+            launch_vortex_after_div(d, h->c, h->P.spacing_r, h->cap, st);
+            h->ep_vort = h->sorts;
+        }
     } else if (s == "VF_prepareAttribute") {
         if ((r = ensure_iv_boundary(h))) return r;
+        if (h->in_staging) ++h->sorts;
         enq_iv_prepare(h, h->in_staging, st);
         h->in_staging = false;
         h->ns_valid = false;
@@ -1931,11 +1980,13 @@ int sphgpu_stage(sphgpu_t h, const char* name, SphStepStats* stats) {
             launch_iv_integrate(d, h->cap, st);
             h->in_staging = true;
         } else if ((r = enq_iv_loops(h, false, s == "VF_divergenceFreeSolver"))) return r;
+        h->ep_acc = h->ep_loop = h->sorts;
     } else if (s == "wc_computeForce") {
         if (h->in_staging) { h->err = "run neighbourSearch first"; return SPHGPU_EINVAL; }
         const bool surf = h->P.th_h != 0.f || h->P.th_r != 0.f || h->P.th_bt != 0.f;
         if (surf) launch_wc_normal(d, h->c, h->cap, st);
         launch_wc_force(d, h->c, h->cap, st, surf);
+        h->ep_acc = h->sorts;
         h->in_staging = true;
         h->ns_valid = false;
     } else {

@@ -3,8 +3,9 @@ the C ABI) against the CPU oracle (the restatement pinned bit for bit to the
 compiled reference by tests/test_oracle.py) on the same seeded inputs.
 
 * 1,000,000-particle DFSPH dam break (100^3 block, r = 0.01 m, 4 x 2 x 2 m
-  box): cell ids and neighbour sets bit-exact, rho and alpha within 1e-5 per
-  element -- from the seeded lattice and from a settled state (300 GPU steps
+  box): cell ids and neighbour sets bit-exact, rho within 1e-5 per element,
+  alpha within 1e-5 or 8 times the float oracle's own error against its
+  FP64 build, per element -- from the seeded lattice and from a settled state (300 GPU steps
   into the collapse); from the settled state also the non-pressure forces,
   the density solver with a pinned iteration count, and one whole step.
   Reference: SphBase.cpp:849-1089 (grid, neighbour search), DFSPH.cpp:84-193
@@ -99,7 +100,28 @@ def _check_ns(sc, **kw):
     assert pairs > 25 * sc.n_fluid
     assert elem_rel(g.get_boundary("volume"), o.get_solid("volume")) < 1e-6
     assert elem_rel(g.get("density"), o.get("density")) < RTOL
-    assert elem_rel(g.get("DFalpha"), o.get("DFalpha")) < RTOL
+    # alpha = rho / (|sum m gradW|^2 + sum |m gradW|^2): where few neighbours
+    # sit near the cut, (2 - q)^2 turns an ulp of q into a large relative
+    # error of the gradient, in the float reference as on the GPU.  Per
+    # particle, the GPU's distance from the FP64 oracle is held to 1e-5 or to
+    # 8 times the float oracle's own distance from it, whichever is larger.
+    from oracle import make_scene_oracle
+    from helpers import GPU_ONLY
+    p = dict(COMMON)
+    p.update(kw)
+    od = make_scene_oracle(sc, f64=True, **{k: v for k, v in p.items() if k not in GPU_ONLY})
+    for st in ("neighbourSearch", "updateSolidPartWeight", "DF_constantDensitySolverFirst"):
+        od.stage(st)
+    a64 = od.get("DFalpha")
+    od.close()
+    assert np.all(a64 > 0)
+    ag, a32 = g.get("DFalpha").astype(np.float64), o.get("DFalpha")
+    r_gpu = np.abs(ag - a64) / np.abs(a64)
+    r_f32 = np.abs(a32 - a64) / np.abs(a64)
+    worst = int(np.argmax(r_gpu / np.maximum(RTOL, 8 * r_f32)))
+    print("alpha: max rel gpu %.3e, f32 %.3e; worst particle %d: gpu %.3e f32 %.3e, %d neighbours"
+          % (r_gpu.max(), r_f32.max(), worst, r_gpu[worst], r_f32[worst], g.neighbours()[0][worst]))
+    assert np.all(r_gpu <= np.maximum(RTOL, 8 * r_f32))
     g.close()
     o.close()
 
