@@ -104,7 +104,8 @@ def test_divergence_free_solver_from_shared_state():
 @pytest.mark.parametrize("cfl", [0, 1])
 def test_dfsph_steps_from_shared_state(cfl):
     """Each step starts both paths from the same state (the GPU's), then
-    compares.  When the FP64 error sums of the two paths land on different
+    compares -- the state after the step, and the non-pressure acceleration
+    and rho_adv, which the step computes before its re-sort.  When the FP64 error sums of the two paths land on different
     sides of the goal, the iteration counts differ by one and the fields are
     compared at the size of one Jacobi correction instead."""
     sc, g, o = make_pair(cfl=cfl)
@@ -123,6 +124,9 @@ def test_dfsph_steps_from_shared_state(cfl):
         assert elem_rel(g.get("density"), o.get("density")) < tol, k
         assert rel_err(g.get("velocity"), o.get("velocity")) < tol * 10, k
         assert rel_err(g.get("position"), o.get("position"), scale=1.0) < 1e-6, k
+        # written before the step's re-sort, read back in reference order
+        assert rel_err(g.get("acce_adv"), o.get("acce_adv")) < RTOL, k
+        assert elem_rel(g.get("density_adv"), o.get("density_adv")) < tol, k
     assert same >= 3
 
 
