@@ -69,6 +69,13 @@ struct sphgpu_scene {
     SphParams P;
     int device = 0;
     cudaStream_t stream = nullptr, stream2 = nullptr;
+    // host-buffer step: the integrated positions leave on stream3 while the
+    // neighbour search and the divergence loop run (sphgpu_step_host)
+    cudaStream_t stream3 = nullptr;
+    cudaEvent_t ev_out[2] = {nullptr, nullptr};
+    float* out_xyz = nullptr;
+    int out_n = 0;
+    bool out_xyz_done = false;
     int cap = 0, stride = 0, ncap = 48;
     GridGeom g{};
     SolverConst c{};
@@ -796,6 +803,13 @@ int graph_for(sphgpu_scene* h, int key, cudaGraphExec_t* out, int (*build)(sphgp
 
 int df_graph_build(sphgpu_scene* h, bool cap) { return enq_df_step(h, cap); }
 int df1_graph_build(sphgpu_scene* h, bool cap) { return enq_df_part1(h, cap); }
+// part 1 and the positions the integration will write, in reference order
+// (d.aux4 as 3 floats per particle), for a host-buffer step
+int df1o_graph_build(sphgpu_scene* h, bool cap) {
+    int r = enq_df_part1(h, cap);
+    if (!r) launch_integrated_to_ref(h->d, h->cap, (float*)h->d.aux4, h->stream);
+    return r;
+}
 int df2_graph_build(sphgpu_scene* h, bool cap) { return enq_df_part2(h, cap); }
 
 // SphWithBullet::updateSolids' exchange with the rigid-body world: the
@@ -903,7 +917,8 @@ int enq_steps(sphgpu_scene* h, int solver, int nsteps) {
         for (int s = 0; s < nsteps; ++s) {
             if (h->use_graphs && !h->prof.on) {
                 cudaGraphExec_t ex;
-                const int key = solver == SPHGPU_PCISPH ? 100 : (solver == SPHGPU_IISPH_M ? 200 : 300);
+                // DFSPH keys use bits 0-8; these sit above them
+                const int key = (solver == SPHGPU_PCISPH ? 1 : (solver == SPHGPU_IISPH_M ? 2 : 3)) << 12;
                 int r = graph_for(h, key, &ex,
                                   solver == SPHGPU_PCISPH ? pci_graph_build
                                                           : (solver == SPHGPU_IISPH_M ? ii_graph_build : iv_graph_build));
@@ -940,7 +955,23 @@ int enq_steps(sphgpu_scene* h, int solver, int nsteps) {
         for (int s = 0; s < nsteps; ++s) {
             const int key = (h->mlp ? h->ws_mode : 0) | (h->record_ksum ? 4 : 0) | (h->P.cfl ? 8 : 0) |
                             (h->P.enable_vortex << 6);
-            if (h->use_graphs && !h->prof.on) {
+            if (h->out_xyz && nsteps == 1 && !dyn && h->use_graphs && !h->prof.on) {
+                // the step as two graphs with the output of the integrated
+                // positions between them, on stream3, joined at the end
+                cudaGraphExec_t ex1, ex2;
+                int r = graph_for(h, key | 16 | 256, &ex1, df1o_graph_build);
+                if (!r) r = graph_for(h, key | 32, &ex2, df2_graph_build);
+                if (r) return r;
+                CK(cudaGraphLaunch(ex1, h->stream));
+                CK(cudaEventRecord(h->ev_out[0], h->stream));
+                CK(cudaStreamWaitEvent(h->stream3, h->ev_out[0], 0));
+                CK(cudaMemcpyAsync(h->out_xyz, h->d.aux4, sizeof(float) * 3 * (size_t)h->out_n,
+                                   cudaMemcpyDeviceToHost, h->stream3));
+                CK(cudaEventRecord(h->ev_out[1], h->stream3));
+                CK(cudaGraphLaunch(ex2, h->stream));
+                CK(cudaStreamWaitEvent(h->stream, h->ev_out[1], 0));
+                h->out_xyz_done = true;
+            } else if (h->use_graphs && !h->prof.on) {
                 cudaGraphExec_t ex;
                 int r = dyn ? graph_for(h, key | 16, &ex, df1_graph_build) : graph_for(h, key, &ex, df_graph_build);
                 if (r) return r;
@@ -1174,7 +1205,10 @@ static int create_impl(const SphParams* p, int device, int max_fluid, int nscene
         return SPHGPU_ECUDA;
     }
     if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&h->stream2, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaStreamCreateWithFlags(&h->stream2, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&h->stream3, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_out[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_out[1], cudaEventDisableTiming) != cudaSuccess) {
         delete h;
         return SPHGPU_ECUDA;
     }
@@ -1253,8 +1287,12 @@ int sphgpu_destroy(sphgpu_t h) {
     cudaSetDevice(h->device);
     cudaStreamSynchronize(h->stream);
     free_scene(h);
+    cudaStreamSynchronize(h->stream3);
     cudaStreamDestroy(h->stream);
     cudaStreamDestroy(h->stream2);
+    cudaStreamDestroy(h->stream3);
+    cudaEventDestroy(h->ev_out[0]);
+    cudaEventDestroy(h->ev_out[1]);
     delete h;
     return 0;
 }
@@ -1566,8 +1604,27 @@ int sphgpu_step_host(sphgpu_t h, int solver, const float* xyz, const float* vel,
         if (xyz && (r = sphgpu_set_fluid(h, "position", xyz)) < 0) return r;
         if (vel && (r = sphgpu_set_fluid(h, "velocity", vel)) < 0) return r;
     }
-    r = sphgpu_step(h, solver, 1, stats);
+    // With both outputs wanted and nothing removed so far, a graph-run DFSPH
+    // step copies the integrated positions out (in reference order) while
+    // its neighbour search and divergence loop run, and the velocities are
+    // reordered and queued behind the step before the host waits.
+    const int n0 = h->h_stats->n_active;
+    const bool overlap = fast && xyz_out && vel_out && !h->in_staging;
+    h->out_xyz = overlap ? xyz_out : nullptr;
+    h->out_n = n0;
+    h->out_xyz_done = false;
+    r = sphgpu_step_async(h, solver, 1);
+    h->out_xyz = nullptr;
+    if (r) return r;
+    float* tv = (float*)h->d.vadv;
+    if (h->out_xyz_done) {
+        launch_to_ref_order(h->d.vel, h->d.gid, n0, tv, h->stream);
+        CK(cudaMemcpyAsync(vel_out, tv, sizeof(float) * 3 * (size_t)n0, cudaMemcpyDeviceToHost, h->stream));
+    }
+    r = sphgpu_synchronize(h, stats);
+    if (stats) stats->steps = 1;
     if (r && r != SPHGPU_EMAXITER) return r;
+    if (h->out_xyz_done && h->total_removed == 0) return r;
     int r2 = 0;
     if (h->total_removed == 0 && xyz_out && vel_out) {
         // both outputs reordered on the device, copied out back to back
@@ -1575,7 +1632,6 @@ int sphgpu_step_host(sphgpu_t h, int solver, const float* xyz, const float* vel,
         const int n = h->h_stats->n_active;
         const bool stg = h->in_staging;
         float* tx = (float*)d.aux4;
-        float* tv = (float*)d.vadv;
         launch_to_ref_order(stg ? d.pos_s : d.pos, stg ? d.gid_s : d.gid, n, tx, h->stream);
         launch_to_ref_order(stg ? d.vel_s : d.vel, stg ? d.gid_s : d.gid, n, tv, h->stream);
         CK(cudaMemcpyAsync(xyz_out, tx, sizeof(float) * 3 * (size_t)n, cudaMemcpyDeviceToHost, h->stream));

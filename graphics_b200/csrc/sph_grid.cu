@@ -364,6 +364,23 @@ __global__ void k_state_in(const float* xyz3, const float* vel3, const int* gid,
     if (__syncthreads_or(diff) && threadIdx.x == 0) atomicOr(changed, 1);
 }
 
+// The positions the integration (k_hash, integrate mode) will write, in
+// the same round-to-nearest operations, scattered into reference order:
+// a host-buffer step copies them out while the rest of the step runs (the
+// divergence loop changes velocities only).
+__global__ void k_integrated_to_ref(DevScene s, float* out3) {
+    const int n = s.st->n_active;
+    const int i = blockIdx.x * NT + threadIdx.x;
+    if (i >= n) return;
+    float4 p = s.pos[i];
+    const float dt = dt_of(s, p);
+    const float4 v = s.pv[2 * i + 1];
+    const size_t g = (size_t)s.gid[i] * 3;
+    out3[g] = __fadd_rn(p.x, __fmul_rn(v.x, dt));
+    out3[g + 1] = __fadd_rn(p.y, __fmul_rn(v.y, dt));
+    out3[g + 2] = __fadd_rn(p.z, __fmul_rn(v.z, dt));
+}
+
 __global__ void k_from_ref_order(const float* src3, const int* gid, int n, float4* dst) {
     int p = blockIdx.x * NT + threadIdx.x;
     if (p >= n) return;
@@ -384,6 +401,9 @@ void launch_to_ref_order(const float4* src, const int* gid, int n, float* dst3, 
 void launch_state_in(const float* xyz3, const float* vel3, const int* gid, int n, const float4* pos, float4* vel,
                      float4* prv, int* changed, cudaStream_t st) {
     if (n > 0) k_state_in<<<nblk(n, NT), NT, 0, st>>>(xyz3, vel3, gid, n, pos, vel, prv, changed);
+}
+void launch_integrated_to_ref(const DevScene& s, int n_max, float* out3, cudaStream_t st) {
+    if (n_max > 0) k_integrated_to_ref<<<nblk(n_max, NT), NT, 0, st>>>(s, out3);
 }
 void launch_from_ref_order(const float* src3, const int* gid, int n, float4* dst, cudaStream_t st) {
     if (n > 0) k_from_ref_order<<<nblk(n, NT), NT, 0, st>>>(src3, gid, n, dst);

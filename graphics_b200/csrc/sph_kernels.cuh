@@ -180,6 +180,7 @@ void launch_count_active(const DevScene& s, const GridGeom& g, cudaStream_t st);
 void launch_build(const DevScene& s, const GridGeom& g, const SolverConst& c, int mode, int n_max, cudaStream_t st,
                   int bs = 128);
 void launch_to_ref_order(const float4* src, const int* gid, int n, float* dst3, cudaStream_t st);
+void launch_integrated_to_ref(const DevScene& s, int n_max, float* out3, cudaStream_t st);
 void launch_from_ref_order(const float* src3, const int* gid, int n, float4* dst, cudaStream_t st);
 // host state (reference order) into a sorted state with valid lists:
 // velocities copied in, *changed set when a position differs

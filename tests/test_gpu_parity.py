@@ -271,3 +271,25 @@ def test_step_host_matches_device_steps():
         np.testing.assert_array_equal(po, ref.get("position"))
         np.testing.assert_array_equal(vo, ref.get("velocity"))
         pos, vel = po.copy(), vo.copy()
+
+
+def test_step_host_removal_during_step():
+    """A host-buffer step whose integration carries particles out of the
+    domain: the positions copied out while the step runs include them, so
+    the outputs are read again after the step -- the survivors, in
+    reference order, bit for bit as the device path gives them."""
+    sc, g, o = make_pair(cfl=0, dt=1e-3)
+    sc2, ref, o2 = make_pair(cfl=0, dt=1e-3)
+    g.step("dfsph", 2)
+    ref.step("dfsph", 2)
+    pos, vel = g.get("position"), g.get("velocity")
+    vel = vel.copy()
+    vel[5] = (1.0e4, 0.0, 0.0)
+    ref.set("velocity", vel)
+    po, vo = np.zeros_like(pos), np.zeros_like(vel)
+    st = g.step_host("dfsph", pos, vel, po, vo)
+    ref.step("dfsph", 1)
+    m = ref.n_fluid  # the fast particle's neighbours may follow it out
+    assert m < len(pos) and g.n_fluid == m and st["removed"] == len(pos) - m
+    np.testing.assert_array_equal(po[:m], ref.get("position"))
+    np.testing.assert_array_equal(vo[:m], ref.get("velocity"))
