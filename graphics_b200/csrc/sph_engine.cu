@@ -2696,6 +2696,14 @@ int sphgpu_debug_set(sphgpu_t h, const char* key, int value) {
     std::string k(key);
     if (k == "record_kappa_sum") { h->record_ksum = value; invalidate_graphs(h); return 0; }
     if (k == "use_graphs") { h->use_graphs = value != 0; return 0; }
+    if (k == "carveout_sweeps" || k == "carveout_build") {
+        // measurement knob: the kernels' preferred L1/shared split
+        cudaSetDevice(h->device);
+        if (k == "carveout_sweeps") set_sweep_carveout(value);
+        else set_build_carveout(value);
+        invalidate_graphs(h);
+        return cudaPeekAtLastError() == cudaSuccess ? 0 : SPHGPU_ECUDA;
+    }
     if (k == "reset_kappa_sum") {
         cudaMemsetAsync(h->d.ksum, 0, sizeof(float) * h->cap, h->stream);
         return cudaStreamSynchronize(h->stream) == cudaSuccess ? 0 : SPHGPU_ECUDA;

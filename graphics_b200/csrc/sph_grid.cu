@@ -449,6 +449,21 @@ static void launch_build_bs(const DevScene& s, const GridGeom& g, const SolverCo
     else launch_build_st<BS, false>(s, g, c, mode, nb, st);
 }
 
+template <int BS>
+static void build_carveout_bs(int pct) {
+    const cudaFuncAttribute a = cudaFuncAttributePreferredSharedMemoryCarveout;
+    cudaFuncSetAttribute(k_build<1, BS, true>, a, pct);
+    cudaFuncSetAttribute(k_build<1, BS, false>, a, pct);
+}
+// preferred shared-memory carveout of the DFSPH list build (percent; -1 =
+// the driver's choice): the staged rows take shared memory from the L1 that
+// caches the candidates' records
+void set_build_carveout(int pct) {
+    build_carveout_bs<64>(pct);
+    build_carveout_bs<128>(pct);
+    build_carveout_bs<256>(pct);
+}
+
 void launch_build(const DevScene& s, const GridGeom& g, const SolverConst& c, int mode, int n_max, cudaStream_t st,
                   int bs) {
     if (bs == 64) launch_build_bs<64>(s, g, c, mode, n_max, st);
