@@ -197,7 +197,11 @@ int sphgpu_synchronize(sphgpu_t h, SphStepStats* stats);
  * When the device state ended a DFSPH step (lists valid, no particle ever
  * removed), the upload is compared with it on the device: velocities are
  * taken as given, and the neighbour search runs again only if a position
- * differs -- handing back the previous output costs the transfers only. */
+ * differs -- handing back the previous output costs the transfers only.  In
+ * that case, with graphs on, the positions the step's integration produces
+ * are copied into xyz_out while its neighbour search and divergence loop
+ * still run (pinned xyz_out makes the copy overlap; a step that removes
+ * particles writes both outputs again afterwards). */
 int sphgpu_step_host(sphgpu_t h, int solver, const float* xyz, const float* vel, float* xyz_out,
                      float* vel_out, SphStepStats* stats);
 
