@@ -758,6 +758,20 @@ int enq_iv_step(sphgpu_scene* h, bool capturing) {
     return 0;
 }
 
+// WCSPH step from the staged state: neighbour search with density and
+// pressure, (surface normals,) forces and the integration into staging
+int enq_wc_step(sphgpu_scene* h, bool) {
+    cudaStream_t st = h->stream;
+    launch_step_begin(h->d, st);
+    enq_ns(h, 0, 2, st);
+    const bool surf = h->P.th_h != 0.f || h->P.th_r != 0.f || h->P.th_bt != 0.f;
+    if (surf) launch(h, "wc_normal", st, [&] { launch_wc_normal(h->d, h->c, h->cap, st); });
+    launch(h, "wc_force", st, [&] { launch_wc_force(h->d, h->c, h->cap, st, surf); });
+    CK(cudaMemcpyAsync(h->h_stats, h->d.st, sizeof(DevStats), cudaMemcpyDeviceToHost, st));
+    return 0;
+}
+
+int wc_graph_build(sphgpu_scene* h, bool cap) { return enq_wc_step(h, cap); }
 int pci_graph_build(sphgpu_scene* h, bool cap) { return enq_pci_step(h, cap); }
 int ii_graph_build(sphgpu_scene* h, bool cap) { return enq_ii_step(h, cap); }
 int iv_graph_build(sphgpu_scene* h, bool cap) { return enq_iv_step(h, cap); }
@@ -1004,19 +1018,23 @@ int enq_steps(sphgpu_scene* h, int solver, int nsteps) {
         }
         return 0;
     }
-    // WCSPH: NS + density/pressure (fused), forces + integrate into staging
+    // WCSPH: NS + density/pressure (fused), forces + integrate into staging;
+    // one graph per step (at 27 k particles the step is launch-bound)
     for (int s = 0; s < nsteps; ++s) {
         if (!h->in_staging) stage_from_sorted(h, h->cap);
-        launch_step_begin(h->d, h->stream);
-        enq_ns(h, 0, 2, h->stream);
-        const bool surf = h->P.th_h != 0.f || h->P.th_r != 0.f || h->P.th_bt != 0.f;
-        if (surf) launch(h, "wc_normal", h->stream, [&] { launch_wc_normal(h->d, h->c, h->cap, h->stream); });
-        launch(h, "wc_force", h->stream, [&] { launch_wc_force(h->d, h->c, h->cap, h->stream, surf); });
+        if (h->use_graphs && !h->prof.on) {
+            cudaGraphExec_t ex;
+            int r = graph_for(h, 4 << 12, &ex, wc_graph_build);
+            if (r) return r;
+            CK(cudaGraphLaunch(ex, h->stream));
+        } else {
+            int r = enq_wc_step(h, false);
+            if (r) return r;
+            prof_collect(h);
+        }
         h->ep_acc = h->ep_loop = ++h->sorts;
         h->in_staging = true;
         h->ns_valid = false;
-        CK(cudaMemcpyAsync(h->h_stats, h->d.st, sizeof(DevStats), cudaMemcpyDeviceToHost, h->stream));
-        prof_collect(h);
         h->frame++;
     }
     return 0;

@@ -162,6 +162,19 @@ def test_graph_and_host_loops_identical_and_deterministic():
         np.testing.assert_array_equal(a, b)
 
 
+def test_wcsph_graph_and_host_steps_identical():
+    """The WCSPH step as one CUDA graph per step and launched from the host
+    give the same state bit for bit."""
+    out = []
+    for graphs in (1, 0):
+        sc, g, o = make_pair(visc_alpha=0.01, boundary_visc=0.01, dt=2.5e-4, soundSpeed_cs=18.708287)
+        g.debug_set("use_graphs", graphs)
+        g.step("wcsph", 6)
+        out.append((g.get("position"), g.get("velocity"), g.get("density"), g.get("acceleration")))
+    for a, b in zip(out[0], out[1]):
+        np.testing.assert_array_equal(a, b)
+
+
 def test_wcsph_pressure_force_and_steps():
     kw = dict(dt=2.5e-4, soundSpeed_cs=18.708287)
     sc, g, o = make_pair(visc_alpha=0.01, boundary_visc=0.01, **kw)
