@@ -57,6 +57,8 @@ ALG_BYTES = {
     "df_div_b": lambda nb: 16 + 4 + 4 + 32 + 4 * nb,
     "df_forces": lambda nb: 32 + 4 * nb + 16,
     "build_first": lambda nb: (16 + 4 + 4 * nb) + (16 + 4 * nb + 8),
+    # the list build with rho/alpha and the divergence loop's first sweep A
+    "build_first_div": lambda nb: (16 + 4 + 4 * nb) + (16 + 4 * nb + 8) + (16 + 16 + 4 + 4 * nb + 4),
     "hash": lambda nb: 24 + 64,
     "reorder": lambda nb: 32 + 80,
     # IISph (volume form) loop sweeps (not in the byte model; own compulsory
@@ -658,7 +660,7 @@ def profile_kernels(g, args, hbm, peak_kind, sc):
             "alg_bytes_per_particle": round(ALG_BYTES[dom](nb), 1), "mean_neighbours": round(nb, 2)}
     # neighbour + density kernels (hash with integration, cell ranges,
     # counting sort + reindex, list build with rho/alpha)
-    ns_keys = [k for k in ("hash", "scan", "reorder", "build_first") if k in full]
+    ns_keys = [k for k in ("hash", "scan", "reorder", "build_first", "build_first_div") if k in full]
     ns_s = sum(full[k][0] for k in ns_keys) / 1e3
     ns_bytes = sum(full[k][1] for k in ns_keys)
     roof["neighbour_density_group"] = {"kernels": ns_keys, "us_per_step": round(ns_s * 1e6, 1),

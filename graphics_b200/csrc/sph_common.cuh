@@ -65,6 +65,9 @@ struct SolverConst {
     float ws_scale;    // applied fraction of the predicted warm-start stiffness
     int cap;           // neighbour cap
     int stride;        // ELL column stride (>= fluid capacity)
+    int l2pol;         // L2 eviction priority of the sweeps' loads: bits 0-1 the
+                       // neighbour lists, bits 2-3 the gathered records
+                       // (0 normal, 1 evict first, 2 evict last)
     // IISph (volume form, IISph.cpp): spline of the per-pair h = (d_a + d_b)/2
     // (= d, one diameter for all particles), rest volume d^3, per-phase mass
     // rho0 * beta * d^3 (beta = 1), kinematic viscosity of fluid / boundary
@@ -171,6 +174,29 @@ __device__ __forceinline__ void ld_record32(const float4* p, float4& a, float4& 
                  : "l"(p));
 }
 
+// L2 cache policy (createpolicy) of the given eviction priority: 0 normal,
+// 1 evict first, 2 evict last
+__device__ __forceinline__ unsigned long long l2_policy(int pri) {
+    unsigned long long p;
+    if (pri == 1) asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    else if (pri == 2) asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    else asm("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+// the 32-byte record load under an L2 cache policy
+__device__ __forceinline__ void ld_record32_pol(const float4* p, float4& a, float4& b, unsigned long long pol) {
+    asm volatile("ld.global.nc.L2::cache_hint.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8], %9;"
+                 : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
+                 : "l"(p), "l"(pol));
+}
+__device__ __forceinline__ float4 ld_f4_pol(const float4* p, unsigned long long pol) {
+    float4 a;
+    asm volatile("ld.global.nc.L2::cache_hint.v4.f32 {%0,%1,%2,%3}, [%4], %5;"
+                 : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w)
+                 : "l"(p), "l"(pol));
+    return a;
+}
+
 // ELL4 addressing (see the layout note at the top)
 __device__ __forceinline__ size_t ell_index(size_t stride, int p, int k) {
     return ((size_t)(k >> 2) * stride + (size_t)p) * 4 + (k & 3);
@@ -178,6 +204,15 @@ __device__ __forceinline__ size_t ell_index(size_t stride, int p, int k) {
 __device__ __forceinline__ int ell_get(const int* L, size_t stride, int p, int k) { return L[ell_index(stride, p, k)]; }
 __device__ __forceinline__ int4 ell_group(const int* L, size_t stride, int p, int g) {
     return __ldg(reinterpret_cast<const int4*>(L) + (size_t)g * stride + p);
+}
+// one group under an L2 cache policy
+__device__ __forceinline__ int4 ell_group_pol(const int* L, size_t stride, int p, int g, unsigned long long pol) {
+    int4 v;
+    const int4* a = reinterpret_cast<const int4*>(L) + (size_t)g * stride + p;
+    asm volatile("ld.global.nc.L2::cache_hint.v4.s32 {%0,%1,%2,%3}, [%4], %5;"
+                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+                 : "l"(a), "l"(pol));
+    return v;
 }
 
 // ---- reductions ----

@@ -27,31 +27,6 @@
 namespace {
 constexpr int NT = 128;
 
-// last-block FP64 reduction of per-block partials; returns true in the
-// thread that holds the total (thread 0 of the last block).
-template <int BS>
-__device__ __forceinline__ bool finish_sum(double* partial, unsigned* ticket, double v, double* total) {
-    __shared__ bool last;
-    if (threadIdx.x == 0) {
-        partial[blockIdx.x] = v;
-        __threadfence();
-        unsigned t = atomicAdd(ticket, 1u);
-        last = (t == gridDim.x - 1);
-    }
-    __syncthreads();
-    if (!last) return false;
-    __threadfence();
-    __shared__ double sh[BS / 32];
-    double acc = 0;
-    for (int i = threadIdx.x; i < (int)gridDim.x; i += BS) acc += ((volatile double*)partial)[i];
-    double tot = block_sum_double<BS>(acc, sh);
-    if (threadIdx.x == 0) {
-        *total = tot;
-        *ticket = 0u;
-    }
-    return threadIdx.x == 0;
-}
-
 // per-step counters (the last step's values are reported)
 __global__ void k_step_begin(DevScene s) {
     DevStats* st = s.st;
@@ -168,11 +143,12 @@ __device__ __forceinline__ float div_sweep(const DevScene& s, const SolverConst&
     const int cnt = s.ncount[p];
     const int ng = (cnt + 3) >> 2;
     const size_t stride = (size_t)c.stride;
+    const unsigned long long polL = l2_policy(c.l2pol & 3), polR = l2_policy((c.l2pol >> 2) & 3);
     float acc = 0.f;
-    int4 nxt = ng ? ell_group(s.nbr, stride, p, 0) : make_int4(0, 0, 0, 0);
+    int4 nxt = ng ? ell_group_pol(s.nbr, stride, p, 0, polL) : make_int4(0, 0, 0, 0);
     for (int gi = 0; gi < ng; ++gi) {
         const int4 cur = nxt;
-        if (gi + 1 < ng) nxt = ell_group(s.nbr, stride, p, gi + 1);
+        if (gi + 1 < ng) nxt = ell_group_pol(s.nbr, stride, p, gi + 1, polL);
         const unsigned e[4] = {(unsigned)cur.x, (unsigned)cur.y, (unsigned)cur.z, (unsigned)cur.w};
         float4 pb[4], vb[4];
         bool ok[4], bnd[4];
@@ -182,15 +158,11 @@ __device__ __forceinline__ float div_sweep(const DevScene& s, const SolverConst&
             const unsigned u = ok[t] ? e[t] : (unsigned)p;
             bnd[t] = (u & BND_FLAG) != 0u;
             const float4* rec = (bnd[t] ? s.bpv : s.pv) + 2 * (size_t)(u & BND_MASK);
-            ld_record32(rec, pb[t], vb[t]);
+            ld_record32_pol(rec, pb[t], vb[t], polR);
         }
 #pragma unroll
         for (int t = 0; t < 4; ++t) {
-            const float m = bnd[t] ? c.rho0 * pb[t].w : c.fm0;
-            const float xx = pa.x - pb[t].x, xy = pa.y - pb[t].y, xz = pa.z - pb[t].z;
-            const float f = grad_over_r(c.k, xx * xx + xy * xy + xz * xz);
-            const float dot = xx * (va.x - vb[t].x) + xy * (va.y - vb[t].y) + xz * (va.z - vb[t].z);
-            const float nacc = fmaf(dot * f, m, acc);
+            const float nacc = div_term(c, pa, va, pb[t], vb[t], bnd[t], acc);
             acc = ok[t] ? nacc : acc;
         }
     }
@@ -249,10 +221,11 @@ __global__ void __launch_bounds__(BS) k_df_vupdate(DevScene s, SolverConst c, do
         const int cnt = s.ncount[p];
         const int ng = (cnt + 3) >> 2;
         const size_t stride = (size_t)c.stride;
-        int4 nxt = ng ? ell_group(s.nbr, stride, p, 0) : make_int4(0, 0, 0, 0);
+        const unsigned long long polL = l2_policy(c.l2pol & 3), polR = l2_policy((c.l2pol >> 2) & 3);
+        int4 nxt = ng ? ell_group_pol(s.nbr, stride, p, 0, polL) : make_int4(0, 0, 0, 0);
         for (int gi = 0; gi < ng; ++gi) {
             const int4 cur = nxt;
-            if (gi + 1 < ng) nxt = ell_group(s.nbr, stride, p, gi + 1);
+            if (gi + 1 < ng) nxt = ell_group_pol(s.nbr, stride, p, gi + 1, polL);
             const unsigned e[4] = {(unsigned)cur.x, (unsigned)cur.y, (unsigned)cur.z, (unsigned)cur.w};
             float4 pb[4];
             bool ok[4], bnd[4];
@@ -262,7 +235,7 @@ __global__ void __launch_bounds__(BS) k_df_vupdate(DevScene s, SolverConst c, do
                 const unsigned u = ok[t] ? e[t] : (unsigned)p;
                 bnd[t] = (u & BND_FLAG) != 0u;
                 const unsigned j = u & BND_MASK;
-                pb[t] = __ldg(bnd[t] ? s.bpv + 2 * (size_t)j : s.pk + j);
+                pb[t] = ld_f4_pol(bnd[t] ? s.bpv + 2 * (size_t)j : s.pk + j, polR);
             }
 #pragma unroll
             for (int t = 0; t < 4; ++t) {

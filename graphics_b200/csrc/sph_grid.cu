@@ -128,7 +128,13 @@ constexpr int LROW = 52;
 // mode 0: neighbour lists only; 1: + DFSPH rho and alpha
 // (DF_constantDensitySolverFirst, DFSPH.cpp:84-193); 2: + WCSPH rho and Tait
 // pressure (WcSph::wc_computePressure, WcSph.cpp:99-153); 3: + IISph
-// sphDensity, gamma, sphVolume and alpha (IISph.cpp:100-402).
+// sphDensity, gamma, sphVolume and alpha (IISph.cpp:100-402); 4: mode 1 and,
+// over the same list in the same pass, the first sweep A of the divergence
+// loop that follows the neighbour search (DFSPH.cpp:795-835: Drho/Dt, its
+// clamp, kappa_v, the FP64 error sum) -- every neighbour's 32-byte
+// {position, velocity} record is gathered once for both, and the loop then
+// starts with its velocity update (the per-pair term is div_term, the one the
+// separate sweep uses, so the results are the same bit for bit).
 //
 // STAGED (cap <= 48): a kept neighbour is one predicated shared-memory store
 // into the thread's row -- no divergent branch around a global store in the
@@ -142,6 +148,7 @@ __global__ void __launch_bounds__(BS) k_build(DevScene s, GridGeom g, SolverCons
     const int n = s.st->n_active;
     const int p = blockIdx.x * BS + threadIdx.x;
     int cnt = 0, over = 0;
+    double ddiv = 0.0;  // MODE 4: this particle's Drho/Dt for the FP64 error
     const bool act = p < n;
     if (act) {
         const float4 pa = s.pos[p];
@@ -242,17 +249,24 @@ __global__ void __launch_bounds__(BS) k_build(DevScene s, GridGeom g, SolverCons
             // phase 2: rho and alpha over the stored list (all lanes busy)
             float density = ker_W(c.k, 0.f) * fm0;
             float a1x = 0.f, a1y = 0.f, a1z = 0.f, a2 = 0.f;
+            float dacc = 0.f;  // MODE 4: the divergence sum
+            const float4 va = MODE == 4 ? s.pv[2 * p + 1] : make_float4(0.f, 0.f, 0.f, 0.f);
             for (int k = 0; k < cnt; ++k) {
                 const unsigned e = STAGED ? (unsigned)row[k] : (unsigned)out[ell_index(stride, p, k)];
                 const bool bnd = (e & BND_FLAG) != 0u;
-                const float4 pb = __ldg((bnd ? BP : P) + (e & BND_MASK));
+                float4 pb, vb;
+                // pv / bpv hold {the position (boundary: with its volume) of
+                // pos / bpos, the velocity}
+                if (MODE == 4) ld_record32((bnd ? s.bpv : s.pv) + 2 * (size_t)(e & BND_MASK), pb, vb);
+                else pb = __ldg((bnd ? BP : P) + (e & BND_MASK));
+                if (MODE == 4) dacc = div_term(c, pa, va, pb, vb, bnd, dacc);
                 const float xx = pa.x - pb.x, xy = pa.y - pb.y, xz = pa.z - pb.z;
                 const float len2 = dis_square_rn(pa.x, pa.y, pa.z, pb.x, pb.y, pb.z);
                 float w, f;
                 kernel_pair(c.k, len2, w, f);
                 const float m = bnd ? rho0 * pb.w : fm0;
                 density = fmaf(m, w, density);
-                if (MODE == 1) {
+                if (MODE == 1 || MODE == 4) {
                     const float fm = f * m;
                     a1x = fmaf(xx, fm, a1x);
                     a1y = fmaf(xy, fm, a1y);
@@ -261,12 +275,24 @@ __global__ void __launch_bounds__(BS) k_build(DevScene s, GridGeom g, SolverCons
                     a2 = fmaf(t, t, a2);
                 }
             }
-            if (MODE == 1) {
+            if (MODE == 1 || MODE == 4) {
                 s.rho[p] = density;
                 s.prv[2 * p] = make_float4(pa.x, pa.y, pa.z, density);
                 float al = a1x * a1x + a1y * a1y + a1z * a1z + a2;
                 if (al < 1.0e-6f) al = 1.0e-6f;
-                s.alpha[p] = density / al;
+                const float alpha = density / al;
+                s.alpha[p] = alpha;
+                if (MODE == 4) {
+                    // the divergence loop's first sweep A, as k_df_div_a
+                    const float dt = *s.dt;
+                    float dd = dacc;
+                    if (dd < 0.f || (density + dd * dt) < c.rho0) dd = 0.f;  // DFSPH.cpp:829-832
+                    const float kv = dd * alpha / dt;                         // DFSPH.cpp:835
+                    s.pk[p] = make_float4(pa.x, pa.y, pa.z, kv / density);
+                    s.kappav[p] = kv;
+                    s.aux1[p] = dd;
+                    ddiv = (double)dd;
+                }
             } else {
                 s.rho[p] = density;
                 // Tait, WcSph.cpp:142-146 (NEGLECT_NEGATIVE_PRESSURE)
@@ -284,6 +310,13 @@ __global__ void __launch_bounds__(BS) k_build(DevScene s, GridGeom g, SolverCons
         if (tot) atomicAdd(&s.st->nbr_total, (unsigned long long)tot);
         if (ov) { atomicAdd(&s.st->overflow, ov); atomicOr(&s.st->status, 8u); }
         if (mx) atomicMax(&s.st->max_nbrs, mx);
+    }
+    if (MODE == 4) {
+        // mean Drho/Dt of the iteration (k_df_div_a's FP64 error)
+        __shared__ double shd[BS / 32];
+        const double bsum = block_sum_double<BS>(ddiv, shd);
+        double t;
+        if (finish_sum<BS>(s.partial, &s.st->ticket[1], bsum, &t)) s.st->err_div = n > 0 ? t / (double)n : 0.0;
     }
 }
 
@@ -436,6 +469,7 @@ static void launch_build_st(const DevScene& s, const GridGeom& g, const SolverCo
     if (mode == 0) k_build<0, BS, STAGED><<<nb, BS, sm, st>>>(s, g, c);
     else if (mode == 1) k_build<1, BS, STAGED><<<nb, BS, sm, st>>>(s, g, c);
     else if (mode == 2) k_build<2, BS, STAGED><<<nb, BS, sm, st>>>(s, g, c);
+    else if (mode == 4) k_build<4, BS, STAGED><<<nb, BS, sm, st>>>(s, g, c);
     else k_build<3, BS, STAGED><<<nb, BS, sm, st>>>(s, g, c);
 }
 
@@ -454,6 +488,8 @@ static void build_carveout_bs(int pct) {
     const cudaFuncAttribute a = cudaFuncAttributePreferredSharedMemoryCarveout;
     cudaFuncSetAttribute(k_build<1, BS, true>, a, pct);
     cudaFuncSetAttribute(k_build<1, BS, false>, a, pct);
+    cudaFuncSetAttribute(k_build<4, BS, true>, a, pct);
+    cudaFuncSetAttribute(k_build<4, BS, false>, a, pct);
 }
 // preferred shared-memory carveout of the DFSPH list build (percent; -1 =
 // the driver's choice): the staged rows take shared memory from the L1 that

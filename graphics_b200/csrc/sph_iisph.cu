@@ -40,29 +40,6 @@
 namespace {
 constexpr int NT = 128;
 
-template <int BS>
-__device__ __forceinline__ bool finish_sum(double* partial, unsigned* ticket, double v, double* total) {
-    __shared__ bool last;
-    if (threadIdx.x == 0) {
-        partial[blockIdx.x] = v;
-        __threadfence();
-        unsigned t = atomicAdd(ticket, 1u);
-        last = (t == gridDim.x - 1);
-    }
-    __syncthreads();
-    if (!last) return false;
-    __threadfence();
-    __shared__ double sh[BS / 32];
-    double acc = 0;
-    for (int i = threadIdx.x; i < (int)gridDim.x; i += BS) acc += ((volatile double*)partial)[i];
-    double tot = block_sum_double<BS>(acc, sh);
-    if (threadIdx.x == 0) {
-        *total = tot;
-        *ticket = 0u;
-    }
-    return threadIdx.x == 0;
-}
-
 // Boundary particle p: its neighbour list in the reference's order (27 cells,
 // per cell the fluid range then the boundary range; same-solid neighbours
 // skipped for rigid solids, SphBase.cpp:922), capped at c.cap entries of

@@ -170,13 +170,54 @@ __device__ __forceinline__ bool scene_active(const DevScene& s, float4 pa) {
     return s.nscenes <= 1 || s.b.active[scene_of(pa)] != 0;
 }
 
+// last-block FP64 reduction of per-block partials; returns true in the
+// thread that holds the total (thread 0 of the last block).  The partials
+// are summed in block order, so the total is the same from run to run.
+template <int BS>
+__device__ __forceinline__ bool finish_sum(double* partial, unsigned* ticket, double v, double* total) {
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+        partial[blockIdx.x] = v;
+        __threadfence();
+        unsigned t = atomicAdd(ticket, 1u);
+        last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return false;
+    __threadfence();
+    __shared__ double sh[BS / 32];
+    double acc = 0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += BS) acc += ((volatile double*)partial)[i];
+    double tot = block_sum_double<BS>(acc, sh);
+    if (threadIdx.x == 0) {
+        *total = tot;
+        *ticket = 0u;
+    }
+    return threadIdx.x == 0;
+}
+
+// One pair's term of the DFSPH divergence sums, m_j gradW_ij . (v_i - v_j)
+// (DFSPH.cpp:589-617, 795-825), accumulated into acc: neighbour j's record
+// {pb = (x, y, z, volume or phase), vb = loop velocity}; boundary mass
+// rho0 * volume.  The Jacobi sweeps and the list build's fused first
+// divergence sweep share it, so both round the same way.
+__device__ __forceinline__ float div_term(const SolverConst& c, float4 pa, float4 va, float4 pb, float4 vb, bool bnd,
+                                          float acc) {
+    const float m = bnd ? c.rho0 * pb.w : c.fm0;
+    const float xx = pa.x - pb.x, xy = pa.y - pb.y, xz = pa.z - pb.z;
+    const float f = grad_over_r(c.k, xx * xx + xy * xy + xz * xz);
+    const float dot = xx * (va.x - vb.x) + xy * (va.y - vb.y) + xz * (va.z - vb.z);
+    return fmaf(dot * f, m, acc);
+}
+
 // ---- neighbour search (sph_grid.cu) ----
 void launch_hash(const DevScene& s, const GridGeom& g, int integrate, int n_old, cudaStream_t st);
 // carry: bit 0 hist, bit 1 cA, bit 2 cB, bit 3 cC (staging -> sorted)
 void launch_scatter_reorder(const DevScene& s, const GridGeom& g, int n_old, int carry, cudaStream_t st);
 void launch_count_active(const DevScene& s, const GridGeom& g, cudaStream_t st);
 // mode 0: lists only; 1: lists + DFSPH rho/alpha; 2: lists + WCSPH rho/pressure;
-// 3: lists + IISph VF_prepareAttribute / sphDensity (ivs)
+// 3: lists + IISph VF_prepareAttribute / sphDensity (ivs); 4: mode 1 + the
+// divergence loop's first sweep A (Drho/Dt, kappa_v, FP64 error)
 void launch_build(const DevScene& s, const GridGeom& g, const SolverConst& c, int mode, int n_max, cudaStream_t st,
                   int bs = 128);
 void launch_to_ref_order(const float4* src, const int* gid, int n, float* dst3, cudaStream_t st);
