@@ -79,10 +79,11 @@ __global__ void __launch_bounds__(BS) k_df_forces(DevScene s, SolverConst c, int
         const int cnt = s.ncount[p];
         const int ng = (cnt + 3) >> 2;
         const size_t stride = (size_t)c.stride;
-        int4 nxt = ng ? ell_group(s.nbr, stride, p, 0) : make_int4(0, 0, 0, 0);
+        const unsigned long long polL = l2_policy(c.l2pol & 3);  // lists stream through L2
+    int4 nxt = ng ? ell_group_pol(s.nbr, stride, p, 0, polL) : make_int4(0, 0, 0, 0);
         for (int gi = 0; gi < ng; ++gi) {
             const int4 cur = nxt;
-            if (gi + 1 < ng) nxt = ell_group(s.nbr, stride, p, gi + 1);
+            if (gi + 1 < ng) nxt = ell_group_pol(s.nbr, stride, p, gi + 1, polL);
             const unsigned e[4] = {(unsigned)cur.x, (unsigned)cur.y, (unsigned)cur.z, (unsigned)cur.w};
             // one 32-byte record per neighbour: {(x, y, z, rho), v} or, for a
             // boundary particle, {(x, y, z, volume), singleVelocity + velocity}

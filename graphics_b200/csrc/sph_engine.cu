@@ -31,6 +31,8 @@ void launch_ws_features(const DevScene& s, const SolverConst& c, const MlpDev& m
 void launch_ws_infer(const DevScene& s, const SolverConst& c, const MlpDev& m, const __nv_bfloat16* xn, int n_max,
                      int sm_count, cudaStream_t st);
 void launch_ws_post(const DevScene& s, const SolverConst& c, float* yout, int n_max, cudaStream_t st);
+void launch_ws_features_infer(const DevScene& s, const SolverConst& c, const MlpDev& m, float dt_max, float alpha_ref,
+                              int n_max, int sm_count, cudaStream_t st);
 void launch_ws_append(const float* X, const float* y, int n_max, const int* n_act, int every, int* offset, float* dsX,
                       float* dsy, int* ds_count, int ds_cap, cudaStream_t st);
 
@@ -115,6 +117,7 @@ struct sphgpu_scene {
     // 1 M: density sweeps A/B 135/74 -> 129/72 us; records evict-last: no gain)
     int l2pol = 1;
     int fuse_div = 1;  // DFSPH: the list build performs the divergence loop's first sweep A
+    int fuse_ws = 1;   // warm start: features and inference in one kernel
     // learned warm start: 0 off, 1 apply the network, 2 record training data
     sphgpu_mlp* mlp = nullptr;
     int ws_mode = 0;
@@ -583,7 +586,12 @@ int enq_df_part1(sphgpu_scene* h, bool capturing) {
             launch_vortex_second(d, h->c, h->P.enable_vortex, h->P.vort_alpha, h->P.vort_zeta, h->P.vort_nu_t,
                                  h->P.spacing_r, h->cap, st);
         });
-    if (ws == 1 || ws == 3) {
+    if (ws == 1 && h->fuse_ws) {
+        launch(h, "ws_features_infer", st, [&] {
+            launch_ws_features_infer(d, h->c, h->mlp->m, h->P.dt_max, h->alpha_ref, h->cap, h->sm_count, st);
+        });
+        launch(h, "df_warm", st, [&] { launch_df_warm_correction(d, h->c, h->cap, st, h->tune.sweep_b); });
+    } else if (ws == 1 || ws == 3) {
         launch(h, "ws_features", st, [&] {
             launch_ws_features(d, h->c, h->mlp->m, ws == 1 ? 1 : 2, h->P.dt_max, h->alpha_ref, nullptr, h->xn, h->cap,
                                st);
@@ -2750,6 +2758,7 @@ int sphgpu_debug_set(sphgpu_t h, const char* key, int value) {
     if (k == "record_kappa_sum") { h->record_ksum = value; invalidate_graphs(h); return 0; }
     if (k == "use_graphs") { h->use_graphs = value != 0; return 0; }
     if (k == "fuse_div") { h->fuse_div = value != 0; invalidate_graphs(h); return 0; }
+    if (k == "fuse_ws") { h->fuse_ws = value != 0; invalidate_graphs(h); return 0; }
     if (k == "l2_policy") {
         // measurement knob: L2 eviction priorities of the sweeps' list and
         // record loads (SolverConst::l2pol)

@@ -229,10 +229,11 @@ __device__ __forceinline__ float iv_div_sum(const DevScene& s, const SolverConst
     const size_t stride = (size_t)c.stride;
     const float Vf = c.iv_V;
     float acc = 0.f;
-    int4 nxt = ng ? ell_group(s.nbr, stride, p, 0) : make_int4(0, 0, 0, 0);
+    const unsigned long long polL = l2_policy(c.l2pol & 3);  // lists stream through L2
+    int4 nxt = ng ? ell_group_pol(s.nbr, stride, p, 0, polL) : make_int4(0, 0, 0, 0);
     for (int gi = 0; gi < ng; ++gi) {
         const int4 cur = nxt;
-        if (gi + 1 < ng) nxt = ell_group(s.nbr, stride, p, gi + 1);
+        if (gi + 1 < ng) nxt = ell_group_pol(s.nbr, stride, p, gi + 1, polL);
         const unsigned e[4] = {(unsigned)cur.x, (unsigned)cur.y, (unsigned)cur.z, (unsigned)cur.w};
         float4 pb[4], vb[4];
         bool ok[4], bnd[4];
@@ -369,10 +370,11 @@ __global__ void __launch_bounds__(BS) k_iv_sweep_b(DevScene s, SolverConst c, in
             const int cnt = s.ncount[p];
             const int ng = (cnt + 3) >> 2;
             const size_t stride = (size_t)c.stride;
-            int4 nxt = ng ? ell_group(s.nbr, stride, p, 0) : make_int4(0, 0, 0, 0);
+            const unsigned long long polL = l2_policy(c.l2pol & 3);  // lists stream through L2
+    int4 nxt = ng ? ell_group_pol(s.nbr, stride, p, 0, polL) : make_int4(0, 0, 0, 0);
             for (int gi = 0; gi < ng; ++gi) {
                 const int4 cur = nxt;
-                if (gi + 1 < ng) nxt = ell_group(s.nbr, stride, p, gi + 1);
+                if (gi + 1 < ng) nxt = ell_group_pol(s.nbr, stride, p, gi + 1, polL);
                 const unsigned e[4] = {(unsigned)cur.x, (unsigned)cur.y, (unsigned)cur.z, (unsigned)cur.w};
                 float4 pb[4];
                 float kb[4];

@@ -43,6 +43,30 @@ __device__ __forceinline__ float gelu(float z) {
     const float hz = 0.5f * z;
     return fmaf(hz, tanh_hw(u), hz);
 }
+// GELU of two activations at once with sm_100's packed FP32 operations
+// (f32x2: each lane rounded as its scalar form), the same operations in the
+// same order as gelu(), so the results are the same bit for bit; in:
+// z = acc + bias per lane, out: the pair rounded to BF16 and packed
+__device__ __forceinline__ unsigned long long f2(float lo, float hi) {
+    unsigned long long r;
+    asm("mov.b64 %0, {%1,%2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void gelu_x2(float a0, float a1, float2 bias, float& g0, float& g1) {
+    unsigned long long z, zz, k, u, hz, t, g;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(z) : "l"(f2(a0, a1)), "l"(f2(bias.x, bias.y)));
+    asm("mul.rn.f32x2 %0, %1, %1;" : "=l"(zz) : "l"(z));
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(k) : "l"(f2(0.0356774081f, 0.0356774081f)), "l"(zz),
+        "l"(f2(0.7978845608f, 0.7978845608f)));
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(u) : "l"(z), "l"(k));
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(hz) : "l"(f2(0.5f, 0.5f)), "l"(z));
+    float u0, u1;
+    asm("mov.b64 {%0,%1}, %2;" : "=f"(u0), "=f"(u1) : "l"(u));
+    t = f2(tanh_hw(u0), tanh_hw(u1));
+    asm("fma.rn.f32x2 %0, %1, %2, %1;" : "=l"(g) : "l"(hz), "l"(t));
+    asm("mov.b64 {%0,%1}, %2;" : "=f"(g0), "=f"(g1) : "l"(g));
+}
+
 // d/dz: (1 + t) / 2 + (z / 2) (1 - t^2) (k0 + 3 k1 z^2)
 __device__ __forceinline__ float gelu_d(float z) {
     const float z2 = z * z;
@@ -378,10 +402,11 @@ __device__ __forceinline__ void ws_features(const DevScene& s, const SolverConst
     // current group's record gathers); entries past the count read the
     // particle's own record and are masked out
     const int ng = (cnt + 3) >> 2;
-    int4 nxt = ng ? ell_group(s.nbr, stride, p, 0) : make_int4(0, 0, 0, 0);
+    const unsigned long long polL = l2_policy(c.l2pol & 3);  // lists stream through L2
+    int4 nxt = ng ? ell_group_pol(s.nbr, stride, p, 0, polL) : make_int4(0, 0, 0, 0);
     for (int gi = 0; gi < ng; ++gi) {
         const int4 cur = nxt;
-        if (gi + 1 < ng) nxt = ell_group(s.nbr, stride, p, gi + 1);
+        if (gi + 1 < ng) nxt = ell_group_pol(s.nbr, stride, p, gi + 1, polL);
         const unsigned e4[4] = {(unsigned)cur.x, (unsigned)cur.y, (unsigned)cur.z, (unsigned)cur.w};
         float4 pb[4], vb[4];
         bool ok[4], bnd[4];
@@ -481,8 +506,9 @@ struct InferSmem {
     float y[TR];
 };
 
-__global__ void __launch_bounds__(TR) k_ws_infer(DevScene s, SolverConst c, MlpDev m, const __nv_bfloat16* xn) {
-    __shared__ InferSmem S;
+// the weights as per-lane B fragments, the biases and W3 (all threads of the
+// block; the caller synchronises)
+__device__ __forceinline__ void infer_pack(InferSmem& S, const MlpDev& m) {
     const __nv_bfloat16* W = m.w_bf16;
     for (int i = threadIdx.x; i < 8 * 32; i += TR) {
         const int nt = i >> 5, lane = i & 31, g = lane >> 2, t = lane & 3, col = nt * 8 + g;
@@ -503,67 +529,135 @@ __global__ void __launch_bounds__(TR) k_ws_infer(DevScene s, SolverConst c, MlpD
         S.w3[i] = __bfloat162float(W[MLP_OFF_W3 + i]);
     }
     if (threadIdx.x == 0) S.b3 = m.master[MLP_OFF_B3];
+}
+
+// The network on the warp's 32 rows [rt, rt + 32) of the block tile:
+// row(r) gives the 32-byte BF16 feature row r (the 16 normalised
+// features); the outputs (before the label scale) go to S.y[rt + r].
+template <class Row>
+__device__ __forceinline__ void infer_rows(InferSmem& S, Row row, int rt0) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    for (int mt = 0; mt < 2; ++mt) {
+        const int rt = rt0 + mt * 16;
+        const uint32_t* x0 = row(rt + g);
+        const uint32_t* x1 = row(rt + g + 8);
+        const uint32_t a[4] = {x0[t], x1[t], x0[4 + t], x1[4 + t]};
+        uint32_t h[4][4];
+#pragma unroll
+        for (int nt = 0; nt < 8; ++nt) {
+            float cc[4] = {0.f, 0.f, 0.f, 0.f};
+            const uint2 b = S.w1f[nt * 32 + lane];
+            const uint32_t bb[2] = {b.x, b.y};
+            mma16816(cc, a, bb);
+            const int col = nt * 8 + 2 * t;
+            const float2 bb1 = *reinterpret_cast<const float2*>(S.b1 + col);
+            float g0, g1, g2, g3;
+            gelu_x2(cc[0], cc[1], bb1, g0, g1);
+            gelu_x2(cc[2], cc[3], bb1, g2, g3);
+            const uint32_t u01 = pack2(__float2bfloat16_rn(g0), __float2bfloat16_rn(g1));
+            const uint32_t u23 = pack2(__float2bfloat16_rn(g2), __float2bfloat16_rn(g3));
+            h[nt >> 1][(nt & 1) * 2] = u01;
+            h[nt >> 1][(nt & 1) * 2 + 1] = u23;
+        }
+        float y0 = 0.f, y1 = 0.f;
+#pragma unroll
+        for (int nt = 0; nt < 8; ++nt) {
+            float cc[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk) {
+                const uint2 b = S.w2f[(kk * 8 + nt) * 32 + lane];
+                const uint32_t bb[2] = {b.x, b.y};
+                mma16816(cc, h[kk], bb);
+            }
+            const int col = nt * 8 + 2 * t;
+            const float2 bb2 = *reinterpret_cast<const float2*>(S.b2 + col);
+            float g0, g1, g2, g3;
+            gelu_x2(cc[0], cc[1], bb2, g0, g1);
+            gelu_x2(cc[2], cc[3], bb2, g2, g3);
+            y0 = fmaf(g0, S.w3[col], y0);
+            y0 = fmaf(g1, S.w3[col + 1], y0);
+            y1 = fmaf(g2, S.w3[col], y1);
+            y1 = fmaf(g3, S.w3[col + 1], y1);
+        }
+        y0 += __shfl_xor_sync(0xffffffffu, y0, 1);
+        y0 += __shfl_xor_sync(0xffffffffu, y0, 2);
+        y1 += __shfl_xor_sync(0xffffffffu, y1, 1);
+        y1 += __shfl_xor_sync(0xffffffffu, y1, 2);
+        if (t == 0) {
+            S.y[rt + g] = y0 + S.b3;
+            S.y[rt + g + 8] = y1 + S.b3;
+        }
+    }
+}
+
+// the prediction of particle p from its network output: negative
+// predictions are not applied (the loop only adds pressure)
+__device__ __forceinline__ void infer_apply(const DevScene& s, const SolverConst& c, const MlpDev& m, int p, float y) {
+    const float* nrm = m.norm;
+    const float kpred = y / nrm[2 * MLP_IN + 1] + nrm[2 * MLP_IN];
+    const float kw = c.ws_scale * fmaxf(kpred, 0.f);
+    s.kwarm[p] = kw;
+    s.pk[p].w = kw / s.rho[p];  // read by the warm-correction sweep
+}
+
+__global__ void __launch_bounds__(TR) k_ws_infer(DevScene s, SolverConst c, MlpDev m, const __nv_bfloat16* xn) {
+    __shared__ InferSmem S;
+    infer_pack(S, m);
     __syncthreads();
     const int n = s.st->n_active;
-    const float* nrm = m.norm;
-    const float ysd = nrm[2 * MLP_IN + 1], ymean = nrm[2 * MLP_IN];
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    const int w = threadIdx.x >> 5;
     for (int base = blockIdx.x * TR; base < n; base += gridDim.x * TR) {
-        for (int mt = 0; mt < 2; ++mt) {
-            const int rt = w * 32 + mt * 16;  // tile row offset inside the block's 128 rows
-            const int r0 = base + rt + g, r1 = r0 + 8;
-            const uint32_t* x0 = reinterpret_cast<const uint32_t*>(xn + (size_t)min(r0, n - 1) * MLP_IN);
-            const uint32_t* x1 = reinterpret_cast<const uint32_t*>(xn + (size_t)min(r1, n - 1) * MLP_IN);
-            const uint32_t a[4] = {__ldg(x0 + t), __ldg(x1 + t), __ldg(x0 + 4 + t), __ldg(x1 + 4 + t)};
-            uint32_t h[4][4];
-#pragma unroll
-            for (int nt = 0; nt < 8; ++nt) {
-                float cc[4] = {0.f, 0.f, 0.f, 0.f};
-                const uint2 b = S.w1f[nt * 32 + lane];
-                const uint32_t bb[2] = {b.x, b.y};
-                mma16816(cc, a, bb);
-                const int col = nt * 8 + 2 * t;
-                const uint32_t u01 = pack2(__float2bfloat16_rn(gelu(cc[0] + S.b1[col])),
-                                           __float2bfloat16_rn(gelu(cc[1] + S.b1[col + 1])));
-                const uint32_t u23 = pack2(__float2bfloat16_rn(gelu(cc[2] + S.b1[col])),
-                                           __float2bfloat16_rn(gelu(cc[3] + S.b1[col + 1])));
-                h[nt >> 1][(nt & 1) * 2] = u01;
-                h[nt >> 1][(nt & 1) * 2 + 1] = u23;
-            }
-            float y0 = 0.f, y1 = 0.f;
-#pragma unroll
-            for (int nt = 0; nt < 8; ++nt) {
-                float cc[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-                for (int kk = 0; kk < 4; ++kk) {
-                    const uint2 b = S.w2f[(kk * 8 + nt) * 32 + lane];
-                    const uint32_t bb[2] = {b.x, b.y};
-                    mma16816(cc, h[kk], bb);
-                }
-                const int col = nt * 8 + 2 * t;
-                y0 = fmaf(gelu(cc[0] + S.b2[col]), S.w3[col], y0);
-                y0 = fmaf(gelu(cc[1] + S.b2[col + 1]), S.w3[col + 1], y0);
-                y1 = fmaf(gelu(cc[2] + S.b2[col]), S.w3[col], y1);
-                y1 = fmaf(gelu(cc[3] + S.b2[col + 1]), S.w3[col + 1], y1);
-            }
-            y0 += __shfl_xor_sync(0xffffffffu, y0, 1);
-            y0 += __shfl_xor_sync(0xffffffffu, y0, 2);
-            y1 += __shfl_xor_sync(0xffffffffu, y1, 1);
-            y1 += __shfl_xor_sync(0xffffffffu, y1, 2);
-            if (t == 0) {
-                S.y[rt + g] = y0 + S.b3;
-                S.y[rt + g + 8] = y1 + S.b3;
-            }
-        }
+        infer_rows(S, [&](int r) {
+            return reinterpret_cast<const uint32_t*>(xn + (size_t)min(base + r, n - 1) * MLP_IN);
+        }, w * 32);
         __syncwarp();
         const int p = base + threadIdx.x;
+        if (p < n) infer_apply(s, c, m, p, S.y[threadIdx.x]);
+        __syncwarp();
+    }
+}
+
+// Features and inference in one pass: each thread gathers its particle's
+// features (a neighbour sweep, bound by the L1 gathers), writes them
+// normalised as a BF16 row into shared memory, and its warp runs the
+// network on its 32 rows (bound by the GELUs' issue slots); resident warps
+// in the two phases overlap.  Persistent blocks pack the weights once.  The
+// rows and the network are those of k_ws_features<1> + k_ws_infer, so the
+// predictions are the same bit for bit.
+struct FusedSmem {
+    InferSmem I;
+    uint32_t x[TR][MLP_IN / 2];
+};
+__global__ void __launch_bounds__(TR) k_ws_features_infer(DevScene s, SolverConst c, MlpDev m, float dt_max,
+                                                          float alpha_ref) {
+    __shared__ FusedSmem S;
+    infer_pack(S.I, m);
+    __syncthreads();
+    const int n = s.st->n_active;
+    const int w = threadIdx.x >> 5;
+    const float* nrm = m.norm;
+    for (int base = blockIdx.x * TR; base < n; base += gridDim.x * TR) {
+        const int p = base + threadIdx.x;
         if (p < n) {
-            const float kpred = S.y[threadIdx.x] / ysd + ymean;
-            // negative predictions are not applied (the loop only adds pressure)
-            const float kw = c.ws_scale * fmaxf(kpred, 0.f);
-            s.kwarm[p] = kw;
-            s.pk[p].w = kw / s.rho[p];  // read by the warm-correction sweep
+            float x[MLP_IN];
+            float pred = 0.f, divt = 0.f;
+            ws_features(s, c, p, *s.dt, dt_max, alpha_ref, x, pred, divt);
+            s.wsbuf[p] = make_float2(pred, divt);
+#pragma unroll
+            for (int i = 0; i < MLP_IN / 2; ++i)
+                S.x[threadIdx.x][i] =
+                    pack2(__float2bfloat16_rn((x[2 * i] - nrm[2 * i]) * nrm[MLP_IN + 2 * i]),
+                          __float2bfloat16_rn((x[2 * i + 1] - nrm[2 * i + 1]) * nrm[MLP_IN + 2 * i + 1]));
         }
+        // (a block-wide barrier: in the last tile a warp past the count reads
+        // another warp's row)
+        __syncthreads();
+        // rows past the count repeat the last particle's row, as k_ws_infer's
+        // clamped reads do (their outputs are discarded)
+        const int last = min(n - 1 - base, TR - 1);
+        infer_rows(S.I, [&](int r) { return S.x[min(r, last)]; }, w * 32);
+        __syncwarp();
+        if (p < n) infer_apply(s, c, m, p, S.I.y[threadIdx.x]);
         __syncwarp();
     }
 }
@@ -622,6 +716,17 @@ void launch_ws_infer(const DevScene& s, const SolverConst& c, const MlpDev& m, c
     const int cap = sm_count * 8;  // persistent: each block packs the weights once
     if (blocks > cap) blocks = cap;
     k_ws_infer<<<blocks, TR, 0, st>>>(s, c, m, xn);
+}
+
+void launch_ws_features_infer(const DevScene& s, const SolverConst& c, const MlpDev& m, float dt_max, float alpha_ref,
+                              int n_max, int sm_count, cudaStream_t st) {
+    static int per_sm = 0;  // resident blocks per SM (the kernel's registers and shared memory)
+    if (!per_sm && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ws_features_infer, TR, 0) != cudaSuccess)
+        per_sm = 4;
+    if (per_sm < 1) per_sm = 1;
+    int blocks = (n_max + TR - 1) / TR;
+    if (blocks > sm_count * per_sm) blocks = sm_count * per_sm;
+    k_ws_features_infer<<<blocks, TR, 0, st>>>(s, c, m, dt_max, alpha_ref);
 }
 
 void launch_ws_post(const DevScene& s, const SolverConst& c, float* yout, int n_max, cudaStream_t st) {
