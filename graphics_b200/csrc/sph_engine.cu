@@ -32,7 +32,7 @@ void launch_ws_infer(const DevScene& s, const SolverConst& c, const MlpDev& m, c
                      int sm_count, cudaStream_t st);
 void launch_ws_post(const DevScene& s, const SolverConst& c, float* yout, int n_max, cudaStream_t st);
 void launch_ws_features_infer(const DevScene& s, const SolverConst& c, const MlpDev& m, float dt_max, float alpha_ref,
-                              int n_max, int sm_count, cudaStream_t st);
+                              __nv_bfloat16* xn, int n_max, int sm_count, cudaStream_t st);
 void launch_ws_append(const float* X, const float* y, int n_max, const int* n_act, int every, int* offset, float* dsX,
                       float* dsy, int* ds_count, int ds_cap, cudaStream_t st);
 
@@ -78,6 +78,18 @@ struct sphgpu_scene {
     float* out_xyz = nullptr;
     int out_n = 0;
     bool out_xyz_done = false;
+    // host-buffer step, speculative: the step's first part runs on the
+    // device state while stream4 copies the host inputs in and checks them
+    // against that state (in_xyz / in_vel, d_diff -> h_diff); the second part
+    // starts only if they were equal
+    cudaStream_t stream4 = nullptr;
+    cudaEvent_t ev_in[2] = {nullptr, nullptr};
+    float* in_xyz = nullptr;
+    float* in_vel = nullptr;
+    int* d_diff = nullptr;
+    int* h_diff = nullptr;
+    bool spec_pending = false, spec_failed = false;
+    int spec = 1;  // debug knob "speculative_host_step"
     int cap = 0, stride = 0, ncap = 48;
     GridGeom g{};
     SolverConst c{};
@@ -402,6 +414,9 @@ void free_scene(sphgpu_scene* h) {
     if (h->d_batch) cudaFree(h->d_batch);
     if (h->h_stats) cudaFreeHost(h->h_stats);
     if (h->h_cont) cudaFreeHost(h->h_cont);
+    if (h->h_diff) cudaFreeHost(h->h_diff);
+    for (void* q : {(void*)h->in_xyz, (void*)h->in_vel, (void*)h->d_diff})
+        if (q) cudaFree(q);
     for (auto& kv : h->graphs) cudaGraphExecDestroy(kv.second);
     for (auto e : h->prof.pool) cudaEventDestroy(e);
 }
@@ -588,7 +603,7 @@ int enq_df_part1(sphgpu_scene* h, bool capturing) {
         });
     if (ws == 1 && h->fuse_ws) {
         launch(h, "ws_features_infer", st, [&] {
-            launch_ws_features_infer(d, h->c, h->mlp->m, h->P.dt_max, h->alpha_ref, h->cap, h->sm_count, st);
+            launch_ws_features_infer(d, h->c, h->mlp->m, h->P.dt_max, h->alpha_ref, h->xn, h->cap, h->sm_count, st);
         });
         launch(h, "df_warm", st, [&] { launch_df_warm_correction(d, h->c, h->cap, st, h->tune.sweep_b); });
     } else if (ws == 1 || ws == 3) {
@@ -610,6 +625,16 @@ int enq_df_part1(sphgpu_scene* h, bool capturing) {
     h->record_ksum = rec;
     if (r) return r;
     enq_rigid_forces(h, st);
+    return 0;
+}
+
+int enq_df_part2(sphgpu_scene* h, bool capturing) {
+    DevScene& d = h->d;
+    cudaStream_t st = h->stream;
+    // the warm start's history and training label (part 2, so that part 1
+    // leaves every carried per-particle array as it found it: a speculative
+    // host step may run part 1 again)
+    const int ws = h->mlp ? h->ws_mode : 0;
     if (ws) {
         launch(h, "ws_post", st, [&] { launch_ws_post(d, h->c, ws == 2 ? h->recY : nullptr, h->cap, st); });
         if (ws == 2) {
@@ -618,12 +643,6 @@ int enq_df_part1(sphgpu_scene* h, bool capturing) {
                              m->ds_count, m->ds_cap, st);
         }
     }
-    return 0;
-}
-
-int enq_df_part2(sphgpu_scene* h, bool capturing) {
-    DevScene& d = h->d;
-    cudaStream_t st = h->stream;
     enq_boundary_update(h, st);
     const int vort = h->P.enable_vortex ? 2 : 0;  // carry cA (w or n0) through the sort
     const bool fused = fused_div(h);
@@ -1022,9 +1041,22 @@ int enq_steps(sphgpu_scene* h, int solver, int nsteps) {
                 CK(cudaGraphLaunch(ex1, h->stream));
                 CK(cudaEventRecord(h->ev_out[0], h->stream));
                 CK(cudaStreamWaitEvent(h->stream3, h->ev_out[0], 0));
+                // the output may be the input buffer: after the input copy
+                if (h->spec_pending) CK(cudaStreamWaitEvent(h->stream3, h->ev_in[1], 0));
                 CK(cudaMemcpyAsync(h->out_xyz, h->d.aux4, sizeof(float) * 3 * (size_t)h->out_n,
                                    cudaMemcpyDeviceToHost, h->stream3));
                 CK(cudaEventRecord(h->ev_out[1], h->stream3));
+                if (h->spec_pending) {
+                    // part 1 ran ahead of the check of the host inputs
+                    // (sphgpu_step_host): part 2, which re-sorts the state,
+                    // starts only if they equal the state part 1 read
+                    h->spec_pending = false;
+                    CK(cudaEventSynchronize(h->ev_in[1]));
+                    if (*h->h_diff) {
+                        h->spec_failed = true;
+                        return 0;
+                    }
+                }
                 CK(cudaGraphLaunch(ex2, h->stream));
                 CK(cudaStreamWaitEvent(h->stream, h->ev_out[1], 0));
                 h->out_xyz_done = true;
@@ -1268,8 +1300,11 @@ static int create_impl(const SphParams* p, int device, int max_fluid, int nscene
     if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&h->stream2, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&h->stream3, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&h->stream4, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&h->ev_out[0], cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&h->ev_out[1], cudaEventDisableTiming) != cudaSuccess) {
+        cudaEventCreateWithFlags(&h->ev_out[1], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_in[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_in[1], cudaEventDisableTiming) != cudaSuccess) {
         delete h;
         return SPHGPU_ECUDA;
     }
@@ -1349,11 +1384,15 @@ int sphgpu_destroy(sphgpu_t h) {
     cudaStreamSynchronize(h->stream);
     free_scene(h);
     cudaStreamSynchronize(h->stream3);
+    cudaStreamSynchronize(h->stream4);
     cudaStreamDestroy(h->stream);
     cudaStreamDestroy(h->stream2);
     cudaStreamDestroy(h->stream3);
+    cudaStreamDestroy(h->stream4);
     cudaEventDestroy(h->ev_out[0]);
     cudaEventDestroy(h->ev_out[1]);
+    cudaEventDestroy(h->ev_in[0]);
+    cudaEventDestroy(h->ev_in[1]);
     delete h;
     return 0;
 }
@@ -1635,6 +1674,40 @@ int sphgpu_step(sphgpu_t h, int solver, int nsteps, SphStepStats* stats) {
 // output (the usual loop) pays for the transfers, not for a search.  The
 // transfers are stream-ordered, with one host synchronisation for the
 // comparison and one at the end.
+// The outputs of a host-buffer step after the step was enqueued: the
+// velocities (and, unless they left during the step, the positions) in
+// reference order.
+static int finish_host_step(sphgpu_scene* h, float* vel_out, float* xyz_out, SphStepStats* stats) {
+    int r = 0;
+    const int n0 = h->out_n;
+    float* tv = (float*)h->d.vadv;
+    if (h->out_xyz_done) {
+        launch_to_ref_order(h->d.vel, h->d.gid, n0, tv, h->stream);
+        CK(cudaMemcpyAsync(vel_out, tv, sizeof(float) * 3 * (size_t)n0, cudaMemcpyDeviceToHost, h->stream));
+    }
+    r = sphgpu_synchronize(h, stats);
+    if (stats) stats->steps = 1;
+    if (r && r != SPHGPU_EMAXITER) return r;
+    if (h->out_xyz_done && h->total_removed == 0) return r;
+    int r2 = 0;
+    if (h->total_removed == 0 && xyz_out && vel_out) {
+        // both outputs reordered on the device, copied out back to back
+        DevScene& d = h->d;
+        const int n = h->h_stats->n_active;
+        const bool stg = h->in_staging;
+        float* tx = (float*)d.aux4;
+        launch_to_ref_order(stg ? d.pos_s : d.pos, stg ? d.gid_s : d.gid, n, tx, h->stream);
+        launch_to_ref_order(stg ? d.vel_s : d.vel, stg ? d.gid_s : d.gid, n, tv, h->stream);
+        CK(cudaMemcpyAsync(xyz_out, tx, sizeof(float) * 3 * (size_t)n, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(vel_out, tv, sizeof(float) * 3 * (size_t)n, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        return r;
+    }
+    if (xyz_out) r2 = sphgpu_get_fluid(h, "position", xyz_out) < 0 ? SPHGPU_ECUDA : 0;
+    if (!r2 && vel_out) r2 = sphgpu_get_fluid(h, "velocity", vel_out) < 0 ? SPHGPU_ECUDA : 0;
+    return r2 ? r2 : r;
+}
+
 int sphgpu_step_host(sphgpu_t h, int solver, const float* xyz, const float* vel, float* xyz_out, float* vel_out,
                      SphStepStats* stats) {
     if (!h) return SPHGPU_EINVAL;
@@ -1643,13 +1716,74 @@ int sphgpu_step_host(sphgpu_t h, int solver, const float* xyz, const float* vel,
     CK(cudaStreamSynchronize(h->stream));
     const bool fast = xyz && vel && solver == SPHGPU_DFSPH && h->total_removed == 0 && !h->in_staging &&
                       h->ns_valid && h->nscenes == 1 && h->R.nd == 0;
+    // Speculative form (the common loop: the host hands back the state the
+    // last step returned): the step's first part (forces, density loop, the
+    // integrated positions) runs on the device state while stream4 copies
+    // the host inputs in and compares them with that state bit for bit; part
+    // 1 writes no carried per-particle array (the warm start's history is
+    // written in part 2, its kappa sum restarts from zero), so when the
+    // inputs differ the step is run again from them.
+    const bool spec = fast && h->spec && xyz_out && vel_out && h->use_graphs && !h->prof.on &&
+                      h->P.enable_vortex == 0 && !h->record_ksum && (!h->mlp || h->ws_mode <= 1);
+    const int n_in = h->h_stats->n_active;
+    if (spec) {
+        DevScene& d = h->d;
+        const size_t b3 = sizeof(float) * 3 * (size_t)h->cap;
+        if (!h->in_xyz && (cudaMalloc((void**)&h->in_xyz, b3) != cudaSuccess ||
+                           cudaMalloc((void**)&h->in_vel, b3) != cudaSuccess ||
+                           cudaMalloc((void**)&h->d_diff, sizeof(int)) != cudaSuccess ||
+                           cudaMallocHost((void**)&h->h_diff, sizeof(int)) != cudaSuccess)) {
+            h->err = "out of device memory (host-step input buffers)";
+            return SPHGPU_ENOMEM;
+        }
+        cudaStream_t s4 = h->stream4;
+        CK(cudaEventRecord(h->ev_in[0], h->stream));
+        CK(cudaStreamWaitEvent(s4, h->ev_in[0], 0));
+        CK(cudaMemsetAsync(h->d_diff, 0, sizeof(int), s4));
+        CK(cudaMemcpyAsync(h->in_xyz, xyz, sizeof(float) * 3 * (size_t)n_in, cudaMemcpyHostToDevice, s4));
+        CK(cudaMemcpyAsync(h->in_vel, vel, sizeof(float) * 3 * (size_t)n_in, cudaMemcpyHostToDevice, s4));
+        launch_state_check(h->in_xyz, h->in_vel, d.gid, n_in, d.pos, d.vel, h->d_diff, s4);
+        CK(cudaMemcpyAsync(h->h_diff, h->d_diff, sizeof(int), cudaMemcpyDeviceToHost, s4));
+        CK(cudaEventRecord(h->ev_in[1], s4));
+        h->spec_pending = true;
+        h->spec_failed = false;
+        h->out_xyz = xyz_out;
+        h->out_n = n_in;
+        h->out_xyz_done = false;
+        r = sphgpu_step_async(h, solver, 1);
+        h->out_xyz = nullptr;
+        const bool checked = !h->spec_pending;
+        h->spec_pending = false;
+        if (!checked) CK(cudaStreamSynchronize(s4));  // the step did not take the two-graph path
+        if (r) return r;
+        if (h->spec_failed || (!checked && *h->h_diff)) {
+            // the host state differs: back to the state the step started
+            // from (part 1 changed no carried array; the kappa sum restarts)
+            h->spec_failed = false;
+            CK(cudaStreamSynchronize(h->stream));
+            CK(cudaStreamSynchronize(h->stream3));
+            if (!checked) {
+                h->err = "host step: inputs differ after a step that was not speculative";
+                return SPHGPU_ECUDA;
+            }
+            if (h->mlp && h->ws_mode == 1) CK(cudaMemsetAsync(d.ksum, 0, sizeof(float) * h->cap, h->stream));
+        } else {
+            return finish_host_step(h, vel_out, xyz_out, stats);
+        }
+    }
     if (fast) {
         DevScene& d = h->d;
-        const int n = h->h_stats->n_active;
+        const int n = n_in;
         float* tx = (float*)d.aux4;
         float* tv = (float*)d.vadv;
-        CK(cudaMemcpyAsync(tx, xyz, sizeof(float) * 3 * (size_t)n, cudaMemcpyHostToDevice, h->stream));
-        CK(cudaMemcpyAsync(tv, vel, sizeof(float) * 3 * (size_t)n, cudaMemcpyHostToDevice, h->stream));
+        if (spec) {
+            // the inputs are on the device already
+            tx = h->in_xyz;
+            tv = h->in_vel;
+        } else {
+            CK(cudaMemcpyAsync(tx, xyz, sizeof(float) * 3 * (size_t)n, cudaMemcpyHostToDevice, h->stream));
+            CK(cudaMemcpyAsync(tv, vel, sizeof(float) * 3 * (size_t)n, cudaMemcpyHostToDevice, h->stream));
+        }
         CK(cudaMemsetAsync(&d.st->cont, 0, sizeof(int), h->stream));
         launch_state_in(tx, tv, d.gid, n, d.pos, d.vel, d.prv, &d.st->cont, h->stream);
         CK(cudaMemcpyAsync(h->h_cont, &d.st->cont, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
@@ -1677,32 +1811,7 @@ int sphgpu_step_host(sphgpu_t h, int solver, const float* xyz, const float* vel,
     r = sphgpu_step_async(h, solver, 1);
     h->out_xyz = nullptr;
     if (r) return r;
-    float* tv = (float*)h->d.vadv;
-    if (h->out_xyz_done) {
-        launch_to_ref_order(h->d.vel, h->d.gid, n0, tv, h->stream);
-        CK(cudaMemcpyAsync(vel_out, tv, sizeof(float) * 3 * (size_t)n0, cudaMemcpyDeviceToHost, h->stream));
-    }
-    r = sphgpu_synchronize(h, stats);
-    if (stats) stats->steps = 1;
-    if (r && r != SPHGPU_EMAXITER) return r;
-    if (h->out_xyz_done && h->total_removed == 0) return r;
-    int r2 = 0;
-    if (h->total_removed == 0 && xyz_out && vel_out) {
-        // both outputs reordered on the device, copied out back to back
-        DevScene& d = h->d;
-        const int n = h->h_stats->n_active;
-        const bool stg = h->in_staging;
-        float* tx = (float*)d.aux4;
-        launch_to_ref_order(stg ? d.pos_s : d.pos, stg ? d.gid_s : d.gid, n, tx, h->stream);
-        launch_to_ref_order(stg ? d.vel_s : d.vel, stg ? d.gid_s : d.gid, n, tv, h->stream);
-        CK(cudaMemcpyAsync(xyz_out, tx, sizeof(float) * 3 * (size_t)n, cudaMemcpyDeviceToHost, h->stream));
-        CK(cudaMemcpyAsync(vel_out, tv, sizeof(float) * 3 * (size_t)n, cudaMemcpyDeviceToHost, h->stream));
-        CK(cudaStreamSynchronize(h->stream));
-        return r;
-    }
-    if (xyz_out) r2 = sphgpu_get_fluid(h, "position", xyz_out) < 0 ? SPHGPU_ECUDA : 0;
-    if (!r2 && vel_out) r2 = sphgpu_get_fluid(h, "velocity", vel_out) < 0 ? SPHGPU_ECUDA : 0;
-    return r2 ? r2 : r;
+    return finish_host_step(h, vel_out, xyz_out, stats);
 }
 
 int sphgpu_get_fluid(sphgpu_t h, const char* field, float* out) {
@@ -2759,6 +2868,7 @@ int sphgpu_debug_set(sphgpu_t h, const char* key, int value) {
     if (k == "use_graphs") { h->use_graphs = value != 0; return 0; }
     if (k == "fuse_div") { h->fuse_div = value != 0; invalidate_graphs(h); return 0; }
     if (k == "fuse_ws") { h->fuse_ws = value != 0; invalidate_graphs(h); return 0; }
+    if (k == "speculative_host_step") { h->spec = value != 0; return 0; }
     if (k == "l2_policy") {
         // measurement knob: L2 eviction priorities of the sweeps' list and
         // record loads (SolverConst::l2pol)

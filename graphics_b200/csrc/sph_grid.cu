@@ -397,6 +397,24 @@ __global__ void k_state_in(const float* xyz3, const float* vel3, const int* gid,
     if (__syncthreads_or(diff) && threadIdx.x == 0) atomicOr(changed, 1);
 }
 
+// Host state (reference order) against the sorted device state, bit for bit
+// (positions and velocities): *differs set if any particle differs.  Reads
+// only, so it can run while a step that has not yet re-sorted reads the same
+// arrays.
+__global__ void k_state_check(const float* xyz3, const float* vel3, const int* gid, int n, const float4* pos,
+                              const float4* vel, int* differs) {
+    const int p = blockIdx.x * NT + threadIdx.x;
+    int diff = 0;
+    if (p < n) {
+        const size_t g = (size_t)gid[p] * 3;
+        const float4 x = pos[p], v = vel[p];
+        diff = (__float_as_int(x.x) != __float_as_int(xyz3[g])) | (__float_as_int(x.y) != __float_as_int(xyz3[g + 1])) |
+               (__float_as_int(x.z) != __float_as_int(xyz3[g + 2])) | (__float_as_int(v.x) != __float_as_int(vel3[g])) |
+               (__float_as_int(v.y) != __float_as_int(vel3[g + 1])) | (__float_as_int(v.z) != __float_as_int(vel3[g + 2]));
+    }
+    if (__syncthreads_or(diff) && threadIdx.x == 0) atomicOr(differs, 1);
+}
+
 // The positions the integration (k_hash, integrate mode) will write, in
 // the same round-to-nearest operations, scattered into reference order:
 // a host-buffer step copies them out while the rest of the step runs (the
@@ -434,6 +452,10 @@ void launch_to_ref_order(const float4* src, const int* gid, int n, float* dst3, 
 void launch_state_in(const float* xyz3, const float* vel3, const int* gid, int n, const float4* pos, float4* vel,
                      float4* prv, int* changed, cudaStream_t st) {
     if (n > 0) k_state_in<<<nblk(n, NT), NT, 0, st>>>(xyz3, vel3, gid, n, pos, vel, prv, changed);
+}
+void launch_state_check(const float* xyz3, const float* vel3, const int* gid, int n, const float4* pos,
+                        const float4* vel, int* differs, cudaStream_t st) {
+    if (n > 0) k_state_check<<<nblk(n, NT), NT, 0, st>>>(xyz3, vel3, gid, n, pos, vel, differs);
 }
 void launch_integrated_to_ref(const DevScene& s, int n_max, float* out3, cudaStream_t st) {
     if (n_max > 0) k_integrated_to_ref<<<nblk(n_max, NT), NT, 0, st>>>(s, out3);

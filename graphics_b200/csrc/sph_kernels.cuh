@@ -222,6 +222,9 @@ void launch_build(const DevScene& s, const GridGeom& g, const SolverConst& c, in
                   int bs = 128);
 void launch_to_ref_order(const float4* src, const int* gid, int n, float* dst3, cudaStream_t st);
 void launch_integrated_to_ref(const DevScene& s, int n_max, float* out3, cudaStream_t st);
+// host state (reference order) bit for bit against the sorted state: *differs |= 1
+void launch_state_check(const float* xyz3, const float* vel3, const int* gid, int n, const float4* pos,
+                        const float4* vel, int* differs, cudaStream_t st);
 void set_sweep_carveout(int pct);
 void set_build_carveout(int pct);
 void launch_from_ref_order(const float* src3, const int* gid, int n, float4* dst, cudaStream_t st);

@@ -629,7 +629,7 @@ struct FusedSmem {
     uint32_t x[TR][MLP_IN / 2];
 };
 __global__ void __launch_bounds__(TR) k_ws_features_infer(DevScene s, SolverConst c, MlpDev m, float dt_max,
-                                                          float alpha_ref) {
+                                                          float alpha_ref, __nv_bfloat16* xn) {
     __shared__ FusedSmem S;
     infer_pack(S.I, m);
     __syncthreads();
@@ -643,11 +643,17 @@ __global__ void __launch_bounds__(TR) k_ws_features_infer(DevScene s, SolverCons
             float pred = 0.f, divt = 0.f;
             ws_features(s, c, p, *s.dt, dt_max, alpha_ref, x, pred, divt);
             s.wsbuf[p] = make_float2(pred, divt);
+            uint32_t u[MLP_IN / 2];
 #pragma unroll
-            for (int i = 0; i < MLP_IN / 2; ++i)
-                S.x[threadIdx.x][i] =
-                    pack2(__float2bfloat16_rn((x[2 * i] - nrm[2 * i]) * nrm[MLP_IN + 2 * i]),
-                          __float2bfloat16_rn((x[2 * i + 1] - nrm[2 * i + 1]) * nrm[MLP_IN + 2 * i + 1]));
+            for (int i = 0; i < MLP_IN / 2; ++i) {
+                u[i] = pack2(__float2bfloat16_rn((x[2 * i] - nrm[2 * i]) * nrm[MLP_IN + 2 * i]),
+                             __float2bfloat16_rn((x[2 * i + 1] - nrm[2 * i + 1]) * nrm[MLP_IN + 2 * i + 1]));
+                S.x[threadIdx.x][i] = u[i];
+            }
+            // the normalised row also goes out (the ws_features getter reads it)
+            uint4* dst = reinterpret_cast<uint4*>(xn + (size_t)p * MLP_IN);
+            dst[0] = make_uint4(u[0], u[1], u[2], u[3]);
+            dst[1] = make_uint4(u[4], u[5], u[6], u[7]);
         }
         // (a block-wide barrier: in the last tile a warp past the count reads
         // another warp's row)
@@ -719,14 +725,14 @@ void launch_ws_infer(const DevScene& s, const SolverConst& c, const MlpDev& m, c
 }
 
 void launch_ws_features_infer(const DevScene& s, const SolverConst& c, const MlpDev& m, float dt_max, float alpha_ref,
-                              int n_max, int sm_count, cudaStream_t st) {
+                              __nv_bfloat16* xn, int n_max, int sm_count, cudaStream_t st) {
     static int per_sm = 0;  // resident blocks per SM (the kernel's registers and shared memory)
     if (!per_sm && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ws_features_infer, TR, 0) != cudaSuccess)
         per_sm = 4;
     if (per_sm < 1) per_sm = 1;
     int blocks = (n_max + TR - 1) / TR;
     if (blocks > sm_count * per_sm) blocks = sm_count * per_sm;
-    k_ws_features_infer<<<blocks, TR, 0, st>>>(s, c, m, dt_max, alpha_ref);
+    k_ws_features_infer<<<blocks, TR, 0, st>>>(s, c, m, dt_max, alpha_ref, xn);
 }
 
 void launch_ws_post(const DevScene& s, const SolverConst& c, float* yout, int n_max, cudaStream_t st) {

@@ -162,6 +162,23 @@ def test_graph_and_host_loops_identical_and_deterministic():
         np.testing.assert_array_equal(a, b)
 
 
+@pytest.mark.parametrize("graphs", [1, 0])
+def test_fused_divergence_sweep_identical_to_separate(graphs):
+    # the list build's fused first divergence sweep (build mode 4) against the
+    # separate k_df_div_a launch, on a dam break that settles over the steps
+    # (several divergence iterations in the first ones)
+    out = []
+    for fused in (1, 0):
+        sc, g, o = make_pair(scene=small_dam_break((16, 16, 16), r=0.025, seed=3), cfl=1)
+        g.debug_set("use_graphs", graphs)
+        g.debug_set("fuse_div", fused)
+        its = [g.step("dfsph", 1)["iter_divergence"] for _ in range(6)]
+        out.append((g.get("position"), g.get("velocity"), g.get("density"), g.get("DFkappaV"), its))
+    for a, b in zip(out[0][:4], out[1][:4]):
+        np.testing.assert_array_equal(a, b)
+    assert out[0][4] == out[1][4]
+
+
 def test_wcsph_graph_and_host_steps_identical():
     """The WCSPH step as one CUDA graph per step and launched from the host
     give the same state bit for bit."""
@@ -284,6 +301,48 @@ def test_step_host_matches_device_steps():
         np.testing.assert_array_equal(po, ref.get("position"))
         np.testing.assert_array_equal(vo, ref.get("velocity"))
         pos, vel = po.copy(), vo.copy()
+
+
+def test_step_host_speculative_with_warm_start_in_place():
+    """The speculative host step (part 1 runs while the inputs are copied in
+    and checked) with the learned warm start attached and the output arrays
+    the input arrays: handed-back state, changed velocities and a moved
+    particle each give the device path's step bit for bit, and so does the
+    same sequence with the speculation off."""
+    from graphics_b200 import _lib
+    from graphics_b200.warmstart import WarmStartNet, attach
+    net = WarmStartNet(device=0, dataset_cap=1024, seed=4)
+    rng = np.random.default_rng(4)
+    net.set_params(rng.normal(0, 0.05, _lib.MLP_NPARAM).astype(np.float32))
+    net.set_norm(np.concatenate([np.zeros(16), np.ones(16), [0.0, 50.0]]).astype(np.float32))
+    runs = []
+    for spec in (1, 0):
+        sc, g, o = make_pair(cfl=1)
+        sc2, ref, o2 = make_pair(cfl=1)
+        g.debug_set("speculative_host_step", spec)
+        for x in (g, ref):
+            x.step("dfsph", 2)
+            attach(x, net, 1)
+            x.step("dfsph", 1)
+        pos, vel = g.get("position"), g.get("velocity")
+        out = []
+        for k in range(4):
+            if k == 1:
+                vel *= np.float32(0.5)
+                ref.set("velocity", vel)
+            if k == 3:
+                pos[11] += np.float32(0.001)
+                ref.set("position", pos)
+            g.step_host("dfsph", pos, vel, pos, vel)  # in place
+            ref.step("dfsph", 1)
+            np.testing.assert_array_equal(pos, ref.get("position"))
+            np.testing.assert_array_equal(vel, ref.get("velocity"))
+            np.testing.assert_array_equal(g.get("kappa_warm"), ref.get("kappa_warm"))
+            out.append((pos.copy(), vel.copy()))
+        runs.append(out)
+    for a, b in zip(runs[0], runs[1]):
+        np.testing.assert_array_equal(a[0], b[0])
+        np.testing.assert_array_equal(a[1], b[1])
 
 
 def test_step_host_removal_during_step():

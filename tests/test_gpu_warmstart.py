@@ -244,3 +244,35 @@ def test_feature_gather_matches_cpu_restatement():
     excess = np.abs(feat - ref) - (2.0 ** -7 * np.abs(ref) + 2e-3 * scale)
     assert np.all(excess <= 0), excess.max(0)
     assert np.abs(x[:, 4]).max() > 0 and np.abs(x[:, 11]).max() > 0  # the history features are exercised
+
+
+@pytest.mark.parametrize("graphs", [1, 0])
+def test_fused_features_inference_identical_to_separate(graphs):
+    # k_ws_features_infer (features gathered and the network run in one
+    # kernel, packed-pair GELU) against k_ws_features + k_ws_infer
+    from graphics_b200.scene import small_dam_break
+    from graphics_b200.sph import GpuScene, params_for_scene
+    from graphics_b200.warmstart import attach
+    rng = np.random.default_rng(11)
+    net = _net(seed=2)
+    w, norm = _random_state(rng)
+    net.set_params(0.2 * w)
+    norm[-1] = 50.0
+    net.set_norm(norm)
+    sc = small_dam_break((14, 14, 14), r=0.025, seed=5)
+    out = []
+    for fused in (1, 0):
+        g = GpuScene(params_for_scene(sc, dt=1e-3, nu=1e-3), sc.n_fluid, device=0)
+        g.set_boundary(sc.boundary_pos)
+        g.add_fluid(sc.fluid_pos, sc.fluid_vel, rho0=sc.rho0)
+        g.debug_set("use_graphs", graphs)
+        g.debug_set("fuse_ws", fused)
+        g.step("dfsph", 2)
+        attach(g, net, 1)
+        its = [g.step("dfsph", 1)["iter_density"] for _ in range(3)]
+        out.append((g.get("kappa_warm"), g.get("position"), its))
+        g.close()
+    assert np.any(out[0][0] > 0)
+    np.testing.assert_array_equal(out[0][0], out[1][0])
+    np.testing.assert_array_equal(out[0][1], out[1][1])
+    assert out[0][2] == out[1][2]
