@@ -201,7 +201,14 @@ int sphgpu_synchronize(sphgpu_t h, SphStepStats* stats);
  * that case, with graphs on, the positions the step's integration produces
  * are copied into xyz_out while its neighbour search and divergence loop
  * still run (pinned xyz_out makes the copy overlap; a step that removes
- * particles writes both outputs again afterwards). */
+ * particles writes both outputs again afterwards).  With both outputs wanted,
+ * graphs on, no vorticity option and no kappa-sum recording, the step is
+ * speculative: its first part (forces, density loop, integrated positions)
+ * runs on the device state while a second stream copies xyz/vel in and
+ * compares them with that state bit for bit; the re-sorting second part
+ * starts only if they are equal, otherwise the step runs again from the
+ * uploaded state (same results either way; pinned xyz/vel make the upload
+ * overlap; xyz_out may be xyz and vel_out vel). */
 int sphgpu_step_host(sphgpu_t h, int solver, const float* xyz, const float* vel, float* xyz_out,
                      float* vel_out, SphStepStats* stats);
 
