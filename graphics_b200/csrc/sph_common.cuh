@@ -65,6 +65,7 @@ struct SolverConst {
     float ws_scale;    // applied fraction of the predicted warm-start stiffness
     int cap;           // neighbour cap
     int stride;        // ELL column stride (>= fluid capacity)
+    int lanes;         // threads per particle of the WCSPH list build and force pass (1 or 4)
     int l2pol;         // L2 eviction priority of the sweeps' loads: bits 0-1 the
                        // neighbour lists, bits 2-3 the gathered records
                        // (0 normal, 1 evict first, 2 evict last)

@@ -130,6 +130,9 @@ struct sphgpu_scene {
     int l2pol = 1;
     int fuse_div = 1;  // DFSPH: the list build performs the divergence loop's first sweep A
     int fuse_ws = 1;   // warm start: features and inference in one kernel
+    // WCSPH threads per particle: 0 = by size (4 up to 262,144 particles of
+    // capacity, 1 above), else 1 or 4 (debug knob "wc_lanes")
+    int wc_lanes = 0;
     // learned warm start: 0 off, 1 apply the network, 2 record training data
     sphgpu_mlp* mlp = nullptr;
     int ws_mode = 0;
@@ -282,6 +285,7 @@ void fill_solver_const(sphgpu_scene* h) {
     c.cap = h->ncap;
     c.stride = h->stride;
     c.l2pol = h->l2pol;
+    c.lanes = h->wc_lanes ? h->wc_lanes : (h->cap <= (1 << 18) ? 4 : 1);
     c.ws_scale = P.ws_scale;
     // IISph: per-pair h = (d + d)/2 = d (SphBase.h:855-915 with one diameter)
     {
@@ -828,7 +832,7 @@ int enq_wc_step(sphgpu_scene* h, bool) {
     enq_ns(h, 0, 2, st);
     const bool surf = h->P.th_h != 0.f || h->P.th_r != 0.f || h->P.th_bt != 0.f;
     if (surf) launch(h, "wc_normal", st, [&] { launch_wc_normal(h->d, h->c, h->cap, st); });
-    launch(h, "wc_force", st, [&] { launch_wc_force(h->d, h->c, h->cap, st, surf); });
+    launch(h, "wc_force", st, [&] { launch_wc_force(h->d, h->c, h->cap, st, surf, h->c.lanes); });
     CK(cudaMemcpyAsync(h->h_stats, h->d.st, sizeof(DevStats), cudaMemcpyDeviceToHost, st));
     return 0;
 }
@@ -2211,7 +2215,7 @@ int sphgpu_stage(sphgpu_t h, const char* name, SphStepStats* stats) {
         if (h->in_staging) { h->err = "run neighbourSearch first"; return SPHGPU_EINVAL; }
         const bool surf = h->P.th_h != 0.f || h->P.th_r != 0.f || h->P.th_bt != 0.f;
         if (surf) launch_wc_normal(d, h->c, h->cap, st);
-        launch_wc_force(d, h->c, h->cap, st, surf);
+        launch_wc_force(d, h->c, h->cap, st, surf, h->c.lanes);
         h->ep_acc = h->sorts;
         h->in_staging = true;
         h->ns_valid = false;
@@ -2868,6 +2872,13 @@ int sphgpu_debug_set(sphgpu_t h, const char* key, int value) {
     if (k == "use_graphs") { h->use_graphs = value != 0; return 0; }
     if (k == "fuse_div") { h->fuse_div = value != 0; invalidate_graphs(h); return 0; }
     if (k == "fuse_ws") { h->fuse_ws = value != 0; invalidate_graphs(h); return 0; }
+    if (k == "wc_lanes") {
+        if (value != 0 && value != 1 && value != 4) return SPHGPU_EINVAL;
+        h->wc_lanes = value;
+        fill_solver_const(h);
+        invalidate_graphs(h);
+        return 0;
+    }
     if (k == "speculative_host_step") { h->spec = value != 0; return 0; }
     if (k == "l2_policy") {
         // measurement knob: L2 eviction priorities of the sweeps' list and

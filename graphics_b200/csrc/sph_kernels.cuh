@@ -264,7 +264,9 @@ void launch_batch_count(const DevScene& s, int nscenes, cudaStream_t st);
 
 // ---- WCSPH (sph_wcsph.cu) ----
 // surf: with surface tension and adhesion (the normals of launch_wc_normal in vA)
-void launch_wc_force(const DevScene& s, const SolverConst& c, int n_max, cudaStream_t st, bool surf = false);
+// lanes: threads per particle (1, or 4 for small scenes)
+void launch_wc_force(const DevScene& s, const SolverConst& c, int n_max, cudaStream_t st, bool surf = false,
+                     int lanes = 1);
 void launch_wc_normal(const DevScene& s, const SolverConst& c, int n_max, cudaStream_t st);
 
 // ---- PCISPH / IISPH_M (sph_pci_ii.cu) ----

@@ -212,6 +212,40 @@ def test_wcsph_pressure_force_and_steps():
     assert rel_err(g.get("position"), o.get("position"), scale=1.0) < 1e-6
 
 
+@pytest.mark.parametrize("surf", [0, 1])
+def test_wcsph_lanes_match_one_thread_per_particle(surf):
+    """The small-scene WCSPH kernels (4 threads per particle: list build
+    with density and pressure, force pass) against one thread per particle
+    on the same scene: the neighbour lists bit for bit, densities, pressures
+    and accelerations to rounding, and the trajectory over steps."""
+    kw = dict(dt=2.5e-4, soundSpeed_cs=18.708287)
+    if surf:
+        kw.update(th_h=0.1, th_r=0.5, th_bt=0.3)
+    out = []
+    for lanes in (1, 4):
+        sc, g, o = make_pair(visc_alpha=0.01, boundary_visc=0.01, **kw)
+        g.debug_set("wc_lanes", lanes)
+        g.stage("wc_computePressure")
+        lists = g.neighbours()
+        fields = [g.get("density"), g.get("presure")]
+        g.stage("wc_computeForce")
+        fields.append(g.get("acceleration"))
+        for _ in range(20):
+            g.step("wcsph", 1)
+        fields.append(g.get("position"))
+        out.append((lists, fields))
+    (c1, t1, i1), (c4, t4, i4) = out[0][0], out[1][0]
+    np.testing.assert_array_equal(c1, c4)
+    m = np.arange(t1.shape[1])[None, :] < c1[:, None]
+    np.testing.assert_array_equal(t1[m], t4[m])
+    np.testing.assert_array_equal(i1[m], i4[m])
+    f1, f4 = out[0][1], out[1][1]
+    assert elem_rel(f1[0], f4[0]) < 1e-6
+    assert rel_err(f1[1], f4[1]) < 1e-4
+    assert rel_err(f1[2], f4[2]) < 1e-5
+    assert rel_err(f1[3], f4[3], scale=1.0) < 1e-6
+
+
 def test_wcsph_surface_tension_and_adhesion():
     """m_TH.h / r / bt set (the reference's demo values): the surface
     normal, cohesion, curvature and adhesion terms against the oracle's
