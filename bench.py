@@ -189,6 +189,19 @@ class ClockSampler:
             self.p = None
         return self
 
+    def wait_first(self, timeout=5.0):
+        """Block until nvidia-smi has written its first sample (its start-up
+        takes a fraction of a second), so that the timed region is covered."""
+        t0 = time.perf_counter()
+        while self.p and time.perf_counter() - t0 < timeout:
+            try:
+                if os.path.getsize(self.path) > 0:
+                    return self
+            except OSError:
+                pass
+            time.sleep(0.02)
+        return self
+
     def stop(self):
         if self.p:
             self.p.terminate()
@@ -199,7 +212,7 @@ class ClockSampler:
             self.f.close()
 
     def __enter__(self):
-        return self.start()
+        return self.start().wait_first()
 
     def __exit__(self, *a):
         self.stop()
@@ -396,6 +409,9 @@ def run_ours(args):
     if args.settle > 0:
         g.step("dfsph", args.settle)
     settle_pos, settle_vel = g.get("position"), g.get("velocity")
+    # clock samples from the warm-up on (nvidia-smi's first sample arrives
+    # before the timed region starts)
+    clk = ClockSampler(local).start()
     g.step("dfsph", max(args.warmup, 1))
 
     # snapshot of the state the timed region starts from; the end-to-end run,
@@ -407,7 +423,7 @@ def run_ours(args):
     snap_vel[:] = g.get("velocity")
     g.set("position", snap_pos)  # same restaging the host-buffer path performs
     g.step("dfsph", 0)
-    clk = ClockSampler(local).start()
+    clk.wait_first()
     ms_max, st = timed_window(g, "dfsph", args.steps, stream, torch, dist, nvtx="timed_plain")
     end_pos = g.get("position")
     st_plain = st
@@ -498,8 +514,8 @@ def run_ours(args):
                               "dt": st["dt"], "status": st["status"], "neighbour_overflow": st["neighbour_overflow"]},
                 "kernels": kern, "iisph": iisph, "roofline": roof, "fp64_check": fp64, "cpu_baseline": cpu,
                 "e2e": e2e, "gpu_launches": launches, "subarms": subarms, "warm_start": warm,
-                "clocks": clk.summary("the plain and warm-start timed windows, the kernel profile and the e2e "
-                                      "replay")}
+                "clocks": clk.summary("the warm-up, the plain and warm-start timed windows, the kernel profiles "
+                                      "and the e2e replay")}
         print(json.dumps(line))
     if dist:
         dist.destroy_process_group()
