@@ -154,23 +154,49 @@ __global__ void __launch_bounds__(NT) k_pci_density(DevScene s, SolverConst c, f
     float mine = 0.f;
     if (p < n) {
         const float4 xa = s.aux4[p];
-        const int ph = phase_of(s.pos[p]);
+        const float4 pa = s.pos[p];
+        const int ph = phase_of(pa);
         const float fm0 = c.fm_ph[ph], rho0 = c.rho0_ph[ph];
         float density = ker_W(c.k, 0.f) * fm0;
         const int cnt = s.ncount[p];
+        const int ng = (cnt + 3) >> 2;
         const size_t stride = (size_t)c.stride;
-        for (int k = 0; k < cnt; ++k) {
-            bool bnd;
-            unsigned j;
-            nbr_fetch(s, (unsigned)ell_get(s.nbr, stride, p, k), bnd, j);
-            const float4 xb = bnd ? s.bpos[j] : s.aux4[j];
-            const float dis = sqrtf(dis_square_rn(xa.x, xa.y, xa.z, xb.x, xb.y, xb.z));
-            if (dis < c.hs) density += (bnd ? rho0 * xb.w : fm0) * ker_W(c.k, dis);
+        const unsigned long long polL = l2_policy(c.l2pol & 3);  // lists stream through L2
+        // four list entries per 16-byte load, the next group's issued before
+        // the current group's gathers; the sum stays in list order
+        int4 nxt = ng ? ell_group_pol(s.nbr, stride, p, 0, polL) : make_int4(0, 0, 0, 0);
+        for (int gi = 0; gi < ng; ++gi) {
+            const int4 cur = nxt;
+            if (gi + 1 < ng) nxt = ell_group_pol(s.nbr, stride, p, gi + 1, polL);
+            const unsigned e[4] = {(unsigned)cur.x, (unsigned)cur.y, (unsigned)cur.z, (unsigned)cur.w};
+            float4 xb[4];
+            bool bnd[4];
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                const unsigned u = gi * 4 + t < cnt ? e[t] : (unsigned)p;
+                unsigned j;
+                nbr_fetch(s, u, bnd[t], j);
+                xb[t] = __ldg(bnd[t] ? s.bpos + j : s.aux4 + j);
+            }
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                if (gi * 4 + t >= cnt) break;
+                const float dis = sqrtf(dis_square_rn(xa.x, xa.y, xa.z, xb[t].x, xb[t].y, xb[t].z));
+                if (dis < c.hs) density += (bnd[t] ? rho0 * xb[t].w : fm0) * ker_W(c.k, dis);
+            }
         }
         s.rho[p] = density;
         float e = density - rho0;
         if (e < 0.f) e = 0.f;  // NEGLECT_NEGATIVE_PRESSURE (SphBase.h:32)
-        s.kr[p] += delta * e;
+        const float pr = s.kr[p] + delta * e;
+        s.kr[p] = pr;
+        // the record the pressure sweep gathers per fluid neighbour:
+        // {position (w: phase bits), (p/rho^2, p/(rho/m)^2)} -- the
+        // neighbour's factors of PciSph.cpp:383-420, each a function of the
+        // neighbour alone, computed once here instead of once per pair
+        const float db = density / fm0;
+        s.prv[2 * p] = pa;
+        s.prv[2 * p + 1] = make_float4(pr / (density * density), pr / (db * db), 0.f, 0.f);
         mine = e / rho0;
     }
     // max of non-negative floats: their bit patterns order as ints (NaN and
@@ -197,34 +223,52 @@ __global__ void __launch_bounds__(NT) k_pci_pressure(DevScene s, SolverConst c, 
         const float sa = pra / (ra * ra);
         float px = 0.f, py = 0.f, pz = 0.f;
         const int cnt = s.ncount[p];
+        const int ng = (cnt + 3) >> 2;
         const size_t stride = (size_t)c.stride;
-        for (int k = 0; k < cnt; ++k) {
-            bool bnd;
-            unsigned j;
-            nbr_fetch(s, (unsigned)ell_get(s.nbr, stride, p, k), bnd, j);
-            const float4 pb = bnd ? s.bpos[j] : s.pos[j];
-            const float xx = pa.x - pb.x, xy = pa.y - pb.y, xz = pa.z - pb.z;
-            const float len2 = xx * xx + xy * xy + xz * xz;
-            if (len2 == 0.f) { ++zero; continue; }
-            const float f = grad_over_r(c.k, len2);
-            float acce;
-            if (bnd) {
-                if (!(pra > 0.f)) continue;
-                acce = f * (-rho0 * pb.w * (2.f * pra / (ra * ra)));
-            } else {
-                const float rb = s.rho[j], prb = s.kr[j];
-                const int phb = phase_of(pb);
-                if (phb == ph) {
-                    acce = f * (-fm0 * (sa + prb / (rb * rb)));
-                } else {
-                    const float fmb = c.fm_ph[phb];
-                    const float da = ra / fm0, db = rb / fmb;
-                    acce = f * (-1.f / fm0 * (pra / (da * da) + prb / (db * db)));
-                }
+        const unsigned long long polL = l2_policy(c.l2pol & 3);  // lists stream through L2
+        // one 32-byte record per fluid neighbour ({position, (rho, p)}, written
+        // by this iteration's density sweep); boundary neighbours: position
+        // and volume
+        int4 nxt = ng ? ell_group_pol(s.nbr, stride, p, 0, polL) : make_int4(0, 0, 0, 0);
+        for (int gi = 0; gi < ng; ++gi) {
+            const int4 cur = nxt;
+            if (gi + 1 < ng) nxt = ell_group_pol(s.nbr, stride, p, gi + 1, polL);
+            const unsigned e[4] = {(unsigned)cur.x, (unsigned)cur.y, (unsigned)cur.z, (unsigned)cur.w};
+            float4 pbs[4], rps[4];
+            bool bnd[4];
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                const unsigned u = gi * 4 + t < cnt ? e[t] : (unsigned)p;
+                unsigned j;
+                nbr_fetch(s, u, bnd[t], j);
+                ld_record32(bnd[t] ? s.bpv + 2 * (size_t)j : s.prv + 2 * (size_t)j, pbs[t], rps[t]);
             }
-            px = fmaf(xx, acce, px);
-            py = fmaf(xy, acce, py);
-            pz = fmaf(xz, acce, pz);
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                if (gi * 4 + t >= cnt) break;
+                const float4 pb = pbs[t];
+                const float xx = pa.x - pb.x, xy = pa.y - pb.y, xz = pa.z - pb.z;
+                const float len2 = xx * xx + xy * xy + xz * xz;
+                if (len2 == 0.f) { ++zero; continue; }
+                const float f = grad_over_r(c.k, len2);
+                float acce;
+                if (bnd[t]) {
+                    if (!(pra > 0.f)) continue;
+                    acce = f * (-rho0 * pb.w * (2.f * pra / (ra * ra)));
+                } else {
+                    // rps: (p_j / rho_j^2, p_j / (rho_j / m_j)^2)
+                    const int phb = phase_of(pb);
+                    if (phb == ph) {
+                        acce = f * (-fm0 * (sa + rps[t].x));
+                    } else {
+                        const float da = ra / fm0;
+                        acce = f * (-1.f / fm0 * (pra / (da * da) + rps[t].y));
+                    }
+                }
+                px = fmaf(xx, acce, px);
+                py = fmaf(xy, acce, py);
+                pz = fmaf(xz, acce, pz);
+            }
         }
         s.ap[p] = make_float4(px, py, pz, 0.f);
         const float4 a = s.acc[p];
