@@ -443,7 +443,13 @@ __global__ void __launch_bounds__(NT) k_ii_aii(DevScene s, SolverConst c, int ph
     const int p = blockIdx.x * NT + threadIdx.x;
     if (p >= n) return;
     const float4 pa = s.pos[p];
-    if (phase_of(pa) != phase) return;
+    // every particle's record for the sum sweep of this phase's loop:
+    // {position, (p_l, rho)} (the other phases keep their carried values)
+    s.prv[2 * p] = pa;
+    if (phase_of(pa) != phase) {
+        s.prv[2 * p + 1] = make_float4(s.cA[p].w, s.cB[p].w, 0.f, 0.f);
+        return;
+    }
     const float dt = *s.dt;
     const float fm0 = c.fm_ph[phase], rho0 = c.rho0_ph[phase];
     const float4 da = s.cB[p];  // (d_ii, rho)
@@ -476,40 +482,64 @@ __global__ void __launch_bounds__(NT) k_ii_aii(DevScene s, SolverConst c, int ph
     if (tv2 == 0.f) tv2 = 1.f;
     reinterpret_cast<float*>(s.cC + p)[3] = tv2;
     s.aux1[p] = ra + tv1;
-    reinterpret_cast<float*>(s.cA + p)[3] = (float)(0.5 * (double)s.kr[p]);
+    const float pl = (float)(0.5 * (double)s.kr[p]);
+    reinterpret_cast<float*>(s.cA + p)[3] = pl;
+    s.prv[2 * p + 1] = make_float4(pl, ra, 0.f, 0.f);
 }
 
 // sum_j d_ij p_j = -dt^2 sum_f m_k p_j / rho_j^2 gradW (IISph_M.cpp:290-313);
 // every particle also saves its p_l as the previous iterate
+// Records: prv = {position, (p_l, rho)} (written by k_ii_aii for every
+// particle, p_l updated by k_ii_press), read here per fluid neighbour in one
+// 32-byte load; this kernel writes every particle's record for k_ii_press,
+// pv = {(d_ii, previous iterate p_l), (sum_j d_ij p_j, 0)}.
 __global__ void __launch_bounds__(NT) k_ii_sum(DevScene s, SolverConst c, int phase) {
     const int n = s.st->n_active;
     const int p = blockIdx.x * NT + threadIdx.x;
     if (p >= n) return;
     const float4 pa = s.pos[p];
-    s.pl2[p] = s.cA[p].w;
-    if (phase_of(pa) != phase) return;
-    const float dt = *s.dt;
-    const float fm0 = c.fm_ph[phase];
-    float tx = 0.f, ty = 0.f, tz = 0.f;
-    const int cnt = s.ncount[p];
-    const size_t stride = (size_t)c.stride;
-    for (int k = 0; k < cnt; ++k) {
-        bool bnd;
-        unsigned j;
-        nbr_fetch(s, (unsigned)ell_get(s.nbr, stride, p, k), bnd, j);
-        if (bnd) continue;
-        const float4 pb = s.pos[j];
-        const float xx = pa.x - pb.x, xy = pa.y - pb.y, xz = pa.z - pb.z;
-        const float f = grad_over_r(c.k, xx * xx + xy * xy + xz * xz);
-        const float rb = s.cB[j].w;
-        const float q = -(fm0 * s.cA[j].w) / (rb * rb) * f;
-        tx = fmaf(xx, q, tx);
-        ty = fmaf(xy, q, ty);
-        tz = fmaf(xz, q, tz);
+    const float pla = s.cA[p].w;
+    s.pl2[p] = pla;
+    const float4 db = s.cB[p];
+    float4 cc = s.cC[p];
+    if (phase_of(pa) == phase) {
+        const float dt = *s.dt;
+        const float fm0 = c.fm_ph[phase];
+        float tx = 0.f, ty = 0.f, tz = 0.f;
+        const int cnt = s.ncount[p];
+        const int ng = (cnt + 3) >> 2;
+        const size_t stride = (size_t)c.stride;
+        const unsigned long long polL = l2_policy(c.l2pol & 3);  // lists stream through L2
+        int4 nxt = ng ? ell_group_pol(s.nbr, stride, p, 0, polL) : make_int4(0, 0, 0, 0);
+        for (int gi = 0; gi < ng; ++gi) {
+            const int4 cur = nxt;
+            if (gi + 1 < ng) nxt = ell_group_pol(s.nbr, stride, p, gi + 1, polL);
+            const unsigned e[4] = {(unsigned)cur.x, (unsigned)cur.y, (unsigned)cur.z, (unsigned)cur.w};
+            float4 pb[4], rb[4];
+            bool use[4];
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                // boundary neighbours add nothing here: they read the own record
+                use[t] = gi * 4 + t < cnt && !(e[t] & BND_FLAG);
+                ld_record32(s.prv + 2 * (size_t)(use[t] ? e[t] : (unsigned)p), pb[t], rb[t]);
+            }
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                if (!use[t]) continue;
+                const float xx = pa.x - pb[t].x, xy = pa.y - pb[t].y, xz = pa.z - pb[t].z;
+                const float f = grad_over_r(c.k, xx * xx + xy * xy + xz * xz);
+                const float q = -(fm0 * rb[t].x) / (rb[t].y * rb[t].y) * f;
+                tx = fmaf(xx, q, tx);
+                ty = fmaf(xy, q, ty);
+                tz = fmaf(xz, q, tz);
+            }
+        }
+        const float dt2 = dt * dt;
+        cc = make_float4(tx * dt2, ty * dt2, tz * dt2, cc.w);
+        s.cC[p] = cc;
     }
-    const float dt2 = dt * dt;
-    const float4 cc = s.cC[p];
-    s.cC[p] = make_float4(tx * dt2, ty * dt2, tz * dt2, cc.w);
+    s.pv[2 * p] = make_float4(db.x, db.y, db.z, pla);
+    s.pv[2 * p + 1] = make_float4(cc.x, cc.y, cc.z, 0.f);
 }
 
 // relaxed Jacobi update (IISph_M.cpp:315-351) and the loop decision (:352-358)
@@ -530,24 +560,42 @@ __global__ void __launch_bounds__(NT) k_ii_press(DevScene s, SolverConst c, int 
             const float qd = dt * dt * fm0 / (ra * ra);
             float ft = 0.f;
             const int cnt = s.ncount[p];
+            const int ng = (cnt + 3) >> 2;
             const size_t stride = (size_t)c.stride;
-            for (int k = 0; k < cnt; ++k) {
-                bool bnd;
-                unsigned j;
-                nbr_fetch(s, (unsigned)ell_get(s.nbr, stride, p, k), bnd, j);
-                const float4 pb = bnd ? s.bpos[j] : s.pos[j];
-                const float xx = pa.x - pb.x, xy = pa.y - pb.y, xz = pa.z - pb.z;
-                const float f = grad_over_r(c.k, xx * xx + xy * xy + xz * xz);
-                const float g0 = xx * f, g1 = xy * f, g2 = xz * f;
-                if (bnd) {
-                    ft += (rho0 * pb.w) * (ca.x * g0 + ca.y * g1 + ca.z * g2);
-                } else {
-                    const float4 db = s.cB[j], sb = s.cC[j];
-                    const float plb = s.pl2[j];
-                    const float t0 = (ca.x - db.x * plb) - (sb.x - g0 * qd * pla);
-                    const float t1 = (ca.y - db.y * plb) - (sb.y - g1 * qd * pla);
-                    const float t2 = (ca.z - db.z * plb) - (sb.z - g2 * qd * pla);
-                    ft += fm0 * (t0 * g0 + t1 * g1 + t2 * g2);
+            const unsigned long long polL = l2_policy(c.l2pol & 3);  // lists stream through L2
+            // per fluid neighbour: its position and its k_ii_sum record
+            // {(d_jj, previous p_l), (sum_k d_jk p_k, 0)}; boundary: position
+            // and volume
+            int4 nxt = ng ? ell_group_pol(s.nbr, stride, p, 0, polL) : make_int4(0, 0, 0, 0);
+            for (int gi = 0; gi < ng; ++gi) {
+                const int4 cur = nxt;
+                if (gi + 1 < ng) nxt = ell_group_pol(s.nbr, stride, p, gi + 1, polL);
+                const unsigned e[4] = {(unsigned)cur.x, (unsigned)cur.y, (unsigned)cur.z, (unsigned)cur.w};
+                float4 pb[4], db[4], sb[4];
+                bool bnd[4];
+#pragma unroll
+                for (int t = 0; t < 4; ++t) {
+                    const unsigned u = gi * 4 + t < cnt ? e[t] : (unsigned)p;
+                    unsigned j;
+                    nbr_fetch(s, u, bnd[t], j);
+                    pb[t] = __ldg(bnd[t] ? s.bpos + j : s.pos + j);
+                    ld_record32(s.pv + 2 * (size_t)(bnd[t] ? (unsigned)p : j), db[t], sb[t]);
+                }
+#pragma unroll
+                for (int t = 0; t < 4; ++t) {
+                    if (gi * 4 + t >= cnt) break;
+                    const float xx = pa.x - pb[t].x, xy = pa.y - pb[t].y, xz = pa.z - pb[t].z;
+                    const float f = grad_over_r(c.k, xx * xx + xy * xy + xz * xz);
+                    const float g0 = xx * f, g1 = xy * f, g2 = xz * f;
+                    if (bnd[t]) {
+                        ft += (rho0 * pb[t].w) * (ca.x * g0 + ca.y * g1 + ca.z * g2);
+                    } else {
+                        const float plb = db[t].w;
+                        const float t0 = (ca.x - db[t].x * plb) - (sb[t].x - g0 * qd * pla);
+                        const float t1 = (ca.y - db[t].y * plb) - (sb[t].y - g1 * qd * pla);
+                        const float t2 = (ca.z - db[t].z * plb) - (sb[t].z - g2 * qd * pla);
+                        ft += fm0 * (t0 * g0 + t1 * g1 + t2 * g2);
+                    }
                 }
             }
             const float aii = ca.w, radv = s.aux1[p];
@@ -561,6 +609,7 @@ __global__ void __launch_bounds__(NT) k_ii_press(DevScene s, SolverConst c, int 
             }
             reinterpret_cast<float*>(s.cA + p)[3] = t;
             s.kr[p] = t;
+            s.prv[2 * p + 1] = make_float4(t, ra, 0.f, 0.f);  // the next sum sweep's p_l
         }
     }
     __shared__ double sh[NT / 32];
