@@ -1733,12 +1733,21 @@ int sphgpu_step_host(sphgpu_t h, int solver, const float* xyz, const float* vel,
     if (spec) {
         DevScene& d = h->d;
         const size_t b3 = sizeof(float) * 3 * (size_t)h->cap;
-        if (!h->in_xyz && (cudaMalloc((void**)&h->in_xyz, b3) != cudaSuccess ||
-                           cudaMalloc((void**)&h->in_vel, b3) != cudaSuccess ||
-                           cudaMalloc((void**)&h->d_diff, sizeof(int)) != cudaSuccess ||
-                           cudaMallocHost((void**)&h->h_diff, sizeof(int)) != cudaSuccess)) {
-            h->err = "out of device memory (host-step input buffers)";
-            return SPHGPU_ENOMEM;
+        if (!h->h_diff) {
+            // all four or none: a partial allocation is released again
+            if (cudaMalloc((void**)&h->in_xyz, b3) != cudaSuccess ||
+                cudaMalloc((void**)&h->in_vel, b3) != cudaSuccess ||
+                cudaMalloc((void**)&h->d_diff, sizeof(int)) != cudaSuccess ||
+                cudaMallocHost((void**)&h->h_diff, sizeof(int)) != cudaSuccess) {
+                for (void* q : {(void*)h->in_xyz, (void*)h->in_vel, (void*)h->d_diff})
+                    if (q) cudaFree(q);
+                h->in_xyz = h->in_vel = nullptr;
+                h->d_diff = nullptr;
+                h->h_diff = nullptr;
+                cudaGetLastError();  // the failed allocation's error, reported here instead
+                h->err = "out of device memory (host-step input buffers)";
+                return SPHGPU_ENOMEM;
+            }
         }
         cudaStream_t s4 = h->stream4;
         CK(cudaEventRecord(h->ev_in[0], h->stream));
