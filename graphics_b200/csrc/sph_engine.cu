@@ -2874,6 +2874,16 @@ int sphgpu_get_solid_force(sphgpu_t h, int solid_id, double force[3], double tor
     return 0;
 }
 
+// Test and measurement switches (not part of the drop-in interface):
+//   use_graphs             0: host-driven loops, each kernel its own launch
+//   record_kappa_sum       sum the density loop's kappa per particle
+//   reset_kappa_sum        clear that sum
+//   carveout_sweeps/_build preferred L1/shared split of the sweeps / list build
+//   l2_policy              L2 eviction priorities of the sweeps' list and record loads
+//   fuse_div               DFSPH: the list build runs the divergence loop's first sweep A
+//   fuse_ws                warm start: feature gather and network in one kernel
+//   speculative_host_step  sphgpu_step_host runs part 1 while checking its inputs
+//   wc_lanes               WCSPH threads per particle (0 by size, 1, 4)
 int sphgpu_debug_set(sphgpu_t h, const char* key, int value) {
     if (!h || !key) return SPHGPU_EINVAL;
     std::string k(key);
