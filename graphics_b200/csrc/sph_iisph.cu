@@ -371,7 +371,7 @@ __global__ void __launch_bounds__(BS) k_iv_sweep_b(DevScene s, SolverConst c, in
             const int ng = (cnt + 3) >> 2;
             const size_t stride = (size_t)c.stride;
             const unsigned long long polL = l2_policy(c.l2pol & 3);  // lists stream through L2
-    int4 nxt = ng ? ell_group_pol(s.nbr, stride, p, 0, polL) : make_int4(0, 0, 0, 0);
+            int4 nxt = ng ? ell_group_pol(s.nbr, stride, p, 0, polL) : make_int4(0, 0, 0, 0);
             for (int gi = 0; gi < ng; ++gi) {
                 const int4 cur = nxt;
                 if (gi + 1 < ng) nxt = ell_group_pol(s.nbr, stride, p, gi + 1, polL);
