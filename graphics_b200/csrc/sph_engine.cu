@@ -523,7 +523,7 @@ int enq_df_density_loop(sphgpu_scene* h, bool capturing) {
         });
         if (h->nscenes > 1)
             launch(h, "batch_decide", st, [&] {
-                launch_batch_decide(d, h->c, 0, h->nscenes, 0.0, P.df_density_goal, P.df_density_min_iter,
+                launch_batch_decide(d, h->c, 0, h->nscenes, h->cap, 0.0, P.df_density_goal, P.df_density_min_iter,
                                     P.df_density_max_iter, hd, use, st);
             });
     });
@@ -546,7 +546,7 @@ int enq_df_div_loop(sphgpu_scene* h, bool capturing, bool fused = false) {
         div_b(st, hd, use);
         if (h->nscenes > 1)
             launch(h, "batch_decide", st, [&] {
-                launch_batch_decide(d, h->c, 1, h->nscenes, P.df_div_goal_abs, P.df_div_goal_rel, P.df_div_min_iter,
+                launch_batch_decide(d, h->c, 1, h->nscenes, h->cap, P.df_div_goal_abs, P.df_div_goal_rel, P.df_div_min_iter,
                                     P.df_div_max_iter, hd, use, st);
             });
     };
@@ -594,7 +594,7 @@ int enq_df_part1(sphgpu_scene* h, bool capturing) {
     if (dyn && !(h->mlp && h->ws_mode)) cudaMemsetAsync(d.ksum, 0, sizeof(float) * h->cap, st);
     if (h->P.cfl && h->nscenes > 1)
         launch(h, "cfl", st, [&] {
-            launch_batch_cfl(d, h->nscenes, h->P.cfl_factor, h->P.particle_d, h->P.dt_max, h->P.dt_min, st);
+            launch_batch_cfl(d, h->nscenes, h->cap, h->P.cfl_factor, h->P.particle_d, h->P.dt_max, h->P.dt_min, st);
         });
     else if (h->P.cfl)
         launch(h, "cfl", st, [&] { launch_cfl(d, h->cap, h->P.cfl_factor, h->P.particle_d, h->P.dt_max, h->P.dt_min, st); });
@@ -1343,7 +1343,7 @@ static int create_impl(const SphParams* p, int device, int max_fluid, int nscene
     if (!r && nscenes > 1) {
         // per-scene state: grids, then one block for the BatchDev arrays
         const size_t S = (size_t)nscenes;
-        const size_t bytes = S * (sizeof(float) + 7 * sizeof(int) + 3 * sizeof(double)) + 256;
+        const size_t bytes = S * (sizeof(float) + 9 * sizeof(int) + 3 * sizeof(double)) + 256 + sizeof(int);
         if (cudaMalloc((void**)&h->d_geom, S * sizeof(GridGeom)) != cudaSuccess ||
             cudaMalloc(&h->d_batch, bytes) != cudaSuccess) {
             r = SPHGPU_ENOMEM;
@@ -1362,6 +1362,8 @@ static int create_impl(const SphParams* p, int device, int max_fluid, int nscene
             b.total_it_density = (int*)q; q += S * sizeof(int);
             b.total_it_div = (int*)q; q += S * sizeof(int);
             b.n = (int*)q; q += S * sizeof(int);
+            b.sticket = (unsigned*)q; q += S * sizeof(unsigned);
+            b.chunk0 = (int*)q; q += (S + 1) * sizeof(int);
             b.status = (unsigned*)q;
             b.geom = h->d_geom;
             std::vector<float> dts(S, p->dt);

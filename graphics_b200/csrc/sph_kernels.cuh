@@ -48,7 +48,13 @@ struct BatchDev {
     double* err_density;   // [nscenes]
     double* err_div;
     double* vmax;
+    // per-scene reductions in chunks of BATCH_CHUNK particles: chunk0[sc]
+    // is the scene's first chunk (exclusive prefix, chunk0[nscenes] the
+    // total), sticket[sc] counts the scene's finished chunks
+    int* chunk0;           // [nscenes + 1]
+    unsigned* sticket;     // [nscenes]
 };
+constexpr int BATCH_CHUNK = 4096;
 
 // Per-scene device pointers passed to every kernel by value.
 struct DevScene {
@@ -255,10 +261,12 @@ void launch_call_begin(const DevScene& s, cudaStream_t st);
 
 // ---- batch of scenes (sph_batch.cu) ----
 void launch_batch_loop_reset(const DevScene& s, int nscenes, int which, cudaStream_t st);
-void launch_batch_decide(const DevScene& s, const SolverConst& c, int which, int nscenes, double goal_abs,
+// n_cap: particle capacity (bounds the number of chunks)
+void launch_batch_decide(const DevScene& s, const SolverConst& c, int which, int nscenes, int n_cap, double goal_abs,
                          double goal_rel, int min_it, int max_it, unsigned long long cond_handle, int use_handle,
                          cudaStream_t st);
-void launch_batch_cfl(const DevScene& s, int nscenes, float cfl, float d, float dt_max, float dt_min, cudaStream_t st);
+void launch_batch_cfl(const DevScene& s, int nscenes, int n_cap, float cfl, float d, float dt_max, float dt_min,
+                      cudaStream_t st);
 void launch_batch_call_begin(const DevScene& s, int nscenes, cudaStream_t st);
 void launch_batch_count(const DevScene& s, int nscenes, cudaStream_t st);
 
