@@ -401,22 +401,34 @@ void launch_df_div_b(const DevScene& s, const SolverConst& c, int n_max, double 
     DISPATCH_BS(bs, (k_df_vupdate<B, 1, 1><<<nblk(n_max, B), B, 0, st>>>(
                         s, c, goal_abs, goal_rel, min_it, max_it, (cudaGraphConditionalHandle)cond_handle, use_handle)));
 }
+// every block-size instantiation of the per-neighbour sweep kernels
+template <int B, class F>
+static void each_sweep_kernel_bs(F f) {
+    f((const void*)k_df_forces<B>);
+    f((const void*)k_df_dens_a<B>);
+    f((const void*)k_df_div_a<B>);
+    f((const void*)k_df_vupdate<B, 0, 1>);
+    f((const void*)k_df_vupdate<B, 0, 0>);
+    f((const void*)k_df_vupdate<B, 1, 1>);
+}
+template <class F>
+static void each_sweep_kernel(F f) {
+    each_sweep_kernel_bs<64>(f);
+    each_sweep_kernel_bs<128>(f);
+    each_sweep_kernel_bs<256>(f);
+}
 // preferred shared-memory carveout (percent of the unified L1/shared
 // storage; -1 = the driver's choice) of the per-neighbour sweep kernels
-template <int B>
-static void sweep_carveout_bs(int pct) {
-    const cudaFuncAttribute a = cudaFuncAttributePreferredSharedMemoryCarveout;
-    cudaFuncSetAttribute(k_df_forces<B>, a, pct);
-    cudaFuncSetAttribute(k_df_dens_a<B>, a, pct);
-    cudaFuncSetAttribute(k_df_div_a<B>, a, pct);
-    cudaFuncSetAttribute(k_df_vupdate<B, 0, 1>, a, pct);
-    cudaFuncSetAttribute(k_df_vupdate<B, 0, 0>, a, pct);
-    cudaFuncSetAttribute(k_df_vupdate<B, 1, 1>, a, pct);
-}
 void set_sweep_carveout(int pct) {
-    sweep_carveout_bs<64>(pct);
-    sweep_carveout_bs<128>(pct);
-    sweep_carveout_bs<256>(pct);
+    each_sweep_kernel([&](const void* k) { cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, pct); });
+}
+// loads every instantiation now (the runtime loads a kernel at its first
+// launch, which would land inside the autotuner's first timed candidate)
+void preload_sweep_kernels() {
+    each_sweep_kernel([](const void* k) {
+        cudaFuncAttributes a;
+        cudaFuncGetAttributes(&a, k);
+    });
 }
 void launch_cfl(const DevScene& s, int n_max, float cfl, float d, float dt_max, float dt_min, cudaStream_t st) {
     k_cfl<<<nblk(n_max, NT * CFL_ITEMS), NT, 0, st>>>(s, cfl, d, dt_max, dt_min);

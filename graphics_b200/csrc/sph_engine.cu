@@ -535,26 +535,27 @@ int enq_df_div_loop(sphgpu_scene* h, bool capturing, bool fused = false) {
     const SphParams& P = h->P;
     launch_df_loop_reset(d, 1, h->stream);
     if (h->nscenes > 1) launch_batch_loop_reset(d, h->nscenes, 1, h->stream);
+    // the velocity update and, for a batch, the per-scene decisions
     auto div_b = [&](cudaStream_t st, unsigned long long hd, int use) {
         launch(h, "df_div_b", st, [&] {
             launch_df_div_b(d, h->c, h->cap, P.df_div_goal_abs, P.df_div_goal_rel, P.df_div_min_iter,
                             P.df_div_max_iter, hd, use, st, h->tune.sweep_b);
         });
-    };
-    auto body = [&](cudaStream_t st, unsigned long long hd, int use) {
-        launch(h, "df_div_a", st, [&] { launch_df_div_a(d, h->c, h->cap, st, h->tune.sweep_a); });
-        div_b(st, hd, use);
         if (h->nscenes > 1)
             launch(h, "batch_decide", st, [&] {
                 launch_batch_decide(d, h->c, 1, h->nscenes, h->cap, P.df_div_goal_abs, P.df_div_goal_rel, P.df_div_min_iter,
                                     P.df_div_max_iter, hd, use, st);
             });
     };
+    auto body = [&](cudaStream_t st, unsigned long long hd, int use) {
+        launch(h, "df_div_a", st, [&] { launch_df_div_a(d, h->c, h->cap, st, h->tune.sweep_a); });
+        div_b(st, hd, use);
+    };
     return enq_loop(h, capturing, body, div_b, fused);
 }
 
-// the list build runs the divergence loop's first sweep A (single scenes)
-bool fused_div(const sphgpu_scene* h) { return h->fuse_div && h->nscenes <= 1; }
+// the list build runs the divergence loop's first sweep A
+bool fused_div(const sphgpu_scene* h) { return h->fuse_div != 0; }
 
 // The body of one DFSPH step after the first neighbour search
 // (DFSPH::sphStep, DFSPH.cpp:52-62), with the learned warm start when a
@@ -2635,6 +2636,8 @@ int sphgpu_autotune(sphgpu_t h, int solver, int steps_per_candidate, char* repor
     if (!h || steps_per_candidate <= 0) return SPHGPU_EINVAL;
     if (solver != SPHGPU_DFSPH) { h->err = "the autotuner covers the DFSPH step"; return SPHGPU_ENOTIMPL; }
     cudaSetDevice(h->device);
+    preload_sweep_kernels();
+    preload_build_kernels();
     const int cands[3] = {64, 128, 256};
     const char* cls[4] = {"forces", "sweep_a", "sweep_b", "build"};
     double best_t[4] = {1e30, 1e30, 1e30, 1e30};
@@ -2658,7 +2661,7 @@ int sphgpu_autotune(sphgpu_t h, int solver, int steps_per_candidate, char* repor
             return n ? t / n : 1e30;
         };
         const double t[4] = {avg({"df_forces"}), avg({"df_density_a", "df_div_a"}), avg({"df_density_b", "df_div_b"}),
-                             avg({"build_first"})};
+                             avg({"build_first", "build_first_div"})};
         char buf[256];
         snprintf(buf, sizeof buf, "%s\"%d\": {\"forces\": %.2f, \"sweep_a\": %.2f, \"sweep_b\": %.2f, \"build\": %.2f}",
                  ci ? ", " : "", b, 1e3 * t[0], 1e3 * t[1], 1e3 * t[2], 1e3 * t[3]);

@@ -284,7 +284,7 @@ __global__ void __launch_bounds__(BS) k_build(DevScene s, GridGeom g, SolverCons
                 s.alpha[p] = alpha;
                 if (MODE == 4) {
                     // the divergence loop's first sweep A, as k_df_div_a
-                    const float dt = *s.dt;
+                    const float dt = dt_of(s, pa);
                     float dd = dacc;
                     if (dd < 0.f || (density + dd * dt) < c.rho0) dd = 0.f;  // DFSPH.cpp:829-832
                     const float kv = dd * alpha / dt;                         // DFSPH.cpp:835
@@ -311,8 +311,9 @@ __global__ void __launch_bounds__(BS) k_build(DevScene s, GridGeom g, SolverCons
         if (ov) { atomicAdd(&s.st->overflow, ov); atomicOr(&s.st->status, 8u); }
         if (mx) atomicMax(&s.st->max_nbrs, mx);
     }
-    if (MODE == 4) {
-        // mean Drho/Dt of the iteration (k_df_div_a's FP64 error)
+    if (MODE == 4 && s.nscenes <= 1) {
+        // mean Drho/Dt of the iteration (k_df_div_a's FP64 error; a batch
+        // reduces per scene in k_batch_decide)
         __shared__ double shd[BS / 32];
         const double bsum = block_sum_double<BS>(ddiv, shd);
         double t;
@@ -607,21 +608,32 @@ static void launch_build_bs(const DevScene& s, const GridGeom& g, const SolverCo
     else launch_build_st<BS, false>(s, g, c, mode, nb, st);
 }
 
-template <int BS>
-static void build_carveout_bs(int pct) {
-    const cudaFuncAttribute a = cudaFuncAttributePreferredSharedMemoryCarveout;
-    cudaFuncSetAttribute(k_build<1, BS, true>, a, pct);
-    cudaFuncSetAttribute(k_build<1, BS, false>, a, pct);
-    cudaFuncSetAttribute(k_build<4, BS, true>, a, pct);
-    cudaFuncSetAttribute(k_build<4, BS, false>, a, pct);
+// every block-size instantiation of the DFSPH list build (modes 1 and 4)
+template <int BS, class F>
+static void each_build_kernel_bs(F f) {
+    f((const void*)k_build<1, BS, true>);
+    f((const void*)k_build<1, BS, false>);
+    f((const void*)k_build<4, BS, true>);
+    f((const void*)k_build<4, BS, false>);
+}
+template <class F>
+static void each_build_kernel(F f) {
+    each_build_kernel_bs<64>(f);
+    each_build_kernel_bs<128>(f);
+    each_build_kernel_bs<256>(f);
 }
 // preferred shared-memory carveout of the DFSPH list build (percent; -1 =
 // the driver's choice): the staged rows take shared memory from the L1 that
 // caches the candidates' records
 void set_build_carveout(int pct) {
-    build_carveout_bs<64>(pct);
-    build_carveout_bs<128>(pct);
-    build_carveout_bs<256>(pct);
+    each_build_kernel([&](const void* k) { cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, pct); });
+}
+// loads every instantiation now (see preload_sweep_kernels)
+void preload_build_kernels() {
+    each_build_kernel([](const void* k) {
+        cudaFuncAttributes a;
+        cudaFuncGetAttributes(&a, k);
+    });
 }
 
 void launch_build(const DevScene& s, const GridGeom& g, const SolverConst& c, int mode, int n_max, cudaStream_t st,

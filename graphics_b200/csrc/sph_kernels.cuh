@@ -233,6 +233,8 @@ void launch_state_check(const float* xyz3, const float* vel3, const int* gid, in
                         const float4* vel, int* differs, cudaStream_t st);
 void set_sweep_carveout(int pct);
 void set_build_carveout(int pct);
+void preload_sweep_kernels();
+void preload_build_kernels();
 void launch_from_ref_order(const float* src3, const int* gid, int n, float4* dst, cudaStream_t st);
 // host state (reference order) into a sorted state with valid lists:
 // velocities copied in, *changed set when a position differs

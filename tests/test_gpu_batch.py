@@ -41,6 +41,24 @@ def test_batch_matches_single_scenes():
     b.close()
 
 
+@pytest.mark.parametrize("graphs", [1, 0])
+def test_batch_fused_divergence_sweep_identical_to_separate(graphs):
+    # the list build's fused first divergence sweep in a batch (per-scene dt,
+    # per-scene decisions) against the separate sweep A launch
+    out = []
+    for fused in (1, 0):
+        b = batch_to_gpu(_scenes(), **KW)
+        b.debug_set("use_graphs", graphs)
+        b.debug_set("fuse_div", fused)
+        b.step("dfsph", 5)
+        its = [(s["total_iter_divergence"], s["total_iter_density"]) for s in b.scene_stats()]
+        out.append((b.get("position"), b.get("velocity"), b.get("DFkappaV"), its))
+        b.close()
+    for a, c in zip(out[0][:3], out[1][:3]):
+        np.testing.assert_array_equal(a, c)
+    assert out[0][3] == out[1][3]
+
+
 def test_batch_scenes_converge_independently():
     """Scenes of different sizes need different iteration counts: each
     stops at its own goal (the loop runs while any scene is active)."""
@@ -67,6 +85,10 @@ def test_autotune_picks_block_sizes_and_keeps_results():
     rep = g1.autotune("dfsph", 1)
     assert set(rep["chosen"]) == {"forces", "sweep_a", "sweep_b", "build"}
     assert all(v in (64, 128, 256) for v in rep["chosen"].values())
+    # every kernel class was timed at every candidate (the list build under
+    # either of its DFSPH names, with or without the fused divergence sweep)
+    for cand in rep["candidates"].values():
+        assert all(0 < t < 1e6 for t in cand.values()), cand
     g2.step("dfsph", 3)  # g1 advanced 3 steps while tuning
     s1, s2 = g1.step("dfsph", 4), g2.step("dfsph", 4)
     assert s1["total_iter_density"] == s2["total_iter_density"]
