@@ -134,7 +134,8 @@ constexpr int LROW = 52;
 // clamp, kappa_v, the FP64 error sum) -- every neighbour's 32-byte
 // {position, velocity} record is gathered once for both, and the loop then
 // starts with its velocity update (the per-pair term is div_term, the one the
-// separate sweep uses, so the results are the same bit for bit).
+// separate sweep uses, so the results are the same bit for bit); 5: mode 4 in
+// a batch (each scene's own dt; the loop decisions reduce per scene).
 //
 // STAGED (cap <= 48): a kept neighbour is one predicated shared-memory store
 // into the thread's row -- no divergent branch around a global store in the
@@ -143,6 +144,7 @@ constexpr int LROW = 52;
 // memory.  Otherwise entries go straight to the global ELL list.
 template <int MODE, int BS, bool STAGED>
 __global__ void __launch_bounds__(BS) k_build(DevScene s, GridGeom g, SolverConst c) {
+    constexpr bool DIV = MODE == 4 || MODE == 5;  // the fused first divergence sweep
     extern __shared__ int4 list_smem[];
     int* const row = reinterpret_cast<int*>(list_smem) + (STAGED ? threadIdx.x * LROW : 0);
     const int n = s.st->n_active;
@@ -250,23 +252,23 @@ __global__ void __launch_bounds__(BS) k_build(DevScene s, GridGeom g, SolverCons
             float density = ker_W(c.k, 0.f) * fm0;
             float a1x = 0.f, a1y = 0.f, a1z = 0.f, a2 = 0.f;
             float dacc = 0.f;  // MODE 4: the divergence sum
-            const float4 va = MODE == 4 ? s.pv[2 * p + 1] : make_float4(0.f, 0.f, 0.f, 0.f);
+            const float4 va = DIV ? s.pv[2 * p + 1] : make_float4(0.f, 0.f, 0.f, 0.f);
             for (int k = 0; k < cnt; ++k) {
                 const unsigned e = STAGED ? (unsigned)row[k] : (unsigned)out[ell_index(stride, p, k)];
                 const bool bnd = (e & BND_FLAG) != 0u;
                 float4 pb, vb;
                 // pv / bpv hold {the position (boundary: with its volume) of
                 // pos / bpos, the velocity}
-                if (MODE == 4) ld_record32((bnd ? s.bpv : s.pv) + 2 * (size_t)(e & BND_MASK), pb, vb);
+                if (DIV) ld_record32((bnd ? s.bpv : s.pv) + 2 * (size_t)(e & BND_MASK), pb, vb);
                 else pb = __ldg((bnd ? BP : P) + (e & BND_MASK));
-                if (MODE == 4) dacc = div_term(c, pa, va, pb, vb, bnd, dacc);
+                if (DIV) dacc = div_term(c, pa, va, pb, vb, bnd, dacc);
                 const float xx = pa.x - pb.x, xy = pa.y - pb.y, xz = pa.z - pb.z;
                 const float len2 = dis_square_rn(pa.x, pa.y, pa.z, pb.x, pb.y, pb.z);
                 float w, f;
                 kernel_pair(c.k, len2, w, f);
                 const float m = bnd ? rho0 * pb.w : fm0;
                 density = fmaf(m, w, density);
-                if (MODE == 1 || MODE == 4) {
+                if (MODE == 1 || DIV) {
                     const float fm = f * m;
                     a1x = fmaf(xx, fm, a1x);
                     a1y = fmaf(xy, fm, a1y);
@@ -275,16 +277,16 @@ __global__ void __launch_bounds__(BS) k_build(DevScene s, GridGeom g, SolverCons
                     a2 = fmaf(t, t, a2);
                 }
             }
-            if (MODE == 1 || MODE == 4) {
+            if (MODE == 1 || DIV) {
                 s.rho[p] = density;
                 s.prv[2 * p] = make_float4(pa.x, pa.y, pa.z, density);
                 float al = a1x * a1x + a1y * a1y + a1z * a1z + a2;
                 if (al < 1.0e-6f) al = 1.0e-6f;
                 const float alpha = density / al;
                 s.alpha[p] = alpha;
-                if (MODE == 4) {
+                if (DIV) {
                     // the divergence loop's first sweep A, as k_df_div_a
-                    const float dt = dt_of(s, pa);
+                    const float dt = MODE == 5 ? s.b.dt[scene_of(pa)] : *s.dt;
                     float dd = dacc;
                     if (dd < 0.f || (density + dd * dt) < c.rho0) dd = 0.f;  // DFSPH.cpp:829-832
                     const float kv = dd * alpha / dt;                         // DFSPH.cpp:835
@@ -311,9 +313,9 @@ __global__ void __launch_bounds__(BS) k_build(DevScene s, GridGeom g, SolverCons
         if (ov) { atomicAdd(&s.st->overflow, ov); atomicOr(&s.st->status, 8u); }
         if (mx) atomicMax(&s.st->max_nbrs, mx);
     }
-    if (MODE == 4 && s.nscenes <= 1) {
-        // mean Drho/Dt of the iteration (k_df_div_a's FP64 error; a batch
-        // reduces per scene in k_batch_decide)
+    if (MODE == 4) {
+        // mean Drho/Dt of the iteration (k_df_div_a's FP64 error; a batch,
+        // mode 5, reduces per scene in k_batch_decide)
         __shared__ double shd[BS / 32];
         const double bsum = block_sum_double<BS>(ddiv, shd);
         double t;
@@ -594,6 +596,7 @@ static void launch_build_st(const DevScene& s, const GridGeom& g, const SolverCo
     if (mode == 0) k_build<0, BS, STAGED><<<nb, BS, sm, st>>>(s, g, c);
     else if (mode == 1) k_build<1, BS, STAGED><<<nb, BS, sm, st>>>(s, g, c);
     else if (mode == 2) k_build<2, BS, STAGED><<<nb, BS, sm, st>>>(s, g, c);
+    else if (mode == 4 && s.nscenes > 1) k_build<5, BS, STAGED><<<nb, BS, sm, st>>>(s, g, c);
     else if (mode == 4) k_build<4, BS, STAGED><<<nb, BS, sm, st>>>(s, g, c);
     else k_build<3, BS, STAGED><<<nb, BS, sm, st>>>(s, g, c);
 }
@@ -615,6 +618,8 @@ static void each_build_kernel_bs(F f) {
     f((const void*)k_build<1, BS, false>);
     f((const void*)k_build<4, BS, true>);
     f((const void*)k_build<4, BS, false>);
+    f((const void*)k_build<5, BS, true>);
+    f((const void*)k_build<5, BS, false>);
 }
 template <class F>
 static void each_build_kernel(F f) {

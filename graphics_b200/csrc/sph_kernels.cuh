@@ -223,7 +223,8 @@ void launch_scatter_reorder(const DevScene& s, const GridGeom& g, int n_old, int
 void launch_count_active(const DevScene& s, const GridGeom& g, cudaStream_t st);
 // mode 0: lists only; 1: lists + DFSPH rho/alpha; 2: lists + WCSPH rho/pressure;
 // 3: lists + IISph VF_prepareAttribute / sphDensity (ivs); 4: mode 1 + the
-// divergence loop's first sweep A (Drho/Dt, kappa_v, FP64 error)
+// divergence loop's first sweep A (Drho/Dt, kappa_v, and for a single scene
+// the FP64 error; a batch runs it with each scene's dt)
 void launch_build(const DevScene& s, const GridGeom& g, const SolverConst& c, int mode, int n_max, cudaStream_t st,
                   int bs = 128);
 void launch_to_ref_order(const float4* src, const int* gid, int n, float* dst3, cudaStream_t st);
