@@ -640,7 +640,9 @@ int enq_df_part2(sphgpu_scene* h, bool capturing) {
     // leaves every carried per-particle array as it found it: a speculative
     // host step may run part 1 again)
     const int ws = h->mlp ? h->ws_mode : 0;
-    if (ws) {
+    // with a network applied (no recording) the hash kernel writes the history
+    const int ws_in_hash = ws == 1 ? 4 : 0;
+    if (ws && !ws_in_hash) {
         launch(h, "ws_post", st, [&] { launch_ws_post(d, h->c, ws == 2 ? h->recY : nullptr, h->cap, st); });
         if (ws == 2) {
             sphgpu_mlp* m = h->mlp;
@@ -651,7 +653,7 @@ int enq_df_part2(sphgpu_scene* h, bool capturing) {
     enq_boundary_update(h, st);
     const int vort = h->P.enable_vortex ? 2 : 0;  // carry cA (w or n0) through the sort
     const bool fused = fused_div(h);
-    enq_ns(h, 1 | vort, fused ? 4 : 1, st, 1 | vort);
+    enq_ns(h, 1 | vort | ws_in_hash, fused ? 4 : 1, st, 1 | vort);
     int r = enq_df_div_loop(h, capturing, fused);
     if (r) return r;
     if (h->P.enable_vortex == 3)

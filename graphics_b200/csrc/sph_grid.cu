@@ -44,7 +44,16 @@ __global__ void __launch_bounds__(NT) k_hash(DevScene s, GridGeom g, int integra
             s.pos_s[i] = p;
             s.vel_s[i] = v;
             s.gid_s[i] = s.gid[i];
-            s.hist_s[i] = s.hist[i];
+            if (integrate & 4) {
+                // the learned warm start's history of this step (as k_ws_post):
+                // the step's kappa sum with the applied prediction, and the
+                // step's (predicted error, divergence term); the sum restarts
+                const float2 w = s.wsbuf[i];
+                s.hist_s[i] = make_float4(s.ksum[i] + s.kwarm[i], w.x, w.y, 0.f);
+                s.ksum[i] = 0.f;
+            } else {
+                s.hist_s[i] = s.hist[i];
+            }
             if (integrate & 2) s.cA_s[i] = s.cA[i];  // DFSPH vorticity state carried through the sort
         } else {
             p = s.pos_s[i];

@@ -217,6 +217,8 @@ __device__ __forceinline__ float div_term(const SolverConst& c, float4 pa, float
 }
 
 // ---- neighbour search (sph_grid.cu) ----
+// integrate: bit 0 the DFSPH position update, bit 1 carry cA, bit 2 the
+// learned warm start's history from this step's sums (k_ws_post's job)
 void launch_hash(const DevScene& s, const GridGeom& g, int integrate, int n_old, cudaStream_t st);
 // carry: bit 0 hist, bit 1 cA, bit 2 cB, bit 3 cC (staging -> sorted)
 void launch_scatter_reorder(const DevScene& s, const GridGeom& g, int n_old, int carry, cudaStream_t st);
